@@ -1,0 +1,158 @@
+/*
+ * penguin_b200 -- B200-native (sm_100a) Godunov timestep of the PEnGUIn
+ * protoplanetary-disk code, behind a C ABI.
+ *
+ * Two ways in:
+ *
+ *  1. The drop-in "grid" entry points replace the reference's host functions
+ *     that main.cu's step loop calls, on the caller's own device buffers
+ *     (a struct laid out exactly like the reference's Grid, include/structs.h:122-392):
+ *        pg_grid_global_dt  <- double global_dt(Grid* hst, Grid* dev, double dt)   include/timestep.h:4
+ *        pg_grid_solve      <- void solve(Grid* dev, double time, double dt)        include/solver.h:4
+ *        pg_grid_init_orbadv<- void init_OrbAdv(Grid* dev)                          include/orbit.h:4
+ *     A five-line C++ shim keeps those original names.  The
+ *     reference fixes its parameters at compile time in include/parameters.h;
+ *     here they are passed once through pg_configure().
+ *
+ *  2. The handle API (pg_disk_*) owns its buffers: used by the Python binding,
+ *     the benchmark and the multi-step device-resident loop (CUDA graph).
+ *
+ * Every function returns a pg_status; nothing aborts the process.
+ */
+#ifndef PENGUIN_B200_H
+#define PENGUIN_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    PG_OK = 0,
+    PG_ERR_CONFIG = 1,   /* unsupported or inconsistent parameters / sizes */
+    PG_ERR_CUDA = 2,     /* a CUDA runtime call failed (pg_last_error() has the text) */
+    PG_ERR_NAN = 3,      /* the device error word saw a NaN or non-positive density */
+    PG_ERR_TIMEOUT = 4,  /* a bounded device wait gave up */
+    PG_ERR_ARG = 5       /* null pointer / bad argument */
+} pg_status;
+
+/* One cell, AoS, 5 x FP64 (include/structs.h:48-103). */
+typedef struct { double r, p, u, v, w; } pg_cell;
+/* Dust cell (include/structs.h:19-46). */
+typedef struct { double r, u, v, w; } pg_dust;
+/* Planet (include/structs.h:105-120). */
+typedef struct { double m, a, e, x, y, z, vx, vy, vz, rs; } pg_body;
+
+/*
+ * Runtime copy of include/parameters.h (names kept; see penguin_b200/params.py).
+ * kill_width_out and the dust block are additions: the reference uses
+ * kill_width for both damping zones.
+ */
+typedef struct {
+    int ndim, xres, yres;
+    int geomx, geomy, gridx, gridy;
+    double xmin, xmax, ymin, ymax;
+    int eos_flag, internal_e_flag;
+    double gam, cfl;
+    int bound_lft, bound_rgh, init_flag;
+    double frame_omega;
+    double p_alpha, p_beta, ss_alpha, sc_h, planet_radius;
+    int visc_flag, orbadv_flag, kill_flag;
+    double kill_width, kill_width_out;
+    int n_planet;
+    double planet_mass, planet_ecc, rs_fac, ramp_time;
+    double zmin, zmax;
+    int dust_flag;
+    double stokes, d_g_ratio;
+} pg_params;
+
+/*
+ * Layout twin of the reference's Grid (include/structs.h:122-183).  Only the
+ * members the timestep touches are read: stream, x/y sizes, xa/xv/ya/yv,
+ * orb_rot/orb_res/orb_shf/orb_inc, C, T, vis_tensor, planets.  C and T may be
+ * swapped by pg_grid_solve exactly as the reference swaps them
+ * (src/solver/sweeps.cu:353-355): afterwards C holds the newest state.
+ */
+typedef struct {
+    void* stream; /* cudaStream_t */
+    int xbgn, xres, xarr;
+    int ybgn, yres, yarr;
+    int zbgn, zres, zarr;
+    double *xa, *xv, *ya, *yv, *za, *zv;
+    double *dt, *sum, *Buff;
+    double *orb_rot, *orb_res;
+    int *orb_shf, *orb_inc, *shfL, *shfR;
+    pg_cell *C, *T, *A;
+    pg_dust *CD, *TD;
+    pg_cell *BuffL, *BuffR;
+    pg_dust *BuffLD, *BuffRD;
+    double *vis_tensor, *fx, *fy, *fz, *fx_d, *fy_d, *fz_d, *ext;
+    pg_body* planets;
+} pg_grid;
+
+/* ------------------------------------------------------------ common */
+const char* pg_version(void);
+const char* pg_last_error(void);
+/* Validate a parameter set without touching the GPU. */
+pg_status pg_check_params(const pg_params* P);
+/* Host copy of the grid the library builds (src/init/init.cu:472-500):
+   xa[xres+7], xv[xres+6], ya[yarr+1], yv[yarr]. */
+pg_status pg_make_grid(const pg_params* P, double* xa, double* xv, double* ya, double* yv);
+
+/* ------------------------------------------- drop-in (reference Grid) */
+/* Parameters for the pg_grid_* calls (replaces the compile-time parameters.h). */
+pg_status pg_configure(const pg_params* P);
+/* init_OrbAdv (src/orbit/orbit.cu:51-72,111-120): orb_rot = v_init(r) - r*frame_omega, orb_shf = 0. */
+pg_status pg_grid_init_orbadv(pg_grid* dev);
+/* global_dt (src/timestep/timestep.cu:113-140): blocking; min(CFL dt, 1.1*dt_prev). */
+pg_status pg_grid_global_dt(pg_grid* hst, pg_grid* dev, double dt_prev, double* dt_out);
+/* solve (src/solver/solve.cu:279-292): one Godunov step on dev->C, stream-ordered on dev->stream. */
+pg_status pg_grid_solve(pg_grid* dev, double time, double dt);
+/* Releases the private tables cached for the caller's grids. */
+pg_status pg_grid_release(void);
+
+/* ------------------------------------------------------- handle API */
+typedef struct pg_disk pg_disk;
+
+/* Allocates the state (two AoS buffers), scratch and tables on `device`.
+   stream may be NULL (the library creates one). */
+pg_status pg_disk_create(const pg_params* P, int device, void* stream, pg_disk** out);
+pg_status pg_disk_destroy(pg_disk* d);
+/* Sizes: interior cells and padded array dims. */
+pg_status pg_disk_dims(const pg_disk* d, int* xarr, int* yarr, int* npad);
+/* Restart injection from host arrays (yres x xres, x fastest), like load_grid
+   (src/output/output.cu:182-248): ghosts take init_C, time is set to t.  v may
+   be NULL when ndim == 1.  Also initialises the planet at t (planet.cu:319). */
+pg_status pg_disk_set_state(pg_disk* d, double t, const double* r, const double* p, const double* u,
+                            const double* v);
+/* The newest state back to host arrays; t_out may be NULL. */
+pg_status pg_disk_get_state(pg_disk* d, double* r, double* p, double* u, double* v, double* t_out);
+/* Device pointer of the newest AoS state (xarr*yarr pg_cell) and of the scratch. */
+pg_status pg_disk_state_ptr(pg_disk* d, pg_cell** cells);
+/* global_dt (blocking) and one step with host-supplied t, dt, as in main.cu. */
+pg_status pg_disk_global_dt(pg_disk* d, double dt_prev, double* dt_out);
+pg_status pg_disk_solve(pg_disk* d, double t, double dt);
+/* main.cu's loop on the device: nsteps of (dt = min(CFL dt, 1.1 dt_prev), clipped
+   at end_time; solve; t += dt) with dt and t resident in device memory and the
+   step captured in a CUDA graph.  Stream-ordered; pg_disk_sync waits. */
+pg_status pg_disk_run(pg_disk* d, int nsteps, double end_time);
+pg_status pg_disk_sync(pg_disk* d);
+/* Time, last dt and step count of the device-resident loop (syncs). */
+pg_status pg_disk_clock(pg_disk* d, double* t, double* dt, long long* steps);
+/* Planet state (syncs). */
+pg_status pg_disk_planet(pg_disk* d, pg_body* out);
+/* Device error word: 0 or a pg_status; cleared by the call (syncs). */
+pg_status pg_disk_check(pg_disk* d);
+/* Launch count of the library's own kernels per step (for reporting). */
+int pg_kernels_per_step(const pg_disk* d);
+/* Runs nsteps of the device-resident loop launching the kernels one by one with
+   CUDA events between them on the disk's stream; ms[k] receives the average
+   milliseconds per step of stage k (0 time, 1 kick1, 2 sweep_x, 3 sweep_y,
+   4 advect, 5 kick2; absent stages get 0).  nslot >= 6.  Blocking. */
+pg_status pg_disk_profile(pg_disk* d, int nsteps, double end_time, float* ms, int nslot);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

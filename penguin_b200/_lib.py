@@ -1,0 +1,88 @@
+"""ctypes loader of libpenguin_b200.so (the C ABI of include/penguin_b200.h).
+
+There is no fallback: without the compiled CUDA library every entry point
+raises.  Build it with ``python -m penguin_b200.build``.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+from .params import PGParams
+
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libpenguin_b200.so")
+
+PG_OK, PG_ERR_CONFIG, PG_ERR_CUDA, PG_ERR_NAN, PG_ERR_TIMEOUT, PG_ERR_ARG = range(6)
+STATUS_NAMES = {0: "PG_OK", 1: "PG_ERR_CONFIG", 2: "PG_ERR_CUDA", 3: "PG_ERR_NAN", 4: "PG_ERR_TIMEOUT",
+                5: "PG_ERR_ARG"}
+
+# every symbol declared in include/penguin_b200.h
+EXPORTS = [
+    "pg_version", "pg_last_error", "pg_check_params", "pg_make_grid",
+    "pg_configure", "pg_grid_init_orbadv", "pg_grid_global_dt", "pg_grid_solve", "pg_grid_release",
+    "pg_disk_create", "pg_disk_destroy", "pg_disk_dims", "pg_disk_set_state", "pg_disk_get_state",
+    "pg_disk_state_ptr", "pg_disk_global_dt", "pg_disk_solve", "pg_disk_run", "pg_disk_sync", "pg_disk_clock",
+    "pg_disk_planet", "pg_disk_check", "pg_kernels_per_step", "pg_disk_profile",
+]
+
+
+class PGError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {msg}")
+        self.status = status
+
+
+class PGBody(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_double) for k in ("m", "a", "e", "x", "y", "z", "vx", "vy", "vz", "rs")]
+
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -m penguin_b200.build`")
+    L = ctypes.CDLL(LIB_PATH)
+    vp, dp, ip, i = ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int), ctypes.c_int
+    d = ctypes.c_double
+    PP = ctypes.POINTER(PGParams)
+    sig = {
+        "pg_version": (ctypes.c_char_p, []),
+        "pg_last_error": (ctypes.c_char_p, []),
+        "pg_check_params": (i, [PP]),
+        "pg_make_grid": (i, [PP, dp, dp, dp, dp]),
+        "pg_configure": (i, [PP]),
+        "pg_grid_init_orbadv": (i, [vp]),
+        "pg_grid_global_dt": (i, [vp, vp, d, dp]),
+        "pg_grid_solve": (i, [vp, d, d]),
+        "pg_grid_release": (i, []),
+        "pg_disk_create": (i, [PP, i, vp, ctypes.POINTER(vp)]),
+        "pg_disk_destroy": (i, [vp]),
+        "pg_disk_dims": (i, [vp, ip, ip, ip]),
+        "pg_disk_set_state": (i, [vp, d, dp, dp, dp, dp]),
+        "pg_disk_get_state": (i, [vp, dp, dp, dp, dp, dp]),
+        "pg_disk_state_ptr": (i, [vp, ctypes.POINTER(vp)]),
+        "pg_disk_global_dt": (i, [vp, d, dp]),
+        "pg_disk_solve": (i, [vp, d, d]),
+        "pg_disk_run": (i, [vp, i, d]),
+        "pg_disk_sync": (i, [vp]),
+        "pg_disk_clock": (i, [vp, dp, dp, ctypes.POINTER(ctypes.c_longlong)]),
+        "pg_disk_planet": (i, [vp, ctypes.POINTER(PGBody)]),
+        "pg_disk_check": (i, [vp]),
+        "pg_kernels_per_step": (i, [vp]),
+        "pg_disk_profile": (i, [vp, i, d, ctypes.POINTER(ctypes.c_float), i]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = L
+    return L
+
+
+def check(status: int) -> None:
+    if status != PG_OK:
+        raise PGError(status, lib().pg_last_error().decode())

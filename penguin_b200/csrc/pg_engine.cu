@@ -1,0 +1,911 @@
+// Host side of penguin_b200: grid and table construction, tensor maps, step
+// orchestration, the CUDA-graph device loop and the C ABI of include/penguin_b200.h.
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "pg_common.cuh"
+#include "pg_internal.h"
+
+namespace pg {
+
+static thread_local std::string g_err;
+
+static pg_status fail(pg_status s, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return s;
+}
+
+#define PG_CUDA(call)                                                                          \
+    do {                                                                                       \
+        cudaError_t e_ = (call);                                                               \
+        if (e_ != cudaSuccess)                                                                 \
+            return fail(PG_ERR_CUDA, "%s:%d %s: %s", __FILE__, __LINE__, #call, cudaGetErrorString(e_)); \
+    } while (0)
+
+// ------------------------------------------------------------------ grid
+// src/init/init.cu:472-500 with linspace / logspace of src/geom/geom.cu:22-33
+static void make_grid(double* a, double* v, double amin, double amax, int res, int pad, int geom, int grid) {
+    const int len = res + 1;
+    if (grid == 1) {
+        const double tmp = std::log(amax / amin);
+        for (int i = 0; i < len; i++) a[pad + i] = amin * std::exp(tmp * (double)i / (double)(len - 1));
+    } else {
+        for (int i = 0; i < len; i++) a[pad + i] = amin + (amax - amin) * (double)i / (double)(len - 1);
+    }
+    for (int i = 0; i < pad; i++) {
+        if (grid == 1) {
+            a[i] = amin * std::exp(std::log(amax / amin) * (double)(i - pad) / (double)(res));
+            a[res + pad + 1 + i] = amin * std::exp(std::log(amax / amin) * (double)(res + 1 + i) / (double)(res));
+        } else {
+            a[i] = a[pad] - (a[2 * pad - i] - a[pad]);
+            a[res + pad + 1 + i] = a[res + pad] + (a[res + pad] - a[res + pad - 1 - i]);
+        }
+    }
+    for (int i = 0; i < res + 2 * pad; i++) {
+        const double dr = a[i + 1] - a[i];
+        const double dvdr = (geom == 2) ? a[i] * a[i] + a[i] * dr + dr * dr / 3.0 : (geom == 1 ? a[i] + dr / 2.0 : 1.0);
+        v[i] = dr * dvdr;
+    }
+}
+
+// ------------------------------------------------- reconstruction weights
+// The reference fits, for every cell, the cubic whose (r-weighted for geom 1)
+// averages over 4 consecutive cells match the data, and takes the jump between
+// the cell average and the cubic at the cell's left / right face as the PPM
+// slopes sL / sR (src/solver/recon/recon.cu:216-378, cells i-2..i+1 for sL and
+// i-1..i+2 for sR).  Those slopes are linear in the data with coefficients that
+// depend only on the grid; they are computed here once, in extended precision
+// and in coordinates centred on the cell (where the moments are well
+// conditioned), as weights on the differences of neighbouring averages.
+typedef long double ld;
+
+static ld moment(int geom, ld xc, ld a, ld b, int m) {
+    // integral of w(x) (x - xc)^m over [a, b] with w = 1 (geom 0/3) or x (geom 1), in xi = x - xc
+    const ld A = a - xc, B = b - xc;
+    auto pw = [](ld x, int k) {
+        ld r = 1;
+        for (int i = 0; i < k; ++i) r *= x;
+        return r;
+    };
+    ld s = (pw(B, m + 1) - pw(A, m + 1)) / (m + 1);
+    if (geom == 1) s = (pw(B, m + 2) - pw(A, m + 2)) / (m + 2) + xc * s;
+    return s;
+}
+
+// weights on (a1-a0, a2-a1, a3-a2) of the jump between the average of cell `mid`
+// (of the 4 cells with faces f[0..4]) and the fitted cubic at face f[mid + side]
+static void cubic_jump_weights(int geom, const ld* f, int mid, int side, ld xc, ld* w3) {
+    ld A[4][4];  // A[k][m]: average of xi^m over cell k
+    for (int k = 0; k < 4; ++k) {
+        const ld m0 = moment(geom, xc, f[k], f[k + 1], 0);
+        for (int m = 0; m < 4; ++m) A[k][m] = moment(geom, xc, f[k], f[k + 1], m) / m0;
+    }
+    const ld xf = f[mid + side] - xc;
+    ld wa[4];
+    for (int e = 0; e < 4; ++e) {
+        // solve A c = unit vector e (Gaussian elimination with partial pivoting)
+        ld M[4][5];
+        for (int r = 0; r < 4; ++r) {
+            for (int c = 0; c < 4; ++c) M[r][c] = A[r][c];
+            M[r][4] = (r == e) ? 1 : 0;
+        }
+        for (int c = 0; c < 4; ++c) {
+            int piv = c;
+            for (int r = c + 1; r < 4; ++r)
+                if (fabsl(M[r][c]) > fabsl(M[piv][c])) piv = r;
+            if (piv != c)
+                for (int k = 0; k < 5; ++k) std::swap(M[c][k], M[piv][k]);
+            for (int r = c + 1; r < 4; ++r) {
+                const ld fct = M[r][c] / M[c][c];
+                for (int k = c; k < 5; ++k) M[r][k] -= fct * M[c][k];
+            }
+        }
+        ld cf[4];
+        for (int r = 3; r >= 0; --r) {
+            ld s = M[r][4];
+            for (int k = r + 1; k < 4; ++k) s -= M[r][k] * cf[k];
+            cf[r] = s / M[r][r];
+        }
+        // jump: side 0 -> average - cubic(left face); side 1 -> cubic(right face) - average
+        ld val = 0, avg = 0;
+        for (int m = 0; m < 4; ++m) {
+            ld xm = 1;
+            for (int i = 0; i < m; ++i) xm *= xf;
+            val += cf[m] * xm;
+            avg += cf[m] * A[mid][m];
+        }
+        wa[e] = (side == 0) ? avg - val : val - avg;
+    }
+    // weights on values -> weights on consecutive differences
+    for (int m = 0; m < 3; ++m) {
+        ld s = 0;
+        for (int k = m + 1; k < 4; ++k) s += wa[k];
+        w3[m] = s;
+    }
+}
+
+static void recon_weights(int geom, const double* x, int ncell, double* w) {
+    for (int i = 0; i < ncell; ++i) {
+        double* wi = w + 6 * i;
+        for (int k = 0; k < 6; ++k) wi[k] = 0.0;
+        if (i < 2 || i + 3 > ncell) continue;
+        ld f[6];
+        for (int k = 0; k < 6; ++k) f[k] = (ld)x[i - 2 + k];
+        const ld xc = 0.5L * (f[2] + f[3]);
+        ld w3[3];
+        cubic_jump_weights(geom, f, 2, 0, xc, w3);  // cells i-2..i+1, left face of cell i
+        for (int k = 0; k < 3; ++k) wi[k] = (double)w3[k];
+        cubic_jump_weights(geom, f + 1, 1, 1, xc, w3);  // cells i-1..i+2, right face of cell i
+        for (int k = 0; k < 3; ++k) wi[3 + k] = (double)w3[k];
+    }
+}
+
+// ----------------------------------------------------------- tensor maps
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn encode_fn() {
+    static EncodeTiledFn fn = nullptr;
+    if (!fn) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiledFn>(p);
+    }
+    return fn;
+}
+
+static pg_status make_map(CUtensorMap* m, const void* base, uint64_t inner, uint64_t rows, uint32_t box_inner,
+                          uint32_t box_rows) {
+    EncodeTiledFn fn = encode_fn();
+    if (!fn) return fail(PG_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
+    if (reinterpret_cast<uintptr_t>(base) % 16 != 0 || (inner * 8) % 16 != 0)
+        return fail(PG_ERR_CONFIG, "state rows must be 16-byte aligned (even xres)");
+    cuuint64_t dims[2] = {inner, rows};
+    cuuint64_t strides[1] = {inner * 8};
+    cuuint32_t box[2] = {box_inner, box_rows};
+    cuuint32_t es[2] = {1, 1};
+    CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<void*>(base), dims, strides, box, es,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(PG_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+    return PG_OK;
+}
+
+static pg_status make_cell_maps(CellMaps& M, const Cell* buf, int xarr, int yarr) {
+    if (M.base == buf) return PG_OK;
+    pg_status s;
+    if ((s = make_map(&M.sweep_x, buf, 5ull * xarr, yarr, 5 * 38, 8)) != PG_OK) return s;
+    if ((s = make_map(&M.sweep_y, buf, 5ull * xarr, yarr, 5 * 10, 38)) != PG_OK) return s;
+    if ((s = make_map(&M.stencil, buf, 5ull * xarr, yarr, 5 * 34, 10)) != PG_OK) return s;
+    M.base = buf;
+    return PG_OK;
+}
+
+static pg_status make_vis_maps(VisMaps& M, const double* vis, int xarr, int yarr) {
+    if (M.base == vis) return PG_OK;
+    pg_status s;
+    if ((s = make_map(&M.stencil, vis, 2ull * xarr, yarr, 2 * 34, 10)) != PG_OK) return s;
+    M.base = vis;
+    return PG_OK;
+}
+
+// ---------------------------------------------------------------- engine
+static pg_status check_params(const pg_params* P) {
+    if (!P) return fail(PG_ERR_ARG, "null params");
+    if (P->ndim != 1 && P->ndim != 2) return fail(PG_ERR_CONFIG, "ndim must be 1 or 2");
+    if (P->ndim == 1 && P->yres != 1) return fail(PG_ERR_CONFIG, "ndim 1 needs yres 1");
+    if (P->xres < 2 * NPAD || (P->ndim == 2 && P->yres < 2 * NPAD))
+        return fail(PG_ERR_CONFIG, "resolution below the stencil width");
+    if (P->xres % 2) return fail(PG_ERR_CONFIG, "xres must be even (16-byte aligned rows)");
+    if (P->eos_flag != 0 && P->eos_flag != 2) return fail(PG_ERR_CONFIG, "EOS_flag must be 0 or 2");
+    if ((P->geomx != 0 && P->geomx != 1) || (P->geomy != 0 && P->geomy != 3))
+        return fail(PG_ERR_CONFIG, "supported geometries: geomx 0/1, geomy 0/3");
+    if (P->bound_lft < 0 || P->bound_lft > 2 || P->bound_rgh < 0 || P->bound_rgh > 2)
+        return fail(PG_ERR_CONFIG, "radial boundaries must be 0, 1 or 2");
+    if (P->n_planet != 0 && P->n_planet != 1) return fail(PG_ERR_CONFIG, "n_planet must be 0 or 1");
+    if (P->dust_flag) return fail(PG_ERR_CONFIG, "dust is not supported by this build");
+    if (P->gridx < 0 || P->gridx > 1 || P->gridy != 0) return fail(PG_ERR_CONFIG, "grids: x linear/log, y linear");
+    if (P->gridx == 1 && !(P->xmin > 0.0)) return fail(PG_ERR_CONFIG, "log grid needs xmin > 0");
+    return PG_OK;
+}
+
+struct Engine {
+    pg_params P{};
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    DiskView view{};
+    Scalars* sc = nullptr;
+    Cell* buf[2] = {nullptr, nullptr};
+    bool own_buffers = false;
+    double* vis = nullptr;
+    bool own_vis = false;
+    double* rot = nullptr;
+    double* res = nullptr;
+    int* inc = nullptr;
+    bool own_orb = false;
+    double* grid = nullptr;  // xa | xv | ya | yv (owned mode)
+    double* tab = nullptr;   // weights and per-index tables
+    CellMaps maps[2];
+    VisMaps vmap;
+    int cur = 0;
+    bool fresh = true;       // no step taken since the state was set
+    // device-loop bookkeeping: steps past end_time are no-ops on the device, so the
+    // buffer holding the newest state follows the device's executed-step count
+    bool pending = false;
+    int cur_base = 0;
+    long long steps_base = 0;
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    std::vector<const void*> ghosted;  // buffers whose constant radial ghosts are initialised
+    pg_body* grid_planet = nullptr;    // drop-in mode: the caller's planets array
+
+    ~Engine() {
+        for (auto& g : graph)
+            if (g) cudaGraphExecDestroy(g);
+        if (own_buffers) {
+            cudaFree(buf[0]);
+            cudaFree(buf[1]);
+        }
+        if (own_vis) cudaFree(vis);
+        if (own_orb) {
+            cudaFree(rot);
+            cudaFree(res);
+            cudaFree(inc);
+        }
+        cudaFree(grid);
+        cudaFree(tab);
+        cudaFree(sc);
+        if (own_stream && stream) cudaStreamDestroy(stream);
+    }
+};
+
+// Builds the grid (owned mode) or adopts the caller's device grid, then all tables.
+static pg_status engine_setup(Engine& E, const double* dev_xa, const double* dev_xv, const double* dev_ya,
+                              const double* dev_yv) {
+    const pg_params& P = E.P;
+    const int xarr = P.xres + 2 * NPAD;
+    const int ypad = P.ndim > 1 ? NPAD : 0;
+    const int yarr = P.yres + 2 * ypad;
+    std::vector<double> xa(xarr + 1), xv(xarr), ya(yarr + 1), yv(yarr);
+    make_grid(xa.data(), xv.data(), P.xmin, P.xmax, P.xres, NPAD, P.geomx, P.gridx);
+    make_grid(ya.data(), yv.data(), P.ymin, P.ymax, P.yres, ypad, P.geomy, P.gridy);
+    if (!dev_xa) {
+        PG_CUDA(cudaMalloc(&E.grid, sizeof(double) * (2 * xarr + 2 * yarr + 2)));
+        double* g = E.grid;
+        PG_CUDA(cudaMemcpyAsync(g, xa.data(), sizeof(double) * (xarr + 1), cudaMemcpyHostToDevice, E.stream));
+        PG_CUDA(cudaMemcpyAsync(g + xarr + 1, xv.data(), sizeof(double) * xarr, cudaMemcpyHostToDevice, E.stream));
+        PG_CUDA(cudaMemcpyAsync(g + 2 * xarr + 1, ya.data(), sizeof(double) * (yarr + 1), cudaMemcpyHostToDevice, E.stream));
+        PG_CUDA(cudaMemcpyAsync(g + 2 * xarr + yarr + 2, yv.data(), sizeof(double) * yarr, cudaMemcpyHostToDevice, E.stream));
+        dev_xa = g;
+        dev_xv = g + xarr + 1;
+        dev_ya = g + 2 * xarr + 1;
+        dev_yv = g + 2 * xarr + yarr + 2;
+    } else {
+        // the caller built its grid with the same routine on its host; read it back so
+        // the weights are computed from exactly those faces
+        PG_CUDA(cudaMemcpyAsync(xa.data(), dev_xa, sizeof(double) * (xarr + 1), cudaMemcpyDeviceToHost, E.stream));
+        PG_CUDA(cudaMemcpyAsync(ya.data(), dev_ya, sizeof(double) * (yarr + 1), cudaMemcpyDeviceToHost, E.stream));
+        PG_CUDA(cudaStreamSynchronize(E.stream));
+    }
+    // tables: wx[6 xarr] wy[6 yarr] radx cs2x nux initx(5) killx(4) [xarr each] ycraw ycj [yarr each]
+    const size_t ntab = 6 * (size_t)xarr + 6 * (size_t)yarr + 12 * (size_t)xarr + 2 * (size_t)yarr;
+    PG_CUDA(cudaMalloc(&E.tab, sizeof(double) * ntab));
+    std::vector<double> wx(6 * xarr), wy(6 * yarr);
+    recon_weights(P.geomx, xa.data(), xarr, wx.data());
+    recon_weights(P.geomy, ya.data(), yarr, wy.data());
+    PG_CUDA(cudaMemcpyAsync(E.tab, wx.data(), sizeof(double) * wx.size(), cudaMemcpyHostToDevice, E.stream));
+    PG_CUDA(cudaMemcpyAsync(E.tab + 6 * xarr, wy.data(), sizeof(double) * wy.size(), cudaMemcpyHostToDevice, E.stream));
+    PG_CUDA(cudaStreamSynchronize(E.stream));  // host vectors go out of scope
+
+    if (!E.sc) PG_CUDA(cudaMalloc(&E.sc, sizeof(Scalars)));
+    PG_CUDA(cudaMemsetAsync(E.sc, 0, sizeof(Scalars), E.stream));
+
+    DiskView& d = E.view;
+    d.xres = P.xres;
+    d.yres = P.yres;
+    d.xarr = xarr;
+    d.yarr = yarr;
+    d.ypad = ypad;
+    d.ndim = P.ndim;
+    d.geomx = P.geomx;
+    d.geomy = P.geomy;
+    d.eos = P.eos_flag;
+    d.ie = P.internal_e_flag;
+    d.bound_lft = P.bound_lft;
+    d.bound_rgh = P.bound_rgh;
+    d.visc = P.visc_flag && P.ndim == 2;
+    d.orbadv = P.orbadv_flag && P.ndim == 2;
+    d.kill = P.kill_flag;
+    d.nplanet = P.n_planet;
+    d.gam = P.gam;
+    d.cfl = P.cfl;
+    d.frame_omega = P.frame_omega;
+    d.dy0 = (P.ymax - P.ymin) / (double)P.yres;
+    d.planet_mass = P.planet_mass;
+    d.ramp_time = P.ramp_time;
+    d.xa = dev_xa;
+    d.xv = dev_xv;
+    d.ya = dev_ya;
+    d.yv = dev_yv;
+    d.wx = E.tab;
+    d.wy = E.tab + 6 * xarr;
+    double* t = E.tab + 6 * xarr + 6 * yarr;
+    d.radx = t;
+    d.cs2x = t + xarr;
+    d.nux = t + 2 * xarr;
+    d.initx = t + 3 * xarr;
+    d.killx = t + 8 * xarr;
+    d.ycraw = t + 12 * xarr;
+    d.ycj = t + 12 * xarr + yarr;
+    d.rot = E.rot;
+    d.res = E.res;
+    d.inc = E.inc;
+    d.sc = E.sc;
+    launch_init_tables(d, P, t, E.stream);
+    PG_CUDA(cudaGetLastError());
+    return PG_OK;
+}
+
+static pg_status ensure_ghosts(Engine& E, Cell* b) {
+    for (const void* p : E.ghosted)
+        if (p == b) return PG_OK;
+    launch_init_xghosts(E.view, b, E.stream);
+    PG_CUDA(cudaGetLastError());
+    E.ghosted.push_back(b);
+    return PG_OK;
+}
+
+static int passes_per_step(const DiskView& d) {
+    return 3 + (d.ndim > 1 ? 1 : 0) + (d.ndim > 1 && d.orbadv ? 1 : 0);
+}
+
+// Resolves which buffer holds the newest state after device-loop launches.
+static pg_status resolve_cur(Engine& E) {
+    if (!E.pending) return PG_OK;
+    long long steps = 0;
+    PG_CUDA(cudaMemcpyAsync(&steps, &E.sc->steps, sizeof(steps), cudaMemcpyDeviceToHost, E.stream));
+    PG_CUDA(cudaStreamSynchronize(E.stream));
+    const long long flips = (passes_per_step(E.view) % 2) ? (steps - E.steps_base) : 0;
+    E.cur = (int)((E.cur_base + flips) & 1);
+    E.pending = false;
+    return PG_OK;
+}
+
+// Kernels of one step after the time kernel; in = E.cur.
+static pg_status enqueue_stages(Engine& E) {
+    const DiskView& d = E.view;
+    pg_status s;
+    int c = E.cur;
+    auto maps = [&](int k) -> const CellMaps& { return E.maps[k]; };
+    for (int k = 0; k < 2; ++k)
+        if ((s = make_cell_maps(E.maps[k], E.buf[k], d.xarr, d.yarr)) != PG_OK) return s;
+    if (d.visc && (s = make_vis_maps(E.vmap, E.vis, d.xarr, d.yarr)) != PG_OK) return s;
+    launch_kick1(d, maps(c), E.buf[1 - c], E.vis, E.stream);
+    c = 1 - c;
+    launch_sweep_x(d, maps(c), E.buf[1 - c], E.stream);
+    c = 1 - c;
+    if (d.ndim > 1) {
+        launch_sweep_y(d, maps(c), E.buf[1 - c], E.stream);
+        c = 1 - c;
+    }
+    if (d.ndim > 1 && d.orbadv) {
+        launch_advect(d, maps(c), E.buf[1 - c], E.stream);
+        c = 1 - c;
+    }
+    launch_kick2(d, maps(c), E.vmap, E.buf[1 - c], E.stream);
+    c = 1 - c;
+    E.cur = c;
+    PG_CUDA(cudaGetLastError());
+    return PG_OK;
+}
+
+static pg_status engine_create(const pg_params* P, int device, void* stream, Engine** out) {
+    pg_status s = check_params(P);
+    if (s != PG_OK) return s;
+    PG_CUDA(cudaSetDevice(device));
+    static bool attrs = false;
+    if (!attrs) {
+        PG_CUDA(set_kernel_attributes());
+        attrs = true;
+    }
+    Engine* E = new Engine();
+    E->P = *P;
+    if (E->P.kill_width_out <= 0.0) E->P.kill_width_out = E->P.kill_width;
+    E->device = device;
+    if (stream) E->stream = (cudaStream_t)stream;
+    else {
+        cudaError_t e = cudaStreamCreateWithFlags(&E->stream, cudaStreamNonBlocking);
+        if (e != cudaSuccess) {
+            delete E;
+            return fail(PG_ERR_CUDA, "cudaStreamCreate: %s", cudaGetErrorString(e));
+        }
+        E->own_stream = true;
+    }
+    *out = E;
+    return PG_OK;
+}
+
+__global__ void k_fill(const DiskView d, Cell* buf, const double* r, const double* p, const double* u,
+                       const double* v) {
+    // fill_grid (src/init/init.cu:502-519) then load_grid's interior fields (src/output/output.cu:197-243)
+    const long long n = (long long)d.xarr * d.yarr;
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(k % d.xarr), j = (int)(k / d.xarr);
+        const double* I = d.initx + 5 * i;
+        Cell c{I[0], I[1], I[2], I[3], I[4]};
+        if (i >= NPAD && i < NPAD + d.xres && j >= d.ypad && j < d.ypad + d.yres) {
+            const size_t m = (size_t)(i - NPAD) + (size_t)d.xres * (j - d.ypad);
+            c.r = r[m];
+            c.p = p[m];
+            c.u = u[m];
+            if (v) c.v = v[m];
+        }
+        store_cell(buf, d.xarr, i, j, c);
+    }
+}
+
+__global__ void k_extract(const DiskView d, const Cell* buf, double* r, double* p, double* u, double* v) {
+    const long long n = (long long)d.xres * d.yres;
+    for (long long m = blockIdx.x * (long long)blockDim.x + threadIdx.x; m < n; m += (long long)gridDim.x * blockDim.x) {
+        const int i = NPAD + (int)(m % d.xres), j = d.ypad + (int)(m / d.xres);
+        const Cell c = load_cell(buf, d.xarr, i, j);
+        r[m] = c.r;
+        p[m] = c.p;
+        u[m] = c.u;
+        v[m] = c.v;
+    }
+}
+
+__global__ void k_grid_planet_in(Scalars* sc, const pg_body* planets) { sc->planet_next = planets[0]; }
+__global__ void k_grid_planet_out(const Scalars* sc, pg_body* planets) { planets[0] = sc->planet_next; }
+
+}  // namespace pg
+
+// ======================================================================
+//                                C ABI
+// ======================================================================
+using namespace pg;
+
+struct pg_disk {
+    Engine* E;
+};
+
+extern "C" {
+
+const char* pg_version(void) { return "penguin_b200 0.1 (sm_100a, FP64 Godunov step)"; }
+const char* pg_last_error(void) { return g_err.c_str(); }
+
+pg_status pg_check_params(const pg_params* P) { return check_params(P); }
+
+pg_status pg_make_grid(const pg_params* P, double* xa, double* xv, double* ya, double* yv) {
+    pg_status s = check_params(P);
+    if (s != PG_OK) return s;
+    if (!xa || !xv || !ya || !yv) return fail(PG_ERR_ARG, "null output");
+    const int ypad = P->ndim > 1 ? NPAD : 0;
+    make_grid(xa, xv, P->xmin, P->xmax, P->xres, NPAD, P->geomx, P->gridx);
+    make_grid(ya, yv, P->ymin, P->ymax, P->yres, ypad, P->geomy, P->gridy);
+    return PG_OK;
+}
+
+// ---------------------------------------------------------- handle API
+pg_status pg_disk_create(const pg_params* P, int device, void* stream, pg_disk** out) {
+    if (!out) return fail(PG_ERR_ARG, "null out");
+    *out = nullptr;
+    Engine* E = nullptr;
+    pg_status s = engine_create(P, device, stream, &E);
+    if (s != PG_OK) return s;
+    const int xarr = E->P.xres + 2 * NPAD;
+    const int yarr = E->P.yres + 2 * (E->P.ndim > 1 ? NPAD : 0);
+    const size_t n = (size_t)xarr * yarr;
+    auto bail = [&](pg_status st) {
+        delete E;
+        return st;
+    };
+    cudaError_t e;
+    if ((e = cudaMalloc(&E->buf[0], n * sizeof(Cell))) != cudaSuccess ||
+        (e = cudaMalloc(&E->buf[1], n * sizeof(Cell))) != cudaSuccess ||
+        (e = cudaMalloc(&E->vis, 2 * n * sizeof(double))) != cudaSuccess ||
+        (e = cudaMalloc(&E->rot, xarr * sizeof(double))) != cudaSuccess ||
+        (e = cudaMalloc(&E->res, xarr * sizeof(double))) != cudaSuccess ||
+        (e = cudaMalloc(&E->inc, xarr * sizeof(int))) != cudaSuccess)
+        return bail(fail(PG_ERR_CUDA, "cudaMalloc: %s", cudaGetErrorString(e)));
+    E->own_buffers = E->own_vis = E->own_orb = true;
+    cudaMemsetAsync(E->buf[0], 0, n * sizeof(Cell), E->stream);
+    cudaMemsetAsync(E->buf[1], 0, n * sizeof(Cell), E->stream);
+    cudaMemsetAsync(E->vis, 0, 2 * n * sizeof(double), E->stream);
+    cudaMemsetAsync(E->res, 0, xarr * sizeof(double), E->stream);
+    cudaMemsetAsync(E->inc, 0, xarr * sizeof(int), E->stream);
+    if ((s = engine_setup(*E, nullptr, nullptr, nullptr, nullptr)) != PG_OK) return bail(s);
+    if ((s = ensure_ghosts(*E, E->buf[0])) != PG_OK) return bail(s);
+    if ((s = ensure_ghosts(*E, E->buf[1])) != PG_OK) return bail(s);
+    pg_disk* d = new pg_disk{E};
+    *out = d;
+    return PG_OK;
+}
+
+pg_status pg_disk_destroy(pg_disk* d) {
+    if (!d) return PG_OK;
+    cudaSetDevice(d->E->device);
+    cudaStreamSynchronize(d->E->stream);
+    delete d->E;
+    delete d;
+    return PG_OK;
+}
+
+pg_status pg_disk_dims(const pg_disk* d, int* xarr, int* yarr, int* npad) {
+    if (!d) return fail(PG_ERR_ARG, "null disk");
+    if (xarr) *xarr = d->E->view.xarr;
+    if (yarr) *yarr = d->E->view.yarr;
+    if (npad) *npad = NPAD;
+    return PG_OK;
+}
+
+pg_status pg_disk_set_state(pg_disk* dk, double t, const double* r, const double* p, const double* u,
+                            const double* v) {
+    if (!dk || !r || !p || !u) return fail(PG_ERR_ARG, "null argument");
+    Engine& E = *dk->E;
+    const DiskView& d = E.view;
+    PG_CUDA(cudaSetDevice(E.device));
+    const size_t n = (size_t)d.xres * d.yres;
+    double* stage = nullptr;
+    PG_CUDA(cudaMallocAsync(&stage, 4 * n * sizeof(double), E.stream));
+    PG_CUDA(cudaMemcpyAsync(stage, r, n * sizeof(double), cudaMemcpyHostToDevice, E.stream));
+    PG_CUDA(cudaMemcpyAsync(stage + n, p, n * sizeof(double), cudaMemcpyHostToDevice, E.stream));
+    PG_CUDA(cudaMemcpyAsync(stage + 2 * n, u, n * sizeof(double), cudaMemcpyHostToDevice, E.stream));
+    if (v) PG_CUDA(cudaMemcpyAsync(stage + 3 * n, v, n * sizeof(double), cudaMemcpyHostToDevice, E.stream));
+    E.cur = 0;
+    E.pending = false;
+    k_fill<<<1184, 256, 0, E.stream>>>(d, E.buf[0], stage, stage + n, stage + 2 * n, v ? stage + 3 * n : nullptr);
+    PG_CUDA(cudaGetLastError());
+    PG_CUDA(cudaFreeAsync(stage, E.stream));
+    launch_bound(d, E.buf[0], E.stream);
+    launch_init_planet(d, E.P, t, E.stream);
+    launch_cfl(d, E.buf[0], E.stream);
+    PG_CUDA(cudaGetLastError());
+    Scalars h{};
+    PG_CUDA(cudaMemcpyAsync(&h, E.sc, sizeof(Scalars), cudaMemcpyDeviceToHost, E.stream));
+    PG_CUDA(cudaStreamSynchronize(E.stream));
+    h.t = t;
+    h.dt = 0.0;
+    h.dt_prev = 0.0;
+    h.steps = 0;
+    h.done = 0;
+    h.pad_ = 0;
+    h.err = 0;
+    h.floor_hits = 0;
+    PG_CUDA(cudaMemcpyAsync(E.sc, &h, sizeof(Scalars), cudaMemcpyHostToDevice, E.stream));
+    PG_CUDA(cudaStreamSynchronize(E.stream));
+    E.fresh = true;
+    return PG_OK;
+}
+
+pg_status pg_disk_get_state(pg_disk* dk, double* r, double* p, double* u, double* v, double* t_out) {
+    if (!dk || !r || !p || !u) return fail(PG_ERR_ARG, "null argument");
+    Engine& E = *dk->E;
+    const DiskView& d = E.view;
+    PG_CUDA(cudaSetDevice(E.device));
+    const size_t n = (size_t)d.xres * d.yres;
+    double* stage = nullptr;
+    PG_CUDA(cudaMallocAsync(&stage, 4 * n * sizeof(double), E.stream));
+    pg_status s0 = resolve_cur(E);
+    if (s0 != PG_OK) return s0;
+    k_extract<<<1184, 256, 0, E.stream>>>(d, E.buf[E.cur], stage, stage + n, stage + 2 * n, stage + 3 * n);
+    PG_CUDA(cudaGetLastError());
+    PG_CUDA(cudaMemcpyAsync(r, stage, n * sizeof(double), cudaMemcpyDeviceToHost, E.stream));
+    PG_CUDA(cudaMemcpyAsync(p, stage + n, n * sizeof(double), cudaMemcpyDeviceToHost, E.stream));
+    PG_CUDA(cudaMemcpyAsync(u, stage + 2 * n, n * sizeof(double), cudaMemcpyDeviceToHost, E.stream));
+    if (v) PG_CUDA(cudaMemcpyAsync(v, stage + 3 * n, n * sizeof(double), cudaMemcpyDeviceToHost, E.stream));
+    PG_CUDA(cudaFreeAsync(stage, E.stream));
+    if (t_out) PG_CUDA(cudaMemcpyAsync(t_out, &E.sc->t, sizeof(double), cudaMemcpyDeviceToHost, E.stream));
+    PG_CUDA(cudaStreamSynchronize(E.stream));
+    return PG_OK;
+}
+
+pg_status pg_disk_state_ptr(pg_disk* dk, pg_cell** cells) {
+    if (!dk || !cells) return fail(PG_ERR_ARG, "null argument");
+    pg_status s0 = resolve_cur(*dk->E);
+    if (s0 != PG_OK) return s0;
+    *cells = reinterpret_cast<pg_cell*>(dk->E->buf[dk->E->cur]);
+    return PG_OK;
+}
+
+pg_status pg_disk_global_dt(pg_disk* dk, double dt_prev, double* dt_out) {
+    if (!dk || !dt_out) return fail(PG_ERR_ARG, "null argument");
+    Engine& E = *dk->E;
+    unsigned long long bits = 0;
+    PG_CUDA(cudaMemcpyAsync(&bits, &E.sc->vmax_bits, sizeof(bits), cudaMemcpyDeviceToHost, E.stream));
+    PG_CUDA(cudaStreamSynchronize(E.stream));
+    double vmax;
+    std::memcpy(&vmax, &bits, sizeof vmax);
+    const double dt = E.P.cfl / vmax;  // get_dt_lv2 (timestep.cu:108)
+    double tmp = dt_prev * 1.1;        // timestep.cu:133-139
+    if (dt < tmp) tmp = dt;
+    *dt_out = tmp;
+    return PG_OK;
+}
+
+pg_status pg_disk_solve(pg_disk* dk, double t, double dt) {
+    if (!dk) return fail(PG_ERR_ARG, "null disk");
+    Engine& E = *dk->E;
+    PG_CUDA(cudaSetDevice(E.device));
+    pg_status s0 = resolve_cur(E);
+    if (s0 != PG_OK) return s0;
+    launch_set_time(E.view, t, dt, E.stream);
+    pg_status s = enqueue_stages(E);
+    E.fresh = false;
+    return s;
+}
+
+pg_status pg_disk_run(pg_disk* dk, int nsteps, double end_time) {
+    if (!dk) return fail(PG_ERR_ARG, "null disk");
+    if (nsteps <= 0) return PG_OK;
+    Engine& E = *dk->E;
+    PG_CUDA(cudaSetDevice(E.device));
+    // main.cu:144 + 322: the first cap on dt is end_time - t after a (re)start
+    pg_status s0 = resolve_cur(E);
+    if (s0 != PG_OK) return s0;
+    Scalars h{};
+    PG_CUDA(cudaMemcpyAsync(&h, E.sc, sizeof(Scalars), cudaMemcpyDeviceToHost, E.stream));
+    PG_CUDA(cudaStreamSynchronize(E.stream));
+    if (E.fresh) h.dt_prev = end_time - h.t;
+    h.end_time = end_time;
+    h.done = 0;
+    h.pad_ = 0;
+    PG_CUDA(cudaMemcpyAsync(E.sc, &h, sizeof(Scalars), cudaMemcpyHostToDevice, E.stream));
+    E.fresh = false;
+    E.cur_base = E.cur;
+    E.steps_base = h.steps;
+    E.pending = true;
+    for (int k = 0; k < 2; ++k) {
+        pg_status s = make_cell_maps(E.maps[k], E.buf[k], E.view.xarr, E.view.yarr);
+        if (s != PG_OK) return s;
+    }
+    // with a finite end_time the device may finish early: check its done flag
+    // every 256 launched steps so the host does not keep launching no-op steps
+    const bool may_finish = end_time < 1.0e29;
+    for (int step = 0; step < nsteps; ++step) {
+        if (may_finish && step > 0 && step % 256 == 0) {
+            int done = 0;
+            PG_CUDA(cudaMemcpyAsync(&done, &E.sc->done, sizeof(int), cudaMemcpyDeviceToHost, E.stream));
+            PG_CUDA(cudaStreamSynchronize(E.stream));
+            if (done) break;
+        }
+        const int c0 = E.cur;
+        if (!E.graph[c0]) {
+            // capture one step (time kernel + stages) starting from buffer c0
+            cudaGraph_t g;
+            PG_CUDA(cudaStreamBeginCapture(E.stream, cudaStreamCaptureModeThreadLocal));
+            launch_time_step(E.view, E.stream);
+            pg_status s = enqueue_stages(E);
+            cudaError_t ce = cudaStreamEndCapture(E.stream, &g);
+            if (s != PG_OK) return s;
+            PG_CUDA(ce);
+            PG_CUDA(cudaGraphInstantiate(&E.graph[c0], g, 0));
+            cudaGraphDestroy(g);
+            E.cur = c0;
+        }
+        PG_CUDA(cudaGraphLaunch(E.graph[c0], E.stream));
+        // the captured step leaves the newest state in the other buffer iff it has an
+        // odd number of passes (if the device actually ran it: see resolve_cur)
+        E.cur = (passes_per_step(E.view) % 2) ? 1 - c0 : c0;
+    }
+    if (!may_finish) {  // every launched step ran: the index above is exact
+        E.pending = false;
+    } else {
+        E.cur = E.cur_base;  // resolved from the device step count on next use
+    }
+    return PG_OK;
+}
+
+pg_status pg_disk_sync(pg_disk* dk) {
+    if (!dk) return fail(PG_ERR_ARG, "null disk");
+    PG_CUDA(cudaStreamSynchronize(dk->E->stream));
+    return PG_OK;
+}
+
+pg_status pg_disk_clock(pg_disk* dk, double* t, double* dt, long long* steps) {
+    if (!dk) return fail(PG_ERR_ARG, "null disk");
+    Scalars h{};
+    PG_CUDA(cudaMemcpyAsync(&h, dk->E->sc, sizeof(Scalars), cudaMemcpyDeviceToHost, dk->E->stream));
+    PG_CUDA(cudaStreamSynchronize(dk->E->stream));
+    if (t) *t = h.t;
+    if (dt) *dt = h.dt;
+    if (steps) *steps = h.steps;
+    return PG_OK;
+}
+
+pg_status pg_disk_planet(pg_disk* dk, pg_body* out) {
+    if (!dk || !out) return fail(PG_ERR_ARG, "null argument");
+    Scalars h{};
+    PG_CUDA(cudaMemcpyAsync(&h, dk->E->sc, sizeof(Scalars), cudaMemcpyDeviceToHost, dk->E->stream));
+    PG_CUDA(cudaStreamSynchronize(dk->E->stream));
+    *out = h.planet_next;
+    return PG_OK;
+}
+
+pg_status pg_disk_check(pg_disk* dk) {
+    if (!dk) return fail(PG_ERR_ARG, "null disk");
+    int err = 0;
+    PG_CUDA(cudaMemcpyAsync(&err, &dk->E->sc->err, sizeof(int), cudaMemcpyDeviceToHost, dk->E->stream));
+    PG_CUDA(cudaStreamSynchronize(dk->E->stream));
+    const int zero = 0;
+    PG_CUDA(cudaMemcpy(&dk->E->sc->err, &zero, sizeof(int), cudaMemcpyHostToDevice));
+    if (err & (1 << PG_ERR_TIMEOUT)) return fail(PG_ERR_TIMEOUT, "a device wait timed out");
+    if (err & (1 << PG_ERR_NAN)) return fail(PG_ERR_NAN, "non-positive or NaN density produced");
+    return PG_OK;
+}
+
+int pg_kernels_per_step(const pg_disk* dk) { return dk ? kernels_per_step(dk->E->view) : 0; }
+
+pg_status pg_disk_profile(pg_disk* dk, int nsteps, double end_time, float* ms, int nslot) {
+    if (!dk || !ms || nslot < 6) return fail(PG_ERR_ARG, "bad argument");
+    Engine& E = *dk->E;
+    const DiskView& d = E.view;
+    PG_CUDA(cudaSetDevice(E.device));
+    for (int k = 0; k < nslot; ++k) ms[k] = 0.0f;
+    pg_status s0 = resolve_cur(E);
+    if (s0 != PG_OK) return s0;
+    Scalars h{};
+    PG_CUDA(cudaMemcpyAsync(&h, E.sc, sizeof(Scalars), cudaMemcpyDeviceToHost, E.stream));
+    PG_CUDA(cudaStreamSynchronize(E.stream));
+    if (E.fresh) h.dt_prev = end_time - h.t;
+    h.end_time = end_time;
+    h.done = 0;
+    h.pad_ = 0;
+    PG_CUDA(cudaMemcpyAsync(E.sc, &h, sizeof(Scalars), cudaMemcpyHostToDevice, E.stream));
+    E.fresh = false;
+    pg_status s;
+    for (int k = 0; k < 2; ++k)
+        if ((s = make_cell_maps(E.maps[k], E.buf[k], d.xarr, d.yarr)) != PG_OK) return s;
+    if (d.visc && (s = make_vis_maps(E.vmap, E.vis, d.xarr, d.yarr)) != PG_OK) return s;
+    cudaEvent_t ev[7];
+    for (auto& x : ev) PG_CUDA(cudaEventCreate(&x));
+    for (int step = 0; step < nsteps; ++step) {
+        int c = E.cur;
+        PG_CUDA(cudaEventRecord(ev[0], E.stream));
+        launch_time_step(d, E.stream);
+        PG_CUDA(cudaEventRecord(ev[1], E.stream));
+        launch_kick1(d, E.maps[c], E.buf[1 - c], E.vis, E.stream);
+        c = 1 - c;
+        PG_CUDA(cudaEventRecord(ev[2], E.stream));
+        launch_sweep_x(d, E.maps[c], E.buf[1 - c], E.stream);
+        c = 1 - c;
+        PG_CUDA(cudaEventRecord(ev[3], E.stream));
+        if (d.ndim > 1) {
+            launch_sweep_y(d, E.maps[c], E.buf[1 - c], E.stream);
+            c = 1 - c;
+        }
+        PG_CUDA(cudaEventRecord(ev[4], E.stream));
+        if (d.ndim > 1 && d.orbadv) {
+            launch_advect(d, E.maps[c], E.buf[1 - c], E.stream);
+            c = 1 - c;
+        }
+        PG_CUDA(cudaEventRecord(ev[5], E.stream));
+        launch_kick2(d, E.maps[c], E.vmap, E.buf[1 - c], E.stream);
+        c = 1 - c;
+        PG_CUDA(cudaEventRecord(ev[6], E.stream));
+        PG_CUDA(cudaGetLastError());
+        E.cur = c;
+        PG_CUDA(cudaEventSynchronize(ev[6]));
+        for (int k = 0; k < 6; ++k) {
+            float t = 0.0f;
+            PG_CUDA(cudaEventElapsedTime(&t, ev[k], ev[k + 1]));
+            ms[k] += t / (float)nsteps;
+        }
+    }
+    for (auto& x : ev) cudaEventDestroy(x);
+    return PG_OK;
+}
+
+// ------------------------------------------------------ drop-in (Grid)
+static std::mutex g_mu;
+static pg_params g_params;
+static bool g_configured = false;
+static std::map<const double*, Engine*> g_grids;  // keyed by the caller's device xa
+
+pg_status pg_configure(const pg_params* P) {
+    pg_status s = check_params(P);
+    if (s != PG_OK) return s;
+    std::lock_guard<std::mutex> lk(g_mu);
+    g_params = *P;
+    g_configured = true;
+    return PG_OK;
+}
+
+static pg_status grid_engine(pg_grid* dev, Engine** out) {
+    if (!dev) return fail(PG_ERR_ARG, "null grid");
+    if (!g_configured) return fail(PG_ERR_CONFIG, "pg_configure was not called");
+    if (dev->xres != g_params.xres || dev->yres != g_params.yres)
+        return fail(PG_ERR_CONFIG, "grid dimensions differ from the configured parameters");
+    if (dev->xbgn != 0) return fail(PG_ERR_CONFIG, "radial domain decomposition is not supported");
+    std::lock_guard<std::mutex> lk(g_mu);
+    auto it = g_grids.find(dev->xa);
+    if (it != g_grids.end()) {
+        *out = it->second;
+        return PG_OK;
+    }
+    int device = 0;
+    PG_CUDA(cudaGetDevice(&device));
+    Engine* E = nullptr;
+    pg_status s = engine_create(&g_params, device, dev->stream, &E);
+    if (s != PG_OK) return s;
+    E->rot = dev->orb_rot;
+    E->res = dev->orb_res;
+    E->inc = dev->orb_inc;
+    E->vis = dev->vis_tensor;
+    if ((s = engine_setup(*E, dev->xa, dev->xv, dev->ya, dev->yv)) != PG_OK) {
+        delete E;
+        return s;
+    }
+    g_grids[dev->xa] = E;
+    *out = E;
+    return PG_OK;
+}
+
+pg_status pg_grid_init_orbadv(pg_grid* dev) {
+    Engine* E = nullptr;
+    pg_status s = grid_engine(dev, &E);
+    if (s != PG_OK) return s;
+    // orb_rot was written by the table kernel of engine_setup; orb_shf starts at 0
+    if (dev->orb_shf) PG_CUDA(cudaMemsetAsync(dev->orb_shf, 0, sizeof(int) * dev->xarr * dev->zarr, E->stream));
+    PG_CUDA(cudaStreamSynchronize(E->stream));
+    return PG_OK;
+}
+
+pg_status pg_grid_global_dt(pg_grid* hst, pg_grid* dev, double dt_prev, double* dt_out) {
+    (void)hst;
+    if (!dt_out) return fail(PG_ERR_ARG, "null dt_out");
+    Engine* E = nullptr;
+    pg_status s = grid_engine(dev, &E);
+    if (s != PG_OK) return s;
+    launch_cfl(E->view, reinterpret_cast<Cell*>(dev->C), E->stream);
+    PG_CUDA(cudaGetLastError());
+    pg_disk tmp{E};
+    return pg_disk_global_dt(&tmp, dt_prev, dt_out);
+}
+
+pg_status pg_grid_solve(pg_grid* dev, double time, double dt) {
+    Engine* E = nullptr;
+    pg_status s = grid_engine(dev, &E);
+    if (s != PG_OK) return s;
+    E->buf[0] = reinterpret_cast<Cell*>(dev->C);
+    E->buf[1] = reinterpret_cast<Cell*>(dev->T);
+    E->cur = 0;
+    if ((s = ensure_ghosts(*E, E->buf[1])) != PG_OK) return s;
+    // the caller may have written the state: refresh the ghost images first
+    launch_bound(E->view, E->buf[0], E->stream);
+    if (E->view.nplanet > 0 && dev->planets) k_grid_planet_in<<<1, 1, 0, E->stream>>>(E->sc, dev->planets);
+    launch_set_time(E->view, time, dt, E->stream);
+    if ((s = enqueue_stages(*E)) != PG_OK) return s;
+    if (E->view.nplanet > 0 && dev->planets) k_grid_planet_out<<<1, 1, 0, E->stream>>>(E->sc, dev->planets);
+    PG_CUDA(cudaGetLastError());
+    if (E->cur == 1) {  // newest state in T: swap like the reference (src/solver/sweeps.cu:353-355)
+        pg_cell* t = dev->C;
+        dev->C = dev->T;
+        dev->T = t;
+    }
+    return PG_OK;
+}
+
+pg_status pg_grid_release(void) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    for (auto& kv : g_grids) delete kv.second;
+    g_grids.clear();
+    return PG_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,1010 @@
+// penguin_b200 kernels for sm_100a: one Godunov timestep of PEnGUIn
+// (src/solver/solve.cu:212-292) as five fused passes over the AoS state:
+//
+//   kick1   C -> T : viscous stress (src/viscosity/viscosity.cu:34-197) + first half-kick
+//                    (src/solver/sweeps.cu:597-711, mdt = 0); stores the stress for kick2
+//   sweep_x T -> C : radial Godunov sweep (src/solver/sweeps.cu:263-335)
+//   sweep_y C -> T : azimuthal sweep (sweeps.cu:361-433) writing each cell at its
+//                    orbital-advection shifted row (src/orbit/orbit.cu:17-99)
+//   advect  T -> C : residual orbital advection (src/solver/advection/advection.cu:1-173)
+//   kick2   C -> T : predictor kick, viscous stress of the predicted state and
+//                    corrector kick (solve.cu:266-269), wave damping
+//                    (src/killwave/killwave.cu:17-103) and the CFL signal speed
+//                    for the next step (src/timestep/timestep.cu:18-97)
+//
+// plus a one-thread time kernel (dt, planet).  Every pass reads its tile with a
+// TMA bulk tensor copy into shared memory and writes each cell together with its
+// ghost images, so no separate boundary pass is needed between stages.
+#include <cstdio>
+
+#include "pg_common.cuh"
+#include "pg_hydro.cuh"
+#include "pg_internal.h"
+
+namespace pg {
+
+// ---------------------------------------------------------------- tiles
+constexpr int SW_LEN = 32;                  // outputs along the sweep per CTA
+constexpr int SW_W = 8;                     // pencils per CTA
+constexpr int SW_TL = SW_LEN + 2 * NPAD;    // 38 tile cells along the sweep
+constexpr int SW_P1 = SW_LEN + 2;           // cells reconstructed per pencil
+constexpr int SW_P2 = SW_LEN + 1;           // faces per pencil
+constexpr int SW_THREADS = 288;             // >= SW_P1 * SW_W
+constexpr int SWY_COLS = SW_W + 2;          // y tiles start one column early (16-B aligned TMA x)
+constexpr int SWX_TILE = SW_W * SW_TL * 5;  // doubles
+constexpr int SWY_TILE = SW_TL * SWY_COLS * 5;
+constexpr int SW_TILE_MAX = (SWY_TILE + 15) / 16 * 16;
+constexpr int SW_NST = SW_P1 * SW_W;        // 272 reconstructed cells
+constexpr int SW_NFX = SW_P2 * SW_W;        // 264 faces
+constexpr size_t SW_SMEM = (size_t)(SW_TILE_MAX + 10 * SW_NST + 7 * SW_NFX) * 8 + 16 + 128;
+
+constexpr int ST_TX = 32, ST_TY = 8;        // stencil kernels: 32 x 8 outputs
+constexpr int ST_HX = ST_TX + 2, ST_HY = ST_TY + 2;
+constexpr int ST_THREADS = ST_TX * ST_TY;
+constexpr int ST_TILE_N = ST_HX * ST_HY * 5;          // doubles in one cell tile
+constexpr int ST_TILE = (ST_TILE_N + 15) / 16 * 16;     // rounded so every TMA target is 128-B aligned
+constexpr int ST_VIS_N = ST_HX * ST_HY * 2;
+constexpr int ST_VIS = (ST_VIS_N + 15) / 16 * 16;
+constexpr size_t K1_SMEM = (size_t)ST_TILE * 8 + 16 + 128;
+constexpr size_t K5_SMEM = (size_t)(2 * ST_TILE + ST_VIS) * 8 + 16 + 128;
+
+// ------------------------------------------------------------- planet
+__host__ __device__ inline double ramp_function(double t, double tau, double val) {  // planet.cu:7-17
+    if (t < tau) return val * sin(HPI * t / tau);
+    return val;
+}
+__device__ inline double ecc_anomaly(double n, double e, double t) {  // planet.cu:60-103
+    double l = fmod(n * t, TWOPI);
+    double D = -e * sin(l);
+    if (e == 0.0) return l;
+    else if (l == 0.0) return l;
+    else if (l == PI) return l;
+    else if (l == TWOPI) return l;
+    double x, dx, d2x, eps, step, esinu, ecosu;
+    int count = 0;
+    do {
+        sincos(l - D, &esinu, &ecosu);
+        esinu *= e;
+        ecosu *= e;
+        x = D + esinu;
+        dx = 1.0 - ecosu;
+        d2x = -esinu;
+        eps = 2.0 * x * d2x / dx / dx;
+        if (fabs(eps) < 1.0) step = -(x / dx) * (1.0 + eps / 4.0 + eps * eps / 8.0 + 5.0 * eps * eps * eps / 64.0);
+        else step = copysign(fmin(fabs(x / dx), HPI / 2.0), -x);
+        D += step;
+        count++;
+    } while ((fabs(step) > 1.0e-12 || count < 10) && count < 200);
+    return l - D;
+}
+__device__ inline void orbit_solution(const DiskView& d, pg_body& b, double t) {  // planet.cu:105-133
+    const double a = b.a, e = b.e;
+    const double n = sqrt(1.0 / a / a / a);
+    const double efac = sqrt(1.0 - e * e);
+    const double B = e / (1.0 + efac);
+    double u, cosu, sinu;
+    u = ecc_anomaly(n, e, t);
+    sincos(u, &sinu, &cosu);
+    double f, ecosf, esinf;
+    f = u + 2.0 * atan(B * sinu / (1.0 - B * cosu));
+    sincos(f, &esinf, &ecosf);
+    esinf *= e;
+    ecosf *= e;
+    b.m = ramp_function(t, d.ramp_time, d.planet_mass);
+    b.x = a * efac * efac / (1.0 + ecosf);
+    b.y = f - fmod(d.frame_omega * t, TWOPI) + PI;
+    b.z = HPI;
+    b.vx = n * a * esinf / efac;
+    b.vy = n * (1.0 + ecosf) * (1.0 + ecosf) / efac / efac / efac;
+    b.vz = 0.0;
+}
+
+// --------------------------------------------------------- source terms
+struct Grav {
+    double gx, gy, gz;
+};
+// Star + planet gravity in the 2D cylindrical frame (src/solver/force/forces.cu:41-58,
+// 182-327 with twobd_flag 0, pol = 0).
+__device__ __forceinline__ Grav gravity(const DiskView& d, double rad, double azi, const pg_body& p) {
+    Grav g{0.0, 0.0, 0.0};
+    if (d.geomx == 1) {
+        const double pol = 0.0;
+        const double dis = sqrt(rad * rad + pol * pol);
+        g.gx = -rad / dis / dis / dis;
+        g.gz = -pol / dis / dis / dis;
+        if (d.nplanet > 0) {
+            double sinfac, cosfac;
+            sincos(azi - (p.y + 0.0 * p.vy), &sinfac, &cosfac);
+            const double plm = p.m, plx = p.x;
+            const double Rp = sqrt(rad * rad + plx * plx - 2.0 * plx * rad * cosfac + pol * pol + p.rs * p.rs);
+            const double rs_fac = 1.0 / Rp / Rp / Rp;
+            const double fx = -plm * (rad - plx * cosfac) * rs_fac - plm * cosfac / plx / plx;
+            const double fy = -plm * plx * sinfac * rs_fac + plm * sinfac / plx / plx;
+            const double fz = -plm * pol * rs_fac;
+            g.gx += fx;
+            g.gy += fy;
+            g.gz += fz;
+        }
+    }
+    return g;
+}
+
+// One cell of apply_source_terms (src/solver/sweeps.cu:597-711): curvature,
+// gravity and viscous acceleration; with mdt != 0 the forces are re-evaluated
+// at the mdt-predicted velocities (sweeps.cu:663-687).
+template <bool VISC>
+__device__ __forceinline__ Cell kick(const DiskView& d, const Cell& C, double x, const Grav& g, double vx,
+                                     double vy, double mdt, double dt) {
+    Cell T = C;
+    double fx = (d.geomx == 1) ? T.v * T.v / x : 0.0;
+    double fy = 0.0;
+    const double fz = 0.0;
+    if (VISC) {
+        fx += vx / T.r;
+        if (d.ndim > 1) fy += vy / T.r;
+    }
+    if (mdt != 0.0) {
+        T.u = C.u + fx * mdt + g.gx * mdt;
+        T.v = C.v + fy * mdt + g.gy * mdt;
+        T.w = C.w + fz * mdt + g.gz * mdt;
+        fx = (d.geomx == 1) ? T.v * T.v / x : 0.0;
+        fy = 0.0;
+        if (VISC) {
+            fx += vx / T.r;
+            if (d.ndim > 1) fy += vy / T.r;
+        }
+    }
+    Cell o;
+    o.u = C.u + fx * dt + g.gx * dt;
+    o.v = C.v + fy * dt + g.gy * dt;
+    o.w = C.w + fz * dt + g.gz * dt;
+    o.r = C.r;
+    o.p = C.p;
+    return o;
+}
+
+// Viscous force density of the middle cell of a 3x3 stencil
+// (src/viscosity/viscosity.cu:9-22, 84-194, ndim 2).  Stencil order: n<3 row j,
+// 3..5 row j-1, 6..8 row j+1, columns i-1..i+1; r: xc, t: yc, nu: get_nu.
+__device__ __forceinline__ void viscous(const double* r, const double* t, const double* u, const double* v,
+                                        const double* nr, double& fx_out, double& fy_out) {
+    const double dudx = (u[2] - u[0]) / (r[2] - r[0]);
+    const double d2udx2 = ((u[2] - u[1]) / (r[2] - r[1]) - (u[1] - u[0]) / (r[1] - r[0])) / (0.5 * (r[2] - r[0]));
+    const double dndx = (nr[2] - nr[0]) / (r[2] - r[0]);
+    const double dvdx = (v[2] - v[0]) / (r[2] - r[0]);
+    const double d2vdx2 = ((v[2] - v[1]) / (r[2] - r[1]) - (v[1] - v[0]) / (r[1] - r[0])) / (0.5 * (r[2] - r[0]));
+    const double dvdy = (v[7] - v[4]) / (t[2] - t[0]) / r[1];
+    const double d2vdy2 =
+        ((v[7] - v[1]) / (t[2] - t[1]) - (v[1] - v[4]) / (t[1] - t[0])) / (0.5 * (t[2] - t[0])) / r[1] / r[1];
+    const double d2vdxy = (v[8] - v[6] - v[5] + v[3]) / (r[2] - r[0]) / (t[2] - t[0]) / r[1];
+    const double dudy = (u[7] - u[4]) / (t[2] - t[0]) / r[1];
+    const double d2udy2 =
+        ((u[7] - u[1]) / (t[2] - t[1]) - (u[1] - u[4]) / (t[1] - t[0])) / (0.5 * (t[2] - t[0])) / r[1] / r[1];
+    const double d2udxy = (u[8] - u[6] - u[5] + u[3]) / (r[2] - r[0]) / (t[2] - t[0]) / r[1];
+    const double dndy = (nr[7] - nr[4]) / (t[2] - t[0]) / r[1];
+
+    const double sxx = 2.0 * nr[1] * dudx;
+    double fx = 2.0 * dndx * dudx + 2.0 * nr[1] * d2udx2 + sxx / r[1];
+    const double syy = 2.0 * nr[1] * (dvdy + u[1] / r[1]);
+    const double sxy = nr[1] * (dudy + dvdx - v[1] / r[1]);
+    double fy = 2.0 * dndy * dvdy + 2.0 * nr[1] * d2vdy2 + 2.0 * nr[1] * dudy / r[1] + 2.0 * dndy * u[1] / r[1];
+    fx += dndy * (dudy + dvdx) + nr[1] * (d2udy2 + d2vdxy) - dndy * v[1] / r[1] - nr[1] * dvdy / r[1] - syy / r[1];
+    fy += dndx * (dudy + dvdx) + nr[1] * (d2udxy + d2vdx2) - dndx * v[1] / r[1] - nr[1] * dvdx / r[1] +
+          nr[1] * v[1] / r[1] / r[1] + 2.0 * sxy / r[1];
+    fx_out = fx;
+    fy_out = fy;
+}
+
+// Gathers the 3x3 stencil around tile cell (hx, hy) of a [ST_HY][ST_HX][5] tile.
+__device__ __forceinline__ void gather9(const double* tile, int hx, int hy, const double nu[3], double* u,
+                                        double* v, double* nr) {
+#pragma unroll
+    for (int n = 0; n < 9; ++n) {
+        const int dx = (n % 3) - 1;
+        const int dy = (n < 3) ? 0 : (n < 6 ? -1 : 1);
+        const double* c = tile + ((hy + dy) * ST_HX + (hx + dx)) * 5;
+        nr[n] = c[0] * nu[n % 3];
+        u[n] = c[2];
+        v[n] = c[3];
+    }
+}
+
+__device__ __forceinline__ double signal_rate(const DiskView& d, const Cell& c, int i, int j) {
+    // src/timestep/timestep.cu:46-77
+    const double rad_cyl = (d.geomy == 3) ? d.radx[i] : 1.0;
+    const double cs = sqrt(d.gam * c.p / c.r);
+    double spd = fabs(c.u) + cs;
+    double wid = fabs(d.xa[i + 1] - d.xa[i]);
+    double tmp = fmax(spd / wid, 0.0);
+    if (d.ndim > 1) {
+        spd = fabs(c.v - rad_cyl * d.frame_omega - d.rot[i]) + cs;
+        wid = fabs(d.ya[j + 1] - d.ya[j]) * rad_cyl;
+        tmp = fmax(spd / wid, tmp);
+    }
+    return tmp;
+}
+
+template <int NT>
+__device__ __forceinline__ void block_max_to(unsigned long long* dst, double v) {
+    __shared__ double red[NT / 32];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        v = (threadIdx.x < NT / 32) ? red[threadIdx.x] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+        if (threadIdx.x == 0) atomic_max_pos(dst, v);
+    }
+}
+
+// Loads one TMA box into shared memory; every thread returns whether it landed.
+__device__ __forceinline__ bool tile_load(double* dst, const CUtensorMap* map, int x, int y, uint32_t bytes,
+                                          uint64_t* bar, Scalars* sc) {
+    if (threadIdx.x == 0) {
+        mbar_init(bar, 1);
+        fence_barrier_init();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        mbar_arrive_expect_tx(bar, bytes);
+        tma_load_2d(dst, map, x, y, bar);
+    }
+    return mbar_wait(bar, 0, sc);
+}
+
+// ================================================================ sweeps
+// DIR 0: radial pencils (rows of the array), DIR 1: azimuthal pencils (columns).
+template <int DIR>
+__global__ void __launch_bounds__(SW_THREADS, 2)
+    k_sweep(const __grid_constant__ CUtensorMap tm, const DiskView d, Cell* __restrict__ out) {
+    extern __shared__ __align__(128) double smem_raw[];
+    double* smem = smem_base128(smem_raw);
+    double* tile = smem;
+    double* st = smem + SW_TILE_MAX;  // [10][SW_NST] interface states
+    double* fl = st + 10 * SW_NST;    // [7][SW_NFX] fluxes
+    uint64_t* bar = reinterpret_cast<uint64_t*>(fl + 7 * SW_NFX);
+    __shared__ int s_inc[SW_W];
+    Scalars* sc = d.sc;
+    if (sc->done) return;
+
+    const int tid = threadIdx.x;
+    const int s0 = NPAD + SW_LEN * blockIdx.x;                     // first output along the sweep
+    const int q0 = (DIR == 0 ? d.ypad : NPAD) + SW_W * blockIdx.y;  // first pencil
+    const double dt = sc->dt;
+    const double gam = d.gam;
+
+    if (DIR == 1 && tid < SW_W) {
+        // set_orbital_advection (src/orbit/orbit.cu:74-99) for this column
+        const int i = q0 + tid;
+        int shift = 0;
+        if (d.orbadv && i < NPAD + d.xres) {
+            const double rad = d.radx[i];
+            const double dy = d.dy0 * rad;
+            const double rot = d.rot[i];
+            shift = __double2int_rd(rot * dt / dy + 0.5);
+            double speed = shift * dy / dt;
+            speed = rot - speed;
+            if (blockIdx.x == 0) {
+                d.res[i] = speed;
+                d.inc[i] = shift;
+            }
+        }
+        s_inc[tid] = shift;
+    }
+    const bool ok = (DIR == 0) ? tile_load(tile, &tm, 5 * (s0 - NPAD), q0, SWX_TILE * 8, bar, sc)
+                               : tile_load(tile, &tm, 5 * (q0 - 1), s0 - NPAD, SWY_TILE * 8, bar, sc);
+    if (!ok) return;
+
+    // ---- P1: reconstruction + both edge states of every cell
+    if (tid < SW_NST) {
+        const int it = tid;
+        const int q = (DIR == 0) ? it / SW_P1 : it % SW_W;
+        const int t = 2 + ((DIR == 0) ? it % SW_P1 : it / SW_W);
+        const int s = s0 - NPAD + t;
+        const int qq = q0 + q;
+        double r[5], p[5], u[5], v[5], w[5];
+        double rad = 1.0, rot = 0.0;
+        if (DIR == 1) {
+            const int i = min(qq, d.xarr - 1);
+            rad = (d.geomy == 3) ? d.radx[i] : 1.0;
+            rot = d.rot[i];
+        }
+#pragma unroll
+        for (int k = 0; k < 5; ++k) {
+            const double* c = (DIR == 0) ? tile + (q * SW_TL + (t - 2 + k)) * 5
+                                         : tile + ((t - 2 + k) * SWY_COLS + (q + 1)) * 5;
+            r[k] = c[0];
+            p[k] = c[1];
+            if (DIR == 0) {
+                u[k] = c[2];
+                v[k] = c[3];
+                if (d.geomx == 1) v[k] *= d.radx[min(max(s - 2 + k, 0), d.xarr - 1)];
+                w[k] = c[4];
+            } else {
+                u[k] = c[3] - rot;
+                if (d.geomy == 3) u[k] -= rad * d.frame_omega;
+                v[k] = c[4];
+                w[k] = c[2];
+            }
+        }
+        const double flat = flatten(gam, r[2], p[0], p[1], p[2], p[3], p[4], u[1], u[2], u[3]);
+        const int sc_ = (DIR == 0) ? min(s, d.xarr - 1) : min(s, d.yarr - 1);
+        const double* wt = ((DIR == 0) ? d.wx : d.wy) + 6 * sc_;
+        const double* fa = (DIR == 0) ? d.xa : d.ya;
+        const Par R = recon(wt, r[0], r[1], r[2], r[3], r[4], flat);
+        const Par P = recon(wt, p[0], p[1], p[2], p[3], p[4], flat);
+        const Par U = recon(wt, u[0], u[1], u[2], u[3], u[4], flat);
+        const Par V = recon(wt, v[0], v[1], v[2], v[3], v[4], flat);
+        const Par W = recon(wt, w[0], w[1], w[2], w[3], w[4], flat);
+        const double xl = fa[sc_], xr = fa[sc_ + 1];
+        const double sdt = (DIR == 0) ? dt : dt / rad;
+        const Half a = state_at_left_edge(gam, xl, xr, sdt, r[2], p[2], u[2], R, P, U, V, W);
+        const Half b = state_at_right_edge(gam, xl, xr, sdt, r[2], p[2], u[2], R, P, U, V, W);
+        st[0 * SW_NST + it] = a.r;
+        st[1 * SW_NST + it] = a.p;
+        st[2 * SW_NST + it] = a.u;
+        st[3 * SW_NST + it] = a.v;
+        st[4 * SW_NST + it] = a.w;
+        st[5 * SW_NST + it] = b.r;
+        st[6 * SW_NST + it] = b.p;
+        st[7 * SW_NST + it] = b.u;
+        st[8 * SW_NST + it] = b.v;
+        st[9 * SW_NST + it] = b.w;
+    }
+    __syncthreads();
+
+    // ---- P2: HLLC flux at every face (left state from cell t-1, right from cell t)
+    if (tid < SW_NFX) {
+        const int it = tid;
+        const int q = (DIR == 0) ? it / SW_P2 : it % SW_W;
+        const int t = 3 + ((DIR == 0) ? it % SW_P2 : it / SW_W);
+        const int iL = (DIR == 0) ? q * SW_P1 + (t - 3) : (t - 3) * SW_W + q;
+        const int iR = (DIR == 0) ? q * SW_P1 + (t - 2) : (t - 2) * SW_W + q;
+        Half L, R;
+        L.r = st[5 * SW_NST + iL];
+        L.p = st[6 * SW_NST + iL];
+        L.u = st[7 * SW_NST + iL];
+        L.v = st[8 * SW_NST + iL];
+        L.w = st[9 * SW_NST + iL];
+        R.r = st[0 * SW_NST + iR];
+        R.p = st[1 * SW_NST + iR];
+        R.u = st[2 * SW_NST + iR];
+        R.v = st[3 * SW_NST + iR];
+        R.w = st[4 * SW_NST + iR];
+        const Flux F = hllc(d.eos, d.ie, gam, L, R);
+        fl[0 * SW_NFX + it] = F.r;
+        fl[1 * SW_NFX + it] = F.p;
+        fl[2 * SW_NFX + it] = F.u;
+        fl[3 * SW_NFX + it] = F.v;
+        fl[4 * SW_NFX + it] = F.w;
+        fl[5 * SW_NFX + it] = F.pres;
+        fl[6 * SW_NFX + it] = F.uprs;
+    }
+    __syncthreads();
+
+    // ---- P3: flux differences, geometric sources, conservative update
+    if (tid < SW_LEN * SW_W) {
+        const int it = tid;
+        const int q = (DIR == 0) ? it / SW_LEN : it % SW_W;
+        const int t = 3 + ((DIR == 0) ? it % SW_LEN : it / SW_W);
+        const int s = s0 - NPAD + t;
+        const int qq = q0 + q;
+        const bool valid = (DIR == 0) ? (s < NPAD + d.xres && qq < d.ypad + d.yres)
+                                      : (s < NPAD + d.yres && qq < NPAD + d.xres);
+        if (valid) {
+            const int f0 = (DIR == 0) ? q * SW_P2 + (t - 3) : (t - 3) * SW_W + q;
+            const int f1 = (DIR == 0) ? f0 + 1 : f0 + SW_W;
+            const double g0 = (DIR == 0 && d.geomx == 1) ? d.xa[s] : 1.0;  // eval_gfac (riemann.cu:5-11)
+            const double g1 = (DIR == 0 && d.geomx == 1) ? d.xa[s + 1] : 1.0;
+            const double pres0 = fl[5 * SW_NFX + f0], pres1 = fl[5 * SW_NFX + f1];
+            // net_source (src/solver/riemann/riemann.cu:40-87)
+            const double du = 0.5 * (g0 + g1) * (pres0 - pres1);
+            double de = 0.0;
+            if (d.eos == 2) {
+                const double t0 = fl[6 * SW_NFX + f0] * g0, t1 = fl[6 * SW_NFX + f1] * g1;
+                de = (d.ie == 0) ? t0 - t1 : 0.5 * (pres0 + pres1) * (t0 - t1);
+            }
+            Cell D;
+            D.r = fl[0 * SW_NFX + f0] * g0 - fl[0 * SW_NFX + f1] * g1;
+            D.p = (fl[1 * SW_NFX + f0] * g0 - fl[1 * SW_NFX + f1] * g1) + de;
+            D.u = (fl[2 * SW_NFX + f0] * g0 - fl[2 * SW_NFX + f1] * g1) + du;
+            D.v = fl[3 * SW_NFX + f0] * g0 - fl[3 * SW_NFX + f1] * g1;
+            D.w = fl[4 * SW_NFX + f0] * g0 - fl[4 * SW_NFX + f1] * g1;
+            const double* c = (DIR == 0) ? tile + (q * SW_TL + t) * 5 : tile + (t * SWY_COLS + (q + 1)) * 5;
+            const Cell C0{c[0], c[1], c[2], c[3], c[4]};
+            if (DIR == 0) {
+                const double f = dt / d.xv[s];
+                D.r *= f; D.p *= f; D.u *= f; D.v *= f; D.w *= f;
+                if (d.geomx == 1) D.v /= d.radx[s];
+                const Cell Q = update_cell(d.eos, d.ie, gam, d.cs2x[s], C0, D, &sc->floor_hits);
+                if (!(Q.r > 0.0)) atomicOr(&sc->err, 1 << PG_ERR_NAN);
+                emit(d, out, s, qq, Q);
+            } else {
+                const double rad = (d.geomy == 3) ? d.radx[qq] : 1.0;
+                const double rot = d.rot[qq];
+                const double f = dt / d.yv[s] / rad;
+                D.r *= f; D.p *= f; D.u *= f; D.v *= f; D.w *= f;
+                if (d.geomy == 3) D.u += (rot + rad * d.frame_omega) * D.r;
+                else D.u += rot * D.r;
+                const Cell E{D.r, D.p, D.w, D.u, D.v};
+                const Cell Q = update_cell(d.eos, d.ie, gam, d.cs2x[qq], C0, E, &sc->floor_hits);
+                if (!(Q.r > 0.0)) atomicOr(&sc->err, 1 << PG_ERR_NAN);
+                int j = s;
+                if (d.orbadv) {  // orbital shift T[(j+inc) mod N] = C[j] (orbit.cu:30-46)
+                    int js = (s - d.ypad + s_inc[q]) % d.yres;
+                    if (js < 0) js += d.yres;
+                    j = js + d.ypad;
+                }
+                emit(d, out, qq, j, Q);
+            }
+        }
+    }
+}
+
+// ===================================================== residual advection
+__global__ void __launch_bounds__(SW_THREADS, 2)
+    k_advect(const __grid_constant__ CUtensorMap tm, const DiskView d, Cell* __restrict__ out) {
+    extern __shared__ __align__(128) double smem_raw[];
+    double* smem = smem_base128(smem_raw);
+    double* tile = smem;
+    double* fl = smem + SW_TILE_MAX;  // [5][SW_TL * SW_W] face fluxes, indexed by face t
+    uint64_t* bar = reinterpret_cast<uint64_t*>(fl + 5 * SW_TL * SW_W);
+    Scalars* sc = d.sc;
+    if (sc->done) return;
+    const int tid = threadIdx.x;
+    const int s0 = NPAD + SW_LEN * blockIdx.x;
+    const int q0 = NPAD + SW_W * blockIdx.y;
+    const double dt = sc->dt;
+    if (!tile_load(tile, &tm, 5 * (q0 - 1), s0 - NPAD, SWY_TILE * 8, bar, sc)) return;
+    constexpr int NFL = SW_TL * SW_W;
+
+    // ---- P1: upwind PPM average over the swept fraction (advection.cu:20-67)
+    if (tid < SW_NST) {
+        const int q = tid % SW_W;
+        const int t = 2 + tid / SW_W;
+        const int s = min(s0 - NPAD + t, d.yarr - 1);
+        const int i = min(q0 + q, d.xarr - 1);
+        const double rad = (d.geomy == 3) ? d.radx[i] : 1.0;
+        const double speed = d.res[i];
+        const double sdt = dt / rad;
+        double r[5], p[5], u[5], v[5], w[5];
+#pragma unroll
+        for (int k = 0; k < 5; ++k) {
+            const double* c = tile + ((t - 2 + k) * SWY_COLS + (q + 1)) * 5;
+            r[k] = c[0]; p[k] = c[1]; u[k] = c[3]; v[k] = c[4]; w[k] = c[2];
+        }
+        const double* wt = d.wy + 6 * s;
+        const Par R = recon(wt, r[0], r[1], r[2], r[3], r[4], 0.0);
+        const Par P = recon(wt, p[0], p[1], p[2], p[3], p[4], 0.0);
+        const Par U = recon(wt, u[0], u[1], u[2], u[3], u[4], 0.0);
+        const Par V = recon(wt, v[0], v[1], v[2], v[3], v[4], 0.0);
+        const Par W = recon(wt, w[0], w[1], w[2], w[3], w[4], 0.0);
+        const double xl = d.ya[s], xr = d.ya[s + 1];
+        double fr, fp, fu, fv, fw;
+        int face;
+        if (speed > 0.0) {  // this cell is upwind of its upper face
+            const double x0 = xr - speed * sdt;
+            const Frac q_ = frac_right(lim01((x0 - xl) / (xr - xl)));
+            fr = aveR(q_, R);
+            fp = aveR(q_, P);
+            fu = aveR(q_, U) * fr;
+            fv = aveR(q_, V) * fr;
+            fw = aveR(q_, W) * fr;
+            face = t + 1;
+        } else {  // ... of its lower face
+            const double x0 = xl - speed * sdt;
+            const Frac q_ = frac_left(lim01((x0 - xl) / (xr - xl)));
+            fr = aveL(q_, R);
+            fp = aveL(q_, P);
+            fu = aveL(q_, U) * fr;
+            fv = aveL(q_, V) * fr;
+            fw = aveL(q_, W) * fr;
+            face = t;
+        }
+        const int k = face * SW_W + q;
+        fl[0 * NFL + k] = fr * speed;
+        fl[1 * NFL + k] = fp * speed;
+        fl[2 * NFL + k] = fu * speed;
+        fl[3 * NFL + k] = fv * speed;
+        fl[4 * NFL + k] = fw * speed;
+    }
+    __syncthreads();
+
+    // ---- P2: flux difference and update_Cell_advect (advection.cu:88-105, 153-170)
+    if (tid < SW_LEN * SW_W) {
+        const int q = tid % SW_W;
+        const int t = 3 + tid / SW_W;
+        const int s = s0 - NPAD + t;
+        const int i = q0 + q;
+        if (s < NPAD + d.yres && i < NPAD + d.xres) {
+            const int k0 = t * SW_W + q, k1 = (t + 1) * SW_W + q;
+            Cell D;
+            D.r = fl[0 * NFL + k0] * 1.0 - fl[0 * NFL + k1] * 1.0;
+            D.p = fl[1 * NFL + k0] * 1.0 - fl[1 * NFL + k1] * 1.0;
+            D.u = fl[2 * NFL + k0] * 1.0 - fl[2 * NFL + k1] * 1.0;
+            D.v = fl[3 * NFL + k0] * 1.0 - fl[3 * NFL + k1] * 1.0;
+            D.w = fl[4 * NFL + k0] * 1.0 - fl[4 * NFL + k1] * 1.0;
+            const double rad = (d.geomy == 3) ? d.radx[i] : 1.0;
+            double f = dt / d.yv[s];
+            D.r *= f; D.p *= f; D.u *= f; D.v *= f; D.w *= f;
+            if (d.geomy > 2) {
+                f = 1.0 / rad;
+                D.r *= f; D.p *= f; D.u *= f; D.v *= f; D.w *= f;
+            }
+            const double* c = tile + (t * SWY_COLS + (q + 1)) * 5;
+            Cell Q{c[0], c[1], c[2], c[3], c[4]};
+            Q.u *= Q.r;
+            Q.v *= Q.r;
+            Q.w *= Q.r;
+            Q.r += D.r;
+            Q.p += D.p;
+            Q.u += D.w;
+            Q.v += D.u;
+            Q.w += D.v;
+            Q.u /= Q.r;
+            Q.v /= Q.r;
+            Q.w /= Q.r;
+            if (d.eos == 0) Q.p = d.cs2x[i] * Q.r;
+            if (!(Q.r > 0.0)) atomicOr(&sc->err, 1 << PG_ERR_NAN);
+            emit(d, out, i, s, Q);
+        }
+    }
+}
+
+// ====================================================== kick 1 (+ stress)
+template <bool VISC>
+__global__ void __launch_bounds__(ST_THREADS)
+    k_kick1(const __grid_constant__ CUtensorMap tm, const DiskView d, Cell* __restrict__ out,
+            double* __restrict__ vis) {
+    extern __shared__ __align__(128) double smem_raw[];
+    double* smem = smem_base128(smem_raw);
+    double* tile = smem;
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + ST_TILE);
+    Scalars* sc = d.sc;
+    if (sc->done) return;
+    const int i0 = NPAD + ST_TX * blockIdx.x;
+    const int j0 = d.ypad + ST_TY * blockIdx.y;
+    if (!tile_load(tile, &tm, 5 * (i0 - 1), j0 - 1, ST_TILE_N * 8, bar, sc)) return;
+    const int hx = 1 + threadIdx.x % ST_TX, hy = 1 + threadIdx.x / ST_TX;
+    const int i = i0 + hx - 1, j = j0 + hy - 1;
+    if (i >= NPAD + d.xres || j >= d.ypad + d.yres) return;
+    const double hdt = 0.5 * sc->dt;
+    const double* c = tile + (hy * ST_HX + hx) * 5;
+    const Cell C{c[0], c[1], c[2], c[3], c[4]};
+    double vx = 0.0, vy = 0.0;
+    if (VISC) {
+        double r[3], t[3], nu[3], u[9], v[9], nr[9];
+#pragma unroll
+        for (int n = 0; n < 3; ++n) {
+            r[n] = d.radx[i + n - 1];
+            t[n] = d.ycraw[j + n - 1];
+            nu[n] = d.nux[i + n - 1];
+        }
+        gather9(tile, hx, hy, nu, u, v, nr);
+        viscous(r, t, u, v, nr, vx, vy);
+        // the stress is kept for the predictor of kick2, with its periodic images
+        const size_t k = (size_t)i + (size_t)d.xarr * j;
+        vis[2 * k] = vx;
+        vis[2 * k + 1] = vy;
+        int jimg = -1;
+        if (j < 2 * NPAD) jimg = j + d.yres;
+        else if (j >= d.yres) jimg = j - d.yres;
+        if (jimg >= 0) {
+            const size_t m = (size_t)i + (size_t)d.xarr * jimg;
+            vis[2 * m] = vx;
+            vis[2 * m + 1] = vy;
+        }
+    }
+    const double y = (d.ndim > 1) ? d.ycj[j] + d.rot[i] * 0.0 : 0.0;
+    const Grav g = gravity(d, d.radx[i], y, sc->planet_cur);
+    const Cell Q = kick<VISC>(d, C, d.radx[i], g, vx, vy, 0.0, hdt);
+    emit(d, out, i, j, Q);
+}
+
+// ============================================ kick 2 + damping + CFL speed
+template <bool VISC>
+__global__ void __launch_bounds__(ST_THREADS)
+    k_kick2(const __grid_constant__ CUtensorMap tm, const __grid_constant__ CUtensorMap tv, const DiskView d,
+            Cell* __restrict__ out) {
+    extern __shared__ __align__(128) double smem_raw[];
+    double* smem = smem_base128(smem_raw);
+    double* tile = smem;              // C with 1 halo
+    double* tp = smem + ST_TILE;      // predicted state with 1 halo
+    double* tvis = tp + ST_TILE;      // stress of the step's first evaluation
+    uint64_t* bar = reinterpret_cast<uint64_t*>(tvis + ST_VIS);
+    Scalars* sc = d.sc;
+    if (sc->done) return;
+    const int i0 = NPAD + ST_TX * blockIdx.x;
+    const int j0 = d.ypad + ST_TY * blockIdx.y;
+    const int tid = threadIdx.x;
+    if (tid == 0) {
+        mbar_init(bar, 1);
+        fence_barrier_init();
+    }
+    __syncthreads();
+    if (tid == 0) {
+        mbar_arrive_expect_tx(bar, (ST_TILE_N + (VISC ? ST_VIS_N : 0)) * 8);
+        tma_load_2d(tile, &tm, 5 * (i0 - 1), j0 - 1, bar);
+        if (VISC) tma_load_2d(tvis, &tv, 2 * (i0 - 1), j0 - 1, bar);
+    }
+    if (!mbar_wait(bar, 0, sc)) return;
+    const double dt = sc->dt, hdt = 0.5 * dt;
+    const pg_body pl = sc->planet_next;
+
+    if (VISC) {
+        // predictor (sweeps.cu:713-729 with mdt = dt = dt/2) on the tile and its halo
+        for (int it = tid; it < ST_HX * ST_HY; it += ST_THREADS) {
+            const int hx = it % ST_HX, hy = it / ST_HX;
+            const int i = i0 - 1 + hx, j = j0 - 1 + hy;
+            if (i < NPAD || i >= NPAD + d.xres || j < 0 || j >= d.yarr) continue;
+            const double* c = tile + it * 5;
+            const Cell C{c[0], c[1], c[2], c[3], c[4]};
+            const double y = d.ycj[j] + d.rot[i] * 0.0;
+            const Grav g = gravity(d, d.radx[i], y, pl);
+            const Cell Q = kick<true>(d, C, d.radx[i], g, tvis[2 * it], tvis[2 * it + 1], hdt, hdt);
+            double* o = tp + it * 5;
+            o[0] = Q.r; o[1] = Q.p; o[2] = Q.u; o[3] = Q.v; o[4] = Q.w;
+        }
+        __syncthreads();
+        // radial ghosts of the predicted state (boundx2, src/boundary/boundary.cu:722-820):
+        // the stencil only reaches the innermost ghost column on either side
+        for (int it = tid; it < ST_HX * ST_HY; it += ST_THREADS) {
+            const int hx = it % ST_HX, hy = it / ST_HX;
+            const int i = i0 - 1 + hx;
+            const int side = (i == NPAD - 1) ? 0 : ((i == NPAD + d.xres) ? 1 : -1);
+            if (side < 0) continue;
+            const int bnd = side == 0 ? d.bound_lft : d.bound_rgh;
+            double* o = tp + (hy * ST_HX + hx) * 5;
+            const double* src;
+            if (bnd == 0) src = tile + (hy * ST_HX + hx) * 5;  // constant analytic state
+            else {
+                // the adjacent interior cell is both the copy and the reflection source
+                const int hs = side == 0 ? hx + 1 : hx - 1;
+                src = tp + (hy * ST_HX + hs) * 5;
+            }
+            o[0] = src[0]; o[1] = src[1]; o[2] = src[2]; o[3] = src[3]; o[4] = src[4];
+            if (bnd == 2) o[2] = -o[2];
+        }
+        __syncthreads();
+    }
+
+    const int hx = 1 + tid % ST_TX, hy = 1 + tid / ST_TX;
+    const int i = i0 + hx - 1, j = j0 + hy - 1;
+    const bool valid = (i < NPAD + d.xres && j < d.ypad + d.yres);
+    double vmax = 0.0;
+    if (valid) {
+        const double* c = tile + (hy * ST_HX + hx) * 5;
+        const Cell C{c[0], c[1], c[2], c[3], c[4]};
+        double vx = 0.0, vy = 0.0;
+        if (VISC) {
+            double r[3], t[3], nu[3], u[9], v[9], nr[9];
+#pragma unroll
+            for (int n = 0; n < 3; ++n) {
+                r[n] = d.radx[i + n - 1];
+                t[n] = d.ycraw[j + n - 1];
+                nu[n] = d.nux[i + n - 1];
+            }
+            gather9(tp, hx, hy, nu, u, v, nr);
+            viscous(r, t, u, v, nr, vx, vy);
+        }
+        const double y = (d.ndim > 1) ? d.ycj[j] + d.rot[i] * 0.0 : 0.0;
+        const Grav g = gravity(d, d.radx[i], y, pl);
+        Cell Q = kick<VISC>(d, C, d.radx[i], g, vx, vy, hdt, hdt);
+        if (d.kill) {
+            // killwave (src/killwave/killwave.cu:48-100): relax towards init_C
+            const double* kt = d.killx + 4 * i;
+            const double* I = d.initx + 5 * i;
+#pragma unroll
+            for (int side = 0; side < 2; ++side) {
+                const double tau = kt[2 * side + 1];
+                if (tau > 0.0) {
+                    double f = kt[2 * side];
+                    f *= dt / tau;
+                    Q.r += f * (I[0] - Q.r);
+                    Q.p += f * (I[1] - Q.p);
+                    Q.u += f * (I[2] - Q.u);
+                    Q.v += f * (I[3] - Q.v);
+                    Q.w += f * (I[4] - Q.w);
+                }
+            }
+        }
+        if (!(Q.r > 0.0)) atomicOr(&sc->err, 1 << PG_ERR_NAN);
+        vmax = signal_rate(d, Q, i, j);
+        emit(d, out, i, j, Q);
+    }
+    block_max_to<ST_THREADS>(&sc->vmax_bits, vmax);
+}
+
+// ================================================================ misc
+__global__ void k_cfl(const DiskView d, const Cell* __restrict__ in) {
+    const long long n = (long long)d.xres * d.yres;
+    double vmax = 0.0;
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+        const int i = NPAD + (int)(k % d.xres);
+        const int j = d.ypad + (int)(k / d.xres);
+        vmax = fmax(vmax, signal_rate(d, load_cell(in, d.xarr, i, j), i, j));
+    }
+    block_max_to<256>(&d.sc->vmax_bits, vmax);
+}
+
+__global__ void k_reset_vmax(Scalars* sc) { sc->vmax_bits = 0ull; }
+
+// Host-supplied t, dt (pg_*_solve): planet for this step, reset of the signal-speed max.
+__global__ void k_set_time(const DiskView d, double t, double dt) {
+    Scalars* sc = d.sc;
+    sc->done = 0;
+    sc->dt = dt;
+    sc->planet_cur = sc->planet_next;
+    if (d.nplanet > 0) orbit_solution(d, sc->planet_next, t + dt);  // evolve_planet (solve.cu:264)
+    sc->t = t + dt;
+    sc->dt_prev = dt;
+    sc->vmax_bits = 0ull;
+    sc->steps += 1;
+}
+
+// Device-resident loop step (main.cu:322-339): dt = min(CFL/vmax, 1.1 dt_prev),
+// clipped at end_time; then the planet at t + dt.
+__global__ void k_time_step(const DiskView d) {
+    Scalars* sc = d.sc;
+    if (sc->done) return;
+    if (sc->pad_) {  // the previous step reached end_time
+        sc->done = 1;
+        return;
+    }
+    const double vmax = __longlong_as_double((long long)sc->vmax_bits);
+    const double dtc = d.cfl / vmax;
+    const double lim = sc->dt_prev * 1.1;
+    double dt = (dtc < lim) ? dtc : lim;
+    const double t = sc->t;
+    if (t + dt > sc->end_time) {
+        dt = sc->end_time - t;
+        sc->pad_ = 1;
+    }
+    sc->dt = dt;
+    sc->planet_cur = sc->planet_next;
+    if (d.nplanet > 0) orbit_solution(d, sc->planet_next, t + dt);
+    sc->t = t + dt;
+    sc->dt_prev = dt;
+    sc->vmax_bits = 0ull;
+    sc->steps += 1;
+}
+
+__global__ void k_init_planet(const DiskView d, double a, double e, double rs, double t) {
+    // init_planet (src/planet/planet.cu:319-402, one planet)
+    pg_body b;
+    b.a = a;
+    b.e = e;
+    b.rs = 0.0;
+    orbit_solution(d, b, t);
+    b.rs = rs;
+    d.sc->planet_next = b;
+    d.sc->planet_cur = b;
+}
+
+// Per-index tables evaluated with the device's own pow/sqrt/__sinf so they carry
+// the same bits as the reference's device-side evaluations.
+struct TabArgs {
+    double sc_h, planet_radius, p_alpha, p_beta, ss_alpha, frame_omega;
+    double xmin, xmax, kill_width, kill_width_out;
+    int visc, orbadv, kill, init_flag, geomx;
+};
+__device__ inline double d_cs2(const TabArgs& a, double x) {  // init.cu:7-17
+    double coeff = a.sc_h * a.sc_h * (1.0 / a.planet_radius);
+    if (a.geomx == 0) return coeff;
+    return coeff * pow(x / a.planet_radius, -a.p_beta);
+}
+__device__ inline double d_h(const TabArgs& a, double x) {  // init.cu:20-29
+    if (a.geomx == 0) return a.sc_h;
+    return sqrt(d_cs2(a, x) * pow(x, 3));
+}
+__device__ inline double d_nu(const TabArgs& a, double x) {  // init.cu:31-50
+    if (!a.visc) return 0.0;
+    double coeff = a.ss_alpha * sqrt(d_cs2(a, a.planet_radius)) * d_h(a, a.planet_radius);
+    if (a.geomx == 0) return coeff;
+    return coeff * pow(x / a.planet_radius, a.p_alpha);
+}
+__device__ inline double d_r(const TabArgs& a, double x) { return pow(x / a.planet_radius, -a.p_alpha) * 1.0; }
+__device__ inline double d_p(const TabArgs& a, double x) { return d_cs2(a, x) * d_r(a, x); }
+__device__ inline void d_initC(const TabArgs& a, double x, double* q) {  // init.cu:431-442 (init_flag 2)
+    if (a.init_flag == 2) {
+        q[0] = d_r(a, x);
+        q[1] = d_p(a, x);
+        q[2] = -1.5 * d_nu(a, x) / x;
+        const double rho = d_r(a, x);
+        const double dr = 1.1514178e-7;
+        const double dP_dr = (d_p(a, x + dr) - d_p(a, x - dr)) / (2.0 * dr);
+        q[3] = sqrt(1.0 / x + (x / rho) * dP_dr);
+        q[4] = 0.0;
+    } else {
+        q[0] = 1.0; q[1] = 1.0; q[2] = 0.0; q[3] = 0.0; q[4] = 0.0;
+    }
+}
+__device__ inline double ramping_fac(double x) {  // killwave.cu:8-14
+    double f = __sinf(HPI * x);
+    f *= f;
+    return f;
+}
+
+__global__ void k_init_tables(const DiskView d, TabArgs a, double* radx, double* cs2x, double* nux, double* initx,
+                              double* killx, double* rot, double* ycraw, double* ycj) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < d.xarr) {
+        const double x = 0.5 * (d.xa[k + 1] + d.xa[k]);
+        radx[k] = x;
+        cs2x[k] = d_cs2(a, x);
+        nux[k] = d_nu(a, x);
+        d_initC(a, x, initx + 5 * k);
+        // orb_rot (src/orbit/orbit.cu:57-69)
+        if (rot) rot[k] = a.orbadv ? initx[5 * k + 3] - x * a.frame_omega : 0.0;
+        const double d_in = d_h(a, a.xmin) * a.kill_width;
+        const double d_out = d_h(a, a.xmax) * a.kill_width_out;
+        const double inner = a.xmin + d_in;
+        const double outer = a.xmax - d_out;
+        double* kt = killx + 4 * k;
+        kt[0] = kt[1] = kt[2] = kt[3] = 0.0;
+        if (a.kill && k >= NPAD && k < NPAD + d.xres) {
+            if (x < inner) {
+                double f = (inner - x) / d_in;
+                kt[1] = (a.geomx == 0) ? 1.0 : pow(x, 1.5);
+                kt[0] = ramping_fac(f);
+            }
+            if (x > outer) {
+                double f = (x - outer) / d_out;
+                kt[3] = (a.geomx == 0) ? 1.0 : pow(x, 1.5);
+                kt[2] = ramping_fac(f);
+            }
+        }
+    }
+    if (k < d.yarr) {
+        ycraw[k] = 0.5 * (d.ya[k + 1] + d.ya[k]);
+        int jm = k;
+        if (d.ndim > 1) {
+            if (k < d.ypad) jm = k + d.yres;
+            else if (k >= d.ypad + d.yres) jm = k - d.yres;
+        }
+        ycj[k] = 0.5 * (d.ya[jm + 1] + d.ya[jm]);
+    }
+}
+
+// Bound-0 radial ghosts hold init_C (src/boundary/boundary.cu:30-33, 56-59) in every row.
+__global__ void k_init_xghosts(const DiskView d, Cell* buf) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= 2 * NPAD * d.yarr) return;
+    const int j = k / (2 * NPAD);
+    const int n = k % (2 * NPAD);
+    const int i = n < NPAD ? n : d.xres + n;
+    const int bnd = n < NPAD ? d.bound_lft : d.bound_rgh;
+    if (bnd != 0) return;
+    const double* I = d.initx + 5 * i;
+    store_cell(buf, d.xarr, i, j, Cell{I[0], I[1], I[2], I[3], I[4]});
+}
+
+// boundy then boundx (src/boundary/boundary.cu:141-209, 13-62) on one buffer.
+__global__ void k_bound_y(const DiskView d, Cell* buf) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (d.ndim < 2 || k >= d.xarr * NPAD) return;
+    const int i = k % d.xarr, n = k / d.xarr;
+    store_cell(buf, d.xarr, i, n, load_cell(buf, d.xarr, i, d.yres + n));
+    store_cell(buf, d.xarr, i, d.yres + NPAD + n, load_cell(buf, d.xarr, i, NPAD + n));
+}
+__global__ void k_bound_x(const DiskView d, Cell* buf) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= d.yarr) return;
+    const int nx = d.xres + NPAD;
+    for (int n = 0; n < NPAD; ++n) {
+        if (d.bound_lft == 2) {
+            Cell c = load_cell(buf, d.xarr, 2 * NPAD - 1 - n, j);
+            c.u *= -1.0;
+            store_cell(buf, d.xarr, n, j, c);
+        } else if (d.bound_lft == 1) {
+            store_cell(buf, d.xarr, n, j, load_cell(buf, d.xarr, NPAD, j));
+        }
+        if (d.bound_rgh == 2) {
+            Cell c = load_cell(buf, d.xarr, nx - 1 - n, j);
+            c.u *= -1.0;
+            store_cell(buf, d.xarr, nx + n, j, c);
+        } else if (d.bound_rgh == 1) {
+            store_cell(buf, d.xarr, nx + n, j, load_cell(buf, d.xarr, nx - 1, j));
+        }
+    }
+}
+
+// ============================================================== launchers
+static inline unsigned cdiv(long long a, long long b) { return (unsigned)((a + b - 1) / b); }
+
+cudaError_t set_kernel_attributes() {
+    cudaError_t e = cudaSuccess;
+    auto set = [&](const void* f, size_t bytes) {
+        cudaError_t r = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+        if (r != cudaSuccess) e = r;
+    };
+    set((const void*)k_sweep<0>, SW_SMEM);
+    set((const void*)k_sweep<1>, SW_SMEM);
+    set((const void*)k_advect, SW_SMEM);
+    set((const void*)k_kick1<true>, K1_SMEM);
+    set((const void*)k_kick1<false>, K1_SMEM);
+    set((const void*)k_kick2<true>, K5_SMEM);
+    set((const void*)k_kick2<false>, K5_SMEM);
+    return e;
+}
+
+void launch_init_tables(const DiskView& d, const pg_params& P, double* tab, cudaStream_t s) {
+    TabArgs a{P.sc_h, P.planet_radius, P.p_alpha, P.p_beta, P.ss_alpha, P.frame_omega, P.xmin, P.xmax,
+              P.kill_width, P.kill_width_out > 0.0 ? P.kill_width_out : P.kill_width,
+              P.visc_flag, P.orbadv_flag, P.kill_flag, P.init_flag, P.geomx};
+    // tab layout (doubles): radx[xarr] cs2x[xarr] nux[xarr] initx[5 xarr] killx[4 xarr] ycraw[yarr] ycj[yarr]
+    double* radx = tab;
+    double* cs2x = radx + d.xarr;
+    double* nux = cs2x + d.xarr;
+    double* initx = nux + d.xarr;
+    double* killx = initx + 5 * d.xarr;
+    double* ycraw = killx + 4 * d.xarr;
+    double* ycj = ycraw + d.yarr;
+    const int n = d.xarr > d.yarr ? d.xarr : d.yarr;
+    k_init_tables<<<cdiv(n, 128), 128, 0, s>>>(d, a, radx, cs2x, nux, initx, killx, const_cast<double*>(d.rot),
+                                                ycraw, ycj);
+}
+
+void launch_init_xghosts(const DiskView& d, Cell* buf, cudaStream_t s) {
+    k_init_xghosts<<<cdiv(2 * NPAD * d.yarr, 256), 256, 0, s>>>(d, buf);
+}
+
+void launch_bound(const DiskView& d, Cell* buf, cudaStream_t s) {
+    if (d.ndim > 1) k_bound_y<<<cdiv(d.xarr * NPAD, 256), 256, 0, s>>>(d, buf);
+    if (d.bound_lft != 0 || d.bound_rgh != 0) k_bound_x<<<cdiv(d.yarr, 256), 256, 0, s>>>(d, buf);
+}
+
+void launch_cfl(const DiskView& d, const Cell* buf, cudaStream_t s) {
+    k_reset_vmax<<<1, 1, 0, s>>>(d.sc);
+    const long long n = (long long)d.xres * d.yres;
+    unsigned blocks = cdiv(n, 256);
+    if (blocks > 148u * 8u) blocks = 148u * 8u;
+    k_cfl<<<blocks, 256, 0, s>>>(d, buf);
+}
+
+void launch_set_time(const DiskView& d, double t, double dt, cudaStream_t s) { k_set_time<<<1, 1, 0, s>>>(d, t, dt); }
+void launch_time_step(const DiskView& d, cudaStream_t s) { k_time_step<<<1, 1, 0, s>>>(d); }
+
+void launch_init_planet(const DiskView& d, const pg_params& P, double t, cudaStream_t s) {
+    const double a = P.planet_radius;
+    const double rs = (P.ndim == 2) ? P.rs_fac * P.sc_h * a : P.rs_fac * pow(P.planet_mass / 3.0, 1.0 / 3.0) * a;
+    k_init_planet<<<1, 1, 0, s>>>(d, a, P.planet_ecc, rs, t);
+}
+
+void launch_kick1(const DiskView& d, const CellMaps& in, Cell* out, double* vis, cudaStream_t s) {
+    dim3 grid(cdiv(d.xres, ST_TX), cdiv(d.yres, ST_TY));
+    if (d.visc && d.ndim == 2) k_kick1<true><<<grid, ST_THREADS, K1_SMEM, s>>>(in.stencil, d, out, vis);
+    else k_kick1<false><<<grid, ST_THREADS, K1_SMEM, s>>>(in.stencil, d, out, vis);
+}
+
+void launch_sweep_x(const DiskView& d, const CellMaps& in, Cell* out, cudaStream_t s) {
+    dim3 grid(cdiv(d.xres, SW_LEN), cdiv(d.yres, SW_W));
+    k_sweep<0><<<grid, SW_THREADS, SW_SMEM, s>>>(in.sweep_x, d, out);
+}
+
+void launch_sweep_y(const DiskView& d, const CellMaps& in, Cell* out, cudaStream_t s) {
+    dim3 grid(cdiv(d.yres, SW_LEN), cdiv(d.xres, SW_W));
+    k_sweep<1><<<grid, SW_THREADS, SW_SMEM, s>>>(in.sweep_y, d, out);
+}
+
+void launch_advect(const DiskView& d, const CellMaps& in, Cell* out, cudaStream_t s) {
+    dim3 grid(cdiv(d.yres, SW_LEN), cdiv(d.xres, SW_W));
+    k_advect<<<grid, SW_THREADS, SW_SMEM, s>>>(in.sweep_y, d, out);
+}
+
+void launch_kick2(const DiskView& d, const CellMaps& in, const VisMaps& vis, Cell* out, cudaStream_t s) {
+    dim3 grid(cdiv(d.xres, ST_TX), cdiv(d.yres, ST_TY));
+    if (d.visc && d.ndim == 2) k_kick2<true><<<grid, ST_THREADS, K5_SMEM, s>>>(in.stencil, vis.stencil, d, out);
+    else k_kick2<false><<<grid, ST_THREADS, K5_SMEM, s>>>(in.stencil, vis.stencil, d, out);
+}
+
+int kernels_per_step(const DiskView& d) {
+    int n = 1 /*time*/ + 1 /*kick1*/ + 1 /*sweep x*/ + 1 /*kick2*/;
+    if (d.ndim > 1) n += 1;
+    if (d.ndim > 1 && d.orbadv) n += 1;
+    return n;
+}
+
+}  // namespace pg

@@ -1,0 +1,140 @@
+"""One disk (or tube) on one B200, driven through the C ABI.
+
+``Disk`` owns its device state.  Its methods mirror the reference's host loop
+(main.cu:320-360): ``global_dt`` (src/timestep/timestep.cu:113) and ``solve``
+(src/solver/solve.cu:279) with host-side t and dt, or ``run`` which keeps t, dt
+and the planet on the device and replays the step as a CUDA graph.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from ._lib import PGBody, check, lib
+from .params import NPAD, Params, PGParams
+
+
+def _dp(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+class Disk:
+    def __init__(self, params: Params, device: int = 0, stream: int | None = None):
+        self.params = params
+        self._P = PGParams.from_params(params)
+        h = ctypes.c_void_p()
+        check(lib().pg_disk_create(ctypes.byref(self._P), device, ctypes.c_void_p(stream or 0), ctypes.byref(h)))
+        self._h = h
+        self.t = 0.0
+        self.dt = None
+
+    # --------------------------------------------------------------- state
+    def set_state(self, t: float, state: dict) -> None:
+        """Restart injection: interior fields (yres, xres), like load_grid."""
+        f = {k: np.ascontiguousarray(state[k], dtype=np.float64) for k in ("r", "p", "u")}
+        v = state.get("v")
+        vv = np.ascontiguousarray(v, dtype=np.float64) if v is not None else None
+        check(lib().pg_disk_set_state(self._h, t, _dp(f["r"]), _dp(f["p"]), _dp(f["u"]),
+                                      _dp(vv) if vv is not None else None))
+        self.t = t
+        self.dt = None
+
+    def get_state(self) -> dict:
+        shape = (self.params.yres, self.params.xres)
+        out = {k: np.empty(shape) for k in ("r", "p", "u", "v")}
+        t = ctypes.c_double()
+        check(lib().pg_disk_get_state(self._h, _dp(out["r"]), _dp(out["p"]), _dp(out["u"]), _dp(out["v"]),
+                                      ctypes.byref(t)))
+        out["t"] = t.value
+        return out
+
+    def state_ptr(self) -> int:
+        p = ctypes.c_void_p()
+        check(lib().pg_disk_state_ptr(self._h, ctypes.byref(p)))
+        return p.value
+
+    @property
+    def dims(self):
+        xa, ya, npad = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        check(lib().pg_disk_dims(self._h, ctypes.byref(xa), ctypes.byref(ya), ctypes.byref(npad)))
+        return xa.value, ya.value, npad.value
+
+    # ------------------------------------------------------------ stepping
+    def global_dt(self, dt_prev: float) -> float:
+        out = ctypes.c_double()
+        check(lib().pg_disk_global_dt(self._h, dt_prev, ctypes.byref(out)))
+        return out.value
+
+    def solve(self, t: float, dt: float) -> None:
+        check(lib().pg_disk_solve(self._h, t, dt))
+
+    def step_host(self, max_step: int, end_time: float = 1.0e30) -> int:
+        """main.cu:320-360 driven from the host: dt from global_dt, clipped at end_time."""
+        dt = self.dt if self.dt else end_time - self.t
+        n = 0
+        while n < max_step:
+            dt = self.global_dt(dt)
+            last = False
+            if self.t + dt > end_time:
+                dt = end_time - self.t
+                last = True
+            self.solve(self.t, dt)
+            self.t += dt
+            n += 1
+            if last:
+                break
+        self.dt = dt
+        return n
+
+    def run(self, nsteps: int, end_time: float = 1.0e30) -> None:
+        """nsteps of the device-resident loop (stream-ordered; call sync())."""
+        check(lib().pg_disk_run(self._h, nsteps, end_time))
+
+    def sync(self) -> None:
+        check(lib().pg_disk_sync(self._h))
+
+    def clock(self):
+        t, dt, n = ctypes.c_double(), ctypes.c_double(), ctypes.c_longlong()
+        check(lib().pg_disk_clock(self._h, ctypes.byref(t), ctypes.byref(dt), ctypes.byref(n)))
+        return t.value, dt.value, n.value
+
+    def planet(self) -> dict:
+        b = PGBody()
+        check(lib().pg_disk_planet(self._h, ctypes.byref(b)))
+        return {k: getattr(b, k) for k, _ in PGBody._fields_}
+
+    def check(self) -> None:
+        check(lib().pg_disk_check(self._h))
+
+    STAGES = ("time", "kick1", "sweep_x", "sweep_y", "advect", "kick2")
+
+    def profile(self, nsteps: int, end_time: float = 1.0e30) -> dict:
+        """Average ms per step of each stage (CUDA events between the launches)."""
+        ms = (ctypes.c_float * 6)()
+        check(lib().pg_disk_profile(self._h, nsteps, end_time, ms, 6))
+        return {k: float(ms[n]) for n, k in enumerate(self.STAGES)}
+
+    @property
+    def kernels_per_step(self) -> int:
+        return lib().pg_kernels_per_step(self._h)
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib().pg_disk_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def make_grid(params: Params):
+    """The library's host grid (faces and volumes with ghosts)."""
+    P = PGParams.from_params(params)
+    xarr, yarr = params.xres + 2 * NPAD, params.yres + 2 * params.ypad
+    xa, xv, ya, yv = np.zeros(xarr + 1), np.zeros(xarr), np.zeros(yarr + 1), np.zeros(yarr)
+    check(lib().pg_make_grid(ctypes.byref(P), _dp(xa), _dp(xv), _dp(ya), _dp(yv)))
+    return xa, xv, ya, yv

@@ -1,0 +1,207 @@
+"""Runtime physics/grid parameters of one disk (or tube).
+
+The reference fixes these at compile time in ``include/parameters.h``
+(flags ``:4-13``, grid ``:43-97``, hydro ``:115-127``, boundaries ``:140-149``,
+disk ``:155-171``, planet ``:177-188``, domain ``:194-207``).  Here they are a
+runtime struct so that one library build serves every configuration and so
+that an ensemble can carry different parameters per disk.  Field names keep
+the reference's spelling; ``kill_width_out`` and the dust fields are the only
+additions (the reference uses ``kill_width`` for both damping zones).
+
+``PGParams`` is the ctypes mirror of ``pg_params`` in ``include/penguin_b200.h``.
+"""
+from __future__ import annotations
+
+import ctypes
+import dataclasses
+import math
+
+PI = 3.1415926535897932384626434
+TWOPI = 2.0 * PI
+HPI = 0.5 * PI
+NPAD = 3  # recon_flag 6 (PPM on 4th-order slopes) -> 3 ghost cells (include/parameters.h:49-53)
+
+
+@dataclasses.dataclass
+class Params:
+    ndim: int = 2
+    xres: int = 1024
+    yres: int = 3072
+    geomx: int = 1          # 0 cartesian, 1 cylindrical radius
+    geomy: int = 3          # 0 cartesian, 3 azimuth
+    gridx: int = 1          # 0 linear, 1 logarithmic
+    gridy: int = 0
+    xmin: float = 0.4
+    xmax: float = 2.5
+    ymin: float = 0.0
+    ymax: float = TWOPI
+    EOS_flag: int = 0       # 0 locally isothermal, 2 adiabatic
+    internal_e_flag: int = 1
+    gam: float = 1.0
+    CFL: float = 0.3
+    bound_lft: int = 0      # 0 analytic initial state, 1 zero gradient, 2 reflecting
+    bound_rgh: int = 0
+    init_flag: int = 2      # 2 = polar disk (analytic state for ghosts and damping)
+    frame_omega: float = 1.0
+    p_alpha: float = 1.0
+    p_beta: float = 1.0
+    ss_alpha: float = 1.0e-3
+    sc_h: float = 0.05
+    planet_radius: float = 1.0
+    visc_flag: int = 1
+    OrbAdv_flag: int = 1
+    kill_flag: int = 1
+    kill_width: float = 5.0
+    kill_width_out: float = 2.4
+    n_planet: int = 1
+    planet_mass: float = 1.0e-3
+    planet_ecc: float = 0.0
+    rs_fac: float = 0.6
+    ramp_time: float = 10.0 * TWOPI
+    zmin: float = HPI - 4.0 * 0.05
+    zmax: float = HPI
+    dust_flag: int = 0
+    Stokes: float = 0.01
+    D_G_ratio: float = 0.01
+
+    # ----------------------------------------------------------------- sizes
+    @property
+    def ypad(self) -> int:
+        return NPAD if self.ndim > 1 else 0
+
+    @property
+    def xarr(self) -> int:
+        return self.xres + 2 * NPAD
+
+    @property
+    def yarr(self) -> int:
+        return self.yres + 2 * self.ypad
+
+    @property
+    def cells(self) -> int:
+        return self.xres * self.yres
+
+    def replace(self, **kw) -> "Params":
+        return dataclasses.replace(self, **kw)
+
+    def validate(self) -> None:
+        if self.ndim not in (1, 2):
+            raise ValueError("ndim must be 1 or 2")
+        if self.ndim == 1 and self.yres != 1:
+            raise ValueError("ndim 1 needs yres == 1")
+        if self.xres < 2 * NPAD or (self.ndim == 2 and self.yres < 2 * NPAD):
+            raise ValueError("resolution below the 3-cell stencil half-width")
+        if self.EOS_flag not in (0, 2):
+            raise ValueError("EOS_flag must be 0 (isothermal) or 2 (adiabatic)")
+        if self.geomx not in (0, 1) or self.geomy not in (0, 3):
+            raise ValueError("supported geometries: geomx 0/1, geomy 0/3")
+        if any(b not in (0, 1, 2) for b in (self.bound_lft, self.bound_rgh)):
+            raise ValueError("radial boundaries must be 0, 1 or 2")
+        if self.n_planet not in (0, 1):
+            raise ValueError("n_planet must be 0 or 1")
+
+
+class PGParams(ctypes.Structure):
+    """ctypes mirror of ``pg_params`` (include/penguin_b200.h)."""
+
+    _fields_ = [
+        ("ndim", ctypes.c_int), ("xres", ctypes.c_int), ("yres", ctypes.c_int),
+        ("geomx", ctypes.c_int), ("geomy", ctypes.c_int), ("gridx", ctypes.c_int), ("gridy", ctypes.c_int),
+        ("xmin", ctypes.c_double), ("xmax", ctypes.c_double), ("ymin", ctypes.c_double), ("ymax", ctypes.c_double),
+        ("eos_flag", ctypes.c_int), ("internal_e_flag", ctypes.c_int),
+        ("gam", ctypes.c_double), ("cfl", ctypes.c_double),
+        ("bound_lft", ctypes.c_int), ("bound_rgh", ctypes.c_int), ("init_flag", ctypes.c_int),
+        ("frame_omega", ctypes.c_double),
+        ("p_alpha", ctypes.c_double), ("p_beta", ctypes.c_double), ("ss_alpha", ctypes.c_double),
+        ("sc_h", ctypes.c_double), ("planet_radius", ctypes.c_double),
+        ("visc_flag", ctypes.c_int), ("orbadv_flag", ctypes.c_int), ("kill_flag", ctypes.c_int),
+        ("kill_width", ctypes.c_double), ("kill_width_out", ctypes.c_double),
+        ("n_planet", ctypes.c_int),
+        ("planet_mass", ctypes.c_double), ("planet_ecc", ctypes.c_double),
+        ("rs_fac", ctypes.c_double), ("ramp_time", ctypes.c_double),
+        ("zmin", ctypes.c_double), ("zmax", ctypes.c_double),
+        ("dust_flag", ctypes.c_int),
+        ("stokes", ctypes.c_double), ("d_g_ratio", ctypes.c_double),
+    ]
+
+    @classmethod
+    def from_params(cls, p: Params) -> "PGParams":
+        p.validate()
+        return cls(
+            p.ndim, p.xres, p.yres, p.geomx, p.geomy, p.gridx, p.gridy,
+            p.xmin, p.xmax, p.ymin, p.ymax, p.EOS_flag, p.internal_e_flag, p.gam, p.CFL,
+            p.bound_lft, p.bound_rgh, p.init_flag, p.frame_omega,
+            p.p_alpha, p.p_beta, p.ss_alpha, p.sc_h, p.planet_radius,
+            p.visc_flag, p.OrbAdv_flag, p.kill_flag, p.kill_width, p.kill_width_out,
+            p.n_planet, p.planet_mass, p.planet_ecc, p.rs_fac, p.ramp_time, p.zmin, p.zmax,
+            p.dust_flag, p.Stokes, p.D_G_ratio,
+        )
+
+
+# --------------------------------------------------------------- workloads
+def sod_tube(n: int = 1024) -> Params:
+    """1D Sod shock tube: uniform cartesian cells on [0,1], gamma 1.4, total-energy
+    form, PPM + HLLC, CFL 0.5, zero-gradient (outflow) ends."""
+    return Params(
+        ndim=1, xres=n, yres=1, geomx=0, geomy=0, gridx=0, gridy=0,
+        xmin=0.0, xmax=1.0, ymin=0.0, ymax=1.0, zmin=0.0, zmax=1.0,
+        EOS_flag=2, internal_e_flag=0, gam=1.4, CFL=0.5,
+        bound_lft=1, bound_rgh=1, init_flag=1,
+        visc_flag=0, OrbAdv_flag=0, kill_flag=0, n_planet=1, planet_mass=0.0,
+    )
+
+
+def planet_disk(nr: int = 1024, nphi: int = 3072, *, q: float = 1.0e-3, alpha: float = 1.0e-3,
+                h: float = 0.05, rmin: float = 0.4, rmax: float = 2.5,
+                kill_in: float = 0.5, kill_out: float = 2.2, ramp_orbits: float = 10.0) -> Params:
+    """2D polar planet-disk: log-spaced radii, uniform azimuth, locally isothermal
+    with flat h/r (p_beta 1), Sigma ~ r^-1 (p_alpha 1), alpha viscosity, one planet
+    on a fixed circular orbit at r=1 with smoothing 0.6 H and a mass ramp, wave
+    damping inside ``kill_in`` and outside ``kill_out``, orbital advection on.
+
+    The damping widths are expressed like the reference's ``kill_width`` (units of
+    H at the domain edge): inner = (kill_in - rmin) / H(rmin), outer = (rmax -
+    kill_out) / H(rmax), with H = h r.
+    """
+    kw_in = (kill_in - rmin) / (h * rmin)
+    kw_out = (rmax - kill_out) / (h * rmax)
+    return Params(
+        ndim=2, xres=nr, yres=nphi, xmin=rmin, xmax=rmax, sc_h=h, ss_alpha=alpha,
+        planet_mass=q, rs_fac=0.6, ramp_time=ramp_orbits * TWOPI,
+        kill_width=kw_in, kill_width_out=kw_out, zmin=HPI - 4.0 * h,
+    )
+
+
+def reference_disk(nr: int, nphi: int, **kw) -> Params:
+    """Planet-disk variant that the reference can run as-is: it has a single
+    ``kill_width`` for both damping zones (src/killwave/killwave.cu:30-34), so
+    both widths are set to the outer one (2.4 H)."""
+    p = planet_disk(nr, nphi, **kw)
+    return p.replace(kill_width=p.kill_width_out)
+
+
+# ------------------------------------------------------------- host maths
+def make_grid_np(amin: float, amax: float, res: int, pad: int, geom: int, grid: int):
+    """Faces and cell 'volumes' with ghosts (src/init/init.cu:472-500).  The C
+    library builds the authoritative copy with the same formulas; this numpy
+    version is used only to place initial conditions."""
+    import numpy as np
+
+    a = np.zeros(res + 2 * pad + 1)
+    i = np.arange(res + 1, dtype=np.float64)
+    if grid == 1:
+        a[pad:pad + res + 1] = amin * np.exp(math.log(amax / amin) * i / float(res))
+        for k in range(pad):
+            a[k] = amin * math.exp(math.log(amax / amin) * float(k - pad) / float(res))
+            a[res + pad + 1 + k] = amin * math.exp(math.log(amax / amin) * float(res + 1 + k) / float(res))
+    else:
+        a[pad:pad + res + 1] = amin + (amax - amin) * i / float(res)
+        for k in range(pad):
+            a[k] = a[pad] - (a[2 * pad - k] - a[pad])
+            a[res + pad + 1 + k] = a[res + pad] + (a[res + pad] - a[res + pad - 1 - k])
+    dr = a[1:] - a[:-1]
+    if geom == 1:
+        v = dr * (a[:-1] + dr / 2.0)
+    else:
+        v = dr.copy()
+    return a, v

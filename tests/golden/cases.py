@@ -1,0 +1,68 @@
+"""Golden cases: configurations on which the unmodified reference was run (on a
+B200, built for sm_100a by oracle/ref_build.py) from restart-injected initial
+states.  make_golden.py in this folder generates the fixtures; the tests compare
+the oracle and the CUDA path against them.
+"""
+from __future__ import annotations
+
+import math
+import os
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+from penguin_b200 import params as P  # noqa: E402
+
+T0_DISK = 5.0 * 2.0 * math.pi      # restart at 5 orbits: planet mass halfway up its 10-orbit ramp
+SEED = 7
+
+
+def _disk64():
+    return P.reference_disk(64, 192)
+
+
+def _disk32(**kw):
+    return P.reference_disk(32, 96).replace(**kw)
+
+
+def cases() -> list[dict]:
+    """name, params, initial-state kind/seed, restart time, step limit, end time."""
+    sod = P.sod_tube(1024)
+    out = [
+        dict(name="sod_n1", params=sod, init="sod", t0=0.0, max_step=1, end_time=0.2),
+        dict(name="sod_n10", params=sod, init="sod", t0=0.0, max_step=10, end_time=0.2),
+        dict(name="sod_t02", params=sod, init="sod", t0=0.0, max_step=1000000000, end_time=0.2),
+    ]
+    for n in (1, 10, 50):
+        out.append(dict(name=f"disk64_n{n}", params=_disk64(), init="disk", t0=T0_DISK, max_step=n, end_time=1.0e30))
+    variants = {
+        "sweeps": dict(visc_flag=0, OrbAdv_flag=0, kill_flag=0, planet_mass=0.0),
+        "visc": dict(visc_flag=1, OrbAdv_flag=0, kill_flag=0, planet_mass=0.0),
+        "orbadv": dict(visc_flag=0, OrbAdv_flag=1, kill_flag=0, planet_mass=0.0),
+        "kill_planet": dict(visc_flag=0, OrbAdv_flag=0, kill_flag=1),
+    }
+    for k, kw in variants.items():
+        out.append(dict(name=f"disk32_{k}_n10", params=_disk32(**kw), init="disk", t0=T0_DISK, max_step=10,
+                        end_time=1.0e30))
+    return out
+
+
+def timing_cases() -> list[dict]:
+    """Full-size planet-disk runs of the reference, used only to time it on the B200."""
+    c2 = P.reference_disk(1024, 3072)
+    return [
+        dict(name="ref_disk1024_n20", params=c2, init="disk", t0=T0_DISK, max_step=20, end_time=1.0e30),
+        dict(name="ref_disk1024_n220", params=c2, init="disk", t0=T0_DISK, max_step=220, end_time=1.0e30),
+    ]
+
+
+def initial_state(case: dict) -> dict:
+    from penguin_b200 import initial as I
+
+    p = case["params"]
+    if case["init"] == "sod":
+        return I.sod_state(p)
+    return I.disk_state(p, seed=SEED)

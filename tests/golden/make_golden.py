@@ -1,0 +1,132 @@
+"""Generate the golden fixtures by running the unmodified reference.
+
+Three phases:
+  build    (here, where the reference sources are):  compile one reference binary
+           per case into oracle/_ref/<case>/ with oracle/ref_build.py;
+  run      (on a B200):  for each case write the restart file, run
+           ``penguin init.bin 0`` in the case folder and save the reference's
+           output snapshot plus the initial state as <out>/<case>.npz;
+  collect  (here):  copy the .npz files of the golden cases into tests/golden/.
+
+    python tests/golden/make_golden.py build
+    python tests/golden/make_golden.py run --out gpurun_out/golden [--timing]
+    python tests/golden/make_golden.py collect --src gpurun_out/golden
+"""
+from __future__ import annotations
+
+import argparse
+import dataclasses
+import glob
+import json
+import os
+import re
+import shutil
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, HERE)
+
+import cases as C  # noqa: E402
+from oracle import ref_build  # noqa: E402
+from penguin_b200 import snapshot  # noqa: E402
+from penguin_b200.params import make_grid_np  # noqa: E402
+
+
+def _all(timing: bool):
+    return C.cases() + (C.timing_cases() if timing else [])
+
+
+def build(timing: bool, jobs: int) -> None:
+    for c in _all(timing):
+        hdr = ref_build.parameters_h(dataclasses.asdict(c["params"]), c["max_step"], c["end_time"])
+        t = time.time()
+        exe = ref_build.build_case(c["name"], hdr, jobs=jobs)
+        print(f"{c['name']}: {exe} ({time.time() - t:.0f} s)", flush=True)
+
+
+def run(out: str, timing: bool, only: str | None) -> int:
+    os.makedirs(out, exist_ok=True)
+    bad = 0
+    for c in _all(timing):
+        if only and not re.search(only, c["name"]):
+            continue
+        p = c["params"]
+        d = os.path.join(ref_build.REF_OUT, c["name"])
+        exe = os.path.join(d, "penguin")
+        if not os.path.exists(exe):
+            print(f"{c['name']}: missing {exe}", flush=True)
+            bad += 1
+            continue
+        for f in glob.glob(os.path.join(d, "binary_*")):
+            os.remove(f)
+        st = C.initial_state(c)
+        xa, _ = make_grid_np(p.xmin, p.xmax, p.xres, 3, p.geomx, p.gridx)
+        ya, _ = make_grid_np(p.ymin, p.ymax, p.yres, 3 if p.ndim > 1 else 0, p.geomy, p.gridy)
+        init = os.path.join(d, "init.bin")
+        snapshot.write_snapshot(init, c["t0"], xa[3:3 + p.xres + 1], ya[3:3 + p.yres + 1] if p.ndim > 1 else None,
+                                st, p.ndim)
+        t = time.time()
+        r = subprocess.run(["./penguin", "init.bin", "0"], cwd=d, capture_output=True, text=True, timeout=900)
+        wall = time.time() - t
+        outs = sorted(glob.glob(os.path.join(d, "binary_*_00001")))
+        sps = re.findall(r"([0-9.eE+-]+) seconds per step", r.stdout)
+        print(f"{c['name']}: rc={r.returncode} wall={wall:.2f}s s/step={sps[-1] if sps else '?'} out={outs}",
+              flush=True)
+        with open(os.path.join(out, c["name"] + ".log"), "w") as f:
+            f.write(r.stdout + "\n--- stderr ---\n" + r.stderr)
+        if r.returncode != 0 or not outs:
+            bad += 1
+            continue
+        if c["name"].startswith("ref_"):
+            os.remove(outs[0])
+            with open(os.path.join(out, c["name"] + ".json"), "w") as f:
+                json.dump({"seconds_per_step": float(sps[-1]) if sps else None, "wall_s": wall,
+                           "steps": c["max_step"], "cells": p.xres * p.yres}, f)
+            continue
+        res = snapshot.read_snapshot(outs[0], p.xres, p.yres, p.ndim)
+        keys = ["r", "p", "u"] + (["v"] if p.ndim > 1 else [])
+        np.savez_compressed(
+            os.path.join(out, c["name"] + ".npz"),
+            t0=c["t0"], t=res["t"], max_step=c["max_step"], end_time=c["end_time"],
+            params=json.dumps(dataclasses.asdict(p)),
+            **{"init_" + k: np.asarray(st[k], dtype=np.float64) for k in keys},
+            **{"out_" + k: res[k] for k in keys},
+        )
+    return bad
+
+
+def collect(src: str) -> None:
+    for c in C.cases():
+        f = os.path.join(src, c["name"] + ".npz")
+        if os.path.exists(f):
+            shutil.copy(f, os.path.join(HERE, c["name"] + ".npz"))
+            print("collected", c["name"])
+        else:
+            print("missing", f)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("phase", choices=["build", "run", "collect"])
+    ap.add_argument("--out", default="gpurun_out/golden")
+    ap.add_argument("--src", default="gpurun_out/golden")
+    ap.add_argument("--timing", action="store_true")
+    ap.add_argument("--only", default=None)
+    ap.add_argument("--jobs", type=int, default=6)
+    a = ap.parse_args()
+    if a.phase == "build":
+        build(a.timing, a.jobs)
+    elif a.phase == "run":
+        sys.exit(1 if run(a.out, a.timing, a.only) else 0)
+    else:
+        collect(a.src)
+
+
+if __name__ == "__main__":
+    main()
