@@ -1,0 +1,46 @@
+"""The reference's own main.cu, relinked through penguin_b200/shim against
+libpenguin_b200.so, run on a golden case.  Needs a B200
+and the relinked executable (built next to the reference objects by
+__graft_entry__.build() where the reference sources are available)."""
+import glob
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import cases as C
+from penguin_b200 import snapshot
+from penguin_b200.params import make_grid_np
+
+pytestmark = pytest.mark.gpu
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+
+
+def rel_l1(a, b):
+    return np.abs(a - b).sum() / np.abs(b).sum()
+
+
+@pytest.mark.parametrize("name", ["disk64_n10"])
+def test_relinked_main_reproduces_reference(name, tmp_path):
+    exe = os.path.join(ROOT, "oracle", "_ref", name, "dropin", "penguin")
+    fx = os.path.join(GOLDEN, name + ".npz")
+    if not os.path.exists(exe) or not os.path.exists(fx):
+        pytest.skip("relinked executable or fixture not available")
+    case = [c for c in C.cases() if c["name"] == name][0]
+    p = case["params"]
+    z = np.load(fx)
+    xa, _ = make_grid_np(p.xmin, p.xmax, p.xres, 3, p.geomx, p.gridx)
+    ya, _ = make_grid_np(p.ymin, p.ymax, p.yres, 3, p.geomy, p.gridy)
+    st = {k: z["init_" + k] for k in ("r", "p", "u", "v")}
+    snapshot.write_snapshot(str(tmp_path / "init.bin"), float(z["t0"]), xa[3:3 + p.xres + 1],
+                            ya[3:3 + p.yres + 1], st, 2)
+    r = subprocess.run([exe, "init.bin", "0"], cwd=tmp_path, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    out = glob.glob(str(tmp_path / "binary_*_00001"))
+    assert out, r.stdout
+    res = snapshot.read_snapshot(out[0], p.xres, p.yres, 2)
+    assert res["t"] == pytest.approx(float(z["t"]), rel=1e-13)
+    for k in ("r", "p", "u", "v"):
+        assert rel_l1(res[k], z["out_" + k]) < 1e-12, k

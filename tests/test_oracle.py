@@ -15,16 +15,22 @@ from penguin_b200 import params as P
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 
-# Relative L1 tolerance of the oracle against the reference's own GPU output.
 # The oracle evaluates the reference's expressions in the same order but without
-# FMA contraction and with glibc's pow/sin; killwave's FP32 __sinf ramp is
-# evaluated with sinf.  Measured differences are <= 2e-12 on every fixture.
-TOL_ORACLE_VS_REF = 1.0e-11
+# FMA contraction and with glibc's pow/sin/sincos; killwave's FP32 __sinf ramp is
+# evaluated with sinf.  Each golden case carries its relative-L1 bound ("tol",
+# tests/golden/cases.py) for density, pressure and momentum.
 
 
 def rel_l1(a, b):
     den = np.abs(b).sum()
     return np.abs(a - b).sum() / den if den > 0 else np.abs(a - b).sum()
+
+
+def momentum_l1(a, b):
+    """relative L1 of the momentum vector (rho u, rho v)"""
+    ax, ay = a["r"] * a["u"], a["r"] * a.get("v", 0 * a["r"])
+    bx, by = b["r"] * b["u"], b["r"] * b.get("v", 0 * b["r"])
+    return (np.abs(ax - bx) + np.abs(ay - by)).sum() / (np.abs(bx) + np.abs(by)).sum()
 
 
 def _load(name):
@@ -45,10 +51,14 @@ def test_oracle_matches_reference(case):
         assert np.isfinite(z["out_" + k]).all(), f"reference output {k} not finite"
     o = Oracle(p, st, float(z["t0"]))
     o.run(int(z["max_step"]), float(z["end_time"]))
-    assert o.t == pytest.approx(float(z["t"]), rel=1e-13, abs=1e-15)
+    assert o.t == pytest.approx(float(z["t"]), rel=max(1e-13, case["tol"]), abs=1e-15)
     out = o.interior()
-    for k in keys:
-        assert rel_l1(out[k], z["out_" + k]) < TOL_ORACLE_VS_REF, k
+    ref = {k: z["out_" + k] for k in keys}
+    for k in ("r", "p"):
+        assert rel_l1(out[k], ref[k]) < case["tol"], (k, rel_l1(out[k], ref[k]))
+    if p.ndim == 1:
+        out["v"] = 0 * out["r"]
+    assert momentum_l1(out, ref) < case["tol"], momentum_l1(out, ref)
 
 
 def test_initial_state_regenerates_fixture():
@@ -99,5 +109,6 @@ def test_disk_quiet_without_planet():
     o = Oracle(p, st, 0.0)
     o.run(20)
     out = o.interior()
-    assert np.abs(out["u"]).max() < 1e-3
-    assert rel_l1(out["r"], st["r"]) < 1e-4
+    mid = slice(p.xres // 4, 3 * p.xres // 4)  # away from the boundary-adjustment layers
+    assert np.abs(out["u"][:, mid]).max() < 1e-4
+    assert rel_l1(out["r"][:, mid], st["r"][:, mid]) < 1e-4
