@@ -33,15 +33,21 @@ def cases() -> list[dict]:
     # tol: relative-L1 bound (density, pressure and momentum) between the oracle and
     # the reference's own output, set from the measured differences with margin.
     # Cases with the planet amplify rounding-level differences near it step by step.
+    # cuda_tol: the same bound for the CUDA path against the reference's output.  It
+    # is tighter than tol on the disks (same CUDA math library as the reference) and
+    # looser on the Sod tube, where the precomputed slope weights round differently
+    # from the reference's per-call moment algebra and the limiter / monotonicity
+    # branches at the discontinuities amplify that (measured 3.8e-10 after 10 steps).
     sod = P.sod_tube(1024)
     out = [
-        dict(name="sod_n1", params=sod, init="sod", t0=0.0, max_step=1, end_time=0.2, tol=1e-14),
-        dict(name="sod_n10", params=sod, init="sod", t0=0.0, max_step=10, end_time=0.2, tol=1e-11),
-        dict(name="sod_t02", params=sod, init="sod", t0=0.0, max_step=1000000000, end_time=0.2, tol=5e-12),
+        dict(name="sod_n1", params=sod, init="sod", t0=0.0, max_step=1, end_time=0.2, tol=1e-14, cuda_tol=1e-14),
+        dict(name="sod_n10", params=sod, init="sod", t0=0.0, max_step=10, end_time=0.2, tol=1e-11, cuda_tol=1e-9),
+        dict(name="sod_t02", params=sod, init="sod", t0=0.0, max_step=1000000000, end_time=0.2, tol=5e-12,
+             cuda_tol=5e-10),
     ]
-    for n, tol in ((1, 1e-12), (10, 1e-10), (50, 1e-9)):
+    for n, tol, ctol in ((1, 1e-12, 1e-13), (10, 1e-10, 2e-12), (50, 1e-9, 1e-10)):
         out.append(dict(name=f"disk64_n{n}", params=_disk64(), init="disk", t0=T0_DISK, max_step=n, end_time=1.0e30,
-                        tol=tol))
+                        tol=tol, cuda_tol=ctol))
     variants = {
         "sweeps": dict(visc_flag=0, OrbAdv_flag=0, kill_flag=0, planet_mass=0.0),
         "visc": dict(visc_flag=1, OrbAdv_flag=0, kill_flag=0, planet_mass=0.0),
@@ -50,7 +56,7 @@ def cases() -> list[dict]:
     }
     for k, kw in variants.items():
         out.append(dict(name=f"disk32_{k}_n10", params=_disk32(**kw), init="disk", t0=T0_DISK, max_step=10,
-                        end_time=1.0e30, tol=2e-12 if k == "kill_planet" else 1e-14))
+                        end_time=1.0e30, tol=2e-12 if k == "kill_planet" else 1e-14, cuda_tol=1e-13))
     return out
 
 

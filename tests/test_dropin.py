@@ -41,6 +41,9 @@ def test_relinked_main_reproduces_reference(name, tmp_path):
     out = glob.glob(str(tmp_path / "binary_*_00001"))
     assert out, r.stdout
     res = snapshot.read_snapshot(out[0], p.xres, p.yres, 2)
-    assert res["t"] == pytest.approx(float(z["t"]), rel=1e-13)
-    for k in ("r", "p", "u", "v"):
-        assert rel_l1(res[k], z["out_" + k]) < 1e-12, k
+    assert res["t"] == pytest.approx(float(z["t"]), rel=max(1e-13, case["cuda_tol"]))
+    for k in ("r", "p"):
+        assert rel_l1(res[k], z["out_" + k]) < case["cuda_tol"], k
+    mx, my = res["r"] * res["u"], res["r"] * res["v"]
+    rx, ry = z["out_r"] * z["out_u"], z["out_r"] * z["out_v"]
+    assert (np.abs(mx - rx) + np.abs(my - ry)).sum() / (np.abs(rx) + np.abs(ry)).sum() < case["cuda_tol"]
