@@ -58,6 +58,15 @@ struct DiskView {
     const double* nux;    // get_nu(xc(i))
     const double* initx;  // init_C(xc(i)) (5 per i; the disk's analytic state is axisymmetric)
     const double* killx;  // per i: {ramp_in, tau_in, ramp_out, tau_out} (0 ramp = no damping)
+    const double* idx_x;  // 1 / (xa[i+1] - xa[i])
+    const double* ixv;    // 1 / xv[i]
+    const double* irad;   // 1 / xc(i)
+    const double* gstar;  // star gravity -r/|r|^3 at xc(i) (z = 0)
+    const double* visx;   // per i: 1/(r[i+1]-r[i-1]), 1/(r[i+1]-r[i]), 1/(r[i]-r[i-1]), 1/(0.5 (r[i+1]-r[i-1])), 1/r[i]
+    const double* idx_y;  // 1 / (ya[j+1] - ya[j])
+    const double* iyv;    // 1 / yv[j]
+    const double* visy;   // per j: 1/(t[j+1]-t[j-1]), 1/(t[j+1]-t[j]), 1/(t[j]-t[j-1]), 1/(0.5 (t[j+1]-t[j-1]))
+    double* trig;         // per step, per row: sin, cos of (azimuth - planet y) for planet_cur, then planet_next
     const double* rot;    // orb_rot
     double* res;          // orb_res
     int* inc;             // orb_inc

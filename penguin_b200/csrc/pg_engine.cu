@@ -301,8 +301,9 @@ static pg_status engine_setup(Engine& E, const double* dev_xa, const double* dev
         PG_CUDA(cudaMemcpyAsync(ya.data(), dev_ya, sizeof(double) * (yarr + 1), cudaMemcpyDeviceToHost, E.stream));
         PG_CUDA(cudaStreamSynchronize(E.stream));
     }
-    // tables: wx[6 xarr] wy[6 yarr] radx cs2x nux initx(5) killx(4) [xarr each] ycraw ycj [yarr each]
-    const size_t ntab = 6 * (size_t)xarr + 6 * (size_t)yarr + 12 * (size_t)xarr + 2 * (size_t)yarr;
+    // tables: wx[6 xarr] wy[6 yarr] | radx cs2x nux initx(5) killx(4) idx_x ixv irad gstar visx(5) [xarr each]
+    //         | ycraw ycj idx_y iyv visy(4) [yarr each] | trig [4 yarr + 2]
+    const size_t ntab = 6 * (size_t)xarr + 6 * (size_t)yarr + 21 * (size_t)xarr + 8 * (size_t)yarr + 4 * (size_t)yarr + 2;
     PG_CUDA(cudaMalloc(&E.tab, sizeof(double) * ntab));
     std::vector<double> wx(6 * xarr), wy(6 * yarr);
     recon_weights(P.geomx, xa.data(), xarr, wx.data());
@@ -349,8 +350,18 @@ static pg_status engine_setup(Engine& E, const double* dev_xa, const double* dev
     d.nux = t + 2 * xarr;
     d.initx = t + 3 * xarr;
     d.killx = t + 8 * xarr;
-    d.ycraw = t + 12 * xarr;
-    d.ycj = t + 12 * xarr + yarr;
+    d.idx_x = t + 12 * xarr;
+    d.ixv = t + 13 * xarr;
+    d.irad = t + 14 * xarr;
+    d.gstar = t + 15 * xarr;
+    d.visx = t + 16 * xarr;
+    d.ycraw = t + 21 * xarr;
+    d.ycj = t + 21 * xarr + yarr;
+    d.idx_y = t + 21 * xarr + 2 * yarr;
+    d.iyv = t + 21 * xarr + 3 * yarr;
+    d.visy = t + 21 * xarr + 4 * yarr;
+    d.trig = t + 21 * xarr + 8 * yarr;
+    PG_CUDA(cudaMemsetAsync(d.trig, 0, sizeof(double) * (4 * (size_t)yarr + 2), E.stream));
     d.rot = E.rot;
     d.res = E.res;
     d.inc = E.inc;

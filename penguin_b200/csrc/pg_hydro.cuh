@@ -66,14 +66,14 @@ __device__ __forceinline__ double aveR(const Frac& f, const Par& p) {
 __device__ __forceinline__ double lim01(double a) { return fmin(fmax(a, 0.0), 1.0); }  // solve.cu:14
 __device__ __forceinline__ double exp_lim(double x) { return fmax(1.0 + x, 1.0e-6); }    // solve.cu:29
 
-// Shock flattening coefficient of the middle cell (src/solver/recon/PPM.cu:7-62).
-__device__ __forceinline__ double flatten(double gam, double r0, double pm2, double pm1, double p0, double pp1,
-                                          double pp2, double um1, double u0, double up1) {
-    const double cs = sqrt(gam * p0 / r0);
+// Shock flattening coefficient of the middle cell (src/solver/recon/PPM.cu:7-62);
+// inv_cs = 1/sqrt(gam p0 / r0) is shared with the interface states.
+__device__ __forceinline__ double flatten(double inv_cs, double p0, double pm2, double pm1, double pp1, double pp2,
+                                          double um1, double u0, double up1) {
     const double dp1f = pp1 - p0, dp2f = pp2 - pm1;
     const double dp1b = p0 - pm1, dp2b = pp1 - pm2;
-    const double Mf = (u0 - up1) / cs;
-    const double Mb = (um1 - u0) / cs;
+    const double Mf = (u0 - up1) * inv_cs;
+    const double Mb = (um1 - u0) * inv_cs;
     double f = 0.0;
     if ((Mf > 0.0 || Mb > 0.0) && dp2f != 0.0 && dp2b != 0.0) {
         double ddp = 10.0 * fmax(0.0, fabs(dp1f / dp2f - 0.5) - 0.25);
@@ -90,37 +90,38 @@ struct Half {
 };
 
 // Interface state on the LEFT edge of a cell = the right state of the face
-// below it (src/solver/riemann/states.cu:151-206).  xl/xr: faces of the cell,
-// sdt: dt/rad, r0c/p0c/u0c: cell averages.
-__device__ __forceinline__ Half state_at_left_edge(double gam, double xl, double xr, double sdt, double r0c,
-                                                   double p0c, double u0c, const Par& R, const Par& Pp,
+// below it (src/solver/riemann/states.cu:151-206).  xl: left face, idx = 1/(xr-xl),
+// sdt: dt/rad, cs0 = sqrt(gam p/r) of the cell averages r0c, p0c, u0c.
+__device__ __forceinline__ Half state_at_left_edge(double gam, double xl, double idx, double sdt, double cs0,
+                                                   double r0c, double p0c, double u0c, const Par& R, const Par& Pp,
                                                    const Par& U, const Par& V, const Par& W) {
     const double hdt = 0.5 * sdt;
-    double cs = sqrt(gam * p0c / r0c);
     double tmp = fmin(u0c, 0.0);
-    tmp = xl - tmp * sdt + cs * sdt;
-    Frac q = frac_left(lim01((tmp - xl) / (xr - xl)));
+    tmp = xl - tmp * sdt + cs0 * sdt;
+    Frac q = frac_left(lim01((tmp - xl) * idx));
     const double rmin = r0c * 1.0e-10, pmin = p0c * 1.0e-10;
     const double ur = aveL(q, U);
     const double dis = fmin(ur, 0.0) * sdt;
     tmp = xl - dis;
-    q = frac_left(lim01((tmp - xl) / (xr - xl)));
+    q = frac_left(lim01((tmp - xl) * idx));
     double r0 = aveL(q, R), p0 = aveL(q, Pp);
     const double u0 = aveL(q, U);
     r0 = fmax(r0, rmin);
     p0 = fmax(p0, pmin);
-    cs = sqrt(gam * p0 / r0);
+    const double ir0 = 1.0 / r0;
+    const double cs = sqrt(gam * p0 * ir0);
     tmp = xl - dis + cs * sdt;
-    q = frac_left(lim01((tmp - xl) / (xr - xl)));
+    q = frac_left(lim01((tmp - xl) * idx));
     double u_ = aveL(q, U), p_ = aveL(q, Pp);
-    u_ = 2.0 * (u_ - u0) / (cs * sdt);
-    p_ = 2.0 * (p_ - p0) / (cs * sdt);
+    const double k = 2.0 / (cs * sdt);
+    u_ = (u_ - u0) * k;
+    p_ = (p_ - p0) * k;
     u_ *= -hdt;
     p_ *= -hdt;
     Half s;
     s.r = r0 * exp_lim(u_);
     s.p = p0 * exp_lim(gam * u_);
-    s.u = u0 + p_ / r0 + 0.0;
+    s.u = u0 + p_ * ir0 + 0.0;
     s.v = aveL(q, V);
     s.w = aveL(q, W);
     return s;
@@ -128,35 +129,36 @@ __device__ __forceinline__ Half state_at_left_edge(double gam, double xl, double
 
 // Interface state on the RIGHT edge of a cell = the left state of the face
 // above it (src/solver/riemann/states.cu:210-264).
-__device__ __forceinline__ Half state_at_right_edge(double gam, double xl, double xr, double sdt, double r0c,
-                                                    double p0c, double u0c, const Par& R, const Par& Pp,
-                                                    const Par& U, const Par& V, const Par& W) {
+__device__ __forceinline__ Half state_at_right_edge(double gam, double xl, double xr, double idx, double sdt,
+                                                    double cs0, double r0c, double p0c, double u0c, const Par& R,
+                                                    const Par& Pp, const Par& U, const Par& V, const Par& W) {
     const double hdt = 0.5 * sdt;
-    double cs = sqrt(gam * p0c / r0c);
     double tmp = fmax(u0c, 0.0);
-    tmp = xr - tmp * sdt - cs * sdt;
-    Frac q = frac_right(lim01((tmp - xl) / (xr - xl)));
+    tmp = xr - tmp * sdt - cs0 * sdt;
+    Frac q = frac_right(lim01((tmp - xl) * idx));
     const double rmin = r0c * 1.0e-10, pmin = p0c * 1.0e-10;
     const double ul = aveR(q, U);
     const double dis = fmax(ul, 0.0) * sdt;
     tmp = xr - dis;
-    q = frac_right(lim01((tmp - xl) / (xr - xl)));
+    q = frac_right(lim01((tmp - xl) * idx));
     double r0 = aveR(q, R), p0 = aveR(q, Pp);
     const double u0 = aveR(q, U);
     r0 = fmax(r0, rmin);
     p0 = fmax(p0, pmin);
-    cs = sqrt(gam * p0 / r0);
+    const double ir0 = 1.0 / r0;
+    const double cs = sqrt(gam * p0 * ir0);
     tmp = xr - dis - cs * sdt;
-    q = frac_right(lim01((tmp - xl) / (xr - xl)));
+    q = frac_right(lim01((tmp - xl) * idx));
     double u_ = aveR(q, U), p_ = aveR(q, Pp);
-    u_ = 2.0 * (u0 - u_) / (cs * sdt);
-    p_ = 2.0 * (p0 - p_) / (cs * sdt);
+    const double k = 2.0 / (cs * sdt);
+    u_ = (u0 - u_) * k;
+    p_ = (p0 - p_) * k;
     u_ *= -hdt;
     p_ *= -hdt;
     Half s;
     s.r = r0 * exp_lim(u_);
     s.p = p0 * exp_lim(gam * u_);
-    s.u = u0 + p_ / r0 + 0.0;
+    s.u = u0 + p_ * ir0 + 0.0;
     s.v = aveR(q, V);
     s.w = aveR(q, W);
     return s;
@@ -186,7 +188,10 @@ struct Flux {
 };
 
 // Wave speeds (src/solver/riemann/wave_speeds.cu:24-35, 288-333) and the HLLC
-// fluxes (src/solver/riemann/HLLC.cu:10-77) at one face, us = 0.
+// fluxes (src/solver/riemann/HLLC.cu:10-77) at one face, us = 0.  The reference
+// forms all four candidate fluxes and picks one by the signs of sl, sr, sm
+// (HLLC.cu:2-8); here the signs are tested first and only the selected
+// candidate is formed.
 __device__ __forceinline__ Flux hllc(int eos, int ie, double gam, const Half& L, const Half& R) {
     const double cl = sqrt(gam * L.p / L.r);
     const double cr = sqrt(gam * R.p / R.r);
@@ -194,62 +199,50 @@ __device__ __forceinline__ Flux hllc(int eos, int ie, double gam, const Half& L,
     const double p_ = 0.5 * (R.p + L.p);
     const double pm = p_ * exp_lim(0.5 * gam * (L.u - R.u) / c_);
     const double srl = sqrt(L.r), srr = sqrt(R.r);
-    const double u_ = (srl * L.u + srr * R.u) / (srl + srr);
-    const double n2 = 0.5 * srl * srr / ((srl + srr) * (srl + srr));
-    const double cc = sqrt((cl * cl * srl + cr * cr * srr) / (srl + srr) + n2 * (R.u - L.u) * (R.u - L.u));
+    const double is = 1.0 / (srl + srr);
+    const double u_ = (srl * L.u + srr * R.u) * is;
+    const double n2 = 0.5 * srl * srr * (is * is);
+    const double cc = sqrt((cl * cl * srl + cr * cr * srr) * is + n2 * (R.u - L.u) * (R.u - L.u));
     const double sl = u_ - cc, sr = u_ + cc;
     double sm = (L.r * L.u * cl + R.r * R.u * cr) / (L.r * cl + R.r * cr);
-    sm += (L.p - R.p) / (L.r + R.r) / (0.5 * (cl + cr));
-    sm += 0.0 * (fmax(L.u, 0.0) + fmax(-R.u, 0.0)) / (cl + cr);
+    sm += (L.p - R.p) / ((L.r + R.r) * (0.5 * (cl + cr)));
 
+    // side of every upwinded quantity: left iff sl >= 0, or sr >= 0 and sm >= 0
+    const bool left = (signbit(sl) == 0) || (signbit(sr) == 0 && signbit(sm) == 0);
+    const Half& S = left ? L : R;
     Flux F;
-    double fl = L.u * L.r;
-    double f_l = sm * L.r * (sl - L.u) / (sl - sm);
-    double f_r = sm * R.r * (sr - R.u) / (sr - sm);
-    double fr = R.u * R.r;
-    F.r = pick(fl, f_l, f_r, fr, sl, sm, sr);
-    F.u = pick(L.u, L.u, R.u, R.u, sl, sm, sr) * F.r;
-    F.v = pick(L.v, L.v, R.v, R.v, sl, sm, sr) * F.r;
-    F.w = pick(L.w, L.w, R.w, R.w, sl, sm, sr) * F.r;
-    if (eos > 0) {
-        const double el = energy(eos, ie, gam, L.r, L.p, L.u, 0.0, 0.0);
-        const double er = energy(eos, ie, gam, R.r, R.p, R.u, 0.0, 0.0);
-        F.p = pick(el, el, er, er, sl, sm, sr) * F.r;
-    } else {
-        F.p = 0.0;
+    if (signbit(sl) == 0 || signbit(sr) != 0) {  // supersonic: the upwind state's own fluxes
+        F.r = S.u * S.r;
+        F.pres = S.p;
+        F.uprs = (ie == 0) ? S.u * S.p : S.u;
+    } else {  // star region on the side of the contact
+        const double s_ = left ? sl : sr;
+        const double inv = 1.0 / (s_ - sm);
+        F.r = sm * S.r * (s_ - S.u) * inv;
+        F.pres = (s_ * pm - sm * S.p) * inv;
+        if (ie == 0) F.uprs = sm * (s_ * pm - S.u * S.p) * inv;
+        else F.uprs = sm * (s_ * pm - S.u * S.p) / (s_ * pm - sm * S.p);
     }
-    fl = L.p;
-    f_l = (sl * pm - sm * L.p) / (sl - sm);
-    f_r = (sr * pm - sm * R.p) / (sr - sm);
-    fr = R.p;
-    F.pres = pick(fl, f_l, f_r, fr, sl, sm, sr);
-    if (eos == 2) {
-        if (ie == 0) {
-            fl = L.u * L.p;
-            f_l = sm * (sl * pm - L.u * L.p) / (sl - sm);
-            f_r = sm * (sr * pm - R.u * R.p) / (sr - sm);
-            fr = R.u * R.p;
-        } else {
-            fl = L.u;
-            f_l = sm * (sl * pm - L.u * L.p) / (sl * pm - sm * L.p);
-            f_r = sm * (sr * pm - R.u * R.p) / (sr * pm - sm * R.p);
-            fr = R.u;
-        }
-        F.uprs = pick(fl, f_l, f_r, fr, sl, sm, sr);
-    } else {
-        F.uprs = 0.0;
-    }
+    F.u = S.u * F.r;
+    F.v = S.v * F.r;
+    F.w = S.w * F.r;
+    F.p = (eos > 0) ? energy(eos, ie, gam, S.r, S.p, S.u, 0.0, 0.0) * F.r : 0.0;
+    if (eos != 2) F.uprs = 0.0;
     return F;
 }
 
-// Conservative update with floors (src/solver/sweeps.cu:218-261).  cs2: get_cs2 at the cell.
+// Conservative update with floors (src/solver/sweeps.cu:218-261).  cs2: get_cs2
+// at the cell.  For the isothermal EOS the energy slot is dead (it is
+// overwritten by cs2 r), so it is not formed.
 __device__ __forceinline__ Cell update_cell(int eos, int ie, double gam, double cs2, Cell Q, const Cell& D,
                                             int* floor_hits) {
     const double r_min = fmax(Q.r * 1.0e-10, SMALLR);
     const double p_min = fmax(Q.p * 1.0e-10, SMALLP);
     const double u_old = Q.u, v_old = Q.v, w_old = Q.w;
-    Q.p = energy(eos, ie, gam, Q.r, Q.p, Q.u, Q.v, Q.w);
-    Q.p *= Q.r;
+    if (eos == 2) {
+        Q.p = energy(eos, ie, gam, Q.r, Q.p, Q.u, Q.v, Q.w);
+        Q.p *= Q.r;
+    }
     Q.u *= Q.r;
     Q.v *= Q.r;
     Q.w *= Q.r;
@@ -258,9 +251,10 @@ __device__ __forceinline__ Cell update_cell(int eos, int ie, double gam, double 
     Q.u += D.u;
     Q.v += D.v;
     Q.w += D.w;
-    Q.u /= Q.r;
-    Q.v /= Q.r;
-    Q.w /= Q.r;
+    const double ir = 1.0 / Q.r;
+    Q.u *= ir;
+    Q.v *= ir;
+    Q.w *= ir;
     if (Q.r < r_min) {
         Q.r = r_min;
         Q.p = p_min;

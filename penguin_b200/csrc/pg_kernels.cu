@@ -104,26 +104,22 @@ struct Grav {
     double gx, gy, gz;
 };
 // Star + planet gravity in the 2D cylindrical frame (src/solver/force/forces.cu:41-58,
-// 182-327 with twobd_flag 0, pol = 0).
-__device__ __forceinline__ Grav gravity(const DiskView& d, double rad, double azi, const pg_body& p) {
+// 182-327 with twobd_flag 0, pol = 0).  The star term is a per-radius table; the
+// planet's angle enters through the per-row sin/cos table of this step
+// (k_planet_trig) and 1/x_p^2 through the table's tail.
+__device__ __forceinline__ Grav gravity(const DiskView& d, int i, double rad, double sinfac, double cosfac,
+                                        double iplx2, const pg_body& p) {
     Grav g{0.0, 0.0, 0.0};
     if (d.geomx == 1) {
-        const double pol = 0.0;
-        const double dis = sqrt(rad * rad + pol * pol);
-        g.gx = -rad / dis / dis / dis;
-        g.gz = -pol / dis / dis / dis;
+        g.gx = d.gstar[i];
+        g.gz = -0.0;
         if (d.nplanet > 0) {
-            double sinfac, cosfac;
-            sincos(azi - (p.y + 0.0 * p.vy), &sinfac, &cosfac);
             const double plm = p.m, plx = p.x;
-            const double Rp = sqrt(rad * rad + plx * plx - 2.0 * plx * rad * cosfac + pol * pol + p.rs * p.rs);
-            const double rs_fac = 1.0 / Rp / Rp / Rp;
-            const double fx = -plm * (rad - plx * cosfac) * rs_fac - plm * cosfac / plx / plx;
-            const double fy = -plm * plx * sinfac * rs_fac + plm * sinfac / plx / plx;
-            const double fz = -plm * pol * rs_fac;
-            g.gx += fx;
-            g.gy += fy;
-            g.gz += fz;
+            const double Rp = sqrt(rad * rad + plx * plx - 2.0 * plx * rad * cosfac + p.rs * p.rs);
+            const double ir = 1.0 / Rp;
+            const double rs_fac = ir * ir * ir;
+            g.gx += -plm * (rad - plx * cosfac) * rs_fac - plm * cosfac * iplx2;
+            g.gy += -plm * plx * sinfac * rs_fac + plm * sinfac * iplx2;
         }
     }
     return g;
@@ -133,25 +129,26 @@ __device__ __forceinline__ Grav gravity(const DiskView& d, double rad, double az
 // gravity and viscous acceleration; with mdt != 0 the forces are re-evaluated
 // at the mdt-predicted velocities (sweeps.cu:663-687).
 template <bool VISC>
-__device__ __forceinline__ Cell kick(const DiskView& d, const Cell& C, double x, const Grav& g, double vx,
+__device__ __forceinline__ Cell kick(const DiskView& d, const Cell& C, double ix, const Grav& g, double vx,
                                      double vy, double mdt, double dt) {
     Cell T = C;
-    double fx = (d.geomx == 1) ? T.v * T.v / x : 0.0;
+    const double ir = VISC ? 1.0 / C.r : 0.0;  // T.r == C.r throughout
+    double fx = (d.geomx == 1) ? T.v * T.v * ix : 0.0;
     double fy = 0.0;
     const double fz = 0.0;
     if (VISC) {
-        fx += vx / T.r;
-        if (d.ndim > 1) fy += vy / T.r;
+        fx += vx * ir;
+        if (d.ndim > 1) fy += vy * ir;
     }
     if (mdt != 0.0) {
         T.u = C.u + fx * mdt + g.gx * mdt;
         T.v = C.v + fy * mdt + g.gy * mdt;
         T.w = C.w + fz * mdt + g.gz * mdt;
-        fx = (d.geomx == 1) ? T.v * T.v / x : 0.0;
+        fx = (d.geomx == 1) ? T.v * T.v * ix : 0.0;
         fy = 0.0;
         if (VISC) {
-            fx += vx / T.r;
-            if (d.ndim > 1) fy += vy / T.r;
+            fx += vx * ir;
+            if (d.ndim > 1) fy += vy * ir;
         }
     }
     Cell o;
@@ -165,32 +162,34 @@ __device__ __forceinline__ Cell kick(const DiskView& d, const Cell& C, double x,
 
 // Viscous force density of the middle cell of a 3x3 stencil
 // (src/viscosity/viscosity.cu:9-22, 84-194, ndim 2).  Stencil order: n<3 row j,
-// 3..5 row j-1, 6..8 row j+1, columns i-1..i+1; r: xc, t: yc, nu: get_nu.
-__device__ __forceinline__ void viscous(const double* r, const double* t, const double* u, const double* v,
-                                        const double* nr, double& fx_out, double& fy_out) {
-    const double dudx = (u[2] - u[0]) / (r[2] - r[0]);
-    const double d2udx2 = ((u[2] - u[1]) / (r[2] - r[1]) - (u[1] - u[0]) / (r[1] - r[0])) / (0.5 * (r[2] - r[0]));
-    const double dndx = (nr[2] - nr[0]) / (r[2] - r[0]);
-    const double dvdx = (v[2] - v[0]) / (r[2] - r[0]);
-    const double d2vdx2 = ((v[2] - v[1]) / (r[2] - r[1]) - (v[1] - v[0]) / (r[1] - r[0])) / (0.5 * (r[2] - r[0]));
-    const double dvdy = (v[7] - v[4]) / (t[2] - t[0]) / r[1];
-    const double d2vdy2 =
-        ((v[7] - v[1]) / (t[2] - t[1]) - (v[1] - v[4]) / (t[1] - t[0])) / (0.5 * (t[2] - t[0])) / r[1] / r[1];
-    const double d2vdxy = (v[8] - v[6] - v[5] + v[3]) / (r[2] - r[0]) / (t[2] - t[0]) / r[1];
-    const double dudy = (u[7] - u[4]) / (t[2] - t[0]) / r[1];
-    const double d2udy2 =
-        ((u[7] - u[1]) / (t[2] - t[1]) - (u[1] - u[4]) / (t[1] - t[0])) / (0.5 * (t[2] - t[0])) / r[1] / r[1];
-    const double d2udxy = (u[8] - u[6] - u[5] + u[3]) / (r[2] - r[0]) / (t[2] - t[0]) / r[1];
-    const double dndy = (nr[7] - nr[4]) / (t[2] - t[0]) / r[1];
+// 3..5 row j-1, 6..8 row j+1, columns i-1..i+1.  The grid spacings enter as
+// per-index reciprocals: X = {1/(r2-r0), 1/(r2-r1), 1/(r1-r0), 1/(0.5(r2-r0)), 1/r1},
+// Y = {1/(t2-t0), 1/(t2-t1), 1/(t1-t0), 1/(0.5(t2-t0))}.
+__device__ __forceinline__ void viscous(const double* __restrict__ X, const double* __restrict__ Y, const double* u,
+                                        const double* v, const double* nr, double& fx_out, double& fy_out) {
+    const double i_r20 = X[0], i_r21 = X[1], i_r10 = X[2], i_hr20 = X[3], i_r1 = X[4];
+    const double i_t20 = Y[0], i_t21 = Y[1], i_t10 = Y[2], i_ht20 = Y[3];
+    const double dudx = (u[2] - u[0]) * i_r20;
+    const double d2udx2 = ((u[2] - u[1]) * i_r21 - (u[1] - u[0]) * i_r10) * i_hr20;
+    const double dndx = (nr[2] - nr[0]) * i_r20;
+    const double dvdx = (v[2] - v[0]) * i_r20;
+    const double d2vdx2 = ((v[2] - v[1]) * i_r21 - (v[1] - v[0]) * i_r10) * i_hr20;
+    const double dvdy = (v[7] - v[4]) * i_t20 * i_r1;
+    const double d2vdy2 = ((v[7] - v[1]) * i_t21 - (v[1] - v[4]) * i_t10) * i_ht20 * i_r1 * i_r1;
+    const double d2vdxy = (v[8] - v[6] - v[5] + v[3]) * i_r20 * i_t20 * i_r1;
+    const double dudy = (u[7] - u[4]) * i_t20 * i_r1;
+    const double d2udy2 = ((u[7] - u[1]) * i_t21 - (u[1] - u[4]) * i_t10) * i_ht20 * i_r1 * i_r1;
+    const double d2udxy = (u[8] - u[6] - u[5] + u[3]) * i_r20 * i_t20 * i_r1;
+    const double dndy = (nr[7] - nr[4]) * i_t20 * i_r1;
 
     const double sxx = 2.0 * nr[1] * dudx;
-    double fx = 2.0 * dndx * dudx + 2.0 * nr[1] * d2udx2 + sxx / r[1];
-    const double syy = 2.0 * nr[1] * (dvdy + u[1] / r[1]);
-    const double sxy = nr[1] * (dudy + dvdx - v[1] / r[1]);
-    double fy = 2.0 * dndy * dvdy + 2.0 * nr[1] * d2vdy2 + 2.0 * nr[1] * dudy / r[1] + 2.0 * dndy * u[1] / r[1];
-    fx += dndy * (dudy + dvdx) + nr[1] * (d2udy2 + d2vdxy) - dndy * v[1] / r[1] - nr[1] * dvdy / r[1] - syy / r[1];
-    fy += dndx * (dudy + dvdx) + nr[1] * (d2udxy + d2vdx2) - dndx * v[1] / r[1] - nr[1] * dvdx / r[1] +
-          nr[1] * v[1] / r[1] / r[1] + 2.0 * sxy / r[1];
+    double fx = 2.0 * dndx * dudx + 2.0 * nr[1] * d2udx2 + sxx * i_r1;
+    const double syy = 2.0 * nr[1] * (dvdy + u[1] * i_r1);
+    const double sxy = nr[1] * (dudy + dvdx - v[1] * i_r1);
+    double fy = 2.0 * dndy * dvdy + 2.0 * nr[1] * d2vdy2 + 2.0 * nr[1] * dudy * i_r1 + 2.0 * dndy * u[1] * i_r1;
+    fx += dndy * (dudy + dvdx) + nr[1] * (d2udy2 + d2vdxy) - dndy * v[1] * i_r1 - nr[1] * dvdy * i_r1 - syy * i_r1;
+    fy += dndx * (dudy + dvdx) + nr[1] * (d2udxy + d2vdx2) - dndx * v[1] * i_r1 - nr[1] * dvdx * i_r1 +
+          nr[1] * v[1] * i_r1 * i_r1 + 2.0 * sxy * i_r1;
     fx_out = fx;
     fy_out = fy;
 }
@@ -210,16 +209,14 @@ __device__ __forceinline__ void gather9(const double* tile, int hx, int hy, cons
 }
 
 __device__ __forceinline__ double signal_rate(const DiskView& d, const Cell& c, int i, int j) {
-    // src/timestep/timestep.cu:46-77
+    // src/timestep/timestep.cu:46-77 (cell widths as reciprocals)
     const double rad_cyl = (d.geomy == 3) ? d.radx[i] : 1.0;
     const double cs = sqrt(d.gam * c.p / c.r);
     double spd = fabs(c.u) + cs;
-    double wid = fabs(d.xa[i + 1] - d.xa[i]);
-    double tmp = fmax(spd / wid, 0.0);
+    double tmp = fmax(spd * d.idx_x[i], 0.0);
     if (d.ndim > 1) {
         spd = fabs(c.v - rad_cyl * d.frame_omega - d.rot[i]) + cs;
-        wid = fabs(d.ya[j + 1] - d.ya[j]) * rad_cyl;
-        tmp = fmax(spd / wid, tmp);
+        tmp = fmax(spd * (d.idx_y[j] * ((d.geomy == 3) ? d.irad[i] : 1.0)), tmp);
     }
     return tmp;
 }
@@ -305,10 +302,11 @@ __global__ void __launch_bounds__(SW_THREADS, 2)
         const int s = s0 - NPAD + t;
         const int qq = q0 + q;
         double r[5], p[5], u[5], v[5], w[5];
-        double rad = 1.0, rot = 0.0;
+        double rad = 1.0, rot = 0.0, irad_q = 1.0;
         if (DIR == 1) {
             const int i = min(qq, d.xarr - 1);
             rad = (d.geomy == 3) ? d.radx[i] : 1.0;
+            irad_q = (d.geomy == 3) ? d.irad[i] : 1.0;
             rot = d.rot[i];
         }
 #pragma unroll
@@ -329,19 +327,21 @@ __global__ void __launch_bounds__(SW_THREADS, 2)
                 w[k] = c[2];
             }
         }
-        const double flat = flatten(gam, r[2], p[0], p[1], p[2], p[3], p[4], u[1], u[2], u[3]);
+        const double cs0 = sqrt(gam * p[2] / r[2]);
+        const double flat = flatten(1.0 / cs0, p[2], p[0], p[1], p[3], p[4], u[1], u[2], u[3]);
         const int sc_ = (DIR == 0) ? min(s, d.xarr - 1) : min(s, d.yarr - 1);
         const double* wt = ((DIR == 0) ? d.wx : d.wy) + 6 * sc_;
         const double* fa = (DIR == 0) ? d.xa : d.ya;
+        const double idx = ((DIR == 0) ? d.idx_x : d.idx_y)[sc_];
         const Par R = recon(wt, r[0], r[1], r[2], r[3], r[4], flat);
         const Par P = recon(wt, p[0], p[1], p[2], p[3], p[4], flat);
         const Par U = recon(wt, u[0], u[1], u[2], u[3], u[4], flat);
         const Par V = recon(wt, v[0], v[1], v[2], v[3], v[4], flat);
         const Par W = recon(wt, w[0], w[1], w[2], w[3], w[4], flat);
         const double xl = fa[sc_], xr = fa[sc_ + 1];
-        const double sdt = (DIR == 0) ? dt : dt / rad;
-        const Half a = state_at_left_edge(gam, xl, xr, sdt, r[2], p[2], u[2], R, P, U, V, W);
-        const Half b = state_at_right_edge(gam, xl, xr, sdt, r[2], p[2], u[2], R, P, U, V, W);
+        const double sdt = (DIR == 0) ? dt : dt * irad_q;
+        const Half a = state_at_left_edge(gam, xl, idx, sdt, cs0, r[2], p[2], u[2], R, P, U, V, W);
+        const Half b = state_at_right_edge(gam, xl, xr, idx, sdt, cs0, r[2], p[2], u[2], R, P, U, V, W);
         st[0 * SW_NST + it] = a.r;
         st[1 * SW_NST + it] = a.p;
         st[2 * SW_NST + it] = a.u;
@@ -415,16 +415,16 @@ __global__ void __launch_bounds__(SW_THREADS, 2)
             const double* c = (DIR == 0) ? tile + (q * SW_TL + t) * 5 : tile + (t * SWY_COLS + (q + 1)) * 5;
             const Cell C0{c[0], c[1], c[2], c[3], c[4]};
             if (DIR == 0) {
-                const double f = dt / d.xv[s];
+                const double f = dt * d.ixv[s];
                 D.r *= f; D.p *= f; D.u *= f; D.v *= f; D.w *= f;
-                if (d.geomx == 1) D.v /= d.radx[s];
+                if (d.geomx == 1) D.v *= d.irad[s];
                 const Cell Q = update_cell(d.eos, d.ie, gam, d.cs2x[s], C0, D, &sc->floor_hits);
                 if (!(Q.r > 0.0)) atomicOr(&sc->err, 1 << PG_ERR_NAN);
                 emit(d, out, s, qq, Q);
             } else {
                 const double rad = (d.geomy == 3) ? d.radx[qq] : 1.0;
                 const double rot = d.rot[qq];
-                const double f = dt / d.yv[s] / rad;
+                const double f = dt * d.iyv[s] * ((d.geomy == 3) ? d.irad[qq] : 1.0);
                 D.r *= f; D.p *= f; D.u *= f; D.v *= f; D.w *= f;
                 if (d.geomy == 3) D.u += (rot + rad * d.frame_omega) * D.r;
                 else D.u += rot * D.r;
@@ -466,9 +466,9 @@ __global__ void __launch_bounds__(SW_THREADS, 2)
         const int t = 2 + tid / SW_W;
         const int s = min(s0 - NPAD + t, d.yarr - 1);
         const int i = min(q0 + q, d.xarr - 1);
-        const double rad = (d.geomy == 3) ? d.radx[i] : 1.0;
         const double speed = d.res[i];
-        const double sdt = dt / rad;
+        const double sdt = dt * ((d.geomy == 3) ? d.irad[i] : 1.0);
+        const double idx = d.idx_y[s];
         double r[5], p[5], u[5], v[5], w[5];
 #pragma unroll
         for (int k = 0; k < 5; ++k) {
@@ -486,7 +486,7 @@ __global__ void __launch_bounds__(SW_THREADS, 2)
         int face;
         if (speed > 0.0) {  // this cell is upwind of its upper face
             const double x0 = xr - speed * sdt;
-            const Frac q_ = frac_right(lim01((x0 - xl) / (xr - xl)));
+            const Frac q_ = frac_right(lim01((x0 - xl) * idx));
             fr = aveR(q_, R);
             fp = aveR(q_, P);
             fu = aveR(q_, U) * fr;
@@ -495,7 +495,7 @@ __global__ void __launch_bounds__(SW_THREADS, 2)
             face = t + 1;
         } else {  // ... of its lower face
             const double x0 = xl - speed * sdt;
-            const Frac q_ = frac_left(lim01((x0 - xl) / (xr - xl)));
+            const Frac q_ = frac_left(lim01((x0 - xl) * idx));
             fr = aveL(q_, R);
             fp = aveL(q_, P);
             fu = aveL(q_, U) * fr;
@@ -526,11 +526,10 @@ __global__ void __launch_bounds__(SW_THREADS, 2)
             D.u = fl[2 * NFL + k0] * 1.0 - fl[2 * NFL + k1] * 1.0;
             D.v = fl[3 * NFL + k0] * 1.0 - fl[3 * NFL + k1] * 1.0;
             D.w = fl[4 * NFL + k0] * 1.0 - fl[4 * NFL + k1] * 1.0;
-            const double rad = (d.geomy == 3) ? d.radx[i] : 1.0;
-            double f = dt / d.yv[s];
+            double f = dt * d.iyv[s];
             D.r *= f; D.p *= f; D.u *= f; D.v *= f; D.w *= f;
             if (d.geomy > 2) {
-                f = 1.0 / rad;
+                f = d.irad[i];
                 D.r *= f; D.p *= f; D.u *= f; D.v *= f; D.w *= f;
             }
             const double* c = tile + (t * SWY_COLS + (q + 1)) * 5;
@@ -543,9 +542,10 @@ __global__ void __launch_bounds__(SW_THREADS, 2)
             Q.u += D.w;
             Q.v += D.u;
             Q.w += D.v;
-            Q.u /= Q.r;
-            Q.v /= Q.r;
-            Q.w /= Q.r;
+            const double ir = 1.0 / Q.r;
+            Q.u *= ir;
+            Q.v *= ir;
+            Q.w *= ir;
             if (d.eos == 0) Q.p = d.cs2x[i] * Q.r;
             if (!(Q.r > 0.0)) atomicOr(&sc->err, 1 << PG_ERR_NAN);
             emit(d, out, i, s, Q);
@@ -575,15 +575,11 @@ __global__ void __launch_bounds__(ST_THREADS)
     const Cell C{c[0], c[1], c[2], c[3], c[4]};
     double vx = 0.0, vy = 0.0;
     if (VISC) {
-        double r[3], t[3], nu[3], u[9], v[9], nr[9];
+        double nu[3], u[9], v[9], nr[9];
 #pragma unroll
-        for (int n = 0; n < 3; ++n) {
-            r[n] = d.radx[i + n - 1];
-            t[n] = d.ycraw[j + n - 1];
-            nu[n] = d.nux[i + n - 1];
-        }
+        for (int n = 0; n < 3; ++n) nu[n] = d.nux[i + n - 1];
         gather9(tile, hx, hy, nu, u, v, nr);
-        viscous(r, t, u, v, nr, vx, vy);
+        viscous(d.visx + 5 * i, d.visy + 4 * j, u, v, nr, vx, vy);
         // the stress is kept for the predictor of kick2, with its periodic images
         const size_t k = (size_t)i + (size_t)d.xarr * j;
         vis[2 * k] = vx;
@@ -597,9 +593,9 @@ __global__ void __launch_bounds__(ST_THREADS)
             vis[2 * m + 1] = vy;
         }
     }
-    const double y = (d.ndim > 1) ? d.ycj[j] + d.rot[i] * 0.0 : 0.0;
-    const Grav g = gravity(d, d.radx[i], y, sc->planet_cur);
-    const Cell Q = kick<VISC>(d, C, d.radx[i], g, vx, vy, 0.0, hdt);
+    const double* tr = d.trig + 4 * j;
+    const Grav g = gravity(d, i, d.radx[i], tr[0], tr[1], d.trig[4 * d.yarr], sc->planet_cur);
+    const Cell Q = kick<VISC>(d, C, d.irad[i], g, vx, vy, 0.0, hdt);
     emit(d, out, i, j, Q);
 }
 
@@ -632,6 +628,7 @@ __global__ void __launch_bounds__(ST_THREADS)
     if (!mbar_wait(bar, 0, sc)) return;
     const double dt = sc->dt, hdt = 0.5 * dt;
     const pg_body pl = sc->planet_next;
+    const double iplx2 = d.trig[4 * d.yarr + 1];
 
     if (VISC) {
         // predictor (sweeps.cu:713-729 with mdt = dt = dt/2) on the tile and its halo
@@ -641,9 +638,9 @@ __global__ void __launch_bounds__(ST_THREADS)
             if (i < NPAD || i >= NPAD + d.xres || j < 0 || j >= d.yarr) continue;
             const double* c = tile + it * 5;
             const Cell C{c[0], c[1], c[2], c[3], c[4]};
-            const double y = d.ycj[j] + d.rot[i] * 0.0;
-            const Grav g = gravity(d, d.radx[i], y, pl);
-            const Cell Q = kick<true>(d, C, d.radx[i], g, tvis[2 * it], tvis[2 * it + 1], hdt, hdt);
+            const double* tr = d.trig + 4 * j + 2;
+            const Grav g = gravity(d, i, d.radx[i], tr[0], tr[1], iplx2, pl);
+            const Cell Q = kick<true>(d, C, d.irad[i], g, tvis[2 * it], tvis[2 * it + 1], hdt, hdt);
             double* o = tp + it * 5;
             o[0] = Q.r; o[1] = Q.p; o[2] = Q.u; o[3] = Q.v; o[4] = Q.w;
         }
@@ -679,19 +676,15 @@ __global__ void __launch_bounds__(ST_THREADS)
         const Cell C{c[0], c[1], c[2], c[3], c[4]};
         double vx = 0.0, vy = 0.0;
         if (VISC) {
-            double r[3], t[3], nu[3], u[9], v[9], nr[9];
+            double nu[3], u[9], v[9], nr[9];
 #pragma unroll
-            for (int n = 0; n < 3; ++n) {
-                r[n] = d.radx[i + n - 1];
-                t[n] = d.ycraw[j + n - 1];
-                nu[n] = d.nux[i + n - 1];
-            }
+            for (int n = 0; n < 3; ++n) nu[n] = d.nux[i + n - 1];
             gather9(tp, hx, hy, nu, u, v, nr);
-            viscous(r, t, u, v, nr, vx, vy);
+            viscous(d.visx + 5 * i, d.visy + 4 * j, u, v, nr, vx, vy);
         }
-        const double y = (d.ndim > 1) ? d.ycj[j] + d.rot[i] * 0.0 : 0.0;
-        const Grav g = gravity(d, d.radx[i], y, pl);
-        Cell Q = kick<VISC>(d, C, d.radx[i], g, vx, vy, hdt, hdt);
+        const double* tr = d.trig + 4 * j + 2;
+        const Grav g = gravity(d, i, d.radx[i], tr[0], tr[1], iplx2, pl);
+        Cell Q = kick<VISC>(d, C, d.irad[i], g, vx, vy, hdt, hdt);
         if (d.kill) {
             // killwave (src/killwave/killwave.cu:48-100): relax towards init_C
             const double* kt = d.killx + 4 * i;
@@ -828,7 +821,7 @@ __device__ inline double ramping_fac(double x) {  // killwave.cu:8-14
 }
 
 __global__ void k_init_tables(const DiskView d, TabArgs a, double* radx, double* cs2x, double* nux, double* initx,
-                              double* killx, double* rot, double* ycraw, double* ycj) {
+                              double* killx, double* rot, double* ycraw, double* ycj, double* xrec, double* yrec) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k < d.xarr) {
         const double x = 0.5 * (d.xa[k + 1] + d.xa[k]);
@@ -856,6 +849,26 @@ __global__ void k_init_tables(const DiskView d, TabArgs a, double* radx, double*
                 kt[2] = ramping_fac(f);
             }
         }
+        // reciprocals and star gravity; xrec layout: idx_x, ixv, irad, gstar [xarr each], visx [5 xarr]
+        xrec[k] = 1.0 / (d.xa[k + 1] - d.xa[k]);
+        xrec[d.xarr + k] = 1.0 / d.xv[k];
+        xrec[2 * d.xarr + k] = 1.0 / x;
+        if (a.geomx == 1) {
+            const double dis = sqrt(x * x + 0.0 * 0.0);
+            xrec[3 * d.xarr + k] = -x / dis / dis / dis;  // forces.cu:203-204
+        } else {
+            xrec[3 * d.xarr + k] = 0.0;
+        }
+        double* vx = xrec + 4 * d.xarr + 5 * k;
+        vx[0] = vx[1] = vx[2] = vx[3] = vx[4] = 0.0;
+        if (k >= 1 && k + 1 < d.xarr) {
+            const double r0 = 0.5 * (d.xa[k] + d.xa[k - 1]), r2 = 0.5 * (d.xa[k + 2] + d.xa[k + 1]);
+            vx[0] = 1.0 / (r2 - r0);
+            vx[1] = 1.0 / (r2 - x);
+            vx[2] = 1.0 / (x - r0);
+            vx[3] = 1.0 / (0.5 * (r2 - r0));
+            vx[4] = 1.0 / x;
+        }
     }
     if (k < d.yarr) {
         ycraw[k] = 0.5 * (d.ya[k + 1] + d.ya[k]);
@@ -865,6 +878,37 @@ __global__ void k_init_tables(const DiskView d, TabArgs a, double* radx, double*
             else if (k >= d.ypad + d.yres) jm = k - d.yres;
         }
         ycj[k] = 0.5 * (d.ya[jm + 1] + d.ya[jm]);
+        // yrec layout: idx_y, iyv [yarr each], visy [4 yarr]
+        yrec[k] = 1.0 / (d.ya[k + 1] - d.ya[k]);
+        yrec[d.yarr + k] = 1.0 / d.yv[k];
+        double* vy = yrec + 2 * d.yarr + 4 * k;
+        vy[0] = vy[1] = vy[2] = vy[3] = 0.0;
+        if (k >= 1 && k + 1 < d.yarr) {
+            const double t0 = 0.5 * (d.ya[k] + d.ya[k - 1]), t1 = 0.5 * (d.ya[k + 1] + d.ya[k]);
+            const double t2 = 0.5 * (d.ya[k + 2] + d.ya[k + 1]);
+            vy[0] = 1.0 / (t2 - t0);
+            vy[1] = 1.0 / (t2 - t1);
+            vy[2] = 1.0 / (t1 - t0);
+            vy[3] = 1.0 / (0.5 * (t2 - t0));
+        }
+    }
+}
+
+// Per row, sin and cos of (azimuth - planet angle) for the planet of the first
+// half-kick and for the planet at t+dt, and 1/x_p^2 of both (forces.cu:41-58).
+__global__ void k_planet_trig(const DiskView d) {
+    const Scalars* sc = d.sc;
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    const pg_body& a = sc->planet_cur;
+    const pg_body& b = sc->planet_next;
+    if (j < d.yarr) {
+        double* t = d.trig + 4 * j;
+        sincos(d.ycj[j] - (a.y + 0.0 * a.vy), &t[0], &t[1]);
+        sincos(d.ycj[j] - (b.y + 0.0 * b.vy), &t[2], &t[3]);
+    }
+    if (j == 0) {
+        d.trig[4 * d.yarr] = 1.0 / a.x / a.x;
+        d.trig[4 * d.yarr + 1] = 1.0 / b.x / b.x;
     }
 }
 
@@ -934,17 +978,19 @@ void launch_init_tables(const DiskView& d, const pg_params& P, double* tab, cuda
     TabArgs a{P.sc_h, P.planet_radius, P.p_alpha, P.p_beta, P.ss_alpha, P.frame_omega, P.xmin, P.xmax,
               P.kill_width, P.kill_width_out > 0.0 ? P.kill_width_out : P.kill_width,
               P.visc_flag, P.orbadv_flag, P.kill_flag, P.init_flag, P.geomx};
-    // tab layout (doubles): radx[xarr] cs2x[xarr] nux[xarr] initx[5 xarr] killx[4 xarr] ycraw[yarr] ycj[yarr]
+    // tab layout (doubles), see table_layout() in pg_engine.cu
     double* radx = tab;
     double* cs2x = radx + d.xarr;
     double* nux = cs2x + d.xarr;
     double* initx = nux + d.xarr;
     double* killx = initx + 5 * d.xarr;
-    double* ycraw = killx + 4 * d.xarr;
+    double* xrec = killx + 4 * d.xarr;    // 9 xarr
+    double* ycraw = xrec + 9 * d.xarr;
     double* ycj = ycraw + d.yarr;
+    double* yrec = ycj + d.yarr;          // 6 yarr
     const int n = d.xarr > d.yarr ? d.xarr : d.yarr;
     k_init_tables<<<cdiv(n, 128), 128, 0, s>>>(d, a, radx, cs2x, nux, initx, killx, const_cast<double*>(d.rot),
-                                                ycraw, ycj);
+                                                ycraw, ycj, xrec, yrec);
 }
 
 void launch_init_xghosts(const DiskView& d, Cell* buf, cudaStream_t s) {
@@ -964,8 +1010,14 @@ void launch_cfl(const DiskView& d, const Cell* buf, cudaStream_t s) {
     k_cfl<<<blocks, 256, 0, s>>>(d, buf);
 }
 
-void launch_set_time(const DiskView& d, double t, double dt, cudaStream_t s) { k_set_time<<<1, 1, 0, s>>>(d, t, dt); }
-void launch_time_step(const DiskView& d, cudaStream_t s) { k_time_step<<<1, 1, 0, s>>>(d); }
+void launch_set_time(const DiskView& d, double t, double dt, cudaStream_t s) {
+    k_set_time<<<1, 1, 0, s>>>(d, t, dt);
+    k_planet_trig<<<cdiv(d.yarr, 256), 256, 0, s>>>(d);
+}
+void launch_time_step(const DiskView& d, cudaStream_t s) {
+    k_time_step<<<1, 1, 0, s>>>(d);
+    k_planet_trig<<<cdiv(d.yarr, 256), 256, 0, s>>>(d);
+}
 
 void launch_init_planet(const DiskView& d, const pg_params& P, double t, cudaStream_t s) {
     const double a = P.planet_radius;
@@ -1001,7 +1053,7 @@ void launch_kick2(const DiskView& d, const CellMaps& in, const VisMaps& vis, Cel
 }
 
 int kernels_per_step(const DiskView& d) {
-    int n = 1 /*time*/ + 1 /*kick1*/ + 1 /*sweep x*/ + 1 /*kick2*/;
+    int n = 2 /*time, planet trig*/ + 1 /*kick1*/ + 1 /*sweep x*/ + 1 /*kick2*/;
     if (d.ndim > 1) n += 1;
     if (d.ndim > 1 && d.orbadv) n += 1;
     return n;
