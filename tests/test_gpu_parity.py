@@ -131,8 +131,11 @@ def test_mass_conserved_closed_box():
     d.sync()
     g = d.get_state()
     assert abs(g["r"].sum() / r.sum() - 1.0) < 1e-13
-    # parity over a short horizon: the sheared blob is unstable, so rounding-level
-    # differences grow exponentially over hundreds of steps
+    # parity on a linear-amplitude blob at rest (acoustic waves only): the sheared
+    # flow above drives shocks into the walls, where limiter branches amplify
+    # rounding-level differences
+    st = {"r": 1.0 + 1e-3 * (r - 1.0) / 0.3, "u": 0 * r, "v": 0 * r}
+    st["p"] = 0.09 * st["r"]
     d = Disk(p)
     d.set_state(0.0, st)
     d.run(20)
