@@ -112,6 +112,20 @@ pg_status pg_grid_solve(pg_grid* dev, double time, double dt);
 /* Releases the private tables cached for the caller's grids. */
 pg_status pg_grid_release(void);
 
+/*
+ * No counterpart in the reference.  The CFL step size of global_dt for callers
+ * that cannot allocate device memory (their own pool or fixed budget owns the
+ * GPU): it reads the caller's state C (xarr*yarr cells), faces xa/ya and
+ * orb_rot (NULL = no orbital advection) and keeps its scratch in a fixed
+ * 64 KiB file-scope device array instead of cudaMalloc'd memory.  Grids above
+ * 8192*4096 interior cells are rejected (PG_ERR_CONFIG).  The first call on a
+ * device resolves the array's device address once, with that device current.
+ * Calls that overlap on the GPU share the array and race.
+ * Blocking; dt = min(CFL dt, 1.1*dt_prev) like pg_grid_global_dt.
+ */
+pg_status pg_global_dt_noalloc(const pg_params* P, const pg_cell* C, const double* xa, const double* ya,
+                               const double* orb_rot, double dt_prev, double* dt_out, void* stream);
+
 /* ------------------------------------------------------- handle API */
 typedef struct pg_disk pg_disk;
 

@@ -20,6 +20,7 @@ STATUS_NAMES = {0: "PG_OK", 1: "PG_ERR_CONFIG", 2: "PG_ERR_CUDA", 3: "PG_ERR_NAN
 EXPORTS = [
     "pg_version", "pg_last_error", "pg_check_params", "pg_make_grid",
     "pg_configure", "pg_grid_init_orbadv", "pg_grid_global_dt", "pg_grid_solve", "pg_grid_release",
+    "pg_global_dt_noalloc",
     "pg_disk_create", "pg_disk_destroy", "pg_disk_dims", "pg_disk_set_state", "pg_disk_get_state",
     "pg_disk_state_ptr", "pg_disk_global_dt", "pg_disk_solve", "pg_disk_run", "pg_disk_sync", "pg_disk_clock",
     "pg_disk_planet", "pg_disk_check", "pg_kernels_per_step", "pg_disk_profile",
@@ -59,6 +60,7 @@ def lib() -> ctypes.CDLL:
         "pg_grid_global_dt": (i, [vp, vp, d, dp]),
         "pg_grid_solve": (i, [vp, d, d]),
         "pg_grid_release": (i, []),
+        "pg_global_dt_noalloc": (i, [PP, vp, vp, vp, vp, d, dp, vp]),
         "pg_disk_create": (i, [PP, i, vp, ctypes.POINTER(vp)]),
         "pg_disk_destroy": (i, [vp]),
         "pg_disk_dims": (i, [vp, ip, ip, ip]),

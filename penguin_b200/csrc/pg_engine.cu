@@ -26,6 +26,8 @@ static pg_status fail(pg_status s, const char* fmt, ...) {
     return s;
 }
 
+void set_last_error(const char* msg) { g_err = msg; }
+
 #define PG_CUDA(call)                                                                          \
     do {                                                                                       \
         cudaError_t e_ = (call);                                                               \

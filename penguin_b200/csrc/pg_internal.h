@@ -34,6 +34,7 @@ void launch_advect(const DiskView& d, const CellMaps& in, Cell* out, cudaStream_
 void launch_kick2(const DiskView& d, const CellMaps& in, const VisMaps& vis, Cell* out, cudaStream_t s);
 void launch_init_planet(const DiskView& d, const pg_params& P, double t, cudaStream_t s);
 int kernels_per_step(const DiskView& d);
+void set_last_error(const char* msg);
 cudaError_t set_kernel_attributes();
 
 }  // namespace pg
