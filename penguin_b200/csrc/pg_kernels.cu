@@ -36,7 +36,8 @@ constexpr int SWY_TILE = SW_TL * SWY_COLS * 5;
 constexpr int SW_TILE_MAX = (SWY_TILE + 15) / 16 * 16;
 constexpr int SW_NST = SW_P1 * SW_W;        // 272 reconstructed cells
 constexpr int SW_NFX = SW_P2 * SW_W;        // 264 faces
-constexpr size_t SW_SMEM = (size_t)(SW_TILE_MAX + 10 * SW_NST + 7 * SW_NFX) * 8 + 16 + 128;
+constexpr size_t SW_SMEM = (size_t)(2 * SW_TILE_MAX + 10 * SW_NST + 7 * SW_NFX) * 8 + 16 + 128;
+constexpr size_t AD_SMEM = (size_t)(2 * SW_TILE_MAX + 5 * SW_TL * SW_W) * 8 + 16 + 128;
 
 constexpr int ST_TX = 32, ST_TY = 8;        // stencil kernels: 32 x 8 outputs
 constexpr int ST_HX = ST_TX + 2, ST_HY = ST_TY + 2;
@@ -45,8 +46,8 @@ constexpr int ST_TILE_N = ST_HX * ST_HY * 5;          // doubles in one cell til
 constexpr int ST_TILE = (ST_TILE_N + 15) / 16 * 16;     // rounded so every TMA target is 128-B aligned
 constexpr int ST_VIS_N = ST_HX * ST_HY * 2;
 constexpr int ST_VIS = (ST_VIS_N + 15) / 16 * 16;
-constexpr size_t K1_SMEM = (size_t)ST_TILE * 8 + 16 + 128;
-constexpr size_t K5_SMEM = (size_t)(2 * ST_TILE + ST_VIS) * 8 + 16 + 128;
+constexpr size_t K1_SMEM = (size_t)2 * ST_TILE * 8 + 16 + 128;
+constexpr size_t K5_SMEM = (size_t)(3 * ST_TILE + 2 * ST_VIS) * 8 + 16 + 128;
 
 // ------------------------------------------------------------- planet
 __host__ __device__ inline double ramp_function(double t, double tau, double val) {  // planet.cu:7-17
@@ -236,41 +237,78 @@ __device__ __forceinline__ void block_max_to(unsigned long long* dst, double v) 
     }
 }
 
-// Loads one TMA box into shared memory; every thread returns whether it landed.
-__device__ __forceinline__ bool tile_load(double* dst, const CUtensorMap* map, int x, int y, uint32_t bytes,
-                                          uint64_t* bar, Scalars* sc) {
+// Two-stage TMA pipeline of a persistent CTA: tile k computes from stage k&1
+// while tile k+1 streams into the other stage.  Barrier k&1 completes phase
+// (k>>1)&1 when tile k has landed.
+__device__ __forceinline__ void pipe_init(uint64_t* bar) {
     if (threadIdx.x == 0) {
-        mbar_init(bar, 1);
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
         fence_barrier_init();
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
-        mbar_arrive_expect_tx(bar, bytes);
-        tma_load_2d(dst, map, x, y, bar);
-    }
-    return mbar_wait(bar, 0, sc);
+}
+// thread 0: one box into a stage (the stage's previous generic reads are ordered
+// before the async-proxy write by the fence)
+__device__ __forceinline__ void issue_box(double* dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
+    tma_load_2d(dst, map, x, y, bar);
+}
+__device__ __forceinline__ void issue_begin(uint64_t* bar, uint32_t bytes) {
+    fence_proxy_async();
+    mbar_arrive_expect_tx(bar, bytes);
+}
+// every thread of the CTA gets the same answer, so a timed-out wait makes the
+// whole CTA leave together
+__device__ __forceinline__ bool pipe_wait(uint64_t* bar, int k, Scalars* sc) {
+    const bool ok = mbar_wait(&bar[k & 1], (uint32_t)((k >> 1) & 1), sc);
+    return __syncthreads_and(ok ? 1 : 0) != 0;
+}
+// after a timed-out wait: before the CTA leaves, wait (again bounded) for the
+// copy of tile k+1 if one was issued, so no copy lands in released shared memory
+__device__ __forceinline__ void pipe_drain(uint64_t* bar, int k, bool issued_next, Scalars* sc) {
+    if (threadIdx.x == 0 && issued_next) mbar_wait(&bar[(k + 1) & 1], (uint32_t)(((k + 1) >> 1) & 1), sc);
 }
 
 // ================================================================ sweeps
 // DIR 0: radial pencils (rows of the array), DIR 1: azimuthal pencils (columns).
 template <int DIR>
 __global__ void __launch_bounds__(SW_THREADS, 2)
-    k_sweep(const __grid_constant__ CUtensorMap tm, const DiskView d, Cell* __restrict__ out) {
+    k_sweep(const __grid_constant__ CUtensorMap tm, const DiskView d, Cell* __restrict__ out, int ntx, int ntiles) {
     extern __shared__ __align__(128) double smem_raw[];
     double* smem = smem_base128(smem_raw);
-    double* tile = smem;
-    double* st = smem + SW_TILE_MAX;  // [10][SW_NST] interface states
-    double* fl = st + 10 * SW_NST;    // [7][SW_NFX] fluxes
+    auto stage = [&](int n) { return smem + (n & 1) * SW_TILE_MAX; };
+    double* st = smem + 2 * SW_TILE_MAX;  // [10][SW_NST] interface states
+    double* fl = st + 10 * SW_NST;        // [7][SW_NFX] fluxes
     uint64_t* bar = reinterpret_cast<uint64_t*>(fl + 7 * SW_NFX);
     __shared__ int s_inc[SW_W];
     Scalars* sc = d.sc;
     if (sc->done) return;
 
     const int tid = threadIdx.x;
-    const int s0 = NPAD + SW_LEN * blockIdx.x;                     // first output along the sweep
-    const int q0 = (DIR == 0 ? d.ypad : NPAD) + SW_W * blockIdx.y;  // first pencil
     const double dt = sc->dt;
     const double gam = d.gam;
+    const uint32_t bytes = (DIR == 0 ? SWX_TILE : SWY_TILE) * 8;
+    auto origin = [&](int tile, int& s0, int& q0) {
+        const int bx = tile % ntx, by = tile / ntx;
+        s0 = NPAD + SW_LEN * bx;                     // first output along the sweep
+        q0 = (DIR == 0 ? d.ypad : NPAD) + SW_W * by;  // first pencil
+    };
+    auto issue = [&](int tile, int k) {
+        int s0, q0;
+        origin(tile, s0, q0);
+        issue_begin(&bar[k & 1], bytes);
+        if (DIR == 0) issue_box(stage(k), &tm, 5 * (s0 - NPAD), q0, &bar[k & 1]);
+        else issue_box(stage(k), &tm, 5 * (q0 - 1), s0 - NPAD, &bar[k & 1]);
+    };
+    pipe_init(bar);
+    if ((int)blockIdx.x >= ntiles) return;
+    if (tid == 0) issue(blockIdx.x, 0);
+    int kt = 0;
+    for (int tile_id = blockIdx.x; tile_id < ntiles; tile_id += gridDim.x, ++kt) {
+    if (tid == 0 && tile_id + (int)gridDim.x < ntiles) issue(tile_id + gridDim.x, kt + 1);
+    int s0, q0;
+    origin(tile_id, s0, q0);
+    double* tile = stage(kt);
 
     if (DIR == 1 && tid < SW_W) {
         // set_orbital_advection (src/orbit/orbit.cu:74-99) for this column
@@ -283,16 +321,17 @@ __global__ void __launch_bounds__(SW_THREADS, 2)
             shift = __double2int_rd(rot * dt / dy + 0.5);
             double speed = shift * dy / dt;
             speed = rot - speed;
-            if (blockIdx.x == 0) {
+            if (s0 == NPAD) {
                 d.res[i] = speed;
                 d.inc[i] = shift;
             }
         }
         s_inc[tid] = shift;
     }
-    const bool ok = (DIR == 0) ? tile_load(tile, &tm, 5 * (s0 - NPAD), q0, SWX_TILE * 8, bar, sc)
-                               : tile_load(tile, &tm, 5 * (q0 - 1), s0 - NPAD, SWY_TILE * 8, bar, sc);
-    if (!ok) return;
+    if (!pipe_wait(bar, kt, sc)) {
+        pipe_drain(bar, kt, tile_id + (int)gridDim.x < ntiles, sc);
+        return;
+    }
 
     // ---- P1: reconstruction + both edge states of every cell
     if (tid < SW_NST) {
@@ -441,24 +480,46 @@ __global__ void __launch_bounds__(SW_THREADS, 2)
             }
         }
     }
+    __syncthreads();  // stage k&1, the state / flux arrays and s_inc are free again
+    }
 }
 
 // ===================================================== residual advection
 __global__ void __launch_bounds__(SW_THREADS, 2)
-    k_advect(const __grid_constant__ CUtensorMap tm, const DiskView d, Cell* __restrict__ out) {
+    k_advect(const __grid_constant__ CUtensorMap tm, const DiskView d, Cell* __restrict__ out, int ntx, int ntiles) {
     extern __shared__ __align__(128) double smem_raw[];
     double* smem = smem_base128(smem_raw);
-    double* tile = smem;
-    double* fl = smem + SW_TILE_MAX;  // [5][SW_TL * SW_W] face fluxes, indexed by face t
+    auto stage = [&](int n) { return smem + (n & 1) * SW_TILE_MAX; };
+    double* fl = smem + 2 * SW_TILE_MAX;  // [5][SW_TL * SW_W] face fluxes, indexed by face t
     uint64_t* bar = reinterpret_cast<uint64_t*>(fl + 5 * SW_TL * SW_W);
     Scalars* sc = d.sc;
     if (sc->done) return;
     const int tid = threadIdx.x;
-    const int s0 = NPAD + SW_LEN * blockIdx.x;
-    const int q0 = NPAD + SW_W * blockIdx.y;
     const double dt = sc->dt;
-    if (!tile_load(tile, &tm, 5 * (q0 - 1), s0 - NPAD, SWY_TILE * 8, bar, sc)) return;
     constexpr int NFL = SW_TL * SW_W;
+    auto origin = [&](int tile, int& s0, int& q0) {
+        s0 = NPAD + SW_LEN * (tile % ntx);
+        q0 = NPAD + SW_W * (tile / ntx);
+    };
+    auto issue = [&](int tile, int k) {
+        int s0, q0;
+        origin(tile, s0, q0);
+        issue_begin(&bar[k & 1], SWY_TILE * 8);
+        issue_box(stage(k), &tm, 5 * (q0 - 1), s0 - NPAD, &bar[k & 1]);
+    };
+    pipe_init(bar);
+    if ((int)blockIdx.x >= ntiles) return;
+    if (tid == 0) issue(blockIdx.x, 0);
+    int kt = 0;
+    for (int tile_id = blockIdx.x; tile_id < ntiles; tile_id += gridDim.x, ++kt) {
+    if (tid == 0 && tile_id + (int)gridDim.x < ntiles) issue(tile_id + gridDim.x, kt + 1);
+    int s0, q0;
+    origin(tile_id, s0, q0);
+    double* tile = stage(kt);
+    if (!pipe_wait(bar, kt, sc)) {
+        pipe_drain(bar, kt, tile_id + (int)gridDim.x < ntiles, sc);
+        return;
+    }
 
     // ---- P1: upwind PPM average over the swept fraction (advection.cu:20-67)
     if (tid < SW_NST) {
@@ -551,161 +612,201 @@ __global__ void __launch_bounds__(SW_THREADS, 2)
             emit(d, out, i, s, Q);
         }
     }
+    __syncthreads();
+    }
 }
 
 // ====================================================== kick 1 (+ stress)
 template <bool VISC>
 __global__ void __launch_bounds__(ST_THREADS)
     k_kick1(const __grid_constant__ CUtensorMap tm, const DiskView d, Cell* __restrict__ out,
-            double* __restrict__ vis) {
+            double* __restrict__ vis, int ntx, int ntiles) {
     extern __shared__ __align__(128) double smem_raw[];
     double* smem = smem_base128(smem_raw);
-    double* tile = smem;
-    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + ST_TILE);
+    auto stage = [&](int n) { return smem + (n & 1) * ST_TILE; };
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + 2 * ST_TILE);
     Scalars* sc = d.sc;
     if (sc->done) return;
-    const int i0 = NPAD + ST_TX * blockIdx.x;
-    const int j0 = d.ypad + ST_TY * blockIdx.y;
-    if (!tile_load(tile, &tm, 5 * (i0 - 1), j0 - 1, ST_TILE_N * 8, bar, sc)) return;
-    const int hx = 1 + threadIdx.x % ST_TX, hy = 1 + threadIdx.x / ST_TX;
-    const int i = i0 + hx - 1, j = j0 + hy - 1;
-    if (i >= NPAD + d.xres || j >= d.ypad + d.yres) return;
+    const int tid = threadIdx.x;
     const double hdt = 0.5 * sc->dt;
-    const double* c = tile + (hy * ST_HX + hx) * 5;
-    const Cell C{c[0], c[1], c[2], c[3], c[4]};
-    double vx = 0.0, vy = 0.0;
-    if (VISC) {
-        double nu[3], u[9], v[9], nr[9];
-#pragma unroll
-        for (int n = 0; n < 3; ++n) nu[n] = d.nux[i + n - 1];
-        gather9(tile, hx, hy, nu, u, v, nr);
-        viscous(d.visx + 5 * i, d.visy + 4 * j, u, v, nr, vx, vy);
-        // the stress is kept for the predictor of kick2, with its periodic images
-        const size_t k = (size_t)i + (size_t)d.xarr * j;
-        vis[2 * k] = vx;
-        vis[2 * k + 1] = vy;
-        int jimg = -1;
-        if (j < 2 * NPAD) jimg = j + d.yres;
-        else if (j >= d.yres) jimg = j - d.yres;
-        if (jimg >= 0) {
-            const size_t m = (size_t)i + (size_t)d.xarr * jimg;
-            vis[2 * m] = vx;
-            vis[2 * m + 1] = vy;
-        }
+    auto origin = [&](int tile, int& i0, int& j0) {
+        i0 = NPAD + ST_TX * (tile % ntx);
+        j0 = d.ypad + ST_TY * (tile / ntx);
+    };
+    auto issue = [&](int tile, int k) {
+        int i0, j0;
+        origin(tile, i0, j0);
+        issue_begin(&bar[k & 1], ST_TILE_N * 8);
+        issue_box(stage(k), &tm, 5 * (i0 - 1), j0 - 1, &bar[k & 1]);
+    };
+    pipe_init(bar);
+    if ((int)blockIdx.x >= ntiles) return;
+    if (tid == 0) issue(blockIdx.x, 0);
+    int kt = 0;
+    for (int tile_id = blockIdx.x; tile_id < ntiles; tile_id += gridDim.x, ++kt) {
+        if (tid == 0 && tile_id + (int)gridDim.x < ntiles) issue(tile_id + gridDim.x, kt + 1);
+        int i0, j0;
+        origin(tile_id, i0, j0);
+        const double* tile = stage(kt);
+        if (!pipe_wait(bar, kt, sc)) {
+        pipe_drain(bar, kt, tile_id + (int)gridDim.x < ntiles, sc);
+        return;
     }
-    const double* tr = d.trig + 4 * j;
-    const Grav g = gravity(d, i, d.radx[i], tr[0], tr[1], d.trig[4 * d.yarr], sc->planet_cur);
-    const Cell Q = kick<VISC>(d, C, d.irad[i], g, vx, vy, 0.0, hdt);
-    emit(d, out, i, j, Q);
+        const int hx = 1 + tid % ST_TX, hy = 1 + tid / ST_TX;
+        const int i = i0 + hx - 1, j = j0 + hy - 1;
+        if (i < NPAD + d.xres && j < d.ypad + d.yres) {
+            const double* c = tile + (hy * ST_HX + hx) * 5;
+            const Cell C{c[0], c[1], c[2], c[3], c[4]};
+            double vx = 0.0, vy = 0.0;
+            if (VISC) {
+                double nu[3], u[9], v[9], nr[9];
+#pragma unroll
+                for (int n = 0; n < 3; ++n) nu[n] = d.nux[i + n - 1];
+                gather9(tile, hx, hy, nu, u, v, nr);
+                viscous(d.visx + 5 * i, d.visy + 4 * j, u, v, nr, vx, vy);
+                // the stress is kept for the predictor of kick2, with its periodic images
+                const size_t m0 = (size_t)i + (size_t)d.xarr * j;
+                vis[2 * m0] = vx;
+                vis[2 * m0 + 1] = vy;
+                int jimg = -1;
+                if (j < 2 * NPAD) jimg = j + d.yres;
+                else if (j >= d.yres) jimg = j - d.yres;
+                if (jimg >= 0) {
+                    const size_t m = (size_t)i + (size_t)d.xarr * jimg;
+                    vis[2 * m] = vx;
+                    vis[2 * m + 1] = vy;
+                }
+            }
+            const double* tr = d.trig + 4 * j;
+            const Grav g = gravity(d, i, d.radx[i], tr[0], tr[1], d.trig[4 * d.yarr], sc->planet_cur);
+            const Cell Q = kick<VISC>(d, C, d.irad[i], g, vx, vy, 0.0, hdt);
+            emit(d, out, i, j, Q);
+        }
+        __syncthreads();
+    }
 }
 
 // ============================================ kick 2 + damping + CFL speed
 template <bool VISC>
 __global__ void __launch_bounds__(ST_THREADS)
     k_kick2(const __grid_constant__ CUtensorMap tm, const __grid_constant__ CUtensorMap tv, const DiskView d,
-            Cell* __restrict__ out) {
+            Cell* __restrict__ out, int ntx, int ntiles) {
     extern __shared__ __align__(128) double smem_raw[];
     double* smem = smem_base128(smem_raw);
-    double* tile = smem;              // C with 1 halo
-    double* tp = smem + ST_TILE;      // predicted state with 1 halo
-    double* tvis = tp + ST_TILE;      // stress of the step's first evaluation
-    uint64_t* bar = reinterpret_cast<uint64_t*>(tvis + ST_VIS);
+    auto stage = [&](int n) { return smem + (n & 1) * ST_TILE; };                   // C with 1 halo
+    auto vstage = [&](int n) { return smem + 2 * ST_TILE + (n & 1) * ST_VIS; };  // stress of the first evaluation
+    double* tp = smem + 2 * ST_TILE + 2 * ST_VIS;                      // predicted state with 1 halo
+    uint64_t* bar = reinterpret_cast<uint64_t*>(tp + ST_TILE);
     Scalars* sc = d.sc;
     if (sc->done) return;
-    const int i0 = NPAD + ST_TX * blockIdx.x;
-    const int j0 = d.ypad + ST_TY * blockIdx.y;
     const int tid = threadIdx.x;
-    if (tid == 0) {
-        mbar_init(bar, 1);
-        fence_barrier_init();
-    }
-    __syncthreads();
-    if (tid == 0) {
-        mbar_arrive_expect_tx(bar, (ST_TILE_N + (VISC ? ST_VIS_N : 0)) * 8);
-        tma_load_2d(tile, &tm, 5 * (i0 - 1), j0 - 1, bar);
-        if (VISC) tma_load_2d(tvis, &tv, 2 * (i0 - 1), j0 - 1, bar);
-    }
-    if (!mbar_wait(bar, 0, sc)) return;
     const double dt = sc->dt, hdt = 0.5 * dt;
     const pg_body pl = sc->planet_next;
     const double iplx2 = d.trig[4 * d.yarr + 1];
-
-    if (VISC) {
-        // predictor (sweeps.cu:713-729 with mdt = dt = dt/2) on the tile and its halo
-        for (int it = tid; it < ST_HX * ST_HY; it += ST_THREADS) {
-            const int hx = it % ST_HX, hy = it / ST_HX;
-            const int i = i0 - 1 + hx, j = j0 - 1 + hy;
-            if (i < NPAD || i >= NPAD + d.xres || j < 0 || j >= d.yarr) continue;
-            const double* c = tile + it * 5;
-            const Cell C{c[0], c[1], c[2], c[3], c[4]};
-            const double* tr = d.trig + 4 * j + 2;
-            const Grav g = gravity(d, i, d.radx[i], tr[0], tr[1], iplx2, pl);
-            const Cell Q = kick<true>(d, C, d.irad[i], g, tvis[2 * it], tvis[2 * it + 1], hdt, hdt);
-            double* o = tp + it * 5;
-            o[0] = Q.r; o[1] = Q.p; o[2] = Q.u; o[3] = Q.v; o[4] = Q.w;
-        }
-        __syncthreads();
-        // radial ghosts of the predicted state (boundx2, src/boundary/boundary.cu:722-820):
-        // the stencil only reaches the innermost ghost column on either side
-        for (int it = tid; it < ST_HX * ST_HY; it += ST_THREADS) {
-            const int hx = it % ST_HX, hy = it / ST_HX;
-            const int i = i0 - 1 + hx;
-            const int side = (i == NPAD - 1) ? 0 : ((i == NPAD + d.xres) ? 1 : -1);
-            if (side < 0) continue;
-            const int bnd = side == 0 ? d.bound_lft : d.bound_rgh;
-            double* o = tp + (hy * ST_HX + hx) * 5;
-            const double* src;
-            if (bnd == 0) src = tile + (hy * ST_HX + hx) * 5;  // constant analytic state
-            else {
-                // the adjacent interior cell is both the copy and the reflection source
-                const int hs = side == 0 ? hx + 1 : hx - 1;
-                src = tp + (hy * ST_HX + hs) * 5;
-            }
-            o[0] = src[0]; o[1] = src[1]; o[2] = src[2]; o[3] = src[3]; o[4] = src[4];
-            if (bnd == 2) o[2] = -o[2];
-        }
-        __syncthreads();
+    auto origin = [&](int tile, int& i0, int& j0) {
+        i0 = NPAD + ST_TX * (tile % ntx);
+        j0 = d.ypad + ST_TY * (tile / ntx);
+    };
+    auto issue = [&](int tile, int k) {
+        int i0, j0;
+        origin(tile, i0, j0);
+        issue_begin(&bar[k & 1], (ST_TILE_N + (VISC ? ST_VIS_N : 0)) * 8);
+        issue_box(stage(k), &tm, 5 * (i0 - 1), j0 - 1, &bar[k & 1]);
+        if (VISC) issue_box(vstage(k), &tv, 2 * (i0 - 1), j0 - 1, &bar[k & 1]);
+    };
+    pipe_init(bar);
+    double vmax = 0.0;
+    if ((int)blockIdx.x < ntiles) {
+        if (tid == 0) issue(blockIdx.x, 0);
+        int kt = 0;
+        for (int tile_id = blockIdx.x; tile_id < ntiles; tile_id += gridDim.x, ++kt) {
+            if (tid == 0 && tile_id + (int)gridDim.x < ntiles) issue(tile_id + gridDim.x, kt + 1);
+            int i0, j0;
+            origin(tile_id, i0, j0);
+            const double* tile = stage(kt);
+            const double* tvis = vstage(kt);
+            if (!pipe_wait(bar, kt, sc)) {
+        pipe_drain(bar, kt, tile_id + (int)gridDim.x < ntiles, sc);
+        return;
     }
 
-    const int hx = 1 + tid % ST_TX, hy = 1 + tid / ST_TX;
-    const int i = i0 + hx - 1, j = j0 + hy - 1;
-    const bool valid = (i < NPAD + d.xres && j < d.ypad + d.yres);
-    double vmax = 0.0;
-    if (valid) {
-        const double* c = tile + (hy * ST_HX + hx) * 5;
-        const Cell C{c[0], c[1], c[2], c[3], c[4]};
-        double vx = 0.0, vy = 0.0;
-        if (VISC) {
-            double nu[3], u[9], v[9], nr[9];
-#pragma unroll
-            for (int n = 0; n < 3; ++n) nu[n] = d.nux[i + n - 1];
-            gather9(tp, hx, hy, nu, u, v, nr);
-            viscous(d.visx + 5 * i, d.visy + 4 * j, u, v, nr, vx, vy);
-        }
-        const double* tr = d.trig + 4 * j + 2;
-        const Grav g = gravity(d, i, d.radx[i], tr[0], tr[1], iplx2, pl);
-        Cell Q = kick<VISC>(d, C, d.irad[i], g, vx, vy, hdt, hdt);
-        if (d.kill) {
-            // killwave (src/killwave/killwave.cu:48-100): relax towards init_C
-            const double* kt = d.killx + 4 * i;
-            const double* I = d.initx + 5 * i;
-#pragma unroll
-            for (int side = 0; side < 2; ++side) {
-                const double tau = kt[2 * side + 1];
-                if (tau > 0.0) {
-                    double f = kt[2 * side];
-                    f *= dt / tau;
-                    Q.r += f * (I[0] - Q.r);
-                    Q.p += f * (I[1] - Q.p);
-                    Q.u += f * (I[2] - Q.u);
-                    Q.v += f * (I[3] - Q.v);
-                    Q.w += f * (I[4] - Q.w);
+            if (VISC) {
+                // predictor (sweeps.cu:713-729 with mdt = dt = dt/2) on the tile and its halo
+                for (int it = tid; it < ST_HX * ST_HY; it += ST_THREADS) {
+                    const int hx = it % ST_HX, hy = it / ST_HX;
+                    const int i = i0 - 1 + hx, j = j0 - 1 + hy;
+                    if (i < NPAD || i >= NPAD + d.xres || j < 0 || j >= d.yarr) continue;
+                    const double* c = tile + it * 5;
+                    const Cell C{c[0], c[1], c[2], c[3], c[4]};
+                    const double* tr = d.trig + 4 * j + 2;
+                    const Grav g = gravity(d, i, d.radx[i], tr[0], tr[1], iplx2, pl);
+                    const Cell Q = kick<true>(d, C, d.irad[i], g, tvis[2 * it], tvis[2 * it + 1], hdt, hdt);
+                    double* o = tp + it * 5;
+                    o[0] = Q.r; o[1] = Q.p; o[2] = Q.u; o[3] = Q.v; o[4] = Q.w;
                 }
+                __syncthreads();
+                // radial ghosts of the predicted state (boundx2, src/boundary/boundary.cu:722-820):
+                // the stencil only reaches the innermost ghost column on either side
+                for (int it = tid; it < ST_HX * ST_HY; it += ST_THREADS) {
+                    const int hx = it % ST_HX, hy = it / ST_HX;
+                    const int i = i0 - 1 + hx;
+                    const int side = (i == NPAD - 1) ? 0 : ((i == NPAD + d.xres) ? 1 : -1);
+                    if (side < 0) continue;
+                    const int bnd = side == 0 ? d.bound_lft : d.bound_rgh;
+                    double* o = tp + (hy * ST_HX + hx) * 5;
+                    const double* src;
+                    if (bnd == 0) src = tile + (hy * ST_HX + hx) * 5;  // constant analytic state
+                    else {
+                        // the adjacent interior cell is both the copy and the reflection source
+                        const int hs = side == 0 ? hx + 1 : hx - 1;
+                        src = tp + (hy * ST_HX + hs) * 5;
+                    }
+                    o[0] = src[0]; o[1] = src[1]; o[2] = src[2]; o[3] = src[3]; o[4] = src[4];
+                    if (bnd == 2) o[2] = -o[2];
+                }
+                __syncthreads();
             }
+
+            const int hx = 1 + tid % ST_TX, hy = 1 + tid / ST_TX;
+            const int i = i0 + hx - 1, j = j0 + hy - 1;
+            if (i < NPAD + d.xres && j < d.ypad + d.yres) {
+                const double* c = tile + (hy * ST_HX + hx) * 5;
+                const Cell C{c[0], c[1], c[2], c[3], c[4]};
+                double vx = 0.0, vy = 0.0;
+                if (VISC) {
+                    double nu[3], u[9], v[9], nr[9];
+#pragma unroll
+                    for (int n = 0; n < 3; ++n) nu[n] = d.nux[i + n - 1];
+                    gather9(tp, hx, hy, nu, u, v, nr);
+                    viscous(d.visx + 5 * i, d.visy + 4 * j, u, v, nr, vx, vy);
+                }
+                const double* tr = d.trig + 4 * j + 2;
+                const Grav g = gravity(d, i, d.radx[i], tr[0], tr[1], iplx2, pl);
+                Cell Q = kick<VISC>(d, C, d.irad[i], g, vx, vy, hdt, hdt);
+                if (d.kill) {
+                    // killwave (src/killwave/killwave.cu:48-100): relax towards init_C
+                    const double* kt = d.killx + 4 * i;
+                    const double* I = d.initx + 5 * i;
+#pragma unroll
+                    for (int side = 0; side < 2; ++side) {
+                        const double tau = kt[2 * side + 1];
+                        if (tau > 0.0) {
+                            double f = kt[2 * side];
+                            f *= dt / tau;
+                            Q.r += f * (I[0] - Q.r);
+                            Q.p += f * (I[1] - Q.p);
+                            Q.u += f * (I[2] - Q.u);
+                            Q.v += f * (I[3] - Q.v);
+                            Q.w += f * (I[4] - Q.w);
+                        }
+                    }
+                }
+                if (!(Q.r > 0.0)) atomicOr(&sc->err, 1 << PG_ERR_NAN);
+                vmax = fmax(vmax, signal_rate(d, Q, i, j));
+                emit(d, out, i, j, Q);
+            }
+            __syncthreads();
         }
-        if (!(Q.r > 0.0)) atomicOr(&sc->err, 1 << PG_ERR_NAN);
-        vmax = signal_rate(d, Q, i, j);
-        emit(d, out, i, j, Q);
     }
     block_max_to<ST_THREADS>(&sc->vmax_bits, vmax);
 }
@@ -963,10 +1064,12 @@ cudaError_t set_kernel_attributes() {
     auto set = [&](const void* f, size_t bytes) {
         cudaError_t r = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
         if (r != cudaSuccess) e = r;
+        r = cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+        if (r != cudaSuccess) e = r;
     };
     set((const void*)k_sweep<0>, SW_SMEM);
     set((const void*)k_sweep<1>, SW_SMEM);
-    set((const void*)k_advect, SW_SMEM);
+    set((const void*)k_advect, AD_SMEM);
     set((const void*)k_kick1<true>, K1_SMEM);
     set((const void*)k_kick1<false>, K1_SMEM);
     set((const void*)k_kick2<true>, K5_SMEM);
@@ -1025,31 +1128,75 @@ void launch_init_planet(const DiskView& d, const pg_params& P, double t, cudaStr
     k_init_planet<<<1, 1, 0, s>>>(d, a, P.planet_ecc, rs, t);
 }
 
+// Persistent grid: as many CTAs as fit on the GPU at once, each looping over tiles.
+static unsigned persistent_grid(const void* kernel, int threads, size_t smem, long long ntiles) {
+    static int nsm = 0;
+    if (nsm == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+        if (nsm <= 0) nsm = 148;
+    }
+    // occupancy of each kernel, queried once (launches repeat every step)
+    static const void* keys[16] = {nullptr};
+    static int vals[16] = {0};
+    int per_sm = 0;
+    for (int n = 0; n < 16 && keys[n]; ++n)
+        if (keys[n] == kernel) per_sm = vals[n];
+    if (per_sm == 0) {
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem) != cudaSuccess ||
+            per_sm < 1)
+            per_sm = 1;
+        for (int n = 0; n < 16; ++n)
+            if (!keys[n]) {
+                keys[n] = kernel;
+                vals[n] = per_sm;
+                break;
+            }
+    }
+    long long g = (long long)per_sm * nsm;
+    if (g > ntiles) g = ntiles;
+    return (unsigned)(g < 1 ? 1 : g);
+}
+
 void launch_kick1(const DiskView& d, const CellMaps& in, Cell* out, double* vis, cudaStream_t s) {
-    dim3 grid(cdiv(d.xres, ST_TX), cdiv(d.yres, ST_TY));
-    if (d.visc && d.ndim == 2) k_kick1<true><<<grid, ST_THREADS, K1_SMEM, s>>>(in.stencil, d, out, vis);
-    else k_kick1<false><<<grid, ST_THREADS, K1_SMEM, s>>>(in.stencil, d, out, vis);
+    const int ntx = (int)cdiv(d.xres, ST_TX), nt = ntx * (int)cdiv(d.yres, ST_TY);
+    if (d.visc && d.ndim == 2) {
+        const unsigned g = persistent_grid((const void*)k_kick1<true>, ST_THREADS, K1_SMEM, nt);
+        k_kick1<true><<<g, ST_THREADS, K1_SMEM, s>>>(in.stencil, d, out, vis, ntx, nt);
+    } else {
+        const unsigned g = persistent_grid((const void*)k_kick1<false>, ST_THREADS, K1_SMEM, nt);
+        k_kick1<false><<<g, ST_THREADS, K1_SMEM, s>>>(in.stencil, d, out, vis, ntx, nt);
+    }
 }
 
 void launch_sweep_x(const DiskView& d, const CellMaps& in, Cell* out, cudaStream_t s) {
-    dim3 grid(cdiv(d.xres, SW_LEN), cdiv(d.yres, SW_W));
-    k_sweep<0><<<grid, SW_THREADS, SW_SMEM, s>>>(in.sweep_x, d, out);
+    const int ntx = (int)cdiv(d.xres, SW_LEN), nt = ntx * (int)cdiv(d.yres, SW_W);
+    const unsigned g = persistent_grid((const void*)k_sweep<0>, SW_THREADS, SW_SMEM, nt);
+    k_sweep<0><<<g, SW_THREADS, SW_SMEM, s>>>(in.sweep_x, d, out, ntx, nt);
 }
 
 void launch_sweep_y(const DiskView& d, const CellMaps& in, Cell* out, cudaStream_t s) {
-    dim3 grid(cdiv(d.yres, SW_LEN), cdiv(d.xres, SW_W));
-    k_sweep<1><<<grid, SW_THREADS, SW_SMEM, s>>>(in.sweep_y, d, out);
+    const int ntx = (int)cdiv(d.yres, SW_LEN), nt = ntx * (int)cdiv(d.xres, SW_W);
+    const unsigned g = persistent_grid((const void*)k_sweep<1>, SW_THREADS, SW_SMEM, nt);
+    k_sweep<1><<<g, SW_THREADS, SW_SMEM, s>>>(in.sweep_y, d, out, ntx, nt);
 }
 
 void launch_advect(const DiskView& d, const CellMaps& in, Cell* out, cudaStream_t s) {
-    dim3 grid(cdiv(d.yres, SW_LEN), cdiv(d.xres, SW_W));
-    k_advect<<<grid, SW_THREADS, SW_SMEM, s>>>(in.sweep_y, d, out);
+    const int ntx = (int)cdiv(d.yres, SW_LEN), nt = ntx * (int)cdiv(d.xres, SW_W);
+    const unsigned g = persistent_grid((const void*)k_advect, SW_THREADS, AD_SMEM, nt);
+    k_advect<<<g, SW_THREADS, AD_SMEM, s>>>(in.sweep_y, d, out, ntx, nt);
 }
 
 void launch_kick2(const DiskView& d, const CellMaps& in, const VisMaps& vis, Cell* out, cudaStream_t s) {
-    dim3 grid(cdiv(d.xres, ST_TX), cdiv(d.yres, ST_TY));
-    if (d.visc && d.ndim == 2) k_kick2<true><<<grid, ST_THREADS, K5_SMEM, s>>>(in.stencil, vis.stencil, d, out);
-    else k_kick2<false><<<grid, ST_THREADS, K5_SMEM, s>>>(in.stencil, vis.stencil, d, out);
+    const int ntx = (int)cdiv(d.xres, ST_TX), nt = ntx * (int)cdiv(d.yres, ST_TY);
+    if (d.visc && d.ndim == 2) {
+        const unsigned g = persistent_grid((const void*)k_kick2<true>, ST_THREADS, K5_SMEM, nt);
+        k_kick2<true><<<g, ST_THREADS, K5_SMEM, s>>>(in.stencil, vis.stencil, d, out, ntx, nt);
+    } else {
+        const unsigned g = persistent_grid((const void*)k_kick2<false>, ST_THREADS, K5_SMEM, nt);
+        k_kick2<false><<<g, ST_THREADS, K5_SMEM, s>>>(in.stencil, vis.stencil, d, out, ntx, nt);
+    }
 }
 
 int kernels_per_step(const DiskView& d) {

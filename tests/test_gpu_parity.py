@@ -144,7 +144,10 @@ def test_mass_conserved_closed_box():
     o = Oracle(p, st, 0.0)
     o.run(20)
     ref = o.interior()
-    _check(g, ref, p, 1e-12)
+    assert rel_l1(g["r"], ref["r"]) < 1e-14 and rel_l1(g["p"], ref["p"]) < 1e-14
+    # the acoustic momentum is ~1e-4 of rho*cs, so an ulp of the pressure
+    # gradient is ~1e-12 of it: the momentum bound is relative to that small signal
+    assert momentum_l1(g, ref) < 5e-11
 
 
 def test_planet_follows_reference_orbit():
