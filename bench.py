@@ -36,6 +36,10 @@ PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
 # AoS Cell (5 x FP64) and reads and writes it once; kick1 also writes the
 # 2-component stress and kick2 reads it back.
 ALGO_BYTES = {"time": 0, "kick1": 96, "sweep_x": 80, "sweep_y": 80, "advect": 80, "kick2": 96}
+# FP32-mixed form: three FP32 residual planes (Sigma, v_r, v_phi) read and written
+# once per pass, plus the 2-component FP32 stress written by kick1 and read by kick2
+ALGO_BYTES_F32 = {"time": 0, "kick1": 32, "sweep_x": 24, "sweep_y": 24, "advect": 24, "kick2": 32}
+ENSEMBLE_STEPS = 500
 
 
 def workload(nr=1024, nphi=3072):
@@ -146,6 +150,84 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def timed(stream, fn):
+    """Device time (ms) of fn() on `stream`, bracketed by synchronisation."""
+    import torch
+
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    fn()
+    e1.record(stream)
+    e1.synchronize()
+    return e0.elapsed_time(e1)
+
+
+def roofline_of(prof, cells, algo, pk):
+    stage = max((k for k in prof if algo.get(k)), key=lambda k: prof[k])
+    achieved = algo[stage] * cells / (prof[stage] / 1000.0) / 1e9
+    return {"bound": "hbm", "kernel": stage, "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
+            "frac": achieved / pk["hbm_gbs"], "peak_source": pk["source"], "algorithmic_bytes_per_cell": algo[stage]}
+
+
+def measure_fp32(p, state, K, W, local, stream, pk):
+    """The FP32-mixed form (an ensemble of one) on the same disk and step count."""
+    from penguin_b200.ensemble import Ensemble
+
+    e = Ensemble([p], device=local, stream=stream.cuda_stream)
+    e.set_state(0, 0.0, state)
+    e.run(W)
+    e.sync()
+    e.check()
+    ms = timed(stream, lambda: e.run(K))
+    e.check()
+    prof = e.profile(max(5, min(50, K // 10)))
+    out = {"value": p.cells * K / (ms / 1000.0), "ms_per_step": ms / K, "steps": K,
+           "dtype": "f32 (FP64 dt, orbital shift, totals)", "stage_ms": prof,
+           "roofline": roofline_of(prof, p.cells, ALGO_BYTES_F32, pk), "gpu_launches": e.kernels_per_step * K}
+    e.close()
+    return out
+
+
+def measure_ensemble(local, stream, steps):
+    """48 seeded disks of uneven size: one FP32-mixed ensemble (one persistent
+    launch per pass, graph-captured step) against the same disks run one after
+    another by the plain FP64 form, `steps` steps each with their own dt."""
+    from penguin_b200 import initial as I
+    from penguin_b200 import params as P
+    from penguin_b200.disk import Disk
+    from penguin_b200.ensemble import Ensemble
+
+    ps = P.disk_ensemble()
+    sts = [I.disk_state(p, seed=100 + k) for k, p in enumerate(ps)]
+    cells = sum(p.cells for p in ps)
+    e = Ensemble(ps, device=local, stream=stream.cuda_stream)
+    for k, st in enumerate(sts):
+        e.set_state(k, 0.0, st)
+    e.run(3)
+    e.sync()
+    ms_e = timed(stream, lambda: e.run(steps))
+    e.check()
+    launches = e.kernels_per_step * steps
+    e.close()
+    # each disk timed on its own (device time of its graph launches), summed
+    ms_s = 0.0
+    for p, st in zip(ps, sts):
+        d = Disk(p, device=local, stream=stream.cuda_stream)
+        d.set_state(0.0, st)
+        d.run(3)
+        d.sync()
+        ms_s += timed(stream, lambda: d.run(steps))
+        d.check()
+        d.close()
+    v_e = cells * steps / (ms_e / 1000.0)
+    v_s = cells * steps / (ms_s / 1000.0)
+    return {"disks": len(ps), "cells": cells, "steps": steps, "value": v_e, "ms_per_step": ms_e / steps,
+            "gpu_launches": launches, "sequential_fp64": {"value": v_s, "ms_per_step": ms_s / steps},
+            "over_sequential_fp64": v_e / v_s,
+            "config": "Nr in 32*[4,16], Nphi=3Nr, q log-U[1e-5,3e-3], alpha log-U[1e-4,1e-2], h/r U[0.03,0.08], seed 2024"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -153,6 +235,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-forms", action="store_true", help="skip the FP32-mixed and ensemble measurements")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -278,6 +361,11 @@ def main():
         "clocks": clocks,
         "e2e": e2e,
     }
+    if not args.no_forms:
+        f32 = measure_fp32(p, state, K, W, local, stream, pk)
+        f32["over_fp64"] = f32["value"] / (value / world)
+        line["fp32_mixed"] = f32
+        line["ensemble"] = measure_ensemble(local, stream, ENSEMBLE_STEPS)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(p, state, 0.0)
     if rank == 0:

@@ -166,6 +166,44 @@ int pg_kernels_per_step(const pg_disk* d);
    4 advect, 5 kick2; absent stages get 0).  nslot >= 6.  Blocking. */
 pg_status pg_disk_profile(pg_disk* d, int nsteps, double end_time, float* ms, int nslot);
 
+/* ------------------------------------------- FP32-mixed ensembles of disks
+ * No counterpart in the reference, which runs one compile-time configured disk
+ * per process.  n planet-disks (each its own pg_params: size, q, alpha, h/r ...)
+ * advanced together by the FP32-mixed step: FP32 residual state against the
+ * FP64 initial disk, FP32 reconstruction and HLLC in deviation form, FP64
+ * orbital shift, dt and totals.  One persistent launch per pass for all disks;
+ * the step is a CUDA graph.  Each disk keeps its own clock and CFL dt.  Only
+ * polar, isothermal disks with analytic radial boundaries and orbital advection
+ * (the planet-disk family) are accepted: PG_ERR_CONFIG otherwise. */
+typedef struct pg_ens pg_ens;
+
+/* Validates n parameter sets for the FP32 form (no GPU needed). */
+pg_status pg_ens_check_params(const pg_params* P, int n);
+pg_status pg_ens_create(const pg_params* P, int n, int device, void* stream, pg_ens** out);
+pg_status pg_ens_destroy(pg_ens* e);
+int pg_ens_size(const pg_ens* e);
+pg_status pg_ens_dims(const pg_ens* e, int k, int* xres, int* yres);
+/* Disk k's state from host arrays of xres*yres interior cells (density,
+   radial and azimuthal velocity; the pressure is cs^2 Sigma); v may be NULL
+   (the initial disk's v).  Blocking. */
+pg_status pg_ens_set_state(pg_ens* e, int k, double t, const double* r, const double* u, const double* v);
+pg_status pg_ens_get_state(pg_ens* e, int k, double* r, double* p, double* u, double* v, double* t_out);
+/* nsteps steps of every disk (each with its own dt, clipped at end_time; a disk
+   that reached end_time stays unchanged).  Stream-ordered; pg_ens_sync waits. */
+pg_status pg_ens_run(pg_ens* e, int nsteps, double end_time);
+pg_status pg_ens_sync(pg_ens* e);
+pg_status pg_ens_clock(pg_ens* e, int k, double* t, double* dt, long long* steps);
+pg_status pg_ens_planet(pg_ens* e, int k, pg_body* out);
+/* Device error words of all disks, cleared by the call (syncs). */
+pg_status pg_ens_check(pg_ens* e);
+/* Disk k's mass sum(Sigma dV) and angular momentum sum(Sigma r v dV), FP64
+   with compensated summation (syncs). */
+pg_status pg_ens_totals(pg_ens* e, int k, double* mass, double* angmom);
+int pg_ens_kernels_per_step(const pg_ens* e);
+/* As pg_disk_profile, for the whole ensemble (slots 0 clocks + planet tables,
+   1 kick1, 2 sweep_x, 3 sweep_y, 4 advect, 5 kick2). */
+pg_status pg_ens_profile(pg_ens* e, int nsteps, double end_time, float* ms, int nslot);
+
 #ifdef __cplusplus
 }
 #endif

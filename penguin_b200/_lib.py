@@ -24,6 +24,9 @@ EXPORTS = [
     "pg_disk_create", "pg_disk_destroy", "pg_disk_dims", "pg_disk_set_state", "pg_disk_get_state",
     "pg_disk_state_ptr", "pg_disk_global_dt", "pg_disk_solve", "pg_disk_run", "pg_disk_sync", "pg_disk_clock",
     "pg_disk_planet", "pg_disk_check", "pg_kernels_per_step", "pg_disk_profile",
+    "pg_ens_check_params", "pg_ens_create", "pg_ens_destroy", "pg_ens_size", "pg_ens_dims", "pg_ens_set_state",
+    "pg_ens_get_state", "pg_ens_run", "pg_ens_sync", "pg_ens_clock", "pg_ens_planet", "pg_ens_check",
+    "pg_ens_totals", "pg_ens_kernels_per_step", "pg_ens_profile",
 ]
 
 
@@ -76,6 +79,21 @@ def lib() -> ctypes.CDLL:
         "pg_disk_check": (i, [vp]),
         "pg_kernels_per_step": (i, [vp]),
         "pg_disk_profile": (i, [vp, i, d, ctypes.POINTER(ctypes.c_float), i]),
+        "pg_ens_check_params": (i, [PP, i]),
+        "pg_ens_create": (i, [PP, i, i, vp, ctypes.POINTER(vp)]),
+        "pg_ens_destroy": (i, [vp]),
+        "pg_ens_size": (i, [vp]),
+        "pg_ens_dims": (i, [vp, i, ip, ip]),
+        "pg_ens_set_state": (i, [vp, i, d, dp, dp, dp]),
+        "pg_ens_get_state": (i, [vp, i, dp, dp, dp, dp, dp]),
+        "pg_ens_run": (i, [vp, i, d]),
+        "pg_ens_sync": (i, [vp]),
+        "pg_ens_clock": (i, [vp, i, dp, dp, ctypes.POINTER(ctypes.c_longlong)]),
+        "pg_ens_planet": (i, [vp, i, ctypes.POINTER(PGBody)]),
+        "pg_ens_check": (i, [vp]),
+        "pg_ens_totals": (i, [vp, i, dp, dp]),
+        "pg_ens_kernels_per_step": (i, [vp]),
+        "pg_ens_profile": (i, [vp, i, d, ctypes.POINTER(ctypes.c_float), i]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

@@ -136,6 +136,15 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, i
         : "memory");
 }
 
+// 3D tiled bulk tensor load global -> shared, completion on an mbarrier.
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int x, int y, int z, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+        "[%5];" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+        : "memory");
+}
+
 // --------------------------------------------------------- state writes
 __device__ __forceinline__ void store_cell(Cell* out, int xarr, int i, int j, const Cell& c) {
     double* q = reinterpret_cast<double*>(out + (size_t)i + (size_t)xarr * j);
@@ -193,6 +202,53 @@ __device__ __forceinline__ Cell load_cell(const Cell* in, int xarr, int i, int j
 __device__ __forceinline__ void atomic_max_pos(unsigned long long* a, double v) {
     if (!(v > 0.0)) return;
     atomicMax(a, (unsigned long long)__double_as_longlong(v));
+}
+
+template <int NT>
+__device__ __forceinline__ void block_max_to(unsigned long long* dst, double v) {
+    __shared__ double red[NT / 32];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        v = (threadIdx.x < NT / 32) ? red[threadIdx.x] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+        if (threadIdx.x == 0) atomic_max_pos(dst, v);
+    }
+}
+
+// Two-stage TMA pipeline of a persistent CTA: tile k computes from stage k&1
+// while tile k+1 streams into the other stage.  Barrier k&1 completes phase
+// (k>>1)&1 when tile k has landed.
+__device__ __forceinline__ void pipe_init(uint64_t* bar) {
+    if (threadIdx.x == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        fence_barrier_init();
+    }
+    __syncthreads();
+}
+// thread 0: one box into a stage (the stage's previous generic reads are ordered
+// before the async-proxy write by the fence)
+__device__ __forceinline__ void issue_box(double* dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
+    tma_load_2d(dst, map, x, y, bar);
+}
+__device__ __forceinline__ void issue_begin(uint64_t* bar, uint32_t bytes) {
+    fence_proxy_async();
+    mbar_arrive_expect_tx(bar, bytes);
+}
+// every thread of the CTA gets the same answer, so a timed-out wait makes the
+// whole CTA leave together
+__device__ __forceinline__ bool pipe_wait(uint64_t* bar, int k, Scalars* sc) {
+    const bool ok = mbar_wait(&bar[k & 1], (uint32_t)((k >> 1) & 1), sc);
+    return __syncthreads_and(ok ? 1 : 0) != 0;
+}
+// after a timed-out wait: before the CTA leaves, wait (again bounded) for the
+// copy of tile k+1 if one was issued, so no copy lands in released shared memory
+__device__ __forceinline__ void pipe_drain(uint64_t* bar, int k, bool issued_next, Scalars* sc) {
+    if (threadIdx.x == 0 && issued_next) mbar_wait(&bar[(k + 1) & 1], (uint32_t)(((k + 1) >> 1) & 1), sc);
 }
 
 }  // namespace pg

@@ -452,6 +452,53 @@ static pg_status engine_create(const pg_params* P, int device, void* stream, Eng
     return PG_OK;
 }
 
+// Tables-only disk for the FP32 form: grid, FP64 tables, orbital-advection
+// arrays and device scalars of one disk on stream s, without state buffers.
+pg_status table_engine_create(const pg_params* P, int device, cudaStream_t s, Engine** out) {
+    *out = nullptr;
+    Engine* E = nullptr;
+    pg_status st = engine_create(P, device, s, &E);
+    if (st != PG_OK) return st;
+    const int xarr = E->P.xres + 2 * NPAD;
+    cudaError_t e;
+    if ((e = cudaMalloc(&E->rot, xarr * sizeof(double))) != cudaSuccess ||
+        (e = cudaMalloc(&E->res, xarr * sizeof(double))) != cudaSuccess ||
+        (e = cudaMalloc(&E->inc, xarr * sizeof(int))) != cudaSuccess) {
+        delete E;
+        return fail(PG_ERR_CUDA, "cudaMalloc: %s", cudaGetErrorString(e));
+    }
+    E->own_orb = true;
+    cudaMemsetAsync(E->res, 0, xarr * sizeof(double), E->stream);
+    cudaMemsetAsync(E->inc, 0, xarr * sizeof(int), E->stream);
+    if ((st = engine_setup(*E, nullptr, nullptr, nullptr, nullptr)) != PG_OK) {
+        delete E;
+        return st;
+    }
+    *out = E;
+    return PG_OK;
+}
+void engine_destroy(Engine* E) { delete E; }
+const DiskView& engine_view(const Engine* E) { return E->view; }
+void engine_init_planet(Engine* E, double t) { launch_init_planet(E->view, E->P, t, E->stream); }
+
+// 3D FP32 tensor map over `planes` planes of rows x pitch floats.
+pg_status make_map3_f32(CUtensorMap* m, const float* base, uint64_t pitch, uint64_t rows, uint64_t planes,
+                        uint32_t bx, uint32_t by, uint32_t bz) {
+    EncodeTiledFn fn = encode_fn();
+    if (!fn) return fail(PG_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
+    if (reinterpret_cast<uintptr_t>(base) % 16 != 0 || (pitch * 4) % 16 != 0)
+        return fail(PG_ERR_CONFIG, "FP32 planes must have 16-byte aligned rows");
+    cuuint64_t dims[3] = {pitch, rows, planes};
+    cuuint64_t strides[2] = {pitch * 4, pitch * rows * 4};
+    cuuint32_t box[3] = {bx, by, bz};
+    cuuint32_t es[3] = {1, 1, 1};
+    CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float*>(base), dims, strides, box, es,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(PG_ERR_CUDA, "cuTensorMapEncodeTiled (3D FP32) failed (%d)", (int)r);
+    return PG_OK;
+}
+
 __global__ void k_fill(const DiskView d, Cell* buf, const double* r, const double* p, const double* u,
                        const double* v) {
     // fill_grid (src/init/init.cu:502-519) then load_grid's interior fields (src/output/output.cu:197-243)

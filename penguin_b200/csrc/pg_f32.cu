@@ -1,0 +1,1096 @@
+// FP32-mixed Godunov step for ensembles of 2D polar planet-disks (sm_100a).
+//
+// The same five fused passes as the FP64 kernels (kick1 C->T, radial sweep T->C,
+// azimuthal sweep + orbital shift C->T, residual advection T->C, kick2 +
+// damping + CFL rate C->T), on FP32 residual planes.  Every pass is ONE
+// persistent launch over the concatenated tile lists of all disks in the
+// ensemble: a CTA walks tiles blockIdx.x, blockIdx.x + gridDim.x, ... and finds
+// each tile's disk by binary search over per-disk tile offsets, so disks of
+// uneven size share the GPU without one launch per disk.  Tiles arrive through
+// 3D TMA copies (x, y, plane) whose tensor maps live in device memory, one set
+// per disk, double-buffered as in the FP64 kernels.
+//
+// A disk whose clock reached end_time has its tiles copied through unchanged, so
+// the two state buffers of all disks stay in step.
+#include <cstdio>
+
+#include "pg_common.cuh"
+#include "pg_f32.cuh"
+#include "pg_internal.h"
+#include "pg_planet.cuh"
+
+namespace pg {
+namespace f32 {
+
+constexpr int T_LEN = 32, T_W = 8;           // outputs along / across the sweep per tile
+constexpr int P1N = (T_LEN + 2) * T_W;       // 272 reconstructed cells
+constexpr int P2N = (T_LEN + 1) * T_W;       // 264 faces
+constexpr int SWT = 288;                     // sweep threads
+constexpr int XB_W = 40, XB_H = 8, XPL = XB_W * XB_H, XS = XPL * NPL;                  // radial tile: 960 floats
+constexpr int YB_W = 12, YB_H = 38, YPL = YB_W * YB_H, YS = (YPL * NPL + 31) / 32 * 32;  // azimuthal: 1376
+constexpr int SB_W = 36, SB_H = 10, SPL = SB_W * SB_H, SS = (SPL * NPL + 31) / 32 * 32;  // stencil: 1088
+constexpr int VS = (SPL * 2 + 31) / 32 * 32;                                            // stress: 736
+constexpr int STT = 256;                     // stencil threads (32 x 8 cells)
+constexpr int NSX = 13, NSY = 8;             // floats kept per reconstructed cell
+constexpr int NFA = (T_LEN + 6) * T_W;       // advection faces per tile
+constexpr size_t SX_SMEM = (size_t)(2 * XS + NSX * P1N + 4 * P2N) * 4 + 16 + 128;
+constexpr size_t SY_SMEM = (size_t)(2 * YS + NSY * P1N + 4 * P2N) * 4 + 16 + 128;
+constexpr size_t AD_SMEM = (size_t)(2 * YS + 3 * NFA) * 4 + 16 + 128;
+constexpr size_t K1_SMEM = (size_t)(2 * SS) * 4 + 16 + 128;
+constexpr size_t K2_SMEM = (size_t)(3 * SS + 2 * VS) * 4 + 16 + 128;
+static_assert(XS % 32 == 0 && YS % 32 == 0 && SS % 32 == 0 && VS % 32 == 0, "128-B aligned TMA stages");
+static_assert((2 * XS + NSX * P1N + 4 * P2N) % 2 == 0 && (2 * YS + NSY * P1N + 4 * P2N) % 2 == 0 &&
+                  (2 * YS + 3 * NFA) % 2 == 0 && (3 * SS + 2 * VS) % 2 == 0,
+              "8-B aligned barriers");
+
+__device__ __forceinline__ float* smem_base128f(float* p) {
+    const uintptr_t a = reinterpret_cast<uintptr_t>(p);
+    return reinterpret_cast<float*>((a + 127) & ~uintptr_t(127));
+}
+
+// disk owning global tile `tile`: the largest k with first[k] <= tile
+__device__ __forceinline__ int find_disk(const int* __restrict__ first, int nd, int tile) {
+    int lo = 0, hi = nd - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (first[mid] <= tile) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// Interior cell (i, j) and its periodic azimuthal image (boundary.cu:141-209).
+__device__ __forceinline__ void emit32(const View32& w, float* out, int i, int j, float a, float b, float c) {
+    const size_t pl = w.plane();
+    size_t m = (size_t)j * w.pitch + i;
+    out[m] = a;
+    out[pl + m] = b;
+    out[2 * pl + m] = c;
+    int jimg = -1;
+    if (j < 2 * NPAD) jimg = j + w.yres;
+    else if (j >= w.yres) jimg = j - w.yres;
+    if (jimg >= 0) {
+        m = (size_t)jimg * w.pitch + i;
+        out[m] = a;
+        out[pl + m] = b;
+        out[2 * pl + m] = c;
+    }
+}
+
+// Star + planet gravity (forces.cu:182-327) without the star term, which is in
+// X_ABG.  |r - r_p|^2 = (r - x_p)^2 + 2 r x_p (1 - cos) + rs^2 has no cancellation.
+// which: 0 = planet of the first half-kick, 1 = planet at t + dt.
+__device__ __forceinline__ void gravity32(const View32& w, int i, int j, int which, float& gx, float& gy) {
+    gx = 0.0f;
+    gy = 0.0f;
+    if (w.nplanet == 0) return;
+    const float* tr = w.trow(j) + 3 * which;
+    const float* s = w.tscal() + 4 * which;
+    const float m = s[0], xp = s[1], rs2 = s[2], ip2 = s[3];
+    const float dr = w.tcol()[2 * i + which];
+    const float rad = w.x(X_RAD)[i];
+    const float R2 = dr * dr + 2.0f * rad * xp * tr[2] + rs2;
+    const float ir = rsqrtf(R2);
+    const float rf = ir * ir * ir;
+    gx = -m * (dr + xp * tr[2]) * rf - m * tr[1] * ip2;
+    gy = -m * xp * tr[0] * rf + m * tr[0] * ip2;
+}
+
+// Half-kick of the residual velocities (sweeps.cu:597-711 with geomx 1):
+// v^2/r - 1/r^2 = X_ABG + (2 v0/r + dv/r) dv.  mdt != 0 re-evaluates the
+// curvature term at the mdt-predicted velocity (sweeps.cu:663-687).
+__device__ __forceinline__ void kick32(const View32& w, int i, float dS, float& du, float& dv, float vx, float vy,
+                                       float gx, float gy, float mdt, float dt, bool visc) {
+    const float iS = visc ? 1.0f / (w.x(X_SBG)[i] + dS) : 0.0f;
+    const float abg = w.x(X_ABG)[i], v2r = w.x(X_V2R)[i], ir = w.x(X_IRAD)[i];
+    float fx = abg + (v2r + dv * ir) * dv + vx * iS;
+    const float fy = vy * iS;
+    if (mdt != 0.0f) {
+        const float dvT = dv + fy * mdt + gy * mdt;
+        fx = abg + (v2r + dvT * ir) * dvT + vx * iS;
+    }
+    du = du + fx * dt + gx * dt;
+    dv = dv + fy * dt + gy * dt;
+}
+
+// Viscous force density at stencil-tile cell (x, y) of planes {dS, du, dv} with
+// row length SB_W: residual part plus background part (viscosity.cu:84-194).
+__device__ __forceinline__ void stress32(const View32& w, const float* tile, int x, int y, int i, int j, float& vx,
+                                         float& vy) {
+    const float* nu = w.x(X_NU);
+    const float* vb = w.x(X_VBG) + 7 * i;
+    const float* X = w.x(X_VISX) + 5 * i;
+    const float* Y = w.y(Y_VISY) + 4 * j;
+    const float* S = tile;
+    const float* U = tile + SPL;
+    const float* V = tile + 2 * SPL;
+    const int c = y * SB_W + x;
+    const float n1 = nu[i];
+    const float nr1 = (w.x(X_SBG)[i] + S[c]) * n1;
+    const float dndx = (vb[6] + S[c + 1] * nu[i + 1] - S[c - 1] * nu[i - 1]) * X[0];
+    const float dndy = (S[c + SB_W] - S[c - SB_W]) * n1 * Y[0] * X[4];
+    float u[9], v[9];
+#pragma unroll
+    for (int n = 0; n < 9; ++n) {
+        const int dx = (n % 3) - 1;
+        const int dy = (n < 3) ? 0 : (n < 6 ? -1 : 1);
+        u[n] = U[c + dy * SB_W + dx];
+        v[n] = V[c + dy * SB_W + dx];
+    }
+    float fx, fy;
+    viscous32(X, Y, u, v, nr1, dndx, dndy, fx, fy);
+    vx = fx + vb[0] * nr1 + vb[1] * dndx + vb[2] * dndy;
+    vy = fy + vb[3] * nr1 + vb[4] * dndx + vb[5] * dndy;
+}
+
+// CFL signal rate (timestep.cu:46-77) in FP64 from the residuals.
+__device__ __forceinline__ double rate64(const View32& w, int i, int j, float du, float dv) {
+    const DiskView& d = w.d64;
+    const double cs = w.cs64[i];
+    const double u = d.initx[5 * i + 2] + (double)du;
+    const double vn = (d.initx[5 * i + 3] - d.radx[i] * d.frame_omega - d.rot[i]) + (double)dv;
+    const double a = (fabs(u) + cs) * d.idx_x[i];
+    const double b = (fabs(vn) + cs) * (d.idx_y[j] * d.irad[i]);
+    return fmax(a, b);
+}
+
+// ============================================================ radial sweep
+__global__ void __launch_bounds__(SWT) k32_sweep_x(const View32* __restrict__ V, const int* __restrict__ first,
+                                                   int nd, int ntiles, int in) {
+    extern __shared__ __align__(128) float fsm_raw[];
+    float* sm = smem_base128f(fsm_raw);
+    auto stage = [&](int n) { return sm + (n & 1) * XS; };
+    float* st = sm + 2 * XS;      // [NSX][P1N]
+    float* fl = st + NSX * P1N;   // [4][P2N]
+    uint64_t* bar = reinterpret_cast<uint64_t*>(fl + 4 * P2N);
+    const int tid = threadIdx.x;
+    auto locate = [&](int tile, int& k, int& s0, int& q0) {
+        k = find_disk(first, nd, tile);
+        const int loc = tile - first[k];
+        const int ntx = V[k].ntx[0];
+        s0 = NPAD + T_LEN * (loc % ntx);
+        q0 = NPAD + T_W * (loc / ntx);
+    };
+    auto issue = [&](int tile, int kt) {
+        int k, s0, q0;
+        locate(tile, k, s0, q0);
+        issue_begin(&bar[kt & 1], XS * 4);
+        tma_load_3d(stage(kt), V[k].maps + 3 * in + 0, s0 - NPAD, q0, 0, &bar[kt & 1]);
+    };
+    pipe_init(bar);
+    if ((int)blockIdx.x >= ntiles) return;
+    if (tid == 0) issue(blockIdx.x, 0);
+    int kt = 0;
+    for (int tile_id = blockIdx.x; tile_id < ntiles; tile_id += gridDim.x, ++kt) {
+        if (tid == 0 && tile_id + (int)gridDim.x < ntiles) issue(tile_id + gridDim.x, kt + 1);
+        int k, s0, q0;
+        locate(tile_id, k, s0, q0);
+        const View32& w = V[k];
+        Scalars* sc = w.d64.sc;
+        const float* T = stage(kt);
+        if (!pipe_wait(bar, kt, sc)) {
+            pipe_drain(bar, kt, tile_id + (int)gridDim.x < ntiles, sc);
+            return;
+        }
+        const bool done = sc->done != 0;
+        const float dtf = (float)sc->dt;
+        const float gam = w.gam;
+        if (!done) {
+            // ---- P1: deviations, reconstruction, both edge states of every cell
+            if (tid < P1N) {
+                const int q = tid / (T_LEN + 2), t = 2 + tid % (T_LEN + 2);
+                const int s = s0 - NPAD + t;
+                const int sc_ = min(s, w.xarr - 1);
+                const float* r0 = T + q * XB_W + (t - 2);
+                float dS[5], du[5], dv[5];
+#pragma unroll
+                for (int m = 0; m < 5; ++m) {
+                    dS[m] = r0[m];
+                    du[m] = r0[XPL + m];
+                    dv[m] = r0[2 * XPL + m];
+                }
+                const float* db = w.x(X_DBG) + 16 * sc_;
+                const float* cs2t = w.x(X_CS2);
+                const float* radt = w.x(X_RAD);
+                const float cs2c = cs2t[sc_], radc = radt[sc_];
+                float aS[5], aP[5], aU[5], aL[5];
+#pragma unroll
+                for (int m = 0; m < 5; ++m) {
+                    if (m == 2) {
+                        aS[m] = aP[m] = aU[m] = aL[m] = 0.0f;
+                        continue;
+                    }
+                    const int kk = m < 2 ? m : m - 1;
+                    const int sk = min(max(s - 2 + m, 0), w.xarr - 1);
+                    aS[m] = (dS[m] - dS[2]) + db[kk];
+                    aP[m] = (cs2t[sk] * dS[m] - cs2c * dS[2]) + db[4 + kk];
+                    aU[m] = (du[m] - du[2]) + db[8 + kk];
+                    aL[m] = (radt[sk] * dv[m] - radc * dv[2]) + db[12 + kk];
+                }
+                const float Sc = w.x(X_SBG)[sc_] + dS[2];
+                const float pc = w.x(X_PBG)[sc_] + cs2c * dS[2];
+                const float uc = w.x(X_UBG)[sc_] + du[2];
+                const float cs0 = sqrtf(gam * pc / Sc);
+                const float flat = flatten32(1.0f / cs0, pc, aP[0], aP[1], aP[3], aP[4], aU[1], aU[3]);
+                const float* wt = w.x(X_WX) + 6 * sc_;
+                const Par32 R = recon32(wt, aS[0], aS[1], aS[3], aS[4], flat);
+                const Par32 P = recon32(wt, aP[0], aP[1], aP[3], aP[4], flat);
+                const Par32 U = recon32(wt, aU[0], aU[1], aU[3], aU[4], flat);
+                const Par32 L = recon32(wt, aL[0], aL[1], aL[3], aL[4], flat);
+                const float idx = w.x(X_IDX)[sc_];
+                const HS a = left_edge32(gam, idx, dtf, cs0, Sc, pc, uc, R, P, U, L);
+                const HS b = right_edge32(gam, idx, dtf, cs0, Sc, pc, uc, R, P, U, L);
+                float* o = st + tid;
+                o[0] = a.rd;
+                o[P1N] = a.pd;
+                o[2 * P1N] = a.u;
+                o[3 * P1N] = a.v;
+                o[4 * P1N] = b.rd;
+                o[5 * P1N] = b.pd;
+                o[6 * P1N] = b.u;
+                o[7 * P1N] = b.v;
+                o[8 * P1N] = aS[3];  // jumps to the right neighbour
+                o[9 * P1N] = aP[3];
+                o[10 * P1N] = aL[3];
+                o[11 * P1N] = Sc;
+                o[12 * P1N] = pc;
+            }
+            __syncthreads();
+            // ---- P2: HLLC at every face, referenced to the face's left cell
+            if (tid < P2N) {
+                const int q = tid / (T_LEN + 1), f = tid % (T_LEN + 1);
+                const int iL = q * (T_LEN + 2) + f, iR = iL + 1;
+                HS L, R;
+                L.rd = st[4 * P1N + iL];
+                L.pd = st[5 * P1N + iL];
+                L.u = st[6 * P1N + iL];
+                L.v = st[7 * P1N + iL];
+                R.rd = st[iR] + st[8 * P1N + iL];
+                R.pd = st[P1N + iR] + st[9 * P1N + iL];
+                R.u = st[2 * P1N + iR];
+                R.v = st[3 * P1N + iR] + st[10 * P1N + iL];
+                const FX F = hllc32(gam, st[11 * P1N + iL], st[12 * P1N + iL], L, R);
+                fl[tid] = F.r;
+                fl[P2N + tid] = F.u;
+                fl[2 * P2N + tid] = F.v;
+                fl[3 * P2N + tid] = F.pd;
+            }
+            __syncthreads();
+        }
+        // ---- P3: residual update (sweeps.cu:218-261, 300-335)
+        if (tid < T_LEN * T_W) {
+            const int q = tid / T_LEN, o = tid % T_LEN;
+            const int s = s0 + o, j = q0 + q;
+            if (s < NPAD + w.xres && j < NPAD + w.yres) {
+                const float* c = T + q * XB_W + NPAD + o;
+                const float dS0 = c[0], du0 = c[XPL], dv0 = c[2 * XPL];
+                float dSn = dS0, dun = du0, dvn = dv0;
+                if (!done) {
+                    const int iC = q * (T_LEN + 2) + 1 + o;
+                    const int f0 = q * (T_LEN + 1) + o, f1 = f0 + 1;
+                    const float g0 = w.x(X_XA)[s], g1 = w.x(X_XA)[s + 1];
+                    const float f = dtf * w.x(X_IXV)[s];
+                    const float Fr0 = fl[f0], Fr1 = fl[f1];
+                    const float Dr = (Fr0 * g0 - Fr1 * g1) * f;
+                    // pres0 - pres1 = (p[s-1] - p[s]) + (pd0 - pd1)
+                    const float dpres = (fl[3 * P2N + f0] - fl[3 * P2N + f1]) - st[9 * P1N + iC - 1];
+                    const float Du = ((fl[P2N + f0] * g0 - fl[P2N + f1] * g1) + 0.5f * (g0 + g1) * dpres) * f;
+                    // D(Sigma v) - v D(Sigma) with l = r v: faces referenced to cells s-1 and s
+                    const float Dv = (g0 * Fr0 * (fl[2 * P2N + f0] - st[10 * P1N + iC - 1]) - g1 * Fr1 * fl[2 * P2N + f1]) *
+                                     f * w.x(X_IRAD)[s];
+                    const float Sc = st[11 * P1N + iC];
+                    const float uc = w.x(X_UBG)[s] + du0;
+                    const float Sn = Sc + Dr;
+                    const float rmin = fmaxf(Sc * 1.0e-10f, 1.0e-10f);
+                    if (Sn < rmin) {
+                        dSn = rmin - w.x(X_SBG)[s];
+                        atomicAdd(&sc->floor_hits, 1);
+                    } else {
+                        const float iS = 1.0f / Sn;
+                        dSn = dS0 + Dr;
+                        dun = du0 + (Du - uc * Dr) * iS;
+                        dvn = dv0 + Dv * iS;
+                    }
+                    if (!(Sn > 0.0f)) atomicOr(&sc->err, 1 << PG_ERR_NAN);
+                }
+                emit32(w, w.buf[in ^ 1], s, j, dSn, dun, dvn);
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// ========================================= azimuthal sweep + orbital shift
+__global__ void __launch_bounds__(SWT) k32_sweep_y(const View32* __restrict__ V, const int* __restrict__ first,
+                                                   int nd, int ntiles, int in) {
+    extern __shared__ __align__(128) float fsm_raw[];
+    float* sm = smem_base128f(fsm_raw);
+    auto stage = [&](int n) { return sm + (n & 1) * YS; };
+    float* st = sm + 2 * YS;      // [NSY][P1N]
+    float* fl = st + NSY * P1N;   // [4][P2N]
+    uint64_t* bar = reinterpret_cast<uint64_t*>(fl + 4 * P2N);
+    __shared__ int s_inc[T_W];
+    const int tid = threadIdx.x;
+    const int* fst = first + (nd + 1);
+    auto locate = [&](int tile, int& k, int& s0, int& q0) {
+        k = find_disk(fst, nd, tile);
+        const int loc = tile - fst[k];
+        const int ntx = V[k].ntx[1];
+        s0 = NPAD + T_LEN * (loc % ntx);  // first output row
+        q0 = NPAD + T_W * (loc / ntx);    // first column
+    };
+    auto issue = [&](int tile, int kt) {
+        int k, s0, q0;
+        locate(tile, k, s0, q0);
+        issue_begin(&bar[kt & 1], YPL * NPL * 4);
+        tma_load_3d(stage(kt), V[k].maps + 3 * in + 1, q0 - NPAD, s0 - NPAD, 0, &bar[kt & 1]);
+    };
+    pipe_init(bar);
+    if ((int)blockIdx.x >= ntiles) return;
+    if (tid == 0) issue(blockIdx.x, 0);
+    int kt = 0;
+    for (int tile_id = blockIdx.x; tile_id < ntiles; tile_id += gridDim.x, ++kt) {
+        if (tid == 0 && tile_id + (int)gridDim.x < ntiles) issue(tile_id + gridDim.x, kt + 1);
+        int k, s0, q0;
+        locate(tile_id, k, s0, q0);
+        const View32& w = V[k];
+        Scalars* sc = w.d64.sc;
+        const float* T = stage(kt);
+        const bool done = sc->done != 0;
+        const double dt = sc->dt;
+        const float dtf = (float)dt;
+        const float gam = w.gam;
+        if (tid < T_W) {
+            // set_orbital_advection (src/orbit/orbit.cu:74-99) in FP64 for this column
+            const int i = q0 + tid;
+            int shift = 0;
+            if (!done && w.orbadv && i < NPAD + w.xres) {
+                const DiskView& d = w.d64;
+                const double dy = d.dy0 * d.radx[i];
+                const double rot = d.rot[i];
+                shift = __double2int_rd(rot * dt / dy + 0.5);
+                double speed = shift * dy / dt;
+                speed = rot - speed;
+                if (s0 == NPAD) {
+                    d.res[i] = speed;
+                    d.inc[i] = shift;
+                }
+            }
+            s_inc[tid] = shift;
+        }
+        if (!pipe_wait(bar, kt, sc)) {
+            pipe_drain(bar, kt, tile_id + (int)gridDim.x < ntiles, sc);
+            return;
+        }
+        if (!done) {
+            // ---- P1: background-relative deviations along the column
+            if (tid < P1N) {
+                const int q = tid % T_W, t = 2 + tid / T_W;
+                const int i = min(q0 + q, w.xarr - 1);
+                const int jc = min(s0 - NPAD + t, w.yarr - 1);
+                const float* col = T + (q + NPAD) + (t - 2) * YB_W;
+                float dS[5], du[5], dv[5];
+#pragma unroll
+                for (int m = 0; m < 5; ++m) {
+                    dS[m] = col[m * YB_W];
+                    du[m] = col[YPL + m * YB_W];
+                    dv[m] = col[2 * YPL + m * YB_W];
+                }
+                float aS[5], aN[5], aT[5];
+#pragma unroll
+                for (int m = 0; m < 5; ++m) {
+                    aS[m] = dS[m] - dS[2];
+                    aN[m] = dv[m] - dv[2];
+                    aT[m] = du[m] - du[2];
+                }
+                const float cs2 = w.x(X_CS2)[i];
+                const float Sc = w.x(X_SBG)[i] + dS[2];
+                const float pc = cs2 * Sc;
+                const float cs0 = w.x(X_CS0)[i];
+                const float un = dv[2] + w.x(X_EPS)[i];
+                // p = cs2 Sigma along the column: pressure ratios are density ratios
+                const float flat = flatten32(1.0f / cs0, Sc, aS[0], aS[1], aS[3], aS[4], aN[1], aN[3]);
+                const float* wt = w.y(Y_WY) + 6 * jc;
+                const Par32 R = recon32(wt, aS[0], aS[1], aS[3], aS[4], flat);
+                const Par32 N = recon32(wt, aN[0], aN[1], aN[3], aN[4], flat);
+                const Par32 Tt = recon32(wt, aT[0], aT[1], aT[3], aT[4], flat);
+                const Par32 P{cs2 * R.sL, cs2 * R.sR};
+                const float sdt = dtf * w.x(X_IRAD)[i];
+                const float idy = w.y(Y_IDY)[jc];
+                HS a = left_edge32(gam, idy, sdt, cs0, Sc, pc, un, R, P, N, Tt);
+                HS b = right_edge32(gam, idy, sdt, cs0, Sc, pc, un, R, P, N, Tt);
+                a.rd += dS[2];
+                a.pd += cs2 * dS[2];
+                a.v += du[2];
+                b.rd += dS[2];
+                b.pd += cs2 * dS[2];
+                b.v += du[2];
+                float* o = st + tid;
+                o[0] = a.rd;
+                o[P1N] = a.pd;
+                o[2 * P1N] = a.u;
+                o[3 * P1N] = a.v;
+                o[4 * P1N] = b.rd;
+                o[5 * P1N] = b.pd;
+                o[6 * P1N] = b.u;
+                o[7 * P1N] = b.v;
+            }
+            __syncthreads();
+            // ---- P2: HLLC referenced to the background (constant along the column)
+            if (tid < P2N) {
+                const int q = tid % T_W, f = tid / T_W;
+                const int i = min(q0 + q, w.xarr - 1);
+                const int iL = f * T_W + q, iR = iL + T_W;
+                HS L, R;
+                L.rd = st[4 * P1N + iL];
+                L.pd = st[5 * P1N + iL];
+                L.u = st[6 * P1N + iL];
+                L.v = st[7 * P1N + iL];
+                R.rd = st[iR];
+                R.pd = st[P1N + iR];
+                R.u = st[2 * P1N + iR];
+                R.v = st[3 * P1N + iR];
+                const FX F = hllc32(gam, w.x(X_SBG)[i], w.x(X_PBG)[i], L, R);
+                fl[tid] = F.r;
+                fl[P2N + tid] = F.u;
+                fl[2 * P2N + tid] = F.v;
+                fl[3 * P2N + tid] = F.pd;
+            }
+            __syncthreads();
+        }
+        // ---- P3: residual update (sweeps.cu:361-433) and the orbital shift (orbit.cu:30-46)
+        if (tid < T_LEN * T_W) {
+            const int q = tid % T_W, o = tid / T_W;
+            const int j = s0 + o, i = q0 + q;
+            if (j < NPAD + w.yres && i < NPAD + w.xres) {
+                const float* c = T + (NPAD + o) * YB_W + NPAD + q;
+                const float dS0 = c[0], du0 = c[YPL], dv0 = c[2 * YPL];
+                float dSn = dS0, dun = du0, dvn = dv0;
+                int jo = j;
+                if (!done) {
+                    const int f0 = o * T_W + q, f1 = f0 + T_W;
+                    const float f = dtf * w.y(Y_IYV)[j] * w.x(X_IRAD)[i];
+                    const float Fr0 = fl[f0], Fr1 = fl[f1];
+                    const float Dr = (Fr0 - Fr1) * f;
+                    const float Dn = ((fl[P2N + f0] - fl[P2N + f1]) + (fl[3 * P2N + f0] - fl[3 * P2N + f1])) * f;
+                    const float Dt = (Fr0 * (fl[2 * P2N + f0] - du0) - Fr1 * (fl[2 * P2N + f1] - du0)) * f;
+                    const float Sc = w.x(X_SBG)[i] + dS0;
+                    const float Sn = Sc + Dr;
+                    const float un = dv0 + w.x(X_EPS)[i];
+                    const float rmin = fmaxf(Sc * 1.0e-10f, 1.0e-10f);
+                    if (Sn < rmin) {
+                        dSn = rmin - w.x(X_SBG)[i];
+                        atomicAdd(&sc->floor_hits, 1);
+                    } else {
+                        const float iS = 1.0f / Sn;
+                        dSn = dS0 + Dr;
+                        dvn = dv0 + (Dn - un * Dr) * iS;
+                        dun = du0 + Dt * iS;
+                    }
+                    if (!(Sn > 0.0f)) atomicOr(&sc->err, 1 << PG_ERR_NAN);
+                    if (w.orbadv) {
+                        int js = (j - NPAD + s_inc[q]) % w.yres;
+                        if (js < 0) js += w.yres;
+                        jo = js + NPAD;
+                    }
+                }
+                emit32(w, w.buf[in ^ 1], i, jo, dSn, dun, dvn);
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// ===================================================== residual advection
+__global__ void __launch_bounds__(SWT) k32_advect(const View32* __restrict__ V, const int* __restrict__ first,
+                                                  int nd, int ntiles, int in) {
+    extern __shared__ __align__(128) float fsm_raw[];
+    float* sm = smem_base128f(fsm_raw);
+    auto stage = [&](int n) { return sm + (n & 1) * YS; };
+    float* fl = sm + 2 * YS;  // [3][NFA]: mass flux, then the upwind carriers of v and u
+    uint64_t* bar = reinterpret_cast<uint64_t*>(fl + 3 * NFA);
+    const int tid = threadIdx.x;
+    const int* fst = first + (nd + 1);
+    auto locate = [&](int tile, int& k, int& s0, int& q0) {
+        k = find_disk(fst, nd, tile);
+        const int loc = tile - fst[k];
+        const int ntx = V[k].ntx[1];
+        s0 = NPAD + T_LEN * (loc % ntx);
+        q0 = NPAD + T_W * (loc / ntx);
+    };
+    auto issue = [&](int tile, int kt) {
+        int k, s0, q0;
+        locate(tile, k, s0, q0);
+        issue_begin(&bar[kt & 1], YPL * NPL * 4);
+        tma_load_3d(stage(kt), V[k].maps + 3 * in + 1, q0 - NPAD, s0 - NPAD, 0, &bar[kt & 1]);
+    };
+    pipe_init(bar);
+    if ((int)blockIdx.x >= ntiles) return;
+    if (tid == 0) issue(blockIdx.x, 0);
+    int kt = 0;
+    for (int tile_id = blockIdx.x; tile_id < ntiles; tile_id += gridDim.x, ++kt) {
+        if (tid == 0 && tile_id + (int)gridDim.x < ntiles) issue(tile_id + gridDim.x, kt + 1);
+        int k, s0, q0;
+        locate(tile_id, k, s0, q0);
+        const View32& w = V[k];
+        Scalars* sc = w.d64.sc;
+        const float* T = stage(kt);
+        if (!pipe_wait(bar, kt, sc)) {
+            pipe_drain(bar, kt, tile_id + (int)gridDim.x < ntiles, sc);
+            return;
+        }
+        const bool done = sc->done != 0;
+        const double dt = sc->dt;
+        const float dtf = (float)dt;
+        if (!done) {
+            // ---- P1: upwind PPM average over the swept fraction (advection.cu:20-67)
+            if (tid < P1N) {
+                const int q = tid % T_W, t = 2 + tid / T_W;
+                const int i = min(q0 + q, w.xarr - 1);
+                const int jc = min(s0 - NPAD + t, w.yarr - 1);
+                const DiskView& d = w.d64;
+                const double speed = d.res[i];
+                // the swept fraction in FP64: |res| dt / (r dphi)
+                const float yf = (float)fmin(fmax(fabs(speed) * (dt * d.irad[i]) * d.idx_y[jc], 0.0), 1.0);
+                const float* col = T + (q + NPAD) + (t - 2) * YB_W;
+                float dS[5], du[5], dv[5];
+#pragma unroll
+                for (int m = 0; m < 5; ++m) {
+                    dS[m] = col[m * YB_W];
+                    du[m] = col[YPL + m * YB_W];
+                    dv[m] = col[2 * YPL + m * YB_W];
+                }
+                const float* wt = w.y(Y_WY) + 6 * jc;
+                const Par32 R = recon32(wt, dS[0] - dS[2], dS[1] - dS[2], dS[3] - dS[2], dS[4] - dS[2], 0.0f);
+                const Par32 N = recon32(wt, dv[0] - dv[2], dv[1] - dv[2], dv[3] - dv[2], dv[4] - dv[2], 0.0f);
+                const Par32 Tt = recon32(wt, du[0] - du[2], du[1] - du[2], du[3] - du[2], du[4] - du[2], 0.0f);
+                const Frac32 qf = frac32(yf);
+                float fr, fn, ft;
+                int face;
+                if (speed > 0.0) {
+                    fr = aveR32(qf, R);
+                    fn = aveR32(qf, N);
+                    ft = aveR32(qf, Tt);
+                    face = t + 1;
+                } else {
+                    fr = aveL32(qf, R);
+                    fn = aveL32(qf, N);
+                    ft = aveL32(qf, Tt);
+                    face = t;
+                }
+                const float Sc = w.x(X_SBG)[i] + dS[2];
+                const int m = face * T_W + q;
+                fl[m] = (Sc + fr) * (float)speed;
+                fl[NFA + m] = dv[2] + fn;
+                fl[2 * NFA + m] = du[2] + ft;
+            }
+            __syncthreads();
+        }
+        // ---- P2: flux difference and update_Cell_advect (advection.cu:88-105, 153-170)
+        if (tid < T_LEN * T_W) {
+            const int q = tid % T_W, o = tid / T_W;
+            const int s = s0 + o, i = q0 + q;
+            if (s < NPAD + w.yres && i < NPAD + w.xres) {
+                const float* c = T + (NPAD + o) * YB_W + NPAD + q;
+                const float dS0 = c[0], du0 = c[YPL], dv0 = c[2 * YPL];
+                float dSn = dS0, dun = du0, dvn = dv0;
+                if (!done) {
+                    const int k0 = (NPAD + o) * T_W + q, k1 = k0 + T_W;
+                    const float f = dtf * w.y(Y_IYV)[s] * w.x(X_IRAD)[i];
+                    const float F0 = fl[k0], F1 = fl[k1];
+                    const float Dr = (F0 - F1) * f;
+                    const float Sn = (w.x(X_SBG)[i] + dS0) + Dr;
+                    const float iS = 1.0f / Sn;
+                    dSn = dS0 + Dr;
+                    dvn = dv0 + (F0 * (fl[NFA + k0] - dv0) - F1 * (fl[NFA + k1] - dv0)) * f * iS;
+                    dun = du0 + (F0 * (fl[2 * NFA + k0] - du0) - F1 * (fl[2 * NFA + k1] - du0)) * f * iS;
+                    if (!(Sn > 0.0f)) atomicOr(&sc->err, 1 << PG_ERR_NAN);
+                }
+                emit32(w, w.buf[in ^ 1], i, s, dSn, dun, dvn);
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// ====================================================== kick 1 (+ stress)
+__global__ void __launch_bounds__(STT) k32_kick1(const View32* __restrict__ V, const int* __restrict__ first, int nd,
+                                                 int ntiles, int in) {
+    extern __shared__ __align__(128) float fsm_raw[];
+    float* sm = smem_base128f(fsm_raw);
+    auto stage = [&](int n) { return sm + (n & 1) * SS; };
+    uint64_t* bar = reinterpret_cast<uint64_t*>(sm + 2 * SS);
+    const int tid = threadIdx.x;
+    const int* fst = first + 2 * (nd + 1);
+    auto locate = [&](int tile, int& k, int& i0, int& j0) {
+        k = find_disk(fst, nd, tile);
+        const int loc = tile - fst[k];
+        const int ntx = V[k].ntx[2];
+        i0 = NPAD + T_LEN * (loc % ntx);
+        j0 = NPAD + T_W * (loc / ntx);
+    };
+    auto issue = [&](int tile, int kt) {
+        int k, i0, j0;
+        locate(tile, k, i0, j0);
+        issue_begin(&bar[kt & 1], SPL * NPL * 4);
+        tma_load_3d(stage(kt), V[k].maps + 3 * in + 2, i0 - NPAD, j0 - 1, 0, &bar[kt & 1]);
+    };
+    pipe_init(bar);
+    if ((int)blockIdx.x >= ntiles) return;
+    if (tid == 0) issue(blockIdx.x, 0);
+    int kt = 0;
+    for (int tile_id = blockIdx.x; tile_id < ntiles; tile_id += gridDim.x, ++kt) {
+        if (tid == 0 && tile_id + (int)gridDim.x < ntiles) issue(tile_id + gridDim.x, kt + 1);
+        int k, i0, j0;
+        locate(tile_id, k, i0, j0);
+        const View32& w = V[k];
+        Scalars* sc = w.d64.sc;
+        const float* T = stage(kt);
+        if (!pipe_wait(bar, kt, sc)) {
+            pipe_drain(bar, kt, tile_id + (int)gridDim.x < ntiles, sc);
+            return;
+        }
+        const bool done = sc->done != 0;
+        const float hdt = (float)(0.5 * sc->dt);
+        const int hx = tid % T_LEN, hy = tid / T_LEN;
+        const int i = i0 + hx, j = j0 + hy;
+        if (i < NPAD + w.xres && j < NPAD + w.yres) {
+            const int x = hx + NPAD, y = hy + 1;
+            const int c = y * SB_W + x;
+            const float dS0 = T[c];
+            float du = T[SPL + c], dv = T[2 * SPL + c];
+            if (!done) {
+                float vx = 0.0f, vy = 0.0f;
+                if (w.visc) {
+                    stress32(w, T, x, y, i, j, vx, vy);
+                    // kept for the predictor of kick2, with the periodic image
+                    const size_t pl = w.plane();
+                    size_t m = (size_t)j * w.pitch + i;
+                    w.vis[m] = vx;
+                    w.vis[pl + m] = vy;
+                    int jimg = -1;
+                    if (j < 2 * NPAD) jimg = j + w.yres;
+                    else if (j >= w.yres) jimg = j - w.yres;
+                    if (jimg >= 0) {
+                        m = (size_t)jimg * w.pitch + i;
+                        w.vis[m] = vx;
+                        w.vis[pl + m] = vy;
+                    }
+                }
+                float gx, gy;
+                gravity32(w, i, j, 0, gx, gy);
+                kick32(w, i, dS0, du, dv, vx, vy, gx, gy, 0.0f, hdt, w.visc != 0);
+            }
+            emit32(w, w.buf[in ^ 1], i, j, dS0, du, dv);
+        }
+        __syncthreads();
+    }
+}
+
+// ============================================ kick 2 + damping + CFL speed
+__global__ void __launch_bounds__(STT) k32_kick2(const View32* __restrict__ V, const int* __restrict__ first, int nd,
+                                                 int ntiles, int in) {
+    extern __shared__ __align__(128) float fsm_raw[];
+    float* sm = smem_base128f(fsm_raw);
+    auto stage = [&](int n) { return sm + (n & 1) * SS; };
+    auto vstage = [&](int n) { return sm + 2 * SS + (n & 1) * VS; };
+    float* tp = sm + 2 * SS + 2 * VS;  // predicted state with 1 halo, same layout as a stage
+    uint64_t* bar = reinterpret_cast<uint64_t*>(tp + SS);
+    const int tid = threadIdx.x;
+    const int* fst = first + 2 * (nd + 1);
+    auto locate = [&](int tile, int& k, int& i0, int& j0) {
+        k = find_disk(fst, nd, tile);
+        const int loc = tile - fst[k];
+        const int ntx = V[k].ntx[2];
+        i0 = NPAD + T_LEN * (loc % ntx);
+        j0 = NPAD + T_W * (loc / ntx);
+    };
+    auto issue = [&](int tile, int kt) {
+        int k, i0, j0;
+        locate(tile, k, i0, j0);
+        const View32& w = V[k];
+        issue_begin(&bar[kt & 1], (SPL * NPL + (w.visc ? SPL * 2 : 0)) * 4);
+        tma_load_3d(stage(kt), w.maps + 3 * in + 2, i0 - NPAD, j0 - 1, 0, &bar[kt & 1]);
+        if (w.visc) tma_load_3d(vstage(kt), w.maps + 6, i0 - NPAD, j0 - 1, 0, &bar[kt & 1]);
+    };
+    pipe_init(bar);
+    double vmax = 0.0;
+    int vk = -1;  // disk whose signal rate vmax holds
+    if ((int)blockIdx.x < ntiles) {
+        if (tid == 0) issue(blockIdx.x, 0);
+        int kt = 0;
+        for (int tile_id = blockIdx.x; tile_id < ntiles; tile_id += gridDim.x, ++kt) {
+            if (tid == 0 && tile_id + (int)gridDim.x < ntiles) issue(tile_id + gridDim.x, kt + 1);
+            int k, i0, j0;
+            locate(tile_id, k, i0, j0);
+            const View32& w = V[k];
+            Scalars* sc = w.d64.sc;
+            if (k != vk) {  // uniform over the CTA: flush the previous disk's maximum
+                if (vk >= 0) block_max_to<STT>(&V[vk].d64.sc->vmax_bits, vmax);
+                vmax = 0.0;
+                vk = k;
+            }
+            const float* T = stage(kt);
+            const float* TV = vstage(kt);
+            if (!pipe_wait(bar, kt, sc)) {
+                pipe_drain(bar, kt, tile_id + (int)gridDim.x < ntiles, sc);
+                return;
+            }
+            const bool done = sc->done != 0;
+            const double dt = sc->dt;
+            const float dtf = (float)dt, hdt = (float)(0.5 * dt);
+            const bool visc = w.visc != 0;
+            if (!done && visc) {
+                // predictor (sweeps.cu:713-729, mdt = dt = dt/2) with the stress of kick1, on
+                // the tile and its halo; outside the radial range the ghosts keep init_C (zero
+                // residuals) as boundx2 does for boundary 0 (boundary.cu:722-820)
+                for (int it = tid; it < (T_LEN + 2) * SB_H; it += STT) {
+                    const int hx = it % (T_LEN + 2), hy = it / (T_LEN + 2);
+                    const int x = hx + NPAD - 1, y = hy;
+                    const int i = i0 - 1 + hx, j = j0 - 1 + hy;
+                    const int c = y * SB_W + x;
+                    float dS = T[c], du = T[SPL + c], dv = T[2 * SPL + c];
+                    if (i >= NPAD && i < NPAD + w.xres && j < w.yarr) {
+                        float gx, gy;
+                        gravity32(w, i, j, 1, gx, gy);
+                        kick32(w, i, dS, du, dv, TV[c], TV[SPL + c], gx, gy, hdt, hdt, true);
+                    }
+                    tp[c] = dS;
+                    tp[SPL + c] = du;
+                    tp[2 * SPL + c] = dv;
+                }
+                __syncthreads();
+            }
+            const int hx = tid % T_LEN, hy = tid / T_LEN;
+            const int i = i0 + hx, j = j0 + hy;
+            if (i < NPAD + w.xres && j < NPAD + w.yres) {
+                const int x = hx + NPAD, y = hy + 1;
+                const int c = y * SB_W + x;
+                float dS = T[c], du = T[SPL + c], dv = T[2 * SPL + c];
+                if (!done) {
+                    float vx = 0.0f, vy = 0.0f;
+                    if (visc) stress32(w, tp, x, y, i, j, vx, vy);
+                    float gx, gy;
+                    gravity32(w, i, j, 1, gx, gy);
+                    kick32(w, i, dS, du, dv, vx, vy, gx, gy, hdt, hdt, visc);
+                    if (w.kill) {
+                        // killwave (killwave.cu:48-100): relax towards init_C, i.e. residuals towards 0
+                        const float* kw = w.x(X_KILL) + 4 * i;
+#pragma unroll
+                        for (int side = 0; side < 2; ++side) {
+                            const float itau = kw[2 * side + 1];
+                            if (itau > 0.0f) {
+                                const float f = kw[2 * side] * (dtf * itau);
+                                dS -= f * dS;
+                                du -= f * du;
+                                dv -= f * dv;
+                            }
+                        }
+                    }
+                    if (!(w.x(X_SBG)[i] + dS > 0.0f)) atomicOr(&sc->err, 1 << PG_ERR_NAN);
+                    vmax = fmax(vmax, rate64(w, i, j, du, dv));
+                }
+                emit32(w, w.buf[in ^ 1], i, j, dS, du, dv);
+            }
+            __syncthreads();
+        }
+    }
+    if (vk >= 0) block_max_to<STT>(&V[vk].d64.sc->vmax_bits, vmax);
+}
+
+// ================================================================ misc
+// One thread per disk: dt, clock and planet of the step.
+__global__ void k32_time(const View32* __restrict__ V, int nd) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < nd) advance_clock(V[k].d64);
+}
+
+// Per disk (blockIdx.y): the step's planet table (see TRIG_ROW).
+__global__ void k32_trig(const View32* __restrict__ V) {
+    const View32& w = V[blockIdx.y];
+    const Scalars* sc = w.d64.sc;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const pg_body& a = sc->planet_cur;
+    const pg_body& b = sc->planet_next;
+    if (k < w.yarr) {
+        float* t = w.trig + (size_t)TRIG_ROW * k;
+#pragma unroll
+        for (int which = 0; which < 2; ++which) {
+            const pg_body& p = which ? b : a;
+            double s, c;
+            sincos(0.5 * (w.d64.ycj[k] - (p.y + 0.0 * p.vy)), &s, &c);
+            t[3 * which] = (float)(2.0 * s * c);
+            t[3 * which + 1] = (float)(1.0 - 2.0 * s * s);
+            t[3 * which + 2] = (float)(2.0 * s * s);
+        }
+    }
+    if (k < w.xarr) {
+        float* c = w.trig + (size_t)TRIG_ROW * w.yn + 2 * k;
+        c[0] = (float)(w.d64.radx[k] - a.x);
+        c[1] = (float)(w.d64.radx[k] - b.x);
+    }
+    if (k == 0) {
+        float* s = w.trig + (size_t)TRIG_ROW * w.yn + 2 * (size_t)w.xn;
+        s[0] = (float)a.m;
+        s[1] = (float)a.x;
+        s[2] = (float)(a.rs * a.rs);
+        s[3] = (float)(1.0 / a.x / a.x);
+        s[4] = (float)b.m;
+        s[5] = (float)b.x;
+        s[6] = (float)(b.rs * b.rs);
+        s[7] = (float)(1.0 / b.x / b.x);
+    }
+}
+
+// Signal rate of a state just written by set_state (one disk).
+__global__ void k32_cfl(const View32* __restrict__ V, int b) {
+    const View32& w = *V;
+    const float* buf = w.buf[b];
+    const size_t pl = w.plane();
+    const long long n = (long long)w.xres * w.yres;
+    double vmax = 0.0;
+    for (long long m = blockIdx.x * (long long)blockDim.x + threadIdx.x; m < n; m += (long long)gridDim.x * blockDim.x) {
+        const int i = NPAD + (int)(m % w.xres), j = NPAD + (int)(m / w.xres);
+        const size_t c = (size_t)j * w.pitch + i;
+        vmax = fmax(vmax, rate64(w, i, j, buf[pl + c], buf[2 * pl + c]));
+    }
+    block_max_to<256>(&w.d64.sc->vmax_bits, vmax);
+}
+
+// Host state (FP64 interior arrays) -> residual planes with their azimuthal images.
+__global__ void k32_fill(const View32* __restrict__ V, int b, const double* r, const double* u, const double* v) {
+    const View32& w = *V;
+    const long long n = (long long)w.xres * w.yres;
+    for (long long m = blockIdx.x * (long long)blockDim.x + threadIdx.x; m < n; m += (long long)gridDim.x * blockDim.x) {
+        const int i = NPAD + (int)(m % w.xres), j = NPAD + (int)(m / w.xres);
+        const double* I = w.d64.initx + 5 * i;
+        emit32(w, w.buf[b], i, j, (float)(r[m] - I[0]), (float)(u[m] - I[2]), v ? (float)(v[m] - I[3]) : 0.0f);
+    }
+}
+
+__global__ void k32_extract(const View32* __restrict__ V, int b, double* r, double* p, double* u, double* v) {
+    const View32& w = *V;
+    const float* buf = w.buf[b];
+    const size_t pl = w.plane();
+    const long long n = (long long)w.xres * w.yres;
+    for (long long m = blockIdx.x * (long long)blockDim.x + threadIdx.x; m < n; m += (long long)gridDim.x * blockDim.x) {
+        const int i = NPAD + (int)(m % w.xres), j = NPAD + (int)(m / w.xres);
+        const size_t c = (size_t)j * w.pitch + i;
+        const double* I = w.d64.initx + 5 * i;
+        const double rr = I[0] + (double)buf[c];
+        r[m] = rr;
+        p[m] = w.d64.cs2x[i] * rr;
+        u[m] = I[2] + (double)buf[pl + c];
+        v[m] = I[3] + (double)buf[2 * pl + c];
+    }
+}
+
+// Mass and angular momentum, sum Sigma dV and sum Sigma r v dV with dV = xv yv,
+// in FP64 with compensated (Kahan) accumulation per thread, then one partial
+// pair per block, summed on the host in block order (deterministic).
+__global__ void k32_totals(const View32* __restrict__ V, int b, double* part) {
+    const View32& w = *V;
+    const DiskView& d = w.d64;
+    const float* buf = w.buf[b];
+    const size_t pl = w.plane();
+    const long long n = (long long)w.xres * w.yres;
+    double sm = 0.0, cm = 0.0, sl = 0.0, cl = 0.0;
+    for (long long m = blockIdx.x * (long long)blockDim.x + threadIdx.x; m < n; m += (long long)gridDim.x * blockDim.x) {
+        const int i = NPAD + (int)(m % w.xres), j = NPAD + (int)(m / w.xres);
+        const size_t c = (size_t)j * w.pitch + i;
+        const double dV = d.xv[i] * d.yv[j];
+        const double S = d.initx[5 * i] + (double)buf[c];
+        const double vv = d.initx[5 * i + 3] + (double)buf[2 * pl + c];
+        double y = S * dV - cm;
+        double t = sm + y;
+        cm = (t - sm) - y;
+        sm = t;
+        y = S * d.radx[i] * vv * dV - cl;
+        t = sl + y;
+        cl = (t - sl) - y;
+        sl = t;
+    }
+    __shared__ double rm[256], rl[256];
+    rm[threadIdx.x] = sm;
+    rl[threadIdx.x] = sl;
+    __syncthreads();
+    for (int h = 128; h > 0; h >>= 1) {
+        if ((int)threadIdx.x < h) {
+            rm[threadIdx.x] += rm[threadIdx.x + h];
+            rl[threadIdx.x] += rl[threadIdx.x + h];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        part[2 * blockIdx.x] = rm[0];
+        part[2 * blockIdx.x + 1] = rl[0];
+    }
+}
+
+// FP32 tables of one disk from its FP64 tables (slots in pg_f32.cuh).
+__global__ void k32_init_tables(const View32 w, float* tx, float* ty, double* cs64) {
+    const DiskView& d = w.d64;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    auto X = [&](int slot) { return tx + (size_t)slot * w.xn; };
+    auto Y = [&](int slot) { return ty + (size_t)slot * w.yn; };
+    if (k < w.xarr) {
+        const int i = k;
+        const double* I = d.initx + 5 * i;
+        X(X_SBG)[i] = (float)I[0];
+        X(X_PBG)[i] = (float)I[1];
+        X(X_UBG)[i] = (float)I[2];
+        X(X_CS2)[i] = (float)d.cs2x[i];
+        X(X_RAD)[i] = (float)d.radx[i];
+        X(X_IRAD)[i] = (float)d.irad[i];
+        X(X_IDX)[i] = (float)d.idx_x[i];
+        X(X_IXV)[i] = (float)d.ixv[i];
+        X(X_XA)[i] = (float)d.xa[i];
+        if (i == w.xarr - 1) X(X_XA)[i + 1] = (float)d.xa[i + 1];
+        X(X_NU)[i] = (float)d.nux[i];
+        X(X_ABG)[i] = (float)(I[3] * I[3] * d.irad[i] + d.gstar[i]);
+        X(X_V2R)[i] = (float)(2.0 * I[3] * d.irad[i]);
+        X(X_EPS)[i] = (float)(I[3] - d.radx[i] * d.frame_omega - d.rot[i]);
+        const double cs = sqrt(d.gam * d.cs2x[i]);
+        X(X_CS0)[i] = (float)cs;
+        cs64[i] = cs;
+        float* db = X(X_DBG) + 16 * i;
+        const int offs[4] = {-2, -1, 1, 2};
+        for (int kk = 0; kk < 4; ++kk) {
+            const int ik = min(max(i + offs[kk], 0), w.xarr - 1);
+            const double* J = d.initx + 5 * ik;
+            db[kk] = (float)(J[0] - I[0]);
+            db[4 + kk] = (float)(J[1] - I[1]);
+            db[8 + kk] = (float)(J[2] - I[2]);
+            db[12 + kk] = (float)(d.radx[ik] * J[3] - d.radx[i] * I[3]);
+        }
+        for (int m = 0; m < 6; ++m) X(X_WX)[6 * i + m] = (float)d.wx[6 * i + m];
+        for (int m = 0; m < 5; ++m) X(X_VISX)[5 * i + m] = (float)d.visx[5 * i + m];
+        float* vb = X(X_VBG) + 7 * i;
+        for (int m = 0; m < 7; ++m) vb[m] = 0.0f;
+        if (i >= 1 && i + 1 < w.xarr) {
+            // the background's viscous force density, linear in (nr1, dndx, dndy): the
+            // reference's stencil with v_r0, v_phi0 axisymmetric (all d/dphi terms vanish)
+            const double* Xr = d.visx + 5 * i;
+            const double i_r20 = Xr[0], i_r21 = Xr[1], i_r10 = Xr[2], i_hr20 = Xr[3], i_r1 = Xr[4];
+            const double u0 = d.initx[5 * (i - 1) + 2], u1 = I[2], u2 = d.initx[5 * (i + 1) + 2];
+            const double v0 = d.initx[5 * (i - 1) + 3], v1 = I[3], v2 = d.initx[5 * (i + 1) + 3];
+            const double dudx = (u2 - u0) * i_r20;
+            const double d2udx2 = ((u2 - u1) * i_r21 - (u1 - u0) * i_r10) * i_hr20;
+            const double dvdx = (v2 - v0) * i_r20;
+            const double d2vdx2 = ((v2 - v1) * i_r21 - (v1 - v0) * i_r10) * i_hr20;
+            vb[0] = (float)(2.0 * d2udx2 + 2.0 * dudx * i_r1 - 2.0 * u1 * i_r1 * i_r1);
+            vb[1] = (float)(2.0 * dudx);
+            vb[2] = (float)(dvdx - v1 * i_r1);
+            vb[3] = (float)(d2vdx2 - dvdx * i_r1 + v1 * i_r1 * i_r1 + 2.0 * (dvdx - v1 * i_r1) * i_r1);
+            vb[4] = (float)(dvdx - v1 * i_r1);
+            vb[5] = (float)(2.0 * u1 * i_r1);
+            vb[6] = (float)(d.initx[5 * (i + 1)] * d.nux[i + 1] - d.initx[5 * (i - 1)] * d.nux[i - 1]);
+        }
+        const double* kt = d.killx + 4 * i;
+        float* kw = X(X_KILL) + 4 * i;
+        kw[0] = (float)kt[0];
+        kw[1] = kt[1] > 0.0 ? (float)(1.0 / kt[1]) : 0.0f;
+        kw[2] = (float)kt[2];
+        kw[3] = kt[3] > 0.0 ? (float)(1.0 / kt[3]) : 0.0f;
+    }
+    if (k < w.yarr) {
+        Y(Y_IDY)[k] = (float)d.idx_y[k];
+        Y(Y_IYV)[k] = (float)d.iyv[k];
+        for (int m = 0; m < 6; ++m) Y(Y_WY)[6 * k + m] = (float)d.wy[6 * k + m];
+        for (int m = 0; m < 4; ++m) Y(Y_VISY)[4 * k + m] = (float)d.visy[4 * k + m];
+    }
+}
+
+// ============================================================== launchers
+static inline unsigned cdiv(long long a, long long b) { return (unsigned)((a + b - 1) / b); }
+
+static unsigned persistent_grid(const void* kernel, int threads, size_t smem, long long ntiles) {
+    static int nsm = 0;
+    if (nsm == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+        if (nsm <= 0) nsm = 148;
+    }
+    static const void* keys[16] = {nullptr};
+    static int vals[16] = {0};
+    int per_sm = 0;
+    for (int n = 0; n < 16 && keys[n]; ++n)
+        if (keys[n] == kernel) per_sm = vals[n];
+    if (per_sm == 0) {
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem) != cudaSuccess ||
+            per_sm < 1)
+            per_sm = 1;
+        for (int n = 0; n < 16; ++n)
+            if (!keys[n]) {
+                keys[n] = kernel;
+                vals[n] = per_sm;
+                break;
+            }
+    }
+    long long g = (long long)per_sm * nsm;
+    if (g > ntiles) g = ntiles;
+    return (unsigned)(g < 1 ? 1 : g);
+}
+
+cudaError_t set_attributes32() {
+    cudaError_t e = cudaSuccess;
+    auto set = [&](const void* f, size_t bytes) {
+        cudaError_t r = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+        if (r != cudaSuccess) e = r;
+        r = cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+        if (r != cudaSuccess) e = r;
+    };
+    set((const void*)k32_sweep_x, SX_SMEM);
+    set((const void*)k32_sweep_y, SY_SMEM);
+    set((const void*)k32_advect, AD_SMEM);
+    set((const void*)k32_kick1, K1_SMEM);
+    set((const void*)k32_kick2, K2_SMEM);
+    return e;
+}
+
+void launch_time32(const View32* V, int nd, cudaStream_t s) { k32_time<<<cdiv(nd, 64), 64, 0, s>>>(V, nd); }
+void launch_trig32(const View32* V, int nd, int maxn, cudaStream_t s) {
+    k32_trig<<<dim3(cdiv(maxn, 128), nd), 128, 0, s>>>(V);
+}
+void launch_pass32(int pass, const View32* V, const int* first, int nd, const int* ntiles, int in, cudaStream_t s) {
+    switch (pass) {
+        case 0: {
+            const unsigned g = persistent_grid((const void*)k32_kick1, STT, K1_SMEM, ntiles[2]);
+            k32_kick1<<<g, STT, K1_SMEM, s>>>(V, first, nd, ntiles[2], in);
+        } break;
+        case 1: {
+            const unsigned g = persistent_grid((const void*)k32_sweep_x, SWT, SX_SMEM, ntiles[0]);
+            k32_sweep_x<<<g, SWT, SX_SMEM, s>>>(V, first, nd, ntiles[0], in);
+        } break;
+        case 2: {
+            const unsigned g = persistent_grid((const void*)k32_sweep_y, SWT, SY_SMEM, ntiles[1]);
+            k32_sweep_y<<<g, SWT, SY_SMEM, s>>>(V, first, nd, ntiles[1], in);
+        } break;
+        case 3: {
+            const unsigned g = persistent_grid((const void*)k32_advect, SWT, AD_SMEM, ntiles[1]);
+            k32_advect<<<g, SWT, AD_SMEM, s>>>(V, first, nd, ntiles[1], in);
+        } break;
+        default: {
+            const unsigned g = persistent_grid((const void*)k32_kick2, STT, K2_SMEM, ntiles[2]);
+            k32_kick2<<<g, STT, K2_SMEM, s>>>(V, first, nd, ntiles[2], in);
+        } break;
+    }
+}
+void launch_cfl32(const View32* Vk, int b, cudaStream_t s) { k32_cfl<<<592, 256, 0, s>>>(Vk, b); }
+void launch_fill32(const View32* Vk, int b, const double* r, const double* u, const double* v, cudaStream_t s) {
+    k32_fill<<<1184, 256, 0, s>>>(Vk, b, r, u, v);
+}
+void launch_extract32(const View32* Vk, int b, double* r, double* p, double* u, double* v, cudaStream_t s) {
+    k32_extract<<<1184, 256, 0, s>>>(Vk, b, r, p, u, v);
+}
+void launch_totals32(const View32* Vk, int b, double* part, int nblocks, cudaStream_t s) {
+    k32_totals<<<nblocks, 256, 0, s>>>(Vk, b, part);
+}
+void launch_init_tables32(const View32& w, float* tx, float* ty, double* cs64, cudaStream_t s) {
+    const int n = w.xarr > w.yarr ? w.xarr : w.yarr;
+    k32_init_tables<<<cdiv(n, 128), 128, 0, s>>>(w, tx, ty, cs64);
+}
+
+}  // namespace f32
+}  // namespace pg

@@ -35,6 +35,31 @@ void launch_kick2(const DiskView& d, const CellMaps& in, const VisMaps& vis, Cel
 void launch_init_planet(const DiskView& d, const pg_params& P, double t, cudaStream_t s);
 int kernels_per_step(const DiskView& d);
 void set_last_error(const char* msg);
+
+// tables-only disks and FP32 tensor maps for the FP32 form (pg_engine.cu)
+struct Engine;
+pg_status table_engine_create(const pg_params* P, int device, cudaStream_t s, Engine** out);
+void engine_destroy(Engine* E);
+const DiskView& engine_view(const Engine* E);
+void engine_init_planet(Engine* E, double t);
+pg_status make_map3_f32(CUtensorMap* m, const float* base, uint64_t pitch, uint64_t rows, uint64_t planes,
+                        uint32_t bx, uint32_t by, uint32_t bz);
 cudaError_t set_kernel_attributes();
+
+
+namespace f32 {
+struct View32;
+// FP32-form launchers (pg_f32.cu); pass 0 kick1, 1 radial sweep, 2 azimuthal sweep,
+// 3 advection, 4 kick2, reading buffer `in` and writing the other one
+cudaError_t set_attributes32();
+void launch_time32(const View32* V, int nd, cudaStream_t s);
+void launch_trig32(const View32* V, int nd, int maxn, cudaStream_t s);
+void launch_pass32(int pass, const View32* V, const int* first, int nd, const int* ntiles, int in, cudaStream_t s);
+void launch_cfl32(const View32* Vk, int b, cudaStream_t s);
+void launch_fill32(const View32* Vk, int b, const double* r, const double* u, const double* v, cudaStream_t s);
+void launch_extract32(const View32* Vk, int b, double* r, double* p, double* u, double* v, cudaStream_t s);
+void launch_totals32(const View32* Vk, int b, double* part, int nblocks, cudaStream_t s);
+void launch_init_tables32(const View32& w, float* tx, float* ty, double* cs64, cudaStream_t s);
+}  // namespace f32
 
 }  // namespace pg

@@ -20,6 +20,7 @@
 #include "pg_common.cuh"
 #include "pg_hydro.cuh"
 #include "pg_internal.h"
+#include "pg_planet.cuh"
 
 namespace pg {
 
@@ -48,57 +49,6 @@ constexpr int ST_VIS_N = ST_HX * ST_HY * 2;
 constexpr int ST_VIS = (ST_VIS_N + 15) / 16 * 16;
 constexpr size_t K1_SMEM = (size_t)2 * ST_TILE * 8 + 16 + 128;
 constexpr size_t K5_SMEM = (size_t)(3 * ST_TILE + 2 * ST_VIS) * 8 + 16 + 128;
-
-// ------------------------------------------------------------- planet
-__host__ __device__ inline double ramp_function(double t, double tau, double val) {  // planet.cu:7-17
-    if (t < tau) return val * sin(HPI * t / tau);
-    return val;
-}
-__device__ inline double ecc_anomaly(double n, double e, double t) {  // planet.cu:60-103
-    double l = fmod(n * t, TWOPI);
-    double D = -e * sin(l);
-    if (e == 0.0) return l;
-    else if (l == 0.0) return l;
-    else if (l == PI) return l;
-    else if (l == TWOPI) return l;
-    double x, dx, d2x, eps, step, esinu, ecosu;
-    int count = 0;
-    do {
-        sincos(l - D, &esinu, &ecosu);
-        esinu *= e;
-        ecosu *= e;
-        x = D + esinu;
-        dx = 1.0 - ecosu;
-        d2x = -esinu;
-        eps = 2.0 * x * d2x / dx / dx;
-        if (fabs(eps) < 1.0) step = -(x / dx) * (1.0 + eps / 4.0 + eps * eps / 8.0 + 5.0 * eps * eps * eps / 64.0);
-        else step = copysign(fmin(fabs(x / dx), HPI / 2.0), -x);
-        D += step;
-        count++;
-    } while ((fabs(step) > 1.0e-12 || count < 10) && count < 200);
-    return l - D;
-}
-__device__ inline void orbit_solution(const DiskView& d, pg_body& b, double t) {  // planet.cu:105-133
-    const double a = b.a, e = b.e;
-    const double n = sqrt(1.0 / a / a / a);
-    const double efac = sqrt(1.0 - e * e);
-    const double B = e / (1.0 + efac);
-    double u, cosu, sinu;
-    u = ecc_anomaly(n, e, t);
-    sincos(u, &sinu, &cosu);
-    double f, ecosf, esinf;
-    f = u + 2.0 * atan(B * sinu / (1.0 - B * cosu));
-    sincos(f, &esinf, &ecosf);
-    esinf *= e;
-    ecosf *= e;
-    b.m = ramp_function(t, d.ramp_time, d.planet_mass);
-    b.x = a * efac * efac / (1.0 + ecosf);
-    b.y = f - fmod(d.frame_omega * t, TWOPI) + PI;
-    b.z = HPI;
-    b.vx = n * a * esinf / efac;
-    b.vy = n * (1.0 + ecosf) * (1.0 + ecosf) / efac / efac / efac;
-    b.vz = 0.0;
-}
 
 // --------------------------------------------------------- source terms
 struct Grav {
@@ -220,53 +170,6 @@ __device__ __forceinline__ double signal_rate(const DiskView& d, const Cell& c, 
         tmp = fmax(spd * (d.idx_y[j] * ((d.geomy == 3) ? d.irad[i] : 1.0)), tmp);
     }
     return tmp;
-}
-
-template <int NT>
-__device__ __forceinline__ void block_max_to(unsigned long long* dst, double v) {
-    __shared__ double red[NT / 32];
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
-    __syncthreads();
-    if (threadIdx.x < 32) {
-        v = (threadIdx.x < NT / 32) ? red[threadIdx.x] : 0.0;
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
-        if (threadIdx.x == 0) atomic_max_pos(dst, v);
-    }
-}
-
-// Two-stage TMA pipeline of a persistent CTA: tile k computes from stage k&1
-// while tile k+1 streams into the other stage.  Barrier k&1 completes phase
-// (k>>1)&1 when tile k has landed.
-__device__ __forceinline__ void pipe_init(uint64_t* bar) {
-    if (threadIdx.x == 0) {
-        mbar_init(&bar[0], 1);
-        mbar_init(&bar[1], 1);
-        fence_barrier_init();
-    }
-    __syncthreads();
-}
-// thread 0: one box into a stage (the stage's previous generic reads are ordered
-// before the async-proxy write by the fence)
-__device__ __forceinline__ void issue_box(double* dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
-    tma_load_2d(dst, map, x, y, bar);
-}
-__device__ __forceinline__ void issue_begin(uint64_t* bar, uint32_t bytes) {
-    fence_proxy_async();
-    mbar_arrive_expect_tx(bar, bytes);
-}
-// every thread of the CTA gets the same answer, so a timed-out wait makes the
-// whole CTA leave together
-__device__ __forceinline__ bool pipe_wait(uint64_t* bar, int k, Scalars* sc) {
-    const bool ok = mbar_wait(&bar[k & 1], (uint32_t)((k >> 1) & 1), sc);
-    return __syncthreads_and(ok ? 1 : 0) != 0;
-}
-// after a timed-out wait: before the CTA leaves, wait (again bounded) for the
-// copy of tile k+1 if one was issued, so no copy lands in released shared memory
-__device__ __forceinline__ void pipe_drain(uint64_t* bar, int k, bool issued_next, Scalars* sc) {
-    if (threadIdx.x == 0 && issued_next) mbar_wait(&bar[(k + 1) & 1], (uint32_t)(((k + 1) >> 1) & 1), sc);
 }
 
 // ================================================================ sweeps
@@ -838,32 +741,8 @@ __global__ void k_set_time(const DiskView d, double t, double dt) {
     sc->steps += 1;
 }
 
-// Device-resident loop step (main.cu:322-339): dt = min(CFL/vmax, 1.1 dt_prev),
-// clipped at end_time; then the planet at t + dt.
-__global__ void k_time_step(const DiskView d) {
-    Scalars* sc = d.sc;
-    if (sc->done) return;
-    if (sc->pad_) {  // the previous step reached end_time
-        sc->done = 1;
-        return;
-    }
-    const double vmax = __longlong_as_double((long long)sc->vmax_bits);
-    const double dtc = d.cfl / vmax;
-    const double lim = sc->dt_prev * 1.1;
-    double dt = (dtc < lim) ? dtc : lim;
-    const double t = sc->t;
-    if (t + dt > sc->end_time) {
-        dt = sc->end_time - t;
-        sc->pad_ = 1;
-    }
-    sc->dt = dt;
-    sc->planet_cur = sc->planet_next;
-    if (d.nplanet > 0) orbit_solution(d, sc->planet_next, t + dt);
-    sc->t = t + dt;
-    sc->dt_prev = dt;
-    sc->vmax_bits = 0ull;
-    sc->steps += 1;
-}
+// Device-resident loop step of one disk (advance_clock).
+__global__ void k_time_step(const DiskView d) { advance_clock(d); }
 
 __global__ void k_init_planet(const DiskView d, double a, double e, double rs, double t) {
     // init_planet (src/planet/planet.cu:319-402, one planet)

@@ -180,6 +180,25 @@ def reference_disk(nr: int, nphi: int, **kw) -> Params:
     return p.replace(kill_width=p.kill_width_out)
 
 
+def disk_ensemble(n: int = 48, seed: int = 2024) -> list:
+    """Seeded ensemble of planet-disks: Nr uniform over the multiples of 32 in
+    [128, 512], Nphi = 3 Nr, q log-uniform in [1e-5, 3e-3], alpha log-uniform in
+    [1e-4, 1e-2], h/r uniform in [0.03, 0.08]; otherwise as ``planet_disk`` on
+    r in [0.4, 2.5].  Draws come from the SplitMix64 sequence, four per disk."""
+    from .initial import splitmix64_uniform
+
+    u = 0.5 * (splitmix64_uniform(seed, 4 * n).reshape(n, 4) + 1.0)  # U(0, 1)
+    out = []
+    sizes = list(range(128, 513, 32))
+    for a, b, c, d in u:
+        nr = sizes[min(int(a * len(sizes)), len(sizes) - 1)]
+        q = 10.0 ** (math.log10(1.0e-5) + b * (math.log10(3.0e-3) - math.log10(1.0e-5)))
+        alpha = 10.0 ** (-4.0 + c * 2.0)
+        h = 0.03 + d * 0.05
+        out.append(planet_disk(nr, 3 * nr, q=q, alpha=alpha, h=h))
+    return out
+
+
 # ------------------------------------------------------------- host maths
 def make_grid_np(amin: float, amax: float, res: int, pad: int, geom: int, grid: int):
     """Faces and cell 'volumes' with ghosts (src/init/init.cu:472-500).  The C
