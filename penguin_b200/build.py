@@ -23,6 +23,9 @@ SOURCES = ["pg_kernels.cu", "pg_engine.cu", "pg_noalloc.cu", "pg_f32.cu", "pg_en
 HEADERS = ["pg_common.cuh", "pg_hydro.cuh", "pg_internal.h", "pg_planet.cuh", "pg_f32.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I" + INCLUDE]
+# The FP32-mixed kernels take the approximate FP32 division and square root
+# (a few ulp); FP64 arithmetic, the FP64 kernels and denormals are unaffected.
+EXTRA = {"pg_f32.cu": ["-prec-div=false", "-prec-sqrt=false"]}
 
 
 def _nvcc() -> str:
@@ -49,7 +52,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
         o = os.path.join(OBJ, src.replace(".cu", ".o"))
         objs.append(o)
         if force or _stale(o, [s] + hdrs):
-            cmd = [nvcc] + ARCH + FLAGS + ["-c", s, "-o", o]
+            cmd = [nvcc] + ARCH + FLAGS + EXTRA.get(src, []) + ["-c", s, "-o", o]
             if verbose:
                 print(" ".join(cmd), flush=True)
             subprocess.run(cmd, check=True)

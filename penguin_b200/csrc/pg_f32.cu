@@ -59,6 +59,18 @@ __device__ __forceinline__ int find_disk(const int* __restrict__ first, int nd, 
     return lo;
 }
 
+// Planar multi-value tables: value m of slot group `slot` at index i.
+template <int N>
+__device__ __forceinline__ void xload(const View32& w, int slot, int i, float* out) {
+#pragma unroll
+    for (int m = 0; m < N; ++m) out[m] = w.tx[(size_t)(slot + m) * w.xn + i];
+}
+template <int N>
+__device__ __forceinline__ void yload(const View32& w, int slot, int j, float* out) {
+#pragma unroll
+    for (int m = 0; m < N; ++m) out[m] = w.ty[(size_t)(slot + m) * w.yn + j];
+}
+
 // Interior cell (i, j) and its periodic azimuthal image (boundary.cu:141-209).
 __device__ __forceinline__ void emit32(const View32& w, float* out, int i, int j, float a, float b, float c) {
     const size_t pl = w.plane();
@@ -118,9 +130,10 @@ __device__ __forceinline__ void kick32(const View32& w, int i, float dS, float& 
 __device__ __forceinline__ void stress32(const View32& w, const float* tile, int x, int y, int i, int j, float& vx,
                                          float& vy) {
     const float* nu = w.x(X_NU);
-    const float* vb = w.x(X_VBG) + 7 * i;
-    const float* X = w.x(X_VISX) + 5 * i;
-    const float* Y = w.y(Y_VISY) + 4 * j;
+    float vb[7], X[5], Y[4];
+    xload<7>(w, X_VBG, i, vb);
+    xload<5>(w, X_VISX, i, X);
+    yload<4>(w, Y_VISY, j, Y);
     const float* S = tile;
     const float* U = tile + SPL;
     const float* V = tile + 2 * SPL;
@@ -209,7 +222,8 @@ __global__ void __launch_bounds__(SWT) k32_sweep_x(const View32* __restrict__ V,
                     du[m] = r0[XPL + m];
                     dv[m] = r0[2 * XPL + m];
                 }
-                const float* db = w.x(X_DBG) + 16 * sc_;
+                float db[16];
+                xload<16>(w, X_DBG, sc_, db);
                 const float* cs2t = w.x(X_CS2);
                 const float* radt = w.x(X_RAD);
                 const float cs2c = cs2t[sc_], radc = radt[sc_];
@@ -232,7 +246,8 @@ __global__ void __launch_bounds__(SWT) k32_sweep_x(const View32* __restrict__ V,
                 const float uc = w.x(X_UBG)[sc_] + du[2];
                 const float cs0 = sqrtf(gam * pc / Sc);
                 const float flat = flatten32(1.0f / cs0, pc, aP[0], aP[1], aP[3], aP[4], aU[1], aU[3]);
-                const float* wt = w.x(X_WX) + 6 * sc_;
+                float wt[6];
+                xload<6>(w, X_WX, sc_, wt);
                 const Par32 R = recon32(wt, aS[0], aS[1], aS[3], aS[4], flat);
                 const Par32 P = recon32(wt, aP[0], aP[1], aP[3], aP[4], flat);
                 const Par32 U = recon32(wt, aU[0], aU[1], aU[3], aU[4], flat);
@@ -410,7 +425,8 @@ __global__ void __launch_bounds__(SWT) k32_sweep_y(const View32* __restrict__ V,
                 const float un = dv[2] + w.x(X_EPS)[i];
                 // p = cs2 Sigma along the column: pressure ratios are density ratios
                 const float flat = flatten32(1.0f / cs0, Sc, aS[0], aS[1], aS[3], aS[4], aN[1], aN[3]);
-                const float* wt = w.y(Y_WY) + 6 * jc;
+                float wt[6];
+                yload<6>(w, Y_WY, jc, wt);
                 const Par32 R = recon32(wt, aS[0], aS[1], aS[3], aS[4], flat);
                 const Par32 N = recon32(wt, aN[0], aN[1], aN[3], aN[4], flat);
                 const Par32 Tt = recon32(wt, aT[0], aT[1], aT[3], aT[4], flat);
@@ -560,7 +576,8 @@ __global__ void __launch_bounds__(SWT) k32_advect(const View32* __restrict__ V, 
                     du[m] = col[YPL + m * YB_W];
                     dv[m] = col[2 * YPL + m * YB_W];
                 }
-                const float* wt = w.y(Y_WY) + 6 * jc;
+                float wt[6];
+                yload<6>(w, Y_WY, jc, wt);
                 const Par32 R = recon32(wt, dS[0] - dS[2], dS[1] - dS[2], dS[3] - dS[2], dS[4] - dS[2], 0.0f);
                 const Par32 N = recon32(wt, dv[0] - dv[2], dv[1] - dv[2], dv[3] - dv[2], dv[4] - dv[2], 0.0f);
                 const Par32 Tt = recon32(wt, du[0] - du[2], du[1] - du[2], du[3] - du[2], du[4] - du[2], 0.0f);
@@ -775,7 +792,8 @@ __global__ void __launch_bounds__(STT) k32_kick2(const View32* __restrict__ V, c
                     kick32(w, i, dS, du, dv, vx, vy, gx, gy, hdt, hdt, visc);
                     if (w.kill) {
                         // killwave (killwave.cu:48-100): relax towards init_C, i.e. residuals towards 0
-                        const float* kw = w.x(X_KILL) + 4 * i;
+                        float kw[4];
+                        xload<4>(w, X_KILL, i, kw);
 #pragma unroll
                         for (int side = 0; side < 2; ++side) {
                             const float itau = kw[2 * side + 1];
@@ -953,20 +971,19 @@ __global__ void k32_init_tables(const View32 w, float* tx, float* ty, double* cs
         const double cs = sqrt(d.gam * d.cs2x[i]);
         X(X_CS0)[i] = (float)cs;
         cs64[i] = cs;
-        float* db = X(X_DBG) + 16 * i;
+
         const int offs[4] = {-2, -1, 1, 2};
         for (int kk = 0; kk < 4; ++kk) {
             const int ik = min(max(i + offs[kk], 0), w.xarr - 1);
             const double* J = d.initx + 5 * ik;
-            db[kk] = (float)(J[0] - I[0]);
-            db[4 + kk] = (float)(J[1] - I[1]);
-            db[8 + kk] = (float)(J[2] - I[2]);
-            db[12 + kk] = (float)(d.radx[ik] * J[3] - d.radx[i] * I[3]);
+            X(X_DBG + kk)[i] = (float)(J[0] - I[0]);
+            X(X_DBG + 4 + kk)[i] = (float)(J[1] - I[1]);
+            X(X_DBG + 8 + kk)[i] = (float)(J[2] - I[2]);
+            X(X_DBG + 12 + kk)[i] = (float)(d.radx[ik] * J[3] - d.radx[i] * I[3]);
         }
-        for (int m = 0; m < 6; ++m) X(X_WX)[6 * i + m] = (float)d.wx[6 * i + m];
-        for (int m = 0; m < 5; ++m) X(X_VISX)[5 * i + m] = (float)d.visx[5 * i + m];
-        float* vb = X(X_VBG) + 7 * i;
-        for (int m = 0; m < 7; ++m) vb[m] = 0.0f;
+        for (int m = 0; m < 6; ++m) X(X_WX + m)[i] = (float)d.wx[6 * i + m];
+        for (int m = 0; m < 5; ++m) X(X_VISX + m)[i] = (float)d.visx[5 * i + m];
+        float vb[7] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
         if (i >= 1 && i + 1 < w.xarr) {
             // the background's viscous force density, linear in (nr1, dndx, dndy): the
             // reference's stencil with v_r0, v_phi0 axisymmetric (all d/dphi terms vanish)
@@ -986,18 +1003,18 @@ __global__ void k32_init_tables(const View32 w, float* tx, float* ty, double* cs
             vb[5] = (float)(2.0 * u1 * i_r1);
             vb[6] = (float)(d.initx[5 * (i + 1)] * d.nux[i + 1] - d.initx[5 * (i - 1)] * d.nux[i - 1]);
         }
+        for (int m = 0; m < 7; ++m) X(X_VBG + m)[i] = vb[m];
         const double* kt = d.killx + 4 * i;
-        float* kw = X(X_KILL) + 4 * i;
-        kw[0] = (float)kt[0];
-        kw[1] = kt[1] > 0.0 ? (float)(1.0 / kt[1]) : 0.0f;
-        kw[2] = (float)kt[2];
-        kw[3] = kt[3] > 0.0 ? (float)(1.0 / kt[3]) : 0.0f;
+        X(X_KILL + 0)[i] = (float)kt[0];
+        X(X_KILL + 1)[i] = kt[1] > 0.0 ? (float)(1.0 / kt[1]) : 0.0f;
+        X(X_KILL + 2)[i] = (float)kt[2];
+        X(X_KILL + 3)[i] = kt[3] > 0.0 ? (float)(1.0 / kt[3]) : 0.0f;
     }
     if (k < w.yarr) {
         Y(Y_IDY)[k] = (float)d.idx_y[k];
         Y(Y_IYV)[k] = (float)d.iyv[k];
-        for (int m = 0; m < 6; ++m) Y(Y_WY)[6 * k + m] = (float)d.wy[6 * k + m];
-        for (int m = 0; m < 4; ++m) Y(Y_VISY)[4 * k + m] = (float)d.visy[4 * k + m];
+        for (int m = 0; m < 6; ++m) Y(Y_WY + m)[k] = (float)d.wy[6 * k + m];
+        for (int m = 0; m < 4; ++m) Y(Y_VISY + m)[k] = (float)d.visy[4 * k + m];
     }
 }
 

@@ -28,8 +28,9 @@ namespace f32 {
 
 constexpr int NPL = 3;  // planes: dS, du, dv
 
-// Per-radius FP32 tables, each slot xn = xarr + 1 floats; multi-value slots are
-// interleaved per index (slot base + width * i).
+// Per-radius FP32 tables, each slot xn = xarr + 1 floats; a table with several
+// values per index takes consecutive slots (slot + m), so that threads of
+// neighbouring radii read neighbouring words.
 enum XSlot {
     X_SBG = 0,    // Sigma_0
     X_PBG = 1,    // p_0 = cs2 Sigma_0
