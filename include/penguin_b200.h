@@ -158,6 +158,11 @@ pg_status pg_disk_clock(pg_disk* d, double* t, double* dt, long long* steps);
 pg_status pg_disk_planet(pg_disk* d, pg_body* out);
 /* Device error word: 0 or a pg_status; cleared by the call (syncs). */
 pg_status pg_disk_check(pg_disk* d);
+/* Torque of the planet on the disk, sum of r g_phi Sigma dV over the interior
+   with the current planet (src/output/output.cu:336-412, global_sum; main.cu
+   prints it divided by q^2/h^2).  2D polar disks with a planet; FP64 with
+   compensated per-thread sums; syncs. */
+pg_status pg_disk_torque(pg_disk* d, double* torque);
 /* Launch count of the library's own kernels per step (for reporting). */
 int pg_kernels_per_step(const pg_disk* d);
 /* Runs nsteps of the device-resident loop launching the kernels one by one with
@@ -199,6 +204,8 @@ pg_status pg_ens_check(pg_ens* e);
 /* Disk k's mass sum(Sigma dV) and angular momentum sum(Sigma r v dV), FP64
    with compensated summation (syncs). */
 pg_status pg_ens_totals(pg_ens* e, int k, double* mass, double* angmom);
+/* Disk k's torque of the planet on the disk, as pg_disk_torque (syncs). */
+pg_status pg_ens_torque(pg_ens* e, int k, double* torque);
 int pg_ens_kernels_per_step(const pg_ens* e);
 /* As pg_disk_profile, for the whole ensemble (slots 0 clocks + planet tables,
    1 kick1, 2 sweep_x, 3 sweep_y, 4 advect, 5 kick2). */

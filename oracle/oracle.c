@@ -1130,6 +1130,36 @@ double orc_global_dt(orc_state* S, double dt_prev)
     return (dt < lim) ? dt : lim;
 }
 
+/* ---------------------------------------------------------------- torque */
+/* Torque of the planet on the disk, sum over cells of r g_phi Sigma dV (2D polar
+ * disk): cal_torque + get_sum_lv1 (src/output/output.cu:336-412) with g_phi of
+ * o_star_planet_grav_cyl at z = 0 (src/output/forces.cu:39-57) for the current
+ * planet; dV = (xa[i+1]^2 - xa[i]^2)/2 (ya[j+1] - ya[j]).  Summed in a fixed
+ * order with compensation (the reference sums in its block order). */
+double orc_torque(const orc_state* S)
+{
+    const orc_params* P = &S->P;
+    if (P->ndim != 2 || P->geomy != 3 || P->n_planet < 1) return 0.0;
+    const orc_body* p = &S->planet;
+    double sum = 0.0, comp = 0.0;
+    for (int j = S->ypad; j < S->ypad + P->yres; j++) {
+        const double azi = 0.5 * (S->ya[j + 1] + S->ya[j]);
+        const double sinfac = sin(azi - p->y), cosfac = cos(azi - p->y);
+        for (int i = NPAD; i < NPAD + P->xres; i++) {
+            const double rad = 0.5 * (S->xa[i + 1] + S->xa[i]);
+            const double Rp = sqrt(rad * rad + p->x * p->x - 2.0 * p->x * rad * cosfac + p->rs * p->rs);
+            const double rs_fac = 1.0 / Rp / Rp / Rp;
+            const double gy = -p->m * p->x * sinfac * rs_fac + p->m * sinfac / p->x / p->x;
+            const double dv = 0.5 * (S->xa[i + 1] * S->xa[i + 1] - S->xa[i] * S->xa[i]) * (S->ya[j + 1] - S->ya[j]);
+            const double y = rad * gy * (S->C[IND(S, i, j)].r * dv) - comp;
+            const double t = sum + y;
+            comp = (t - sum) - y;
+            sum = t;
+        }
+    }
+    return sum;
+}
+
 /* ------------------------------------------------------------- the step */
 /* src/solver/solve.cu:212-292 */
 void orc_solve(orc_state* S, double t, double dt)

@@ -76,6 +76,7 @@ void orc_init_orbadv(orc_state* S);             /* src/orbit/orbit.cu:51,111 */
 void orc_get_planet(const orc_state* S, orc_body* out);
 
 double orc_global_dt(orc_state* S, double dt_prev);  /* src/timestep/timestep.cu:113 */
+double orc_torque(const orc_state* S);                /* src/output/output.cu:336-412 */
 void orc_solve(orc_state* S, double t, double dt);   /* src/solver/solve.cu:279 */
 
 /* main.cu:320-360 with max_step and end_time: returns steps taken, writes final time and last dt */

@@ -83,6 +83,8 @@ def lib():
         L.orc_get_planet.argtypes = [vp, ctypes.POINTER(OrcBody)]
         L.orc_global_dt.restype = ctypes.c_double
         L.orc_global_dt.argtypes = [vp, ctypes.c_double]
+        L.orc_torque.restype = ctypes.c_double
+        L.orc_torque.argtypes = [vp]
         L.orc_solve.argtypes = [vp, ctypes.c_double, ctypes.c_double]
         L.orc_run.restype = ctypes.c_int
         L.orc_run.argtypes = [vp, ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_double, dp, dp]
@@ -154,6 +156,10 @@ class Oracle:
 
     def global_dt(self, dt_prev: float) -> float:
         return lib().orc_global_dt(self.h, dt_prev)
+
+    def torque(self) -> float:
+        """Torque of the planet on the disk (src/output/output.cu:336-412), unnormalised."""
+        return lib().orc_torque(self.h)
 
     def solve(self, t: float, dt: float) -> None:
         lib().orc_solve(self.h, t, dt)

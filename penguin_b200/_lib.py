@@ -23,10 +23,10 @@ EXPORTS = [
     "pg_global_dt_noalloc",
     "pg_disk_create", "pg_disk_destroy", "pg_disk_dims", "pg_disk_set_state", "pg_disk_get_state",
     "pg_disk_state_ptr", "pg_disk_global_dt", "pg_disk_solve", "pg_disk_run", "pg_disk_sync", "pg_disk_clock",
-    "pg_disk_planet", "pg_disk_check", "pg_kernels_per_step", "pg_disk_profile",
+    "pg_disk_planet", "pg_disk_check", "pg_disk_torque", "pg_kernels_per_step", "pg_disk_profile",
     "pg_ens_check_params", "pg_ens_create", "pg_ens_destroy", "pg_ens_size", "pg_ens_dims", "pg_ens_set_state",
     "pg_ens_get_state", "pg_ens_run", "pg_ens_sync", "pg_ens_clock", "pg_ens_planet", "pg_ens_check",
-    "pg_ens_totals", "pg_ens_kernels_per_step", "pg_ens_profile",
+    "pg_ens_totals", "pg_ens_torque", "pg_ens_kernels_per_step", "pg_ens_profile",
 ]
 
 
@@ -77,6 +77,7 @@ def lib() -> ctypes.CDLL:
         "pg_disk_clock": (i, [vp, dp, dp, ctypes.POINTER(ctypes.c_longlong)]),
         "pg_disk_planet": (i, [vp, ctypes.POINTER(PGBody)]),
         "pg_disk_check": (i, [vp]),
+        "pg_disk_torque": (i, [vp, dp]),
         "pg_kernels_per_step": (i, [vp]),
         "pg_disk_profile": (i, [vp, i, d, ctypes.POINTER(ctypes.c_float), i]),
         "pg_ens_check_params": (i, [PP, i]),
@@ -92,6 +93,7 @@ def lib() -> ctypes.CDLL:
         "pg_ens_planet": (i, [vp, i, ctypes.POINTER(PGBody)]),
         "pg_ens_check": (i, [vp]),
         "pg_ens_totals": (i, [vp, i, dp, dp]),
+        "pg_ens_torque": (i, [vp, i, dp]),
         "pg_ens_kernels_per_step": (i, [vp]),
         "pg_ens_profile": (i, [vp, i, d, ctypes.POINTER(ctypes.c_float), i]),
     }

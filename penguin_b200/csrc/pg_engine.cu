@@ -28,6 +28,17 @@ static pg_status fail(pg_status s, const char* fmt, ...) {
 
 void set_last_error(const char* msg) { g_err = msg; }
 
+double compensated_sum(const double* a, int n) {
+    double sum = 0.0, comp = 0.0;
+    for (int k = 0; k < n; ++k) {
+        const double y = a[k] - comp;
+        const double t = sum + y;
+        comp = (t - sum) - y;
+        sum = t;
+    }
+    return sum;
+}
+
 #define PG_CUDA(call)                                                                          \
     do {                                                                                       \
         cudaError_t e_ = (call);                                                               \
@@ -254,6 +265,7 @@ struct Engine {
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     std::vector<const void*> ghosted;  // buffers whose constant radial ghosts are initialised
     pg_body* grid_planet = nullptr;    // drop-in mode: the caller's planets array
+    double* part = nullptr;            // per-block partial sums of diagnostics
 
     ~Engine() {
         for (auto& g : graph)
@@ -270,6 +282,7 @@ struct Engine {
         }
         cudaFree(grid);
         cudaFree(tab);
+        cudaFree(part);
         cudaFree(sc);
         if (own_stream && stream) cudaStreamDestroy(stream);
     }
@@ -806,6 +819,26 @@ pg_status pg_disk_check(pg_disk* dk) {
     PG_CUDA(cudaMemcpy(&dk->E->sc->err, &zero, sizeof(int), cudaMemcpyHostToDevice));
     if (err & (1 << PG_ERR_TIMEOUT)) return fail(PG_ERR_TIMEOUT, "a device wait timed out");
     if (err & (1 << PG_ERR_NAN)) return fail(PG_ERR_NAN, "non-positive or NaN density produced");
+    return PG_OK;
+}
+
+pg_status pg_disk_torque(pg_disk* dk, double* torque) {
+    if (!dk || !torque) return fail(PG_ERR_ARG, "null argument");
+    Engine& E = *dk->E;
+    const DiskView& d = E.view;
+    if (d.ndim != 2 || d.geomy != 3 || d.nplanet < 1)
+        return fail(PG_ERR_CONFIG, "pg_disk_torque: needs a 2D polar disk with a planet");
+    PG_CUDA(cudaSetDevice(E.device));
+    pg_status s0 = resolve_cur(E);
+    if (s0 != PG_OK) return s0;
+    constexpr int nb = 296;
+    if (!E.part) PG_CUDA(cudaMalloc(&E.part, nb * sizeof(double)));
+    launch_torque(d, E.buf[E.cur], E.part, nb, E.stream);
+    PG_CUDA(cudaGetLastError());
+    double h[nb];
+    PG_CUDA(cudaMemcpyAsync(h, E.part, sizeof h, cudaMemcpyDeviceToHost, E.stream));
+    PG_CUDA(cudaStreamSynchronize(E.stream));
+    *torque = compensated_sum(h, nb);
     return PG_OK;
 }
 

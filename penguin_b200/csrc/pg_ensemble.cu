@@ -440,6 +440,20 @@ pg_status pg_ens_totals(pg_ens* e, int k, double* mass, double* angmom) {
     return PG_OK;
 }
 
+pg_status pg_ens_torque(pg_ens* e, int k, double* torque) {
+    pg_status s = check_index(e, k);
+    if (s != PG_OK) return s;
+    if (!torque) return ens_fail(PG_ERR_ARG, "null out");
+    ENS_CUDA(cudaSetDevice(e->device));
+    launch_torque32(e->dV + k, e->cur, e->dPart, kTotalsBlocks, e->stream);
+    ENS_CUDA(cudaGetLastError());
+    std::vector<double> part(kTotalsBlocks);
+    ENS_CUDA(cudaMemcpyAsync(part.data(), e->dPart, sizeof(double) * part.size(), cudaMemcpyDeviceToHost, e->stream));
+    ENS_CUDA(cudaStreamSynchronize(e->stream));
+    *torque = compensated_sum(part.data(), kTotalsBlocks);
+    return PG_OK;
+}
+
 int pg_ens_kernels_per_step(const pg_ens* e) { return e ? 2 + kPasses : 0; }
 
 pg_status pg_ens_profile(pg_ens* e, int nsteps, double end_time, float* ms, int nslot) {

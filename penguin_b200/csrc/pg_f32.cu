@@ -945,6 +945,40 @@ __global__ void k32_totals(const View32* __restrict__ V, int b, double* part) {
     }
 }
 
+// Torque of the planet on the disk, as k_torque of the FP64 kernels
+// (src/output/output.cu:336-412), in FP64 from the residual state.
+__global__ void k32_torque(const View32* __restrict__ V, int b, double* part) {
+    const View32& w = *V;
+    const DiskView& d = w.d64;
+    const pg_body p = d.sc->planet_next;
+    const float* buf = w.buf[b];
+    const long long n = (long long)w.xres * w.yres;
+    double sum = 0.0, comp = 0.0;
+    for (long long m = blockIdx.x * (long long)blockDim.x + threadIdx.x; m < n; m += (long long)gridDim.x * blockDim.x) {
+        const int i = NPAD + (int)(m % w.xres), j = NPAD + (int)(m / w.xres);
+        const double rad = d.radx[i];
+        double sinfac, cosfac;
+        sincos(d.ycraw[j] - p.y, &sinfac, &cosfac);
+        const double Rp = sqrt(rad * rad + p.x * p.x - 2.0 * p.x * rad * cosfac + p.rs * p.rs);
+        const double rs_fac = 1.0 / Rp / Rp / Rp;
+        const double gy = -p.m * p.x * sinfac * rs_fac + p.m * sinfac / p.x / p.x;
+        const double dv = 0.5 * (d.xa[i + 1] * d.xa[i + 1] - d.xa[i] * d.xa[i]) * (d.ya[j + 1] - d.ya[j]);
+        const double S = d.initx[5 * i] + (double)buf[(size_t)j * w.pitch + i];
+        const double y = rad * gy * (S * dv) - comp;
+        const double t = sum + y;
+        comp = (t - sum) - y;
+        sum = t;
+    }
+    __shared__ double red[256];
+    red[threadIdx.x] = sum;
+    __syncthreads();
+    for (int h = 128; h > 0; h >>= 1) {
+        if ((int)threadIdx.x < h) red[threadIdx.x] += red[threadIdx.x + h];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) part[blockIdx.x] = red[0];
+}
+
 // FP32 tables of one disk from its FP64 tables (slots in pg_f32.cuh).
 __global__ void k32_init_tables(const View32 w, float* tx, float* ty, double* cs64) {
     const DiskView& d = w.d64;
@@ -1103,6 +1137,9 @@ void launch_extract32(const View32* Vk, int b, double* r, double* p, double* u, 
 }
 void launch_totals32(const View32* Vk, int b, double* part, int nblocks, cudaStream_t s) {
     k32_totals<<<nblocks, 256, 0, s>>>(Vk, b, part);
+}
+void launch_torque32(const View32* Vk, int b, double* part, int nblocks, cudaStream_t s) {
+    k32_torque<<<nblocks, 256, 0, s>>>(Vk, b, part);
 }
 void launch_init_tables32(const View32& w, float* tx, float* ty, double* cs64, cudaStream_t s) {
     const int n = w.xarr > w.yarr ? w.xarr : w.yarr;

@@ -33,6 +33,9 @@ void launch_sweep_y(const DiskView& d, const CellMaps& in, Cell* out, cudaStream
 void launch_advect(const DiskView& d, const CellMaps& in, Cell* out, cudaStream_t s);
 void launch_kick2(const DiskView& d, const CellMaps& in, const VisMaps& vis, Cell* out, cudaStream_t s);
 void launch_init_planet(const DiskView& d, const pg_params& P, double t, cudaStream_t s);
+void launch_torque(const DiskView& d, const Cell* buf, double* part, int nblocks, cudaStream_t s);
+// compensated sum of n doubles in index order
+double compensated_sum(const double* a, int n);
 int kernels_per_step(const DiskView& d);
 void set_last_error(const char* msg);
 
@@ -59,6 +62,7 @@ void launch_cfl32(const View32* Vk, int b, cudaStream_t s);
 void launch_fill32(const View32* Vk, int b, const double* r, const double* u, const double* v, cudaStream_t s);
 void launch_extract32(const View32* Vk, int b, double* r, double* p, double* u, double* v, cudaStream_t s);
 void launch_totals32(const View32* Vk, int b, double* part, int nblocks, cudaStream_t s);
+void launch_torque32(const View32* Vk, int b, double* part, int nblocks, cudaStream_t s);
 void launch_init_tables32(const View32& w, float* tx, float* ty, double* cs64, cudaStream_t s);
 }  // namespace f32
 

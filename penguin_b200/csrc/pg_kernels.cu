@@ -935,6 +935,37 @@ __global__ void k_bound_x(const DiskView d, Cell* buf) {
     }
 }
 
+// Torque of the planet on the disk (src/output/output.cu:336-412 with g_phi of
+// src/output/forces.cu:39-57 at z = 0, 2D polar): one compensated partial sum of
+// r g_phi Sigma dV per thread, summed per block, dV = (xa[i+1]^2 - xa[i]^2)/2 (ya[j+1] - ya[j]).
+__global__ void k_torque(const DiskView d, const Cell* __restrict__ buf, double* part) {
+    const pg_body p = d.sc->planet_next;
+    const long long n = (long long)d.xres * d.yres;
+    double sum = 0.0, comp = 0.0;
+    for (long long m = blockIdx.x * (long long)blockDim.x + threadIdx.x; m < n; m += (long long)gridDim.x * blockDim.x) {
+        const int i = NPAD + (int)(m % d.xres), j = d.ypad + (int)(m / d.xres);
+        const double rad = d.radx[i];
+        double sinfac, cosfac;
+        sincos(d.ycraw[j] - p.y, &sinfac, &cosfac);
+        const double Rp = sqrt(rad * rad + p.x * p.x - 2.0 * p.x * rad * cosfac + p.rs * p.rs);
+        const double rs_fac = 1.0 / Rp / Rp / Rp;
+        const double gy = -p.m * p.x * sinfac * rs_fac + p.m * sinfac / p.x / p.x;
+        const double dv = 0.5 * (d.xa[i + 1] * d.xa[i + 1] - d.xa[i] * d.xa[i]) * (d.ya[j + 1] - d.ya[j]);
+        const double y = rad * gy * (load_cell(buf, d.xarr, i, j).r * dv) - comp;
+        const double t = sum + y;
+        comp = (t - sum) - y;
+        sum = t;
+    }
+    __shared__ double red[256];
+    red[threadIdx.x] = sum;
+    __syncthreads();
+    for (int h = 128; h > 0; h >>= 1) {
+        if ((int)threadIdx.x < h) red[threadIdx.x] += red[threadIdx.x + h];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) part[blockIdx.x] = red[0];
+}
+
 // ============================================================== launchers
 static inline unsigned cdiv(long long a, long long b) { return (unsigned)((a + b - 1) / b); }
 
@@ -973,6 +1004,10 @@ void launch_init_tables(const DiskView& d, const pg_params& P, double* tab, cuda
     const int n = d.xarr > d.yarr ? d.xarr : d.yarr;
     k_init_tables<<<cdiv(n, 128), 128, 0, s>>>(d, a, radx, cs2x, nux, initx, killx, const_cast<double*>(d.rot),
                                                 ycraw, ycj, xrec, yrec);
+}
+
+void launch_torque(const DiskView& d, const Cell* buf, double* part, int nblocks, cudaStream_t s) {
+    k_torque<<<nblocks, 256, 0, s>>>(d, buf, part);
 }
 
 void launch_init_xghosts(const DiskView& d, Cell* buf, cudaStream_t s) {

@@ -107,6 +107,12 @@ class Disk:
     def check(self) -> None:
         check(lib().pg_disk_check(self._h))
 
+    def torque(self) -> float:
+        """Torque of the planet on the disk (unnormalised; the reference prints it / (q^2/h^2))."""
+        out = ctypes.c_double()
+        check(lib().pg_disk_torque(self._h, ctypes.byref(out)))
+        return out.value
+
     STAGES = ("time", "kick1", "sweep_x", "sweep_y", "advect", "kick2")
 
     def profile(self, nsteps: int, end_time: float = 1.0e30) -> dict:

@@ -83,6 +83,12 @@ class Ensemble:
         check(lib().pg_ens_totals(self._h, k, ctypes.byref(m), ctypes.byref(l)))
         return m.value, l.value
 
+    def torque(self, k: int) -> float:
+        """Torque of the planet on member k (unnormalised, as Disk.torque)."""
+        out = ctypes.c_double()
+        check(lib().pg_ens_torque(self._h, k, ctypes.byref(out)))
+        return out.value
+
     def profile(self, nsteps: int, end_time: float = 1.0e30) -> dict:
         ms = (ctypes.c_float * 6)()
         check(lib().pg_ens_profile(self._h, nsteps, end_time, ms, 6))

@@ -178,3 +178,18 @@ def test_f32_nan_sets_error_word():
     with pytest.raises(PGError) as ei:
         e.check()
     assert ei.value.status == PG_ERR_NAN
+
+
+def test_f32_torque_tracks_fp64():
+    p = P.planet_disk(128, 384)
+    st = I.disk_state(p, seed=4)
+    d = Disk(p)
+    d.set_state(C.T0_DISK, st)
+    d.run(20)
+    d.sync()
+    e = Ensemble([p])
+    e.set_state(0, C.T0_DISK, st)
+    e.run(20)
+    e.sync()
+    # the torque is dominated by the near-planet density, FP32-accurate to ~1e-6 here
+    assert e.torque(0) == pytest.approx(d.torque(), rel=1e-4)

@@ -194,3 +194,18 @@ def test_drop_in_grid_entry_points_match_handle_api():
     assert loop.t == d.t
     for k in _keys(p):
         assert np.array_equal(g[k], h[k]), k
+
+
+def test_torque_matches_oracle():
+    """Torque of the planet on the disk (src/output/output.cu:336-412) after 10 steps."""
+    case = [c for c in C.cases() if c["name"] == "disk64_n10"][0]
+    p = case["params"]
+    st = C.initial_state(case)
+    o = Oracle(p, st, case["t0"])
+    o.run(10)
+    d = Disk(p)
+    d.set_state(case["t0"], st)
+    d.step_host(10)
+    d.check()
+    # the state after 10 steps agrees to ~1e-12 (disk64_n10) and the sum is compensated
+    assert d.torque() == pytest.approx(o.torque(), rel=1e-9)
