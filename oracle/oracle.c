@@ -23,6 +23,7 @@ struct orc_state {
     int xarr, yarr, ypad;
     double *xa, *xv, *ya, *yv, *za, *zv;
     orc_cell *C, *T;
+    orc_dust *CD, *TD;   /* dust_flag only */
     double *vis;
     double *orb_rot, *orb_res;
     int *orb_inc;
@@ -113,6 +114,26 @@ static orc_cell init_C(const orc_params* P, double x, double y, double z)
 }
 static double init_v(const orc_params* P, double x) { return init_C(P, x, 0.0, 0.0).v; }
 
+/* init_CD (src/init/init.cu:351-454, init_flag 2, 2D: get_vertical = 1): dust density
+   D_G_ratio Sigma_0, Keplerian azimuthal velocity and the radial drift solution */
+static orc_dust init_CD(const orc_params* P, double x)
+{
+    orc_dust Q;
+    Q.r = P->d_g_ratio * pow(x / P->planet_radius, -P->p_alpha);
+    double f_gas = init_v(P, x) / sqrt(1.0 / x);
+    double tmp = P->stokes * P->stokes * f_gas;
+    double L = ((1.0 + tmp) / tmp) * (1.0 - sqrt(1.0 - 2.0 * tmp * (1.0 - f_gas) / (1.0 + tmp) / (1.0 + tmp)));
+    double u0 = P->stokes * (L * L - 2.0 * L);
+    double u = (1.0 - sqrt(1.0 - 2.0 * P->stokes * u0)) / P->stokes;
+    L = (1.0 - f_gas + P->stokes * u / 2.0) / (1.0 + P->stokes * u / 2.0);
+    u0 = P->stokes * (L * L - 2.0 * L);
+    u = (1.0 - sqrt(1.0 - 2.0 * P->stokes * u0)) / P->stokes;
+    Q.u = u * sqrt(1.0 / x);
+    Q.v = sqrt(1.0 / x);
+    Q.w = 0.0;
+    return Q;
+}
+
 /* src/EOS/EOS.cu:4-18 */
 static double get_energy(const orc_params* P, double r, double p, double u, double v, double w)
 {
@@ -150,6 +171,10 @@ orc_state* orc_create(const orc_params* P)
     S->C = (orc_cell*)calloc(n, sizeof(orc_cell));
     S->T = (orc_cell*)calloc(n, sizeof(orc_cell));
     S->vis = (double*)calloc(2 * n, sizeof(double));
+    if (P->dust_flag) {
+        S->CD = (orc_dust*)calloc(n, sizeof(orc_dust));
+        S->TD = (orc_dust*)calloc(n, sizeof(orc_dust));
+    }
     S->orb_rot = (double*)calloc(S->xarr, sizeof(double));
     S->orb_res = (double*)calloc(S->xarr, sizeof(double));
     S->orb_inc = (int*)calloc(S->xarr, sizeof(int));
@@ -160,7 +185,7 @@ void orc_destroy(orc_state* S)
 {
     if (!S) return;
     free(S->xa); free(S->xv); free(S->ya); free(S->yv); free(S->za); free(S->zv);
-    free(S->C); free(S->T); free(S->vis);
+    free(S->C); free(S->T); free(S->vis); free(S->CD); free(S->TD);
     free(S->orb_rot); free(S->orb_res); free(S->orb_inc);
     free(S);
 }
@@ -186,6 +211,37 @@ void orc_fill_init(orc_state* S)
     double zc = 0.5 * (S->za[1] + S->za[0]);
     for (int j = 0; j < S->yarr; j++)
         for (int i = 0; i < S->xarr; i++) S->C[IND(S, i, j)] = init_C(&S->P, xc(S, i), yc(S, j), zc);
+    if (S->P.dust_flag)
+        for (int j = 0; j < S->yarr; j++)
+            for (int i = 0; i < S->xarr; i++) S->CD[IND(S, i, j)] = init_CD(&S->P, xc(S, i));
+}
+
+void orc_set_dust(orc_state* S, const double* r, const double* u, const double* v)
+{
+    if (!S->CD) return;
+    int nx = S->P.xres, ny = S->P.yres;
+    for (int j = 0; j < ny; j++)
+        for (int i = 0; i < nx; i++) {
+            orc_dust* d = &S->CD[IND(S, i + NPAD, j + S->ypad)];
+            size_t k = (size_t)i + (size_t)nx * j;
+            d->r = r[k];
+            d->u = u[k];
+            d->v = v[k];
+        }
+}
+
+void orc_get_dust(const orc_state* S, double* r, double* u, double* v)
+{
+    if (!S->CD) return;
+    int nx = S->P.xres, ny = S->P.yres;
+    for (int j = 0; j < ny; j++)
+        for (int i = 0; i < nx; i++) {
+            const orc_dust* d = &S->CD[IND(S, i + NPAD, j + S->ypad)];
+            size_t k = (size_t)i + (size_t)nx * j;
+            r[k] = d->r;
+            u[k] = d->u;
+            v[k] = d->v;
+        }
 }
 
 /* src/output/output.cu:182-248 (only the interior is loaded) */
@@ -329,6 +385,38 @@ void orc_boundy(orc_state* S, int which)
         for (int n = 0; n < yp; n++) {
             C[IND(S, i, n)] = C[IND(S, i, yres + n)];
             C[IND(S, i, yres + yp + n)] = C[IND(S, i, yp + n)];
+        }
+}
+
+/* boundx_dust (src/boundary/boundary.cu:64-113, 592-704 with one device) */
+static void boundx_dust(orc_state* S)
+{
+    const orc_params* P = &S->P;
+    int nx = P->xres + NPAD;
+    for (int j = 0; j < S->yarr; j++) {
+        orc_dust* D = &S->CD[S->xarr * j];
+        for (int n = 0; n < NPAD; n++) {
+            if (P->bound_lft == 2) { D[n] = D[2 * NPAD - 1 - n]; D[n].u *= -1.0; }
+            else if (P->bound_lft == 1) D[n] = D[NPAD];
+            else D[n] = init_CD(P, xc(S, n));
+        }
+        for (int n = 0; n < NPAD; n++) {
+            if (P->bound_rgh == 2) { D[nx + n] = D[nx - 1 - n]; D[nx + n].u *= -1.0; }
+            else if (P->bound_rgh == 1) D[nx + n] = D[nx - 1];
+            else D[nx + n] = init_CD(P, xc(S, nx + n));
+        }
+    }
+}
+
+/* boundy_dust (src/boundary/boundary.cu:211-268, periodic) */
+static void boundy_dust(orc_state* S)
+{
+    if (S->P.ndim < 2) return;
+    int yres = S->P.yres, yp = S->ypad;
+    for (int i = 0; i < S->xarr; i++)
+        for (int n = 0; n < yp; n++) {
+            S->CD[IND(S, i, n)] = S->CD[IND(S, i, yres + n)];
+            S->CD[IND(S, i, yres + yp + n)] = S->CD[IND(S, i, yp + n)];
         }
 }
 
@@ -817,6 +905,238 @@ void orc_sweepy(orc_state* S, double dt)
     orc_cell* t = S->C; S->C = S->T; S->T = t;
 }
 
+/* ----------------------------------------------------------------- dust */
+/* dust_flux (src/solver/dust/dust.cu:6-103): upwind PPM fluxes at the left face of
+   cell i.  The reference reads the flattening coefficient of recon_flag 6 from
+   shared memory that dust_flow never writes (src/solver/recon/PPM.cu:68-77 vs
+   dust.cu:110-117); here it is 0, the value zero-initialised memory gives. */
+static void dust_flux(int i, int geom, const double* xa, const double* r, const double* u, const double* v,
+                      const double* w, const double* flat, double dt, double us, orc_dust* F)
+{
+    double r_par[3], u_par[3];
+    double xl = xa[i], xr = xa[i + 1], tmp, q, ur, ul, u_, r0, u0;
+    double Srr, Sur, Svr, Swr, Srl, Sul, Svl, Swl;
+    get_params(i, geom, xa, u, flat, u_par);
+    tmp = xl - fmin(u_par[1] - u_par[0], 0.0) * dt;
+    q = dimensionless_x(xl, tmp, xr);
+    ur = ppm_aveL(q, u_par);
+    u_ = 0.5 * dt * (ur - u[i]) / (0.5 * (xr - tmp));
+    tmp = xl - fmin(ur, 0.0) * dt;
+    q = dimensionless_x(xl, tmp, xr);
+    get_params(i, geom, xa, r, flat, r_par);
+    r0 = ppm_aveL(q, r_par);
+    u0 = ppm_aveL(q, u_par);
+    Srr = r0 * exp_lim(u_);
+    Sur = u0 + us;
+    get_params(i, geom, xa, v, flat, r_par);
+    get_params(i, geom, xa, w, flat, u_par);
+    Svr = ppm_aveL(q, r_par);
+    Swr = ppm_aveL(q, u_par);
+
+    xl = xa[i - 1];
+    xr = xa[i];
+    get_params(i - 1, geom, xa, u, flat, u_par);
+    tmp = xr - fmax(u_par[1] + u_par[2], 0.0) * dt;
+    q = dimensionless_x(xl, tmp, xr);
+    ul = ppm_aveR(q, u_par);
+    u_ = 0.5 * dt * (u[i - 1] - ul) / (0.5 * (tmp - xl));
+    tmp = xr - fmax(ul, 0.0) * dt;
+    q = dimensionless_x(xl, tmp, xr);
+    get_params(i - 1, geom, xa, r, flat, r_par);
+    r0 = ppm_aveR(q, r_par);
+    u0 = ppm_aveR(q, u_par);
+    Srl = r0 * exp_lim(u_);
+    Sul = u0 + us;
+    get_params(i - 1, geom, xa, v, flat, r_par);
+    get_params(i - 1, geom, xa, w, flat, u_par);
+    Svl = ppm_aveR(q, r_par);
+    Swl = ppm_aveR(q, u_par);
+
+    Srl = fmin(r[i - 1] * dt / (xa[i] - xa[i - 1]), fmax(Sul * Srl, 0.0));
+    Srr = fmax(r[i] * dt / (xa[i] - xa[i + 1]), fmin(Sur * Srr, 0.0));
+    F->r = Srl + Srr;
+    F->u = Srl * Sul + Srr * Sur;
+    F->v = Srl * Svl + Srr * Svr;
+    F->w = Srl * Swl + Srr * Swr;
+}
+
+/* update_Dust (src/solver/dust/dust.cu:149-176) */
+static orc_dust update_dust(const orc_params* P, orc_dust Q, orc_dust D)
+{
+    double r_min = fmax(Q.r * 1.0e-10, P->d_g_ratio * SMALLR);
+    double u_old = Q.u, v_old = Q.v, w_old = Q.w;
+    Q.u *= Q.r; Q.v *= Q.r; Q.w *= Q.r;
+    Q.r += D.r; Q.u += D.u; Q.v += D.v; Q.w += D.w;
+    Q.u /= Q.r; Q.v /= Q.r; Q.w /= Q.r;
+    if (Q.r < r_min) {
+        Q.r = r_min; Q.u = u_old; Q.v = v_old; Q.w = w_old;
+    }
+    return Q;
+}
+
+/* dust_flow (src/solver/dust/dust.cu:105-147) over one pencil: del[c] for c in [3, n-4] */
+static void dust_pencil(int n, int geom, const double* xa, double rad, const double* r, const double* u,
+                        const double* v, const double* w, double dt, double* flat, orc_dust* F, orc_dust* del)
+{
+    double us = 0.5 * dt * 0.0;
+    if (geom > 2) dt /= rad;
+    for (int k = 0; k < n; k++) flat[k] = 0.0;
+    for (int f = NPAD; f <= n - NPAD; f++) dust_flux(f, geom, xa, r, u, v, w, flat, dt, us, &F[f]);
+    for (int c = NPAD; c < n - NPAD; c++) {
+        double g0 = eval_gfac(geom, xa[c]), g1 = eval_gfac(geom, xa[c + 1]);
+        del[c].r = F[c].r * g0 - F[c + 1].r * g1;
+        del[c].u = F[c].u * g0 - F[c + 1].u * g1;
+        del[c].v = F[c].v * g0 - F[c + 1].v * g1;
+        del[c].w = F[c].w * g0 - F[c + 1].w * g1;
+    }
+}
+
+/* sweepx_dust_inplace (src/solver/dust/dust.cu:178-235): CD -> TD, then swap */
+static void sweepx_dust(orc_state* S, double dt)
+{
+    const orc_params* P = &S->P;
+    int n = S->xarr;
+    #pragma omp parallel
+    {
+        double* b = (double*)malloc(5 * (size_t)(n + 1) * sizeof(double));
+        orc_dust* F = (orc_dust*)malloc(2 * (size_t)(n + 1) * sizeof(orc_dust));
+        double *r = b, *u = b + (n + 1), *v = b + 2 * (n + 1), *w = b + 3 * (n + 1), *flat = b + 4 * (n + 1);
+        orc_dust* del = F + (n + 1);
+        #pragma omp for schedule(static)
+        for (int j = S->ypad; j < S->ypad + P->yres; j++) {
+            for (int i = 0; i < n; i++) {
+                const orc_dust* d = &S->CD[IND(S, i, j)];
+                r[i] = d->r; u[i] = d->u; v[i] = d->v; w[i] = d->w;
+                if (P->geomx == 1) v[i] *= xc(S, i);
+            }
+            dust_pencil(n, P->geomx, S->xa, 1.0, r, u, v, w, dt, flat, F, del);
+            for (int i = NPAD; i < n - NPAD; i++) {
+                orc_dust D = del[i];
+                double f = dt / S->xv[i];
+                D.r *= f; D.u *= f; D.v *= f; D.w *= f;
+                if (P->geomx == 1) D.v /= xc(S, i);
+                S->TD[IND(S, i, j)] = update_dust(P, S->CD[IND(S, i, j)], D);
+            }
+        }
+        free(b);
+        free(F);
+    }
+    orc_dust* t = S->CD; S->CD = S->TD; S->TD = t;
+}
+
+/* sweepy_dust_inplace (src/solver/dust/dust.cu:256-326) */
+static void sweepy_dust(orc_state* S, double dt)
+{
+    const orc_params* P = &S->P;
+    int n = S->yarr;
+    #pragma omp parallel
+    {
+        double* b = (double*)malloc(5 * (size_t)(n + 1) * sizeof(double));
+        orc_dust* F = (orc_dust*)malloc(2 * (size_t)(n + 1) * sizeof(orc_dust));
+        double *r = b, *u = b + (n + 1), *v = b + 2 * (n + 1), *w = b + 3 * (n + 1), *flat = b + 4 * (n + 1);
+        orc_dust* del = F + (n + 1);
+        #pragma omp for schedule(static)
+        for (int i = NPAD; i < NPAD + P->xres; i++) {
+            double rad_cyl = (P->geomy == 3) ? xc(S, i) : 1.0;
+            double rot = S->orb_rot[i];
+            for (int j = 0; j < n; j++) {
+                const orc_dust* d = &S->CD[IND(S, i, j)];
+                r[j] = d->r;
+                u[j] = d->v - rot;
+                v[j] = d->w;
+                w[j] = d->u;
+                if (P->geomy == 3) u[j] -= rad_cyl * P->frame_omega;
+            }
+            dust_pencil(n, P->geomy, S->ya, rad_cyl, r, u, v, w, dt, flat, F, del);
+            for (int j = NPAD; j < n - NPAD; j++) {
+                orc_dust D = del[j], E;
+                double f = dt / S->yv[j];
+                D.r *= f; D.u *= f; D.v *= f; D.w *= f;
+                if (P->geomy > 2) {
+                    f = 1.0 / rad_cyl;
+                    D.r *= f; D.u *= f; D.v *= f; D.w *= f;
+                }
+                if (P->geomy == 3) D.u += (rot + rad_cyl * P->frame_omega) * D.r;
+                else D.u += rot * D.r;
+                E.r = D.r; E.v = D.u; E.u = D.w; E.w = D.v;
+                S->TD[IND(S, i, j)] = update_dust(P, S->CD[IND(S, i, j)], E);
+            }
+        }
+        free(b);
+        free(F);
+    }
+    orc_dust* t = S->CD; S->CD = S->TD; S->TD = t;
+}
+
+/* advecty (Dust) + advecty_dust (src/solver/advection/advection.cu:175-357) */
+static void advecty_dust(orc_state* S, double dt)
+{
+    const orc_params* P = &S->P;
+    int n = S->yarr;
+    boundy_dust(S);
+    #pragma omp parallel
+    {
+        double* b = (double*)malloc(5 * (size_t)(n + 1) * sizeof(double));
+        orc_dust* F = (orc_dust*)malloc((size_t)(n + 1) * sizeof(orc_dust));
+        double *r = b, *u = b + (n + 1), *v = b + 2 * (n + 1), *w = b + 3 * (n + 1), *flat = b + 4 * (n + 1);
+        double par[3];
+        #pragma omp for schedule(static)
+        for (int i = NPAD; i < NPAD + P->xres; i++) {
+            double rad = (P->geomy == 3) ? xc(S, i) : 1.0;
+            double speed = S->orb_res[i];
+            double sdt = dt / rad;
+            const double* xa = S->ya;
+            for (int j = 0; j < n; j++) {
+                const orc_dust* d = &S->CD[IND(S, i, j)];
+                r[j] = d->r; u[j] = d->v; v[j] = d->w; w[j] = d->u;
+                flat[j] = 0.0;
+            }
+            for (int f = NPAD; f <= n - NPAD; f++) {
+                orc_dust* D = &F[f];
+                double xl, xr, x0, q;
+                if (speed > 0.0) {
+                    xl = xa[f - 1]; xr = xa[f];
+                    x0 = xr - speed * sdt;
+                    q = dimensionless_x(xl, x0, xr);
+                    get_params(f - 1, P->geomy, xa, r, flat, par); D->r = ppm_aveR(q, par);
+                    get_params(f - 1, P->geomy, xa, u, flat, par); D->u = ppm_aveR(q, par) * D->r;
+                    get_params(f - 1, P->geomy, xa, v, flat, par); D->v = ppm_aveR(q, par) * D->r;
+                    get_params(f - 1, P->geomy, xa, w, flat, par); D->w = ppm_aveR(q, par) * D->r;
+                } else {
+                    xl = xa[f]; xr = xa[f + 1];
+                    x0 = xl - speed * sdt;
+                    q = dimensionless_x(xl, x0, xr);
+                    get_params(f, P->geomy, xa, r, flat, par); D->r = ppm_aveL(q, par);
+                    get_params(f, P->geomy, xa, u, flat, par); D->u = ppm_aveL(q, par) * D->r;
+                    get_params(f, P->geomy, xa, v, flat, par); D->v = ppm_aveL(q, par) * D->r;
+                    get_params(f, P->geomy, xa, w, flat, par); D->w = ppm_aveL(q, par) * D->r;
+                }
+                D->r *= speed; D->u *= speed; D->v *= speed; D->w *= speed;
+            }
+            for (int j = NPAD; j < n - NPAD; j++) {
+                double g0 = eval_gfac(P->geomy, xa[j]), g1 = eval_gfac(P->geomy, xa[j + 1]);
+                orc_dust D, E;
+                double f;
+                D.r = F[j].r * g0 - F[j + 1].r * g1;
+                D.u = F[j].u * g0 - F[j + 1].u * g1;
+                D.v = F[j].v * g0 - F[j + 1].v * g1;
+                D.w = F[j].w * g0 - F[j + 1].w * g1;
+                f = dt / S->yv[j];
+                D.r *= f; D.u *= f; D.v *= f; D.w *= f;
+                if (P->geomy > 2) {
+                    f = 1.0 / rad;
+                    D.r *= f; D.u *= f; D.v *= f; D.w *= f;
+                }
+                E.r = D.r; E.v = D.u; E.u = D.w; E.w = D.v;
+                S->TD[IND(S, i, j)] = update_dust(P, S->CD[IND(S, i, j)], E);
+            }
+        }
+        free(b);
+        free(F);
+    }
+    orc_dust* t = S->CD; S->CD = S->TD; S->TD = t;
+}
+
 /* src/orbit/orbit.cu:74-99 */
 static void set_orbadv(orc_state* S, double dt)
 {
@@ -844,9 +1164,13 @@ static void shift_orbadv(orc_state* S)
             int js = (j + inc) % jmax;
             if (js < 0) js += jmax;
             S->T[IND(S, i, js + S->ypad)] = S->C[IND(S, i, j + S->ypad)];
+            if (S->CD) S->TD[IND(S, i, js + S->ypad)] = S->CD[IND(S, i, j + S->ypad)];
         }
     }
     orc_cell* t = S->C; S->C = S->T; S->T = t;
+    if (S->CD) {
+        orc_dust* td = S->CD; S->CD = S->TD; S->TD = td;
+    }
 }
 
 /* src/solver/advection/advection.cu:1-173 : residual orbital advection C -> T */
@@ -1001,12 +1325,16 @@ static void star_planet_grav_cyl(double rad, double azi, double z, const orc_bod
 }
 
 /*
- * src/solver/sweeps.cu:555-711 with geomx 0/1, ndim <= 2, twobd_flag 0, no dust,
- * no cooling: half-kick of the velocities by curvature, star+planet gravity and
+ * src/solver/sweeps.cu:555-711 with geomx 0/1, ndim <= 2, twobd_flag 0, no
+ * cooling: half-kick of the velocities by curvature, star+planet gravity and
  * the viscous force density; when mdt != 0 the forces are re-evaluated at the
- * mdt-predicted velocities.  out may equal in.
+ * mdt-predicted velocities.  With dust (in_d != NULL) the dust velocities relax
+ * towards the gas ones over the stopping time t_s = Stokes h / (c_s Sigma)
+ * (dust.cu:1-4) with the exponential integrator of sweeps.cu:655-707.  out may
+ * equal in, out_d may equal in_d.
  */
-static void apply_source_terms(orc_state* S, const orc_cell* in, orc_cell* out, double mdt, double dt)
+static void apply_source_terms(orc_state* S, const orc_cell* in, orc_cell* out, const orc_dust* in_d,
+                               orc_dust* out_d, double mdt, double dt)
 {
     const orc_params* P = &S->P;
     int i0 = NPAD - 1, i1 = S->xarr - NPAD + 1;
@@ -1016,6 +1344,12 @@ static void apply_source_terms(orc_state* S, const orc_cell* in, orc_cell* out, 
         for (int i = i0; i < i1; i++) {
             int ind = IND(S, i, j);
             orc_cell C = in[ind], T = C;
+            orc_dust Q = {0.0, 0.0, 0.0, 0.0}, D = Q;
+            double ts = 0.0, fxd = 0.0, fyd = 0.0, dtau;
+            if (in_d) {
+                Q = in_d[ind];
+                D = Q;
+            }
             double x = xc(S, i);
             double y = (P->ndim > 1) ? yc(S, j) + S->orb_rot[i] * 0.0 : 0.0;
             double z = 0.0;
@@ -1032,6 +1366,13 @@ static void apply_source_terms(orc_state* S, const orc_cell* in, orc_cell* out, 
                     gz += tz;
                 }
             }
+            if (in_d) {
+                /* get_t_stop (dust.cu:1-4) and get_d_forces (sweeps.cu:578-595) */
+                ts = P->stokes / (sqrt(P->gam * T.p / T.r) / P->sc_h) / T.r;
+                fxd = (P->geomx == 1) ? D.v * D.v / x : 0.0;
+                fxd = fxd * ts + T.u - Q.u;
+                fyd = 0.0 * ts + T.v - Q.v;
+            }
             /* get_g_forces (sweeps.cu:555-576) */
             fx = (P->geomx == 1) ? T.v * T.v / x : 0.0;
             if (P->visc_flag) fx += S->vis[2 * ind + 0] / T.r;
@@ -1043,6 +1384,16 @@ static void apply_source_terms(orc_state* S, const orc_cell* in, orc_cell* out, 
                 T.u = C.u + fx * mdt + gx * mdt;
                 T.v = C.v + fy * mdt + gy * mdt;
                 T.w = C.w + fz * mdt + gz * mdt;
+                if (in_d) {
+                    dtau = 1.0 - exp(-mdt / ts);
+                    D.u = Q.u + fxd * dtau + gx * ts * dtau;
+                    D.v = Q.v + fyd * dtau + gy * ts * dtau;
+                    D.w = Q.w + 0.0 * dtau + gz * ts * dtau;
+                    ts = P->stokes / (sqrt(P->gam * T.p / T.r) / P->sc_h) / T.r;
+                    fxd = (P->geomx == 1) ? D.v * D.v / x : 0.0;
+                    fxd = fxd * ts + T.u - Q.u;
+                    fyd = 0.0 * ts + T.v - Q.v;
+                }
                 fx = (P->geomx == 1) ? T.v * T.v / x : 0.0;
                 if (P->visc_flag) fx += S->vis[2 * ind + 0] / T.r;
                 if (P->ndim > 1) {
@@ -1057,6 +1408,15 @@ static void apply_source_terms(orc_state* S, const orc_cell* in, orc_cell* out, 
             o.r = in[ind].r;
             o.p = in[ind].p;
             out[ind] = o;
+            if (in_d) {
+                orc_dust od;
+                dtau = 1.0 - exp(-dt / ts);
+                od.u = Q.u + fxd * dtau + gx * ts * dtau;
+                od.v = Q.v + fyd * dtau + gy * ts * dtau;
+                od.w = Q.w + 0.0 * dtau + gz * ts * dtau;
+                od.r = in_d[ind].r;
+                out_d[ind] = od;
+            }
         }
     }
 }
@@ -1115,10 +1475,12 @@ double orc_global_dt(orc_state* S, double dt_prev)
             double rad_cyl = (P->geomy == 3) ? 0.5 * (S->xa[i + 1] + S->xa[i]) : 1.0;
             double cs = sqrt(P->gam * c->p / c->r);
             double spd = fabs(c->u) + cs;
+            if (S->CD) spd = fmax(fabs(S->CD[IND(S, i, j)].u), spd);
             double wid = fabs(S->xa[i + 1] - S->xa[i]);
             double tmp = fmax(spd / wid, 0.0);
             if (P->ndim > 1) {
                 spd = fabs(c->v - rad_cyl * P->frame_omega - S->orb_rot[i]) + cs;
+                if (S->CD) spd = fmax(fabs(S->CD[IND(S, i, j)].v - rad_cyl * P->frame_omega - S->orb_rot[i]), spd);
                 wid = fabs(S->ya[j + 1] - S->ya[j]) * rad_cyl;
                 tmp = fmax(spd / wid, tmp);
             }
@@ -1172,42 +1534,59 @@ void orc_solve(orc_state* S, double t, double dt)
         orc_viscous_forces(S, 0, NULL);
     }
     orc_boundx(S, 0);
-    apply_source_terms(S, S->C, S->C, 0.0, hdt);
+    if (S->CD) boundx_dust(S);
+    apply_source_terms(S, S->C, S->C, S->CD, S->CD, 0.0, hdt);
     orc_boundx(S, 0);
     orc_sweepx(S, dt);
     if (P->ndim > 1) {
         orc_boundy(S, 0);
         orc_sweepy(S, dt);
     }
+    if (S->CD) {  /* DS(), src/solver/solve.cu:240-247 */
+        boundx_dust(S);
+        sweepx_dust(S, dt);
+        if (P->ndim > 1) {
+            boundy_dust(S);
+            sweepy_dust(S, dt);
+        }
+    }
     if (P->orbadv_flag && P->ndim > 1) {
         set_orbadv(S, dt);
         shift_orbadv(S);
         advecty(S, dt);
+        if (S->CD) advecty_dust(S, dt);
     }
     if (P->n_planet > 0) orbit_solution(P, &S->planet, t + dt);
     if (P->visc_flag && P->ndim == 2) {
-        apply_source_terms(S, S->C, S->T, hdt, hdt);
+        apply_source_terms(S, S->C, S->T, S->CD, S->TD, hdt, hdt);
         orc_boundy(S, 1);
         orc_boundx(S, 1);
         orc_viscous_forces(S, 1, NULL);
-        apply_source_terms(S, S->C, S->C, hdt, hdt);
+        apply_source_terms(S, S->C, S->C, S->CD, S->CD, hdt, hdt);
     } else {
-        apply_source_terms(S, S->C, S->C, hdt, hdt);
+        apply_source_terms(S, S->C, S->C, S->CD, S->CD, hdt, hdt);
     }
     if (P->kill_flag) killwave(S, dt);
 }
 
 /* The same step, stage by stage, copying the cell array after every stage the
    stage driver oracle/ref_stages.cu dumps (visc1 if viscous, kick1, sweepx,
-   sweepy, shift and advect with orbital advection, kick2, kill if damping).
-   Returns the number of stages written to out (each xarr*yarr cells). */
-int orc_solve_stages(orc_state* S, double t, double dt, orc_cell* out)
+   sweepy, with dust dsweepx and dsweepy, shift and advect with orbital
+   advection (+ dadvect with dust), kick2, kill if damping), and with dust the
+   dust array into dout after the same stages.  Returns the number of stages
+   written (each xarr*yarr cells). */
+int orc_solve_stages(orc_state* S, double t, double dt, orc_cell* out, orc_dust* dout)
 {
     const orc_params* P = &S->P;
     double hdt = 0.5 * dt;
     size_t n = (size_t)S->xarr * S->yarr;
     int k = 0;
-#define DUMP() memcpy(out + (size_t)(k++) * n, S->C, n * sizeof(orc_cell))
+#define DUMP()                                                                   \
+    do {                                                                         \
+        memcpy(out + (size_t)k * n, S->C, n * sizeof(orc_cell));                 \
+        if (dout && S->CD) memcpy(dout + (size_t)k * n, S->CD, n * sizeof(orc_dust)); \
+        k++;                                                                     \
+    } while (0)
     if (P->visc_flag && P->ndim == 2) {
         orc_boundy(S, 0);
         orc_boundx(S, 0);
@@ -1215,7 +1594,8 @@ int orc_solve_stages(orc_state* S, double t, double dt, orc_cell* out)
         DUMP();
     }
     orc_boundx(S, 0);
-    apply_source_terms(S, S->C, S->C, 0.0, hdt);
+    if (S->CD) boundx_dust(S);
+    apply_source_terms(S, S->C, S->C, S->CD, S->CD, 0.0, hdt);
     DUMP();
     orc_boundx(S, 0);
     orc_sweepx(S, dt);
@@ -1225,22 +1605,36 @@ int orc_solve_stages(orc_state* S, double t, double dt, orc_cell* out)
         orc_sweepy(S, dt);
         DUMP();
     }
+    if (S->CD) {
+        boundx_dust(S);
+        sweepx_dust(S, dt);
+        DUMP();
+        if (P->ndim > 1) {
+            boundy_dust(S);
+            sweepy_dust(S, dt);
+            DUMP();
+        }
+    }
     if (P->orbadv_flag && P->ndim > 1) {
         set_orbadv(S, dt);
         shift_orbadv(S);
         DUMP();
         advecty(S, dt);
         DUMP();
+        if (S->CD) {
+            advecty_dust(S, dt);
+            DUMP();
+        }
     }
     if (P->n_planet > 0) orbit_solution(P, &S->planet, t + dt);
     if (P->visc_flag && P->ndim == 2) {
-        apply_source_terms(S, S->C, S->T, hdt, hdt);
+        apply_source_terms(S, S->C, S->T, S->CD, S->TD, hdt, hdt);
         orc_boundy(S, 1);
         orc_boundx(S, 1);
         orc_viscous_forces(S, 1, NULL);
-        apply_source_terms(S, S->C, S->C, hdt, hdt);
+        apply_source_terms(S, S->C, S->C, S->CD, S->CD, hdt, hdt);
     } else {
-        apply_source_terms(S, S->C, S->C, hdt, hdt);
+        apply_source_terms(S, S->C, S->C, S->CD, S->CD, hdt, hdt);
     }
     DUMP();
     if (P->kill_flag) {

@@ -30,7 +30,8 @@ extern "C" {
 #endif
 
 typedef struct { double r, p, u, v, w; } orc_cell;          /* include/structs.h:48 */
-typedef struct { double m, a, e, x, y, z, vx, vy, vz, rs; } orc_body;  /* include/structs.h:105 */
+typedef struct { double m, a, e, x, y, z, vx, vy, vz, rs; } orc_body;
+typedef struct { double r, u, v, w; } orc_dust;                /* include/structs.h:19 */  /* include/structs.h:105 */
 
 typedef struct {
     int ndim;                 /* 1 or 2 */
@@ -52,6 +53,8 @@ typedef struct {
     int n_planet;             /* 0 or 1 */
     double planet_mass, planet_ecc, rs_fac, ramp_time;
     double zmin, zmax;        /* only enter through the z grid (2D: unused by the physics) */
+    int dust_flag;            /* 1: one pressureless dust fluid (src/solver/dust/dust.cu) */
+    double stokes, d_g_ratio; /* Stokes and D_G_ratio of include/parameters.h */
 } orc_params;
 
 typedef struct orc_state orc_state;
@@ -70,6 +73,10 @@ void orc_set_interior(orc_state* S, const double* r, const double* p, const doub
 void orc_get_interior(const orc_state* S, double* r, double* p, double* u, double* v);
 /* the whole AoS array incl. ghosts, xarr*yarr cells */
 void orc_get_cells(const orc_state* S, orc_cell* out);
+/* dust interior (dust_flag); the dust starts from init_CD (src/init/init.cu:351-454):
+   the reference's restart path does not load dust (src/output/output.cu:182-248) */
+void orc_set_dust(orc_state* S, const double* r, const double* u, const double* v);
+void orc_get_dust(const orc_state* S, double* r, double* u, double* v);
 
 void orc_init_planet(orc_state* S, double t);   /* src/planet/planet.cu:319 */
 void orc_init_orbadv(orc_state* S);             /* src/orbit/orbit.cu:51,111 */
@@ -88,7 +95,7 @@ void orc_boundy(orc_state* S, int which);
 void orc_viscous_forces(orc_state* S, int which, double* vis_out /* 2*xarr*yarr or NULL */);
 void orc_sweepx(orc_state* S, double dt);
 void orc_sweepy(orc_state* S, double dt);
-int orc_solve_stages(orc_state* S, double t, double dt, orc_cell* out);
+int orc_solve_stages(orc_state* S, double t, double dt, orc_cell* out, orc_dust* dout /* or NULL */);
 
 #ifdef __cplusplus
 }

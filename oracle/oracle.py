@@ -33,6 +33,7 @@ class OrcParams(ctypes.Structure):
         ("planet_mass", ctypes.c_double), ("planet_ecc", ctypes.c_double),
         ("rs_fac", ctypes.c_double), ("ramp_time", ctypes.c_double),
         ("zmin", ctypes.c_double), ("zmax", ctypes.c_double),
+        ("dust_flag", ctypes.c_int), ("stokes", ctypes.c_double), ("d_g_ratio", ctypes.c_double),
     ]
 
     @classmethod
@@ -44,6 +45,7 @@ class OrcParams(ctypes.Structure):
             p.p_alpha, p.p_beta, p.ss_alpha, p.sc_h, p.planet_radius,
             p.visc_flag, p.OrbAdv_flag, p.kill_flag, p.kill_width, p.kill_width_out,
             p.n_planet, p.planet_mass, p.planet_ecc, p.rs_fac, p.ramp_time, p.zmin, p.zmax,
+            p.dust_flag, p.Stokes, p.D_G_ratio,
         )
 
 
@@ -85,6 +87,8 @@ def lib():
         L.orc_global_dt.argtypes = [vp, ctypes.c_double]
         L.orc_torque.restype = ctypes.c_double
         L.orc_torque.argtypes = [vp]
+        L.orc_set_dust.argtypes = [vp, dp, dp, dp]
+        L.orc_get_dust.argtypes = [vp, dp, dp, dp]
         L.orc_solve.argtypes = [vp, ctypes.c_double, ctypes.c_double]
         L.orc_run.restype = ctypes.c_int
         L.orc_run.argtypes = [vp, ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_double, dp, dp]
@@ -94,7 +98,7 @@ def lib():
         L.orc_sweepx.argtypes = [vp, ctypes.c_double]
         L.orc_sweepy.argtypes = [vp, ctypes.c_double]
         L.orc_solve_stages.restype = ctypes.c_int
-        L.orc_solve_stages.argtypes = [vp, ctypes.c_double, ctypes.c_double, dp]
+        L.orc_solve_stages.argtypes = [vp, ctypes.c_double, ctypes.c_double, dp, dp]
         _lib = L
     return _lib
 
@@ -157,6 +161,17 @@ class Oracle:
     def global_dt(self, dt_prev: float) -> float:
         return lib().orc_global_dt(self.h, dt_prev)
 
+    def dust(self) -> dict:
+        """Dust interior (dust_flag): r, u, v arrays (yres, xres)."""
+        shape = (self.p.yres, self.p.xres)
+        out = {k: np.zeros(shape) for k in ("r", "u", "v")}
+        lib().orc_get_dust(self.h, _dp(out["r"]), _dp(out["u"]), _dp(out["v"]))
+        return out
+
+    def set_dust(self, d: dict) -> None:
+        f = {k: np.ascontiguousarray(d[k], dtype=np.float64) for k in ("r", "u", "v")}
+        lib().orc_set_dust(self.h, _dp(f["r"]), _dp(f["u"]), _dp(f["v"]))
+
     def torque(self) -> float:
         """Torque of the planet on the disk (src/output/output.cu:336-412), unnormalised."""
         return lib().orc_torque(self.h)
@@ -164,11 +179,13 @@ class Oracle:
     def solve(self, t: float, dt: float) -> None:
         lib().orc_solve(self.h, t, dt)
 
-    def solve_stages(self, t: float, dt: float) -> np.ndarray:
-        """One step, returning the cell array after each stage (see oracle.c)."""
-        buf = np.zeros((8, self.yarr, self.xarr, 5))
-        k = lib().orc_solve_stages(self.h, t, dt, _dp(buf))
-        return buf[:k]
+    def solve_stages(self, t: float, dt: float, dust: bool = False):
+        """One step, returning the cell array after each stage (see oracle.c);
+        with dust=True also the dust arrays after the same stages."""
+        buf = np.zeros((12, self.yarr, self.xarr, 5))
+        dbuf = np.zeros((12, self.yarr, self.xarr, 4)) if dust else None
+        k = lib().orc_solve_stages(self.h, t, dt, _dp(buf), _dp(dbuf) if dust else None)
+        return (buf[:k], dbuf[:k]) if dust else buf[:k]
 
     def run(self, max_step: int, end_time: float = 1.0e30) -> int:
         """main.cu:320-360: dt from global_dt (first call capped by end_time - t),

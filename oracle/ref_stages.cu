@@ -5,10 +5,18 @@
 // parameters.h, this program repeats main.cu's set-up (main.cu:154-305,
 // restart path) and then runs DS() (src/solver/solve.cu:212-277) and killwave
 // one stage at a time, checking for CUDA errors and dumping the whole cell
-// array (ghosts included) after every stage.  Used to pin the oracle stage by
-// stage and to locate discrepancies.
+// array (ghosts included) after every stage, followed by the dust array in
+// dust_flag builds (main.cu's dust allocations are repeated).  Used to pin the
+// oracle stage by stage and to locate discrepancies.
 //
-//   stages <restart file> <steps> <dump file>
+//   stages <restart file> <steps> <dump file> [scrub]
+//
+// With "scrub", a kernel of this driver writes zeros over the dynamic shared
+// memory of every SM right before each dust stage: the reference's dust
+// reconstruction reads a flattening coefficient from shared memory that it never
+// writes under recon_flag 6 (src/solver/recon/PPM.cu:68-77 reached from
+// src/solver/dust/dust.cu:105-147 and src/solver/advection/advection.cu:175-233),
+// so this shows what it computes when that memory holds zeros.
 #include <cstdio>
 #include <cstdlib>
 #include <string>
@@ -33,8 +41,23 @@ void evolve_planet(Grid*, double, double);
 void viscosity_tensor_evaluation1(Grid*);
 void viscosity_tensor_evaluation2(Grid*);
 void killwave(Grid*, double);
+#ifdef dust_flag
+void boundx_dust(Grid*);
+void boundy_dust(Grid*, double);
+void sweepx_dust_inplace(Grid*, double);
+void sweepy_dust_inplace(Grid*, double);
+void advecty_dust(Grid*, double);
+static Dust* g_dhost = nullptr;
+#endif
 
 static FILE* g_dump = nullptr;
+static bool g_scrub = false;
+
+// Zeros the dynamic shared memory of many blocks per SM (diagnostic only).
+__global__ void scrub_smem(int nd) {
+    extern __shared__ double smem[];
+    for (int k = threadIdx.x; k < nd; k += blockDim.x) smem[k] = 0.0;
+}
 static Cell* g_host = nullptr;
 static int g_stage = 0;
 
@@ -47,6 +70,15 @@ static void check(const char* what) {
     }
 }
 
+static void scrub() {
+    if (!g_scrub) return;
+    const int bytes = 227 * 1024;  // one block per SM covering (nearly) all of its shared memory
+    cudaFuncSetAttribute(scrub_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    cudaFuncSetAttribute(scrub_smem, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    scrub_smem<<<148 * 4, 1024, bytes>>>(bytes / 8);
+    check("scrub");
+}
+
 static void dump(Grid* dev, const char* name, double t, double dt) {
     check(name);
     size_t n = (size_t)dev[0].xarr * dev[0].yarr * dev[0].zarr;
@@ -57,6 +89,10 @@ static void dump(Grid* dev, const char* name, double t, double dt) {
     double td[2] = {t, dt};
     fwrite(td, sizeof(double), 2, g_dump);
     fwrite(g_host, sizeof(Cell), n, g_dump);
+#ifdef dust_flag
+    cudaMemcpy(g_dhost, dev[0].CD, n * sizeof(Dust), cudaMemcpyDeviceToHost);
+    fwrite(g_dhost, sizeof(Dust), n, g_dump);
+#endif
     int bad = 0;
     for (size_t k = 0; k < n; ++k)
         if (g_host[k].r != g_host[k].r) ++bad;
@@ -69,6 +105,7 @@ int main(int argc, char** argv) {
         return 2;
     }
     int steps = atoi(argv[2]);
+    g_scrub = (argc > 4 && std::string(argv[4]) == "scrub");
     g_dump = fopen(argv[3], "wb");
     Grid* hst;
     Grid* dev;
@@ -118,6 +155,15 @@ int main(int argc, char** argv) {
     cudaMalloc((void**)&dev->shfR, xpad * zres * sizeof(int));
     cudaMalloc((void**)&dev->planets, n_planet * sizeof(body));
     cudaMemset(dev->T, 0, n * sizeof(Cell));
+#ifdef dust_flag
+    cudaMallocHost((void**)&hst->CD, n * sizeof(Dust));
+    cudaMallocHost((void**)&g_dhost, n * sizeof(Dust));
+    cudaMalloc((void**)&dev->CD, n * sizeof(Dust));
+    cudaMalloc((void**)&dev->TD, n * sizeof(Dust));
+    cudaMalloc((void**)&dev->BuffLD, xpad * yarr * zarr * sizeof(Dust));
+    cudaMalloc((void**)&dev->BuffRD, xpad * yarr * zarr * sizeof(Dust));
+    cudaMemset(dev->TD, 0, n * sizeof(Dust));
+#endif
 
     init(hst);
     double t = load_grid(hst, argv[1]);
@@ -129,6 +175,9 @@ int main(int argc, char** argv) {
     cudaMemcpy(dev->za, hst->za, (zarr + 1) * sizeof(double), cudaMemcpyHostToDevice);
     cudaMemcpy(dev->zv, hst->zv, zarr * sizeof(double), cudaMemcpyHostToDevice);
     cudaMemcpy(dev->C, hst->C, n * sizeof(Cell), cudaMemcpyHostToDevice);
+#ifdef dust_flag
+    cudaMemcpy(dev->CD, hst->CD, n * sizeof(Dust), cudaMemcpyHostToDevice);
+#endif
     cudaMemcpy(dev->planets, hst->planets, n_planet * sizeof(body), cudaMemcpyHostToDevice);
     init_OrbAdv(dev);
     dump(dev, "start", t, 0.0);
@@ -142,6 +191,9 @@ int main(int argc, char** argv) {
         dump(dev, "visc1", t, dt);
 #endif
         boundx(dev);
+#ifdef dust_flag
+        boundx_dust(dev);
+#endif
         apply_source_terms_inplace(dev, 0.0, 0.0, hdt);
         dump(dev, "kick1", t, dt);
         boundx(dev);
@@ -152,12 +204,29 @@ int main(int argc, char** argv) {
         sweepy_inplace(dev, dt);
         dump(dev, "sweepy", t, dt);
 #endif
+#ifdef dust_flag
+        boundx_dust(dev);
+        scrub();
+        sweepx_dust_inplace(dev, dt);
+        dump(dev, "dsweepx", t, dt);
+#if ndim > 1
+        boundy_dust(dev, t + dt);
+        scrub();
+        sweepy_dust_inplace(dev, dt);
+        dump(dev, "dsweepy", t, dt);
+#endif
+#endif
 #ifdef OrbAdv_flag
         set_OrbAdv(dev, dt);
         shift_OrbAdv(dev);
         dump(dev, "shift", t, dt);
         advecty(dev, dt);
         dump(dev, "advect", t, dt);
+#ifdef dust_flag
+        scrub();
+        advecty_dust(dev, dt);
+        dump(dev, "dadvect", t, dt);
+#endif
 #endif
         evolve_planet(dev, t + dt, dt);
 #ifdef visc_flag

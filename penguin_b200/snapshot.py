@@ -21,7 +21,7 @@ def write_snapshot(path: str, t: float, xa: np.ndarray, ya: np.ndarray | None, f
     np.concatenate(parts).tofile(path)
 
 
-def read_snapshot(path: str, xres: int, yres: int, ndim: int) -> dict:
+def read_snapshot(path: str, xres: int, yres: int, ndim: int, dust: bool = False) -> dict:
     dat = np.fromfile(path, dtype=np.float64)
     o = 0
     t = float(dat[o]); o += 1
@@ -34,6 +34,10 @@ def read_snapshot(path: str, xres: int, yres: int, ndim: int) -> dict:
     for k in ["r", "p", "u"] + (["v"] if ndim > 1 else []):
         out[k] = dat[o:o + n].reshape(yres, xres)
         o += n
+    if dust:  # dust_flag builds append the dust r, u (and v, w in 2D), src/output/output.cu:159-176
+        for k in ["dust_r", "dust_u"] + (["dust_v", "dust_w"] if ndim > 1 else []):
+            out[k] = dat[o:o + n].reshape(yres, xres)
+            o += n
     if o != dat.size:
         raise ValueError(f"{path}: {dat.size} values, expected {o}")
     return out

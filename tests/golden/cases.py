@@ -60,6 +60,28 @@ def cases() -> list[dict]:
     return out
 
 
+def dust_cases() -> list[dict]:
+    """Gas + one dust fluid (config 3's physics at 64x192): alpha 1e-4, q 3e-4,
+    Stokes 0.01 and 0.1, dust-to-gas 0.01.  The dust starts from init_CD (the
+    reference's restart loads gas only).  tol: oracle vs the reference's output for
+    the gas and dust fields; the reference's dust reconstruction reads a stale
+    shared-memory flattening coefficient (see oracle/oracle.c, dust_flux), so these
+    fixtures come from its kernels run by oracle/ref_stages.cu with that memory
+    zeroed (make_golden.py, _run_dust).  Measured oracle agreement: 1e-15 after one
+    step, 2e-11 after ten (the planet amplifies gas rounding as in disk64_n10)."""
+    out = []
+    for st, tag in ((0.01, "st001"), (0.1, "st01")):
+        p = P.reference_disk(64, 192, q=3.0e-4, alpha=1.0e-4).replace(dust_flag=1, Stokes=st, D_G_ratio=0.01)
+        out.append(dict(name=f"dust64_{tag}_n10", params=p, init="disk", t0=T0_DISK, max_step=10, end_time=1.0e30,
+                        tol=1e-10, cuda_tol=1e-10, dust=True))
+    p = P.reference_disk(64, 192, q=3.0e-4, alpha=1.0e-4).replace(dust_flag=1, Stokes=0.1, D_G_ratio=0.01)
+    out.append(dict(name="dust64_st01_n1", params=p, init="disk", t0=T0_DISK, max_step=1, end_time=1.0e30,
+                    tol=1e-12, cuda_tol=1e-12, dust=True))
+    out.append(dict(name="dust64_st01_noplanet_n10", params=p.replace(planet_mass=0.0), init="disk", t0=T0_DISK,
+                    max_step=10, end_time=1.0e30, tol=1e-10, cuda_tol=1e-10, dust=True))
+    return out
+
+
 def timing_cases() -> list[dict]:
     """Full-size planet-disk runs of the reference, used only to time it on the B200."""
     c2 = P.reference_disk(1024, 3072)

@@ -39,7 +39,7 @@ from penguin_b200.params import make_grid_np  # noqa: E402
 
 
 def _all(timing: bool):
-    return C.cases() + (C.timing_cases() if timing else [])
+    return C.cases() + C.dust_cases() + (C.timing_cases() if timing else [])
 
 
 def build(timing: bool, jobs: int) -> None:
@@ -48,6 +48,45 @@ def build(timing: bool, jobs: int) -> None:
         t = time.time()
         exe = ref_build.build_case(c["name"], hdr, jobs=jobs)
         print(f"{c['name']}: {exe} ({time.time() - t:.0f} s)", flush=True)
+
+
+def _run_dust(c: dict, d: str, out: str, st: dict) -> int:
+    """Dust cases: the reference's dust reconstruction reads a flattening coefficient
+    from shared memory it never writes (src/solver/recon/PPM.cu:68-77 reached from
+    src/solver/dust/dust.cu:105-147), so its snapshots depend on what earlier kernels
+    left there.  These fixtures are produced by the reference's own kernels driven
+    step by step by oracle/ref_stages.cu with that memory zeroed before each dust
+    stage ("scrub"); the final stage of the last step is stored."""
+    p = c["params"]
+    t = time.time()
+    r = subprocess.run(["./stages", "init.bin", str(c["max_step"]), "stages.bin", "scrub"], cwd=d,
+                       capture_output=True, text=True, timeout=900)
+    wall = time.time() - t
+    with open(os.path.join(out, c["name"] + ".log"), "w") as f:
+        f.write(r.stdout + "\n--- stderr ---\n" + r.stderr)
+    print(f"{c['name']}: rc={r.returncode} wall={wall:.2f}s (stage driver, scrub)", flush=True)
+    if r.returncode != 0 or "CUDA error" in r.stdout:
+        return 1
+    xarr, yarr = p.xres + 6, p.yres + 6
+    n = xarr * yarr
+    rec = 32 + 16 + n * 40 + n * 32
+    raw = np.fromfile(os.path.join(d, "stages.bin"), dtype=np.uint8)
+    last = raw[(raw.size // rec - 1) * rec:]
+    t_stage, dt_stage = np.frombuffer(last[32:48].tobytes())
+    cells = np.frombuffer(last[48:48 + n * 40].tobytes()).reshape(yarr, xarr, 5)[3:-3, 3:-3]
+    dust = np.frombuffer(last[48 + n * 40:].tobytes()).reshape(yarr, xarr, 4)[3:-3, 3:-3]
+    os.remove(os.path.join(d, "stages.bin"))
+    keys = ["r", "p", "u", "v"]
+    res = {k: np.ascontiguousarray(cells[..., m]) for m, k in ((0, "r"), (1, "p"), (2, "u"), (3, "v"))}
+    res.update({"dust_" + k: np.ascontiguousarray(dust[..., m]) for m, k in enumerate(("r", "u", "v", "w"))})
+    np.savez_compressed(
+        os.path.join(out, c["name"] + ".npz"),
+        t0=c["t0"], t=t_stage + dt_stage, max_step=c["max_step"], end_time=c["end_time"],
+        params=json.dumps(dataclasses.asdict(p)), source="ref_stages scrub",
+        **{"init_" + k: np.asarray(st[k], dtype=np.float64) for k in keys},
+        **{"out_" + k: v for k, v in res.items()},
+    )
+    return 0
 
 
 def run(out: str, timing: bool, only: str | None) -> int:
@@ -71,6 +110,9 @@ def run(out: str, timing: bool, only: str | None) -> int:
         init = os.path.join(d, "init.bin")
         snapshot.write_snapshot(init, c["t0"], xa[3:3 + p.xres + 1], ya[3:3 + p.yres + 1] if p.ndim > 1 else None,
                                 st, p.ndim)
+        if c.get("dust"):
+            bad += _run_dust(c, d, out, st)
+            continue
         t = time.time()
         r = subprocess.run(["./penguin", "init.bin", "0"], cwd=d, capture_output=True, text=True, timeout=900)
         wall = time.time() - t
@@ -89,20 +131,22 @@ def run(out: str, timing: bool, only: str | None) -> int:
                 json.dump({"seconds_per_step": float(sps[-1]) if sps else None, "wall_s": wall,
                            "steps": c["max_step"], "cells": p.xres * p.yres}, f)
             continue
-        res = snapshot.read_snapshot(outs[0], p.xres, p.yres, p.ndim)
+        dust = bool(c.get("dust"))
+        res = snapshot.read_snapshot(outs[0], p.xres, p.yres, p.ndim, dust=dust)
         keys = ["r", "p", "u"] + (["v"] if p.ndim > 1 else [])
+        dkeys = ["dust_r", "dust_u", "dust_v", "dust_w"] if dust else []
         np.savez_compressed(
             os.path.join(out, c["name"] + ".npz"),
             t0=c["t0"], t=res["t"], max_step=c["max_step"], end_time=c["end_time"],
             params=json.dumps(dataclasses.asdict(p)),
             **{"init_" + k: np.asarray(st[k], dtype=np.float64) for k in keys},
-            **{"out_" + k: res[k] for k in keys},
+            **{"out_" + k: res[k] for k in keys + dkeys},
         )
     return bad
 
 
 def collect(src: str) -> None:
-    for c in C.cases():
+    for c in C.cases() + C.dust_cases():
         f = os.path.join(src, c["name"] + ".npz")
         if os.path.exists(f):
             shutil.copy(f, os.path.join(HERE, c["name"] + ".npz"))

@@ -61,6 +61,42 @@ def test_oracle_matches_reference(case):
     assert momentum_l1(out, ref) < case["tol"], momentum_l1(out, ref)
 
 
+@pytest.mark.parametrize("case", C.dust_cases(), ids=lambda c: c["name"])
+def test_oracle_dust_matches_reference(case):
+    """Gas + dust (src/solver/dust/dust.cu) against the reference's kernels run
+    with the shared memory that its dust reconstruction reads zeroed (the
+    fixtures' source; see tests/golden/make_golden.py, _run_dust)."""
+    z = _load(case["name"])
+    p = case["params"]
+    st = {k: z["init_" + k] for k in ("r", "p", "u", "v")}
+    o = Oracle(p, st, float(z["t0"]))
+    o.run(int(z["max_step"]), float(z["end_time"]))
+    assert o.t == pytest.approx(float(z["t"]), rel=max(1e-13, case["tol"]))
+    out, d = o.interior(), o.dust()
+    ref = {k: z["out_" + k] for k in ("r", "p", "u", "v")}
+    assert rel_l1(out["r"], ref["r"]) < case["tol"]
+    assert momentum_l1(out, ref) < case["tol"]
+    dref = {k: z["out_dust_" + k] for k in ("r", "u", "v")}
+    assert rel_l1(d["r"], dref["r"]) < case["tol"], rel_l1(d["r"], dref["r"])
+    assert momentum_l1(d, dref) < case["tol"], momentum_l1(d, dref)
+    assert np.all(z["out_dust_w"] == 0.0)
+
+
+def test_oracle_dust_starts_from_init_cd():
+    """init_CD (src/init/init.cu:351-454): Sigma_d = D_G_ratio Sigma_0, v_phi = v_K,
+    and the drift speed solves the terminal-velocity relation of the pressure-
+    supported gas (|v_r,d| grows with St below St = 1)."""
+    p = P.planet_disk(64, 192).replace(dust_flag=1, Stokes=0.01, D_G_ratio=0.01)
+    o = Oracle(p, I.disk_state(p, seed=1), 0.0)
+    d = o.dust()
+    x = I.cell_centres(p)
+    assert np.allclose(d["r"][0], 0.01 / x, rtol=1e-14)
+    assert np.allclose(d["v"][0], np.sqrt(1.0 / x), rtol=1e-14)
+    assert (d["u"] < 0).all()
+    q = P.planet_disk(64, 192).replace(dust_flag=1, Stokes=0.1, D_G_ratio=0.01)
+    assert (np.abs(Oracle(q, I.disk_state(q, seed=1), 0.0).dust()["u"]) > np.abs(d["u"])).all()
+
+
 def test_initial_state_regenerates_fixture():
     """The seeded initial states are reproducible (SplitMix64 noise)."""
     for case in C.cases():
