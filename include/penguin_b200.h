@@ -142,6 +142,12 @@ pg_status pg_disk_set_state(pg_disk* d, double t, const double* r, const double*
                             const double* v);
 /* The newest state back to host arrays; t_out may be NULL. */
 pg_status pg_disk_get_state(pg_disk* d, double* r, double* p, double* u, double* v, double* t_out);
+/* dust_flag: the interior dust (density, radial and azimuthal velocity, host
+   arrays of xres*yres) of the newest state.  pg_disk_set_state resets the dust
+   to init_CD, as the reference's restart does (load_grid reads the gas only,
+   src/output/output.cu:182-248); pg_disk_set_dust then overwrites it. */
+pg_status pg_disk_set_dust(pg_disk* d, const double* r, const double* u, const double* v);
+pg_status pg_disk_get_dust(pg_disk* d, double* r, double* u, double* v);
 /* Device pointer of the newest AoS state (xarr*yarr pg_cell) and of the scratch. */
 pg_status pg_disk_state_ptr(pg_disk* d, pg_cell** cells);
 /* global_dt (blocking) and one step with host-supplied t, dt, as in main.cu. */

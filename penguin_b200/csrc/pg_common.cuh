@@ -71,6 +71,11 @@ struct DiskView {
     double* res;          // orb_res
     int* inc;             // orb_inc
     Scalars* sc;
+    // one pressureless dust fluid (dust_flag, src/solver/dust/dust.cu)
+    int dust;
+    double stokes, sc_h;  // Stokes number; h/r (stopping time t_s = Stokes h / (c_s Sigma), dust.cu:1-4)
+    double dust_rmin;     // D_G_ratio * smallr: the dust density floor of update_Dust (dust.cu:149-176)
+    const double* initd;  // init_CD(xc(i)) (4 per i: r, u, v, w; src/init/init.cu:351-454)
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {

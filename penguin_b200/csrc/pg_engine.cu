@@ -164,6 +164,42 @@ static void recon_weights(int geom, const double* x, int ncell, double* w) {
     }
 }
 
+// ------------------------------------------------------------- init_CD
+// The dust's initial and bound-0 ghost state, evaluated on the host like the
+// reference's fill_grid (src/init/init.cu:502-519) so it carries the same bits:
+// init_CD (init.cu:351-454, init_flag 2, 2D) is D_G_ratio Sigma_0, the
+// Keplerian azimuthal speed and the radial drift of the steady drag solution,
+// refined once from its first-order estimate.  Its drift term takes the
+// difference of nearly equal square roots and the gas v_phi a centred
+// difference of P over 2.3e-7, so one ulp of pow moves it by ~1e-9.
+static void init_cd_table(const pg_params& P, const double* xa, int xarr, double* q) {
+    auto cs2 = [&](double x) {
+        const double coeff = P.sc_h * P.sc_h * (1.0 / P.planet_radius);
+        return P.geomx == 0 ? coeff : coeff * std::pow(x / P.planet_radius, -P.p_beta);
+    };
+    auto rho = [&](double x) { return std::pow(x / P.planet_radius, -P.p_alpha) * 1.0; };
+    auto prs = [&](double x) { return cs2(x) * rho(x); };
+    for (int i = 0; i < xarr; ++i) {
+        const double x = 0.5 * (xa[i + 1] + xa[i]);
+        const double dr = 1.1514178e-7;
+        const double dP_dr = (prs(x + dr) - prs(x - dr)) / (2.0 * dr);
+        const double v_gas = std::sqrt(1.0 / x + (x / rho(x)) * dP_dr);
+        const double st = P.stokes;
+        const double f_gas = v_gas / std::sqrt(1.0 / x);
+        const double tmp = st * st * f_gas;
+        double L = ((1.0 + tmp) / tmp) * (1.0 - std::sqrt(1.0 - 2.0 * tmp * (1.0 - f_gas) / (1.0 + tmp) / (1.0 + tmp)));
+        double u0 = st * (L * L - 2.0 * L);
+        double u = (1.0 - std::sqrt(1.0 - 2.0 * st * u0)) / st;
+        L = (1.0 - f_gas + st * u / 2.0) / (1.0 + st * u / 2.0);
+        u0 = st * (L * L - 2.0 * L);
+        u = (1.0 - std::sqrt(1.0 - 2.0 * st * u0)) / st;
+        q[4 * i + 0] = P.d_g_ratio * std::pow(x / P.planet_radius, -P.p_alpha);
+        q[4 * i + 1] = u * std::sqrt(1.0 / x);
+        q[4 * i + 2] = std::sqrt(1.0 / x);
+        q[4 * i + 3] = 0.0;
+    }
+}
+
 // ----------------------------------------------------------- tensor maps
 typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
@@ -208,6 +244,15 @@ static pg_status make_cell_maps(CellMaps& M, const Cell* buf, int xarr, int yarr
     return PG_OK;
 }
 
+static pg_status make_dust_maps(DustMaps& M, const pg_dust* buf, int xarr, int yarr) {
+    if (M.base == buf) return PG_OK;
+    pg_status s;
+    if ((s = make_map(&M.sweep_x, buf, 4ull * xarr, yarr, 4 * 38, 8)) != PG_OK) return s;
+    if ((s = make_map(&M.sweep_y, buf, 4ull * xarr, yarr, 4 * 10, 38)) != PG_OK) return s;
+    M.base = buf;
+    return PG_OK;
+}
+
 static pg_status make_vis_maps(VisMaps& M, const double* vis, int xarr, int yarr) {
     if (M.base == vis) return PG_OK;
     pg_status s;
@@ -230,7 +275,11 @@ static pg_status check_params(const pg_params* P) {
     if (P->bound_lft < 0 || P->bound_lft > 2 || P->bound_rgh < 0 || P->bound_rgh > 2)
         return fail(PG_ERR_CONFIG, "radial boundaries must be 0, 1 or 2");
     if (P->n_planet != 0 && P->n_planet != 1) return fail(PG_ERR_CONFIG, "n_planet must be 0 or 1");
-    if (P->dust_flag) return fail(PG_ERR_CONFIG, "dust is not supported by this build");
+    if (P->dust_flag) {
+        if (P->ndim != 2) return fail(PG_ERR_CONFIG, "dust needs ndim 2");
+        if (P->init_flag != 2) return fail(PG_ERR_CONFIG, "dust needs init_flag 2 (init_CD)");
+        if (!(P->stokes > 0.0)) return fail(PG_ERR_CONFIG, "dust needs Stokes > 0");
+    }
     if (P->gridx < 0 || P->gridx > 1 || P->gridy != 0) return fail(PG_ERR_CONFIG, "grids: x linear/log, y linear");
     if (P->gridx == 1 && !(P->xmin > 0.0)) return fail(PG_ERR_CONFIG, "log grid needs xmin > 0");
     return PG_OK;
@@ -266,6 +315,8 @@ struct Engine {
     std::vector<const void*> ghosted;  // buffers whose constant radial ghosts are initialised
     pg_body* grid_planet = nullptr;    // drop-in mode: the caller's planets array
     double* part = nullptr;            // per-block partial sums of diagnostics
+    pg_dust* dbuf[2] = {nullptr, nullptr};  // dust_flag: the dust of buf[k] is dbuf[k]
+    DustMaps dmaps[2];
 
     ~Engine() {
         for (auto& g : graph)
@@ -280,6 +331,8 @@ struct Engine {
             cudaFree(res);
             cudaFree(inc);
         }
+        cudaFree(dbuf[0]);
+        cudaFree(dbuf[1]);
         cudaFree(grid);
         cudaFree(tab);
         cudaFree(part);
@@ -318,7 +371,9 @@ static pg_status engine_setup(Engine& E, const double* dev_xa, const double* dev
     }
     // tables: wx[6 xarr] wy[6 yarr] | radx cs2x nux initx(5) killx(4) idx_x ixv irad gstar visx(5) [xarr each]
     //         | ycraw ycj idx_y iyv visy(4) [yarr each] | trig [4 yarr + 2]
-    const size_t ntab = 6 * (size_t)xarr + 6 * (size_t)yarr + 21 * (size_t)xarr + 8 * (size_t)yarr + 4 * (size_t)yarr + 2;
+    //         | initd(4) [xarr] with dust
+    const size_t ntab = 6 * (size_t)xarr + 6 * (size_t)yarr + 21 * (size_t)xarr + 8 * (size_t)yarr + 4 * (size_t)yarr + 2 +
+                        (P.dust_flag ? 4 * (size_t)xarr : 0);
     PG_CUDA(cudaMalloc(&E.tab, sizeof(double) * ntab));
     std::vector<double> wx(6 * xarr), wy(6 * yarr);
     recon_weights(P.geomx, xa.data(), xarr, wx.data());
@@ -377,6 +432,18 @@ static pg_status engine_setup(Engine& E, const double* dev_xa, const double* dev
     d.visy = t + 21 * xarr + 4 * yarr;
     d.trig = t + 21 * xarr + 8 * yarr;
     PG_CUDA(cudaMemsetAsync(d.trig, 0, sizeof(double) * (4 * (size_t)yarr + 2), E.stream));
+    d.dust = P.dust_flag ? 1 : 0;
+    d.stokes = P.stokes;
+    d.sc_h = P.sc_h;
+    d.dust_rmin = P.d_g_ratio * SMALLR;
+    d.initd = P.dust_flag ? d.trig + 4 * (size_t)yarr + 2 : nullptr;
+    if (P.dust_flag) {
+        std::vector<double> cd(4 * (size_t)xarr);
+        init_cd_table(P, xa.data(), xarr, cd.data());
+        PG_CUDA(cudaMemcpyAsync(const_cast<double*>(d.initd), cd.data(), sizeof(double) * cd.size(),
+                                cudaMemcpyHostToDevice, E.stream));
+        PG_CUDA(cudaStreamSynchronize(E.stream));
+    }
     d.rot = E.rot;
     d.res = E.res;
     d.inc = E.inc;
@@ -420,19 +487,28 @@ static pg_status enqueue_stages(Engine& E) {
     for (int k = 0; k < 2; ++k)
         if ((s = make_cell_maps(E.maps[k], E.buf[k], d.xarr, d.yarr)) != PG_OK) return s;
     if (d.visc && (s = make_vis_maps(E.vmap, E.vis, d.xarr, d.yarr)) != PG_OK) return s;
-    launch_kick1(d, maps(c), E.buf[1 - c], E.vis, E.stream);
+    // dust (dust_flag) takes as many passes as the gas, so dbuf[k] pairs with buf[k]
+    pg_dust* const* D = E.dbuf;
+    const bool dust = d.dust != 0;
+    if (dust)
+        for (int k = 0; k < 2; ++k)
+            if ((s = make_dust_maps(E.dmaps[k], E.dbuf[k], d.xarr, d.yarr)) != PG_OK) return s;
+    launch_kick1(d, maps(c), E.buf[1 - c], E.vis, E.stream, dust ? D[c] : nullptr, dust ? D[1 - c] : nullptr);
     c = 1 - c;
     launch_sweep_x(d, maps(c), E.buf[1 - c], E.stream);
+    if (dust) launch_dsweep_x(d, E.dmaps[c], D[1 - c], E.stream);
     c = 1 - c;
     if (d.ndim > 1) {
         launch_sweep_y(d, maps(c), E.buf[1 - c], E.stream);
+        if (dust) launch_dsweep_y(d, E.dmaps[c], D[1 - c], E.stream);
         c = 1 - c;
     }
     if (d.ndim > 1 && d.orbadv) {
         launch_advect(d, maps(c), E.buf[1 - c], E.stream);
+        if (dust) launch_dadvect(d, E.dmaps[c], D[1 - c], E.stream);
         c = 1 - c;
     }
-    launch_kick2(d, maps(c), E.vmap, E.buf[1 - c], E.stream);
+    launch_kick2(d, maps(c), E.vmap, E.buf[1 - c], E.stream, dust ? D[c] : nullptr, dust ? D[1 - c] : nullptr);
     c = 1 - c;
     E.cur = c;
     PG_CUDA(cudaGetLastError());
@@ -446,6 +522,7 @@ static pg_status engine_create(const pg_params* P, int device, void* stream, Eng
     static bool attrs = false;
     if (!attrs) {
         PG_CUDA(set_kernel_attributes());
+        PG_CUDA(set_dust_attributes());
         attrs = true;
     }
     Engine* E = new Engine();
@@ -605,6 +682,15 @@ pg_status pg_disk_create(const pg_params* P, int device, void* stream, pg_disk**
     if ((s = engine_setup(*E, nullptr, nullptr, nullptr, nullptr)) != PG_OK) return bail(s);
     if ((s = ensure_ghosts(*E, E->buf[0])) != PG_OK) return bail(s);
     if ((s = ensure_ghosts(*E, E->buf[1])) != PG_OK) return bail(s);
+    if (E->P.dust_flag) {
+        // both dust buffers hold init_CD everywhere: the bound-0 radial ghosts keep it
+        if ((e = cudaMalloc(&E->dbuf[0], n * sizeof(pg_dust))) != cudaSuccess ||
+            (e = cudaMalloc(&E->dbuf[1], n * sizeof(pg_dust))) != cudaSuccess)
+            return bail(fail(PG_ERR_CUDA, "cudaMalloc: %s", cudaGetErrorString(e)));
+        launch_dust_init(E->view, E->dbuf[0], E->stream);
+        launch_dust_init(E->view, E->dbuf[1], E->stream);
+        if ((e = cudaGetLastError()) != cudaSuccess) return bail(fail(PG_ERR_CUDA, "%s", cudaGetErrorString(e)));
+    }
     pg_disk* d = new pg_disk{E};
     *out = d;
     return PG_OK;
@@ -646,8 +732,9 @@ pg_status pg_disk_set_state(pg_disk* dk, double t, const double* r, const double
     PG_CUDA(cudaGetLastError());
     PG_CUDA(cudaFreeAsync(stage, E.stream));
     launch_bound(d, E.buf[0], E.stream);
+    if (d.dust) launch_dust_init(d, E.dbuf[0], E.stream);  // a restart's dust is init_CD (the gas file only)
     launch_init_planet(d, E.P, t, E.stream);
-    launch_cfl(d, E.buf[0], E.stream);
+    launch_cfl(d, E.buf[0], E.stream, d.dust ? E.dbuf[0] : nullptr);
     PG_CUDA(cudaGetLastError());
     Scalars h{};
     PG_CUDA(cudaMemcpyAsync(&h, E.sc, sizeof(Scalars), cudaMemcpyDeviceToHost, E.stream));
@@ -684,6 +771,51 @@ pg_status pg_disk_get_state(pg_disk* dk, double* r, double* p, double* u, double
     if (v) PG_CUDA(cudaMemcpyAsync(v, stage + 3 * n, n * sizeof(double), cudaMemcpyDeviceToHost, E.stream));
     PG_CUDA(cudaFreeAsync(stage, E.stream));
     if (t_out) PG_CUDA(cudaMemcpyAsync(t_out, &E.sc->t, sizeof(double), cudaMemcpyDeviceToHost, E.stream));
+    PG_CUDA(cudaStreamSynchronize(E.stream));
+    return PG_OK;
+}
+
+pg_status pg_disk_set_dust(pg_disk* dk, const double* r, const double* u, const double* v) {
+    if (!dk || !r || !u || !v) return fail(PG_ERR_ARG, "null argument");
+    Engine& E = *dk->E;
+    const DiskView& d = E.view;
+    if (!d.dust) return fail(PG_ERR_CONFIG, "the disk has no dust (dust_flag 0)");
+    PG_CUDA(cudaSetDevice(E.device));
+    pg_status s0 = resolve_cur(E);
+    if (s0 != PG_OK) return s0;
+    const size_t n = (size_t)d.xres * d.yres;
+    double* stage = nullptr;
+    PG_CUDA(cudaMallocAsync(&stage, 3 * n * sizeof(double), E.stream));
+    PG_CUDA(cudaMemcpyAsync(stage, r, n * sizeof(double), cudaMemcpyHostToDevice, E.stream));
+    PG_CUDA(cudaMemcpyAsync(stage + n, u, n * sizeof(double), cudaMemcpyHostToDevice, E.stream));
+    PG_CUDA(cudaMemcpyAsync(stage + 2 * n, v, n * sizeof(double), cudaMemcpyHostToDevice, E.stream));
+    launch_dust_fill(d, E.dbuf[E.cur], stage, stage + n, stage + 2 * n, E.stream);
+    PG_CUDA(cudaGetLastError());
+    PG_CUDA(cudaFreeAsync(stage, E.stream));
+    // the CFL rate of the first step includes the dust speeds
+    launch_cfl(d, E.buf[E.cur], E.stream, E.dbuf[E.cur]);
+    PG_CUDA(cudaGetLastError());
+    PG_CUDA(cudaStreamSynchronize(E.stream));
+    return PG_OK;
+}
+
+pg_status pg_disk_get_dust(pg_disk* dk, double* r, double* u, double* v) {
+    if (!dk || !r || !u || !v) return fail(PG_ERR_ARG, "null argument");
+    Engine& E = *dk->E;
+    const DiskView& d = E.view;
+    if (!d.dust) return fail(PG_ERR_CONFIG, "the disk has no dust (dust_flag 0)");
+    PG_CUDA(cudaSetDevice(E.device));
+    pg_status s0 = resolve_cur(E);
+    if (s0 != PG_OK) return s0;
+    const size_t n = (size_t)d.xres * d.yres;
+    double* stage = nullptr;
+    PG_CUDA(cudaMallocAsync(&stage, 3 * n * sizeof(double), E.stream));
+    launch_dust_extract(d, E.dbuf[E.cur], stage, stage + n, stage + 2 * n, E.stream);
+    PG_CUDA(cudaGetLastError());
+    PG_CUDA(cudaMemcpyAsync(r, stage, n * sizeof(double), cudaMemcpyDeviceToHost, E.stream));
+    PG_CUDA(cudaMemcpyAsync(u, stage + n, n * sizeof(double), cudaMemcpyDeviceToHost, E.stream));
+    PG_CUDA(cudaMemcpyAsync(v, stage + 2 * n, n * sizeof(double), cudaMemcpyDeviceToHost, E.stream));
+    PG_CUDA(cudaFreeAsync(stage, E.stream));
     PG_CUDA(cudaStreamSynchronize(E.stream));
     return PG_OK;
 }
@@ -865,6 +997,11 @@ pg_status pg_disk_profile(pg_disk* dk, int nsteps, double end_time, float* ms, i
     for (int k = 0; k < 2; ++k)
         if ((s = make_cell_maps(E.maps[k], E.buf[k], d.xarr, d.yarr)) != PG_OK) return s;
     if (d.visc && (s = make_vis_maps(E.vmap, E.vis, d.xarr, d.yarr)) != PG_OK) return s;
+    pg_dust* const* D = E.dbuf;
+    const bool dust = d.dust != 0;
+    if (dust)
+        for (int k = 0; k < 2; ++k)
+            if ((s = make_dust_maps(E.dmaps[k], E.dbuf[k], d.xarr, d.yarr)) != PG_OK) return s;
     cudaEvent_t ev[7];
     for (auto& x : ev) PG_CUDA(cudaEventCreate(&x));
     for (int step = 0; step < nsteps; ++step) {
@@ -872,23 +1009,26 @@ pg_status pg_disk_profile(pg_disk* dk, int nsteps, double end_time, float* ms, i
         PG_CUDA(cudaEventRecord(ev[0], E.stream));
         launch_time_step(d, E.stream);
         PG_CUDA(cudaEventRecord(ev[1], E.stream));
-        launch_kick1(d, E.maps[c], E.buf[1 - c], E.vis, E.stream);
+        launch_kick1(d, E.maps[c], E.buf[1 - c], E.vis, E.stream, dust ? D[c] : nullptr, dust ? D[1 - c] : nullptr);
         c = 1 - c;
         PG_CUDA(cudaEventRecord(ev[2], E.stream));
         launch_sweep_x(d, E.maps[c], E.buf[1 - c], E.stream);
+        if (dust) launch_dsweep_x(d, E.dmaps[c], D[1 - c], E.stream);
         c = 1 - c;
         PG_CUDA(cudaEventRecord(ev[3], E.stream));
         if (d.ndim > 1) {
             launch_sweep_y(d, E.maps[c], E.buf[1 - c], E.stream);
+            if (dust) launch_dsweep_y(d, E.dmaps[c], D[1 - c], E.stream);
             c = 1 - c;
         }
         PG_CUDA(cudaEventRecord(ev[4], E.stream));
         if (d.ndim > 1 && d.orbadv) {
             launch_advect(d, E.maps[c], E.buf[1 - c], E.stream);
+            if (dust) launch_dadvect(d, E.dmaps[c], D[1 - c], E.stream);
             c = 1 - c;
         }
         PG_CUDA(cudaEventRecord(ev[5], E.stream));
-        launch_kick2(d, E.maps[c], E.vmap, E.buf[1 - c], E.stream);
+        launch_kick2(d, E.maps[c], E.vmap, E.buf[1 - c], E.stream, dust ? D[c] : nullptr, dust ? D[1 - c] : nullptr);
         c = 1 - c;
         PG_CUDA(cudaEventRecord(ev[6], E.stream));
         PG_CUDA(cudaGetLastError());
@@ -925,6 +1065,7 @@ static pg_status grid_engine(pg_grid* dev, Engine** out) {
     if (dev->xres != g_params.xres || dev->yres != g_params.yres)
         return fail(PG_ERR_CONFIG, "grid dimensions differ from the configured parameters");
     if (dev->xbgn != 0) return fail(PG_ERR_CONFIG, "radial domain decomposition is not supported");
+    if (g_params.dust_flag) return fail(PG_ERR_CONFIG, "dust through the pg_grid_* entry points is not supported");
     std::lock_guard<std::mutex> lk(g_mu);
     auto it = g_grids.find(dev->xa);
     if (it != g_grids.end()) {

@@ -19,19 +19,27 @@ struct VisMaps {
     const void* base = nullptr;
     CUtensorMap stencil;   // box {2*34, 10}
 };
+// Tensor maps of one AoS dust buffer (4 doubles per cell).
+struct DustMaps {
+    const void* base = nullptr;
+    CUtensorMap sweep_x;   // box {4*38, 8}
+    CUtensorMap sweep_y;   // box {4*10, 38}
+};
 
 // launch helpers (pg_kernels.cu)
 void launch_init_tables(const DiskView& d, const pg_params& P, double* tab_base, cudaStream_t s);
 void launch_init_xghosts(const DiskView& d, Cell* buf, cudaStream_t s);
 void launch_bound(const DiskView& d, Cell* buf, cudaStream_t s);
-void launch_cfl(const DiskView& d, const Cell* buf, cudaStream_t s);
+void launch_cfl(const DiskView& d, const Cell* buf, cudaStream_t s, const pg_dust* dbuf = nullptr);
 void launch_set_time(const DiskView& d, double t, double dt, cudaStream_t s);
 void launch_time_step(const DiskView& d, cudaStream_t s);
-void launch_kick1(const DiskView& d, const CellMaps& in, Cell* out, double* vis, cudaStream_t s);
+void launch_kick1(const DiskView& d, const CellMaps& in, Cell* out, double* vis, cudaStream_t s,
+                  const pg_dust* din = nullptr, pg_dust* dout = nullptr);
 void launch_sweep_x(const DiskView& d, const CellMaps& in, Cell* out, cudaStream_t s);
 void launch_sweep_y(const DiskView& d, const CellMaps& in, Cell* out, cudaStream_t s);
 void launch_advect(const DiskView& d, const CellMaps& in, Cell* out, cudaStream_t s);
-void launch_kick2(const DiskView& d, const CellMaps& in, const VisMaps& vis, Cell* out, cudaStream_t s);
+void launch_kick2(const DiskView& d, const CellMaps& in, const VisMaps& vis, Cell* out, cudaStream_t s,
+                  const pg_dust* din = nullptr, pg_dust* dout = nullptr);
 void launch_init_planet(const DiskView& d, const pg_params& P, double t, cudaStream_t s);
 void launch_torque(const DiskView& d, const Cell* buf, double* part, int nblocks, cudaStream_t s);
 // compensated sum of n doubles in index order
@@ -48,6 +56,16 @@ void engine_init_planet(Engine* E, double t);
 pg_status make_map3_f32(CUtensorMap* m, const float* base, uint64_t pitch, uint64_t rows, uint64_t planes,
                         uint32_t bx, uint32_t by, uint32_t bz);
 cudaError_t set_kernel_attributes();
+
+// dust passes (pg_dust.cu)
+cudaError_t set_dust_attributes();
+void launch_dsweep_x(const DiskView& d, const DustMaps& in, pg_dust* out, cudaStream_t s);
+void launch_dsweep_y(const DiskView& d, const DustMaps& in, pg_dust* out, cudaStream_t s);
+void launch_dadvect(const DiskView& d, const DustMaps& in, pg_dust* out, cudaStream_t s);
+void launch_dust_init(const DiskView& d, pg_dust* buf, cudaStream_t s);
+void launch_dust_fill(const DiskView& d, pg_dust* buf, const double* r, const double* u, const double* v,
+                      cudaStream_t s);
+void launch_dust_extract(const DiskView& d, const pg_dust* buf, double* r, double* u, double* v, cudaStream_t s);
 
 
 namespace f32 {

@@ -21,6 +21,7 @@
 #include "pg_hydro.cuh"
 #include "pg_internal.h"
 #include "pg_planet.cuh"
+#include "pg_dust.cuh"
 
 namespace pg {
 
@@ -81,7 +82,7 @@ __device__ __forceinline__ Grav gravity(const DiskView& d, int i, double rad, do
 // at the mdt-predicted velocities (sweeps.cu:663-687).
 template <bool VISC>
 __device__ __forceinline__ Cell kick(const DiskView& d, const Cell& C, double ix, const Grav& g, double vx,
-                                     double vy, double mdt, double dt) {
+                                     double vy, double mdt, double dt, double* Tu = nullptr, double* Tv = nullptr) {
     Cell T = C;
     const double ir = VISC ? 1.0 / C.r : 0.0;  // T.r == C.r throughout
     double fx = (d.geomx == 1) ? T.v * T.v * ix : 0.0;
@@ -95,6 +96,8 @@ __device__ __forceinline__ Cell kick(const DiskView& d, const Cell& C, double ix
         T.u = C.u + fx * mdt + g.gx * mdt;
         T.v = C.v + fy * mdt + g.gy * mdt;
         T.w = C.w + fz * mdt + g.gz * mdt;
+        if (Tu) *Tu = T.u;  // the gas velocity the dust drag relaxes towards (sweeps.cu:679-687)
+        if (Tv) *Tv = T.v;
         fx = (d.geomx == 1) ? T.v * T.v * ix : 0.0;
         fy = 0.0;
         if (VISC) {
@@ -159,14 +162,18 @@ __device__ __forceinline__ void gather9(const double* tile, int hx, int hy, cons
     }
 }
 
-__device__ __forceinline__ double signal_rate(const DiskView& d, const Cell& c, int i, int j) {
-    // src/timestep/timestep.cu:46-77 (cell widths as reciprocals)
+__device__ __forceinline__ double signal_rate(const DiskView& d, const Cell& c, int i, int j,
+                                              const DCell* dc = nullptr) {
+    // src/timestep/timestep.cu:46-77 (cell widths as reciprocals); with dust the
+    // dust speeds also bound dt (:64-74)
     const double rad_cyl = (d.geomy == 3) ? d.radx[i] : 1.0;
     const double cs = sqrt(d.gam * c.p / c.r);
     double spd = fabs(c.u) + cs;
+    if (dc) spd = fmax(fabs(dc->u), spd);
     double tmp = fmax(spd * d.idx_x[i], 0.0);
     if (d.ndim > 1) {
         spd = fabs(c.v - rad_cyl * d.frame_omega - d.rot[i]) + cs;
+        if (dc) spd = fmax(fabs(dc->v - rad_cyl * d.frame_omega - d.rot[i]), spd);
         tmp = fmax(spd * (d.idx_y[j] * ((d.geomy == 3) ? d.irad[i] : 1.0)), tmp);
     }
     return tmp;
@@ -523,7 +530,8 @@ __global__ void __launch_bounds__(SW_THREADS, 2)
 template <bool VISC>
 __global__ void __launch_bounds__(ST_THREADS)
     k_kick1(const __grid_constant__ CUtensorMap tm, const DiskView d, Cell* __restrict__ out,
-            double* __restrict__ vis, int ntx, int ntiles) {
+            double* __restrict__ vis, int ntx, int ntiles, const pg_dust* __restrict__ din,
+            pg_dust* __restrict__ dout) {
     extern __shared__ __align__(128) double smem_raw[];
     double* smem = smem_base128(smem_raw);
     auto stage = [&](int n) { return smem + (n & 1) * ST_TILE; };
@@ -584,6 +592,11 @@ __global__ void __launch_bounds__(ST_THREADS)
             const Grav g = gravity(d, i, d.radx[i], tr[0], tr[1], d.trig[4 * d.yarr], sc->planet_cur);
             const Cell Q = kick<VISC>(d, C, d.irad[i], g, vx, vy, 0.0, hdt);
             emit(d, out, i, j, Q);
+            if (din) {  // dust half-kick: drag towards the gas cell C (sweeps.cu:626-707, mdt = 0)
+                const DCell D = dust_kick(d, C, C.u, C.v, load_dust(din, d.xarr, i, j), g.gx, g.gy, g.gz,
+                                          d.irad[i], 0.0, hdt);
+                emit_dust(d, dout, i, j, D);
+            }
         }
         __syncthreads();
     }
@@ -593,7 +606,8 @@ __global__ void __launch_bounds__(ST_THREADS)
 template <bool VISC>
 __global__ void __launch_bounds__(ST_THREADS)
     k_kick2(const __grid_constant__ CUtensorMap tm, const __grid_constant__ CUtensorMap tv, const DiskView d,
-            Cell* __restrict__ out, int ntx, int ntiles) {
+            Cell* __restrict__ out, int ntx, int ntiles, const pg_dust* __restrict__ din,
+            pg_dust* __restrict__ dout) {
     extern __shared__ __align__(128) double smem_raw[];
     double* smem = smem_base128(smem_raw);
     auto stage = [&](int n) { return smem + (n & 1) * ST_TILE; };                   // C with 1 halo
@@ -685,7 +699,8 @@ __global__ void __launch_bounds__(ST_THREADS)
                 }
                 const double* tr = d.trig + 4 * j + 2;
                 const Grav g = gravity(d, i, d.radx[i], tr[0], tr[1], iplx2, pl);
-                Cell Q = kick<VISC>(d, C, d.irad[i], g, vx, vy, hdt, hdt);
+                double Tu = C.u, Tv = C.v;
+                Cell Q = kick<VISC>(d, C, d.irad[i], g, vx, vy, hdt, hdt, &Tu, &Tv);
                 if (d.kill) {
                     // killwave (src/killwave/killwave.cu:48-100): relax towards init_C
                     const double* kt = d.killx + 4 * i;
@@ -705,7 +720,14 @@ __global__ void __launch_bounds__(ST_THREADS)
                     }
                 }
                 if (!(Q.r > 0.0)) atomicOr(&sc->err, 1 << PG_ERR_NAN);
-                vmax = fmax(vmax, signal_rate(d, Q, i, j));
+                if (din) {  // dust corrector half-kick towards the predicted gas velocity (sweeps.cu:663-707)
+                    const DCell D = dust_kick(d, C, Tu, Tv, load_dust(din, d.xarr, i, j), g.gx, g.gy, g.gz,
+                                              d.irad[i], hdt, hdt);
+                    emit_dust(d, dout, i, j, D);
+                    vmax = fmax(vmax, signal_rate(d, Q, i, j, &D));
+                } else {
+                    vmax = fmax(vmax, signal_rate(d, Q, i, j));
+                }
                 emit(d, out, i, j, Q);
             }
             __syncthreads();
@@ -715,13 +737,18 @@ __global__ void __launch_bounds__(ST_THREADS)
 }
 
 // ================================================================ misc
-__global__ void k_cfl(const DiskView d, const Cell* __restrict__ in) {
+__global__ void k_cfl(const DiskView d, const Cell* __restrict__ in, const pg_dust* __restrict__ din) {
     const long long n = (long long)d.xres * d.yres;
     double vmax = 0.0;
     for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
         const int i = NPAD + (int)(k % d.xres);
         const int j = d.ypad + (int)(k / d.xres);
-        vmax = fmax(vmax, signal_rate(d, load_cell(in, d.xarr, i, j), i, j));
+        if (din) {
+            const DCell D = load_dust(din, d.xarr, i, j);
+            vmax = fmax(vmax, signal_rate(d, load_cell(in, d.xarr, i, j), i, j, &D));
+        } else {
+            vmax = fmax(vmax, signal_rate(d, load_cell(in, d.xarr, i, j), i, j));
+        }
     }
     block_max_to<256>(&d.sc->vmax_bits, vmax);
 }
@@ -1019,12 +1046,12 @@ void launch_bound(const DiskView& d, Cell* buf, cudaStream_t s) {
     if (d.bound_lft != 0 || d.bound_rgh != 0) k_bound_x<<<cdiv(d.yarr, 256), 256, 0, s>>>(d, buf);
 }
 
-void launch_cfl(const DiskView& d, const Cell* buf, cudaStream_t s) {
+void launch_cfl(const DiskView& d, const Cell* buf, cudaStream_t s, const pg_dust* dbuf) {
     k_reset_vmax<<<1, 1, 0, s>>>(d.sc);
     const long long n = (long long)d.xres * d.yres;
     unsigned blocks = cdiv(n, 256);
     if (blocks > 148u * 8u) blocks = 148u * 8u;
-    k_cfl<<<blocks, 256, 0, s>>>(d, buf);
+    k_cfl<<<blocks, 256, 0, s>>>(d, buf, dbuf);
 }
 
 void launch_set_time(const DiskView& d, double t, double dt, cudaStream_t s) {
@@ -1073,14 +1100,15 @@ static unsigned persistent_grid(const void* kernel, int threads, size_t smem, lo
     return (unsigned)(g < 1 ? 1 : g);
 }
 
-void launch_kick1(const DiskView& d, const CellMaps& in, Cell* out, double* vis, cudaStream_t s) {
+void launch_kick1(const DiskView& d, const CellMaps& in, Cell* out, double* vis, cudaStream_t s, const pg_dust* din,
+                  pg_dust* dout) {
     const int ntx = (int)cdiv(d.xres, ST_TX), nt = ntx * (int)cdiv(d.yres, ST_TY);
     if (d.visc && d.ndim == 2) {
         const unsigned g = persistent_grid((const void*)k_kick1<true>, ST_THREADS, K1_SMEM, nt);
-        k_kick1<true><<<g, ST_THREADS, K1_SMEM, s>>>(in.stencil, d, out, vis, ntx, nt);
+        k_kick1<true><<<g, ST_THREADS, K1_SMEM, s>>>(in.stencil, d, out, vis, ntx, nt, din, dout);
     } else {
         const unsigned g = persistent_grid((const void*)k_kick1<false>, ST_THREADS, K1_SMEM, nt);
-        k_kick1<false><<<g, ST_THREADS, K1_SMEM, s>>>(in.stencil, d, out, vis, ntx, nt);
+        k_kick1<false><<<g, ST_THREADS, K1_SMEM, s>>>(in.stencil, d, out, vis, ntx, nt, din, dout);
     }
 }
 
@@ -1102,14 +1130,15 @@ void launch_advect(const DiskView& d, const CellMaps& in, Cell* out, cudaStream_
     k_advect<<<g, SW_THREADS, AD_SMEM, s>>>(in.sweep_y, d, out, ntx, nt);
 }
 
-void launch_kick2(const DiskView& d, const CellMaps& in, const VisMaps& vis, Cell* out, cudaStream_t s) {
+void launch_kick2(const DiskView& d, const CellMaps& in, const VisMaps& vis, Cell* out, cudaStream_t s,
+                  const pg_dust* din, pg_dust* dout) {
     const int ntx = (int)cdiv(d.xres, ST_TX), nt = ntx * (int)cdiv(d.yres, ST_TY);
     if (d.visc && d.ndim == 2) {
         const unsigned g = persistent_grid((const void*)k_kick2<true>, ST_THREADS, K5_SMEM, nt);
-        k_kick2<true><<<g, ST_THREADS, K5_SMEM, s>>>(in.stencil, vis.stencil, d, out, ntx, nt);
+        k_kick2<true><<<g, ST_THREADS, K5_SMEM, s>>>(in.stencil, vis.stencil, d, out, ntx, nt, din, dout);
     } else {
         const unsigned g = persistent_grid((const void*)k_kick2<false>, ST_THREADS, K5_SMEM, nt);
-        k_kick2<false><<<g, ST_THREADS, K5_SMEM, s>>>(in.stencil, vis.stencil, d, out, ntx, nt);
+        k_kick2<false><<<g, ST_THREADS, K5_SMEM, s>>>(in.stencil, vis.stencil, d, out, ntx, nt, din, dout);
     }
 }
 
@@ -1117,6 +1146,7 @@ int kernels_per_step(const DiskView& d) {
     int n = 2 /*time, planet trig*/ + 1 /*kick1*/ + 1 /*sweep x*/ + 1 /*kick2*/;
     if (d.ndim > 1) n += 1;
     if (d.ndim > 1 && d.orbadv) n += 1;
+    if (d.dust) n += 1 + (d.ndim > 1 ? 1 : 0) + (d.ndim > 1 && d.orbadv ? 1 : 0);  // dust sweeps, advection
     return n;
 }
 

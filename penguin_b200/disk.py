@@ -49,6 +49,18 @@ class Disk:
         out["t"] = t.value
         return out
 
+    def set_dust(self, dust: dict) -> None:
+        """Interior dust fields r, u, v (yres, xres) of a dust_flag disk; set_state
+        resets the dust to init_CD first, like the reference's restart."""
+        f = {k: np.ascontiguousarray(dust[k], dtype=np.float64) for k in ("r", "u", "v")}
+        check(lib().pg_disk_set_dust(self._h, _dp(f["r"]), _dp(f["u"]), _dp(f["v"])))
+
+    def get_dust(self) -> dict:
+        shape = (self.params.yres, self.params.xres)
+        out = {k: np.empty(shape) for k in ("r", "u", "v")}
+        check(lib().pg_disk_get_dust(self._h, _dp(out["r"]), _dp(out["u"]), _dp(out["v"])))
+        return out
+
     def state_ptr(self) -> int:
         p = ctypes.c_void_p()
         check(lib().pg_disk_state_ptr(self._h, ctypes.byref(p)))

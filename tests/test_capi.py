@@ -59,7 +59,7 @@ def test_params_struct_layout_matches_header(tmp_path):
 
 @pytest.mark.parametrize("bad", [
     dict(ndim=3), dict(EOS_flag=1), dict(xres=31), dict(bound_lft=3), dict(geomx=2), dict(n_planet=2),
-    dict(dust_flag=1), dict(yres=4),
+    dict(dust_flag=1, Stokes=0.0), dict(dust_flag=1, init_flag=1), dict(yres=4),
 ])
 def test_check_params_rejects(bad):
     p = P.planet_disk(64, 192).replace(**bad)
