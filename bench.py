@@ -228,6 +228,45 @@ def measure_ensemble(local, stream, steps):
             "config": "Nr in 32*[4,16], Nphi=3Nr, q log-U[1e-5,3e-3], alpha log-U[1e-4,1e-2], h/r U[0.03,0.08], seed 2024"}
 
 
+DUST_STEPS = 2000
+# FP64 dust passes: the AoS dust cell (4 x FP64) read and written once by each
+# dust sweep and the residual advection; the kicks also read and write it.
+ALGO_BYTES_DUST = {"time": 0, "kick1": 96 + 64, "sweep_x": 80 + 64, "sweep_y": 80 + 64, "advect": 80 + 64,
+                   "kick2": 96 + 64}
+
+
+def measure_dust(local, stream, steps, pk):
+    """Gas + one dust fluid, 768x2048, alpha 1e-4, q 3e-4, dust-to-gas 0.01,
+    Stokes 0.01 and 0.1, plain FP64 form: `steps` steps each from t = 0."""
+    from penguin_b200 import initial as I
+    from penguin_b200 import params as P
+    from penguin_b200.disk import Disk
+
+    out = {}
+    for st in (0.01, 0.1):
+        p = P.dust_disk(stokes=st)
+        d = Disk(p, device=local, stream=stream.cuda_stream)
+        d.set_state(0.0, I.disk_state(p, seed=SEED_DUST))
+        m0 = float(d.get_dust()["r"].sum())
+        d.run(3)
+        d.sync()
+        ms = timed(stream, lambda: d.run(steps))
+        d.check()
+        prof = d.profile(20)
+        dust = d.get_dust()
+        out[f"stokes_{st}"] = {
+            "value": p.cells * steps / (ms / 1000.0), "ms_per_step": ms / steps, "steps": steps,
+            "stage_ms": prof, "roofline": roofline_of(prof, p.cells, ALGO_BYTES_DUST, pk),
+            "gpu_launches": d.kernels_per_step * steps,
+            "dust_sigma_sum_over_initial": float(dust["r"].sum()) / m0,
+        }
+        d.close()
+    return {"workload": "768x2048 gas+dust planet-disk, FP64 form", "dtype": "f64", **out}
+
+
+SEED_DUST = 1234
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -235,7 +274,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--no-forms", action="store_true", help="skip the FP32-mixed and ensemble measurements")
+    ap.add_argument("--no-forms", action="store_true", help="skip the FP32-mixed, ensemble and dust measurements")
+    ap.add_argument("--forms", default="fp32,ensemble,dust",
+                    help="comma list of the extra measurements after the FP64 headline (fp32, ensemble, dust)")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -323,15 +364,19 @@ def main():
 
     barrier()
     g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    h0 = time.perf_counter()
     g0.record(stream)
     check(lib().pg_disk_set_state(disk._h, 0.0, dp(pinned["r"]), dp(pinned["p"]), dp(pinned["u"]), dp(pinned["v"])))
     disk.t, disk.dt = 0.0, None
+    h1 = time.perf_counter()
     disk.step_host(Ke)
+    h2 = time.perf_counter()
     t_out = ctypes.c_double()
     check(lib().pg_disk_get_state(disk._h, dp(out["r"]), dp(out["p"]), dp(out["u"]), dp(out["v"]),
                                   ctypes.byref(t_out)))
     g1.record(stream)
     g1.synchronize()
+    h3 = time.perf_counter()
     e2e_ms = g0.elapsed_time(g1)
     if dist:
         t = torch.tensor([e2e_ms], device="cuda")
@@ -341,6 +386,7 @@ def main():
            "h2d_bytes_per_step": 4 * 8 * cells // Ke,
            "d2h_bytes_per_step": 8 + 4 * 8 * cells // Ke,
            "steps": Ke,
+           "host_ms": {"state_in": 1e3 * (h1 - h0), "loop": 1e3 * (h2 - h1), "state_out": 1e3 * (h3 - h2)},
            "note": "pinned host state in, main.cu host loop (dt read back each step), final state out"}
     if not np.isfinite(out["r"]).all():
         raise RuntimeError("non-finite density after the end-to-end run")
@@ -361,11 +407,15 @@ def main():
         "clocks": clocks,
         "e2e": e2e,
     }
-    if not args.no_forms:
+    forms = set() if args.no_forms else set(x for x in args.forms.split(",") if x)
+    if "fp32" in forms:
         f32 = measure_fp32(p, state, K, W, local, stream, pk)
         f32["over_fp64"] = f32["value"] / (value / world)
         line["fp32_mixed"] = f32
+    if "ensemble" in forms:
         line["ensemble"] = measure_ensemble(local, stream, ENSEMBLE_STEPS)
+    if "dust" in forms:
+        line["dust"] = measure_dust(local, stream, min(DUST_STEPS, max(K, 3)), pk)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(p, state, 0.0)
     if rank == 0:

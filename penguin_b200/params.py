@@ -172,6 +172,14 @@ def planet_disk(nr: int = 1024, nphi: int = 3072, *, q: float = 1.0e-3, alpha: f
     )
 
 
+def dust_disk(nr: int = 768, nphi: int = 2048, *, stokes: float = 0.01, q: float = 3.0e-4,
+              alpha: float = 1.0e-4, d_g_ratio: float = 0.01) -> Params:
+    """The planet-disk with one pressureless dust fluid (dust_flag): constant
+    Stokes number, initial dust-to-gas ratio ``d_g_ratio``, dust velocity from the
+    drift solution (init_CD, src/init/init.cu:351-454)."""
+    return planet_disk(nr, nphi, q=q, alpha=alpha).replace(dust_flag=1, Stokes=stokes, D_G_ratio=d_g_ratio)
+
+
 def reference_disk(nr: int, nphi: int, **kw) -> Params:
     """Planet-disk variant that the reference can run as-is: it has a single
     ``kill_width`` for both damping zones (src/killwave/killwave.cu:30-34), so
