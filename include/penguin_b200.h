@@ -217,6 +217,43 @@ int pg_ens_kernels_per_step(const pg_ens* e);
    1 kick1, 2 sweep_x, 3 sweep_y, 4 advect, 5 kick2). */
 pg_status pg_ens_profile(pg_ens* e, int nsteps, double end_time, float* ms, int nslot);
 
+/* ---------------------------------------------------------------- adjoint
+ * Gradient of a loss on the surface density after N steps of the FP64 step
+ * with respect to the initial surface density field and (q, alpha, h/r).  No
+ * reference counterpart: the reference has no derivative code.  Covers 2D
+ * polar isothermal disks with analytic radial boundaries, no wave damping and
+ * at most one planet on a circular orbit (pg_adj_check_params).  The run
+ * starts from Sigma0 with v_r = 0 and v_phi = the disk's init_C; dt is the
+ * CFL schedule of the recorded forward run (frozen for differentiation).
+ * Device arrays are interior fields of xres*yres doubles, index i + xres*j. */
+typedef struct pg_adj pg_adj;
+pg_status pg_adj_check_params(const pg_params* P);
+pg_status pg_adj_create(const pg_params* P, int device, void* stream, int checkpoint_every, pg_adj** out);
+pg_status pg_adj_destroy(pg_adj* a);
+/* new (q, alpha, h/r): the disk's tables and their derivatives are rebuilt; a
+   recorded schedule stays valid for replay */
+pg_status pg_adj_set_params(pg_adj* a, double q, double alpha, double h);
+/* nsteps of main.cu's loop from Sigma0 at t0; replay = 0 records the CFL dt
+   schedule, 1 reuses it (finite-difference checks); Sigma after the run into
+   sigma_out (device, may be NULL) */
+pg_status pg_adj_forward(pg_adj* a, const double* sigma0, double t0, int nsteps, int replay, double* sigma_out);
+/* dL/dSigma (device) -> dL/dSigma0 (device, may be NULL), dL/d(q, alpha, h)
+   (host double[3], may be NULL) for the last forward run */
+pg_status pg_adj_backward(pg_adj* a, const double* grad_out, double* grad_sigma0, double* grad_theta);
+/* test support: one step with dt from the newest state; the adjoint's
+   restatement of each pass against the production kernels (max relative
+   difference per pass: kick1, sweep_x, sweep_y, advect, kick2) */
+pg_status pg_adj_model_error(pg_adj* a, double dt, double* err5);
+/* test support: adjoint dot-product test of every pass over one step with dt
+   from the newest state.  dir, lam: device, 5 interior planes (Sigma, v_r,
+   v_phi, kick1's force x, y).  out10[2p] = <lam, J_p dir> (forward mode),
+   out10[2p+1] = <J_p^T lam, dir> (the adjoint), p = kick1, sweep_x, sweep_y,
+   advect, kick2 */
+pg_status pg_adj_dot_test(pg_adj* a, double dt, const double* dir, const double* lam, double* out10);
+pg_status pg_adj_schedule(const pg_adj* a, double* dts, int n);
+int pg_adj_steps(const pg_adj* a);
+long long pg_adj_device_bytes(const pg_adj* a);
+
 #ifdef __cplusplus
 }
 #endif

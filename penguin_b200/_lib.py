@@ -28,6 +28,8 @@ EXPORTS = [
     "pg_ens_check_params", "pg_ens_create", "pg_ens_destroy", "pg_ens_size", "pg_ens_dims", "pg_ens_set_state",
     "pg_ens_get_state", "pg_ens_run", "pg_ens_sync", "pg_ens_clock", "pg_ens_planet", "pg_ens_check",
     "pg_ens_totals", "pg_ens_torque", "pg_ens_kernels_per_step", "pg_ens_profile",
+    "pg_adj_check_params", "pg_adj_create", "pg_adj_destroy", "pg_adj_set_params", "pg_adj_forward",
+    "pg_adj_backward", "pg_adj_model_error", "pg_adj_dot_test", "pg_adj_schedule", "pg_adj_steps", "pg_adj_device_bytes",
 ]
 
 
@@ -97,6 +99,17 @@ def lib() -> ctypes.CDLL:
         "pg_ens_check": (i, [vp]),
         "pg_ens_totals": (i, [vp, i, dp, dp]),
         "pg_ens_torque": (i, [vp, i, dp]),
+        "pg_adj_check_params": (i, [PP]),
+        "pg_adj_create": (i, [PP, i, vp, i, ctypes.POINTER(vp)]),
+        "pg_adj_destroy": (i, [vp]),
+        "pg_adj_set_params": (i, [vp, d, d, d]),
+        "pg_adj_forward": (i, [vp, vp, d, i, i, vp]),
+        "pg_adj_backward": (i, [vp, vp, vp, dp]),
+        "pg_adj_model_error": (i, [vp, d, dp]),
+        "pg_adj_dot_test": (i, [vp, d, vp, vp, dp]),
+        "pg_adj_schedule": (i, [vp, dp, i]),
+        "pg_adj_steps": (i, [vp]),
+        "pg_adj_device_bytes": (ctypes.c_longlong, [vp]),
         "pg_ens_kernels_per_step": (i, [vp]),
         "pg_ens_profile": (i, [vp, i, d, ctypes.POINTER(ctypes.c_float), i]),
     }

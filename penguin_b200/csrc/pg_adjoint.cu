@@ -1,0 +1,1157 @@
+// Discrete adjoint of the FP64 step for the gradient of a loss on the surface
+// density after N steps with respect to the initial surface density field and
+// the disk parameters theta = (q, alpha, h/r).
+//
+// The forward model is the production FP64 step (pg_engine.cu, pg_kernels.cu)
+// replayed with a fixed dt schedule; every pass input is recorded per step of a
+// segment between checkpoints.  The adjoint of a pass is a gather: for each
+// input cell and field, the pass outputs whose stencil contains the cell are
+// re-evaluated with a dual number seeded on that input, and their derivatives
+// are contracted with the output adjoint lambda.  The evaluators below restate
+// the passes (apply_source_terms with the viscous force, sweepx/sweepy with
+// the orbital shift, the residual advection; src/solver/sweeps.cu:218-456,
+// 597-711, src/viscosity/viscosity.cu, src/orbit/orbit.cu:17-99,
+// src/solver/advection/advection.cu:1-173) per output cell on top of the same
+// templated building blocks the sweeps use (pg_hydro.cuh), so the derivative
+// is that of the step as computed, along the branch each limiter, upwind
+// choice, HLLC wave sign and floor takes.
+//
+// The state variables are (Sigma, v_r, v_phi) per interior cell; the pressure
+// of the isothermal disk is tied to them, p = cs^2(r) Sigma, as every update
+// of the forward step writes it.  The parameter derivatives enter through the
+// per-radius tables (cs^2, nu, the bound-0 ghost state init_C, orb_rot and
+// with it the residual speed) and the planet (mass ramp ~ q, smoothing ~ h),
+// whose derivatives are computed on the host.  dt is frozen (the schedule of
+// the recorded forward run), as the CFL minimum is not differentiable.
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "pg_common.cuh"
+#include "pg_dual.cuh"
+#include "pg_hydro.cuh"
+#include "pg_internal.h"
+#include "pg_planet.cuh"
+
+namespace pg {
+namespace adj {
+
+using ad::Dual;
+
+// theta-derivative tables, per parameter: [NTAB][xarr] each
+enum Tab { T_CS2 = 0, T_NU = 1, T_P0 = 2, T_U0 = 3, T_V0 = 4, T_ROT = 5, NTAB = 6 };
+enum Field { F_R = 0, F_U = 1, F_V = 2, F_VX = 3, F_VY = 4 };
+
+struct Args {
+    DiskView d;                // tables of the disk (production layout)
+    const Cell* in;            // pass input, all cells
+    const double* vis;         // kick1's viscous force density (2 per cell), input of kick2
+    pg_body pl[2];             // planet of the first half-kick, of the second
+    double dmdq[2];            // d m / d q of the two planets
+    double drsdh;              // d rs / d h
+    const double* res;         // residual speed per radius
+    const int* inc;            // orbital shift per radius
+    double dt;
+    const double* lam;         // adjoint of the pass output: 3 interior planes (Sigma, v_r, v_phi)
+    const double* lamv;        // adjoint of kick1's force output: 2 interior planes
+    double* lam_in;            // adjoint of the pass input
+    double* lamv_in;           // kick2: adjoint of kick1's force
+    const double* dtab;        // [3][NTAB][xarr]
+    double* gth;               // 3 accumulators
+    const double* dir;         // direction mode (Seed.i == DIRECTION): 5 interior planes r, u, v, vis x, vis y
+};
+
+constexpr int DIRECTION = -2;  // Seed.i: every input cell moves along Args.dir (forward mode)
+
+struct Seed {
+    int i, j, k;  // interior cell (array indices) and field seeded, or i = -1
+    int th;       // parameter seeded, or -1
+};
+
+template <class T>
+struct S3 {
+    T r, p, u, v;
+};
+
+__device__ __forceinline__ int wrap_row(const DiskView& d, int j) {
+    if (j < d.ypad) return j + d.yres;
+    if (j >= d.ypad + d.yres) return j - d.yres;
+    return j;
+}
+__device__ __forceinline__ size_t pidx(const DiskView& d, int i, int j) {  // interior plane index
+    return (size_t)(i - NPAD) + (size_t)d.xres * (j - d.ypad);
+}
+__device__ __forceinline__ size_t plane(const DiskView& d) { return (size_t)d.xres * d.yres; }
+
+template <class T>
+__device__ __forceinline__ void set_d(T&, double) {}
+__device__ __forceinline__ void set_d(Dual& x, double v) { x.d = v; }
+
+// theta-dependent table entry
+template <class T>
+__device__ __forceinline__ T tab(const Args& a, const Seed& s, int which, const double* val, int i) {
+    T o = val[i];
+    if (s.th >= 0) set_d(o, a.dtab[((size_t)s.th * NTAB + which) * a.d.xarr + i]);
+    return o;
+}
+
+// One input cell with its derivative along the seed.  Radial ghosts (bound 0)
+// hold init_C; periodic ghost rows are images of interior rows.
+template <class T>
+__device__ __forceinline__ S3<T> ld(const Args& a, const Seed& s, int i, int j) {
+    const DiskView& d = a.d;
+    const Cell c = load_cell(a.in, d.xarr, i, j);
+    S3<T> o{c.r, c.p, c.u, c.v};
+    if (i < NPAD || i >= NPAD + d.xres) {
+        if (s.th >= 0) {
+            set_d(o.p, a.dtab[((size_t)s.th * NTAB + T_P0) * d.xarr + i]);
+            set_d(o.u, a.dtab[((size_t)s.th * NTAB + T_U0) * d.xarr + i]);
+            set_d(o.v, a.dtab[((size_t)s.th * NTAB + T_V0) * d.xarr + i]);
+        }
+        return o;
+    }
+    if (s.th >= 0) {
+        set_d(o.p, a.dtab[((size_t)s.th * NTAB + T_CS2) * d.xarr + i] * c.r);
+    } else if (s.i == DIRECTION) {
+        const size_t m = pidx(d, i, wrap_row(d, j)), P = plane(d);
+        set_d(o.r, a.dir[m]);
+        set_d(o.p, d.cs2x[i] * a.dir[m]);
+        set_d(o.u, a.dir[P + m]);
+        set_d(o.v, a.dir[2 * P + m]);
+    } else if (s.i == i && s.j == wrap_row(d, j)) {
+        if (s.k == F_R) {
+            set_d(o.r, 1.0);
+            set_d(o.p, d.cs2x[i]);
+        } else if (s.k == F_U) {
+            set_d(o.u, 1.0);
+        } else if (s.k == F_V) {
+            set_d(o.v, 1.0);
+        }
+    }
+    return o;
+}
+
+// kick1's viscous force at a cell (an input of kick2)
+template <class T>
+__device__ __forceinline__ void ld_vis(const Args& a, const Seed& s, int i, int j, T& vx, T& vy) {
+    const size_t m = (size_t)i + (size_t)a.d.xarr * j;
+    vx = a.vis[2 * m];
+    vy = a.vis[2 * m + 1];
+    if (s.th < 0 && s.i == DIRECTION) {
+        if (i >= NPAD && i < NPAD + a.d.xres) {
+            const size_t mm = pidx(a.d, i, wrap_row(a.d, j)), P = plane(a.d);
+            set_d(vx, a.dir[3 * P + mm]);
+            set_d(vy, a.dir[4 * P + mm]);
+        }
+    } else if (s.th < 0 && s.i == i && s.j == wrap_row(a.d, j)) {
+        if (s.k == F_VX) set_d(vx, 1.0);
+        else if (s.k == F_VY) set_d(vy, 1.0);
+    }
+}
+
+// ---------------------------------------------------------------- sweeps
+// Both edge states of cell c of a pencil (src/solver/sweeps.cu:290-330, 390-430):
+// DIR 0 radial (row q), DIR 1 azimuthal (column q).
+template <class T, int DIR>
+__device__ __forceinline__ void edge_states(const Args& a, const Seed& s, int c, int q, HalfT<T>& left,
+                                            HalfT<T>& right) {
+    const DiskView& d = a.d;
+    T r[5], p[5], u[5], v[5];
+    double rad = 1.0, irad_q = 1.0;
+    T rot = 0.0;
+    if (DIR == 1) {
+        rad = d.radx[q];
+        irad_q = d.irad[q];
+        rot = tab<T>(a, s, T_ROT, d.rot, q);
+    }
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+        const S3<T> C = (DIR == 0) ? ld<T>(a, s, c - 2 + k, q) : ld<T>(a, s, q, c - 2 + k);
+        r[k] = C.r;
+        p[k] = C.p;
+        if (DIR == 0) {
+            u[k] = C.u;
+            v[k] = C.v * d.radx[c - 2 + k];  // angular momentum (geomx 1)
+        } else {
+            u[k] = C.v - rot;
+            u[k] -= rad * d.frame_omega;
+            v[k] = C.u;  // the reference's w slot carries v_r in the azimuthal sweep (w = 0 in 2D)
+        }
+    }
+    const T cs0 = sqrt(d.gam * p[2] / r[2]);
+    const T flat = flatten<T>(1.0 / cs0, p[2], p[0], p[1], p[3], p[4], u[1], u[2], u[3]);
+    const double* wt = ((DIR == 0) ? d.wx : d.wy) + 6 * c;
+    const double* fa = (DIR == 0) ? d.xa : d.ya;
+    const double idx = ((DIR == 0) ? d.idx_x : d.idx_y)[c];
+    const ParT<T> R = recon<T>(wt, r[0], r[1], r[2], r[3], r[4], flat);
+    const ParT<T> P = recon<T>(wt, p[0], p[1], p[2], p[3], p[4], flat);
+    const ParT<T> U = recon<T>(wt, u[0], u[1], u[2], u[3], u[4], flat);
+    const ParT<T> V = recon<T>(wt, v[0], v[1], v[2], v[3], v[4], flat);
+    const ParT<T> Z{T(0.0), T(0.0), T(0.0)};
+    const double xl = fa[c], xr = fa[c + 1];
+    const double sdt = (DIR == 0) ? a.dt : a.dt * irad_q;
+    // DIR 0: V is r v_phi (the v slot); DIR 1: V is v_r (the w slot), the v slot is w = 0
+    if (DIR == 0) {
+        left = state_at_left_edge<T>(d.gam, xl, idx, sdt, cs0, r[2], p[2], u[2], R, P, U, V, Z);
+        right = state_at_right_edge<T>(d.gam, xl, xr, idx, sdt, cs0, r[2], p[2], u[2], R, P, U, V, Z);
+    } else {
+        left = state_at_left_edge<T>(d.gam, xl, idx, sdt, cs0, r[2], p[2], u[2], R, P, U, Z, V);
+        right = state_at_right_edge<T>(d.gam, xl, xr, idx, sdt, cs0, r[2], p[2], u[2], R, P, U, Z, V);
+    }
+}
+
+// HLLC flux at face f (between cells f-1 and f) of a pencil.
+template <class T, int DIR>
+__device__ __forceinline__ FluxT<T> face_flux(const Args& a, const Seed& s, int f, int q) {
+    HalfT<T> l0, r0, l1, r1;
+    edge_states<T, DIR>(a, s, f - 1, q, l0, r0);
+    edge_states<T, DIR>(a, s, f, q, l1, r1);
+    return hllc<T>(0, a.d.ie, a.d.gam, r0, l1);
+}
+
+// update_Cell (sweeps.cu:218-261), isothermal: the velocity floor branch and
+// p = cs^2 Sigma afterwards
+template <class T>
+__device__ __forceinline__ S3<T> update_iso(S3<T> Q, T Dr, T Du, T Dv) {
+    const T r_min = fmax(Q.r * 1.0e-10, T(SMALLR));
+    const T u_old = Q.u, v_old = Q.v;
+    Q.u *= Q.r;
+    Q.v *= Q.r;
+    Q.r += Dr;
+    Q.u += Du;
+    Q.v += Dv;
+    const T ir = 1.0 / Q.r;
+    Q.u *= ir;
+    Q.v *= ir;
+    if (Q.r < r_min) {
+        Q.r = r_min;
+        Q.u = u_old;
+        Q.v = v_old;
+    }
+    return Q;
+}
+
+// radial sweep, output cell (i, j)
+template <class T>
+__device__ __forceinline__ S3<T> eval_sx(const Args& a, const Seed& s, int i, int j) {
+    const DiskView& d = a.d;
+    const FluxT<T> F0 = face_flux<T, 0>(a, s, i, j), F1 = face_flux<T, 0>(a, s, i + 1, j);
+    const double g0 = d.xa[i], g1 = d.xa[i + 1];
+    const T du = 0.5 * (g0 + g1) * (F0.pres - F1.pres);
+    T Dr = F0.r * g0 - F1.r * g1;
+    T Du = (F0.u * g0 - F1.u * g1) + du;
+    T Dv = F0.v * g0 - F1.v * g1;
+    const double f = a.dt * d.ixv[i];
+    Dr *= f;
+    Du *= f;
+    Dv *= f;
+    Dv *= d.irad[i];
+    return update_iso<T>(ld<T>(a, s, i, j), Dr, Du, Dv);
+}
+
+// azimuthal sweep, the cell that the orbital shift moves to row j + inc (pre-shift row j)
+template <class T>
+__device__ __forceinline__ S3<T> eval_sy(const Args& a, const Seed& s, int i, int j) {
+    const DiskView& d = a.d;
+    const FluxT<T> F0 = face_flux<T, 1>(a, s, j, i), F1 = face_flux<T, 1>(a, s, j + 1, i);
+    const T du = 0.5 * (1.0 + 1.0) * (F0.pres - F1.pres);
+    T Dr = F0.r * 1.0 - F1.r * 1.0;
+    T Du = (F0.u * 1.0 - F1.u * 1.0) + du;  // v_phi residual flux
+    T Dw = F0.w * 1.0 - F1.w * 1.0;         // v_r flux (w slot)
+    const double f = a.dt * d.iyv[j] * d.irad[i];
+    Dr *= f;
+    Du *= f;
+    Dw *= f;
+    const T rot = tab<T>(a, s, T_ROT, d.rot, i);
+    Du += (rot + d.radx[i] * d.frame_omega) * Dr;
+    return update_iso<T>(ld<T>(a, s, i, j), Dr, Dw, Du);
+}
+
+// residual advection (advection.cu:20-105), output cell (i, j)
+template <class T>
+__device__ __forceinline__ void adv_face(const Args& a, const Seed& s, int i, int f, T speed, T& fr, T& fu, T& fw) {
+    const DiskView& d = a.d;
+    const int c = (val(speed) > 0.0) ? f - 1 : f;  // the upwind cell
+    T r[5], u[5], w[5];
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+        const S3<T> C = ld<T>(a, s, i, c - 2 + k);
+        r[k] = C.r;
+        u[k] = C.v;  // v_phi (u slot of the azimuthal pencil)
+        w[k] = C.u;  // v_r (w slot)
+    }
+    const double* wt = d.wy + 6 * c;
+    const ParT<T> R = recon<T>(wt, r[0], r[1], r[2], r[3], r[4], T(0.0));
+    const ParT<T> U = recon<T>(wt, u[0], u[1], u[2], u[3], u[4], T(0.0));
+    const ParT<T> W = recon<T>(wt, w[0], w[1], w[2], w[3], w[4], T(0.0));
+    const double xl = d.ya[c], xr = d.ya[c + 1];
+    const double sdt = a.dt * d.irad[i];
+    const double idx = d.idx_y[c];
+    T vr, vu, vw;
+    if (val(speed) > 0.0) {
+        const T x0 = xr - speed * sdt;
+        const FracT<T> q = frac_right(lim01((x0 - xl) * idx));
+        vr = aveR(q, R);
+        vu = aveR(q, U) * vr;
+        vw = aveR(q, W) * vr;
+    } else {
+        const T x0 = xl - speed * sdt;
+        const FracT<T> q = frac_left(lim01((x0 - xl) * idx));
+        vr = aveL(q, R);
+        vu = aveL(q, U) * vr;
+        vw = aveL(q, W) * vr;
+    }
+    fr = vr * speed;
+    fu = vu * speed;
+    fw = vw * speed;
+}
+
+template <class T>
+__device__ __forceinline__ S3<T> eval_adv(const Args& a, const Seed& s, int i, int j) {
+    const DiskView& d = a.d;
+    T speed = a.res[i];
+    if (s.th >= 0) set_d(speed, a.dtab[((size_t)s.th * NTAB + T_ROT) * d.xarr + i]);  // res = rot - shift dy/dt
+    T fr0, fu0, fw0, fr1, fu1, fw1;
+    adv_face<T>(a, s, i, j, speed, fr0, fu0, fw0);
+    adv_face<T>(a, s, i, j + 1, speed, fr1, fu1, fw1);
+    T Dr = fr0 * 1.0 - fr1 * 1.0, Du = fu0 * 1.0 - fu1 * 1.0, Dw = fw0 * 1.0 - fw1 * 1.0;
+    double f = a.dt * d.iyv[j];
+    Dr *= f;
+    Du *= f;
+    Dw *= f;
+    f = d.irad[i];
+    Dr *= f;
+    Du *= f;
+    Dw *= f;
+    S3<T> Q = ld<T>(a, s, i, j);
+    Q.u *= Q.r;
+    Q.v *= Q.r;
+    Q.r += Dr;
+    Q.u += Dw;
+    Q.v += Du;
+    const T ir = 1.0 / Q.r;
+    Q.u *= ir;
+    Q.v *= ir;
+    return Q;
+}
+
+// --------------------------------------------------------------- kicks
+// Star + planet gravity (forces.cu:41-58, 182-327), the planet's mass and
+// smoothing length as scalars of type T
+template <class T>
+__device__ __forceinline__ void gravity(const Args& a, const Seed& s, int i, int j, int which, T& gx, T& gy) {
+    const DiskView& d = a.d;
+    const pg_body& p = a.pl[which];
+    gx = d.gstar[i];
+    gy = 0.0;
+    if (d.nplanet > 0) {
+        T plm = p.m, rs = p.rs;
+        if (s.th == 0) set_d(plm, a.dmdq[which]);
+        if (s.th == 2) set_d(rs, a.drsdh);
+        double sinfac, cosfac;
+        sincos(d.ycj[j] - (p.y + 0.0 * p.vy), &sinfac, &cosfac);
+        const double iplx2 = 1.0 / p.x / p.x;
+        const double rad = d.radx[i], plx = p.x;
+        const T Rp = sqrt(rad * rad + plx * plx - 2.0 * plx * rad * cosfac + rs * rs);
+        const T ir = 1.0 / Rp;
+        const T rs_fac = ir * ir * ir;
+        gx += -plm * (rad - plx * cosfac) * rs_fac - plm * cosfac * iplx2;
+        gy += -plm * plx * sinfac * rs_fac + plm * sinfac * iplx2;
+    }
+}
+
+// apply_source_terms for one cell (sweeps.cu:597-711), geomx 1, 2D
+template <class T>
+__device__ __forceinline__ S3<T> kick(const DiskView& d, const S3<T>& C, T gx, T gy, T vx, T vy, double ix,
+                                      double mdt, double dt) {
+    const T ir = d.visc ? 1.0 / C.r : T(0.0);
+    T fx = C.v * C.v * ix;
+    T fy = 0.0;
+    if (d.visc) {
+        fx += vx * ir;
+        fy += vy * ir;
+    }
+    if (mdt != 0.0) {
+        const T tv = C.v + fy * mdt + gy * mdt;
+        fx = tv * tv * ix;
+        fy = 0.0;
+        if (d.visc) {
+            fx += vx * ir;
+            fy += vy * ir;
+        }
+    }
+    S3<T> o = C;
+    o.u = C.u + fx * dt + gx * dt;
+    o.v = C.v + fy * dt + gy * dt;
+    return o;
+}
+
+// viscous force of the 3x3 stencil of states X around (i, j) (viscosity.cu:9-194)
+template <class T>
+__device__ __forceinline__ void stress(const Args& a, const Seed& s, int i, int j, const S3<T>* X, T& vx, T& vy) {
+    const DiskView& d = a.d;
+    T nu[3], u[9], v[9], nr[9];
+#pragma unroll
+    for (int n = 0; n < 3; ++n) nu[n] = tab<T>(a, s, T_NU, d.nux, i + n - 1);
+#pragma unroll
+    for (int n = 0; n < 9; ++n) {
+        nr[n] = X[n].r * nu[n % 3];
+        u[n] = X[n].u;
+        v[n] = X[n].v;
+    }
+    viscous<T>(d.visx + 5 * i, d.visy + 4 * j, u, v, nr, vx, vy);
+}
+
+__device__ __forceinline__ void nb(int n, int& dx, int& dy) {  // stencil order of viscous()
+    dx = (n % 3) - 1;
+    dy = (n < 3) ? 0 : (n < 6 ? -1 : 1);
+}
+
+// kick1: the first half-kick and the viscous force it leaves for kick2
+template <class T>
+__device__ __forceinline__ S3<T> eval_k1(const Args& a, const Seed& s, int i, int j, T& vx, T& vy) {
+    const DiskView& d = a.d;
+    vx = 0.0;
+    vy = 0.0;
+    if (d.visc) {
+        S3<T> X[9];
+#pragma unroll
+        for (int n = 0; n < 9; ++n) {
+            int dx, dy;
+            nb(n, dx, dy);
+            X[n] = ld<T>(a, s, i + dx, j + dy);
+        }
+        stress<T>(a, s, i, j, X, vx, vy);
+    }
+    T gx, gy;
+    gravity<T>(a, s, i, j, 0, gx, gy);
+    return kick<T>(d, ld<T>(a, s, i, j), gx, gy, vx, vy, d.irad[i], 0.0, 0.5 * a.dt);
+}
+
+// kick2: predictor on the 3x3 stencil with kick1's force, the force of the
+// predicted state, corrector (sweeps.cu:663-729, solve.cu:266-275)
+template <class T>
+__device__ __forceinline__ S3<T> eval_k2(const Args& a, const Seed& s, int i, int j) {
+    const DiskView& d = a.d;
+    const double hdt = 0.5 * a.dt;
+    T vx = 0.0, vy = 0.0;
+    if (d.visc) {
+        S3<T> X[9];
+#pragma unroll
+        for (int n = 0; n < 9; ++n) {
+            int dx, dy;
+            nb(n, dx, dy);
+            const int ii = i + dx, jj = j + dy;
+            X[n] = ld<T>(a, s, ii, jj);
+            if (ii >= NPAD && ii < NPAD + d.xres) {  // radial ghosts keep init_C (boundx2, bound 0)
+                T ox, oy, gx, gy;
+                ld_vis<T>(a, s, ii, jj, ox, oy);
+                gravity<T>(a, s, ii, jj, 1, gx, gy);
+                X[n] = kick<T>(d, X[n], gx, gy, ox, oy, d.irad[ii], hdt, hdt);
+            }
+        }
+        stress<T>(a, s, i, j, X, vx, vy);
+    }
+    T gx, gy;
+    gravity<T>(a, s, i, j, 1, gx, gy);
+    return kick<T>(d, ld<T>(a, s, i, j), gx, gy, vx, vy, d.irad[i], hdt, hdt);
+}
+
+// --------------------------------------------------------------- passes
+enum Pass { P_K1 = 0, P_SX = 1, P_SY = 2, P_ADV = 3, P_K2 = 4 };
+
+__device__ __forceinline__ int sy_pre_row(const DiskView& d, const int* inc, int i, int jo) {
+    if (!d.orbadv) return jo;
+    int j = (jo - d.ypad - inc[i]) % d.yres;
+    if (j < 0) j += d.yres;
+    return j + d.ypad;
+}
+__device__ __forceinline__ int sy_post_row(const DiskView& d, const int* inc, int i, int j) {
+    if (!d.orbadv) return j;
+    int js = (j - d.ypad + inc[i]) % d.yres;
+    if (js < 0) js += d.yres;
+    return js + d.ypad;
+}
+
+// Pass output at interior cell (i, jo) (post-shift row for the azimuthal sweep),
+// contracted with the output adjoint: sum over fields of lambda * d(out).
+template <int PASS>
+__device__ __forceinline__ double contract(const Args& a, const Seed& s, int i, int jo) {
+    const DiskView& d = a.d;
+    const size_t P = plane(d), m = pidx(d, i, jo);
+    S3<Dual> q;
+    double extra = 0.0;
+    if (PASS == P_K1) {
+        Dual vx, vy;
+        q = eval_k1<Dual>(a, s, i, jo, vx, vy);
+        if (d.visc) extra = a.lamv[m] * vx.d + a.lamv[P + m] * vy.d;
+    } else if (PASS == P_SX) {
+        q = eval_sx<Dual>(a, s, i, jo);
+    } else if (PASS == P_SY) {
+        q = eval_sy<Dual>(a, s, i, sy_pre_row(d, a.inc, i, jo));
+    } else if (PASS == P_ADV) {
+        q = eval_adv<Dual>(a, s, i, jo);
+    } else {
+        q = eval_k2<Dual>(a, s, i, jo);
+    }
+    return a.lam[m] * q.r.d + a.lam[P + m] * q.u.d + a.lam[2 * P + m] * q.v.d + extra;
+}
+
+constexpr int ADJ_THREADS = 128;
+
+// lambda_in(cell, field) = sum over the outputs whose stencil holds the cell.
+template <int PASS>
+__global__ void __launch_bounds__(ADJ_THREADS) k_adj_state(const Args a) {
+    const DiskView& d = a.d;
+    const long long n = (long long)d.xres * d.yres;
+    const size_t P = plane(d);
+    for (long long m = blockIdx.x * (long long)blockDim.x + threadIdx.x; m < n; m += (long long)gridDim.x * blockDim.x) {
+        const int i = NPAD + (int)(m % d.xres), j = d.ypad + (int)(m / d.xres);
+        const int nk = (PASS == P_K2 && d.visc) ? 5 : 3;
+        for (int k = 0; k < nk; ++k) {
+            const Seed s{i, j, k, -1};
+            double acc = 0.0;
+            if (PASS == P_SX) {
+                for (int o = max(i - 3, NPAD); o <= min(i + 3, NPAD + d.xres - 1); ++o) acc += contract<PASS>(a, s, o, j);
+            } else if (PASS == P_SY) {
+                for (int dj = -3; dj <= 3; ++dj)
+                    acc += contract<PASS>(a, s, i, sy_post_row(d, a.inc, i, wrap_row(d, j + dj)));
+            } else if (PASS == P_ADV) {
+                for (int dj = -3; dj <= 3; ++dj) acc += contract<PASS>(a, s, i, wrap_row(d, j + dj));
+            } else {
+                for (int di = -1; di <= 1; ++di) {
+                    const int o = i + di;
+                    if (o < NPAD || o >= NPAD + d.xres) continue;
+                    for (int dj = -1; dj <= 1; ++dj) acc += contract<PASS>(a, s, o, wrap_row(d, j + dj));
+                }
+            }
+            if (k < 3) a.lam_in[(size_t)k * P + (size_t)m] = acc;
+            else a.lamv_in[(size_t)(k - 3) * P + (size_t)m] = acc;
+        }
+    }
+}
+
+// d loss / d theta: each output cell contracted with its derivative along
+// every parameter, summed over the grid.
+template <int PASS>
+__global__ void __launch_bounds__(ADJ_THREADS) k_adj_theta(const Args a) {
+    const DiskView& d = a.d;
+    const long long n = (long long)d.xres * d.yres;
+    double acc[3] = {0.0, 0.0, 0.0};
+    for (long long m = blockIdx.x * (long long)blockDim.x + threadIdx.x; m < n; m += (long long)gridDim.x * blockDim.x) {
+        const int i = NPAD + (int)(m % d.xres), j = d.ypad + (int)(m / d.xres);
+#pragma unroll 1
+        for (int th = 0; th < 3; ++th) acc[th] += contract<PASS>(a, Seed{-1, -1, -1, th}, i, j);
+    }
+    __shared__ double red[3][ADJ_THREADS];
+    for (int th = 0; th < 3; ++th) red[th][threadIdx.x] = acc[th];
+    __syncthreads();
+    for (int w = ADJ_THREADS / 2; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w)
+            for (int th = 0; th < 3; ++th) red[th][threadIdx.x] += red[th][threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        for (int th = 0; th < 3; ++th) atomicAdd(&a.gth[th], red[th][0]);
+}
+
+// <lambda, J dir> of a pass by forward mode (the adjoint dot-product test)
+template <int PASS>
+__global__ void __launch_bounds__(ADJ_THREADS) k_adj_jvp(const Args a, double* out) {
+    const DiskView& d = a.d;
+    const long long n = (long long)d.xres * d.yres;
+    double acc = 0.0;
+    for (long long m = blockIdx.x * (long long)blockDim.x + threadIdx.x; m < n; m += (long long)gridDim.x * blockDim.x) {
+        const int i = NPAD + (int)(m % d.xres), j = d.ypad + (int)(m / d.xres);
+        acc += contract<PASS>(a, Seed{DIRECTION, 0, 0, -1}, i, j);
+    }
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(out, acc);
+}
+
+// sum of a[k] * b[k] over n entries
+__global__ void k_dot(const double* a, const double* b, long long n, double* out) {
+    double acc = 0.0;
+    for (long long m = blockIdx.x * (long long)blockDim.x + threadIdx.x; m < n; m += (long long)gridDim.x * blockDim.x)
+        acc += a[m] * b[m];
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(out, acc);
+}
+
+// The pass output evaluated by the adjoint's own restatement (double), for the
+// check that it reproduces the production kernels: 3 interior planes.
+template <int PASS>
+__global__ void k_adj_model(const Args a, double* out) {
+    const DiskView& d = a.d;
+    const long long n = (long long)d.xres * d.yres;
+    const size_t P = plane(d);
+    const Seed s{-1, -1, -1, -1};
+    for (long long m = blockIdx.x * (long long)blockDim.x + threadIdx.x; m < n; m += (long long)gridDim.x * blockDim.x) {
+        const int i = NPAD + (int)(m % d.xres), jo = d.ypad + (int)(m / d.xres);
+        S3<double> q;
+        if (PASS == P_K1) {
+            double vx, vy;
+            q = eval_k1<double>(a, s, i, jo, vx, vy);
+        } else if (PASS == P_SX) {
+            q = eval_sx<double>(a, s, i, jo);
+        } else if (PASS == P_SY) {
+            q = eval_sy<double>(a, s, i, sy_pre_row(d, a.inc, i, jo));
+        } else if (PASS == P_ADV) {
+            q = eval_adv<double>(a, s, i, jo);
+        } else {
+            q = eval_k2<double>(a, s, i, jo);
+        }
+        out[m] = q.r;
+        out[P + m] = q.u;
+        out[2 * P + m] = q.v;
+    }
+}
+
+}  // namespace adj
+}  // namespace pg
+
+// ================================================================== host
+namespace pg {
+namespace adj {
+
+// initial state of the differentiated run: Sigma0 given, v_r = 0, v_phi = the
+// disk's init_C (pressure-supported Keplerian), p = cs^2 Sigma0
+__global__ void k_init_state(const DiskView d, const double* sigma0, double* r, double* p, double* u, double* v) {
+    const long long n = (long long)d.xres * d.yres;
+    for (long long m = blockIdx.x * (long long)blockDim.x + threadIdx.x; m < n; m += (long long)gridDim.x * blockDim.x) {
+        const int i = NPAD + (int)(m % d.xres);
+        r[m] = sigma0[m];
+        p[m] = d.cs2x[i] * sigma0[m];
+        u[m] = 0.0;
+        v[m] = d.initx[5 * i + 3];
+    }
+}
+
+// d loss / d theta through the initial v_phi(r; h)
+__global__ void k_init_theta(const DiskView d, const double* lam_v, const double* dtab, double* gth) {
+    const long long n = (long long)d.xres * d.yres;
+    double acc[3] = {0.0, 0.0, 0.0};
+    for (long long m = blockIdx.x * (long long)blockDim.x + threadIdx.x; m < n; m += (long long)gridDim.x * blockDim.x) {
+        const int i = NPAD + (int)(m % d.xres);
+        for (int th = 0; th < 3; ++th) acc[th] += lam_v[m] * dtab[((size_t)th * NTAB + T_V0) * d.xarr + i];
+    }
+    for (int th = 0; th < 3; ++th) {
+        double v = acc[th];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if ((threadIdx.x & 31) == 0) atomicAdd(&gth[th], v);
+    }
+}
+
+// max over the interior of |a - b| / max(|b|, floor) per field (r, u, v) of two
+// sets of 3 interior planes; b given as AoS cells
+__global__ void k_model_err(const DiskView d, const double* a, const Cell* b, unsigned long long* out) {
+    const long long n = (long long)d.xres * d.yres;
+    const size_t P = plane(d);
+    double e = 0.0;
+    for (long long m = blockIdx.x * (long long)blockDim.x + threadIdx.x; m < n; m += (long long)gridDim.x * blockDim.x) {
+        const int i = NPAD + (int)(m % d.xres), j = d.ypad + (int)(m / d.xres);
+        const Cell c = load_cell(b, d.xarr, i, j);
+        e = fmax(e, fabs(a[m] - c.r) / fmax(fabs(c.r), 1e-300));
+        e = fmax(e, fabs(a[P + m] - c.u) / fmax(fabs(c.v), 1e-300));  // velocities relative to |v_phi|
+        e = fmax(e, fabs(a[2 * P + m] - c.v) / fmax(fabs(c.v), 1e-300));
+    }
+    for (int o = 16; o > 0; o >>= 1) e = fmax(e, __shfl_down_sync(0xffffffffu, e, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(out, (unsigned long long)__double_as_longlong(e));
+}
+
+static unsigned grid_for(long long n) {
+    long long g = (n + ADJ_THREADS - 1) / ADJ_THREADS;
+    if (g > 148 * 16) g = 148 * 16;
+    return (unsigned)(g < 1 ? 1 : g);
+}
+
+template <int PASS>
+static void launch_pass(const Args& a, bool theta, cudaStream_t s) {
+    const long long n = (long long)a.d.xres * a.d.yres;
+    k_adj_state<PASS><<<grid_for(n), ADJ_THREADS, 0, s>>>(a);
+    if (theta) k_adj_theta<PASS><<<grid_for(n), ADJ_THREADS, 0, s>>>(a);
+}
+
+template <int PASS>
+static void launch_model(const Args& a, double* out, cudaStream_t s) {
+    const long long n = (long long)a.d.xres * a.d.yres;
+    k_adj_model<PASS><<<grid_for(n), ADJ_THREADS, 0, s>>>(a, out);
+}
+
+}  // namespace adj
+}  // namespace pg
+
+using namespace pg;
+using namespace pg::adj;
+
+struct pg_adj {
+    pg_params P{};
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    pg_disk* disk = nullptr;
+    Engine* E = nullptr;
+    int every = 64;
+    // dt schedule of the recorded forward run
+    double t0 = 0.0;
+    std::vector<double> ts, dts;
+    // checkpoints: state (all cells) and device scalars every `every` steps
+    Cell* ckpt = nullptr;
+    Scalars* ckpt_sc = nullptr;
+    int nckpt = 0;
+    // one segment's pass inputs
+    Cell* stages = nullptr;
+    double* rvis = nullptr;
+    pg_body* rpl = nullptr;
+    double* rres = nullptr;
+    int* rinc = nullptr;
+    // adjoint state and scratch
+    double* lam[2] = {nullptr, nullptr};
+    double* lamv = nullptr;
+    double* lamv_in = nullptr;
+    double* work = nullptr;  // 4 interior planes
+    double* dtab = nullptr;
+    double* gth = nullptr;
+    unsigned long long* err = nullptr;
+    Scalars* ssc = nullptr;  // scratch copy of the device scalars
+    size_t bytes = 0;
+
+    size_t ncell() const { return (size_t)(P.xres + 2 * NPAD) * (P.yres + 2 * NPAD); }
+    size_t nint() const { return (size_t)P.xres * P.yres; }
+};
+
+static thread_local std::string g_adj_err;
+static pg_status adj_fail(pg_status s, const std::string& m) {
+    g_adj_err = m;
+    set_last_error(m.c_str());
+    return s;
+}
+#define ADJ_CUDA(call)                                                                                   \
+    do {                                                                                                 \
+        cudaError_t e_ = (call);                                                                         \
+        if (e_ != cudaSuccess) return adj_fail(PG_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+template <class P>
+static pg_status adj_alloc(pg_adj* a, P** p, size_t bytes) {
+    ADJ_CUDA(cudaMalloc(p, bytes));
+    a->bytes += bytes;
+    return PG_OK;
+}
+
+static void adj_free_run(pg_adj* a) {
+    cudaFree(a->ckpt);
+    cudaFree(a->ckpt_sc);
+    a->ckpt = nullptr;
+    a->ckpt_sc = nullptr;
+    a->nckpt = 0;
+}
+
+// theta-derivative tables from the disk's own tables (values evaluated on the
+// device like the reference's init.cu:7-50, 240-252): cs2 ~ h^2, nu ~ alpha h^2,
+// p0 = cs2 Sigma0, u0 = -1.5 nu / r, v0^2 = 1/r + (r / Sigma0) dP/dr with
+// dP/dr ~ h^2, orb_rot = v0 - r Omega_frame.
+static pg_status adj_tables(pg_adj* a) {
+    const DiskView& d = engine_view(a->E);
+    const int xarr = d.xarr;
+    std::vector<double> radx(xarr), cs2(xarr), nu(xarr), init(5 * (size_t)xarr);
+    ADJ_CUDA(cudaMemcpyAsync(radx.data(), d.radx, xarr * sizeof(double), cudaMemcpyDeviceToHost, a->stream));
+    ADJ_CUDA(cudaMemcpyAsync(cs2.data(), d.cs2x, xarr * sizeof(double), cudaMemcpyDeviceToHost, a->stream));
+    ADJ_CUDA(cudaMemcpyAsync(nu.data(), d.nux, xarr * sizeof(double), cudaMemcpyDeviceToHost, a->stream));
+    ADJ_CUDA(cudaMemcpyAsync(init.data(), d.initx, 5 * xarr * sizeof(double), cudaMemcpyDeviceToHost, a->stream));
+    ADJ_CUDA(cudaStreamSynchronize(a->stream));
+    const pg_params& P = a->P;
+    const double h = P.sc_h, rp = P.planet_radius;
+    std::vector<double> t(3 * (size_t)NTAB * xarr, 0.0);
+    auto at = [&](int th, int tb, int i) -> double& { return t[((size_t)th * NTAB + tb) * xarr + i]; };
+    for (int i = 0; i < xarr; ++i) {
+        const double x = radx[i];
+        // nu / alpha (init.cu:31-50, geomx 1): sqrt(cs2(rp)) H(rp) (x/rp)^p_alpha
+        const double cs2p = h * h * (1.0 / rp) * std::pow(rp / rp, -P.p_beta);
+        const double nua = (P.visc_flag && P.ndim == 2)
+                               ? std::sqrt(cs2p) * std::sqrt(cs2p * std::pow(rp, 3)) * std::pow(x / rp, P.p_alpha)
+                               : 0.0;
+        const double v0 = init[5 * (size_t)i + 3], r0 = init[5 * (size_t)i];
+        at(2, T_CS2, i) = 2.0 * cs2[i] / h;
+        at(1, T_NU, i) = nua;
+        at(2, T_NU, i) = 2.0 * nu[i] / h;
+        at(2, T_P0, i) = 2.0 * cs2[i] * r0 / h;
+        at(1, T_U0, i) = -1.5 * nua / x;
+        at(2, T_U0, i) = -1.5 * (2.0 * nu[i] / h) / x;
+        const double dv0 = (v0 * v0 - 1.0 / x) / (h * v0);
+        at(2, T_V0, i) = dv0;
+        at(2, T_ROT, i) = P.orbadv_flag ? dv0 : 0.0;
+    }
+    ADJ_CUDA(cudaMemcpyAsync(a->dtab, t.data(), t.size() * sizeof(double), cudaMemcpyHostToDevice, a->stream));
+    ADJ_CUDA(cudaStreamSynchronize(a->stream));
+    return PG_OK;
+}
+
+static pg_status adj_make_disk(pg_adj* a) {
+    if (a->disk) {
+        pg_disk_destroy(a->disk);
+        a->disk = nullptr;
+    }
+    pg_status s = pg_disk_create(&a->P, a->device, a->stream, &a->disk);
+    if (s != PG_OK) return s;
+    a->E = disk_engine(a->disk);
+    return adj_tables(a);
+}
+
+extern "C" {
+
+pg_status pg_adj_check_params(const pg_params* P) {
+    if (!P) return adj_fail(PG_ERR_ARG, "null params");
+    if (P->ndim != 2 || P->geomx != 1 || P->geomy != 3)
+        return adj_fail(PG_ERR_CONFIG, "the adjoint covers 2D polar disks (ndim 2, geomx 1, geomy 3)");
+    if (P->eos_flag != 0) return adj_fail(PG_ERR_CONFIG, "the adjoint covers the isothermal disk (EOS_flag 0)");
+    if (P->bound_lft != 0 || P->bound_rgh != 0)
+        return adj_fail(PG_ERR_CONFIG, "the adjoint covers analytic radial boundaries (bound 0)");
+    if (P->kill_flag) return adj_fail(PG_ERR_CONFIG, "the adjoint does not differentiate wave damping (kill_flag 0)");
+    if (P->dust_flag) return adj_fail(PG_ERR_CONFIG, "the adjoint covers the gas only");
+    if (P->n_planet > 0 && P->planet_ecc != 0.0)
+        return adj_fail(PG_ERR_CONFIG, "the adjoint covers a planet on a circular orbit");
+    if (!(P->sc_h > 0.0)) return adj_fail(PG_ERR_CONFIG, "h/r must be positive");
+    return pg_check_params(P);
+}
+
+pg_status pg_adj_create(const pg_params* P, int device, void* stream, int checkpoint_every, pg_adj** out) {
+    if (!out) return adj_fail(PG_ERR_ARG, "null out");
+    *out = nullptr;
+    pg_status s = pg_adj_check_params(P);
+    if (s != PG_OK) return s;
+    if (checkpoint_every < 1) return adj_fail(PG_ERR_ARG, "checkpoint_every must be >= 1");
+    ADJ_CUDA(cudaSetDevice(device));
+    pg_adj* a = new pg_adj();
+    a->P = *P;
+    a->device = device;
+    a->every = checkpoint_every;
+    if (stream) a->stream = (cudaStream_t)stream;
+    else {
+        cudaError_t e = cudaStreamCreateWithFlags(&a->stream, cudaStreamNonBlocking);
+        if (e != cudaSuccess) {
+            delete a;
+            return adj_fail(PG_ERR_CUDA, cudaGetErrorString(e));
+        }
+        a->own_stream = true;
+    }
+    const size_t nc = a->ncell(), ni = a->nint(), xarr = (size_t)P->xres + 2 * NPAD, K = (size_t)a->every;
+    auto bail = [&](pg_status st) {
+        pg_adj_destroy(a);
+        return st;
+    };
+    if ((s = adj_alloc(a, &a->stages, 5 * K * nc * sizeof(Cell))) != PG_OK) return bail(s);
+    if ((s = adj_alloc(a, &a->rvis, 2 * K * nc * sizeof(double))) != PG_OK) return bail(s);
+    if ((s = adj_alloc(a, &a->rpl, 2 * K * sizeof(pg_body))) != PG_OK) return bail(s);
+    if ((s = adj_alloc(a, &a->rres, K * xarr * sizeof(double))) != PG_OK) return bail(s);
+    if ((s = adj_alloc(a, &a->rinc, K * xarr * sizeof(int))) != PG_OK) return bail(s);
+    if ((s = adj_alloc(a, &a->lam[0], 3 * ni * sizeof(double))) != PG_OK) return bail(s);
+    if ((s = adj_alloc(a, &a->lam[1], 3 * ni * sizeof(double))) != PG_OK) return bail(s);
+    if ((s = adj_alloc(a, &a->lamv, 2 * ni * sizeof(double))) != PG_OK) return bail(s);
+    if ((s = adj_alloc(a, &a->lamv_in, 2 * ni * sizeof(double))) != PG_OK) return bail(s);
+    if ((s = adj_alloc(a, &a->work, 4 * ni * sizeof(double))) != PG_OK) return bail(s);
+    if ((s = adj_alloc(a, &a->dtab, 3 * NTAB * xarr * sizeof(double))) != PG_OK) return bail(s);
+    if ((s = adj_alloc(a, &a->gth, 3 * sizeof(double))) != PG_OK) return bail(s);
+    if ((s = adj_alloc(a, &a->err, 5 * sizeof(unsigned long long))) != PG_OK) return bail(s);
+    if ((s = adj_alloc(a, &a->ssc, sizeof(Scalars))) != PG_OK) return bail(s);
+    if ((s = adj_make_disk(a)) != PG_OK) return bail(s);
+    *out = a;
+    return PG_OK;
+}
+
+pg_status pg_adj_destroy(pg_adj* a) {
+    if (!a) return PG_OK;
+    cudaSetDevice(a->device);
+    if (a->stream) cudaStreamSynchronize(a->stream);
+    if (a->disk) pg_disk_destroy(a->disk);
+    adj_free_run(a);
+    cudaFree(a->stages);
+    cudaFree(a->rvis);
+    cudaFree(a->rpl);
+    cudaFree(a->rres);
+    cudaFree(a->rinc);
+    cudaFree(a->lam[0]);
+    cudaFree(a->lam[1]);
+    cudaFree(a->lamv);
+    cudaFree(a->lamv_in);
+    cudaFree(a->work);
+    cudaFree(a->dtab);
+    cudaFree(a->gth);
+    cudaFree(a->err);
+    cudaFree(a->ssc);
+    if (a->own_stream && a->stream) cudaStreamDestroy(a->stream);
+    delete a;
+    return PG_OK;
+}
+
+pg_status pg_adj_set_params(pg_adj* a, double q, double alpha, double h) {
+    if (!a) return adj_fail(PG_ERR_ARG, "null adjoint");
+    pg_params P = a->P;
+    P.planet_mass = q;
+    P.ss_alpha = alpha;
+    P.sc_h = h;
+    pg_status s = pg_adj_check_params(&P);
+    if (s != PG_OK) return s;
+    a->P = P;
+    return adj_make_disk(a);
+}
+
+// Forward run from Sigma0 (device, xres*yres) at t0: nsteps of main.cu's loop,
+// dt from the CFL condition (recorded) or, with replay, the recorded schedule.
+// The state is checkpointed every `every` steps; Sigma after the run goes to
+// sigma_out (device; may be null).
+pg_status pg_adj_forward(pg_adj* a, const double* sigma0, double t0, int nsteps, int replay, double* sigma_out) {
+    if (!a || !sigma0 || nsteps < 1) return adj_fail(PG_ERR_ARG, "bad argument");
+    if (replay && (int)a->dts.size() != nsteps) return adj_fail(PG_ERR_ARG, "no recorded schedule of that length");
+    ADJ_CUDA(cudaSetDevice(a->device));
+    const DiskView& d = engine_view(a->E);
+    const size_t ni = a->nint(), nc = a->ncell();
+    double* w = a->work;
+    k_init_state<<<grid_for((long long)ni), ADJ_THREADS, 0, a->stream>>>(d, sigma0, w, w + ni, w + 2 * ni, w + 3 * ni);
+    ADJ_CUDA(cudaGetLastError());
+    pg_status s = engine_set_state_device(a->E, t0, w, w + ni, w + 2 * ni, w + 3 * ni);
+    if (s != PG_OK) return s;
+    const int nck = (nsteps + a->every - 1) / a->every;
+    if (nck != a->nckpt) {
+        adj_free_run(a);
+        if ((s = adj_alloc(a, &a->ckpt, (size_t)nck * nc * sizeof(Cell))) != PG_OK) return s;
+        if ((s = adj_alloc(a, &a->ckpt_sc, (size_t)nck * sizeof(Scalars))) != PG_OK) return s;
+        a->nckpt = nck;
+    }
+    if (!replay) {
+        a->dts.assign(nsteps, 0.0);
+        a->t0 = t0;
+    } else if (t0 != a->t0) {
+        return adj_fail(PG_ERR_ARG, "replay from another start time");
+    }
+    a->ts.assign(nsteps, 0.0);
+    double t = t0, dt = 1.0e30;
+    for (int n = 0; n < nsteps; ++n) {
+        if (n % a->every == 0 &&
+            (s = engine_save(a->E, a->ckpt + (size_t)(n / a->every) * nc, a->ckpt_sc + n / a->every)) != PG_OK)
+            return s;
+        if (replay) dt = a->dts[n];
+        else {
+            double dtn = 0.0;
+            if ((s = pg_disk_global_dt(a->disk, dt, &dtn)) != PG_OK) return s;
+            dt = dtn;
+            a->dts[n] = dt;
+        }
+        a->ts[n] = t;
+        if ((s = engine_step(a->E, t, dt, nullptr)) != PG_OK) return s;
+        t += dt;
+    }
+    if (sigma_out) {
+        if ((s = engine_extract_device(a->E, w, w + ni, w + 2 * ni, w + 3 * ni)) != PG_OK) return s;
+        ADJ_CUDA(cudaMemcpyAsync(sigma_out, w, ni * sizeof(double), cudaMemcpyDeviceToDevice, a->stream));
+    }
+    ADJ_CUDA(cudaStreamSynchronize(a->stream));
+    return pg_disk_check(a->disk);
+}
+
+static Args base_args(pg_adj* a, int n, int slot, const pg_body* pl) {
+    Args g{};
+    g.d = engine_view(a->E);
+    g.pl[0] = pl[0];
+    g.pl[1] = pl[1];
+    const double tau = a->P.ramp_time;
+    g.dmdq[0] = ramp_function(a->ts[n], tau, 1.0);
+    g.dmdq[1] = ramp_function(a->ts[n] + a->dts[n], tau, 1.0);
+    g.drsdh = a->P.rs_fac * a->P.planet_radius;  // rs = rs_fac h a (2D)
+    const size_t xarr = (size_t)a->P.xres + 2 * NPAD;
+    g.res = a->rres + (size_t)slot * xarr;
+    g.inc = a->rinc + (size_t)slot * xarr;
+    g.vis = a->rvis + (size_t)slot * 2 * a->ncell();
+    g.dt = a->dts[n];
+    g.dtab = a->dtab;
+    g.gth = a->gth;
+    return g;
+}
+
+static StepRecord record_slot(pg_adj* a, int slot) {
+    StepRecord r{};
+    const size_t nc = a->ncell(), xarr = (size_t)a->P.xres + 2 * NPAD;
+    for (int k = 0; k < 5; ++k) r.stage[k] = a->stages + ((size_t)slot * 5 + k) * nc;
+    r.vis = a->rvis + (size_t)slot * 2 * nc;
+    r.planets = a->rpl + 2 * (size_t)slot;
+    r.res = a->rres + (size_t)slot * xarr;
+    r.inc = a->rinc + (size_t)slot * xarr;
+    return r;
+}
+
+// Gradient of a loss L(Sigma after the recorded run): grad_out = dL/dSigma
+// (device, xres*yres) -> dL/dSigma0 (device; may be null) and dL/d(q, alpha, h)
+// (host, 3; may be null).  Recomputes each segment forward from its checkpoint
+// with the recorded dt, then runs the pass adjoints in reverse order.
+pg_status pg_adj_backward(pg_adj* a, const double* grad_out, double* grad_sigma0, double* grad_theta) {
+    if (!a || !grad_out) return adj_fail(PG_ERR_ARG, "bad argument");
+    const int N = (int)a->dts.size();
+    if (N == 0 || a->nckpt == 0) return adj_fail(PG_ERR_ARG, "no recorded forward run");
+    ADJ_CUDA(cudaSetDevice(a->device));
+    const DiskView& d = engine_view(a->E);
+    const size_t ni = a->nint();
+    cudaStream_t st = a->stream;
+    int c = 0;
+    ADJ_CUDA(cudaMemsetAsync(a->lam[0], 0, 3 * ni * sizeof(double), st));
+    ADJ_CUDA(cudaMemcpyAsync(a->lam[0], grad_out, ni * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    ADJ_CUDA(cudaMemsetAsync(a->gth, 0, 3 * sizeof(double), st));
+    ADJ_CUDA(cudaMemsetAsync(a->lamv, 0, 2 * ni * sizeof(double), st));
+    std::vector<pg_body> pl(2 * (size_t)a->every);
+    pg_status s;
+    for (int seg = a->nckpt - 1; seg >= 0; --seg) {
+        const int n0 = seg * a->every, n1 = std::min(n0 + a->every, N);
+        if ((s = engine_restore(a->E, a->ckpt + (size_t)seg * a->ncell(), a->ckpt_sc + seg)) != PG_OK) return s;
+        for (int n = n0; n < n1; ++n) {
+            const StepRecord r = record_slot(a, n - n0);
+            if ((s = engine_step(a->E, a->ts[n], a->dts[n], &r)) != PG_OK) return s;
+        }
+        ADJ_CUDA(cudaMemcpyAsync(pl.data(), a->rpl, 2 * (size_t)(n1 - n0) * sizeof(pg_body), cudaMemcpyDeviceToHost, st));
+        ADJ_CUDA(cudaStreamSynchronize(st));
+        for (int n = n1 - 1; n >= n0; --n) {
+            const int slot = n - n0;
+            const StepRecord r = record_slot(a, slot);
+            Args g = base_args(a, n, slot, &pl[2 * (size_t)slot]);
+            auto run = [&](int pass, const Cell* in) {
+                g.in = in;
+                g.lam = a->lam[c];
+                g.lam_in = a->lam[1 - c];
+                switch (pass) {
+                    case P_K2: g.lamv_in = a->lamv; launch_pass<P_K2>(g, true, st); break;
+                    case P_ADV: launch_pass<P_ADV>(g, true, st); break;
+                    case P_SY: launch_pass<P_SY>(g, true, st); break;
+                    case P_SX: launch_pass<P_SX>(g, true, st); break;
+                    default: g.lamv = a->lamv; launch_pass<P_K1>(g, true, st); break;
+                }
+                c = 1 - c;
+            };
+            run(P_K2, r.stage[4]);
+            if (d.orbadv) run(P_ADV, r.stage[3]);
+            run(P_SY, r.stage[2]);
+            run(P_SX, r.stage[1]);
+            run(P_K1, r.stage[0]);
+            ADJ_CUDA(cudaGetLastError());
+        }
+    }
+    k_init_theta<<<grid_for((long long)ni), ADJ_THREADS, 0, st>>>(d, a->lam[c] + 2 * ni, a->dtab, a->gth);
+    ADJ_CUDA(cudaGetLastError());
+    if (grad_sigma0)
+        ADJ_CUDA(cudaMemcpyAsync(grad_sigma0, a->lam[c], ni * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    if (grad_theta) ADJ_CUDA(cudaMemcpyAsync(grad_theta, a->gth, 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    ADJ_CUDA(cudaStreamSynchronize(st));
+    return PG_OK;
+}
+
+// The adjoint's restatement of each pass against the production kernels: one
+// step from the newest state with dt, maximum relative difference per pass
+// (kick1, sweep_x, sweep_y + shift, advect, kick2) in err[5].
+pg_status pg_adj_model_error(pg_adj* a, double dt, double* err) {
+    if (!a || !err || a->P.ndim != 2) return adj_fail(PG_ERR_ARG, "bad argument");
+    ADJ_CUDA(cudaSetDevice(a->device));
+    const DiskView& d = engine_view(a->E);
+    const size_t ni = a->nint();
+    cudaStream_t st = a->stream;
+    Scalars h{};
+    ADJ_CUDA(cudaMemcpyAsync(&h, d.sc, sizeof(Scalars), cudaMemcpyDeviceToHost, st));
+    ADJ_CUDA(cudaStreamSynchronize(st));
+    a->ts.assign(1, h.t);
+    a->dts.assign(1, dt);
+    const StepRecord r = record_slot(a, 0);
+    pg_status s = engine_step(a->E, h.t, dt, &r);
+    if (s != PG_OK) return s;
+    pg_body pl[2];
+    ADJ_CUDA(cudaMemcpyAsync(pl, a->rpl, sizeof pl, cudaMemcpyDeviceToHost, st));
+    if (a->every < 2) return adj_fail(PG_ERR_ARG, "needs checkpoint_every >= 2");
+    Cell* outK2 = a->stages + 5 * a->ncell();  // slot 1, stage 0: the state after the step
+    if ((s = engine_save(a->E, outK2, a->ssc)) != PG_OK) return s;
+    ADJ_CUDA(cudaStreamSynchronize(st));
+    Args g = base_args(a, 0, 0, pl);
+    ADJ_CUDA(cudaMemsetAsync(a->err, 0, 5 * sizeof(unsigned long long), st));
+    const Cell* outs[5] = {r.stage[1], r.stage[2], d.orbadv ? r.stage[3] : r.stage[4], r.stage[4], outK2};
+    for (int p = 0; p < 5; ++p) {
+        if (p == P_ADV && !d.orbadv) continue;
+        g.in = r.stage[p];
+        switch (p) {
+            case P_K1: launch_model<P_K1>(g, a->work, st); break;
+            case P_SX: launch_model<P_SX>(g, a->work, st); break;
+            case P_SY: launch_model<P_SY>(g, a->work, st); break;
+            case P_ADV: launch_model<P_ADV>(g, a->work, st); break;
+            default: launch_model<P_K2>(g, a->work, st); break;
+        }
+        k_model_err<<<grid_for((long long)ni), ADJ_THREADS, 0, st>>>(d, a->work, outs[p], a->err + p);
+    }
+    ADJ_CUDA(cudaGetLastError());
+    unsigned long long e[5];
+    ADJ_CUDA(cudaMemcpyAsync(e, a->err, sizeof e, cudaMemcpyDeviceToHost, st));
+    ADJ_CUDA(cudaStreamSynchronize(st));
+    for (int p = 0; p < 5; ++p) {
+        double v;
+        std::memcpy(&v, &e[p], sizeof v);
+        err[p] = v;
+    }
+    return PG_OK;
+}
+
+// Adjoint dot-product test of every pass over one step of size dt from the
+// newest state: with a direction dir (device, 5 interior planes: Sigma, v_r,
+// v_phi and kick1's force x, y) and an output adjoint lam (device, 5 planes
+// likewise, the force planes used by kick1 only), out[2p] = <lam, J_p dir> by
+// forward mode and out[2p+1] = <J_p^T lam, dir> by the gather adjoint.
+pg_status pg_adj_dot_test(pg_adj* a, double dt, const double* dir, const double* lam, double* out10) {
+    if (!a || !dir || !lam || !out10 || a->every < 2) return adj_fail(PG_ERR_ARG, "bad argument");
+    ADJ_CUDA(cudaSetDevice(a->device));
+    const DiskView& d = engine_view(a->E);
+    const size_t ni = a->nint();
+    cudaStream_t st = a->stream;
+    Scalars h{};
+    ADJ_CUDA(cudaMemcpyAsync(&h, d.sc, sizeof(Scalars), cudaMemcpyDeviceToHost, st));
+    ADJ_CUDA(cudaStreamSynchronize(st));
+    a->ts.assign(1, h.t);
+    a->dts.assign(1, dt);
+    const StepRecord r = record_slot(a, 0);
+    pg_status s = engine_step(a->E, h.t, dt, &r);
+    if (s != PG_OK) return s;
+    pg_body pl[2];
+    ADJ_CUDA(cudaMemcpyAsync(pl, a->rpl, sizeof pl, cudaMemcpyDeviceToHost, st));
+    ADJ_CUDA(cudaStreamSynchronize(st));
+    double* dev = nullptr;
+    ADJ_CUDA(cudaMallocAsync(&dev, 10 * sizeof(double), st));
+    ADJ_CUDA(cudaMemsetAsync(dev, 0, 10 * sizeof(double), st));
+    Args g = base_args(a, 0, 0, pl);
+    g.dir = dir;
+    g.lam = lam;
+    g.lamv = lam + 3 * ni;
+    g.lam_in = a->lam[1];
+    g.lamv_in = a->lamv_in;
+    const unsigned gr = grid_for((long long)ni);
+    for (int p = 0; p < 5; ++p) {
+        if (p == P_ADV && !d.orbadv) continue;
+        g.in = r.stage[p];
+        switch (p) {
+            case P_K1: k_adj_jvp<P_K1><<<gr, ADJ_THREADS, 0, st>>>(g, dev + 2 * p); k_adj_state<P_K1><<<gr, ADJ_THREADS, 0, st>>>(g); break;
+            case P_SX: k_adj_jvp<P_SX><<<gr, ADJ_THREADS, 0, st>>>(g, dev + 2 * p); k_adj_state<P_SX><<<gr, ADJ_THREADS, 0, st>>>(g); break;
+            case P_SY: k_adj_jvp<P_SY><<<gr, ADJ_THREADS, 0, st>>>(g, dev + 2 * p); k_adj_state<P_SY><<<gr, ADJ_THREADS, 0, st>>>(g); break;
+            case P_ADV: k_adj_jvp<P_ADV><<<gr, ADJ_THREADS, 0, st>>>(g, dev + 2 * p); k_adj_state<P_ADV><<<gr, ADJ_THREADS, 0, st>>>(g); break;
+            default: k_adj_jvp<P_K2><<<gr, ADJ_THREADS, 0, st>>>(g, dev + 2 * p); k_adj_state<P_K2><<<gr, ADJ_THREADS, 0, st>>>(g); break;
+        }
+        k_dot<<<gr, ADJ_THREADS, 0, st>>>(g.lam_in, dir, (long long)(3 * ni), dev + 2 * p + 1);
+        if (p == P_K2 && d.visc) k_dot<<<gr, ADJ_THREADS, 0, st>>>(g.lamv_in, dir + 3 * ni, (long long)(2 * ni), dev + 2 * p + 1);
+    }
+    ADJ_CUDA(cudaGetLastError());
+    ADJ_CUDA(cudaMemcpyAsync(out10, dev, 10 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    ADJ_CUDA(cudaFreeAsync(dev, st));
+    ADJ_CUDA(cudaStreamSynchronize(st));
+    return PG_OK;
+}
+
+pg_status pg_adj_schedule(const pg_adj* a, double* dts, int n) {
+    if (!a || n != (int)a->dts.size()) return adj_fail(PG_ERR_ARG, "schedule length differs");
+    if (dts) std::memcpy(dts, a->dts.data(), n * sizeof(double));
+    return PG_OK;
+}
+
+int pg_adj_steps(const pg_adj* a) { return a ? (int)a->dts.size() : 0; }
+
+long long pg_adj_device_bytes(const pg_adj* a) { return a ? (long long)a->bytes : 0; }
+
+}  // extern "C"

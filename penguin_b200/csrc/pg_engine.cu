@@ -478,11 +478,17 @@ static pg_status resolve_cur(Engine& E) {
     return PG_OK;
 }
 
-// Kernels of one step after the time kernel; in = E.cur.
-static pg_status enqueue_stages(Engine& E) {
+// Kernels of one step after the time kernel; in = E.cur.  With rec, the input
+// of every pass, kick1's stress and the orbital-advection arrays are copied
+// out for the adjoint.
+static pg_status enqueue_stages(Engine& E, const StepRecord* rec = nullptr) {
     const DiskView& d = E.view;
     pg_status s;
     int c = E.cur;
+    const size_t ncell = (size_t)d.xarr * d.yarr;
+    auto save = [&](int k) {
+        if (rec) cudaMemcpyAsync(rec->stage[k], E.buf[c], ncell * sizeof(Cell), cudaMemcpyDeviceToDevice, E.stream);
+    };
     auto maps = [&](int k) -> const CellMaps& { return E.maps[k]; };
     for (int k = 0; k < 2; ++k)
         if ((s = make_cell_maps(E.maps[k], E.buf[k], d.xarr, d.yarr)) != PG_OK) return s;
@@ -493,21 +499,32 @@ static pg_status enqueue_stages(Engine& E) {
     if (dust)
         for (int k = 0; k < 2; ++k)
             if ((s = make_dust_maps(E.dmaps[k], E.dbuf[k], d.xarr, d.yarr)) != PG_OK) return s;
+    save(0);
     launch_kick1(d, maps(c), E.buf[1 - c], E.vis, E.stream, dust ? D[c] : nullptr, dust ? D[1 - c] : nullptr);
+    if (rec && d.visc)
+        cudaMemcpyAsync(rec->vis, E.vis, 2 * ncell * sizeof(double), cudaMemcpyDeviceToDevice, E.stream);
     c = 1 - c;
+    save(1);
     launch_sweep_x(d, maps(c), E.buf[1 - c], E.stream);
     if (dust) launch_dsweep_x(d, E.dmaps[c], D[1 - c], E.stream);
     c = 1 - c;
     if (d.ndim > 1) {
+        save(2);
         launch_sweep_y(d, maps(c), E.buf[1 - c], E.stream);
         if (dust) launch_dsweep_y(d, E.dmaps[c], D[1 - c], E.stream);
+        if (rec) {
+            cudaMemcpyAsync(rec->res, E.res, d.xarr * sizeof(double), cudaMemcpyDeviceToDevice, E.stream);
+            cudaMemcpyAsync(rec->inc, E.inc, d.xarr * sizeof(int), cudaMemcpyDeviceToDevice, E.stream);
+        }
         c = 1 - c;
     }
     if (d.ndim > 1 && d.orbadv) {
+        save(3);
         launch_advect(d, maps(c), E.buf[1 - c], E.stream);
         if (dust) launch_dadvect(d, E.dmaps[c], D[1 - c], E.stream);
         c = 1 - c;
     }
+    save(4);
     launch_kick2(d, maps(c), E.vmap, E.buf[1 - c], E.stream, dust ? D[c] : nullptr, dust ? D[1 - c] : nullptr);
     c = 1 - c;
     E.cur = c;
@@ -634,6 +651,9 @@ struct pg_disk {
     Engine* E;
 };
 
+static pg_status set_state_device(Engine& E, double t, const double* r, const double* p, const double* u,
+                                  const double* v);
+
 extern "C" {
 
 const char* pg_version(void) { return "penguin_b200 0.1 (sm_100a, FP64 Godunov step)"; }
@@ -726,11 +746,21 @@ pg_status pg_disk_set_state(pg_disk* dk, double t, const double* r, const double
     PG_CUDA(cudaMemcpyAsync(stage + n, p, n * sizeof(double), cudaMemcpyHostToDevice, E.stream));
     PG_CUDA(cudaMemcpyAsync(stage + 2 * n, u, n * sizeof(double), cudaMemcpyHostToDevice, E.stream));
     if (v) PG_CUDA(cudaMemcpyAsync(stage + 3 * n, v, n * sizeof(double), cudaMemcpyHostToDevice, E.stream));
+    const pg_status s = set_state_device(E, t, stage, stage + n, stage + 2 * n, v ? stage + 3 * n : nullptr);
+    cudaFreeAsync(stage, E.stream);
+    return s;
+}
+
+}  // extern "C"
+
+// The state of a disk from interior device arrays (xres*yres each; v may be null).
+static pg_status set_state_device(Engine& E, double t, const double* r, const double* p, const double* u,
+                                  const double* v) {
+    const DiskView& d = E.view;
     E.cur = 0;
     E.pending = false;
-    k_fill<<<1184, 256, 0, E.stream>>>(d, E.buf[0], stage, stage + n, stage + 2 * n, v ? stage + 3 * n : nullptr);
+    k_fill<<<1184, 256, 0, E.stream>>>(d, E.buf[0], r, p, u, v);
     PG_CUDA(cudaGetLastError());
-    PG_CUDA(cudaFreeAsync(stage, E.stream));
     launch_bound(d, E.buf[0], E.stream);
     if (d.dust) launch_dust_init(d, E.dbuf[0], E.stream);  // a restart's dust is init_CD (the gas file only)
     launch_init_planet(d, E.P, t, E.stream);
@@ -752,6 +782,60 @@ pg_status pg_disk_set_state(pg_disk* dk, double t, const double* r, const double
     E.fresh = true;
     return PG_OK;
 }
+
+namespace pg {
+
+Engine* disk_engine(pg_disk* d) { return d ? d->E : nullptr; }
+
+pg_status engine_set_state_device(Engine* E, double t, const double* r, const double* p, const double* u,
+                                  const double* v) {
+    PG_CUDA(cudaSetDevice(E->device));
+    return set_state_device(*E, t, r, p, u, v);
+}
+
+// One step of main.cu's loop with a given dt (pg_disk_solve), optionally recording.
+pg_status engine_step(Engine* E, double t, double dt, const StepRecord* rec) {
+    pg_status s0 = resolve_cur(*E);
+    if (s0 != PG_OK) return s0;
+    launch_set_time(E->view, t, dt, E->stream);
+    if (rec) PG_CUDA(cudaMemcpyAsync(rec->planets, &E->sc->planet_cur, 2 * sizeof(pg_body), cudaMemcpyDeviceToDevice,
+                                     E->stream));
+    E->fresh = false;
+    return enqueue_stages(*E, rec);
+}
+
+// The newest state (all cells, ghosts included) and the device scalars (clock, planets).
+pg_status engine_save(Engine* E, Cell* cells, Scalars* sc) {
+    pg_status s0 = resolve_cur(*E);
+    if (s0 != PG_OK) return s0;
+    const size_t n = (size_t)E->view.xarr * E->view.yarr;
+    PG_CUDA(cudaMemcpyAsync(cells, E->buf[E->cur], n * sizeof(Cell), cudaMemcpyDeviceToDevice, E->stream));
+    PG_CUDA(cudaMemcpyAsync(sc, E->sc, sizeof(Scalars), cudaMemcpyDeviceToDevice, E->stream));
+    return PG_OK;
+}
+
+pg_status engine_restore(Engine* E, const Cell* cells, const Scalars* sc) {
+    const size_t n = (size_t)E->view.xarr * E->view.yarr;
+    E->cur = 0;
+    E->pending = false;
+    PG_CUDA(cudaMemcpyAsync(E->buf[0], cells, n * sizeof(Cell), cudaMemcpyDeviceToDevice, E->stream));
+    PG_CUDA(cudaMemcpyAsync(E->sc, sc, sizeof(Scalars), cudaMemcpyDeviceToDevice, E->stream));
+    E->fresh = false;
+    return PG_OK;
+}
+
+// Interior fields of the newest state into device arrays (xres*yres each).
+pg_status engine_extract_device(Engine* E, double* r, double* p, double* u, double* v) {
+    pg_status s0 = resolve_cur(*E);
+    if (s0 != PG_OK) return s0;
+    k_extract<<<1184, 256, 0, E->stream>>>(E->view, E->buf[E->cur], r, p, u, v);
+    PG_CUDA(cudaGetLastError());
+    return PG_OK;
+}
+
+}  // namespace pg
+
+extern "C" {
 
 pg_status pg_disk_get_state(pg_disk* dk, double* r, double* p, double* u, double* v, double* t_out) {
     if (!dk || !r || !p || !u) return fail(PG_ERR_ARG, "null argument");

@@ -26,6 +26,15 @@ struct DustMaps {
     CUtensorMap sweep_y;   // box {4*10, 38}
 };
 
+// Pass inputs of one FP64 step, saved for its adjoint (pg_adjoint.cu).
+struct StepRecord {
+    Cell* stage[5];     // inputs of kick1, sweep_x, sweep_y, advect, kick2 (xarr*yarr AoS each)
+    double* vis;        // kick1's viscous force density (2 per cell, xarr*yarr)
+    pg_body* planets;   // planet of the first half-kick, planet at t + dt
+    double* res;        // orbital-advection residual speed per radius (xarr)
+    int* inc;           // orbital-advection shift per radius (xarr)
+};
+
 // launch helpers (pg_kernels.cu)
 void launch_init_tables(const DiskView& d, const pg_params& P, double* tab_base, cudaStream_t s);
 void launch_init_xghosts(const DiskView& d, Cell* buf, cudaStream_t s);
@@ -49,6 +58,14 @@ void set_last_error(const char* msg);
 
 // tables-only disks and FP32 tensor maps for the FP32 form (pg_engine.cu)
 struct Engine;
+// FP64 disks driven by the adjoint (pg_engine.cu)
+Engine* disk_engine(pg_disk* d);
+pg_status engine_set_state_device(Engine* E, double t, const double* r, const double* p, const double* u,
+                                  const double* v);
+pg_status engine_step(Engine* E, double t, double dt, const StepRecord* rec);
+pg_status engine_save(Engine* E, Cell* cells, Scalars* sc);
+pg_status engine_restore(Engine* E, const Cell* cells, const Scalars* sc);
+pg_status engine_extract_device(Engine* E, double* r, double* p, double* u, double* v);
 pg_status table_engine_create(const pg_params* P, int device, cudaStream_t s, Engine** out);
 void engine_destroy(Engine* E);
 const DiskView& engine_view(const Engine* E);

@@ -114,40 +114,6 @@ __device__ __forceinline__ Cell kick(const DiskView& d, const Cell& C, double ix
     return o;
 }
 
-// Viscous force density of the middle cell of a 3x3 stencil
-// (src/viscosity/viscosity.cu:9-22, 84-194, ndim 2).  Stencil order: n<3 row j,
-// 3..5 row j-1, 6..8 row j+1, columns i-1..i+1.  The grid spacings enter as
-// per-index reciprocals: X = {1/(r2-r0), 1/(r2-r1), 1/(r1-r0), 1/(0.5(r2-r0)), 1/r1},
-// Y = {1/(t2-t0), 1/(t2-t1), 1/(t1-t0), 1/(0.5(t2-t0))}.
-__device__ __forceinline__ void viscous(const double* __restrict__ X, const double* __restrict__ Y, const double* u,
-                                        const double* v, const double* nr, double& fx_out, double& fy_out) {
-    const double i_r20 = X[0], i_r21 = X[1], i_r10 = X[2], i_hr20 = X[3], i_r1 = X[4];
-    const double i_t20 = Y[0], i_t21 = Y[1], i_t10 = Y[2], i_ht20 = Y[3];
-    const double dudx = (u[2] - u[0]) * i_r20;
-    const double d2udx2 = ((u[2] - u[1]) * i_r21 - (u[1] - u[0]) * i_r10) * i_hr20;
-    const double dndx = (nr[2] - nr[0]) * i_r20;
-    const double dvdx = (v[2] - v[0]) * i_r20;
-    const double d2vdx2 = ((v[2] - v[1]) * i_r21 - (v[1] - v[0]) * i_r10) * i_hr20;
-    const double dvdy = (v[7] - v[4]) * i_t20 * i_r1;
-    const double d2vdy2 = ((v[7] - v[1]) * i_t21 - (v[1] - v[4]) * i_t10) * i_ht20 * i_r1 * i_r1;
-    const double d2vdxy = (v[8] - v[6] - v[5] + v[3]) * i_r20 * i_t20 * i_r1;
-    const double dudy = (u[7] - u[4]) * i_t20 * i_r1;
-    const double d2udy2 = ((u[7] - u[1]) * i_t21 - (u[1] - u[4]) * i_t10) * i_ht20 * i_r1 * i_r1;
-    const double d2udxy = (u[8] - u[6] - u[5] + u[3]) * i_r20 * i_t20 * i_r1;
-    const double dndy = (nr[7] - nr[4]) * i_t20 * i_r1;
-
-    const double sxx = 2.0 * nr[1] * dudx;
-    double fx = 2.0 * dndx * dudx + 2.0 * nr[1] * d2udx2 + sxx * i_r1;
-    const double syy = 2.0 * nr[1] * (dvdy + u[1] * i_r1);
-    const double sxy = nr[1] * (dudy + dvdx - v[1] * i_r1);
-    double fy = 2.0 * dndy * dvdy + 2.0 * nr[1] * d2vdy2 + 2.0 * nr[1] * dudy * i_r1 + 2.0 * dndy * u[1] * i_r1;
-    fx += dndy * (dudy + dvdx) + nr[1] * (d2udy2 + d2vdxy) - dndy * v[1] * i_r1 - nr[1] * dvdy * i_r1 - syy * i_r1;
-    fy += dndx * (dudy + dvdx) + nr[1] * (d2udxy + d2vdx2) - dndx * v[1] * i_r1 - nr[1] * dvdx * i_r1 +
-          nr[1] * v[1] * i_r1 * i_r1 + 2.0 * sxy * i_r1;
-    fx_out = fx;
-    fy_out = fy;
-}
-
 // Gathers the 3x3 stencil around tile cell (hx, hy) of a [ST_HY][ST_HX][5] tile.
 __device__ __forceinline__ void gather9(const double* tile, int hx, int hy, const double nu[3], double* u,
                                         double* v, double* nr) {
