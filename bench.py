@@ -265,6 +265,82 @@ def measure_dust(local, stream, steps, pk):
 
 
 SEED_DUST = 1234
+ADJOINT_STEPS = 256
+
+
+def measure_adjoint(steps, local, stream):
+    """Gradient of the azimuthally averaged Sigma(r) misfit after `steps` steps of the
+    256x768 adjoint disk (q 5e-4, alpha 1e-3, h/r 0.05) with respect to the initial
+    Sigma field and (q, alpha, h/r), against a target made by the same code at
+    q 1e-3, alpha 3e-4 from the same seed; checkpoints every 64 steps.  Forward
+    and adjoint timed with CUDA events; central finite differences (FP64) of the
+    loss along a smooth Sigma0 direction and along each parameter check it."""
+    import numpy as np
+    import torch
+
+    from penguin_b200 import initial as I
+    from penguin_b200 import params as P
+    from penguin_b200.adjoint import DiskAdjoint
+
+    p = P.adjoint_disk()
+    s0 = torch.tensor(I.disk_state(p, seed=SEED_DUST)["r"], device=f"cuda:{local}")
+    tgt_model = DiskAdjoint(P.adjoint_disk(q=1.0e-3, alpha=3.0e-4), nsteps=steps, device=local,
+                            stream=stream.cuda_stream)
+    target = tgt_model.forward(s0).mean(0)
+    tgt_model.close()
+    m = DiskAdjoint(p, nsteps=steps, checkpoint_every=64, device=local, stream=stream.cuda_stream)
+
+    def loss(sig):
+        return float(((sig.mean(0) - target) ** 2).sum())
+
+    out = None
+
+    def fwd():
+        nonlocal out
+        out = m.forward(s0)
+
+    ms_f = timed(stream, fwd)
+    g = (2.0 * (out.mean(0) - target) / p.yres)[None, :].expand(p.yres, p.xres).contiguous()
+    res = {}
+
+    def bwd():
+        res["g"] = m.backward(g)
+
+    ms_b = timed(stream, bwd)
+    gs0, gth = res["g"]
+    x = I.cell_centres(p)
+    y = (np.arange(p.yres) + 0.5) * 2 * np.pi / p.yres
+    d = torch.tensor(np.cos(2 * y[:, None] + 1.0) * np.sin(3 * x[None, :]) + 0.3, device=s0.device) * s0
+    ad = float((gs0 * d).sum())
+    fd = {}
+    # steps down to 1e-10: on a noisy disk the exact derivative differs from the
+    # 1e-6 difference quotient at cells on azimuthal pressure extrema, where the
+    # PPM flattening coefficient varies on a 1e-8 scale
+    for eps in (1.0e-6, 1.0e-7, 1.0e-8, 1.0e-9, 1.0e-10):
+        fd[str(eps)] = (loss(m.forward(s0 + eps * d, replay=True)) - loss(m.forward(s0 - eps * d, replay=True))) / (2 * eps)
+    theta = [p.planet_mass, p.ss_alpha, p.sc_h]
+    fdt = []
+    for k in range(3):
+        step = 1.0e-4 * theta[k]
+        v = []
+        for sg in (1, -1):
+            th = list(theta)
+            th[k] += sg * step
+            m.set_theta(*th)
+            v.append(loss(m.forward(s0, replay=True)))
+        fdt.append((v[0] - v[1]) / (2 * step))
+    m.set_theta(*theta)
+    out_line = {
+        "workload": "256x768 gradient disk, FP64 forward + adjoint, checkpoint every 64 steps",
+        "steps": steps, "forward_ms_per_step": ms_f / steps, "adjoint_ms_per_step": ms_b / steps,
+        "adjoint_over_forward": ms_b / ms_f, "device_bytes": m.device_bytes,
+        "fd_sigma0": {"adjoint": ad, "central": fd,
+                      "rel_err": {k: abs(ad - v) / abs(v) for k, v in fd.items()}},
+        "fd_theta": {"names": ["q", "alpha", "h"], "adjoint": [float(v) for v in gth], "central_rel_step_1e-4": fdt,
+                     "rel_err": [abs(a - b) / abs(b) for a, b in zip(gth, fdt)]},
+    }
+    m.close()
+    return out_line
 
 
 def main():
@@ -275,8 +351,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-forms", action="store_true", help="skip the FP32-mixed, ensemble and dust measurements")
-    ap.add_argument("--forms", default="fp32,ensemble,dust",
-                    help="comma list of the extra measurements after the FP64 headline (fp32, ensemble, dust)")
+    ap.add_argument("--forms", default="fp32,ensemble,dust,adjoint",
+                    help="comma list of the extra measurements after the FP64 headline "
+                         "(fp32, ensemble, dust, adjoint)")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -416,6 +493,8 @@ def main():
         line["ensemble"] = measure_ensemble(local, stream, ENSEMBLE_STEPS)
     if "dust" in forms:
         line["dust"] = measure_dust(local, stream, min(DUST_STEPS, max(K, 3)), pk)
+    if "adjoint" in forms:
+        line["adjoint"] = measure_adjoint(min(ADJOINT_STEPS, max(K, 8)), local, stream)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(p, state, 0.0)
     if rank == 0:

@@ -250,6 +250,20 @@ pg_status pg_adj_model_error(pg_adj* a, double dt, double* err5);
    out10[2p+1] = <J_p^T lam, dir> (the adjoint), p = kick1, sweep_x, sweep_y,
    advect, kick2 */
 pg_status pg_adj_dot_test(pg_adj* a, double dt, const double* dir, const double* lam, double* out10);
+/* test support: the tangent of every pass (forward mode on the restated pass)
+   against central differences of the production kernel itself over one step
+   with dt from the newest state; err30[3p + f] = |fd - tangent|_2 / |tangent|_2
+   for f = Sigma, v_r, v_phi; err30[15 + 3p + f] the same with central
+   differences of the restated pass.  Overwrites the disk's state. */
+pg_status pg_adj_pass_check(pg_adj* a, double dt, double eps, const double* dir, double* err30);
+/* test support: each production pass re-run on its recorded input against its
+   recorded output over one step with dt (max relative difference per pass) */
+pg_status pg_adj_replay_diff(pg_adj* a, double dt, double* diff5);
+/* test support: one pass over one step with dt from the newest state; the
+   production outputs for the inputs +- eps dir (fd: 6 interior planes, plus
+   then minus) and the tangent along dir (tlm5: 5 planes).  Overwrites the
+   disk's state. */
+pg_status pg_adj_pass_fields(pg_adj* a, int pass, double dt, double eps, const double* dir, double* fd, double* tlm5);
 pg_status pg_adj_schedule(const pg_adj* a, double* dts, int n);
 int pg_adj_steps(const pg_adj* a);
 long long pg_adj_device_bytes(const pg_adj* a);

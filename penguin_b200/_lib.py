@@ -29,7 +29,7 @@ EXPORTS = [
     "pg_ens_get_state", "pg_ens_run", "pg_ens_sync", "pg_ens_clock", "pg_ens_planet", "pg_ens_check",
     "pg_ens_totals", "pg_ens_torque", "pg_ens_kernels_per_step", "pg_ens_profile",
     "pg_adj_check_params", "pg_adj_create", "pg_adj_destroy", "pg_adj_set_params", "pg_adj_forward",
-    "pg_adj_backward", "pg_adj_model_error", "pg_adj_dot_test", "pg_adj_schedule", "pg_adj_steps", "pg_adj_device_bytes",
+    "pg_adj_backward", "pg_adj_model_error", "pg_adj_dot_test", "pg_adj_pass_check", "pg_adj_replay_diff", "pg_adj_pass_fields", "pg_adj_schedule", "pg_adj_steps", "pg_adj_device_bytes",
 ]
 
 
@@ -107,6 +107,9 @@ def lib() -> ctypes.CDLL:
         "pg_adj_backward": (i, [vp, vp, vp, dp]),
         "pg_adj_model_error": (i, [vp, d, dp]),
         "pg_adj_dot_test": (i, [vp, d, vp, vp, dp]),
+        "pg_adj_pass_check": (i, [vp, d, d, vp, dp]),
+        "pg_adj_replay_diff": (i, [vp, d, dp]),
+        "pg_adj_pass_fields": (i, [vp, i, d, d, vp, vp, vp]),
         "pg_adj_schedule": (i, [vp, dp, i]),
         "pg_adj_steps": (i, [vp]),
         "pg_adj_device_bytes": (ctypes.c_longlong, [vp]),

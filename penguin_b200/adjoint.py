@@ -107,6 +107,32 @@ class DiskAdjoint:
         self.recorded = False
         return out.reshape(5, 2)
 
+    def pass_check(self, sigma0, steps_before: int = 1, eps: float = 1.0e-7, seed: int = 0) -> np.ndarray:
+        """Runs steps_before steps from sigma0, then compares the tangent of every pass
+        of the next step with central differences of the production kernels along a
+        smooth direction: [production, restated] x rows (kick1, sweep_x, sweep_y,
+        advect, kick2) x (Sigma, v_r, v_phi) of |fd - tangent|_2 / |tangent|_2.
+        Leaves no recorded run."""
+        import torch
+
+        s0 = sigma0.detach().to(torch.float64).contiguous()
+        check(lib().pg_adj_forward(self._h, ctypes.c_void_p(s0.data_ptr()), self.t0, steps_before, 0, None))
+        dt = float(self.schedule()[-1])
+        p = self.params
+        x = np.log(np.linspace(1.0, 2.0, p.xres))[None, :]
+        y = (np.arange(p.yres) + 0.5)[:, None] * 2 * np.pi / p.yres
+        rng = np.random.default_rng(seed)
+        ph = rng.uniform(0, 2 * np.pi, size=(5, 2))
+        dirs = torch.tensor(np.stack([np.cos(2 * y + ph[k, 0]) * np.sin(5 * x + ph[k, 1]) + 0.3 for k in range(5)]),
+                            device="cuda", dtype=torch.float64)
+        dirs[0] *= s0
+        dirs[1:3] *= 1.0e-3
+        out = np.zeros(30)
+        check(lib().pg_adj_pass_check(self._h, dt, eps, ctypes.c_void_p(dirs.data_ptr()),
+                                      out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+        self.recorded = False
+        return out.reshape(2, 5, 3)
+
     def schedule(self) -> np.ndarray:
         n = lib().pg_adj_steps(self._h)
         out = np.zeros(n)

@@ -570,6 +570,98 @@ __global__ void __launch_bounds__(ADJ_THREADS) k_adj_jvp(const Args a, double* o
     if ((threadIdx.x & 31) == 0) atomicAdd(out, acc);
 }
 
+// J dir of a pass by forward mode: 5 interior planes (Sigma, v_r, v_phi, and
+// kick1's force x, y)
+template <int PASS>
+__global__ void k_adj_tangent(const Args a, double* out) {
+    const DiskView& d = a.d;
+    const long long n = (long long)d.xres * d.yres;
+    const size_t P = plane(d);
+    const Seed s{DIRECTION, 0, 0, -1};
+    for (long long m = blockIdx.x * (long long)blockDim.x + threadIdx.x; m < n; m += (long long)gridDim.x * blockDim.x) {
+        const int i = NPAD + (int)(m % d.xres), jo = d.ypad + (int)(m / d.xres);
+        S3<Dual> q;
+        Dual vx = 0.0, vy = 0.0;
+        if (PASS == P_K1) q = eval_k1<Dual>(a, s, i, jo, vx, vy);
+        else if (PASS == P_SX) q = eval_sx<Dual>(a, s, i, jo);
+        else if (PASS == P_SY) q = eval_sy<Dual>(a, s, i, sy_pre_row(d, a.inc, i, jo));
+        else if (PASS == P_ADV) q = eval_adv<Dual>(a, s, i, jo);
+        else q = eval_k2<Dual>(a, s, i, jo);
+        out[m] = q.r.d;
+        out[P + m] = q.u.d;
+        out[2 * P + m] = q.v.d;
+        out[3 * P + m] = vx.d;
+        out[4 * P + m] = vy.d;
+    }
+}
+
+// in +- eps dir on every image of every interior cell (p = cs^2 Sigma kept);
+// vis likewise when vis_in is given
+__global__ void k_perturb(const DiskView d, const Cell* in, Cell* out, const double* vis_in, double* vis_out,
+                          const double* dir, double eps) {
+    const long long n = (long long)d.xarr * d.yarr;
+    const size_t P = plane(d);
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(k % d.xarr), j = (int)(k / d.xarr);
+        Cell c = in[k];
+        double vx = 0.0, vy = 0.0;
+        if (vis_in) {
+            vx = vis_in[2 * k];
+            vy = vis_in[2 * k + 1];
+        }
+        if (i >= NPAD && i < NPAD + d.xres) {
+            const size_t m = pidx(d, i, wrap_row(d, j));
+            c.r += eps * dir[m];
+            c.p += eps * d.cs2x[i] * dir[m];
+            c.u += eps * dir[P + m];
+            c.v += eps * dir[2 * P + m];
+            vx += eps * dir[3 * P + m];
+            vy += eps * dir[4 * P + m];
+        }
+        out[k] = c;
+        if (vis_out) {
+            vis_out[2 * k] = vx;
+            vis_out[2 * k + 1] = vy;
+        }
+    }
+}
+
+// central difference of two production outputs against the tangent: per field,
+// sum |fd - tlm|^2 and sum |tlm|^2 (out[0..9])
+__global__ void k_fd_compare(const DiskView d, const Cell* op, const Cell* om, const double* vp, const double* vm,
+                             const double* tlm, double eps, double* out) {
+    const long long n = (long long)d.xres * d.yres;
+    const size_t P = plane(d);
+    for (long long m = blockIdx.x * (long long)blockDim.x + threadIdx.x; m < n; m += (long long)gridDim.x * blockDim.x) {
+        const int i = NPAD + (int)(m % d.xres), j = d.ypad + (int)(m / d.xres);
+        const size_t k = (size_t)i + (size_t)d.xarr * j;
+        double fd[5];
+        fd[0] = (op[k].r - om[k].r) / (2 * eps);
+        fd[1] = (op[k].u - om[k].u) / (2 * eps);
+        fd[2] = (op[k].v - om[k].v) / (2 * eps);
+        fd[3] = vp ? (vp[2 * k] - vm[2 * k]) / (2 * eps) : 0.0;
+        fd[4] = vp ? (vp[2 * k + 1] - vm[2 * k + 1]) / (2 * eps) : 0.0;
+        for (int f = 0; f < 5; ++f) {
+            const double t = tlm[f * P + m];
+            atomicAdd(&out[2 * f], (fd[f] - t) * (fd[f] - t));
+            atomicAdd(&out[2 * f + 1], t * t);
+        }
+    }
+}
+
+// the same for two sets of 3 interior planes (the restated pass)
+__global__ void k_fd_compare_planes(const DiskView d, const double* op, const double* om, const double* tlm,
+                                    double eps, double* out) {
+    const long long n = (long long)d.xres * d.yres;
+    const size_t P = plane(d);
+    for (long long m = blockIdx.x * (long long)blockDim.x + threadIdx.x; m < n; m += (long long)gridDim.x * blockDim.x)
+        for (int f = 0; f < 3; ++f) {
+            const double fd = (op[f * P + m] - om[f * P + m]) / (2 * eps), t = tlm[f * P + m];
+            atomicAdd(&out[2 * f], (fd - t) * (fd - t));
+            atomicAdd(&out[2 * f + 1], t * t);
+        }
+}
+
 // sum of a[k] * b[k] over n entries
 __global__ void k_dot(const double* a, const double* b, long long n, double* out) {
     double acc = 0.0;
@@ -658,6 +750,19 @@ __global__ void k_model_err(const DiskView d, const double* a, const Cell* b, un
     }
     for (int o = 16; o > 0; o >>= 1) e = fmax(e, __shfl_down_sync(0xffffffffu, e, o));
     if ((threadIdx.x & 31) == 0) atomicMax(out, (unsigned long long)__double_as_longlong(e));
+}
+
+// interior r, u, v of an AoS buffer into 3 planes
+__global__ void k_extract_planes(const DiskView d, const Cell* b, double* out) {
+    const long long n = (long long)d.xres * d.yres;
+    const size_t P = plane(d);
+    for (long long m = blockIdx.x * (long long)blockDim.x + threadIdx.x; m < n; m += (long long)gridDim.x * blockDim.x) {
+        const int i = NPAD + (int)(m % d.xres), j = d.ypad + (int)(m / d.xres);
+        const Cell c = load_cell(b, d.xarr, i, j);
+        out[m] = c.r;
+        out[P + m] = c.u;
+        out[2 * P + m] = c.v;
+    }
 }
 
 static unsigned grid_for(long long n) {
@@ -1140,6 +1245,192 @@ pg_status pg_adj_dot_test(pg_adj* a, double dt, const double* dir, const double*
     ADJ_CUDA(cudaGetLastError());
     ADJ_CUDA(cudaMemcpyAsync(out10, dev, 10 * sizeof(double), cudaMemcpyDeviceToHost, st));
     ADJ_CUDA(cudaFreeAsync(dev, st));
+    ADJ_CUDA(cudaStreamSynchronize(st));
+    return PG_OK;
+}
+
+// Tangent of every production pass against central differences of the
+// production kernels themselves over one step of size dt from the newest state:
+// err[3p + 0..2] = |fd - J dir|_2 / |J dir|_2 for Sigma, v_r, v_phi of pass p
+// (kick1, sweep_x, sweep_y, advect, kick2).  dir: device, 5 interior planes.
+// The disk's state is overwritten.
+pg_status pg_adj_pass_check(pg_adj* a, double dt, double eps, const double* dir, double* err30) {
+    if (!a || !dir || !err30 || a->every < 2) return adj_fail(PG_ERR_ARG, "bad argument");
+    double* err15 = err30;
+    ADJ_CUDA(cudaSetDevice(a->device));
+    const DiskView& d = engine_view(a->E);
+    const size_t ni = a->nint(), nc = a->ncell();
+    cudaStream_t st = a->stream;
+    Scalars h{};
+    ADJ_CUDA(cudaMemcpyAsync(&h, d.sc, sizeof(Scalars), cudaMemcpyDeviceToHost, st));
+    ADJ_CUDA(cudaStreamSynchronize(st));
+    a->ts.assign(1, h.t);
+    a->dts.assign(1, dt);
+    const StepRecord r = record_slot(a, 0);
+    pg_status s = engine_step(a->E, h.t, dt, &r);
+    if (s != PG_OK) return s;
+    pg_body pl[2];
+    ADJ_CUDA(cudaMemcpyAsync(pl, a->rpl, sizeof pl, cudaMemcpyDeviceToHost, st));
+    ADJ_CUDA(cudaStreamSynchronize(st));
+    Args g = base_args(a, 0, 0, pl);
+    g.dir = dir;
+    // scratch: slot 1 stages hold perturbed inputs and outputs
+    Cell* pin = a->stages + 5 * nc;
+    Cell* outp = pin + nc;
+    Cell* outm = pin + 2 * nc;
+    double* vin = a->rvis + 2 * nc;  // slot 1 of the recorded forces: the perturbed kick1 force
+    double* vp = nullptr;
+    double* vm = nullptr;
+    double* tlm = nullptr;
+    double* mx = nullptr;
+    ADJ_CUDA(cudaMallocAsync(&vp, 2 * nc * sizeof(double), st));
+    ADJ_CUDA(cudaMallocAsync(&vm, 2 * nc * sizeof(double), st));
+    ADJ_CUDA(cudaMallocAsync(&tlm, 5 * ni * sizeof(double), st));
+    ADJ_CUDA(cudaMallocAsync(&mx, 10 * sizeof(double), st));
+    double *rp = nullptr, *rm = nullptr;
+    ADJ_CUDA(cudaMallocAsync(&rp, 3 * ni * sizeof(double), st));
+    ADJ_CUDA(cudaMallocAsync(&rm, 3 * ni * sizeof(double), st));
+    const unsigned gr = grid_for((long long)nc);
+    for (int p = 0; p < 5; ++p) {
+        if (p == P_ADV && !d.orbadv) {
+            for (int f = 0; f < 3; ++f) err15[3 * p + f] = 0.0;
+            continue;
+        }
+        const bool vis_in = (p == P_K2 && d.visc);
+        for (int sg = 0; sg < 2; ++sg) {
+            const double e = sg == 0 ? eps : -eps;
+            k_perturb<<<gr, ADJ_THREADS, 0, st>>>(d, r.stage[p], pin, vis_in ? r.vis : nullptr, vis_in ? vin : nullptr,
+                                                   dir, e);
+            if ((s = engine_run_pass(a->E, p, pin, sg == 0 ? outp : outm, vis_in ? vin : nullptr,
+                                     sg == 0 ? vp : vm)) != PG_OK)
+                return s;
+            // the restated pass on the same perturbed input, into interior planes
+            Args gm = g;
+            gm.in = pin;
+            if (vis_in) gm.vis = vin;
+            double* o = (sg == 0 ? rp : rm);
+            switch (p) {
+                case P_K1: launch_model<P_K1>(gm, o, st); break;
+                case P_SX: launch_model<P_SX>(gm, o, st); break;
+                case P_SY: launch_model<P_SY>(gm, o, st); break;
+                case P_ADV: launch_model<P_ADV>(gm, o, st); break;
+                default: launch_model<P_K2>(gm, o, st); break;
+            }
+        }
+        g.in = r.stage[p];
+        switch (p) {
+            case P_K1: k_adj_tangent<P_K1><<<gr, ADJ_THREADS, 0, st>>>(g, tlm); break;
+            case P_SX: k_adj_tangent<P_SX><<<gr, ADJ_THREADS, 0, st>>>(g, tlm); break;
+            case P_SY: k_adj_tangent<P_SY><<<gr, ADJ_THREADS, 0, st>>>(g, tlm); break;
+            case P_ADV: k_adj_tangent<P_ADV><<<gr, ADJ_THREADS, 0, st>>>(g, tlm); break;
+            default: k_adj_tangent<P_K2><<<gr, ADJ_THREADS, 0, st>>>(g, tlm); break;
+        }
+        ADJ_CUDA(cudaMemsetAsync(mx, 0, 10 * sizeof(double), st));
+        k_fd_compare<<<gr, ADJ_THREADS, 0, st>>>(d, outp, outm, (p == P_K1 && d.visc) ? vp : nullptr,
+                                                 (p == P_K1 && d.visc) ? vm : nullptr, tlm, eps, mx);
+        double hm[10];
+        ADJ_CUDA(cudaMemcpyAsync(hm, mx, sizeof hm, cudaMemcpyDeviceToHost, st));
+        ADJ_CUDA(cudaStreamSynchronize(st));
+        for (int f = 0; f < 3; ++f)
+            err15[3 * p + f] = hm[2 * f + 1] > 0.0 ? std::sqrt(hm[2 * f] / hm[2 * f + 1]) : std::sqrt(hm[2 * f]);
+        ADJ_CUDA(cudaMemsetAsync(mx, 0, 10 * sizeof(double), st));
+        k_fd_compare_planes<<<gr, ADJ_THREADS, 0, st>>>(d, rp, rm, tlm, eps, mx);
+        ADJ_CUDA(cudaMemcpyAsync(hm, mx, sizeof hm, cudaMemcpyDeviceToHost, st));
+        ADJ_CUDA(cudaStreamSynchronize(st));
+        for (int f = 0; f < 3; ++f)
+            err30[15 + 3 * p + f] = hm[2 * f + 1] > 0.0 ? std::sqrt(hm[2 * f] / hm[2 * f + 1]) : std::sqrt(hm[2 * f]);
+    }
+    cudaFreeAsync(rp, st);
+    cudaFreeAsync(rm, st);
+    cudaFreeAsync(vp, st);
+    cudaFreeAsync(vm, st);
+    cudaFreeAsync(tlm, st);
+    cudaFreeAsync(mx, st);
+    ADJ_CUDA(cudaStreamSynchronize(st));
+    return PG_OK;
+}
+
+// Diagnostic: each production pass re-run on its recorded input against the
+// recorded output (max relative difference per pass).
+pg_status pg_adj_replay_diff(pg_adj* a, double dt, double* diff5) {
+    if (!a || !diff5 || a->every < 2) return adj_fail(PG_ERR_ARG, "bad argument");
+    ADJ_CUDA(cudaSetDevice(a->device));
+    const DiskView& d = engine_view(a->E);
+    const size_t ni = a->nint(), nc = a->ncell();
+    cudaStream_t st = a->stream;
+    Scalars h{};
+    ADJ_CUDA(cudaMemcpyAsync(&h, d.sc, sizeof(Scalars), cudaMemcpyDeviceToHost, st));
+    ADJ_CUDA(cudaStreamSynchronize(st));
+    a->ts.assign(1, h.t);
+    a->dts.assign(1, dt);
+    const StepRecord r = record_slot(a, 0);
+    pg_status s = engine_step(a->E, h.t, dt, &r);
+    if (s != PG_OK) return s;
+    Cell* final_state = a->stages + 5 * nc;
+    if ((s = engine_save(a->E, final_state, a->ssc)) != PG_OK) return s;
+    Cell* out = final_state + nc;
+    ADJ_CUDA(cudaMemsetAsync(a->err, 0, 5 * sizeof(unsigned long long), st));
+    const Cell* next[5] = {r.stage[1], r.stage[2], d.orbadv ? r.stage[3] : r.stage[4], r.stage[4], final_state};
+    for (int p = 0; p < 5; ++p) {
+        if (p == P_ADV && !d.orbadv) continue;
+        if ((s = engine_run_pass(a->E, p, r.stage[p], out, p == P_K2 ? r.vis : nullptr, nullptr)) != PG_OK) return s;
+        k_extract_planes<<<grid_for((long long)ni), ADJ_THREADS, 0, st>>>(d, out, a->work);
+        k_model_err<<<grid_for((long long)ni), ADJ_THREADS, 0, st>>>(d, a->work, next[p], a->err + p);
+    }
+    ADJ_CUDA(cudaGetLastError());
+    unsigned long long e[5];
+    ADJ_CUDA(cudaMemcpyAsync(e, a->err, sizeof e, cudaMemcpyDeviceToHost, st));
+    ADJ_CUDA(cudaStreamSynchronize(st));
+    for (int p = 0; p < 5; ++p) std::memcpy(&diff5[p], &e[p], sizeof(double));
+    return PG_OK;
+}
+
+// Diagnostic: for one pass over one step of size dt from the newest state, the
+// production central difference (fd) and the forward-mode tangent (tlm) along
+// dir, each as 3 interior planes (device).  Overwrites the disk's state.
+pg_status pg_adj_pass_fields(pg_adj* a, int pass, double dt, double eps, const double* dir, double* fd, double* tlm5) {
+    if (!a || !dir || !fd || !tlm5 || a->every < 2 || pass < 0 || pass > 4) return adj_fail(PG_ERR_ARG, "bad argument");
+    ADJ_CUDA(cudaSetDevice(a->device));
+    const DiskView& d = engine_view(a->E);
+    const size_t ni = a->nint(), nc = a->ncell();
+    cudaStream_t st = a->stream;
+    Scalars h{};
+    ADJ_CUDA(cudaMemcpyAsync(&h, d.sc, sizeof(Scalars), cudaMemcpyDeviceToHost, st));
+    ADJ_CUDA(cudaStreamSynchronize(st));
+    a->ts.assign(1, h.t);
+    a->dts.assign(1, dt);
+    const StepRecord r = record_slot(a, 0);
+    pg_status s = engine_step(a->E, h.t, dt, &r);
+    if (s != PG_OK) return s;
+    pg_body pl[2];
+    ADJ_CUDA(cudaMemcpyAsync(pl, a->rpl, sizeof pl, cudaMemcpyDeviceToHost, st));
+    ADJ_CUDA(cudaStreamSynchronize(st));
+    Args g = base_args(a, 0, 0, pl);
+    g.dir = dir;
+    g.in = r.stage[pass];
+    Cell* pin = a->stages + 5 * nc;
+    Cell* outs[2] = {pin + nc, pin + 2 * nc};
+    double* vin = a->rvis + 2 * nc;
+    const bool vis_in = (pass == P_K2 && d.visc);
+    const unsigned gr = grid_for((long long)nc);
+    switch (pass) {
+        case P_K1: k_adj_tangent<P_K1><<<gr, ADJ_THREADS, 0, st>>>(g, tlm5); break;
+        case P_SX: k_adj_tangent<P_SX><<<gr, ADJ_THREADS, 0, st>>>(g, tlm5); break;
+        case P_SY: k_adj_tangent<P_SY><<<gr, ADJ_THREADS, 0, st>>>(g, tlm5); break;
+        case P_ADV: k_adj_tangent<P_ADV><<<gr, ADJ_THREADS, 0, st>>>(g, tlm5); break;
+        default: k_adj_tangent<P_K2><<<gr, ADJ_THREADS, 0, st>>>(g, tlm5); break;
+    }
+    for (int sg = 0; sg < 2; ++sg) {
+        k_perturb<<<gr, ADJ_THREADS, 0, st>>>(d, r.stage[pass], pin, vis_in ? r.vis : nullptr, vis_in ? vin : nullptr,
+                                               dir, sg == 0 ? eps : -eps);
+        if ((s = engine_run_pass(a->E, pass, pin, outs[sg], vis_in ? vin : nullptr, nullptr)) != PG_OK) return s;
+    }
+    k_extract_planes<<<grid_for((long long)ni), ADJ_THREADS, 0, st>>>(d, outs[0], fd);
+    k_extract_planes<<<grid_for((long long)ni), ADJ_THREADS, 0, st>>>(d, outs[1], a->work);
+    ADJ_CUDA(cudaGetLastError());
+    ADJ_CUDA(cudaStreamSynchronize(st));
+    // fd = (plus - minus) / 2 eps on the host side of the caller: both planes returned
+    ADJ_CUDA(cudaMemcpyAsync(fd + 3 * ni, a->work, 3 * ni * sizeof(double), cudaMemcpyDeviceToDevice, st));
     ADJ_CUDA(cudaStreamSynchronize(st));
     return PG_OK;
 }

@@ -824,6 +824,36 @@ pg_status engine_restore(Engine* E, const Cell* cells, const Scalars* sc) {
     return PG_OK;
 }
 
+// One production pass on a given input (test support for the adjoint): in ->
+// out (all cells), kick2 reading vis_in as kick1's force, kick1 leaving its
+// force in vis_out.  The planet and dt are those of the last step taken; the
+// disk's own state is overwritten.
+pg_status engine_run_pass(Engine* E, int pass, const Cell* in, Cell* out, const double* vis_in, double* vis_out) {
+    const DiskView& d = E->view;
+    const size_t n = (size_t)d.xarr * d.yarr;
+    pg_status s;
+    PG_CUDA(cudaMemcpyAsync(E->buf[0], in, n * sizeof(Cell), cudaMemcpyDeviceToDevice, E->stream));
+    for (int k = 0; k < 2; ++k)
+        if ((s = make_cell_maps(E->maps[k], E->buf[k], d.xarr, d.yarr)) != PG_OK) return s;
+    if (d.visc && (s = make_vis_maps(E->vmap, E->vis, d.xarr, d.yarr)) != PG_OK) return s;
+    if (pass == 4 && d.visc && vis_in)
+        PG_CUDA(cudaMemcpyAsync(E->vis, vis_in, 2 * n * sizeof(double), cudaMemcpyDeviceToDevice, E->stream));
+    switch (pass) {
+        case 0: launch_kick1(d, E->maps[0], E->buf[1], E->vis, E->stream); break;
+        case 1: launch_sweep_x(d, E->maps[0], E->buf[1], E->stream); break;
+        case 2: launch_sweep_y(d, E->maps[0], E->buf[1], E->stream); break;
+        case 3: launch_advect(d, E->maps[0], E->buf[1], E->stream); break;
+        default: launch_kick2(d, E->maps[0], E->vmap, E->buf[1], E->stream); break;
+    }
+    PG_CUDA(cudaGetLastError());
+    PG_CUDA(cudaMemcpyAsync(out, E->buf[1], n * sizeof(Cell), cudaMemcpyDeviceToDevice, E->stream));
+    if (pass == 0 && d.visc && vis_out)
+        PG_CUDA(cudaMemcpyAsync(vis_out, E->vis, 2 * n * sizeof(double), cudaMemcpyDeviceToDevice, E->stream));
+    E->cur = 1;
+    E->pending = false;
+    return PG_OK;
+}
+
 // Interior fields of the newest state into device arrays (xres*yres each).
 pg_status engine_extract_device(Engine* E, double* r, double* p, double* u, double* v) {
     pg_status s0 = resolve_cur(*E);

@@ -180,6 +180,13 @@ def dust_disk(nr: int = 768, nphi: int = 2048, *, stokes: float = 0.01, q: float
     return planet_disk(nr, nphi, q=q, alpha=alpha).replace(dust_flag=1, Stokes=stokes, D_G_ratio=d_g_ratio)
 
 
+def adjoint_disk(nr: int = 256, nphi: int = 768, *, q: float = 5.0e-4, alpha: float = 1.0e-3,
+                 h: float = 0.05) -> Params:
+    """The disk of the gradient workload: log r in [0.5, 2], h/r 0.05, alpha 1e-3,
+    q 5e-4, orbital advection, no wave damping (the adjoint covers kill_flag 0)."""
+    return planet_disk(nr, nphi, q=q, alpha=alpha, h=h, rmin=0.5, rmax=2.0).replace(kill_flag=0)
+
+
 def reference_disk(nr: int, nphi: int, **kw) -> Params:
     """Planet-disk variant that the reference can run as-is: it has a single
     ``kill_width`` for both damping zones (src/killwave/killwave.cu:30-34), so
