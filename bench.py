@@ -351,6 +351,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-forms", action="store_true", help="skip the FP32-mixed, ensemble and dust measurements")
+    ap.add_argument("--no-tune", action="store_true", help="default launch configuration instead of the autotuner's")
     ap.add_argument("--forms", default="fp32,ensemble,dust,adjoint",
                     help="comma list of the extra measurements after the FP64 headline "
                          "(fp32, ensemble, dust, adjoint)")
@@ -387,6 +388,7 @@ def main():
     disk.run(W)
     disk.sync()
     disk.check()
+    tuning = disk.autotune(reps=5) if not args.no_tune else None
 
     def barrier():
         if dist:
@@ -475,7 +477,8 @@ def main():
         "config": {"workload": f"planet-disk {p.xres}x{p.yres} FP64 (plain form), seeded 1e-4 Sigma noise, t0=0",
                    "cells_per_gpu": cells, "state_bytes": 2 * 40 * (p.xres + 6) * (p.yres + 6),
                    "l2": "inputs larger than L2 (two 127 MB AoS state buffers)",
-                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                   "tuning": tuning},
         "gpu_launches": disk.kernels_per_step * K,
         "stage_ms": prof,
         "roofline": {"bound": "hbm", "kernel": stage, "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",

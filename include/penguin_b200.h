@@ -142,6 +142,15 @@ pg_status pg_disk_set_state(pg_disk* d, double t, const double* r, const double*
                             const double* v);
 /* The newest state back to host arrays; t_out may be NULL. */
 pg_status pg_disk_get_state(pg_disk* d, double* r, double* p, double* u, double* v, double* t_out);
+/* Autotuner: times every launch configuration of each pass of the step
+   (pencils per tile 8 or 4 for the sweeps and the residual advection, CTAs per
+   SM) on the disk's current state over `reps` launches and keeps the fastest;
+   the state is unchanged and results stay bit for bit the same.  choice (may
+   be NULL, 8 ints): pencils per tile of sweep_x, sweep_y, advect, then CTAs per
+   SM of kick1, sweep_x, sweep_y, advect, kick2 (0: all that fit).
+   pg_disk_set_tuning applies a choice found earlier. */
+pg_status pg_disk_autotune(pg_disk* d, int reps, int* choice);
+pg_status pg_disk_set_tuning(pg_disk* d, const int* choice);
 /* dust_flag: the interior dust (density, radial and azimuthal velocity, host
    arrays of xres*yres) of the newest state.  pg_disk_set_state resets the dust
    to init_CD, as the reference's restart does (load_grid reads the gas only,

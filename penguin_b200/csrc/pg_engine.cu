@@ -240,6 +240,8 @@ static pg_status make_cell_maps(CellMaps& M, const Cell* buf, int xarr, int yarr
     if ((s = make_map(&M.sweep_x, buf, 5ull * xarr, yarr, 5 * 38, 8)) != PG_OK) return s;
     if ((s = make_map(&M.sweep_y, buf, 5ull * xarr, yarr, 5 * 10, 38)) != PG_OK) return s;
     if ((s = make_map(&M.stencil, buf, 5ull * xarr, yarr, 5 * 34, 10)) != PG_OK) return s;
+    if ((s = make_map(&M.sweep_x4, buf, 5ull * xarr, yarr, 5 * 38, 4)) != PG_OK) return s;
+    if ((s = make_map(&M.sweep_y4, buf, 5ull * xarr, yarr, 5 * 6, 38)) != PG_OK) return s;
     M.base = buf;
     return PG_OK;
 }
@@ -317,6 +319,7 @@ struct Engine {
     double* part = nullptr;            // per-block partial sums of diagnostics
     pg_dust* dbuf[2] = {nullptr, nullptr};  // dust_flag: the dust of buf[k] is dbuf[k]
     DustMaps dmaps[2];
+    Tune tune;                               // launch configuration (pg_disk_autotune)
 
     ~Engine() {
         for (auto& g : graph)
@@ -500,17 +503,18 @@ static pg_status enqueue_stages(Engine& E, const StepRecord* rec = nullptr) {
         for (int k = 0; k < 2; ++k)
             if ((s = make_dust_maps(E.dmaps[k], E.dbuf[k], d.xarr, d.yarr)) != PG_OK) return s;
     save(0);
-    launch_kick1(d, maps(c), E.buf[1 - c], E.vis, E.stream, dust ? D[c] : nullptr, dust ? D[1 - c] : nullptr);
+    launch_kick1(d, maps(c), E.buf[1 - c], E.vis, E.stream, dust ? D[c] : nullptr, dust ? D[1 - c] : nullptr,
+                 &E.tune);
     if (rec && d.visc)
         cudaMemcpyAsync(rec->vis, E.vis, 2 * ncell * sizeof(double), cudaMemcpyDeviceToDevice, E.stream);
     c = 1 - c;
     save(1);
-    launch_sweep_x(d, maps(c), E.buf[1 - c], E.stream);
+    launch_sweep_x(d, maps(c), E.buf[1 - c], E.stream, &E.tune);
     if (dust) launch_dsweep_x(d, E.dmaps[c], D[1 - c], E.stream);
     c = 1 - c;
     if (d.ndim > 1) {
         save(2);
-        launch_sweep_y(d, maps(c), E.buf[1 - c], E.stream);
+        launch_sweep_y(d, maps(c), E.buf[1 - c], E.stream, &E.tune);
         if (dust) launch_dsweep_y(d, E.dmaps[c], D[1 - c], E.stream);
         if (rec) {
             cudaMemcpyAsync(rec->res, E.res, d.xarr * sizeof(double), cudaMemcpyDeviceToDevice, E.stream);
@@ -520,12 +524,13 @@ static pg_status enqueue_stages(Engine& E, const StepRecord* rec = nullptr) {
     }
     if (d.ndim > 1 && d.orbadv) {
         save(3);
-        launch_advect(d, maps(c), E.buf[1 - c], E.stream);
+        launch_advect(d, maps(c), E.buf[1 - c], E.stream, &E.tune);
         if (dust) launch_dadvect(d, E.dmaps[c], D[1 - c], E.stream);
         c = 1 - c;
     }
     save(4);
-    launch_kick2(d, maps(c), E.vmap, E.buf[1 - c], E.stream, dust ? D[c] : nullptr, dust ? D[1 - c] : nullptr);
+    launch_kick2(d, maps(c), E.vmap, E.buf[1 - c], E.stream, dust ? D[c] : nullptr, dust ? D[1 - c] : nullptr,
+                 &E.tune);
     c = 1 - c;
     E.cur = c;
     PG_CUDA(cudaGetLastError());
@@ -839,11 +844,11 @@ pg_status engine_run_pass(Engine* E, int pass, const Cell* in, Cell* out, const 
     if (pass == 4 && d.visc && vis_in)
         PG_CUDA(cudaMemcpyAsync(E->vis, vis_in, 2 * n * sizeof(double), cudaMemcpyDeviceToDevice, E->stream));
     switch (pass) {
-        case 0: launch_kick1(d, E->maps[0], E->buf[1], E->vis, E->stream); break;
-        case 1: launch_sweep_x(d, E->maps[0], E->buf[1], E->stream); break;
-        case 2: launch_sweep_y(d, E->maps[0], E->buf[1], E->stream); break;
-        case 3: launch_advect(d, E->maps[0], E->buf[1], E->stream); break;
-        default: launch_kick2(d, E->maps[0], E->vmap, E->buf[1], E->stream); break;
+        case 0: launch_kick1(d, E->maps[0], E->buf[1], E->vis, E->stream, nullptr, nullptr, &E->tune); break;
+        case 1: launch_sweep_x(d, E->maps[0], E->buf[1], E->stream, &E->tune); break;
+        case 2: launch_sweep_y(d, E->maps[0], E->buf[1], E->stream, &E->tune); break;
+        case 3: launch_advect(d, E->maps[0], E->buf[1], E->stream, &E->tune); break;
+        default: launch_kick2(d, E->maps[0], E->vmap, E->buf[1], E->stream, nullptr, nullptr, &E->tune); break;
     }
     PG_CUDA(cudaGetLastError());
     PG_CUDA(cudaMemcpyAsync(out, E->buf[1], n * sizeof(Cell), cudaMemcpyDeviceToDevice, E->stream));
@@ -1090,6 +1095,117 @@ pg_status pg_disk_torque(pg_disk* dk, double* torque) {
 
 int pg_kernels_per_step(const pg_disk* dk) { return dk ? kernels_per_step(dk->E->view) : 0; }
 
+// Autotuner: for every pass, times each launch configuration (pencils per tile
+// W in {8, 4} for the sweeps and the advection; CTAs per SM from 1 to what
+// fits) on the disk's current state with CUDA events over `reps` launches and
+// keeps the fastest.  The state, clock and planet are restored afterwards; the
+// per-cell arithmetic does not depend on the configuration, so results stay
+// bit for bit the same.  choice (may be NULL): w[3] then cps[5].
+pg_status pg_disk_autotune(pg_disk* dk, int reps, int* choice) {
+    if (!dk || reps < 1) return fail(PG_ERR_ARG, "bad argument");
+    Engine& E = *dk->E;
+    const DiskView& d = E.view;
+    PG_CUDA(cudaSetDevice(E.device));
+    pg_status s = resolve_cur(E);
+    if (s != PG_OK) return s;
+    const size_t n = (size_t)d.xarr * d.yarr;
+    Cell* saved = nullptr;
+    Scalars* ssc = nullptr;
+    PG_CUDA(cudaMallocAsync(&saved, n * sizeof(Cell), E.stream));
+    PG_CUDA(cudaMallocAsync(&ssc, sizeof(Scalars), E.stream));
+    const int c = E.cur;
+    PG_CUDA(cudaMemcpyAsync(saved, E.buf[c], n * sizeof(Cell), cudaMemcpyDeviceToDevice, E.stream));
+    PG_CUDA(cudaMemcpyAsync(ssc, E.sc, sizeof(Scalars), cudaMemcpyDeviceToDevice, E.stream));
+    double dt = 0.0;
+    if ((s = pg_disk_global_dt(dk, 1.0e30, &dt)) != PG_OK) return s;
+    Scalars h{};
+    PG_CUDA(cudaMemcpyAsync(&h, E.sc, sizeof(Scalars), cudaMemcpyDeviceToHost, E.stream));
+    PG_CUDA(cudaStreamSynchronize(E.stream));
+    launch_set_time(d, h.t, dt, E.stream);
+    for (int k = 0; k < 2; ++k)
+        if ((s = make_cell_maps(E.maps[k], E.buf[k], d.xarr, d.yarr)) != PG_OK) return s;
+    if (d.visc && (s = make_vis_maps(E.vmap, E.vis, d.xarr, d.yarr)) != PG_OK) return s;
+    cudaEvent_t e0, e1;
+    PG_CUDA(cudaEventCreate(&e0));
+    PG_CUDA(cudaEventCreate(&e1));
+    auto launch = [&](int p, const Tune& t) {
+        switch (p) {
+            case 0: launch_kick1(d, E.maps[c], E.buf[1 - c], E.vis, E.stream, nullptr, nullptr, &t); break;
+            case 1: launch_sweep_x(d, E.maps[c], E.buf[1 - c], E.stream, &t); break;
+            case 2: launch_sweep_y(d, E.maps[c], E.buf[1 - c], E.stream, &t); break;
+            case 3: launch_advect(d, E.maps[c], E.buf[1 - c], E.stream, &t); break;
+            default: launch_kick2(d, E.maps[c], E.vmap, E.buf[1 - c], E.stream, nullptr, nullptr, &t); break;
+        }
+    };
+    Tune best = E.tune;
+    for (int p = 0; p < 5; ++p) {
+        if ((p == 2 && d.ndim < 2) || (p == 3 && !(d.ndim > 1 && d.orbadv))) continue;
+        float best_ms = 1.0e30f;
+        for (int w : {8, 4}) {
+            if (w == 4 && (p == 0 || p == 4)) continue;
+            const int occ = pass_occupancy(d, p, w);
+            for (int cps = 1; cps <= occ; ++cps) {
+                Tune t = best;
+                if (p >= 1 && p <= 3) t.w[p - 1] = w;
+                t.cps[p] = cps;
+                launch(p, t);  // warm-up
+                PG_CUDA(cudaEventRecord(e0, E.stream));
+                for (int r = 0; r < reps; ++r) launch(p, t);
+                PG_CUDA(cudaEventRecord(e1, E.stream));
+                PG_CUDA(cudaEventSynchronize(e1));
+                PG_CUDA(cudaGetLastError());
+                float ms = 0.0f;
+                PG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+                if (ms < best_ms) {
+                    best_ms = ms;
+                    if (p >= 1 && p <= 3) best.w[p - 1] = w;
+                    best.cps[p] = cps;
+                }
+            }
+        }
+        if (p == 0) launch(0, best);  // kick2 reads the force kick1 leaves
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    E.tune = best;
+    for (auto& g : E.graph)
+        if (g) {
+            cudaGraphExecDestroy(g);
+            g = nullptr;
+        }
+    PG_CUDA(cudaMemcpyAsync(E.buf[c], saved, n * sizeof(Cell), cudaMemcpyDeviceToDevice, E.stream));
+    PG_CUDA(cudaMemcpyAsync(E.sc, ssc, sizeof(Scalars), cudaMemcpyDeviceToDevice, E.stream));
+    PG_CUDA(cudaFreeAsync(saved, E.stream));
+    PG_CUDA(cudaFreeAsync(ssc, E.stream));
+    PG_CUDA(cudaStreamSynchronize(E.stream));
+    if (choice) {
+        for (int k = 0; k < 3; ++k) choice[k] = best.w[k];
+        for (int k = 0; k < 5; ++k) choice[3 + k] = best.cps[k];
+    }
+    return PG_OK;
+}
+
+pg_status pg_disk_set_tuning(pg_disk* dk, const int* choice) {
+    if (!dk || !choice) return fail(PG_ERR_ARG, "bad argument");
+    Tune t;
+    for (int k = 0; k < 3; ++k) {
+        if (choice[k] != 8 && choice[k] != 4) return fail(PG_ERR_ARG, "pencils per tile must be 8 or 4");
+        t.w[k] = choice[k];
+    }
+    for (int k = 0; k < 5; ++k) {
+        if (choice[3 + k] < 0) return fail(PG_ERR_ARG, "CTAs per SM must be >= 0");
+        t.cps[k] = choice[3 + k];
+    }
+    Engine& E = *dk->E;
+    E.tune = t;
+    for (auto& g : E.graph)
+        if (g) {
+            cudaGraphExecDestroy(g);
+            g = nullptr;
+        }
+    return PG_OK;
+}
+
 pg_status pg_disk_profile(pg_disk* dk, int nsteps, double end_time, float* ms, int nslot) {
     if (!dk || !ms || nslot < 6) return fail(PG_ERR_ARG, "bad argument");
     Engine& E = *dk->E;
@@ -1123,26 +1239,28 @@ pg_status pg_disk_profile(pg_disk* dk, int nsteps, double end_time, float* ms, i
         PG_CUDA(cudaEventRecord(ev[0], E.stream));
         launch_time_step(d, E.stream);
         PG_CUDA(cudaEventRecord(ev[1], E.stream));
-        launch_kick1(d, E.maps[c], E.buf[1 - c], E.vis, E.stream, dust ? D[c] : nullptr, dust ? D[1 - c] : nullptr);
+        launch_kick1(d, E.maps[c], E.buf[1 - c], E.vis, E.stream, dust ? D[c] : nullptr, dust ? D[1 - c] : nullptr,
+                     &E.tune);
         c = 1 - c;
         PG_CUDA(cudaEventRecord(ev[2], E.stream));
-        launch_sweep_x(d, E.maps[c], E.buf[1 - c], E.stream);
+        launch_sweep_x(d, E.maps[c], E.buf[1 - c], E.stream, &E.tune);
         if (dust) launch_dsweep_x(d, E.dmaps[c], D[1 - c], E.stream);
         c = 1 - c;
         PG_CUDA(cudaEventRecord(ev[3], E.stream));
         if (d.ndim > 1) {
-            launch_sweep_y(d, E.maps[c], E.buf[1 - c], E.stream);
+            launch_sweep_y(d, E.maps[c], E.buf[1 - c], E.stream, &E.tune);
             if (dust) launch_dsweep_y(d, E.dmaps[c], D[1 - c], E.stream);
             c = 1 - c;
         }
         PG_CUDA(cudaEventRecord(ev[4], E.stream));
         if (d.ndim > 1 && d.orbadv) {
-            launch_advect(d, E.maps[c], E.buf[1 - c], E.stream);
+            launch_advect(d, E.maps[c], E.buf[1 - c], E.stream, &E.tune);
             if (dust) launch_dadvect(d, E.dmaps[c], D[1 - c], E.stream);
             c = 1 - c;
         }
         PG_CUDA(cudaEventRecord(ev[5], E.stream));
-        launch_kick2(d, E.maps[c], E.vmap, E.buf[1 - c], E.stream, dust ? D[c] : nullptr, dust ? D[1 - c] : nullptr);
+        launch_kick2(d, E.maps[c], E.vmap, E.buf[1 - c], E.stream, dust ? D[c] : nullptr, dust ? D[1 - c] : nullptr,
+                     &E.tune);
         c = 1 - c;
         PG_CUDA(cudaEventRecord(ev[6], E.stream));
         PG_CUDA(cudaGetLastError());

@@ -14,6 +14,13 @@ struct CellMaps {
     CUtensorMap sweep_x;   // box {5*38, 8}: x-pencils
     CUtensorMap sweep_y;   // box {5*10, 38}: y-pencils (one extra column each side for 16-B alignment)
     CUtensorMap stencil;   // box {5*34, 10}: 32x8 cells + 1 halo
+    CUtensorMap sweep_x4;  // box {5*38, 4}: 4 x-pencils per tile
+    CUtensorMap sweep_y4;  // box {5*6, 38}: 4 y-pencils per tile
+};
+// Launch configuration of the FP64 passes (pg_disk_autotune).
+struct Tune {
+    int w[3] = {8, 8, 8};          // pencils per tile: sweep_x, sweep_y, advect (8 or 4)
+    int cps[5] = {0, 0, 0, 0, 0};  // CTAs per SM: kick1, sweep_x, sweep_y, advect, kick2 (0: all that fit)
 };
 struct VisMaps {
     const void* base = nullptr;
@@ -43,12 +50,13 @@ void launch_cfl(const DiskView& d, const Cell* buf, cudaStream_t s, const pg_dus
 void launch_set_time(const DiskView& d, double t, double dt, cudaStream_t s);
 void launch_time_step(const DiskView& d, cudaStream_t s);
 void launch_kick1(const DiskView& d, const CellMaps& in, Cell* out, double* vis, cudaStream_t s,
-                  const pg_dust* din = nullptr, pg_dust* dout = nullptr);
-void launch_sweep_x(const DiskView& d, const CellMaps& in, Cell* out, cudaStream_t s);
-void launch_sweep_y(const DiskView& d, const CellMaps& in, Cell* out, cudaStream_t s);
-void launch_advect(const DiskView& d, const CellMaps& in, Cell* out, cudaStream_t s);
+                  const pg_dust* din = nullptr, pg_dust* dout = nullptr, const Tune* t = nullptr);
+void launch_sweep_x(const DiskView& d, const CellMaps& in, Cell* out, cudaStream_t s, const Tune* t = nullptr);
+void launch_sweep_y(const DiskView& d, const CellMaps& in, Cell* out, cudaStream_t s, const Tune* t = nullptr);
+void launch_advect(const DiskView& d, const CellMaps& in, Cell* out, cudaStream_t s, const Tune* t = nullptr);
 void launch_kick2(const DiskView& d, const CellMaps& in, const VisMaps& vis, Cell* out, cudaStream_t s,
-                  const pg_dust* din = nullptr, pg_dust* dout = nullptr);
+                  const pg_dust* din = nullptr, pg_dust* dout = nullptr, const Tune* t = nullptr);
+int pass_occupancy(const DiskView& d, int pass, int w);
 void launch_init_planet(const DiskView& d, const pg_params& P, double t, cudaStream_t s);
 void launch_torque(const DiskView& d, const Cell* buf, double* part, int nblocks, cudaStream_t s);
 // compensated sum of n doubles in index order

@@ -26,20 +26,25 @@
 namespace pg {
 
 // ---------------------------------------------------------------- tiles
+// Sweep and advection tiles: SW_LEN outputs along the sweep times W pencils per
+// CTA; W (8 or 4) is chosen per pass by the autotuner (pg_disk_autotune).
 constexpr int SW_LEN = 32;                  // outputs along the sweep per CTA
-constexpr int SW_W = 8;                     // pencils per CTA
 constexpr int SW_TL = SW_LEN + 2 * NPAD;    // 38 tile cells along the sweep
 constexpr int SW_P1 = SW_LEN + 2;           // cells reconstructed per pencil
 constexpr int SW_P2 = SW_LEN + 1;           // faces per pencil
-constexpr int SW_THREADS = 288;             // >= SW_P1 * SW_W
-constexpr int SWY_COLS = SW_W + 2;          // y tiles start one column early (16-B aligned TMA x)
-constexpr int SWX_TILE = SW_W * SW_TL * 5;  // doubles
-constexpr int SWY_TILE = SW_TL * SWY_COLS * 5;
-constexpr int SW_TILE_MAX = (SWY_TILE + 15) / 16 * 16;
-constexpr int SW_NST = SW_P1 * SW_W;        // 272 reconstructed cells
-constexpr int SW_NFX = SW_P2 * SW_W;        // 264 faces
-constexpr size_t SW_SMEM = (size_t)(2 * SW_TILE_MAX + 10 * SW_NST + 7 * SW_NFX) * 8 + 16 + 128;
-constexpr size_t AD_SMEM = (size_t)(2 * SW_TILE_MAX + 5 * SW_TL * SW_W) * 8 + 16 + 128;
+template <int W>
+struct Sw {
+    static constexpr int THREADS = (SW_P1 * W + 31) / 32 * 32;  // 288 for W 8, 160 for W 4
+    static constexpr int MINB = (W == 8) ? 2 : 4;                 // CTAs per SM the registers allow
+    static constexpr int YCOLS = W + 2;                           // y tiles start one column early (16-B TMA x)
+    static constexpr int XTILE = W * SW_TL * 5;                   // doubles
+    static constexpr int YTILE = SW_TL * YCOLS * 5;
+    static constexpr int TILE_MAX = (YTILE + 15) / 16 * 16;
+    static constexpr int NST = SW_P1 * W;                         // reconstructed cells
+    static constexpr int NFX = SW_P2 * W;                         // faces
+    static constexpr size_t SMEM = (size_t)(2 * TILE_MAX + 10 * NST + 7 * NFX) * 8 + 16 + 128;
+    static constexpr size_t AD_SMEM = (size_t)(2 * TILE_MAX + 5 * SW_TL * W) * 8 + 16 + 128;
+};
 
 constexpr int ST_TX = 32, ST_TY = 8;        // stencil kernels: 32 x 8 outputs
 constexpr int ST_HX = ST_TX + 2, ST_HY = ST_TY + 2;
@@ -147,9 +152,12 @@ __device__ __forceinline__ double signal_rate(const DiskView& d, const Cell& c, 
 
 // ================================================================ sweeps
 // DIR 0: radial pencils (rows of the array), DIR 1: azimuthal pencils (columns).
-template <int DIR>
-__global__ void __launch_bounds__(SW_THREADS, 2)
+template <int DIR, int NW>
+__global__ void __launch_bounds__(Sw<NW>::THREADS, Sw<NW>::MINB)
     k_sweep(const __grid_constant__ CUtensorMap tm, const DiskView d, Cell* __restrict__ out, int ntx, int ntiles) {
+    using G = Sw<NW>;
+    constexpr int SW_W = NW, SW_TILE_MAX = G::TILE_MAX, SW_NST = G::NST, SW_NFX = G::NFX, SWY_COLS = G::YCOLS;
+    constexpr int SWX_TILE = G::XTILE, SWY_TILE = G::YTILE;
     extern __shared__ __align__(128) double smem_raw[];
     double* smem = smem_base128(smem_raw);
     auto stage = [&](int n) { return smem + (n & 1) * SW_TILE_MAX; };
@@ -361,8 +369,11 @@ __global__ void __launch_bounds__(SW_THREADS, 2)
 }
 
 // ===================================================== residual advection
-__global__ void __launch_bounds__(SW_THREADS, 2)
+template <int NW>
+__global__ void __launch_bounds__(Sw<NW>::THREADS, Sw<NW>::MINB)
     k_advect(const __grid_constant__ CUtensorMap tm, const DiskView d, Cell* __restrict__ out, int ntx, int ntiles) {
+    using G = Sw<NW>;
+    constexpr int SW_W = NW, SW_TILE_MAX = G::TILE_MAX, SW_NST = G::NST, SWY_COLS = G::YCOLS, SWY_TILE = G::YTILE;
     extern __shared__ __align__(128) double smem_raw[];
     double* smem = smem_base128(smem_raw);
     auto stage = [&](int n) { return smem + (n & 1) * SW_TILE_MAX; };
@@ -970,9 +981,12 @@ cudaError_t set_kernel_attributes() {
         r = cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
         if (r != cudaSuccess) e = r;
     };
-    set((const void*)k_sweep<0>, SW_SMEM);
-    set((const void*)k_sweep<1>, SW_SMEM);
-    set((const void*)k_advect, AD_SMEM);
+    set((const void*)k_sweep<0, 8>, Sw<8>::SMEM);
+    set((const void*)k_sweep<1, 8>, Sw<8>::SMEM);
+    set((const void*)k_advect<8>, Sw<8>::AD_SMEM);
+    set((const void*)k_sweep<0, 4>, Sw<4>::SMEM);
+    set((const void*)k_sweep<1, 4>, Sw<4>::SMEM);
+    set((const void*)k_advect<4>, Sw<4>::AD_SMEM);
     set((const void*)k_kick1<true>, K1_SMEM);
     set((const void*)k_kick1<false>, K1_SMEM);
     set((const void*)k_kick2<true>, K5_SMEM);
@@ -1036,7 +1050,11 @@ void launch_init_planet(const DiskView& d, const pg_params& P, double t, cudaStr
 }
 
 // Persistent grid: as many CTAs as fit on the GPU at once, each looping over tiles.
-static unsigned persistent_grid(const void* kernel, int threads, size_t smem, long long ntiles) {
+static int kernel_occupancy(const void* kernel, int threads, size_t smem);
+
+// Persistent grid: as many CTAs as fit on the GPU at once (at most cps per SM
+// when cps > 0), each looping over tiles.
+static unsigned persistent_grid(const void* kernel, int threads, size_t smem, long long ntiles, int cps = 0) {
     static int nsm = 0;
     if (nsm == 0) {
         int dev = 0;
@@ -1044,67 +1062,102 @@ static unsigned persistent_grid(const void* kernel, int threads, size_t smem, lo
         cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
         if (nsm <= 0) nsm = 148;
     }
+    int per_sm = kernel_occupancy(kernel, threads, smem);
+    if (cps > 0 && cps < per_sm) per_sm = cps;
+    long long g = (long long)per_sm * nsm;
+    if (g > ntiles) g = ntiles;
+    return (unsigned)(g < 1 ? 1 : g);
+}
+
+static int kernel_occupancy(const void* kernel, int threads, size_t smem) {
     // occupancy of each kernel, queried once (launches repeat every step)
-    static const void* keys[16] = {nullptr};
-    static int vals[16] = {0};
+    static const void* keys[32] = {nullptr};
+    static int vals[32] = {0};
     int per_sm = 0;
-    for (int n = 0; n < 16 && keys[n]; ++n)
+    for (int n = 0; n < 32 && keys[n]; ++n)
         if (keys[n] == kernel) per_sm = vals[n];
     if (per_sm == 0) {
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem) != cudaSuccess ||
             per_sm < 1)
             per_sm = 1;
-        for (int n = 0; n < 16; ++n)
+        for (int n = 0; n < 32; ++n)
             if (!keys[n]) {
                 keys[n] = kernel;
                 vals[n] = per_sm;
                 break;
             }
     }
-    long long g = (long long)per_sm * nsm;
-    if (g > ntiles) g = ntiles;
-    return (unsigned)(g < 1 ? 1 : g);
+    return per_sm;
 }
 
 void launch_kick1(const DiskView& d, const CellMaps& in, Cell* out, double* vis, cudaStream_t s, const pg_dust* din,
-                  pg_dust* dout) {
+                  pg_dust* dout, const Tune* t) {
     const int ntx = (int)cdiv(d.xres, ST_TX), nt = ntx * (int)cdiv(d.yres, ST_TY);
+    const int cps = t ? t->cps[0] : 0;
     if (d.visc && d.ndim == 2) {
-        const unsigned g = persistent_grid((const void*)k_kick1<true>, ST_THREADS, K1_SMEM, nt);
+        const unsigned g = persistent_grid((const void*)k_kick1<true>, ST_THREADS, K1_SMEM, nt, cps);
         k_kick1<true><<<g, ST_THREADS, K1_SMEM, s>>>(in.stencil, d, out, vis, ntx, nt, din, dout);
     } else {
-        const unsigned g = persistent_grid((const void*)k_kick1<false>, ST_THREADS, K1_SMEM, nt);
+        const unsigned g = persistent_grid((const void*)k_kick1<false>, ST_THREADS, K1_SMEM, nt, cps);
         k_kick1<false><<<g, ST_THREADS, K1_SMEM, s>>>(in.stencil, d, out, vis, ntx, nt, din, dout);
     }
 }
 
-void launch_sweep_x(const DiskView& d, const CellMaps& in, Cell* out, cudaStream_t s) {
-    const int ntx = (int)cdiv(d.xres, SW_LEN), nt = ntx * (int)cdiv(d.yres, SW_W);
-    const unsigned g = persistent_grid((const void*)k_sweep<0>, SW_THREADS, SW_SMEM, nt);
-    k_sweep<0><<<g, SW_THREADS, SW_SMEM, s>>>(in.sweep_x, d, out, ntx, nt);
+template <int DIR, int W>
+static void sweep_w(const DiskView& d, const CUtensorMap& m, Cell* out, cudaStream_t s, int cps) {
+    const int ntx = (int)cdiv(DIR == 0 ? d.xres : d.yres, SW_LEN);
+    const int nt = ntx * (int)cdiv(DIR == 0 ? d.yres : d.xres, W);
+    const unsigned g = persistent_grid((const void*)k_sweep<DIR, W>, Sw<W>::THREADS, Sw<W>::SMEM, nt, cps);
+    k_sweep<DIR, W><<<g, Sw<W>::THREADS, Sw<W>::SMEM, s>>>(m, d, out, ntx, nt);
 }
 
-void launch_sweep_y(const DiskView& d, const CellMaps& in, Cell* out, cudaStream_t s) {
-    const int ntx = (int)cdiv(d.yres, SW_LEN), nt = ntx * (int)cdiv(d.xres, SW_W);
-    const unsigned g = persistent_grid((const void*)k_sweep<1>, SW_THREADS, SW_SMEM, nt);
-    k_sweep<1><<<g, SW_THREADS, SW_SMEM, s>>>(in.sweep_y, d, out, ntx, nt);
+void launch_sweep_x(const DiskView& d, const CellMaps& in, Cell* out, cudaStream_t s, const Tune* t) {
+    if (t && t->w[0] == 4) sweep_w<0, 4>(d, in.sweep_x4, out, s, t->cps[1]);
+    else sweep_w<0, 8>(d, in.sweep_x, out, s, t ? t->cps[1] : 0);
 }
 
-void launch_advect(const DiskView& d, const CellMaps& in, Cell* out, cudaStream_t s) {
-    const int ntx = (int)cdiv(d.yres, SW_LEN), nt = ntx * (int)cdiv(d.xres, SW_W);
-    const unsigned g = persistent_grid((const void*)k_advect, SW_THREADS, AD_SMEM, nt);
-    k_advect<<<g, SW_THREADS, AD_SMEM, s>>>(in.sweep_y, d, out, ntx, nt);
+void launch_sweep_y(const DiskView& d, const CellMaps& in, Cell* out, cudaStream_t s, const Tune* t) {
+    if (t && t->w[1] == 4) sweep_w<1, 4>(d, in.sweep_y4, out, s, t->cps[2]);
+    else sweep_w<1, 8>(d, in.sweep_y, out, s, t ? t->cps[2] : 0);
+}
+
+template <int W>
+static void advect_w(const DiskView& d, const CUtensorMap& m, Cell* out, cudaStream_t s, int cps) {
+    const int ntx = (int)cdiv(d.yres, SW_LEN), nt = ntx * (int)cdiv(d.xres, W);
+    const unsigned g = persistent_grid((const void*)k_advect<W>, Sw<W>::THREADS, Sw<W>::AD_SMEM, nt, cps);
+    k_advect<W><<<g, Sw<W>::THREADS, Sw<W>::AD_SMEM, s>>>(m, d, out, ntx, nt);
+}
+
+void launch_advect(const DiskView& d, const CellMaps& in, Cell* out, cudaStream_t s, const Tune* t) {
+    if (t && t->w[2] == 4) advect_w<4>(d, in.sweep_y4, out, s, t->cps[3]);
+    else advect_w<8>(d, in.sweep_y, out, s, t ? t->cps[3] : 0);
 }
 
 void launch_kick2(const DiskView& d, const CellMaps& in, const VisMaps& vis, Cell* out, cudaStream_t s,
-                  const pg_dust* din, pg_dust* dout) {
+                  const pg_dust* din, pg_dust* dout, const Tune* t) {
     const int ntx = (int)cdiv(d.xres, ST_TX), nt = ntx * (int)cdiv(d.yres, ST_TY);
+    const int cps = t ? t->cps[4] : 0;
     if (d.visc && d.ndim == 2) {
-        const unsigned g = persistent_grid((const void*)k_kick2<true>, ST_THREADS, K5_SMEM, nt);
+        const unsigned g = persistent_grid((const void*)k_kick2<true>, ST_THREADS, K5_SMEM, nt, cps);
         k_kick2<true><<<g, ST_THREADS, K5_SMEM, s>>>(in.stencil, vis.stencil, d, out, ntx, nt, din, dout);
     } else {
-        const unsigned g = persistent_grid((const void*)k_kick2<false>, ST_THREADS, K5_SMEM, nt);
+        const unsigned g = persistent_grid((const void*)k_kick2<false>, ST_THREADS, K5_SMEM, nt, cps);
         k_kick2<false><<<g, ST_THREADS, K5_SMEM, s>>>(in.stencil, vis.stencil, d, out, ntx, nt, din, dout);
+    }
+}
+
+// CTAs per SM that fit for a pass (0 kick1, 1 sweep_x, 2 sweep_y, 3 advect, 4 kick2) with W pencils
+int pass_occupancy(const DiskView& d, int pass, int w) {
+    const bool v = d.visc && d.ndim == 2;
+    switch (pass) {
+        case 0: return kernel_occupancy(v ? (const void*)k_kick1<true> : (const void*)k_kick1<false>, ST_THREADS, K1_SMEM);
+        case 1: return w == 4 ? kernel_occupancy((const void*)k_sweep<0, 4>, Sw<4>::THREADS, Sw<4>::SMEM)
+                              : kernel_occupancy((const void*)k_sweep<0, 8>, Sw<8>::THREADS, Sw<8>::SMEM);
+        case 2: return w == 4 ? kernel_occupancy((const void*)k_sweep<1, 4>, Sw<4>::THREADS, Sw<4>::SMEM)
+                              : kernel_occupancy((const void*)k_sweep<1, 8>, Sw<8>::THREADS, Sw<8>::SMEM);
+        case 3: return w == 4 ? kernel_occupancy((const void*)k_advect<4>, Sw<4>::THREADS, Sw<4>::AD_SMEM)
+                              : kernel_occupancy((const void*)k_advect<8>, Sw<8>::THREADS, Sw<8>::AD_SMEM);
+        default: return kernel_occupancy(v ? (const void*)k_kick2<true> : (const void*)k_kick2<false>, ST_THREADS, K5_SMEM);
     }
 }
 

@@ -125,6 +125,20 @@ class Disk:
         check(lib().pg_disk_torque(self._h, ctypes.byref(out)))
         return out.value
 
+    TUNING = ("w_sweep_x", "w_sweep_y", "w_advect", "cps_kick1", "cps_sweep_x", "cps_sweep_y", "cps_advect",
+              "cps_kick2")
+
+    def autotune(self, reps: int = 10) -> dict:
+        """Times every launch configuration of each pass on the current state and
+        keeps the fastest (results stay bit for bit the same)."""
+        out = (ctypes.c_int * 8)()
+        check(lib().pg_disk_autotune(self._h, reps, out))
+        return {k: int(out[n]) for n, k in enumerate(self.TUNING)}
+
+    def set_tuning(self, choice: dict) -> None:
+        arr = (ctypes.c_int * 8)(*[int(choice[k]) for k in self.TUNING])
+        check(lib().pg_disk_set_tuning(self._h, arr))
+
     STAGES = ("time", "kick1", "sweep_x", "sweep_y", "advect", "kick2")
 
     def profile(self, nsteps: int, end_time: float = 1.0e30) -> dict:

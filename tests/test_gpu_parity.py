@@ -209,3 +209,33 @@ def test_torque_matches_oracle():
     d.check()
     # the state after 10 steps agrees to ~1e-12 (disk64_n10) and the sum is compensated
     assert d.torque() == pytest.approx(o.torque(), rel=1e-9)
+
+
+def test_autotuned_launches_give_identical_results():
+    """The autotuner changes tiles and grid sizes, not the arithmetic of a cell:
+    the tuned step equals the default one bit for bit, and every configuration
+    it may choose (4 pencils per tile everywhere, one CTA per SM) does too."""
+    case = [c for c in C.cases() if c["name"] == "disk64_n10"][0]
+    p, st = case["params"], C.initial_state(case)
+    ref = Disk(p)
+    ref.set_state(case["t0"], st)
+    ref.run(10)
+    ref.sync()
+    a = ref.get_state()
+    tuned = Disk(p)
+    tuned.set_state(case["t0"], st)
+    choice = tuned.autotune(reps=3)
+    assert set(choice) == set(Disk.TUNING)
+    assert all(choice[k] in (4, 8) for k in Disk.TUNING[:3])
+    tuned.run(10)
+    tuned.sync()
+    b = tuned.get_state()
+    forced = Disk(p)
+    forced.set_state(case["t0"], st)
+    forced.set_tuning(dict(zip(Disk.TUNING, (4, 4, 4, 1, 1, 1, 1, 1))))
+    forced.run(10)
+    forced.sync()
+    c = forced.get_state()
+    for k in _keys(p):
+        assert np.array_equal(a[k], b[k]), k
+        assert np.array_equal(a[k], c[k]), k
