@@ -556,6 +556,260 @@ __global__ void __launch_bounds__(ADJ_THREADS) k_adj_theta(const Args a) {
         for (int th = 0; th < 3; ++th) atomicAdd(&a.gth[th], red[th][0]);
 }
 
+// ------------------------------------------------- structured adjoints
+// Sweeps.  The update of cell i, out_i = U(Q_i, D_i) with D_i linear in the
+// fluxes of its two faces, is transposed per cell (k_adj_upd: the direct
+// adjoint of Q_i and lambda_D of the three update slots); each face flux is a
+// function of the 6 cells around it, transposed per input cell (k_adj_flux: the
+// 7 edge states and 6 HLLC fluxes its stencil reaches, in dual arithmetic, each
+// face contracted with lambda_F assembled from lambda_D of its two cells).
+// Slots: DIR 0 (Sigma, v_r from F.u and the pressure, v_phi from F.v / r);
+// DIR 1 (Sigma, v_r from F.w, v_phi from F.u, the pressure and (rot + r Omega) D_Sigma).
+
+template <int DIR>
+__device__ __forceinline__ void sweep_D(const Args& a, int i, int j, const FluxT<double>& F0, const FluxT<double>& F1,
+                                        double& Dr, double& D1, double& D2) {
+    const DiskView& d = a.d;
+    if (DIR == 0) {
+        const double g0 = d.xa[i], g1 = d.xa[i + 1], f = a.dt * d.ixv[i];
+        Dr = (F0.r * g0 - F1.r * g1) * f;
+        D1 = ((F0.u * g0 - F1.u * g1) + 0.5 * (g0 + g1) * (F0.pres - F1.pres)) * f;
+        D2 = (F0.v * g0 - F1.v * g1) * f * d.irad[i];
+    } else {
+        const double f = a.dt * d.iyv[j] * d.irad[i];
+        Dr = (F0.r * 1.0 - F1.r * 1.0) * f;
+        D2 = ((F0.u * 1.0 - F1.u * 1.0) + 0.5 * (1.0 + 1.0) * (F0.pres - F1.pres)) * f;
+        D2 += (d.rot[i] + d.radx[i] * d.frame_omega) * Dr;
+        D1 = (F0.w * 1.0 - F1.w * 1.0) * f;
+    }
+}
+
+// per cell (i, j) of the pass input (pre-shift row for DIR 1): the direct
+// adjoint of Q into lam_in and lambda_D of the slots into lslot (3 planes)
+template <int DIR>
+__global__ void __launch_bounds__(ADJ_THREADS) k_adj_upd(const Args a, double* lslot) {
+    const DiskView& d = a.d;
+    const long long n = (long long)d.xres * d.yres;
+    const size_t P = plane(d);
+    const Seed s0{-1, -1, -1, -1};
+    for (long long m = blockIdx.x * (long long)blockDim.x + threadIdx.x; m < n; m += (long long)gridDim.x * blockDim.x) {
+        const int i = NPAD + (int)(m % d.xres), j = d.ypad + (int)(m / d.xres);
+        const size_t mo = (DIR == 1) ? pidx(d, i, sy_post_row(d, a.inc, i, j)) : (size_t)m;
+        const double lr = a.lam[mo], lu = a.lam[P + mo], lv = a.lam[2 * P + mo];
+        FluxT<double> F0, F1;
+        if (DIR == 0) {
+            F0 = face_flux<double, 0>(a, s0, i, j);
+            F1 = face_flux<double, 0>(a, s0, i + 1, j);
+        } else {
+            F0 = face_flux<double, 1>(a, s0, j, i);
+            F1 = face_flux<double, 1>(a, s0, j + 1, i);
+        }
+        double Dr, D1, D2;
+        sweep_D<DIR>(a, i, j, F0, F1, Dr, D1, D2);
+        const S3<double> Q = ld<double>(a, s0, i, j);
+        double g[6];
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+            S3<Dual> q{Q.r, Q.p, Q.u, Q.v};
+            Dual r = Dr, u1 = D1, u2 = D2;
+            if (k == 0) q.r.d = 1.0;
+            else if (k == 1) q.u.d = 1.0;
+            else if (k == 2) q.v.d = 1.0;
+            else if (k == 3) r.d = 1.0;
+            else if (k == 4) u1.d = 1.0;
+            else u2.d = 1.0;
+            const S3<Dual> o = update_iso<Dual>(q, r, u1, u2);
+            g[k] = lr * o.r.d + lu * o.u.d + lv * o.v.d;
+        }
+        a.lam_in[m] = g[0];
+        a.lam_in[P + m] = g[1];
+        a.lam_in[2 * P + m] = g[2];
+        lslot[m] = g[3];
+        lslot[P + m] = g[4];
+        lslot[2 * P + m] = g[5];
+    }
+}
+
+// lambda of the flux of face f of a pencil (between pencil cells f-1 and f) from
+// lambda_D of its two cells; position f along the pencil, q the pencil
+template <int DIR>
+__device__ __forceinline__ FluxT<double> face_lambda(const Args& a, const double* lslot, int f, int q) {
+    const DiskView& d = a.d;
+    const size_t P = plane(d);
+    FluxT<double> L{0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    for (int side = 0; side < 2; ++side) {  // 0: cell f (face is its left face, +), 1: cell f-1 (right face, -)
+        const int c = f - side;
+        const double sg = side == 0 ? 1.0 : -1.0;
+        if (DIR == 0) {
+            if (c < NPAD || c >= NPAD + d.xres) continue;
+            const size_t m = pidx(d, c, q);
+            const double g0 = d.xa[c], g1 = d.xa[c + 1], fx = a.dt * d.ixv[c];
+            const double gf = side == 0 ? g0 : g1;
+            L.r += sg * lslot[m] * gf * fx;
+            L.u += sg * lslot[P + m] * gf * fx;
+            L.pres += sg * lslot[P + m] * 0.5 * (g0 + g1) * fx;
+            L.v += sg * lslot[2 * P + m] * gf * fx * d.irad[c];
+        } else {
+            const int cw = wrap_row(d, c);
+            const size_t m = pidx(d, q, cw);
+            const double fy = a.dt * d.iyv[cw] * d.irad[q];
+            const double cc = d.rot[q] + d.radx[q] * d.frame_omega;
+            L.r += sg * fy * (lslot[m] + cc * lslot[2 * P + m]);
+            L.u += sg * fy * lslot[2 * P + m];
+            L.pres += sg * fy * lslot[2 * P + m];
+            L.w += sg * fy * lslot[P + m];
+        }
+    }
+    return L;
+}
+
+template <int DIR>
+__global__ void __launch_bounds__(ADJ_THREADS) k_adj_flux(const Args a, const double* lslot) {
+    const DiskView& d = a.d;
+    const long long n = (long long)d.xres * d.yres;
+    const size_t P = plane(d);
+    for (long long m = blockIdx.x * (long long)blockDim.x + threadIdx.x; m < n; m += (long long)gridDim.x * blockDim.x) {
+        const int i = NPAD + (int)(m % d.xres), j = d.ypad + (int)(m / d.xres);
+        const int c = (DIR == 0) ? i : j;  // position along the pencil
+        const int q = (DIR == 0) ? j : i;  // the pencil
+        // faces whose flux reaches this cell, and the cells whose edge states they use
+        int f0 = c - 2, f1 = c + 3;
+        if (DIR == 0) {
+            f0 = max(f0, NPAD);
+            f1 = min(f1, NPAD + d.xres);
+        }
+        FluxT<double> LF[6];
+        for (int f = f0; f <= f1; ++f) LF[f - (c - 2)] = face_lambda<DIR>(a, lslot, f, q);
+        for (int k = 0; k < 3; ++k) {
+            const Seed s{i, j, k, -1};
+            HalfT<Dual> Le[7], Re[7];  // edge states of pencil cells c-3 .. c+3
+            for (int e = f0 - 1; e <= f1; ++e) {
+                const int ew = (DIR == 0) ? e : wrap_row(d, e);
+                edge_states<Dual, DIR>(a, s, ew, q, Le[e - (c - 3)], Re[e - (c - 3)]);
+            }
+            double acc = 0.0;
+            for (int f = f0; f <= f1; ++f) {
+                const FluxT<Dual> F = hllc<Dual>(0, d.ie, d.gam, Re[f - 1 - (c - 3)], Le[f - (c - 3)]);
+                const FluxT<double>& L = LF[f - (c - 2)];
+                acc += L.r * F.r.d + L.u * F.u.d + L.v * F.v.d + L.w * F.w.d + L.pres * F.pres.d;
+            }
+            a.lam_in[(size_t)k * P + m] += acc;
+        }
+    }
+}
+
+// kick2.  The corrector at each output is transposed per cell (k_adj_k2a: the
+// direct adjoint of C and lambda of the viscous force it reads); the force is a
+// function of the predicted 3x3 stencil, and each predicted cell of its own
+// input and kick1's force: transposed per cell over the 5x5 block of predicted
+// states its force stencils reach (k_adj_k2b).
+template <class T>
+__device__ __forceinline__ S3<T> predicted(const Args& a, const Seed& s, int i, int j) {
+    const DiskView& d = a.d;
+    S3<T> X = ld<T>(a, s, i, j);
+    if (i >= NPAD && i < NPAD + d.xres) {
+        T ox, oy, gx, gy;
+        ld_vis<T>(a, s, i, j, ox, oy);
+        gravity<T>(a, s, i, j, 1, gx, gy);
+        X = kick<T>(d, X, gx, gy, ox, oy, d.irad[i], 0.5 * a.dt, 0.5 * a.dt);
+    }
+    return X;
+}
+
+__global__ void __launch_bounds__(ADJ_THREADS) k_adj_k2a(const Args a, double* ls) {
+    const DiskView& d = a.d;
+    const long long n = (long long)d.xres * d.yres;
+    const size_t P = plane(d);
+    const Seed s0{-1, -1, -1, -1};
+    const double hdt = 0.5 * a.dt;
+    for (long long m = blockIdx.x * (long long)blockDim.x + threadIdx.x; m < n; m += (long long)gridDim.x * blockDim.x) {
+        const int i = NPAD + (int)(m % d.xres), j = d.ypad + (int)(m / d.xres);
+        const double lr = a.lam[m], lu = a.lam[P + m], lv = a.lam[2 * P + m];
+        double vx = 0.0, vy = 0.0;
+        if (d.visc) {
+            S3<double> X[9];
+            for (int k = 0; k < 9; ++k) {
+                int dx, dy;
+                nb(k, dx, dy);
+                X[k] = predicted<double>(a, s0, i + dx, j + dy);
+            }
+            stress<double>(a, s0, i, j, X, vx, vy);
+        }
+        double gx, gy;
+        gravity<double>(a, s0, i, j, 1, gx, gy);
+        const S3<double> C = ld<double>(a, s0, i, j);
+        double g[5];
+        for (int k = 0; k < 5; ++k) {
+            S3<Dual> q{C.r, C.p, C.u, C.v};
+            Dual fx = vx, fy = vy;
+            if (k == 0) q.r.d = 1.0;
+            else if (k == 1) q.u.d = 1.0;
+            else if (k == 2) q.v.d = 1.0;
+            else if (k == 3) fx.d = 1.0;
+            else fy.d = 1.0;
+            const S3<Dual> o = kick<Dual>(d, q, Dual(gx), Dual(gy), fx, fy, d.irad[i], hdt, hdt);
+            g[k] = lr * o.r.d + lu * o.u.d + lv * o.v.d;
+        }
+        a.lam_in[m] = g[0];
+        a.lam_in[P + m] = g[1];
+        a.lam_in[2 * P + m] = g[2];
+        ls[m] = g[3];
+        ls[P + m] = g[4];
+    }
+}
+
+__global__ void __launch_bounds__(ADJ_THREADS) k_adj_k2b(const Args a, const double* ls) {
+    const DiskView& d = a.d;
+    const long long n = (long long)d.xres * d.yres;
+    const size_t P = plane(d);
+    const Seed s0{-1, -1, -1, -1};
+    for (long long m = blockIdx.x * (long long)blockDim.x + threadIdx.x; m < n; m += (long long)gridDim.x * blockDim.x) {
+        const int i = NPAD + (int)(m % d.xres), j = d.ypad + (int)(m / d.xres);
+        // predicted states of the 5x5 block around (i, j)
+        S3<double> T5[25];
+        for (int b = 0; b < 25; ++b) T5[b] = predicted<double>(a, s0, i + (b % 5) - 2, j + (b / 5) - 2);
+        // lambda of the predicted cell (i, j): the force of every output whose stencil holds it
+        double lt[3] = {0.0, 0.0, 0.0};
+        for (int oy = -1; oy <= 1; ++oy)
+            for (int ox = -1; ox <= 1; ++ox) {
+                const int io = i + ox, jo = wrap_row(d, j + oy);
+                if (io < NPAD || io >= NPAD + d.xres) continue;
+                const size_t mo = pidx(d, io, jo);
+                const double lx = ls[mo], ly = ls[P + mo];
+                for (int k = 0; k < 3; ++k) {
+                    S3<Dual> X[9];
+                    for (int t = 0; t < 9; ++t) {
+                        int dx, dy;
+                        nb(t, dx, dy);
+                        const int bx = ox + dx + 2, by = oy + dy + 2;
+                        const S3<double>& v = T5[by * 5 + bx];
+                        X[t] = S3<Dual>{v.r, v.p, v.u, v.v};
+                        if (bx == 2 && by == 2) {
+                            if (k == 0) X[t].r.d = 1.0;
+                            else if (k == 1) X[t].u.d = 1.0;
+                            else X[t].v.d = 1.0;
+                        }
+                    }
+                    Dual vx, vy;
+                    stress<Dual>(a, s0, io, jo, X, vx, vy);
+                    lt[k] += lx * vx.d + ly * vy.d;
+                }
+            }
+        // the predictor of (i, j): its input cell and kick1's force there
+        double g[5];
+        for (int k = 0; k < 5; ++k) {
+            const Seed s{i, j, k, -1};
+            const S3<Dual> X = predicted<Dual>(a, s, i, j);
+            g[k] = lt[0] * X.r.d + lt[1] * X.u.d + lt[2] * X.v.d;
+        }
+        a.lam_in[m] += g[0];
+        a.lam_in[P + m] += g[1];
+        a.lam_in[2 * P + m] += g[2];
+        a.lamv_in[m] = g[3];
+        a.lamv_in[P + m] = g[4];
+    }
+}
+
 // <lambda, J dir> of a pass by forward mode (the adjoint dot-product test)
 template <int PASS>
 __global__ void __launch_bounds__(ADJ_THREADS) k_adj_jvp(const Args a, double* out) {
@@ -771,11 +1025,23 @@ static unsigned grid_for(long long n) {
     return (unsigned)(g < 1 ? 1 : g);
 }
 
+// The adjoint of one pass: lam_in (and lamv_in for kick2) from lam (and lamv
+// for kick1); scratch: 3 interior planes.  theta: also accumulate d/d theta.
 template <int PASS>
-static void launch_pass(const Args& a, bool theta, cudaStream_t s) {
+static void launch_pass(const Args& a, bool theta, double* scratch, cudaStream_t s) {
     const long long n = (long long)a.d.xres * a.d.yres;
-    k_adj_state<PASS><<<grid_for(n), ADJ_THREADS, 0, s>>>(a);
-    if (theta) k_adj_theta<PASS><<<grid_for(n), ADJ_THREADS, 0, s>>>(a);
+    const unsigned g = grid_for(n);
+    if (PASS == P_SX || PASS == P_SY) {
+        constexpr int DIR = (PASS == P_SX) ? 0 : 1;
+        k_adj_upd<DIR><<<g, ADJ_THREADS, 0, s>>>(a, scratch);
+        k_adj_flux<DIR><<<g, ADJ_THREADS, 0, s>>>(a, scratch);
+    } else if (PASS == P_K2 && a.d.visc) {
+        k_adj_k2a<<<g, ADJ_THREADS, 0, s>>>(a, scratch);
+        k_adj_k2b<<<g, ADJ_THREADS, 0, s>>>(a, scratch);
+    } else {
+        k_adj_state<PASS><<<g, ADJ_THREADS, 0, s>>>(a);
+    }
+    if (theta) k_adj_theta<PASS><<<g, ADJ_THREADS, 0, s>>>(a);
 }
 
 template <int PASS>
@@ -820,6 +1086,7 @@ struct pg_adj {
     double* gth = nullptr;
     unsigned long long* err = nullptr;
     Scalars* ssc = nullptr;  // scratch copy of the device scalars
+    double* scratch = nullptr;  // 3 interior planes: lambda of the update slots / of kick1's force
     size_t bytes = 0;
 
     size_t ncell() const { return (size_t)(P.xres + 2 * NPAD) * (P.yres + 2 * NPAD); }
@@ -960,6 +1227,7 @@ pg_status pg_adj_create(const pg_params* P, int device, void* stream, int checkp
     if ((s = adj_alloc(a, &a->gth, 3 * sizeof(double))) != PG_OK) return bail(s);
     if ((s = adj_alloc(a, &a->err, 5 * sizeof(unsigned long long))) != PG_OK) return bail(s);
     if ((s = adj_alloc(a, &a->ssc, sizeof(Scalars))) != PG_OK) return bail(s);
+    if ((s = adj_alloc(a, &a->scratch, 3 * ni * sizeof(double))) != PG_OK) return bail(s);
     if ((s = adj_make_disk(a)) != PG_OK) return bail(s);
     *out = a;
     return PG_OK;
@@ -985,6 +1253,7 @@ pg_status pg_adj_destroy(pg_adj* a) {
     cudaFree(a->gth);
     cudaFree(a->err);
     cudaFree(a->ssc);
+    cudaFree(a->scratch);
     if (a->own_stream && a->stream) cudaStreamDestroy(a->stream);
     delete a;
     return PG_OK;
@@ -1122,11 +1391,11 @@ pg_status pg_adj_backward(pg_adj* a, const double* grad_out, double* grad_sigma0
                 g.lam = a->lam[c];
                 g.lam_in = a->lam[1 - c];
                 switch (pass) {
-                    case P_K2: g.lamv_in = a->lamv; launch_pass<P_K2>(g, true, st); break;
-                    case P_ADV: launch_pass<P_ADV>(g, true, st); break;
-                    case P_SY: launch_pass<P_SY>(g, true, st); break;
-                    case P_SX: launch_pass<P_SX>(g, true, st); break;
-                    default: g.lamv = a->lamv; launch_pass<P_K1>(g, true, st); break;
+                    case P_K2: g.lamv_in = a->lamv; launch_pass<P_K2>(g, true, a->scratch, st); break;
+                    case P_ADV: launch_pass<P_ADV>(g, true, a->scratch, st); break;
+                    case P_SY: launch_pass<P_SY>(g, true, a->scratch, st); break;
+                    case P_SX: launch_pass<P_SX>(g, true, a->scratch, st); break;
+                    default: g.lamv = a->lamv; launch_pass<P_K1>(g, true, a->scratch, st); break;
                 }
                 c = 1 - c;
             };
@@ -1233,11 +1502,11 @@ pg_status pg_adj_dot_test(pg_adj* a, double dt, const double* dir, const double*
         if (p == P_ADV && !d.orbadv) continue;
         g.in = r.stage[p];
         switch (p) {
-            case P_K1: k_adj_jvp<P_K1><<<gr, ADJ_THREADS, 0, st>>>(g, dev + 2 * p); k_adj_state<P_K1><<<gr, ADJ_THREADS, 0, st>>>(g); break;
-            case P_SX: k_adj_jvp<P_SX><<<gr, ADJ_THREADS, 0, st>>>(g, dev + 2 * p); k_adj_state<P_SX><<<gr, ADJ_THREADS, 0, st>>>(g); break;
-            case P_SY: k_adj_jvp<P_SY><<<gr, ADJ_THREADS, 0, st>>>(g, dev + 2 * p); k_adj_state<P_SY><<<gr, ADJ_THREADS, 0, st>>>(g); break;
-            case P_ADV: k_adj_jvp<P_ADV><<<gr, ADJ_THREADS, 0, st>>>(g, dev + 2 * p); k_adj_state<P_ADV><<<gr, ADJ_THREADS, 0, st>>>(g); break;
-            default: k_adj_jvp<P_K2><<<gr, ADJ_THREADS, 0, st>>>(g, dev + 2 * p); k_adj_state<P_K2><<<gr, ADJ_THREADS, 0, st>>>(g); break;
+            case P_K1: k_adj_jvp<P_K1><<<gr, ADJ_THREADS, 0, st>>>(g, dev + 2 * p); launch_pass<P_K1>(g, false, a->scratch, st); break;
+            case P_SX: k_adj_jvp<P_SX><<<gr, ADJ_THREADS, 0, st>>>(g, dev + 2 * p); launch_pass<P_SX>(g, false, a->scratch, st); break;
+            case P_SY: k_adj_jvp<P_SY><<<gr, ADJ_THREADS, 0, st>>>(g, dev + 2 * p); launch_pass<P_SY>(g, false, a->scratch, st); break;
+            case P_ADV: k_adj_jvp<P_ADV><<<gr, ADJ_THREADS, 0, st>>>(g, dev + 2 * p); launch_pass<P_ADV>(g, false, a->scratch, st); break;
+            default: k_adj_jvp<P_K2><<<gr, ADJ_THREADS, 0, st>>>(g, dev + 2 * p); launch_pass<P_K2>(g, false, a->scratch, st); break;
         }
         k_dot<<<gr, ADJ_THREADS, 0, st>>>(g.lam_in, dir, (long long)(3 * ni), dev + 2 * p + 1);
         if (p == P_K2 && d.visc) k_dot<<<gr, ADJ_THREADS, 0, st>>>(g.lamv_in, dir + 3 * ni, (long long)(2 * ni), dev + 2 * p + 1);
