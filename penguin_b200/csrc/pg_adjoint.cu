@@ -682,16 +682,18 @@ __global__ void __launch_bounds__(ADJ_THREADS) k_adj_flux(const Args a, const do
         for (int f = f0; f <= f1; ++f) LF[f - (c - 2)] = face_lambda<DIR>(a, lslot, f, q);
         for (int k = 0; k < 3; ++k) {
             const Seed s{i, j, k, -1};
-            HalfT<Dual> Le[7], Re[7];  // edge states of pencil cells c-3 .. c+3
-            for (int e = f0 - 1; e <= f1; ++e) {
-                const int ew = (DIR == 0) ? e : wrap_row(d, e);
-                edge_states<Dual, DIR>(a, s, ew, q, Le[e - (c - 3)], Re[e - (c - 3)]);
-            }
+            // sweep the faces in order, keeping the right-edge state of the cell below
+            HalfT<Dual> Lc, Rprev;
+            edge_states<Dual, DIR>(a, s, (DIR == 0) ? f0 - 1 : wrap_row(d, f0 - 1), q, Lc, Rprev);
             double acc = 0.0;
+#pragma unroll 1
             for (int f = f0; f <= f1; ++f) {
-                const FluxT<Dual> F = hllc<Dual>(0, d.ie, d.gam, Re[f - 1 - (c - 3)], Le[f - (c - 3)]);
+                HalfT<Dual> Rc;
+                edge_states<Dual, DIR>(a, s, (DIR == 0) ? f : wrap_row(d, f), q, Lc, Rc);
+                const FluxT<Dual> F = hllc<Dual>(0, d.ie, d.gam, Rprev, Lc);
                 const FluxT<double>& L = LF[f - (c - 2)];
                 acc += L.r * F.r.d + L.u * F.u.d + L.v * F.v.d + L.w * F.w.d + L.pres * F.pres.d;
+                Rprev = Rc;
             }
             a.lam_in[(size_t)k * P + m] += acc;
         }
