@@ -151,6 +151,19 @@ pg_status pg_disk_get_state(pg_disk* d, double* r, double* p, double* u, double*
    pg_disk_set_tuning applies a choice found earlier. */
 pg_status pg_disk_autotune(pg_disk* d, int reps, int* choice);
 pg_status pg_disk_set_tuning(pg_disk* d, const int* choice);
+/* Snapshots in the reference's checkpoint format (write_check_point /
+   load_grid, src/output/output.cu:125-248; file names binary_<label>_<frame>,
+   main.cu:403): t, interior faces, r, p, u, v (2D), then the dust fields.
+   average = 1 writes the time average (ave_flag).  Reading restarts the disk
+   from t and the gas fields. */
+pg_status pg_disk_write_snapshot(pg_disk* d, const char* path, int average);
+pg_status pg_disk_read_snapshot(pg_disk* d, const char* path, double* t_out);
+/* ave_flag: the gas state averaged over a save interval by the trapezoid rule
+   of main.cu:343-351, accumulated inside the step; interval <= 0: off.
+   reset = init_average after a save. */
+pg_status pg_disk_set_average(pg_disk* d, double interval);
+pg_status pg_disk_reset_average(pg_disk* d);
+pg_status pg_disk_get_average(pg_disk* d, double* r, double* p, double* u, double* v);
 /* dust_flag: the interior dust (density, radial and azimuthal velocity, host
    arrays of xres*yres) of the newest state.  pg_disk_set_state resets the dust
    to init_CD, as the reference's restart does (load_grid reads the gas only,
@@ -164,7 +177,9 @@ pg_status pg_disk_global_dt(pg_disk* d, double dt_prev, double* dt_out);
 pg_status pg_disk_solve(pg_disk* d, double t, double dt);
 /* main.cu's loop on the device: nsteps of (dt = min(CFL dt, 1.1 dt_prev), clipped
    at end_time; solve; t += dt) with dt and t resident in device memory and the
-   step captured in a CUDA graph.  Stream-ordered; pg_disk_sync waits. */
+   step captured in a CUDA graph.  Stream-ordered; pg_disk_sync waits.  A run
+   continuing one that stopped on a clip at its end_time caps its first dt by
+   the step the clip replaced, as main.cu does after a dump (main.cu:333-338). */
 pg_status pg_disk_run(pg_disk* d, int nsteps, double end_time);
 pg_status pg_disk_sync(pg_disk* d);
 /* Time, last dt and step count of the device-resident loop (syncs). */

@@ -23,6 +23,8 @@ EXPORTS = [
     "pg_global_dt_noalloc",
     "pg_disk_create", "pg_disk_destroy", "pg_disk_dims", "pg_disk_set_state", "pg_disk_get_state",
     "pg_disk_set_dust", "pg_disk_get_dust", "pg_disk_autotune", "pg_disk_set_tuning",
+    "pg_disk_write_snapshot", "pg_disk_read_snapshot", "pg_disk_set_average", "pg_disk_reset_average",
+    "pg_disk_get_average",
     "pg_disk_state_ptr", "pg_disk_global_dt", "pg_disk_solve", "pg_disk_run", "pg_disk_sync", "pg_disk_clock",
     "pg_disk_planet", "pg_disk_check", "pg_disk_torque", "pg_kernels_per_step", "pg_disk_profile",
     "pg_ens_check_params", "pg_ens_create", "pg_ens_destroy", "pg_ens_size", "pg_ens_dims", "pg_ens_set_state",
@@ -75,6 +77,11 @@ def lib() -> ctypes.CDLL:
         "pg_disk_set_dust": (i, [vp, dp, dp, dp]),
         "pg_disk_autotune": (i, [vp, i, ip]),
         "pg_disk_set_tuning": (i, [vp, ip]),
+        "pg_disk_write_snapshot": (i, [vp, ctypes.c_char_p, i]),
+        "pg_disk_read_snapshot": (i, [vp, ctypes.c_char_p, dp]),
+        "pg_disk_set_average": (i, [vp, d]),
+        "pg_disk_reset_average": (i, [vp]),
+        "pg_disk_get_average": (i, [vp, dp, dp, dp, dp]),
         "pg_disk_get_dust": (i, [vp, dp, dp, dp]),
         "pg_disk_state_ptr": (i, [vp, ctypes.POINTER(vp)]),
         "pg_disk_global_dt": (i, [vp, d, dp]),

@@ -34,6 +34,7 @@ struct Scalars {
     int pad_;
     pg_body planet_cur;   // planet used by the first half-kick (from the previous step)
     pg_body planet_next;  // planet at t+dt (src/solver/solve.cu:264)
+    double dt_hold;       // the CFL step a clip at end_time replaced (main.cu:333-338 old_dt)
 };
 
 // Everything a kernel needs to know about one disk (passed by value).
@@ -76,6 +77,9 @@ struct DiskView {
     double stokes, sc_h;  // Stokes number; h/r (stopping time t_s = Stokes h / (c_s Sigma), dust.cu:1-4)
     double dust_rmin;     // D_G_ratio * smallr: the dust density floor of update_Dust (dust.cu:149-176)
     const double* initd;  // init_CD(xc(i)) (4 per i: r, u, v, w; src/init/init.cu:351-454)
+    // time average of the gas state over a save interval (ave_flag, src/output/output.cu:250-330)
+    Cell* ave;            // null: off
+    double ave_T;         // the save interval
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {

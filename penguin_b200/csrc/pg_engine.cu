@@ -320,6 +320,9 @@ struct Engine {
     pg_dust* dbuf[2] = {nullptr, nullptr};  // dust_flag: the dust of buf[k] is dbuf[k]
     DustMaps dmaps[2];
     Tune tune;                               // launch configuration (pg_disk_autotune)
+    Cell* ave = nullptr;                     // time average (pg_disk_set_average)
+    double* snap = nullptr;                  // pinned staging of snapshots
+    size_t snap_n = 0;
 
     ~Engine() {
         for (auto& g : graph)
@@ -336,6 +339,8 @@ struct Engine {
         }
         cudaFree(dbuf[0]);
         cudaFree(dbuf[1]);
+        cudaFree(ave);
+        if (snap) cudaFreeHost(snap);
         cudaFree(grid);
         cudaFree(tab);
         cudaFree(part);
@@ -643,6 +648,32 @@ __global__ void k_extract(const DiskView d, const Cell* buf, double* r, double* 
 }
 
 __global__ void k_grid_planet_in(Scalars* sc, const pg_body* planets) { sc->planet_next = planets[0]; }
+
+// write_check_point's fields (src/output/output.cu:125-180): interior r, p, u,
+// v (2D) of the gas source, then with dust r, u, v (2D), w (2D); x fastest
+__global__ void k_snapshot_planes(const DiskView d, const Cell* gas, const pg_dust* dust, double* out) {
+    const long long n = (long long)d.xres * d.yres;
+    for (long long m = blockIdx.x * (long long)blockDim.x + threadIdx.x; m < n; m += (long long)gridDim.x * blockDim.x) {
+        const int i = NPAD + (int)(m % d.xres), j = d.ypad + (int)(m / d.xres);
+        const size_t k = (size_t)i + (size_t)d.xarr * j;
+        const Cell c = gas[k];
+        double* o = out + m;
+        o[0] = c.r;
+        o[n] = c.p;
+        o[2 * n] = c.u;
+        int f = 3;
+        if (d.ndim > 1) o[(f++) * n] = c.v;
+        if (dust) {
+            const pg_dust q = dust[k];
+            o[(f++) * n] = q.r;
+            o[(f++) * n] = q.u;
+            if (d.ndim > 1) {
+                o[(f++) * n] = q.v;
+                o[(f++) * n] = q.w;
+            }
+        }
+    }
+}
 __global__ void k_grid_planet_out(const Scalars* sc, pg_body* planets) { planets[0] = sc->planet_next; }
 
 }  // namespace pg
@@ -782,6 +813,7 @@ static pg_status set_state_device(Engine& E, double t, const double* r, const do
     h.pad_ = 0;
     h.err = 0;
     h.floor_hits = 0;
+    h.dt_hold = 0.0;
     PG_CUDA(cudaMemcpyAsync(E.sc, &h, sizeof(Scalars), cudaMemcpyHostToDevice, E.stream));
     PG_CUDA(cudaStreamSynchronize(E.stream));
     E.fresh = true;
@@ -986,6 +1018,10 @@ pg_status pg_disk_run(pg_disk* dk, int nsteps, double end_time) {
     PG_CUDA(cudaMemcpyAsync(&h, E.sc, sizeof(Scalars), cudaMemcpyDeviceToHost, E.stream));
     PG_CUDA(cudaStreamSynchronize(E.stream));
     if (E.fresh) h.dt_prev = end_time - h.t;
+    // a run that stopped on a clip at its end_time continues like main.cu after
+    // a dump (main.cu:333-338, 425): the step before the clip caps the next one
+    else if (h.dt_hold > 0.0) h.dt_prev = h.dt_hold;
+    h.dt_hold = 0.0;
     h.end_time = end_time;
     h.done = 0;
     h.pad_ = 0;
@@ -1183,6 +1219,136 @@ pg_status pg_disk_autotune(pg_disk* dk, int reps, int* choice) {
         for (int k = 0; k < 5; ++k) choice[3 + k] = best.cps[k];
     }
     return PG_OK;
+}
+
+static int snapshot_fields(const DiskView& d) {
+    return (d.ndim > 1 ? 4 : 3) + (d.dust ? (d.ndim > 1 ? 4 : 2) : 0);
+}
+
+static void drop_graphs(Engine& E) {
+    for (auto& g : E.graph)
+        if (g) {
+            cudaGraphExecDestroy(g);
+            g = nullptr;
+        }
+}
+
+// ave_flag: the gas state averaged over a save interval T by the trapezoid rule
+// of main.cu:343-351 (A += C (dt/2)/T before and after each step), accumulated
+// in the first and last pass of the step.  interval <= 0 switches it off.
+pg_status pg_disk_set_average(pg_disk* dk, double interval) {
+    if (!dk) return fail(PG_ERR_ARG, "null disk");
+    Engine& E = *dk->E;
+    PG_CUDA(cudaSetDevice(E.device));
+    pg_status s0 = resolve_cur(E);
+    if (s0 != PG_OK) return s0;
+    const size_t n = (size_t)E.view.xarr * E.view.yarr;
+    if (interval > 0.0) {
+        if (!E.ave) PG_CUDA(cudaMalloc(&E.ave, n * sizeof(Cell)));
+        PG_CUDA(cudaMemsetAsync(E.ave, 0, n * sizeof(Cell), E.stream));
+        E.view.ave = E.ave;
+        E.view.ave_T = interval;
+    } else {
+        E.view.ave = nullptr;
+        E.view.ave_T = 0.0;
+    }
+    drop_graphs(E);
+    PG_CUDA(cudaStreamSynchronize(E.stream));
+    return PG_OK;
+}
+
+// init_average (src/output/output.cu:315-330)
+pg_status pg_disk_reset_average(pg_disk* dk) {
+    if (!dk) return fail(PG_ERR_ARG, "null disk");
+    Engine& E = *dk->E;
+    if (!E.view.ave) return fail(PG_ERR_CONFIG, "no time average (pg_disk_set_average)");
+    PG_CUDA(cudaMemsetAsync(E.ave, 0, (size_t)E.view.xarr * E.view.yarr * sizeof(Cell), E.stream));
+    PG_CUDA(cudaStreamSynchronize(E.stream));
+    return PG_OK;
+}
+
+pg_status pg_disk_get_average(pg_disk* dk, double* r, double* p, double* u, double* v) {
+    if (!dk || !r || !p || !u) return fail(PG_ERR_ARG, "null argument");
+    Engine& E = *dk->E;
+    const DiskView& d = E.view;
+    if (!d.ave) return fail(PG_ERR_CONFIG, "no time average (pg_disk_set_average)");
+    PG_CUDA(cudaSetDevice(E.device));
+    const size_t n = (size_t)d.xres * d.yres;
+    double* stage = nullptr;
+    PG_CUDA(cudaMallocAsync(&stage, 4 * n * sizeof(double), E.stream));
+    k_extract<<<1184, 256, 0, E.stream>>>(d, E.ave, stage, stage + n, stage + 2 * n, stage + 3 * n);
+    PG_CUDA(cudaGetLastError());
+    PG_CUDA(cudaMemcpyAsync(r, stage, n * sizeof(double), cudaMemcpyDeviceToHost, E.stream));
+    PG_CUDA(cudaMemcpyAsync(p, stage + n, n * sizeof(double), cudaMemcpyDeviceToHost, E.stream));
+    PG_CUDA(cudaMemcpyAsync(u, stage + 2 * n, n * sizeof(double), cudaMemcpyDeviceToHost, E.stream));
+    if (v) PG_CUDA(cudaMemcpyAsync(v, stage + 3 * n, n * sizeof(double), cudaMemcpyDeviceToHost, E.stream));
+    PG_CUDA(cudaFreeAsync(stage, E.stream));
+    PG_CUDA(cudaStreamSynchronize(E.stream));
+    return PG_OK;
+}
+
+// A snapshot in the reference's checkpoint format (write_check_point,
+// src/output/output.cu:125-180): t, the interior faces xa (and ya in 2D), then
+// the fields.  average = 1 writes the time average of the gas (with the
+// current dust, like main.cu:411-419).  The fields are gathered into planes on
+// the device and written with one host write.
+pg_status pg_disk_write_snapshot(pg_disk* dk, const char* path, int average) {
+    if (!dk || !path) return fail(PG_ERR_ARG, "null argument");
+    Engine& E = *dk->E;
+    const DiskView& d = E.view;
+    if (average && !d.ave) return fail(PG_ERR_CONFIG, "no time average (pg_disk_set_average)");
+    PG_CUDA(cudaSetDevice(E.device));
+    pg_status s0 = resolve_cur(E);
+    if (s0 != PG_OK) return s0;
+    const size_t n = (size_t)d.xres * d.yres, nf = (size_t)snapshot_fields(d);
+    const size_t head = 1 + (size_t)d.xres + 1 + (d.ndim > 1 ? (size_t)d.yres + 1 : 0);
+    const size_t total = head + nf * n;
+    if (E.snap_n < total) {
+        if (E.snap) cudaFreeHost(E.snap);
+        E.snap = nullptr;
+        PG_CUDA(cudaMallocHost(&E.snap, total * sizeof(double)));
+        E.snap_n = total;
+    }
+    double* h = E.snap;
+    double* planes = nullptr;
+    PG_CUDA(cudaMallocAsync(&planes, nf * n * sizeof(double), E.stream));
+    k_snapshot_planes<<<1184, 256, 0, E.stream>>>(d, average ? E.ave : E.buf[E.cur], d.dust ? E.dbuf[E.cur] : nullptr,
+                                                  planes);
+    PG_CUDA(cudaGetLastError());
+    PG_CUDA(cudaMemcpyAsync(h, &E.sc->t, sizeof(double), cudaMemcpyDeviceToHost, E.stream));
+    PG_CUDA(cudaMemcpyAsync(h + 1, d.xa + NPAD, (d.xres + 1) * sizeof(double), cudaMemcpyDeviceToHost, E.stream));
+    if (d.ndim > 1)
+        PG_CUDA(cudaMemcpyAsync(h + 2 + d.xres, d.ya + d.ypad, (d.yres + 1) * sizeof(double), cudaMemcpyDeviceToHost,
+                                E.stream));
+    PG_CUDA(cudaMemcpyAsync(h + head, planes, nf * n * sizeof(double), cudaMemcpyDeviceToHost, E.stream));
+    PG_CUDA(cudaFreeAsync(planes, E.stream));
+    PG_CUDA(cudaStreamSynchronize(E.stream));
+    FILE* f = std::fopen(path, "wb");
+    if (!f) return fail(PG_ERR_ARG, "cannot open %s for writing", path);
+    const size_t w = std::fwrite(h, sizeof(double), total, f);
+    const int c = std::fclose(f);
+    if (w != total || c != 0) return fail(PG_ERR_ARG, "short write to %s", path);
+    return PG_OK;
+}
+
+// Restart from a snapshot (load_grid, src/output/output.cu:182-248): t and the
+// gas fields; the faces are skipped and any dust fields ignored (the dust
+// restarts from init_CD, as in the reference).
+pg_status pg_disk_read_snapshot(pg_disk* dk, const char* path, double* t_out) {
+    if (!dk || !path) return fail(PG_ERR_ARG, "null argument");
+    const DiskView& d = dk->E->view;
+    const size_t n = (size_t)d.xres * d.yres, ng = d.ndim > 1 ? 4 : 3;
+    const size_t head = 1 + (size_t)d.xres + 1 + (d.ndim > 1 ? (size_t)d.yres + 1 : 0);
+    FILE* f = std::fopen(path, "rb");
+    if (!f) return fail(PG_ERR_ARG, "cannot open %s", path);
+    std::vector<double> buf(head + ng * n);
+    const size_t r = std::fread(buf.data(), sizeof(double), buf.size(), f);
+    std::fclose(f);
+    if (r != buf.size()) return fail(PG_ERR_ARG, "%s: %zu values, expected at least %zu", path, r, buf.size());
+    const double* F = buf.data() + head;
+    pg_status s = pg_disk_set_state(dk, buf[0], F, F + n, F + 2 * n, d.ndim > 1 ? F + 3 * n : nullptr);
+    if (s == PG_OK && t_out) *t_out = buf[0];
+    return s;
 }
 
 pg_status pg_disk_set_tuning(pg_disk* dk, const int* choice) {

@@ -133,6 +133,17 @@ __device__ __forceinline__ void gather9(const double* tile, int hx, int hy, cons
     }
 }
 
+// add_grid (src/output/output.cu:250-275): A += C (0.5 dt) / T on the interior
+__device__ __forceinline__ void accumulate_average(const DiskView& d, int i, int j, const Cell& C, double hdt) {
+    const double fac = hdt / d.ave_T;
+    Cell* a = d.ave + (size_t)i + (size_t)d.xarr * j;
+    a->r += C.r * fac;
+    a->p += C.p * fac;
+    a->u += C.u * fac;
+    a->v += C.v * fac;
+    a->w += C.w * fac;
+}
+
 __device__ __forceinline__ double signal_rate(const DiskView& d, const Cell& c, int i, int j,
                                               const DCell* dc = nullptr) {
     // src/timestep/timestep.cu:46-77 (cell widths as reciprocals); with dust the
@@ -569,6 +580,7 @@ __global__ void __launch_bounds__(ST_THREADS)
             const Grav g = gravity(d, i, d.radx[i], tr[0], tr[1], d.trig[4 * d.yarr], sc->planet_cur);
             const Cell Q = kick<VISC>(d, C, d.irad[i], g, vx, vy, 0.0, hdt);
             emit(d, out, i, j, Q);
+            if (d.ave) accumulate_average(d, i, j, C, hdt);  // averaging(dev, 0.5 dt, T) before solve
             if (din) {  // dust half-kick: drag towards the gas cell C (sweeps.cu:626-707, mdt = 0)
                 const DCell D = dust_kick(d, C, C.u, C.v, load_dust(din, d.xarr, i, j), g.gx, g.gy, g.gz,
                                           d.irad[i], 0.0, hdt);
@@ -706,6 +718,7 @@ __global__ void __launch_bounds__(ST_THREADS)
                     vmax = fmax(vmax, signal_rate(d, Q, i, j));
                 }
                 emit(d, out, i, j, Q);
+                if (d.ave) accumulate_average(d, i, j, Q, hdt);  // ... and after it
             }
             __syncthreads();
         }

@@ -74,6 +74,7 @@ __device__ inline void advance_clock(const DiskView& d) {
     double dt = (dtc < lim) ? dtc : lim;
     const double t = sc->t;
     if (t + dt > sc->end_time) {
+        sc->dt_hold = dt;
         dt = sc->end_time - t;
         sc->pad_ = 1;
     }

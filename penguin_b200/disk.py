@@ -125,6 +125,32 @@ class Disk:
         check(lib().pg_disk_torque(self._h, ctypes.byref(out)))
         return out.value
 
+    # ---------------------------------------------------- snapshots, averages
+    def write_snapshot(self, path: str, average: bool = False) -> None:
+        """The newest state (or the time average) in the reference's checkpoint format."""
+        check(lib().pg_disk_write_snapshot(self._h, str(path).encode(), int(average)))
+
+    def read_snapshot(self, path: str) -> float:
+        """Restart from a checkpoint file (t and the gas fields, like load_grid)."""
+        t = ctypes.c_double()
+        check(lib().pg_disk_read_snapshot(self._h, str(path).encode(), ctypes.byref(t)))
+        self.t = t.value
+        self.dt = None
+        return t.value
+
+    def set_average(self, interval: float) -> None:
+        """ave_flag: average the gas over a save interval (0 switches it off)."""
+        check(lib().pg_disk_set_average(self._h, interval))
+
+    def reset_average(self) -> None:
+        check(lib().pg_disk_reset_average(self._h))
+
+    def get_average(self) -> dict:
+        shape = (self.params.yres, self.params.xres)
+        out = {k: np.empty(shape) for k in ("r", "p", "u", "v")}
+        check(lib().pg_disk_get_average(self._h, _dp(out["r"]), _dp(out["p"]), _dp(out["u"]), _dp(out["v"])))
+        return out
+
     TUNING = ("w_sweep_x", "w_sweep_y", "w_advect", "cps_kick1", "cps_sweep_x", "cps_sweep_y", "cps_advect",
               "cps_kick2")
 

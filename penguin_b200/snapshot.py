@@ -45,3 +45,44 @@ def read_snapshot(path: str, xres: int, yres: int, ndim: int, dust: bool = False
 
 def frame_num(n: int) -> str:
     return f"{n:05d}"
+
+
+# include/parameters.h:31,34
+EARTH_MASS = 0.000003
+JUPITER_MASS = 0.0009543
+
+
+def _i(x: float) -> str:
+    """int_to_string of a double argument (src/util/util.cu:18-23): truncation to int."""
+    return str(int(x))
+
+
+def label(p) -> str:
+    """create_label (src/output/output.cu:14-92) for the configurations this library runs
+    (recon_flag 6, alpha viscosity visc_flag 1, no cooling)."""
+    import math
+
+    if p.ndim == 1:
+        s = _i(p.xres)
+    else:
+        s = f"{_i(p.xres)}x{_i(p.yres)}"
+    s += "_h" + _i(1000.0 * p.sc_h)
+    if p.n_planet > 0:
+        if p.planet_mass >= JUPITER_MASS:
+            s += f"_{_i(p.n_planet)}p{_i(p.planet_mass / JUPITER_MASS)}J"
+        else:
+            s += f"_{_i(p.n_planet)}p{_i(p.planet_mass / EARTH_MASS)}E"
+        s += "_e" + _i(p.planet_ecc * 1000.0)
+    if p.visc_flag == 1:
+        s += "_a" + _i(math.log10(p.ss_alpha) * 10.0)
+    if p.ndim > 1 and p.OrbAdv_flag:
+        s += "_OA"
+    if p.dust_flag:
+        s += "_St" + _i(math.log10(p.Stokes) * 10.0)
+    s += "_PPM4"
+    return s
+
+
+def file_name(p, frame: int, average: bool = False) -> str:
+    """binary_<label>_<frame> (main.cu:403), binary_<label>_ave_<frame> for averages (main.cu:414)."""
+    return "binary_" + label(p) + ("_ave_" if average else "_") + frame_num(frame)
