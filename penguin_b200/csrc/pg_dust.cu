@@ -360,6 +360,29 @@ __global__ void k_dust_init(const DiskView d, pg_dust* buf) {
     }
 }
 
+// Bound-0 radial ghosts of a dust buffer: init_CD (boundx_dust,
+// src/boundary/boundary.cu:64-113), every row.
+__global__ void k_dust_xghosts(const DiskView d, pg_dust* buf) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= 2 * NPAD * d.yarr) return;
+    const int j = k / (2 * NPAD), n = k % (2 * NPAD);
+    const int i = n < NPAD ? n : d.xres + n;  // 0..NPAD-1 and NPAD+xres..xarr-1
+    const bool bound0 = (n < NPAD) ? d.bound_lft == 0 : d.bound_rgh == 0;
+    if (!bound0) return;
+    const double* I = d.initd + 4 * i;
+    store_dust(buf, d.xarr, i, j, DCell{I[0], I[1], I[2], I[3]});
+}
+
+// The ghost images of every interior dust cell (boundy_dust and the bound 1/2
+// radial ghosts), for a dust state written by the caller.
+__global__ void k_dust_images(const DiskView d, pg_dust* buf) {
+    const long long n = (long long)d.xres * d.yres;
+    for (long long m = blockIdx.x * (long long)blockDim.x + threadIdx.x; m < n; m += (long long)gridDim.x * blockDim.x) {
+        const int i = NPAD + (int)(m % d.xres), j = d.ypad + (int)(m / d.xres);
+        emit_dust(d, buf, i, j, load_dust(buf, d.xarr, i, j));
+    }
+}
+
 // Interior dust from host arrays (r, u, v) with its ghost images.
 __global__ void k_dust_fill(const DiskView d, pg_dust* buf, const double* r, const double* u, const double* v) {
     const long long n = (long long)d.xres * d.yres;
@@ -424,6 +447,10 @@ void launch_dadvect(const DiskView& d, const DustMaps& in, pg_dust* out, cudaStr
     k_dadvect<<<dust_grid((const void*)k_dadvect, DA_SMEM, nt), DS_THREADS, DA_SMEM, s>>>(in.sweep_y, d, out, ntx, nt);
 }
 void launch_dust_init(const DiskView& d, pg_dust* buf, cudaStream_t s) { k_dust_init<<<592, 256, 0, s>>>(d, buf); }
+void launch_dust_xghosts(const DiskView& d, pg_dust* buf, cudaStream_t s) {
+    k_dust_xghosts<<<(2 * NPAD * d.yarr + 255) / 256, 256, 0, s>>>(d, buf);
+}
+void launch_dust_images(const DiskView& d, pg_dust* buf, cudaStream_t s) { k_dust_images<<<592, 256, 0, s>>>(d, buf); }
 void launch_dust_fill(const DiskView& d, pg_dust* buf, const double* r, const double* u, const double* v,
                       cudaStream_t s) {
     k_dust_fill<<<592, 256, 0, s>>>(d, buf, r, u, v);

@@ -315,6 +315,7 @@ struct Engine {
     long long steps_base = 0;
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     std::vector<const void*> ghosted;  // buffers whose constant radial ghosts are initialised
+    std::vector<const void*> dghosted; // dust buffers likewise (drop-in mode)
     pg_body* grid_planet = nullptr;    // drop-in mode: the caller's planets array
     double* part = nullptr;            // per-block partial sums of diagnostics
     pg_dust* dbuf[2] = {nullptr, nullptr};  // dust_flag: the dust of buf[k] is dbuf[k]
@@ -1463,7 +1464,6 @@ static pg_status grid_engine(pg_grid* dev, Engine** out) {
     if (dev->xres != g_params.xres || dev->yres != g_params.yres)
         return fail(PG_ERR_CONFIG, "grid dimensions differ from the configured parameters");
     if (dev->xbgn != 0) return fail(PG_ERR_CONFIG, "radial domain decomposition is not supported");
-    if (g_params.dust_flag) return fail(PG_ERR_CONFIG, "dust through the pg_grid_* entry points is not supported");
     std::lock_guard<std::mutex> lk(g_mu);
     auto it = g_grids.find(dev->xa);
     if (it != g_grids.end()) {
@@ -1504,7 +1504,7 @@ pg_status pg_grid_global_dt(pg_grid* hst, pg_grid* dev, double dt_prev, double* 
     Engine* E = nullptr;
     pg_status s = grid_engine(dev, &E);
     if (s != PG_OK) return s;
-    launch_cfl(E->view, reinterpret_cast<Cell*>(dev->C), E->stream);
+    launch_cfl(E->view, reinterpret_cast<Cell*>(dev->C), E->stream, E->view.dust ? dev->CD : nullptr);
     PG_CUDA(cudaGetLastError());
     pg_disk tmp{E};
     return pg_disk_global_dt(&tmp, dt_prev, dt_out);
@@ -1520,6 +1520,20 @@ pg_status pg_grid_solve(pg_grid* dev, double time, double dt) {
     if ((s = ensure_ghosts(*E, E->buf[1])) != PG_OK) return s;
     // the caller may have written the state: refresh the ghost images first
     launch_bound(E->view, E->buf[0], E->stream);
+    if (E->view.dust) {
+        if (!dev->CD || !dev->TD) return fail(PG_ERR_ARG, "dust_flag needs the grid's CD and TD");
+        E->dbuf[0] = dev->CD;
+        E->dbuf[1] = dev->TD;
+        for (pg_dust* b : {dev->CD, dev->TD}) {
+            bool seen = false;
+            for (const void* p : E->dghosted) seen = seen || p == b;
+            if (!seen) {
+                launch_dust_xghosts(E->view, b, E->stream);
+                E->dghosted.push_back(b);
+            }
+        }
+        launch_dust_images(E->view, dev->CD, E->stream);
+    }
     if (E->view.nplanet > 0 && dev->planets) k_grid_planet_in<<<1, 1, 0, E->stream>>>(E->sc, dev->planets);
     launch_set_time(E->view, time, dt, E->stream);
     if ((s = enqueue_stages(*E)) != PG_OK) return s;
@@ -1529,6 +1543,11 @@ pg_status pg_grid_solve(pg_grid* dev, double time, double dt) {
         pg_cell* t = dev->C;
         dev->C = dev->T;
         dev->T = t;
+        if (E->view.dust) {  // the dust pairs with the gas (src/solver/dust/dust.cu:230-233)
+            pg_dust* td = dev->CD;
+            dev->CD = dev->TD;
+            dev->TD = td;
+        }
     }
     return PG_OK;
 }

@@ -89,6 +89,8 @@ void launch_dsweep_x(const DiskView& d, const DustMaps& in, pg_dust* out, cudaSt
 void launch_dsweep_y(const DiskView& d, const DustMaps& in, pg_dust* out, cudaStream_t s);
 void launch_dadvect(const DiskView& d, const DustMaps& in, pg_dust* out, cudaStream_t s);
 void launch_dust_init(const DiskView& d, pg_dust* buf, cudaStream_t s);
+void launch_dust_xghosts(const DiskView& d, pg_dust* buf, cudaStream_t s);
+void launch_dust_images(const DiskView& d, pg_dust* buf, cudaStream_t s);
 void launch_dust_fill(const DiskView& d, pg_dust* buf, const double* r, const double* u, const double* v,
                       cudaStream_t s);
 void launch_dust_extract(const DiskView& d, const pg_dust* buf, double* r, double* u, double* v, cudaStream_t s);

@@ -1,5 +1,5 @@
 """The reference's own main.cu, relinked through penguin_b200/shim against
-libpenguin_b200.so, run on a golden case.  Needs a B200
+libpenguin_b200.so, run on golden cases (gas; gas + dust).  Needs a B200
 and the relinked executable (built next to the reference objects by
 __graft_entry__.build() where the reference sources are available)."""
 import glob
@@ -22,13 +22,14 @@ def rel_l1(a, b):
     return np.abs(a - b).sum() / np.abs(b).sum()
 
 
-@pytest.mark.parametrize("name", ["disk64_n10"])
+@pytest.mark.parametrize("name", ["disk64_n10", "dust64_st01_n10"])
 def test_relinked_main_reproduces_reference(name, tmp_path):
     exe = os.path.join(ROOT, "oracle", "_ref", name, "dropin", "penguin")
     fx = os.path.join(GOLDEN, name + ".npz")
     if not os.path.exists(exe) or not os.path.exists(fx):
         pytest.skip("relinked executable or fixture not available")
-    case = [c for c in C.cases() if c["name"] == name][0]
+    case = [c for c in C.cases() + C.dust_cases() if c["name"] == name][0]
+    dust = bool(case.get("dust"))
     p = case["params"]
     z = np.load(fx)
     xa, _ = make_grid_np(p.xmin, p.xmax, p.xres, 3, p.geomx, p.gridx)
@@ -40,10 +41,15 @@ def test_relinked_main_reproduces_reference(name, tmp_path):
     assert r.returncode == 0, r.stdout + r.stderr
     out = glob.glob(str(tmp_path / "binary_*_00001"))
     assert out, r.stdout
-    res = snapshot.read_snapshot(out[0], p.xres, p.yres, 2)
+    res = snapshot.read_snapshot(out[0], p.xres, p.yres, 2, dust=dust)
     assert res["t"] == pytest.approx(float(z["t"]), rel=max(1e-13, case["cuda_tol"]))
     for k in ("r", "p"):
         assert rel_l1(res[k], z["out_" + k]) < case["cuda_tol"], k
     mx, my = res["r"] * res["u"], res["r"] * res["v"]
     rx, ry = z["out_r"] * z["out_u"], z["out_r"] * z["out_v"]
     assert (np.abs(mx - rx) + np.abs(my - ry)).sum() / (np.abs(rx) + np.abs(ry)).sum() < case["cuda_tol"]
+    if dust:  # the reference's dust kernels run with their stale shared memory zeroed (tests/golden/cases.py)
+        assert rel_l1(res["dust_r"], z["out_dust_r"]) < case["cuda_tol"]
+        dx, dy = res["dust_r"] * res["dust_u"], res["dust_r"] * res["dust_v"]
+        ex, ey = z["out_dust_r"] * z["out_dust_u"], z["out_dust_r"] * z["out_dust_v"]
+        assert (np.abs(dx - ex) + np.abs(dy - ey)).sum() / (np.abs(ex) + np.abs(ey)).sum() < case["cuda_tol"]
