@@ -318,6 +318,19 @@ def measure_adjoint(steps, local, stream):
     # PPM flattening coefficient varies on a 1e-8 scale
     for eps in (1.0e-6, 1.0e-7, 1.0e-8, 1.0e-9, 1.0e-10):
         fd[str(eps)] = (loss(m.forward(s0 + eps * d, replay=True)) - loss(m.forward(s0 - eps * d, replay=True))) / (2 * eps)
+    # the same check from a generic smooth state (no noise, a 1 % spiral; the
+    # recorded dt schedule replayed): the quotients converge to the adjoint
+    s0s = torch.tensor(I.disk_state(p, seed=SEED_DUST, noise=0.0)["r"]
+                       * (1.0 + 0.01 * np.sin(y[:, None] + 3.0 * np.log(x[None, :]))), device=s0.device)
+    outs = m.forward(s0s, replay=True)
+    gsm = (2.0 * (outs.mean(0) - target) / p.yres)[None, :].expand(p.yres, p.xres).contiguous()
+    gs_s, _ = m.backward(gsm)
+    ds = d / s0 * s0s
+    ad_s = float((gs_s * ds).sum())
+    fd_s = {}
+    for eps in (1.0e-6, 1.0e-7, 1.0e-8):
+        fd_s[str(eps)] = (loss(m.forward(s0s + eps * ds, replay=True)) -
+                          loss(m.forward(s0s - eps * ds, replay=True))) / (2 * eps)
     theta = [p.planet_mass, p.ss_alpha, p.sc_h]
     fdt = []
     for k in range(3):
@@ -334,8 +347,10 @@ def measure_adjoint(steps, local, stream):
         "workload": "256x768 gradient disk, FP64 forward + adjoint, checkpoint every 64 steps",
         "steps": steps, "forward_ms_per_step": ms_f / steps, "adjoint_ms_per_step": ms_b / steps,
         "adjoint_over_forward": ms_b / ms_f, "device_bytes": m.device_bytes,
-        "fd_sigma0": {"adjoint": ad, "central": fd,
+        "fd_sigma0": {"state": "the workload's noisy disk", "adjoint": ad, "central": fd,
                       "rel_err": {k: abs(ad - v) / abs(v) for k, v in fd.items()}},
+        "fd_sigma0_smooth": {"state": "no noise, 1 % spiral", "adjoint": ad_s, "central": fd_s,
+                             "rel_err": {k: abs(ad_s - v) / abs(v) for k, v in fd_s.items()}},
         "fd_theta": {"names": ["q", "alpha", "h"], "adjoint": [float(v) for v in gth], "central_rel_step_1e-4": fdt,
                      "rel_err": [abs(a - b) / abs(b) for a, b in zip(gth, fdt)]},
     }
