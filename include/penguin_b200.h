@@ -235,6 +235,11 @@ pg_status pg_ens_check(pg_ens* e);
    with compensated summation (syncs). */
 pg_status pg_ens_totals(pg_ens* e, int k, double* mass, double* angmom);
 /* Disk k's torque of the planet on the disk, as pg_disk_torque (syncs). */
+/* dust_flag members (one pressureless dust fluid, FP32-mixed like the gas):
+   the interior dust r, v_r, v_phi of the newest state; set_state resets it to
+   init_CD. */
+pg_status pg_ens_set_dust(pg_ens* e, int k, const double* r, const double* u, const double* v);
+pg_status pg_ens_get_dust(pg_ens* e, int k, double* r, double* u, double* v);
 pg_status pg_ens_torque(pg_ens* e, int k, double* torque);
 int pg_ens_kernels_per_step(const pg_ens* e);
 /* As pg_disk_profile, for the whole ensemble (slots 0 clocks + planet tables,

@@ -29,7 +29,8 @@ EXPORTS = [
     "pg_disk_planet", "pg_disk_check", "pg_disk_torque", "pg_kernels_per_step", "pg_disk_profile",
     "pg_ens_check_params", "pg_ens_create", "pg_ens_destroy", "pg_ens_size", "pg_ens_dims", "pg_ens_set_state",
     "pg_ens_get_state", "pg_ens_run", "pg_ens_sync", "pg_ens_clock", "pg_ens_planet", "pg_ens_check",
-    "pg_ens_totals", "pg_ens_torque", "pg_ens_kernels_per_step", "pg_ens_profile",
+    "pg_ens_totals", "pg_ens_torque", "pg_ens_kernels_per_step", "pg_ens_profile", "pg_ens_set_dust",
+    "pg_ens_get_dust",
     "pg_adj_check_params", "pg_adj_create", "pg_adj_destroy", "pg_adj_set_params", "pg_adj_forward",
     "pg_adj_backward", "pg_adj_model_error", "pg_adj_dot_test", "pg_adj_pass_check", "pg_adj_replay_diff", "pg_adj_pass_fields", "pg_adj_schedule", "pg_adj_steps", "pg_adj_device_bytes",
 ]
@@ -108,6 +109,8 @@ def lib() -> ctypes.CDLL:
         "pg_ens_check": (i, [vp]),
         "pg_ens_totals": (i, [vp, i, dp, dp]),
         "pg_ens_torque": (i, [vp, i, dp]),
+        "pg_ens_set_dust": (i, [vp, i, dp, dp, dp]),
+        "pg_ens_get_dust": (i, [vp, i, dp, dp, dp]),
         "pg_adj_check_params": (i, [PP]),
         "pg_adj_create": (i, [PP, i, vp, i, ctypes.POINTER(vp)]),
         "pg_adj_destroy": (i, [vp]),

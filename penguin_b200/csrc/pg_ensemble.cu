@@ -62,6 +62,8 @@ struct EDisk {
     float* tab = nullptr;
     float* trig = nullptr;
     double* cs64 = nullptr;
+    float* dbuf = nullptr;   // dust_flag: two buffers of NPL residual planes
+    float* dflux = nullptr;  // dust face fluxes
     bool fresh = true;
     View32 v{};
 };
@@ -78,6 +80,8 @@ struct pg_ens {
     CUtensorMap* dMaps = nullptr;
     double* dPart = nullptr;
     int ntiles[3] = {0, 0, 0};
+    int* dDoff = nullptr;               // [3][n + 1] running counts of dust faces and cells
+    long long dcount[3] = {0, 0, 0};    // radial faces, azimuthal faces, cells of all dust disks
     int maxn = 0;
     int cur = 0;
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
@@ -91,12 +95,15 @@ struct pg_ens {
             cudaFree(D.tab);
             cudaFree(D.trig);
             cudaFree(D.cs64);
+            cudaFree(D.dbuf);
+            cudaFree(D.dflux);
             if (D.E) engine_destroy(D.E);
         }
         cudaFree(dV);
         cudaFree(dFirst);
         cudaFree(dMaps);
         cudaFree(dPart);
+        cudaFree(dDoff);
         if (own_stream && stream) cudaStreamDestroy(stream);
     }
 };
@@ -107,7 +114,10 @@ namespace {
 pg_status enqueue_step(pg_ens* e, int in) {
     launch_time32(e->dV, e->n, e->stream);
     launch_trig32(e->dV, e->n, e->maxn, e->stream);
-    for (int p = 0; p < kPasses; ++p) launch_pass32(p, e->dV, e->dFirst, e->n, e->ntiles, in ^ (p & 1), e->stream);
+    for (int p = 0; p < kPasses; ++p) {
+        launch_pass32(p, e->dV, e->dFirst, e->n, e->ntiles, in ^ (p & 1), e->stream);
+        launch_dust_pass32(p, e->dV, e->dDoff, e->n, e->dcount, in ^ (p & 1), e->stream);
+    }
     ENS_CUDA(cudaGetLastError());
     return PG_OK;
 }
@@ -188,6 +198,7 @@ pg_status pg_ens_create(const pg_params* P, int n, int device, void* stream, pg_
         return bail(ens_fail(PG_ERR_CUDA, std::string("cudaMalloc: ") + cudaGetErrorString(ce)));
     std::vector<CUtensorMap> maps(7 * (size_t)n);
     std::vector<View32> hv(n);
+    std::vector<int> doff(3 * (n + 1), 0);
     for (int k = 0; k < n; ++k) {
         EDisk& D = e->disks[k];
         if ((s = table_engine_create(&P[k], device, e->stream, &D.E)) != PG_OK) return bail(s);
@@ -237,6 +248,29 @@ pg_status pg_ens_create(const pg_params* P, int n, int device, void* stream, pg_
                 return bail(s);
         }
         if ((s = make_map3_f32(&m[6], v.vis, v.pitch, v.yarr, 2, 36, 10, 2)) != PG_OK) return bail(s);
+        long long nd3[3] = {0, 0, 0};
+        if (P[k].dust_flag) {
+            // init_CD everywhere: zero residuals
+            const size_t nf = (size_t)(v.xres + 1) * (v.yres + 1);
+            if ((ce = cudaMalloc(&D.dbuf, sizeof(float) * 2 * NPL * plane)) != cudaSuccess ||
+                (ce = cudaMalloc(&D.dflux, sizeof(float) * 3 * nf)) != cudaSuccess)
+                return bail(ens_fail(PG_ERR_CUDA, std::string("cudaMalloc: ") + cudaGetErrorString(ce)));
+            cudaMemsetAsync(D.dbuf, 0, sizeof(float) * 2 * NPL * plane, e->stream);
+            cudaMemsetAsync(D.dflux, 0, sizeof(float) * 3 * nf, e->stream);
+            v.dbuf[0] = D.dbuf;
+            v.dbuf[1] = D.dbuf + NPL * plane;
+            v.dflux = D.dflux;
+            v.dust = 1;
+            v.st_h = (float)(P[k].stokes * P[k].sc_h);
+            v.dust_rmin = (float)(P[k].d_g_ratio * SMALLR);
+            nd3[0] = (long long)(v.xres + 1) * v.yres;
+            nd3[1] = (long long)v.xres * (v.yres + 1);
+            nd3[2] = (long long)v.xres * v.yres;
+        }
+        for (int r = 0; r < 3; ++r) {
+            doff[r * (n + 1) + k + 1] = doff[r * (n + 1) + k] + (int)nd3[r];
+            e->dcount[r] += nd3[r];
+        }
         launch_init_tables32(v, D.tab, D.tab + (size_t)X_NSLOT * v.xn, D.cs64, e->stream);
         first[0 * (n + 1) + k + 1] = first[0 * (n + 1) + k] + v.ntx[0] * cdivi(d.yres, 8);
         first[1 * (n + 1) + k + 1] = first[1 * (n + 1) + k] + v.ntx[1] * cdivi(d.xres, 8);
@@ -245,7 +279,10 @@ pg_status pg_ens_create(const pg_params* P, int n, int device, void* stream, pg_
         hv[k] = v;
     }
     for (int p = 0; p < 3; ++p) e->ntiles[p] = first[p * (n + 1) + n];
-    if ((ce = cudaMemcpyAsync(e->dMaps, maps.data(), sizeof(CUtensorMap) * maps.size(), cudaMemcpyHostToDevice,
+    if ((ce = cudaMalloc(&e->dDoff, sizeof(int) * doff.size())) != cudaSuccess ||
+        (ce = cudaMemcpyAsync(e->dDoff, doff.data(), sizeof(int) * doff.size(), cudaMemcpyHostToDevice, e->stream)) !=
+            cudaSuccess ||
+        (ce = cudaMemcpyAsync(e->dMaps, maps.data(), sizeof(CUtensorMap) * maps.size(), cudaMemcpyHostToDevice,
                               e->stream)) != cudaSuccess ||
         (ce = cudaMemcpyAsync(e->dV, hv.data(), sizeof(View32) * hv.size(), cudaMemcpyHostToDevice, e->stream)) !=
             cudaSuccess ||
@@ -290,6 +327,9 @@ pg_status pg_ens_set_state(pg_ens* e, int k, double t, const double* r, const do
     launch_fill32(e->dV + k, e->cur, st, st + n, v ? st + 2 * n : nullptr, e->stream);
     ENS_CUDA(cudaGetLastError());
     ENS_CUDA(cudaFreeAsync(st, e->stream));
+    if (D.v.dust)  // a restart's dust is init_CD (the reference's load_grid reads the gas only)
+        ENS_CUDA(cudaMemsetAsync(D.v.dbuf[e->cur], 0, sizeof(float) * NPL * (size_t)D.v.pitch * D.v.yarr,
+                                 e->stream));
     engine_init_planet(D.E, t);
     ENS_CUDA(cudaMemsetAsync(&D.v.d64.sc->vmax_bits, 0, sizeof(unsigned long long), e->stream));
     launch_cfl32(e->dV + k, e->cur, e->stream);
@@ -454,7 +494,50 @@ pg_status pg_ens_torque(pg_ens* e, int k, double* torque) {
     return PG_OK;
 }
 
-int pg_ens_kernels_per_step(const pg_ens* e) { return e ? 2 + kPasses : 0; }
+int pg_ens_kernels_per_step(const pg_ens* e) { return e ? 2 + kPasses + (e->dcount[2] > 0 ? 6 : 0) : 0; }
+
+// dust_flag members: the interior dust (absolute r, v_r, v_phi) of the newest state
+pg_status pg_ens_set_dust(pg_ens* e, int k, const double* r, const double* u, const double* v) {
+    pg_status s = check_index(e, k);
+    if (s != PG_OK) return s;
+    if (!r || !u || !v) return ens_fail(PG_ERR_ARG, "null dust array");
+    EDisk& D = e->disks[k];
+    if (!D.v.dust) return ens_fail(PG_ERR_CONFIG, "the disk has no dust (dust_flag 0)");
+    ENS_CUDA(cudaSetDevice(e->device));
+    const size_t n = (size_t)D.v.xres * D.v.yres;
+    double* st = nullptr;
+    ENS_CUDA(cudaMallocAsync(&st, 3 * n * sizeof(double), e->stream));
+    ENS_CUDA(cudaMemcpyAsync(st, r, n * sizeof(double), cudaMemcpyHostToDevice, e->stream));
+    ENS_CUDA(cudaMemcpyAsync(st + n, u, n * sizeof(double), cudaMemcpyHostToDevice, e->stream));
+    ENS_CUDA(cudaMemcpyAsync(st + 2 * n, v, n * sizeof(double), cudaMemcpyHostToDevice, e->stream));
+    launch_dfill32(e->dV + k, e->cur, st, st + n, st + 2 * n, e->stream);
+    ENS_CUDA(cudaFreeAsync(st, e->stream));
+    ENS_CUDA(cudaMemsetAsync(&D.v.d64.sc->vmax_bits, 0, sizeof(unsigned long long), e->stream));
+    launch_cfl32(e->dV + k, e->cur, e->stream);
+    ENS_CUDA(cudaGetLastError());
+    ENS_CUDA(cudaStreamSynchronize(e->stream));
+    return PG_OK;
+}
+
+pg_status pg_ens_get_dust(pg_ens* e, int k, double* r, double* u, double* v) {
+    pg_status s = check_index(e, k);
+    if (s != PG_OK) return s;
+    if (!r || !u || !v) return ens_fail(PG_ERR_ARG, "null dust array");
+    EDisk& D = e->disks[k];
+    if (!D.v.dust) return ens_fail(PG_ERR_CONFIG, "the disk has no dust (dust_flag 0)");
+    ENS_CUDA(cudaSetDevice(e->device));
+    const size_t n = (size_t)D.v.xres * D.v.yres;
+    double* st = nullptr;
+    ENS_CUDA(cudaMallocAsync(&st, 3 * n * sizeof(double), e->stream));
+    launch_dextract32(e->dV + k, e->cur, st, st + n, st + 2 * n, e->stream);
+    ENS_CUDA(cudaGetLastError());
+    ENS_CUDA(cudaMemcpyAsync(r, st, n * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
+    ENS_CUDA(cudaMemcpyAsync(u, st + n, n * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
+    ENS_CUDA(cudaMemcpyAsync(v, st + 2 * n, n * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
+    ENS_CUDA(cudaFreeAsync(st, e->stream));
+    ENS_CUDA(cudaStreamSynchronize(e->stream));
+    return PG_OK;
+}
 
 pg_status pg_ens_profile(pg_ens* e, int nsteps, double end_time, float* ms, int nslot) {
     if (!e || !ms || nslot < 6) return ens_fail(PG_ERR_ARG, "bad argument");
@@ -472,6 +555,7 @@ pg_status pg_ens_profile(pg_ens* e, int nsteps, double end_time, float* ms, int 
         for (int p = 0; p < kPasses; ++p) {
             ENS_CUDA(cudaEventRecord(ev[1 + p], e->stream));
             launch_pass32(p, e->dV, e->dFirst, e->n, e->ntiles, c0 ^ (p & 1), e->stream);
+            launch_dust_pass32(p, e->dV, e->dDoff, e->n, e->dcount, c0 ^ (p & 1), e->stream);
         }
         ENS_CUDA(cudaEventRecord(ev[6], e->stream));
         ENS_CUDA(cudaGetLastError());

@@ -167,6 +167,378 @@ __device__ __forceinline__ double rate64(const View32& w, int i, int j, float du
     return fmax(a, b);
 }
 
+// the dust's CFL rate (timestep.cu:64-74): its speeds without a sound speed
+__device__ __forceinline__ double drate64(const View32& w, int i, int j, float du, float dv) {
+    const DiskView& d = w.d64;
+    const double u = d.initd[4 * i + 1] + (double)du;
+    const double vn = (d.initd[4 * i + 2] - d.radx[i] * d.frame_omega - d.rot[i]) + (double)dv;
+    return fmax(fabs(u) * d.idx_x[i], fabs(vn) * (d.idx_y[j] * d.irad[i]));
+}
+
+// ================================================================ dust
+// One pressureless dust fluid (dust_flag) in the FP32-mixed form: residual
+// planes {dSigma_d, dv_r,d, dv_phi,d} against init_CD, transported by the
+// reference's upwind PPM fluxes with the compression factor and the flux
+// limiter (src/solver/dust/dust.cu:6-147) and updated by update_Dust
+// (dust.cu:149-176) in residual form, e.g. v_new - v = (D(Sigma v) - v D Sigma) /
+// Sigma_new with the transported field taken relative to a neighbouring cell.
+// Each sweep is two launches over all dust disks: one thread per face (the two
+// edge states it needs and the limited fluxes into a scratch array), then one
+// thread per cell.  The dust planes carry no ghost images: rows wrap, and the
+// radial ghosts of boundary 0 hold init_CD, i.e. zero residuals.
+struct DR {
+    float S, u, v;  // residuals
+};
+__device__ __forceinline__ int wrap32(const View32& w, int j) {
+    if (j < NPAD) return j + w.yres;
+    if (j >= NPAD + w.yres) return j - w.yres;
+    return j;
+}
+__device__ __forceinline__ DR dload(const View32& w, const float* b, int i, int j) {
+    if (i < NPAD || i >= NPAD + w.xres) return {0.0f, 0.0f, 0.0f};
+    const size_t pl = w.plane(), m = (size_t)wrap32(w, j) * w.pitch + i;
+    return {b[m], b[pl + m], b[2 * pl + m]};
+}
+__device__ __forceinline__ void dstore(const View32& w, float* b, int i, int j, const DR& c) {
+    const size_t pl = w.plane(), m = (size_t)j * w.pitch + i;
+    b[m] = c.S;
+    b[pl + m] = c.u;
+    b[2 * pl + m] = c.v;
+}
+__device__ __forceinline__ float exp_limf(float x) { return fmaxf(1.0f + x, 1.0e-6f); }
+
+struct DEdge {
+    float S, u, t;  // density and normal velocity (absolute), transported field relative to the cell
+};
+
+// Both edge states of dust cell c of a pencil (dust.cu:6-103): DIR 0 radial
+// (row q; normal v_r, transported r v_phi), DIR 1 azimuthal (column q; normal
+// v_phi - orb_rot - r Omega, transported v_r).  Also the cell's averages.
+template <int DIR>
+__device__ __forceinline__ void dust_edges(const View32& w, const float* b, int c, int q, float dtf, DEdge& L,
+                                           DEdge& R, float& Sc, float& tc) {
+    float aS[5], aU[5], aT[5];
+    const DR C = (DIR == 0) ? dload(w, b, c, q) : dload(w, b, q, c);
+    float idx, sdt, uc;
+    const float* wt;
+    float wts[6];
+    if (DIR == 0) {
+        float db[12];
+        xload<12>(w, X_DDBG, c, db);
+        const float* rad = w.x(X_RAD);
+#pragma unroll
+        for (int m = 0; m < 5; ++m) {
+            if (m == 2) {
+                aS[m] = aU[m] = aT[m] = 0.0f;
+                continue;
+            }
+            const int kk = m < 2 ? m : m - 1;
+            const DR N = dload(w, b, c - 2 + m, q);
+            aS[m] = db[kk] + (N.S - C.S);
+            aU[m] = db[4 + kk] + (N.u - C.u);
+            aT[m] = db[8 + kk] + (rad[c - 2 + m] * N.v - rad[c] * C.v);
+        }
+        xload<6>(w, X_WX, c, wts);
+        wt = wts;
+        idx = w.x(X_IDX)[c];
+        sdt = dtf;
+        Sc = w.x(X_DSBG)[c] + C.S;
+        uc = w.x(X_DUBG)[c] + C.u;
+        tc = C.v;  // only differences of r v_phi are used
+    } else {
+#pragma unroll
+        for (int m = 0; m < 5; ++m) {
+            if (m == 2) {
+                aS[m] = aU[m] = aT[m] = 0.0f;
+                continue;
+            }
+            const DR N = dload(w, b, q, c - 2 + m);
+            aS[m] = N.S - C.S;
+            aU[m] = N.v - C.v;
+            aT[m] = N.u - C.u;
+        }
+        const int cw = wrap32(w, c);
+        yload<6>(w, Y_WY, cw, wts);
+        wt = wts;
+        idx = w.y(Y_IDY)[cw];
+        sdt = dtf * w.x(X_IRAD)[q];
+        Sc = w.x(X_DSBG)[q] + C.S;
+        uc = w.x(X_DEPS)[q] + C.v;
+        tc = C.u;
+    }
+    const Par32 Rp = recon32(wt, aS[0], aS[1], aS[3], aS[4], 0.0f);
+    const Par32 Up = recon32(wt, aU[0], aU[1], aU[3], aU[4], 0.0f);
+    const Par32 Tp = recon32(wt, aT[0], aT[1], aT[3], aT[4], 0.0f);
+    const float dx = 1.0f / idx;
+    {  // left edge: the right state of the face below
+        const float ue = uc - Up.sL;
+        const Frac32 q1 = frac32(lim01f(-fminf(ue, 0.0f) * sdt * idx));
+        const float urd = aveL32(q1, Up);
+        const float u_ = sdt * urd / (dx + fminf(ue, 0.0f) * sdt);
+        const float ur = uc + urd;
+        const Frac32 q2 = frac32(lim01f(-fminf(ur, 0.0f) * sdt * idx));
+        L.S = (Sc + aveL32(q2, Rp)) * exp_limf(u_);
+        L.u = uc + aveL32(q2, Up);
+        L.t = aveL32(q2, Tp);
+    }
+    {  // right edge: the left state of the face above
+        const float ue = uc + Up.sR;
+        const Frac32 q1 = frac32(lim01f(fmaxf(ue, 0.0f) * sdt * idx));
+        const float uld = aveR32(q1, Up);
+        const float u_ = -sdt * uld / (dx - fmaxf(ue, 0.0f) * sdt);
+        const float ul = uc + uld;
+        const Frac32 q2 = frac32(lim01f(fmaxf(ul, 0.0f) * sdt * idx));
+        R.S = (Sc + aveR32(q2, Rp)) * exp_limf(u_);
+        R.u = uc + aveR32(q2, Up);
+        R.t = aveR32(q2, Tp);
+    }
+}
+
+// dust offsets: [3][nd + 1] running counts of radial faces, azimuthal faces, cells
+__device__ __forceinline__ bool dust_unit(const int* doff, int nd, int row, long long g, int& k, int& loc) {
+    const int* o = doff + row * (nd + 1);
+    if (g >= o[nd]) return false;
+    k = find_disk(o, nd, (int)g);
+    loc = (int)(g - o[k]);
+    return true;
+}
+
+// face fluxes of the dust sweeps: DIR 0 radial, DIR 1 azimuthal
+template <int DIR>
+__global__ void __launch_bounds__(256) k32d_faces(const View32* __restrict__ V, const int* __restrict__ doff, int nd,
+                                                 int in) {
+    const long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    int k, loc;
+    if (!dust_unit(doff, nd, DIR, g, k, loc)) return;
+    const View32& w = V[k];
+    if (w.d64.sc->done) return;
+    const float dtf = (float)w.d64.sc->dt;
+    const float* b = w.dbuf[in];
+    int f, q;
+    if (DIR == 0) {
+        f = NPAD + loc % (w.xres + 1);
+        q = NPAD + loc / (w.xres + 1);
+    } else {
+        q = NPAD + loc % w.xres;
+        f = NPAD + loc / w.xres;
+    }
+    DEdge La, Ra, Lb, Rb;
+    float Sa, ta, Sb, tb;
+    dust_edges<DIR>(w, b, f - 1, q, dtf, La, Ra, Sa, ta);
+    dust_edges<DIR>(w, b, f, q, dtf, Lb, Rb, Sb, tb);
+    float ia, ib, sdt;
+    if (DIR == 0) {
+        ia = w.x(X_IDX)[f - 1];
+        ib = w.x(X_IDX)[f];
+        sdt = dtf;
+    } else {
+        ia = w.y(Y_IDY)[wrap32(w, f - 1)];
+        ib = w.y(Y_IDY)[wrap32(w, f)];
+        sdt = dtf * w.x(X_IRAD)[q];
+    }
+    // dust_flow's limiter (dust.cu:120-147)
+    const float Fl = fminf(Sa * sdt * ia, fmaxf(Ra.u * Ra.S, 0.0f));
+    const float Fr = fmaxf(-Sb * sdt * ib, fminf(Lb.u * Lb.S, 0.0f));
+    // the jump of the transported field from cell a to cell b
+    float jab;
+    if (DIR == 0) jab = w.x(X_DDBG + 10)[f - 1] + (w.x(X_RAD)[f] * tb - w.x(X_RAD)[f - 1] * ta);
+    else jab = tb - ta;
+    const size_t fp = (size_t)(w.xres + 1) * (w.yres + 1);
+    const size_t m = (DIR == 0) ? (size_t)(q - NPAD) * (w.xres + 1) + (f - NPAD)
+                                : (size_t)(f - NPAD) * (w.xres + 1) + (q - NPAD);
+    w.dflux[m] = Fl + Fr;
+    w.dflux[fp + m] = Fl * Ra.u + Fr * Lb.u;
+    w.dflux[2 * fp + m] = Fl * Ra.t + Fr * (jab + Lb.t);  // relative to cell a
+}
+
+// update_Dust of one cell from its two faces; DIR 1 writes at the orbital-shifted row
+template <int DIR>
+__global__ void __launch_bounds__(256) k32d_update(const View32* __restrict__ V, const int* __restrict__ doff, int nd,
+                                                  int in) {
+    const long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    int k, loc;
+    if (!dust_unit(doff, nd, 2, g, k, loc)) return;
+    const View32& w = V[k];
+    Scalars* sc = w.d64.sc;
+    const int i = NPAD + loc % w.xres, j = NPAD + loc / w.xres;
+    const float* b = w.dbuf[in];
+    DR Q = dload(w, b, i, j);
+    int jo = j;
+    if (!sc->done) {
+        const float dtf = (float)sc->dt;
+        const size_t fp = (size_t)(w.xres + 1) * (w.yres + 1);
+        size_t m0, m1;
+        float f, g0 = 1.0f, g1 = 1.0f;
+        if (DIR == 0) {
+            m0 = (size_t)(j - NPAD) * (w.xres + 1) + (i - NPAD);
+            m1 = m0 + 1;
+            g0 = w.x(X_XA)[i];
+            g1 = w.x(X_XA)[i + 1];
+            f = dtf * w.x(X_IXV)[i];
+        } else {
+            m0 = (size_t)(j - NPAD) * (w.xres + 1) + (i - NPAD);
+            m1 = m0 + (w.xres + 1);
+            f = dtf * w.y(Y_IYV)[j] * w.x(X_IRAD)[i];
+        }
+        const float F0 = w.dflux[m0], F1 = w.dflux[m1];
+        const float U0 = w.dflux[fp + m0], U1 = w.dflux[fp + m1];
+        const float T0 = w.dflux[2 * fp + m0], T1 = w.dflux[2 * fp + m1];
+        float un, jm;  // normal velocity of the cell; jump of the transported field from the cell below
+        if (DIR == 0) {
+            un = w.x(X_DUBG)[i] + Q.u;
+            const DR P = dload(w, b, i - 1, j);
+            jm = -(w.x(X_DDBG + 9)[i] + (w.x(X_RAD)[i - 1] * P.v - w.x(X_RAD)[i] * Q.v));
+        } else {
+            un = w.x(X_DEPS)[i] + Q.v;
+            const DR P = dload(w, b, i, j - 1);
+            jm = Q.u - P.u;
+        }
+        const float DS = (F0 * g0 - F1 * g1) * f;
+        const float Dn = (g0 * (U0 - F0 * un) - g1 * (U1 - F1 * un)) * f;  // D(Sigma u_n) - u_n D Sigma
+        const float Dt = (g0 * (T0 - F0 * jm) - g1 * T1) * f;              // D(Sigma t) - t D Sigma
+        const float Sc = w.x(X_DSBG)[i] + Q.S;
+        const float Sn = Sc + DS;
+        const float rmin = fmaxf(Sc * 1.0e-10f, w.dust_rmin);
+        if (Sn < rmin) {
+            Q.S = rmin - w.x(X_DSBG)[i];
+        } else {
+            const float iS = 1.0f / Sn;
+            Q.S += DS;
+            if (DIR == 0) {
+                Q.u += Dn * iS;
+                Q.v += Dt * w.x(X_IRAD)[i] * iS;
+            } else {
+                Q.v += Dn * iS;
+                Q.u += Dt * iS;
+            }
+        }
+        if (!(Sn > 0.0f)) atomicOr(&sc->err, 1 << PG_ERR_NAN);
+        if (DIR == 1 && w.orbadv) {  // the gas's shift of this radius (orbit.cu:30-46)
+            int js = (j - NPAD + w.d64.inc[i]) % w.yres;
+            if (js < 0) js += w.yres;
+            jo = js + NPAD;
+        }
+    }
+    dstore(w, w.dbuf[in ^ 1], i, jo, Q);
+}
+
+// residual advection of the dust by orb_res (advection.cu:175-357): the face
+// flux from the upwind cell
+__global__ void __launch_bounds__(256) k32d_adv_faces(const View32* __restrict__ V, const int* __restrict__ doff,
+                                                     int nd, int in) {
+    const long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    int k, loc;
+    if (!dust_unit(doff, nd, 1, g, k, loc)) return;
+    const View32& w = V[k];
+    if (w.d64.sc->done) return;
+    const float dtf = (float)w.d64.sc->dt;
+    const float* b = w.dbuf[in];
+    const int q = NPAD + loc % w.xres, f = NPAD + loc / w.xres;
+    const float speed = (float)w.d64.res[q];
+    const int c = speed > 0.0f ? f - 1 : f;  // the upwind cell
+    float aS[5], aV[5], aU[5];
+    const DR C = dload(w, b, q, c);
+#pragma unroll
+    for (int m = 0; m < 5; ++m) {
+        const DR N = dload(w, b, q, c - 2 + m);
+        aS[m] = N.S - C.S;
+        aV[m] = N.v - C.v;
+        aU[m] = N.u - C.u;
+    }
+    const int cw = wrap32(w, c);
+    float wt[6];
+    yload<6>(w, Y_WY, cw, wt);
+    const Par32 Rp = recon32(wt, aS[0], aS[1], aS[3], aS[4], 0.0f);
+    const Par32 Vp = recon32(wt, aV[0], aV[1], aV[3], aV[4], 0.0f);
+    const Par32 Up = recon32(wt, aU[0], aU[1], aU[3], aU[4], 0.0f);
+    const float sdt = dtf * w.x(X_IRAD)[q], idx = w.y(Y_IDY)[cw];
+    const float Sc = w.x(X_DSBG)[q] + C.S;
+    float fr, fv, fu;
+    if (speed > 0.0f) {
+        const Frac32 fq = frac32(lim01f(speed * sdt * idx));
+        fr = Sc + aveR32(fq, Rp);
+        fv = aveR32(fq, Vp);
+        fu = aveR32(fq, Up);
+    } else {
+        const Frac32 fq = frac32(lim01f(-speed * sdt * idx));
+        fr = Sc + aveL32(fq, Rp);
+        fv = aveL32(fq, Vp);
+        fu = aveL32(fq, Up);
+    }
+    if (c == f) {  // relative to the face's lower cell f - 1
+        const DR P = dload(w, b, q, f - 1);
+        fv += C.v - P.v;
+        fu += C.u - P.u;
+    }
+    const float F = fr * speed;
+    const size_t fp = (size_t)(w.xres + 1) * (w.yres + 1);
+    const size_t m = (size_t)(f - NPAD) * (w.xres + 1) + (q - NPAD);
+    w.dflux[m] = F;
+    w.dflux[fp + m] = F * fv;
+    w.dflux[2 * fp + m] = F * fu;
+}
+
+__global__ void __launch_bounds__(256) k32d_adv_update(const View32* __restrict__ V, const int* __restrict__ doff,
+                                                      int nd, int in) {
+    const long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    int k, loc;
+    if (!dust_unit(doff, nd, 2, g, k, loc)) return;
+    const View32& w = V[k];
+    Scalars* sc = w.d64.sc;
+    const int i = NPAD + loc % w.xres, j = NPAD + loc / w.xres;
+    const float* b = w.dbuf[in];
+    DR Q = dload(w, b, i, j);
+    if (!sc->done) {
+        const float dtf = (float)sc->dt;
+        const size_t fp = (size_t)(w.xres + 1) * (w.yres + 1);
+        const size_t m0 = (size_t)(j - NPAD) * (w.xres + 1) + (i - NPAD), m1 = m0 + (w.xres + 1);
+        const float f = dtf * w.y(Y_IYV)[j] * w.x(X_IRAD)[i];
+        const DR P = dload(w, b, i, j - 1);
+        const float F0 = w.dflux[m0], F1 = w.dflux[m1];
+        const float DS = (F0 - F1) * f;
+        const float Dv = ((w.dflux[fp + m0] - F0 * (Q.v - P.v)) - w.dflux[fp + m1]) * f;
+        const float Du = ((w.dflux[2 * fp + m0] - F0 * (Q.u - P.u)) - w.dflux[2 * fp + m1]) * f;
+        const float Sc = w.x(X_DSBG)[i] + Q.S;
+        const float Sn = Sc + DS;
+        const float rmin = fmaxf(Sc * 1.0e-10f, w.dust_rmin);
+        if (Sn < rmin) {
+            Q.S = rmin - w.x(X_DSBG)[i];
+        } else {
+            const float iS = 1.0f / Sn;
+            Q.S += DS;
+            Q.v += Dv * iS;
+            Q.u += Du * iS;
+        }
+        if (!(Sn > 0.0f)) atomicOr(&sc->err, 1 << PG_ERR_NAN);
+    }
+    dstore(w, w.dbuf[in ^ 1], i, j, Q);
+}
+
+// Drag of the dust towards the gas in a half-kick (sweeps.cu:626-707, the
+// exponential integrator with t_s = St h / (c_s Sigma), dust.cu:1-4) in
+// residual form.  gu, gv: the gas residuals the drag relaxes to at the start;
+// with mdt != 0 the forces are re-evaluated at the mdt-predicted dust velocity
+// and towards the mdt-predicted gas velocity (tu, tv).  gx, gy: planet gravity.
+__device__ __forceinline__ void dust_drag32(const View32& w, int i, float Sg, float gu, float gv, float tu, float tv,
+                                            float gx, float gy, float mdt, float dt, DR& D) {
+    const float ts = w.st_h / (w.x(X_CS0)[i] * Sg);
+    const float ir = w.x(X_IRAD)[i], dabg = w.x(X_DABG)[i], dv2r = w.x(X_DV2R)[i];
+    const float dgu = w.x(X_DGU)[i], dgv = w.x(X_DGV)[i];
+    float vd = D.v;  // dust v_phi residual entering the curvature term
+    float ru = gu, rv = gv;
+    if (mdt != 0.0f) {
+        const float dtm = -expm1f(-mdt / ts);
+        vd = D.v + dtm * ((dgv + gv - D.v) + ts * gy);
+        ru = tu;
+        rv = tv;
+    }
+    const float dtau = -expm1f(-dt / ts);
+    const float fx = (dgu + ru - D.u) + ts * (dabg + (dv2r + vd * ir) * vd + gx);
+    const float fy = (dgv + rv - D.v) + ts * gy;
+    D.u += dtau * fx;
+    D.v += dtau * fy;
+}
+
 // ============================================================ radial sweep
 __global__ void __launch_bounds__(SWT) k32_sweep_x(const View32* __restrict__ V, const int* __restrict__ first,
                                                    int nd, int ntiles, int in) {
@@ -676,6 +1048,9 @@ __global__ void __launch_bounds__(STT) k32_kick1(const View32* __restrict__ V, c
             const int c = y * SB_W + x;
             const float dS0 = T[c];
             float du = T[SPL + c], dv = T[2 * SPL + c];
+            const float gu = du, gv = dv;  // the gas cell the dust drag relaxes to
+            DR D{0.0f, 0.0f, 0.0f};
+            if (w.dust) D = dload(w, w.dbuf[in], i, j);
             if (!done) {
                 float vx = 0.0f, vy = 0.0f;
                 if (w.visc) {
@@ -697,8 +1072,10 @@ __global__ void __launch_bounds__(STT) k32_kick1(const View32* __restrict__ V, c
                 float gx, gy;
                 gravity32(w, i, j, 0, gx, gy);
                 kick32(w, i, dS0, du, dv, vx, vy, gx, gy, 0.0f, hdt, w.visc != 0);
+                if (w.dust) dust_drag32(w, i, w.x(X_SBG)[i] + dS0, gu, gv, 0.0f, 0.0f, gx, gy, 0.0f, hdt, D);
             }
             emit32(w, w.buf[in ^ 1], i, j, dS0, du, dv);
+            if (w.dust) dstore(w, w.dbuf[in ^ 1], i, j, D);
         }
         __syncthreads();
     }
@@ -784,11 +1161,23 @@ __global__ void __launch_bounds__(STT) k32_kick2(const View32* __restrict__ V, c
                 const int x = hx + NPAD, y = hy + 1;
                 const int c = y * SB_W + x;
                 float dS = T[c], du = T[SPL + c], dv = T[2 * SPL + c];
+                DR D{0.0f, 0.0f, 0.0f};
+                if (w.dust) D = dload(w, w.dbuf[in], i, j);
                 if (!done) {
                     float vx = 0.0f, vy = 0.0f;
                     if (visc) stress32(w, tp, x, y, i, j, vx, vy);
                     float gx, gy;
                     gravity32(w, i, j, 1, gx, gy);
+                    if (w.dust) {
+                        // the gas velocity predicted over mdt (sweeps.cu:679-687), towards which
+                        // the dust's corrector relaxes
+                        const float iS = visc ? 1.0f / (w.x(X_SBG)[i] + dS) : 0.0f;
+                        const float ir = w.x(X_IRAD)[i];
+                        const float fx0 = w.x(X_ABG)[i] + (w.x(X_V2R)[i] + dv * ir) * dv + vx * iS;
+                        const float tu = du + fx0 * hdt + gx * hdt, tv = dv + vy * iS * hdt + gy * hdt;
+                        dust_drag32(w, i, w.x(X_SBG)[i] + dS, du, dv, tu, tv, gx, gy, hdt, hdt, D);
+                        vmax = fmax(vmax, drate64(w, i, j, D.u, D.v));
+                    }
                     kick32(w, i, dS, du, dv, vx, vy, gx, gy, hdt, hdt, visc);
                     if (w.kill) {
                         // killwave (killwave.cu:48-100): relax towards init_C, i.e. residuals towards 0
@@ -809,6 +1198,7 @@ __global__ void __launch_bounds__(STT) k32_kick2(const View32* __restrict__ V, c
                     vmax = fmax(vmax, rate64(w, i, j, du, dv));
                 }
                 emit32(w, w.buf[in ^ 1], i, j, dS, du, dv);
+                if (w.dust) dstore(w, w.dbuf[in ^ 1], i, j, D);
             }
             __syncthreads();
         }
@@ -871,8 +1261,32 @@ __global__ void k32_cfl(const View32* __restrict__ V, int b) {
         const int i = NPAD + (int)(m % w.xres), j = NPAD + (int)(m / w.xres);
         const size_t c = (size_t)j * w.pitch + i;
         vmax = fmax(vmax, rate64(w, i, j, buf[pl + c], buf[2 * pl + c]));
+        if (w.dust) vmax = fmax(vmax, drate64(w, i, j, w.dbuf[b][pl + c], w.dbuf[b][2 * pl + c]));
     }
     block_max_to<256>(&w.d64.sc->vmax_bits, vmax);
+}
+
+// dust (absolute FP64 interior arrays) <-> residual planes against init_CD
+__global__ void k32_dfill(const View32* __restrict__ V, int b, const double* r, const double* u, const double* v) {
+    const View32& w = *V;
+    const long long n = (long long)w.xres * w.yres;
+    for (long long m = blockIdx.x * (long long)blockDim.x + threadIdx.x; m < n; m += (long long)gridDim.x * blockDim.x) {
+        const int i = NPAD + (int)(m % w.xres), j = NPAD + (int)(m / w.xres);
+        const double* I = w.d64.initd + 4 * i;
+        dstore(w, w.dbuf[b], i, j, DR{(float)(r[m] - I[0]), (float)(u[m] - I[1]), (float)(v[m] - I[2])});
+    }
+}
+__global__ void k32_dextract(const View32* __restrict__ V, int b, double* r, double* u, double* v) {
+    const View32& w = *V;
+    const long long n = (long long)w.xres * w.yres;
+    for (long long m = blockIdx.x * (long long)blockDim.x + threadIdx.x; m < n; m += (long long)gridDim.x * blockDim.x) {
+        const int i = NPAD + (int)(m % w.xres), j = NPAD + (int)(m / w.xres);
+        const double* I = w.d64.initd + 4 * i;
+        const DR c = dload(w, w.dbuf[b], i, j);
+        r[m] = I[0] + (double)c.S;
+        u[m] = I[1] + (double)c.u;
+        v[m] = I[2] + (double)c.v;
+    }
 }
 
 // Host state (FP64 interior arrays) -> residual planes with their azimuthal images.
@@ -1038,6 +1452,24 @@ __global__ void k32_init_tables(const View32 w, float* tx, float* ty, double* cs
             vb[6] = (float)(d.initx[5 * (i + 1)] * d.nux[i + 1] - d.initx[5 * (i - 1)] * d.nux[i - 1]);
         }
         for (int m = 0; m < 7; ++m) X(X_VBG + m)[i] = vb[m];
+        if (d.initd) {
+            const double* D = d.initd + 4 * i;
+            X(X_DSBG)[i] = (float)D[0];
+            X(X_DUBG)[i] = (float)D[1];
+            X(X_DVBG)[i] = (float)D[2];
+            X(X_DEPS)[i] = (float)(D[2] - d.radx[i] * d.frame_omega - d.rot[i]);
+            X(X_DABG)[i] = (float)(D[2] * D[2] * d.irad[i] + d.gstar[i]);
+            X(X_DV2R)[i] = (float)(2.0 * D[2] * d.irad[i]);
+            X(X_DGU)[i] = (float)(I[2] - D[1]);
+            X(X_DGV)[i] = (float)(I[3] - D[2]);
+            for (int kk = 0; kk < 4; ++kk) {
+                const int ik = min(max(i + offs[kk], 0), w.xarr - 1);
+                const double* E = d.initd + 4 * ik;
+                X(X_DDBG + kk)[i] = (float)(E[0] - D[0]);
+                X(X_DDBG + 4 + kk)[i] = (float)(E[1] - D[1]);
+                X(X_DDBG + 8 + kk)[i] = (float)(d.radx[ik] * E[2] - d.radx[i] * D[2]);
+            }
+        }
         const double* kt = d.killx + 4 * i;
         X(X_KILL + 0)[i] = (float)kt[0];
         X(X_KILL + 1)[i] = kt[1] > 0.0 ? (float)(1.0 / kt[1]) : 0.0f;
@@ -1129,6 +1561,29 @@ void launch_pass32(int pass, const View32* V, const int* first, int nd, const in
     }
 }
 void launch_cfl32(const View32* Vk, int b, cudaStream_t s) { k32_cfl<<<592, 256, 0, s>>>(Vk, b); }
+// the dust part of pass 1 (radial sweep), 2 (azimuthal sweep), 3 (advection);
+// counts: radial faces, azimuthal faces, cells of all dust disks
+void launch_dust_pass32(int pass, const View32* V, const int* doff, int nd, const long long* counts, int in,
+                        cudaStream_t s) {
+    auto grid = [](long long n) { return (unsigned)((n + 255) / 256); };
+    if (counts[2] == 0) return;
+    if (pass == 1) {
+        k32d_faces<0><<<grid(counts[0]), 256, 0, s>>>(V, doff, nd, in);
+        k32d_update<0><<<grid(counts[2]), 256, 0, s>>>(V, doff, nd, in);
+    } else if (pass == 2) {
+        k32d_faces<1><<<grid(counts[1]), 256, 0, s>>>(V, doff, nd, in);
+        k32d_update<1><<<grid(counts[2]), 256, 0, s>>>(V, doff, nd, in);
+    } else if (pass == 3) {
+        k32d_adv_faces<<<grid(counts[1]), 256, 0, s>>>(V, doff, nd, in);
+        k32d_adv_update<<<grid(counts[2]), 256, 0, s>>>(V, doff, nd, in);
+    }
+}
+void launch_dfill32(const View32* Vk, int b, const double* r, const double* u, const double* v, cudaStream_t s) {
+    k32_dfill<<<592, 256, 0, s>>>(Vk, b, r, u, v);
+}
+void launch_dextract32(const View32* Vk, int b, double* r, double* u, double* v, cudaStream_t s) {
+    k32_dextract<<<592, 256, 0, s>>>(Vk, b, r, u, v);
+}
 void launch_fill32(const View32* Vk, int b, const double* r, const double* u, const double* v, cudaStream_t s) {
     k32_fill<<<1184, 256, 0, s>>>(Vk, b, r, u, v);
 }

@@ -51,7 +51,17 @@ enum XSlot {
     X_VISX = 36,  // 5 viscous-stencil reciprocals per i
     X_VBG = 41,   // 7 per i: background viscous force coefficients Ax Bx Cx Ay By Cy, and d(Sigma_0 nu) across i
     X_KILL = 48,  // 4 per i: damping ramp and 1/tau, inner then outer (1/tau = 0: no damping)
-    X_NSLOT = 52
+    // dust (dust_flag): the background is init_CD (src/init/init.cu:351-454)
+    X_DSBG = 52,  // Sigma_d0
+    X_DUBG = 53,  // v_r,d0 (the drift)
+    X_DVBG = 54,  // v_phi,d0
+    X_DEPS = 55,  // v_phi,d0 - orb_rot - r Omega_frame
+    X_DABG = 56,  // v_phi,d0^2/r + star gravity
+    X_DV2R = 57,  // 2 v_phi,d0 / r
+    X_DGU = 58,   // v_r0 - v_r,d0 (gas minus dust background)
+    X_DGV = 59,   // v_phi0 - v_phi,d0
+    X_DDBG = 60,  // 12 per i: background differences at offsets -2,-1,+1,+2 of Sigma_d0, v_r,d0, r v_phi,d0
+    X_NSLOT = 72
 };
 enum YSlot {
     Y_IDY = 0,   // 1/(ya[j+1]-ya[j])
@@ -81,6 +91,13 @@ struct View32 {
     float* trig;
     const double* cs64;       // sqrt(gam cs2) per radius, FP64 (CFL rate)
     DiskView d64;             // FP64 grid, tables, orbital-advection arrays, scalars
+    // dust_flag: residual planes {dSigma_d, dv_r,d, dv_phi,d} against init_CD, no ghost
+    // images (radial ghosts: zero residuals; rows wrap), and face-flux scratch
+    float* dbuf[2];
+    float* dflux;             // 3 planes of (xres + 1) * (yres + 1) faces
+    int dust;
+    float st_h;               // Stokes number times h/r: t_s = st_h / (c_s Sigma) (dust.cu:1-4)
+    float dust_rmin;          // D_G_ratio * smallr
     __device__ __forceinline__ const float* x(int slot) const { return tx + (size_t)slot * xn; }
     __device__ __forceinline__ const float* y(int slot) const { return ty + (size_t)slot * yn; }
     __device__ __forceinline__ size_t plane() const { return (size_t)pitch * yarr; }

@@ -105,6 +105,10 @@ void launch_time32(const View32* V, int nd, cudaStream_t s);
 void launch_trig32(const View32* V, int nd, int maxn, cudaStream_t s);
 void launch_pass32(int pass, const View32* V, const int* first, int nd, const int* ntiles, int in, cudaStream_t s);
 void launch_cfl32(const View32* Vk, int b, cudaStream_t s);
+void launch_dust_pass32(int pass, const View32* V, const int* doff, int nd, const long long* counts, int in,
+                        cudaStream_t s);
+void launch_dfill32(const View32* Vk, int b, const double* r, const double* u, const double* v, cudaStream_t s);
+void launch_dextract32(const View32* Vk, int b, double* r, double* u, double* v, cudaStream_t s);
 void launch_fill32(const View32* Vk, int b, const double* r, const double* u, const double* v, cudaStream_t s);
 void launch_extract32(const View32* Vk, int b, double* r, double* p, double* u, double* v, cudaStream_t s);
 void launch_totals32(const View32* Vk, int b, double* part, int nblocks, cudaStream_t s);

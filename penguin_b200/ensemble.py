@@ -48,6 +48,17 @@ class Ensemble:
         vv = np.ascontiguousarray(v, dtype=np.float64) if v is not None else None
         check(lib().pg_ens_set_state(self._h, k, t, _dp(r), _dp(u), _dp(vv) if vv is not None else None))
 
+    def set_dust(self, k: int, dust: dict) -> None:
+        """Interior dust r, u, v (yres, xres) of dust_flag member k."""
+        f = {n: np.ascontiguousarray(dust[n], dtype=np.float64) for n in ("r", "u", "v")}
+        check(lib().pg_ens_set_dust(self._h, k, _dp(f["r"]), _dp(f["u"]), _dp(f["v"])))
+
+    def get_dust(self, k: int) -> dict:
+        p = self.params[k]
+        out = {n: np.empty((p.yres, p.xres)) for n in ("r", "u", "v")}
+        check(lib().pg_ens_get_dust(self._h, k, _dp(out["r"]), _dp(out["u"]), _dp(out["v"])))
+        return out
+
     def get_state(self, k: int) -> dict:
         p = self.params[k]
         out = {n: np.empty((p.yres, p.xres)) for n in ("r", "p", "u", "v")}
