@@ -238,9 +238,12 @@ ALGO_BYTES_DUST = {"time": 0, "kick1": 96 + 64, "sweep_x": 80 + 64, "sweep_y": 8
 def measure_dust(local, stream, steps, pk):
     """Gas + one dust fluid, 768x2048, alpha 1e-4, q 3e-4, dust-to-gas 0.01,
     Stokes 0.01 and 0.1, plain FP64 form: `steps` steps each from t = 0."""
+    import numpy as np
+
     from penguin_b200 import initial as I
     from penguin_b200 import params as P
     from penguin_b200.disk import Disk
+    from penguin_b200.ensemble import Ensemble
 
     out = {}
     for st in (0.01, 0.1):
@@ -254,14 +257,36 @@ def measure_dust(local, stream, steps, pk):
         d.check()
         prof = d.profile(20)
         dust = d.get_dust()
+        t_end = d.clock()[0]
+        # the FP32-mixed form of the same disk to the same time: its speed and the
+        # error of the azimuthally averaged dust profile against the FP64 form
+        e = Ensemble([p], device=local, stream=stream.cuda_stream)
+        e.set_state(0, 0.0, I.disk_state(p, seed=SEED_DUST))
+        e.run(3)
+        e.sync()
+        e.set_state(0, 0.0, I.disk_state(p, seed=SEED_DUST))
+        ms32 = timed(stream, lambda: e.run(10 ** 7, t_end))
+        e.check()
+        n32 = e.clock(0)[2]
+        d32 = e.get_dust(0)
+        prof64, prof32 = dust["r"].mean(axis=0), d32["r"].mean(axis=0)
+        g64, g32 = d.get_state()["r"].mean(axis=0), e.get_state(0)["r"].mean(axis=0)
+        fp32 = {"value": p.cells * n32 / (ms32 / 1000.0), "ms_per_step": ms32 / n32, "steps": n32,
+                "dust_profile_l1_vs_fp64": float(np.abs(prof32 - prof64).sum() / np.abs(prof64).sum()),
+                "dust_sigma_l1_vs_fp64": float(np.abs(d32["r"] - dust["r"]).sum() / np.abs(dust["r"]).sum()),
+                "gas_profile_l1_vs_fp64": float(np.abs(g32 - g64).sum() / np.abs(g64).sum()),
+                "t": t_end, "gpu_launches": e.kernels_per_step * n32}
+        e.close()
         out[f"stokes_{st}"] = {
             "value": p.cells * steps / (ms / 1000.0), "ms_per_step": ms / steps, "steps": steps,
             "stage_ms": prof, "roofline": roofline_of(prof, p.cells, ALGO_BYTES_DUST, pk),
             "gpu_launches": d.kernels_per_step * steps,
             "dust_sigma_sum_over_initial": float(dust["r"].sum()) / m0,
+            "fp32_mixed": fp32,
         }
         d.close()
-    return {"workload": "768x2048 gas+dust planet-disk, FP64 form", "dtype": "f64", **out}
+    return {"workload": "768x2048 gas+dust planet-disk, FP64 form and FP32-mixed form to the same time",
+            "dtype": "f64 / f32 (FP64 dt, shift)", **out}
 
 
 SEED_DUST = 1234
