@@ -88,7 +88,7 @@ class ReferenceLoop:
         def dbuf(name, arr=None, size=None, dtype=torch.float64):
             t = torch.zeros(size if size is not None else arr.size, dtype=dtype, device=dev)
             if arr is not None:
-                t.copy_(torch.from_numpy(np.ascontiguousarray(arr)))
+                t.copy_(torch.from_numpy(np.array(arr, copy=True, order="C")))
             self._keep[name] = t
             return t.data_ptr()
 
