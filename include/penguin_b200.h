@@ -46,8 +46,8 @@ typedef struct { double m, a, e, x, y, z, vx, vy, vz, rs; } pg_body;
 
 /*
  * Runtime copy of include/parameters.h (names kept; see penguin_b200/params.py).
- * kill_width_out and the dust block are additions: the reference uses
- * kill_width for both damping zones.
+ * kill_width_out is an addition: the reference uses kill_width for both
+ * damping zones.
  */
 typedef struct {
     int ndim, xres, yres;
@@ -65,6 +65,10 @@ typedef struct {
     double zmin, zmax;
     int dust_flag;
     double stokes, d_g_ratio;
+    /* Newtonian cooling of p/r towards cs^2 (src/solver/cool/cool.cu): cool_flag 0
+       off, 1 t_c = beta_cool r^1.5, 2 t_c = beta_cool / Sigma sqrt(p/Sigma) / h */
+    int cool_flag;
+    double beta_cool;
 } pg_params;
 
 /*

@@ -1333,6 +1333,20 @@ static void star_planet_grav_cyl(double rad, double azi, double z, const orc_bod
  * (dust.cu:1-4) with the exponential integrator of sweeps.cu:655-707.  out may
  * equal in, out_d may equal in_d.
  */
+/* ------------------------------------------------------------- cooling */
+/* Relaxation of the specific energy p/r towards cs^2(x) over dt
+   (src/solver/cool/cool.cu:1-33): t_c = beta r_cyl^1.5 (cool_flag 1) or
+   beta / r sqrt(p/r) / h (cool_flag 2, r the density). */
+static double p_cool(const orc_params* P, double x, double p, double r, double dt)
+{
+    double rad_cyl = (P->geomx == 1) ? x : 1.0;
+    double tc = (P->cool_flag == 1) ? pow(rad_cyl, 1.5) * P->beta_cool
+                                    : P->beta_cool * (1.0 / r) * (sqrt(p / r) / P->sc_h);
+    double e = p / r;
+    double e0 = get_cs2(P, x);
+    return r * (e0 + (e - e0) * exp(-dt / tc));
+}
+
 static void apply_source_terms(orc_state* S, const orc_cell* in, orc_cell* out, const orc_dust* in_d,
                                orc_dust* out_d, double mdt, double dt)
 {
@@ -1384,6 +1398,7 @@ static void apply_source_terms(orc_state* S, const orc_cell* in, orc_cell* out, 
                 T.u = C.u + fx * mdt + gx * mdt;
                 T.v = C.v + fy * mdt + gy * mdt;
                 T.w = C.w + fz * mdt + gz * mdt;
+                if (P->cool_flag > 0) T.p = p_cool(P, x, T.p, T.r, mdt);  /* sweeps.cu:668-670 */
                 if (in_d) {
                     dtau = 1.0 - exp(-mdt / ts);
                     D.u = Q.u + fxd * dtau + gx * ts * dtau;
@@ -1406,7 +1421,7 @@ static void apply_source_terms(orc_state* S, const orc_cell* in, orc_cell* out, 
             o.v = C.v + fy * dt + gy * dt;
             o.w = C.w + fz * dt + gz * dt;
             o.r = in[ind].r;
-            o.p = in[ind].p;
+            o.p = (P->cool_flag > 0) ? p_cool(P, x, in[ind].p, in[ind].r, dt) : in[ind].p;  /* sweeps.cu:695-699 */
             out[ind] = o;
             if (in_d) {
                 orc_dust od;

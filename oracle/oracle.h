@@ -55,6 +55,8 @@ typedef struct {
     double zmin, zmax;        /* only enter through the z grid (2D: unused by the physics) */
     int dust_flag;            /* 1: one pressureless dust fluid (src/solver/dust/dust.cu) */
     double stokes, d_g_ratio; /* Stokes and D_G_ratio of include/parameters.h */
+    int cool_flag;            /* 0 off, 1 t_c = beta r^1.5, 2 t_c = beta / r sqrt(p/r) / h (src/solver/cool/cool.cu) */
+    double beta_cool;
 } orc_params;
 
 typedef struct orc_state orc_state;

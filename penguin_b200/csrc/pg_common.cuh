@@ -77,6 +77,10 @@ struct DiskView {
     double stokes, sc_h;  // Stokes number; h/r (stopping time t_s = Stokes h / (c_s Sigma), dust.cu:1-4)
     double dust_rmin;     // D_G_ratio * smallr: the dust density floor of update_Dust (dust.cu:149-176)
     const double* initd;  // init_CD(xc(i)) (4 per i: r, u, v, w; src/init/init.cu:351-454)
+    // Newtonian cooling (cool_flag, src/solver/cool/cool.cu)
+    int cool;
+    double beta_cool;
+    const double* coolx;  // cool 1: t_c(xc(i)) = beta_cool r_cyl^1.5
     // time average of the gas state over a save interval (ave_flag, src/output/output.cu:250-330)
     Cell* ave;            // null: off
     double ave_T;         // the save interval

@@ -80,10 +80,12 @@ __device__ __forceinline__ DCell update_dust(const DiskView& d, DCell Q, const D
 // Dust part of apply_source_terms (sweeps.cu:578-595, 626-707, geomx 1 or 0,
 // 2D): t_s from the gas cell C (T.r = C.r, T.p = C.p); the forces towards the gas
 // velocity T (C itself when mdt = 0, else the gas velocity the kick predicted
-// over mdt: Tu, Tv), re-evaluated at the dust velocity predicted over mdt.
-__device__ __forceinline__ DCell dust_kick(const DiskView& d, const Cell& C, double Tu, double Tv, const DCell& Q,
-                                           double gx, double gy, double gz, double ix, double mdt, double dt) {
-    const double ts = d.stokes / (sqrt(d.gam * C.p / C.r) / d.sc_h) / C.r;
+// over mdt: Tu, Tv), re-evaluated at the dust velocity predicted over mdt with
+// t_s at the predicted pressure Tp (C.p unless cooling changed it).
+__device__ __forceinline__ DCell dust_kick(const DiskView& d, const Cell& C, double Tu, double Tv, double Tp,
+                                           const DCell& Q, double gx, double gy, double gz, double ix, double mdt,
+                                           double dt) {
+    double ts = d.stokes / (sqrt(d.gam * C.p / C.r) / d.sc_h) / C.r;
     double fxd = (d.geomx == 1) ? Q.v * Q.v * ix : 0.0;
     fxd = fxd * ts + C.u - Q.u;
     double fyd = 0.0 * ts + C.v - Q.v;
@@ -92,6 +94,7 @@ __device__ __forceinline__ DCell dust_kick(const DiskView& d, const Cell& C, dou
         DCell D;
         D.u = Q.u + fxd * dtau + gx * ts * dtau;
         D.v = Q.v + fyd * dtau + gy * ts * dtau;
+        ts = d.stokes / (sqrt(d.gam * Tp / C.r) / d.sc_h) / C.r;  // at the predicted (cooled) pressure
         fxd = (d.geomx == 1) ? D.v * D.v * ix : 0.0;
         fxd = fxd * ts + Tu - Q.u;
         fyd = 0.0 * ts + Tv - Q.v;

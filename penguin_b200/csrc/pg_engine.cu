@@ -282,6 +282,8 @@ static pg_status check_params(const pg_params* P) {
         if (P->init_flag != 2) return fail(PG_ERR_CONFIG, "dust needs init_flag 2 (init_CD)");
         if (!(P->stokes > 0.0)) return fail(PG_ERR_CONFIG, "dust needs Stokes > 0");
     }
+    if (P->cool_flag < 0 || P->cool_flag > 2) return fail(PG_ERR_CONFIG, "cool_flag must be 0, 1 or 2");
+    if (P->cool_flag && !(P->beta_cool > 0.0)) return fail(PG_ERR_CONFIG, "cooling needs beta_cool > 0");
     if (P->gridx < 0 || P->gridx > 1 || P->gridy != 0) return fail(PG_ERR_CONFIG, "grids: x linear/log, y linear");
     if (P->gridx == 1 && !(P->xmin > 0.0)) return fail(PG_ERR_CONFIG, "log grid needs xmin > 0");
     return PG_OK;
@@ -380,9 +382,9 @@ static pg_status engine_setup(Engine& E, const double* dev_xa, const double* dev
     }
     // tables: wx[6 xarr] wy[6 yarr] | radx cs2x nux initx(5) killx(4) idx_x ixv irad gstar visx(5) [xarr each]
     //         | ycraw ycj idx_y iyv visy(4) [yarr each] | trig [4 yarr + 2]
-    //         | initd(4) [xarr] with dust
+    //         | initd(4) [xarr] with dust | coolx [xarr] with cool_flag 1
     const size_t ntab = 6 * (size_t)xarr + 6 * (size_t)yarr + 21 * (size_t)xarr + 8 * (size_t)yarr + 4 * (size_t)yarr + 2 +
-                        (P.dust_flag ? 4 * (size_t)xarr : 0);
+                        (P.dust_flag ? 4 * (size_t)xarr : 0) + (P.cool_flag == 1 ? (size_t)xarr : 0);
     PG_CUDA(cudaMalloc(&E.tab, sizeof(double) * ntab));
     std::vector<double> wx(6 * xarr), wy(6 * yarr);
     recon_weights(P.geomx, xa.data(), xarr, wx.data());
@@ -453,6 +455,9 @@ static pg_status engine_setup(Engine& E, const double* dev_xa, const double* dev
                                 cudaMemcpyHostToDevice, E.stream));
         PG_CUDA(cudaStreamSynchronize(E.stream));
     }
+    d.cool = P.cool_flag;
+    d.beta_cool = P.beta_cool;
+    d.coolx = (P.cool_flag == 1) ? d.trig + 4 * (size_t)yarr + 2 + (P.dust_flag ? 4 * (size_t)xarr : 0) : nullptr;
     d.rot = E.rot;
     d.res = E.res;
     d.inc = E.inc;

@@ -85,6 +85,17 @@ __device__ __forceinline__ Grav gravity(const DiskView& d, int i, double rad, do
 // One cell of apply_source_terms (src/solver/sweeps.cu:597-711): curvature,
 // gravity and viscous acceleration; with mdt != 0 the forces are re-evaluated
 // at the mdt-predicted velocities (sweeps.cu:663-687).
+
+// Newtonian cooling of the pressure over dt (src/solver/cool/cool.cu:1-33): the
+// specific energy p/r relaxes towards cs^2(xc) with t_c = beta r_cyl^1.5
+// (cool 1, tabulated) or beta / r sqrt(p/r) / h (cool 2, r the density).
+__device__ __forceinline__ double p_cool(const DiskView& d, int i, double p, double r, double dt) {
+    const double tc = (d.cool == 1) ? d.coolx[i] : d.beta_cool * (1.0 / r) * (sqrt(p / r) / d.sc_h);
+    const double e = p / r;
+    const double e0 = d.cs2x[i];
+    return r * (e0 + (e - e0) * exp(-dt / tc));
+}
+
 template <bool VISC>
 __device__ __forceinline__ Cell kick(const DiskView& d, const Cell& C, double ix, const Grav& g, double vx,
                                      double vy, double mdt, double dt, double* Tu = nullptr, double* Tv = nullptr) {
@@ -578,11 +589,12 @@ __global__ void __launch_bounds__(ST_THREADS)
             }
             const double* tr = d.trig + 4 * j;
             const Grav g = gravity(d, i, d.radx[i], tr[0], tr[1], d.trig[4 * d.yarr], sc->planet_cur);
-            const Cell Q = kick<VISC>(d, C, d.irad[i], g, vx, vy, 0.0, hdt);
+            Cell Q = kick<VISC>(d, C, d.irad[i], g, vx, vy, 0.0, hdt);
+            if (d.cool) Q.p = p_cool(d, i, C.p, C.r, hdt);  // sweeps.cu:695-699
             emit(d, out, i, j, Q);
             if (d.ave) accumulate_average(d, i, j, C, hdt);  // averaging(dev, 0.5 dt, T) before solve
             if (din) {  // dust half-kick: drag towards the gas cell C (sweeps.cu:626-707, mdt = 0)
-                const DCell D = dust_kick(d, C, C.u, C.v, load_dust(din, d.xarr, i, j), g.gx, g.gy, g.gz,
+                const DCell D = dust_kick(d, C, C.u, C.v, C.p, load_dust(din, d.xarr, i, j), g.gx, g.gy, g.gz,
                                           d.irad[i], 0.0, hdt);
                 emit_dust(d, dout, i, j, D);
             }
@@ -690,6 +702,10 @@ __global__ void __launch_bounds__(ST_THREADS)
                 const Grav g = gravity(d, i, d.radx[i], tr[0], tr[1], iplx2, pl);
                 double Tu = C.u, Tv = C.v;
                 Cell Q = kick<VISC>(d, C, d.irad[i], g, vx, vy, hdt, hdt, &Tu, &Tv);
+                // cooling over dt/2; the predictor cools over mdt = dt/2 as well, so Q.p is also
+                // the predicted pressure the dust's second stopping time reads (sweeps.cu:668-699)
+                if (d.cool) Q.p = p_cool(d, i, C.p, C.r, hdt);
+                const double Tp = Q.p;
                 if (d.kill) {
                     // killwave (src/killwave/killwave.cu:48-100): relax towards init_C
                     const double* kt = d.killx + 4 * i;
@@ -710,7 +726,7 @@ __global__ void __launch_bounds__(ST_THREADS)
                 }
                 if (!(Q.r > 0.0)) atomicOr(&sc->err, 1 << PG_ERR_NAN);
                 if (din) {  // dust corrector half-kick towards the predicted gas velocity (sweeps.cu:663-707)
-                    const DCell D = dust_kick(d, C, Tu, Tv, load_dust(din, d.xarr, i, j), g.gx, g.gy, g.gz,
+                    const DCell D = dust_kick(d, C, Tu, Tv, Tp, load_dust(din, d.xarr, i, j), g.gx, g.gy, g.gz,
                                               d.irad[i], hdt, hdt);
                     emit_dust(d, dout, i, j, D);
                     vmax = fmax(vmax, signal_rate(d, Q, i, j, &D));
@@ -828,6 +844,8 @@ __global__ void k_init_tables(const DiskView d, TabArgs a, double* radx, double*
         d_initC(a, x, initx + 5 * k);
         // orb_rot (src/orbit/orbit.cu:57-69)
         if (rot) rot[k] = a.orbadv ? initx[5 * k + 3] - x * a.frame_omega : 0.0;
+        // cooling time of cool_flag 1 (src/solver/cool/cool.cu:1-12, 15-27)
+        if (d.coolx) const_cast<double*>(d.coolx)[k] = pow((a.geomx == 1) ? x : 1.0, 1.5) * d.beta_cool;
         const double d_in = d_h(a, a.xmin) * a.kill_width;
         const double d_out = d_h(a, a.xmax) * a.kill_width_out;
         const double inner = a.xmin + d_in;

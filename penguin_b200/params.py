@@ -63,6 +63,8 @@ class Params:
     dust_flag: int = 0
     Stokes: float = 0.01
     D_G_ratio: float = 0.01
+    cool_flag: int = 0      # 0 off, 1 t_c = beta r^1.5, 2 t_c = beta / Sigma sqrt(p/Sigma) / h
+    beta_cool: float = 0.001
 
     # ----------------------------------------------------------------- sizes
     @property
@@ -99,6 +101,10 @@ class Params:
             raise ValueError("radial boundaries must be 0, 1 or 2")
         if self.n_planet not in (0, 1):
             raise ValueError("n_planet must be 0 or 1")
+        if self.cool_flag not in (0, 1, 2):
+            raise ValueError("cool_flag must be 0, 1 or 2")
+        if self.cool_flag and not self.beta_cool > 0.0:
+            raise ValueError("cooling needs beta_cool > 0")
 
 
 class PGParams(ctypes.Structure):
@@ -122,6 +128,7 @@ class PGParams(ctypes.Structure):
         ("zmin", ctypes.c_double), ("zmax", ctypes.c_double),
         ("dust_flag", ctypes.c_int),
         ("stokes", ctypes.c_double), ("d_g_ratio", ctypes.c_double),
+        ("cool_flag", ctypes.c_int), ("beta_cool", ctypes.c_double),
     ]
 
     @classmethod
@@ -134,7 +141,7 @@ class PGParams(ctypes.Structure):
             p.p_alpha, p.p_beta, p.ss_alpha, p.sc_h, p.planet_radius,
             p.visc_flag, p.OrbAdv_flag, p.kill_flag, p.kill_width, p.kill_width_out,
             p.n_planet, p.planet_mass, p.planet_ecc, p.rs_fac, p.ramp_time, p.zmin, p.zmax,
-            p.dust_flag, p.Stokes, p.D_G_ratio,
+            p.dust_flag, p.Stokes, p.D_G_ratio, p.cool_flag, p.beta_cool,
         )
 
 
@@ -178,6 +185,17 @@ def dust_disk(nr: int = 768, nphi: int = 2048, *, stokes: float = 0.01, q: float
     Stokes number, initial dust-to-gas ratio ``d_g_ratio``, dust velocity from the
     drift solution (init_CD, src/init/init.cu:351-454)."""
     return planet_disk(nr, nphi, q=q, alpha=alpha).replace(dust_flag=1, Stokes=stokes, D_G_ratio=d_g_ratio)
+
+
+def adiabatic_disk(nr: int = 1024, nphi: int = 3072, *, cool_flag: int = 0, beta_cool: float = 0.001,
+                   gam: float = 1.4, internal_e_flag: int = 1, **kw) -> Params:
+    """The planet-disk with an ideal-gas equation of state (EOS_flag 2): p starts
+    at cs^2 Sigma and then evolves with the internal-energy equation (or the total
+    energy with ``internal_e_flag`` 0); optional Newtonian cooling of p/Sigma
+    towards cs^2 (cool_flag 1: t_c = beta r^1.5; 2: t_c = beta / Sigma
+    sqrt(p/Sigma) / h; src/solver/cool/cool.cu)."""
+    return planet_disk(nr, nphi, **kw).replace(EOS_flag=2, gam=gam, internal_e_flag=internal_e_flag,
+                                               cool_flag=cool_flag, beta_cool=beta_cool)
 
 
 def adjoint_disk(nr: int = 256, nphi: int = 768, *, q: float = 5.0e-4, alpha: float = 1.0e-3,

@@ -44,6 +44,11 @@ static const int pgs_dust = 1;
 #else
 static const int pgs_dust = 0;
 #endif
+#if defined(cool_flag) && cool_flag > 0
+static const int pgs_cool = cool_flag;
+#else
+static const int pgs_cool = 0;
+#endif
 #undef ndim
 #undef geomx
 #undef geomy
@@ -54,6 +59,7 @@ static const int pgs_dust = 0;
 #undef visc_flag
 #undef kill_flag
 #undef dust_flag
+#undef cool_flag
 
 #include "penguin_b200.h"
 
@@ -104,6 +110,8 @@ static void pg_shim_configure() {
     P.dust_flag = pgs_dust;
     P.stokes = Stokes;
     P.d_g_ratio = D_G_ratio;
+    P.cool_flag = pgs_cool;
+    P.beta_cool = beta_cool;
     if (pg_configure(&P) != PG_OK) {
         fprintf(stderr, "penguin_b200: %s\n", pg_last_error());
         exit(1);

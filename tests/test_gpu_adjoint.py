@@ -185,3 +185,5 @@ def test_adjoint_rejects_unsupported_disks():
     assert e.value.status == PG_ERR_CONFIG
     with pytest.raises(PGError):
         DiskAdjoint.check_params(P.sod_tube(64))
+    with pytest.raises(PGError):
+        DiskAdjoint.check_params(small_disk().replace(cool_flag=1))
