@@ -69,6 +69,11 @@ typedef struct {
        off, 1 t_c = beta_cool r^1.5, 2 t_c = beta_cool / Sigma sqrt(p/Sigma) / h */
     int cool_flag;
     double beta_cool;
+    /* twobd_flag 1: the star and the planet orbit their barycentre
+       (src/planet/planet.cu:135-175) and pull as inertial point masses; with
+       n_planet 1 (the planet).  Through pg_grid_* the caller's planets array
+       holds the star (planets[0]) and the planet (planets[1]). */
+    int twobd_flag;
 } pg_params;
 
 /*

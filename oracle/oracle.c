@@ -28,6 +28,7 @@ struct orc_state {
     double *orb_rot, *orb_res;
     int *orb_inc;
     orc_body planet;
+    orc_body star;       /* twobd_flag: planets[0] of the reference (planet = planets[1]) */
 };
 
 #define IND(S, i, j) ((i) + (S)->xarr * (j))
@@ -329,13 +330,55 @@ static void orbit_solution(const orc_params* P, orc_body* b, double t)
     b->vy = n * (1.0 + ecosf) * (1.0 + ecosf) / efac / efac / efac;
     b->vz = 0.0;
 }
-/* src/planet/planet.cu:308-317, 319-402 (single planet, twobd_flag 0) */
+/* src/planet/planet.cu:135-175: star and planet on the reduced orbit about their
+   barycentre, in the frame rotating at frame_omega */
+static void two_body_solution(const orc_params* P, orc_body* star, orc_body* planet, double t)
+{
+    double a = star->a, e = star->e;
+    double n = sqrt(1.0 / a / a / a);
+    double efac = sqrt(1.0 - e * e);
+    double B = e / (1.0 + efac);
+    double u = ecc_anomaly(n, e, t);
+    double sinu = sin(u), cosu = cos(u);
+    double f = u + 2.0 * atan(B * sinu / (1.0 - B * cosu));
+    double esinf = sin(f) * e, ecosf = cos(f) * e;
+    double reduced_r = a * efac * efac / (1.0 + ecosf);
+    double reduced_p = f - fmod(P->frame_omega * t, TWOPI) + PI;
+    double mp = ramp_function(t, P->ramp_time, P->planet_mass);
+    star->m = 1.0 / (1.0 + mp);
+    star->x = reduced_r * mp / (1.0 + mp);
+    star->y = fmod(reduced_p + PI, TWOPI);
+    star->z = HPI;
+    star->vx = n * a * esinf / efac * mp / (1.0 + mp);
+    star->vy = n * (1.0 + ecosf) * (1.0 + ecosf) / efac / efac / efac;
+    star->vz = 0.0;
+    planet->m = mp / (1.0 + mp);
+    planet->x = reduced_r * 1.0 / (1.0 + mp);
+    planet->y = reduced_p;
+    planet->z = HPI;
+    planet->vx = n * a * esinf / efac * 1.0 / (1.0 + mp);
+    planet->vy = n * (1.0 + ecosf) * (1.0 + ecosf) / efac / efac / efac;
+    planet->vz = 0.0;
+}
+
+/* evolve_planet (src/planet/planet.cu:291-304) */
+static void evolve_bodies(orc_state* S, double t)
+{
+    if (S->P.n_planet <= 0) return;
+    if (S->P.twobd_flag) two_body_solution(&S->P, &S->star, &S->planet, t);
+    else orbit_solution(&S->P, &S->planet, t);
+}
+
+/* src/planet/planet.cu:308-317, 319-402: one planet, or the star-planet pair of
+   the two-body frame (the star unsmoothed) */
 void orc_init_planet(orc_state* S, double t)
 {
     const orc_params* P = &S->P;
-    S->planet.a = P->planet_radius;
-    S->planet.e = P->planet_ecc;
-    orbit_solution(P, &S->planet, t);
+    S->planet.a = S->star.a = P->planet_radius;
+    S->planet.e = S->star.e = P->planet_ecc;
+    if (P->twobd_flag) two_body_solution(P, &S->star, &S->planet, t);
+    else orbit_solution(P, &S->planet, t);
+    S->star.rs = 0.0;
     if (P->ndim == 2) S->planet.rs = P->rs_fac * P->sc_h * P->planet_radius;
     else S->planet.rs = P->rs_fac * pow(P->planet_mass / 3.0, 1.0 / 3.0) * P->planet_radius;
 }
@@ -1311,6 +1354,20 @@ void orc_viscous_forces(orc_state* S, int which, double* vis_out)
 }
 
 /* ---------------------------------------------------------- source terms */
+/* src/solver/force/forces.cu:89-106 (two-body frame, z = 0): a body pulling as
+   an inertial point mass, no indirect term */
+static void star_planet_grav_cyl_inertial(double rad, double azi, double z, const orc_body* p, double* fx,
+                                          double* fy, double* fz)
+{
+    double sinfac = sin(azi - (p->y + 0.0 * p->vy));
+    double cosfac = cos(azi - (p->y + 0.0 * p->vy));
+    double plm = p->m, plx = p->x;
+    double Rp = sqrt(rad * rad + plx * plx - 2.0 * plx * rad * cosfac + z * z + p->rs * p->rs);
+    double rs_fac = 1.0 / Rp / Rp / Rp;
+    *fx = -plm * (rad - plx * cosfac) * rs_fac;
+    *fy = -plm * plx * sinfac * rs_fac;
+    *fz = -plm * z * rs_fac;
+}
 /* src/solver/force/forces.cu:41-58 (2D: z = 0) */
 static void star_planet_grav_cyl(double rad, double azi, double z, const orc_body* p, double* fx, double* fy, double* fz)
 {
@@ -1325,8 +1382,7 @@ static void star_planet_grav_cyl(double rad, double azi, double z, const orc_bod
 }
 
 /*
- * src/solver/sweeps.cu:555-711 with geomx 0/1, ndim <= 2, twobd_flag 0, no
- * cooling: half-kick of the velocities by curvature, star+planet gravity and
+ * src/solver/sweeps.cu:555-711 with geomx 0/1, ndim <= 2: half-kick of the velocities by curvature, star+planet gravity and
  * the viscous force density; when mdt != 0 the forces are re-evaluated at the
  * mdt-predicted velocities.  With dust (in_d != NULL) the dust velocities relax
  * towards the gas ones over the stopping time t_s = Stokes h / (c_s Sigma)
@@ -1368,7 +1424,17 @@ static void apply_source_terms(orc_state* S, const orc_cell* in, orc_cell* out, 
             double y = (P->ndim > 1) ? yc(S, j) + S->orb_rot[i] * 0.0 : 0.0;
             double z = 0.0;
             double gx = 0.0, gy = 0.0, gz = 0.0, fx, fy = 0.0, fz = 0.0;
-            if (P->geomx == 1) {
+            if (P->geomx == 1 && P->twobd_flag) {
+                /* get_gx/get_gy/get_gz with twobd_flag 1 (forces.cu:194-201, 243-270, 285-292) */
+                const orc_body* B[2] = {&S->star, &S->planet};
+                for (int m = 0; m < 2; m++) {
+                    double tx, ty, tz;
+                    star_planet_grav_cyl_inertial(x, y, z, B[m], &tx, &ty, &tz);
+                    gx += tx;
+                    gy += ty;
+                    gz += tz;
+                }
+            } else if (P->geomx == 1) {
                 double dis = sqrt(x * x + z * z);
                 double tx, ty, tz;
                 gx = -x / dis / dis / dis;
@@ -1526,7 +1592,9 @@ double orc_torque(const orc_state* S)
             const double rad = 0.5 * (S->xa[i + 1] + S->xa[i]);
             const double Rp = sqrt(rad * rad + p->x * p->x - 2.0 * p->x * rad * cosfac + p->rs * p->rs);
             const double rs_fac = 1.0 / Rp / Rp / Rp;
-            const double gy = -p->m * p->x * sinfac * rs_fac + p->m * sinfac / p->x / p->x;
+            /* output_gy (src/output/forces.cu:103-127): inertial in the two-body frame */
+            const double gy = P->twobd_flag ? -p->m * p->x * sinfac * rs_fac
+                                            : -p->m * p->x * sinfac * rs_fac + p->m * sinfac / p->x / p->x;
             const double dv = 0.5 * (S->xa[i + 1] * S->xa[i + 1] - S->xa[i] * S->xa[i]) * (S->ya[j + 1] - S->ya[j]);
             const double y = rad * gy * (S->C[IND(S, i, j)].r * dv) - comp;
             const double t = sum + y;
@@ -1571,7 +1639,7 @@ void orc_solve(orc_state* S, double t, double dt)
         advecty(S, dt);
         if (S->CD) advecty_dust(S, dt);
     }
-    if (P->n_planet > 0) orbit_solution(P, &S->planet, t + dt);
+    evolve_bodies(S, t + dt);
     if (P->visc_flag && P->ndim == 2) {
         apply_source_terms(S, S->C, S->T, S->CD, S->TD, hdt, hdt);
         orc_boundy(S, 1);
@@ -1641,7 +1709,7 @@ int orc_solve_stages(orc_state* S, double t, double dt, orc_cell* out, orc_dust*
             DUMP();
         }
     }
-    if (P->n_planet > 0) orbit_solution(P, &S->planet, t + dt);
+    evolve_bodies(S, t + dt);
     if (P->visc_flag && P->ndim == 2) {
         apply_source_terms(S, S->C, S->T, S->CD, S->TD, hdt, hdt);
         orc_boundy(S, 1);

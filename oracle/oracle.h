@@ -57,6 +57,7 @@ typedef struct {
     double stokes, d_g_ratio; /* Stokes and D_G_ratio of include/parameters.h */
     int cool_flag;            /* 0 off, 1 t_c = beta r^1.5, 2 t_c = beta / r sqrt(p/r) / h (src/solver/cool/cool.cu) */
     double beta_cool;
+    int twobd_flag;           /* 1: star and planet orbit their barycentre (src/planet/planet.cu:135-175) */
 } orc_params;
 
 typedef struct orc_state orc_state;

@@ -35,6 +35,7 @@ class OrcParams(ctypes.Structure):
         ("zmin", ctypes.c_double), ("zmax", ctypes.c_double),
         ("dust_flag", ctypes.c_int), ("stokes", ctypes.c_double), ("d_g_ratio", ctypes.c_double),
         ("cool_flag", ctypes.c_int), ("beta_cool", ctypes.c_double),
+        ("twobd_flag", ctypes.c_int),
     ]
 
     @classmethod
@@ -46,7 +47,7 @@ class OrcParams(ctypes.Structure):
             p.p_alpha, p.p_beta, p.ss_alpha, p.sc_h, p.planet_radius,
             p.visc_flag, p.OrbAdv_flag, p.kill_flag, p.kill_width, p.kill_width_out,
             p.n_planet, p.planet_mass, p.planet_ecc, p.rs_fac, p.ramp_time, p.zmin, p.zmax,
-            p.dust_flag, p.Stokes, p.D_G_ratio, p.cool_flag, p.beta_cool,
+            p.dust_flag, p.Stokes, p.D_G_ratio, p.cool_flag, p.beta_cool, p.twobd_flag,
         )
 
 

@@ -1185,6 +1185,7 @@ pg_status pg_adj_check_params(const pg_params* P) {
     if (P->kill_flag) return adj_fail(PG_ERR_CONFIG, "the adjoint does not differentiate wave damping (kill_flag 0)");
     if (P->dust_flag) return adj_fail(PG_ERR_CONFIG, "the adjoint covers the gas only");
     if (P->cool_flag) return adj_fail(PG_ERR_CONFIG, "the adjoint does not differentiate cooling (cool_flag 0)");
+    if (P->twobd_flag) return adj_fail(PG_ERR_CONFIG, "the adjoint covers a fixed star (twobd_flag 0)");
     if (P->n_planet > 0 && P->planet_ecc != 0.0)
         return adj_fail(PG_ERR_CONFIG, "the adjoint covers a planet on a circular orbit");
     if (!(P->sc_h > 0.0)) return adj_fail(PG_ERR_CONFIG, "h/r must be positive");

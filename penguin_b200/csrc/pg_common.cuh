@@ -35,6 +35,8 @@ struct Scalars {
     pg_body planet_cur;   // planet used by the first half-kick (from the previous step)
     pg_body planet_next;  // planet at t+dt (src/solver/solve.cu:264)
     double dt_hold;       // the CFL step a clip at end_time replaced (main.cu:333-338 old_dt)
+    pg_body star_cur;     // two-body frame (twobd_flag): the star of the first half-kick
+    pg_body star_next;    // ... and at t+dt (planets[0] of the reference; the planet is planets[1])
 };
 
 // Everything a kernel needs to know about one disk (passed by value).
@@ -81,6 +83,10 @@ struct DiskView {
     int cool;
     double beta_cool;
     const double* coolx;  // cool 1: t_c(xc(i)) = beta_cool r_cyl^1.5
+    // two-body frame (twobd_flag, src/planet/planet.cu:135-175): star and planet
+    // orbit their barycentre; gravity of both as point masses, no indirect term
+    int twobd;
+    double* strig;        // per row: sin, cos of (azimuth - star y) for star_cur, then star_next
     // time average of the gas state over a save interval (ave_flag, src/output/output.cu:250-330)
     Cell* ave;            // null: off
     double ave_T;         // the save interval

@@ -283,6 +283,9 @@ static pg_status check_params(const pg_params* P) {
         if (!(P->stokes > 0.0)) return fail(PG_ERR_CONFIG, "dust needs Stokes > 0");
     }
     if (P->cool_flag < 0 || P->cool_flag > 2) return fail(PG_ERR_CONFIG, "cool_flag must be 0, 1 or 2");
+    if (P->twobd_flag != 0 && P->twobd_flag != 1) return fail(PG_ERR_CONFIG, "twobd_flag must be 0 or 1");
+    if (P->twobd_flag && (P->ndim != 2 || P->geomx != 1 || P->n_planet != 1))
+        return fail(PG_ERR_CONFIG, "the two-body frame needs a 2D polar disk with n_planet 1 (the planet; the star is the second body)");
     if (P->cool_flag && !(P->beta_cool > 0.0)) return fail(PG_ERR_CONFIG, "cooling needs beta_cool > 0");
     if (P->gridx < 0 || P->gridx > 1 || P->gridy != 0) return fail(PG_ERR_CONFIG, "grids: x linear/log, y linear");
     if (P->gridx == 1 && !(P->xmin > 0.0)) return fail(PG_ERR_CONFIG, "log grid needs xmin > 0");
@@ -382,9 +385,10 @@ static pg_status engine_setup(Engine& E, const double* dev_xa, const double* dev
     }
     // tables: wx[6 xarr] wy[6 yarr] | radx cs2x nux initx(5) killx(4) idx_x ixv irad gstar visx(5) [xarr each]
     //         | ycraw ycj idx_y iyv visy(4) [yarr each] | trig [4 yarr + 2]
-    //         | initd(4) [xarr] with dust | coolx [xarr] with cool_flag 1
+    //         | initd(4) [xarr] with dust | coolx [xarr] with cool_flag 1 | strig [4 yarr] with twobd_flag
     const size_t ntab = 6 * (size_t)xarr + 6 * (size_t)yarr + 21 * (size_t)xarr + 8 * (size_t)yarr + 4 * (size_t)yarr + 2 +
-                        (P.dust_flag ? 4 * (size_t)xarr : 0) + (P.cool_flag == 1 ? (size_t)xarr : 0);
+                        (P.dust_flag ? 4 * (size_t)xarr : 0) + (P.cool_flag == 1 ? (size_t)xarr : 0) +
+                        (P.twobd_flag ? 4 * (size_t)yarr : 0);
     PG_CUDA(cudaMalloc(&E.tab, sizeof(double) * ntab));
     std::vector<double> wx(6 * xarr), wy(6 * yarr);
     recon_weights(P.geomx, xa.data(), xarr, wx.data());
@@ -458,6 +462,11 @@ static pg_status engine_setup(Engine& E, const double* dev_xa, const double* dev
     d.cool = P.cool_flag;
     d.beta_cool = P.beta_cool;
     d.coolx = (P.cool_flag == 1) ? d.trig + 4 * (size_t)yarr + 2 + (P.dust_flag ? 4 * (size_t)xarr : 0) : nullptr;
+    d.twobd = P.twobd_flag;
+    d.strig = P.twobd_flag ? d.trig + 4 * (size_t)yarr + 2 + (P.dust_flag ? 4 * (size_t)xarr : 0) +
+                                 (P.cool_flag == 1 ? (size_t)xarr : 0)
+                           : nullptr;
+    if (d.strig) PG_CUDA(cudaMemsetAsync(d.strig, 0, sizeof(double) * 4 * (size_t)yarr, E.stream));
     d.rot = E.rot;
     d.res = E.res;
     d.inc = E.inc;
@@ -653,7 +662,16 @@ __global__ void k_extract(const DiskView d, const Cell* buf, double* r, double* 
     }
 }
 
-__global__ void k_grid_planet_in(Scalars* sc, const pg_body* planets) { sc->planet_next = planets[0]; }
+// the caller's planets array: the planet, or the star (planets[0]) and the planet
+// (planets[1]) of the two-body frame
+__global__ void k_grid_planet_in(Scalars* sc, const pg_body* planets, int twobd) {
+    if (twobd) {
+        sc->star_next = planets[0];
+        sc->planet_next = planets[1];
+    } else {
+        sc->planet_next = planets[0];
+    }
+}
 
 // write_check_point's fields (src/output/output.cu:125-180): interior r, p, u,
 // v (2D) of the gas source, then with dust r, u, v (2D), w (2D); x fastest
@@ -680,7 +698,14 @@ __global__ void k_snapshot_planes(const DiskView d, const Cell* gas, const pg_du
         }
     }
 }
-__global__ void k_grid_planet_out(const Scalars* sc, pg_body* planets) { planets[0] = sc->planet_next; }
+__global__ void k_grid_planet_out(const Scalars* sc, pg_body* planets, int twobd) {
+    if (twobd) {
+        planets[0] = sc->star_next;
+        planets[1] = sc->planet_next;
+    } else {
+        planets[0] = sc->planet_next;
+    }
+}
 
 }  // namespace pg
 
@@ -1539,10 +1564,12 @@ pg_status pg_grid_solve(pg_grid* dev, double time, double dt) {
         }
         launch_dust_images(E->view, dev->CD, E->stream);
     }
-    if (E->view.nplanet > 0 && dev->planets) k_grid_planet_in<<<1, 1, 0, E->stream>>>(E->sc, dev->planets);
+    if (E->view.nplanet > 0 && dev->planets)
+        k_grid_planet_in<<<1, 1, 0, E->stream>>>(E->sc, dev->planets, E->view.twobd);
     launch_set_time(E->view, time, dt, E->stream);
     if ((s = enqueue_stages(*E)) != PG_OK) return s;
-    if (E->view.nplanet > 0 && dev->planets) k_grid_planet_out<<<1, 1, 0, E->stream>>>(E->sc, dev->planets);
+    if (E->view.nplanet > 0 && dev->planets)
+        k_grid_planet_out<<<1, 1, 0, E->stream>>>(E->sc, dev->planets, E->view.twobd);
     PG_CUDA(cudaGetLastError());
     if (E->cur == 1) {  // newest state in T: swap like the reference (src/solver/sweeps.cu:353-355)
         pg_cell* t = dev->C;

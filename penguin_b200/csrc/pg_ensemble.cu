@@ -48,6 +48,7 @@ pg_status check32(const pg_params* P, int k) {
     if (P->geomx != 1 || P->geomy != 3) return ens_fail(PG_ERR_CONFIG, pre + "a polar grid (geomx 1, geomy 3)");
     if (P->eos_flag != 0) return ens_fail(PG_ERR_CONFIG, pre + "the isothermal EOS (EOS_flag 0)");
     if (P->cool_flag != 0) return ens_fail(PG_ERR_CONFIG, pre + "no cooling (cool_flag 0)");
+    if (P->twobd_flag != 0) return ens_fail(PG_ERR_CONFIG, pre + "a fixed star (twobd_flag 0)");
     if (P->bound_lft != 0 || P->bound_rgh != 0)
         return ens_fail(PG_ERR_CONFIG, pre + "analytic radial boundaries (bound 0)");
     if (!P->orbadv_flag) return ens_fail(PG_ERR_CONFIG, pre + "orbital advection (OrbAdv_flag 1)");

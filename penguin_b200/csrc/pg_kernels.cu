@@ -82,6 +82,34 @@ __device__ __forceinline__ Grav gravity(const DiskView& d, int i, double rad, do
     return g;
 }
 
+// One body of the two-body frame as an inertial point mass
+// (star_planet_grav_cyl_inertial, src/solver/force/forces.cu:89-106, z = 0).
+__device__ __forceinline__ void inertial_pull(double rad, double sinfac, double cosfac, const pg_body& p, Grav& g) {
+    const double plm = p.m, plx = p.x;
+    const double Rp = sqrt(rad * rad + plx * plx - 2.0 * plx * rad * cosfac + 0.0 * 0.0 + p.rs * p.rs);
+    const double rs_fac = 1.0 / Rp / Rp / Rp;
+    g.gx += -plm * (rad - plx * cosfac) * rs_fac;
+    g.gy += -plm * plx * sinfac * rs_fac;
+    g.gz += -plm * 0.0 * rs_fac;
+}
+
+// Gravity at cell (i, j) with the bodies of the first half-kick (which 0) or at
+// t + dt (which 1).  In the two-body frame (twobd_flag 1, forces.cu:182-327)
+// the star (planets[0]) and the planet (planets[1]) pull as inertial point
+// masses and the fixed-star term and the indirect term drop out.
+__device__ __forceinline__ Grav body_gravity(const DiskView& d, int i, int j, int which, const pg_body& pl,
+                                             const pg_body& st) {
+    const double* tr = d.trig + 4 * j + 2 * which;
+    if (!d.twobd) return gravity(d, i, d.radx[i], tr[0], tr[1], d.trig[4 * d.yarr + which], pl);
+    Grav g{0.0, 0.0, 0.0};
+    if (d.geomx == 1) {
+        const double* ts = d.strig + 4 * j + 2 * which;
+        inertial_pull(d.radx[i], ts[0], ts[1], st, g);
+        inertial_pull(d.radx[i], tr[0], tr[1], pl, g);
+    }
+    return g;
+}
+
 // One cell of apply_source_terms (src/solver/sweeps.cu:597-711): curvature,
 // gravity and viscous acceleration; with mdt != 0 the forces are re-evaluated
 // at the mdt-predicted velocities (sweeps.cu:663-687).
@@ -587,8 +615,7 @@ __global__ void __launch_bounds__(ST_THREADS)
                     vis[2 * m + 1] = vy;
                 }
             }
-            const double* tr = d.trig + 4 * j;
-            const Grav g = gravity(d, i, d.radx[i], tr[0], tr[1], d.trig[4 * d.yarr], sc->planet_cur);
+            const Grav g = body_gravity(d, i, j, 0, sc->planet_cur, sc->star_cur);
             Cell Q = kick<VISC>(d, C, d.irad[i], g, vx, vy, 0.0, hdt);
             if (d.cool) Q.p = p_cool(d, i, C.p, C.r, hdt);  // sweeps.cu:695-699
             emit(d, out, i, j, Q);
@@ -620,7 +647,7 @@ __global__ void __launch_bounds__(ST_THREADS)
     const int tid = threadIdx.x;
     const double dt = sc->dt, hdt = 0.5 * dt;
     const pg_body pl = sc->planet_next;
-    const double iplx2 = d.trig[4 * d.yarr + 1];
+    const pg_body st = sc->star_next;
     auto origin = [&](int tile, int& i0, int& j0) {
         i0 = NPAD + ST_TX * (tile % ntx);
         j0 = d.ypad + ST_TY * (tile / ntx);
@@ -656,8 +683,7 @@ __global__ void __launch_bounds__(ST_THREADS)
                     if (i < NPAD || i >= NPAD + d.xres || j < 0 || j >= d.yarr) continue;
                     const double* c = tile + it * 5;
                     const Cell C{c[0], c[1], c[2], c[3], c[4]};
-                    const double* tr = d.trig + 4 * j + 2;
-                    const Grav g = gravity(d, i, d.radx[i], tr[0], tr[1], iplx2, pl);
+                    const Grav g = body_gravity(d, i, j, 1, pl, st);
                     const Cell Q = kick<true>(d, C, d.irad[i], g, tvis[2 * it], tvis[2 * it + 1], hdt, hdt);
                     double* o = tp + it * 5;
                     o[0] = Q.r; o[1] = Q.p; o[2] = Q.u; o[3] = Q.v; o[4] = Q.w;
@@ -698,8 +724,7 @@ __global__ void __launch_bounds__(ST_THREADS)
                     gather9(tp, hx, hy, nu, u, v, nr);
                     viscous(d.visx + 5 * i, d.visy + 4 * j, u, v, nr, vx, vy);
                 }
-                const double* tr = d.trig + 4 * j + 2;
-                const Grav g = gravity(d, i, d.radx[i], tr[0], tr[1], iplx2, pl);
+                const Grav g = body_gravity(d, i, j, 1, pl, st);
                 double Tu = C.u, Tv = C.v;
                 Cell Q = kick<VISC>(d, C, d.irad[i], g, vx, vy, hdt, hdt, &Tu, &Tv);
                 // cooling over dt/2; the predictor cools over mdt = dt/2 as well, so Q.p is also
@@ -767,7 +792,8 @@ __global__ void k_set_time(const DiskView d, double t, double dt) {
     sc->done = 0;
     sc->dt = dt;
     sc->planet_cur = sc->planet_next;
-    if (d.nplanet > 0) orbit_solution(d, sc->planet_next, t + dt);  // evolve_planet (solve.cu:264)
+    sc->star_cur = sc->star_next;
+    evolve_bodies(d, sc, t + dt);  // evolve_planet (solve.cu:264)
     sc->t = t + dt;
     sc->dt_prev = dt;
     sc->vmax_bits = 0ull;
@@ -778,15 +804,19 @@ __global__ void k_set_time(const DiskView d, double t, double dt) {
 __global__ void k_time_step(const DiskView d) { advance_clock(d); }
 
 __global__ void k_init_planet(const DiskView d, double a, double e, double rs, double t) {
-    // init_planet (src/planet/planet.cu:319-402, one planet)
-    pg_body b;
-    b.a = a;
-    b.e = e;
+    // init_planet (src/planet/planet.cu:319-402): one planet, or the star-planet
+    // pair of the two-body frame (the star unsmoothed)
+    pg_body b{}, s{};
+    b.a = s.a = a;
+    b.e = s.e = e;
     b.rs = 0.0;
-    orbit_solution(d, b, t);
+    if (d.twobd) two_body_solution(d, s, b, t);
+    else orbit_solution(d, b, t);
     b.rs = rs;
     d.sc->planet_next = b;
     d.sc->planet_cur = b;
+    d.sc->star_next = s;
+    d.sc->star_cur = s;
 }
 
 // Per-index tables evaluated with the device's own pow/sqrt/__sinf so they carry
@@ -920,6 +950,11 @@ __global__ void k_planet_trig(const DiskView d) {
         double* t = d.trig + 4 * j;
         sincos(d.ycj[j] - (a.y + 0.0 * a.vy), &t[0], &t[1]);
         sincos(d.ycj[j] - (b.y + 0.0 * b.vy), &t[2], &t[3]);
+        if (d.twobd) {
+            double* u = d.strig + 4 * j;
+            sincos(d.ycj[j] - (sc->star_cur.y + 0.0 * sc->star_cur.vy), &u[0], &u[1]);
+            sincos(d.ycj[j] - (sc->star_next.y + 0.0 * sc->star_next.vy), &u[2], &u[3]);
+        }
     }
     if (j == 0) {
         d.trig[4 * d.yarr] = 1.0 / a.x / a.x;
@@ -984,7 +1019,10 @@ __global__ void k_torque(const DiskView d, const Cell* __restrict__ buf, double*
         sincos(d.ycraw[j] - p.y, &sinfac, &cosfac);
         const double Rp = sqrt(rad * rad + p.x * p.x - 2.0 * p.x * rad * cosfac + p.rs * p.rs);
         const double rs_fac = 1.0 / Rp / Rp / Rp;
-        const double gy = -p.m * p.x * sinfac * rs_fac + p.m * sinfac / p.x / p.x;
+        // the planet's pull (output_gy, src/output/forces.cu:103-127): with the indirect
+        // term, or as an inertial point mass in the two-body frame (global_sum(.., 1))
+        const double gy = d.twobd ? -p.m * p.x * sinfac * rs_fac
+                                  : -p.m * p.x * sinfac * rs_fac + p.m * sinfac / p.x / p.x;
         const double dv = 0.5 * (d.xa[i + 1] * d.xa[i + 1] - d.xa[i] * d.xa[i]) * (d.ya[j + 1] - d.ya[j]);
         const double y = rad * gy * (load_cell(buf, d.xarr, i, j).r * dv) - comp;
         const double t = sum + y;

@@ -58,6 +58,50 @@ __device__ inline void orbit_solution(const D& d, pg_body& b, double t) {  // pl
     b.vz = 0.0;
 }
 
+// The star-planet pair on the reduced orbit (src/planet/planet.cu:135-175),
+// both in the frame rotating at frame_omega: star = planets[0] (mass 1/(1+mp)),
+// planet = planets[1] (mass mp/(1+mp)), mp ramped like a single planet's mass.
+// The a, e and rs members of both bodies are kept.
+template <class D>
+__device__ inline void two_body_solution(const D& d, pg_body& star, pg_body& planet, double t) {
+    const double a = star.a, e = star.e;
+    const double n = sqrt(1.0 / a / a / a);
+    const double efac = sqrt(1.0 - e * e);
+    const double B = e / (1.0 + efac);
+    double u, cosu, sinu;
+    u = ecc_anomaly(n, e, t);
+    sincos(u, &sinu, &cosu);
+    double f, ecosf, esinf;
+    f = u + 2.0 * atan(B * sinu / (1.0 - B * cosu));
+    sincos(f, &esinf, &ecosf);
+    esinf *= e;
+    ecosf *= e;
+    const double reduced_r = a * efac * efac / (1.0 + ecosf);
+    const double reduced_p = f - fmod(d.frame_omega * t, TWOPI) + PI;
+    const double mp = ramp_function(t, d.ramp_time, d.planet_mass);
+    star.m = 1.0 / (1.0 + mp);
+    star.x = reduced_r * mp / (1.0 + mp);
+    star.y = fmod(reduced_p + PI, TWOPI);
+    star.z = HPI;
+    star.vx = n * a * esinf / efac * mp / (1.0 + mp);
+    star.vy = n * (1.0 + ecosf) * (1.0 + ecosf) / efac / efac / efac;
+    star.vz = 0.0;
+    planet.m = mp / (1.0 + mp);
+    planet.x = reduced_r * 1.0 / (1.0 + mp);
+    planet.y = reduced_p;
+    planet.z = HPI;
+    planet.vx = n * a * esinf / efac * 1.0 / (1.0 + mp);
+    planet.vy = n * (1.0 + ecosf) * (1.0 + ecosf) / efac / efac / efac;
+    planet.vz = 0.0;
+}
+
+// evolve_planet (src/planet/planet.cu:291-304): the bodies at time t
+__device__ inline void evolve_bodies(const DiskView& d, Scalars* sc, double t) {
+    if (d.nplanet <= 0) return;
+    if (d.twobd) two_body_solution(d, sc->star_next, sc->planet_next, t);
+    else orbit_solution(d, sc->planet_next, t);
+}
+
 // Device-resident loop step (main.cu:322-339): dt = min(CFL/vmax, 1.1 dt_prev),
 // clipped at end_time; then the planet at t + dt.  A step after the one that
 // reached end_time only sets the done flag.
@@ -80,7 +124,8 @@ __device__ inline void advance_clock(const DiskView& d) {
     }
     sc->dt = dt;
     sc->planet_cur = sc->planet_next;
-    if (d.nplanet > 0) orbit_solution(d, sc->planet_next, t + dt);
+    sc->star_cur = sc->star_next;
+    evolve_bodies(d, sc, t + dt);
     sc->t = t + dt;
     sc->dt_prev = dt;
     sc->vmax_bits = 0ull;

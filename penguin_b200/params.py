@@ -65,6 +65,7 @@ class Params:
     D_G_ratio: float = 0.01
     cool_flag: int = 0      # 0 off, 1 t_c = beta r^1.5, 2 t_c = beta / Sigma sqrt(p/Sigma) / h
     beta_cool: float = 0.001
+    twobd_flag: int = 0     # 1: star and planet orbit their barycentre (two-body frame)
 
     # ----------------------------------------------------------------- sizes
     @property
@@ -105,6 +106,8 @@ class Params:
             raise ValueError("cool_flag must be 0, 1 or 2")
         if self.cool_flag and not self.beta_cool > 0.0:
             raise ValueError("cooling needs beta_cool > 0")
+        if self.twobd_flag not in (0, 1):
+            raise ValueError("twobd_flag must be 0 or 1")
 
 
 class PGParams(ctypes.Structure):
@@ -129,6 +132,7 @@ class PGParams(ctypes.Structure):
         ("dust_flag", ctypes.c_int),
         ("stokes", ctypes.c_double), ("d_g_ratio", ctypes.c_double),
         ("cool_flag", ctypes.c_int), ("beta_cool", ctypes.c_double),
+        ("twobd_flag", ctypes.c_int),
     ]
 
     @classmethod
@@ -141,7 +145,7 @@ class PGParams(ctypes.Structure):
             p.p_alpha, p.p_beta, p.ss_alpha, p.sc_h, p.planet_radius,
             p.visc_flag, p.OrbAdv_flag, p.kill_flag, p.kill_width, p.kill_width_out,
             p.n_planet, p.planet_mass, p.planet_ecc, p.rs_fac, p.ramp_time, p.zmin, p.zmax,
-            p.dust_flag, p.Stokes, p.D_G_ratio, p.cool_flag, p.beta_cool,
+            p.dust_flag, p.Stokes, p.D_G_ratio, p.cool_flag, p.beta_cool, p.twobd_flag,
         )
 
 

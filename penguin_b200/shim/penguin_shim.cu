@@ -49,6 +49,11 @@ static const int pgs_cool = cool_flag;
 #else
 static const int pgs_cool = 0;
 #endif
+#if defined(twobd_flag) && twobd_flag == 1
+static const int pgs_twobd = 1;
+#else
+static const int pgs_twobd = 0;
+#endif
 #undef ndim
 #undef geomx
 #undef geomy
@@ -60,6 +65,7 @@ static const int pgs_cool = 0;
 #undef kill_flag
 #undef dust_flag
 #undef cool_flag
+#undef twobd_flag
 
 #include "penguin_b200.h"
 
@@ -100,7 +106,7 @@ static void pg_shim_configure() {
     P.kill_flag = pgs_kill;
     P.kill_width = kill_width;
     P.kill_width_out = kill_width;
-    P.n_planet = n_planet;
+    P.n_planet = pgs_twobd ? 1 : n_planet;  // the two-body frame's n_planet 2 counts the star
     P.planet_mass = planet_mass;
     P.planet_ecc = planet_ecc;
     P.rs_fac = rs_fac;
@@ -112,6 +118,7 @@ static void pg_shim_configure() {
     P.d_g_ratio = D_G_ratio;
     P.cool_flag = pgs_cool;
     P.beta_cool = beta_cool;
+    P.twobd_flag = pgs_twobd;
     if (pg_configure(&P) != PG_OK) {
         fprintf(stderr, "penguin_b200: %s\n", pg_last_error());
         exit(1);

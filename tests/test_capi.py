@@ -61,6 +61,7 @@ def test_params_struct_layout_matches_header(tmp_path):
     dict(ndim=3), dict(EOS_flag=1), dict(xres=31), dict(bound_lft=3), dict(geomx=2), dict(n_planet=2),
     dict(dust_flag=1, Stokes=0.0), dict(dust_flag=1, init_flag=1), dict(yres=4),
     dict(cool_flag=3), dict(cool_flag=1, beta_cool=0.0),
+    dict(twobd_flag=2), dict(twobd_flag=1, n_planet=0), dict(twobd_flag=1, geomx=0, geomy=0),
 ])
 def test_check_params_rejects(bad):
     p = P.planet_disk(64, 192).replace(**bad)
@@ -76,12 +77,13 @@ def _raw(p):
         p.EOS_flag, p.internal_e_flag, p.gam, p.CFL, p.bound_lft, p.bound_rgh, p.init_flag, p.frame_omega,
         p.p_alpha, p.p_beta, p.ss_alpha, p.sc_h, p.planet_radius, p.visc_flag, p.OrbAdv_flag, p.kill_flag,
         p.kill_width, p.kill_width_out, p.n_planet, p.planet_mass, p.planet_ecc, p.rs_fac, p.ramp_time,
-        p.zmin, p.zmax, p.dust_flag, p.Stokes, p.D_G_ratio, p.cool_flag, p.beta_cool)
+        p.zmin, p.zmax, p.dust_flag, p.Stokes, p.D_G_ratio, p.cool_flag, p.beta_cool, p.twobd_flag)
 
 
 def test_check_params_accepts_workloads():
     for p in (P.sod_tube(1024), P.planet_disk(1024, 3072), P.reference_disk(64, 192),
-              P.reference_disk(64, 192).replace(EOS_flag=2, gam=1.4, cool_flag=2, beta_cool=0.05)):
+              P.reference_disk(64, 192).replace(EOS_flag=2, gam=1.4, cool_flag=2, beta_cool=0.05),
+              P.reference_disk(64, 192).replace(twobd_flag=1)):
         assert _lib.lib().pg_check_params(ctypes.byref(_raw(p))) == _lib.PG_OK
 
 

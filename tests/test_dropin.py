@@ -1,6 +1,6 @@
 """The reference's own main.cu, relinked through penguin_b200/shim against
 libpenguin_b200.so, run on golden cases (gas; gas + dust; an adiabatic disk
-with cooling).  Needs a B200
+with cooling; the two-body frame, whose planets array holds star and planet).  Needs a B200
 and the relinked executable (built next to the reference objects by
 __graft_entry__.build() where the reference sources are available)."""
 import glob
@@ -23,7 +23,7 @@ def rel_l1(a, b):
     return np.abs(a - b).sum() / np.abs(b).sum()
 
 
-@pytest.mark.parametrize("name", ["disk64_n10", "dust64_st01_n10", "adi64_cool1_n10"])
+@pytest.mark.parametrize("name", ["disk64_n10", "dust64_st01_n10", "adi64_cool1_n10", "tb64_n10"])
 def test_relinked_main_reproduces_reference(name, tmp_path):
     exe = os.path.join(ROOT, "oracle", "_ref", name, "dropin", "penguin")
     fx = os.path.join(GOLDEN, name + ".npz")

@@ -23,6 +23,7 @@ def test_seeded_ensemble_has_the_configured_ranges():
     (P.sod_tube(1024), "ndim 2"),
     (P.planet_disk(128, 384).replace(EOS_flag=2), "isothermal"),
     (P.planet_disk(128, 384).replace(cool_flag=1), "no cooling"),
+    (P.planet_disk(128, 384).replace(twobd_flag=1), "fixed star"),
     (P.planet_disk(128, 384).replace(bound_lft=1), "bound 0"),
     (P.planet_disk(128, 384).replace(OrbAdv_flag=0), "orbital advection"),
     (P.planet_disk(32, 96), "at least 64"),

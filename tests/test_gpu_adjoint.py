@@ -187,3 +187,5 @@ def test_adjoint_rejects_unsupported_disks():
         DiskAdjoint.check_params(P.sod_tube(64))
     with pytest.raises(PGError):
         DiskAdjoint.check_params(small_disk().replace(cool_flag=1))
+    with pytest.raises(PGError):
+        DiskAdjoint.check_params(small_disk().replace(twobd_flag=1))
