@@ -305,6 +305,10 @@ pg_status pg_adj_pass_fields(pg_adj* a, int pass, double dt, double eps, const d
 pg_status pg_adj_schedule(const pg_adj* a, double* dts, int n);
 int pg_adj_steps(const pg_adj* a);
 long long pg_adj_device_bytes(const pg_adj* a);
+/* The face fluxes of the sweeps are transposed by hand-written reverse-mode
+   kernels (hand = 1, the default) or by the dual-number kernels (hand = 0,
+   kept as their check).  Both give the same gradient to rounding. */
+pg_status pg_adj_set_sweep_reverse(pg_adj* a, int hand);
 
 #ifdef __cplusplus
 }

@@ -143,6 +143,11 @@ class DiskAdjoint:
     def device_bytes(self) -> int:
         return int(lib().pg_adj_device_bytes(self._h))
 
+    def set_sweep_reverse(self, hand: bool) -> None:
+        """Transpose the sweeps' face fluxes with the hand-written reverse-mode
+        kernels (default) or with the dual-number kernels that check them."""
+        check(lib().pg_adj_set_sweep_reverse(self._h, int(bool(hand))))
+
     def close(self) -> None:
         if getattr(self, "_h", None):
             lib().pg_adj_destroy(self._h)

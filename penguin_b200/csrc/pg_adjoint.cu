@@ -23,12 +23,14 @@
 // with it the residual speed) and the planet (mass ramp ~ q, smoothing ~ h),
 // whose derivatives are computed on the host.  dt is frozen (the schedule of
 // the recorded forward run), as the CFL minimum is not differentiable.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <string>
 #include <vector>
 
 #include "pg_common.cuh"
+#include "pg_adjrev.cuh"
 #include "pg_dual.cuh"
 #include "pg_hydro.cuh"
 #include "pg_internal.h"
@@ -700,6 +702,213 @@ __global__ void __launch_bounds__(ADJ_THREADS) k_adj_flux(const Args a, const do
     }
 }
 
+// ------------------------------------------- hand-written sweep reverse
+// The face fluxes' share of the sweep adjoint in reverse mode, three kernels:
+// per face, the HLLC reverse gives the adjoints of the two half-states it
+// reads (k_rev_face); per cell, the reverse of its edge-state function
+// (reconstruction, flattening, characteristic tracing) gives the adjoints of
+// the 5 cells of its stencil (k_rev_cell); per interior cell, a gather adds
+// them to lam_in (k_rev_gather).  No atomics.  DIR 0 covers the xres + 1 faces
+// of a radial pencil and the cells NPAD - 1 .. NPAD + xres whose half-states
+// they read (stencil entries on the constant bound-0 ghosts drop out); DIR 1,
+// periodic, covers each of the yres faces of a column once, its adjoint
+// collected from both neighbouring cells like face_lambda, so every interior
+// cell owns both of its half-states and ghost-row stencil entries wrap.
+// Buffer per pencil: (n + 2) cells x (8 half-state adjoints + 15 stencil
+// adjoints).
+constexpr int REV_HALF = 8, REV_STEN = 15, REV_SLOT = REV_HALF + REV_STEN;
+
+template <int DIR>
+__device__ __forceinline__ void rev_dims(const DiskView& d, int& n, int& npen, int& p0) {
+    n = (DIR == 0) ? d.xres : d.yres;
+    npen = (DIR == 0) ? d.yres : d.xres;
+    p0 = (DIR == 0) ? NPAD : d.ypad;
+}
+
+// Adjoint of both edge states of pencil cell c (the v slot of DIR 0, the w slot
+// of DIR 1 carry the 4th half-state component); out[k][f]: adjoint of state
+// variable f (Sigma with p = cs^2 Sigma folded in, v_r, v_phi) of stencil cell
+// c - 2 + k.
+template <int DIR>
+__device__ __forceinline__ void edge_rev(const Args& a, int c, int q, const double* bl, const double* br,
+                                         double out[5][3]) {
+    const DiskView& d = a.d;
+    const Seed s0{-1, -1, -1, -1};
+    double r[5], p[5], u[5], v[5];
+    double rad = 1.0, irad_q = 1.0, rot = 0.0;
+    if (DIR == 1) {
+        rad = d.radx[q];
+        irad_q = d.irad[q];
+        rot = d.rot[q];
+    }
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+        const S3<double> C = (DIR == 0) ? ld<double>(a, s0, c - 2 + k, q) : ld<double>(a, s0, q, c - 2 + k);
+        r[k] = C.r;
+        p[k] = C.p;
+        if (DIR == 0) {
+            u[k] = C.u;
+            v[k] = C.v * d.radx[c - 2 + k];
+        } else {
+            u[k] = C.v - rot;
+            u[k] -= rad * d.frame_omega;
+            v[k] = C.u;
+        }
+    }
+    const double cs0 = sqrt(d.gam * p[2] / r[2]);
+    rev::FlatTape ft;
+    const double flat = rev::flatten_tape(1.0 / cs0, p[2], p[0], p[1], p[3], p[4], u[1], u[2], u[3], ft);
+    const double* wt = ((DIR == 0) ? d.wx : d.wy) + 6 * c;
+    const double* fa = (DIR == 0) ? d.xa : d.ya;
+    const double idx = ((DIR == 0) ? d.idx_x : d.idx_y)[c];
+    rev::ReconTape tR, tP, tU, tV;
+    const Par R = rev::recon_tape(wt, r[0], r[1], r[2], r[3], r[4], flat, tR);
+    const Par P = rev::recon_tape(wt, p[0], p[1], p[2], p[3], p[4], flat, tP);
+    const Par U = rev::recon_tape(wt, u[0], u[1], u[2], u[3], u[4], flat, tU);
+    const Par V = rev::recon_tape(wt, v[0], v[1], v[2], v[3], v[4], flat, tV);
+    const Par Z{0.0, 0.0, 0.0};
+    const double xl = fa[c], xr = fa[c + 1];
+    const double sdt = (DIR == 0) ? a.dt : a.dt * irad_q;
+    const Half bsl{bl[0], bl[1], bl[2], DIR == 0 ? bl[3] : 0.0, DIR == 0 ? 0.0 : bl[3]};
+    const Half bsr{br[0], br[1], br[2], DIR == 0 ? br[3] : 0.0, DIR == 0 ? 0.0 : br[3]};
+    double bcs0 = 0.0, br0c = 0.0, bp0c = 0.0, bu0c = 0.0;
+    Par bR{0.0, 0.0, 0.0}, bP{0.0, 0.0, 0.0}, bU{0.0, 0.0, 0.0}, bV{0.0, 0.0, 0.0}, bZ{0.0, 0.0, 0.0};
+    if (DIR == 0) {
+        rev::state_left_rev(d.gam, xl, idx, sdt, cs0, r[2], p[2], u[2], R, P, U, V, Z, bsl, bcs0, br0c, bp0c, bu0c,
+                            bR, bP, bU, bV, bZ);
+        rev::state_right_rev(d.gam, xl, xr, idx, sdt, cs0, r[2], p[2], u[2], R, P, U, V, Z, bsr, bcs0, br0c, bp0c,
+                             bu0c, bR, bP, bU, bV, bZ);
+    } else {
+        rev::state_left_rev(d.gam, xl, idx, sdt, cs0, r[2], p[2], u[2], R, P, U, Z, V, bsl, bcs0, br0c, bp0c, bu0c,
+                            bR, bP, bU, bZ, bV);
+        rev::state_right_rev(d.gam, xl, xr, idx, sdt, cs0, r[2], p[2], u[2], R, P, U, Z, V, bsr, bcs0, br0c, bp0c,
+                             bu0c, bR, bP, bU, bZ, bV);
+    }
+    double ar[5] = {0.0, 0.0, 0.0, 0.0, 0.0}, ap[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    double au[5] = {0.0, 0.0, 0.0, 0.0, 0.0}, av[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    double bflat = 0.0;
+    rev::recon_rev(wt, tR, flat, bR, ar, bflat);
+    rev::recon_rev(wt, tP, flat, bP, ap, bflat);
+    rev::recon_rev(wt, tU, flat, bU, au, bflat);
+    rev::recon_rev(wt, tV, flat, bV, av, bflat);
+    rev::flatten_rev(ft, bflat, ap);
+    // cs0 = sqrt(gam p / r) of the middle cell, which also enters the states directly
+    const double bA = rev::dsqrt(cs0, bcs0);
+    ap[2] += bA * d.gam / r[2] + bp0c;
+    ar[2] += br0c - bA * d.gam * p[2] / (r[2] * r[2]);
+    au[2] += bu0c;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+        const int ik = (DIR == 0) ? c - 2 + k : q;
+        out[k][0] = ar[k] + d.cs2x[ik] * ap[k];
+        if (DIR == 0) {
+            out[k][1] = au[k];
+            out[k][2] = av[k] * d.radx[c - 2 + k];
+        } else {
+            out[k][1] = av[k];
+            out[k][2] = au[k];
+        }
+    }
+}
+
+template <int DIR>
+__global__ void __launch_bounds__(ADJ_THREADS) k_rev_face(const Args a, const double* lslot, double* buf) {
+    const DiskView& d = a.d;
+    int n, npen, p0;
+    rev_dims<DIR>(d, n, npen, p0);
+    const int nf = (DIR == 0) ? n + 1 : n;  // faces per pencil
+    const long long total = (long long)nf * npen;
+    const Seed s0{-1, -1, -1, -1};
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int pen = (int)(t / nf), f = p0 + (int)(t % nf);
+        const int q = ((DIR == 0) ? d.ypad : NPAD) + pen;
+        const FluxT<double> LF = face_lambda<DIR>(a, lslot, f, q);
+        HalfT<double> l0, r0, l1, r1;
+        edge_states<double, DIR>(a, s0, f - 1, q, l0, r0);
+        edge_states<double, DIR>(a, s0, f, q, l1, r1);
+        const double bF[5] = {LF.r, LF.u, LF.v, LF.w, LF.pres};
+        Half bL{0.0, 0.0, 0.0, 0.0, 0.0}, bR{0.0, 0.0, 0.0, 0.0, 0.0};
+        rev::hllc_rev(d.gam, r0, l1, bF, bL, bR);
+        double* pb = buf + (size_t)pen * (n + 2) * REV_SLOT;
+        // the right half-state of cell f - 1 (DIR 1: wrapped to its interior row)
+        const int cm = (DIR == 0) ? f - 1 : wrap_row(d, f - 1);
+        double* o = pb + (size_t)(cm - (p0 - 1)) * REV_SLOT;
+        o[4] = bL.r;
+        o[5] = bL.p;
+        o[6] = bL.u;
+        o[7] = (DIR == 0) ? bL.v : bL.w;
+        o = pb + (size_t)(f - (p0 - 1)) * REV_SLOT;  // the left half-state of cell f
+        o[0] = bR.r;
+        o[1] = bR.p;
+        o[2] = bR.u;
+        o[3] = (DIR == 0) ? bR.v : bR.w;
+        if (DIR == 0 && f == p0) {  // ghost cell p0 - 1 has no left face in the pencil
+            o = pb;
+            o[0] = o[1] = o[2] = o[3] = 0.0;
+        }
+        if (DIR == 0 && f == p0 + n) {  // nor ghost cell p0 + n a right face
+            o = pb + (size_t)(n + 1) * REV_SLOT;
+            o[4] = o[5] = o[6] = o[7] = 0.0;
+        }
+    }
+}
+
+template <int DIR>
+__global__ void __launch_bounds__(ADJ_THREADS) k_rev_cell(const Args a, double* buf) {
+    const DiskView& d = a.d;
+    int n, npen, p0;
+    rev_dims<DIR>(d, n, npen, p0);
+    const int nc = (DIR == 0) ? n + 2 : n;  // cells per pencil with half-state adjoints
+    const int c0 = (DIR == 0) ? p0 - 1 : p0;
+    const long long total = (long long)nc * npen;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int pen = (int)(t / nc), c = c0 + (int)(t % nc);
+        const int q = ((DIR == 0) ? d.ypad : NPAD) + pen;
+        double* o = buf + ((size_t)pen * (n + 2) + (c - (p0 - 1))) * REV_SLOT;
+        double out[5][3];
+        edge_rev<DIR>(a, c, q, o, o + 4, out);
+#pragma unroll
+        for (int k = 0; k < 5; ++k)
+#pragma unroll
+            for (int f = 0; f < 3; ++f) o[REV_HALF + 3 * k + f] = out[k][f];
+    }
+}
+
+template <int DIR>
+__global__ void __launch_bounds__(ADJ_THREADS) k_rev_gather(const Args a, const double* buf) {
+    const DiskView& d = a.d;
+    int n, npen, p0;
+    rev_dims<DIR>(d, n, npen, p0);
+    const long long total = (long long)d.xres * d.yres;
+    const size_t P = plane(d);
+    const int lo = (DIR == 0) ? p0 - 1 : p0, hi = (DIR == 0) ? p0 + n : p0 + n - 1;  // cells holding adjoints
+    for (long long m = blockIdx.x * (long long)blockDim.x + threadIdx.x; m < total;
+         m += (long long)gridDim.x * blockDim.x) {
+        const int i = NPAD + (int)(m % d.xres), j = d.ypad + (int)(m / d.xres);
+        const int pos = (DIR == 0) ? i : j;
+        const int pen = (DIR == 0) ? j - d.ypad : i - NPAD;
+        const double* pb = buf + (size_t)pen * (n + 2) * REV_SLOT;
+        double acc[3] = {0.0, 0.0, 0.0};
+        for (int img = -1; img <= 1; ++img) {  // the cell itself and, periodic, its ghost-row images
+            if (DIR == 0 && img != 0) continue;
+            const int s = pos + img * n;
+            for (int k = 0; k < 5; ++k) {
+                const int src = s + 2 - k;
+                if (src < lo || src > hi) continue;
+                const double* o = pb + (size_t)(src - (p0 - 1)) * REV_SLOT + REV_HALF + 3 * k;
+                acc[0] += o[0];
+                acc[1] += o[1];
+                acc[2] += o[2];
+            }
+        }
+        a.lam_in[m] += acc[0];
+        a.lam_in[P + m] += acc[1];
+        a.lam_in[2 * P + m] += acc[2];
+    }
+}
+
 // kick2.  The corrector at each output is transposed per cell (k_adj_k2a: the
 // direct adjoint of C and lambda of the viscous force it reads); the force is a
 // function of the predicted 3x3 stencil, and each predicted cell of its own
@@ -1029,14 +1238,23 @@ static unsigned grid_for(long long n) {
 
 // The adjoint of one pass: lam_in (and lamv_in for kick2) from lam (and lamv
 // for kick1); scratch: 3 interior planes.  theta: also accumulate d/d theta.
+// rev: buffer of the hand-written sweep reverse, or null for the dual-number
+// kernels (k_adj_flux).
 template <int PASS>
-static void launch_pass(const Args& a, bool theta, double* scratch, cudaStream_t s) {
+static void launch_pass(const Args& a, bool theta, double* scratch, double* rev, cudaStream_t s) {
     const long long n = (long long)a.d.xres * a.d.yres;
     const unsigned g = grid_for(n);
     if (PASS == P_SX || PASS == P_SY) {
         constexpr int DIR = (PASS == P_SX) ? 0 : 1;
         k_adj_upd<DIR><<<g, ADJ_THREADS, 0, s>>>(a, scratch);
-        k_adj_flux<DIR><<<g, ADJ_THREADS, 0, s>>>(a, scratch);
+        if (rev) {
+            const long long pen = (DIR == 0) ? a.d.yres : a.d.xres, len = (DIR == 0) ? a.d.xres + 2 : a.d.yres;
+            k_rev_face<DIR><<<grid_for(pen * len), ADJ_THREADS, 0, s>>>(a, scratch, rev);
+            k_rev_cell<DIR><<<grid_for(pen * len), ADJ_THREADS, 0, s>>>(a, rev);
+            k_rev_gather<DIR><<<g, ADJ_THREADS, 0, s>>>(a, rev);
+        } else {
+            k_adj_flux<DIR><<<g, ADJ_THREADS, 0, s>>>(a, scratch);
+        }
     } else if (PASS == P_K2 && a.d.visc) {
         k_adj_k2a<<<g, ADJ_THREADS, 0, s>>>(a, scratch);
         k_adj_k2b<<<g, ADJ_THREADS, 0, s>>>(a, scratch);
@@ -1089,7 +1307,11 @@ struct pg_adj {
     unsigned long long* err = nullptr;
     Scalars* ssc = nullptr;  // scratch copy of the device scalars
     double* scratch = nullptr;  // 3 interior planes: lambda of the update slots / of kick1's force
+    double* rev = nullptr;      // hand-written sweep reverse: REV_SLOT doubles per pencil cell
+    bool hand = true;           // sweeps in reverse mode (false: the dual-number kernels)
     size_t bytes = 0;
+
+    double* rev_sweeps() const { return hand ? rev : nullptr; }
 
     size_t ncell() const { return (size_t)(P.xres + 2 * NPAD) * (P.yres + 2 * NPAD); }
     size_t nint() const { return (size_t)P.xres * P.yres; }
@@ -1232,6 +1454,11 @@ pg_status pg_adj_create(const pg_params* P, int device, void* stream, int checkp
     if ((s = adj_alloc(a, &a->err, 5 * sizeof(unsigned long long))) != PG_OK) return bail(s);
     if ((s = adj_alloc(a, &a->ssc, sizeof(Scalars))) != PG_OK) return bail(s);
     if ((s = adj_alloc(a, &a->scratch, 3 * ni * sizeof(double))) != PG_OK) return bail(s);
+    {
+        const size_t nx = (size_t)P->xres, ny = (size_t)P->yres;
+        const size_t cells = std::max(ny * (nx + 2), nx * (ny + 2));
+        if ((s = adj_alloc(a, &a->rev, cells * REV_SLOT * sizeof(double))) != PG_OK) return bail(s);
+    }
     if ((s = adj_make_disk(a)) != PG_OK) return bail(s);
     *out = a;
     return PG_OK;
@@ -1258,6 +1485,7 @@ pg_status pg_adj_destroy(pg_adj* a) {
     cudaFree(a->err);
     cudaFree(a->ssc);
     cudaFree(a->scratch);
+    cudaFree(a->rev);
     if (a->own_stream && a->stream) cudaStreamDestroy(a->stream);
     delete a;
     return PG_OK;
@@ -1395,11 +1623,11 @@ pg_status pg_adj_backward(pg_adj* a, const double* grad_out, double* grad_sigma0
                 g.lam = a->lam[c];
                 g.lam_in = a->lam[1 - c];
                 switch (pass) {
-                    case P_K2: g.lamv_in = a->lamv; launch_pass<P_K2>(g, true, a->scratch, st); break;
-                    case P_ADV: launch_pass<P_ADV>(g, true, a->scratch, st); break;
-                    case P_SY: launch_pass<P_SY>(g, true, a->scratch, st); break;
-                    case P_SX: launch_pass<P_SX>(g, true, a->scratch, st); break;
-                    default: g.lamv = a->lamv; launch_pass<P_K1>(g, true, a->scratch, st); break;
+                    case P_K2: g.lamv_in = a->lamv; launch_pass<P_K2>(g, true, a->scratch, a->rev_sweeps(), st); break;
+                    case P_ADV: launch_pass<P_ADV>(g, true, a->scratch, a->rev_sweeps(), st); break;
+                    case P_SY: launch_pass<P_SY>(g, true, a->scratch, a->rev_sweeps(), st); break;
+                    case P_SX: launch_pass<P_SX>(g, true, a->scratch, a->rev_sweeps(), st); break;
+                    default: g.lamv = a->lamv; launch_pass<P_K1>(g, true, a->scratch, a->rev_sweeps(), st); break;
                 }
                 c = 1 - c;
             };
@@ -1506,11 +1734,11 @@ pg_status pg_adj_dot_test(pg_adj* a, double dt, const double* dir, const double*
         if (p == P_ADV && !d.orbadv) continue;
         g.in = r.stage[p];
         switch (p) {
-            case P_K1: k_adj_jvp<P_K1><<<gr, ADJ_THREADS, 0, st>>>(g, dev + 2 * p); launch_pass<P_K1>(g, false, a->scratch, st); break;
-            case P_SX: k_adj_jvp<P_SX><<<gr, ADJ_THREADS, 0, st>>>(g, dev + 2 * p); launch_pass<P_SX>(g, false, a->scratch, st); break;
-            case P_SY: k_adj_jvp<P_SY><<<gr, ADJ_THREADS, 0, st>>>(g, dev + 2 * p); launch_pass<P_SY>(g, false, a->scratch, st); break;
-            case P_ADV: k_adj_jvp<P_ADV><<<gr, ADJ_THREADS, 0, st>>>(g, dev + 2 * p); launch_pass<P_ADV>(g, false, a->scratch, st); break;
-            default: k_adj_jvp<P_K2><<<gr, ADJ_THREADS, 0, st>>>(g, dev + 2 * p); launch_pass<P_K2>(g, false, a->scratch, st); break;
+            case P_K1: k_adj_jvp<P_K1><<<gr, ADJ_THREADS, 0, st>>>(g, dev + 2 * p); launch_pass<P_K1>(g, false, a->scratch, a->rev_sweeps(), st); break;
+            case P_SX: k_adj_jvp<P_SX><<<gr, ADJ_THREADS, 0, st>>>(g, dev + 2 * p); launch_pass<P_SX>(g, false, a->scratch, a->rev_sweeps(), st); break;
+            case P_SY: k_adj_jvp<P_SY><<<gr, ADJ_THREADS, 0, st>>>(g, dev + 2 * p); launch_pass<P_SY>(g, false, a->scratch, a->rev_sweeps(), st); break;
+            case P_ADV: k_adj_jvp<P_ADV><<<gr, ADJ_THREADS, 0, st>>>(g, dev + 2 * p); launch_pass<P_ADV>(g, false, a->scratch, a->rev_sweeps(), st); break;
+            default: k_adj_jvp<P_K2><<<gr, ADJ_THREADS, 0, st>>>(g, dev + 2 * p); launch_pass<P_K2>(g, false, a->scratch, a->rev_sweeps(), st); break;
         }
         k_dot<<<gr, ADJ_THREADS, 0, st>>>(g.lam_in, dir, (long long)(3 * ni), dev + 2 * p + 1);
         if (p == P_K2 && d.visc) k_dot<<<gr, ADJ_THREADS, 0, st>>>(g.lamv_in, dir + 3 * ni, (long long)(2 * ni), dev + 2 * p + 1);
@@ -1717,5 +1945,11 @@ pg_status pg_adj_schedule(const pg_adj* a, double* dts, int n) {
 int pg_adj_steps(const pg_adj* a) { return a ? (int)a->dts.size() : 0; }
 
 long long pg_adj_device_bytes(const pg_adj* a) { return a ? (long long)a->bytes : 0; }
+
+pg_status pg_adj_set_sweep_reverse(pg_adj* a, int hand) {
+    if (!a) return adj_fail(PG_ERR_ARG, "null adjoint");
+    a->hand = hand != 0;
+    return PG_OK;
+}
 
 }  // extern "C"
