@@ -536,6 +536,20 @@ __global__ void __launch_bounds__(ADJ_THREADS) k_adj_state(const Args a) {
 
 // d loss / d theta: each output cell contracted with its derivative along
 // every parameter, summed over the grid.
+// sum of acc[3] over the block (ADJ_THREADS threads, all arriving) into gth
+__device__ __forceinline__ void block_add3(const double* acc, double* gth) {
+    __shared__ double red[3][ADJ_THREADS];
+    for (int th = 0; th < 3; ++th) red[th][threadIdx.x] = acc[th];
+    __syncthreads();
+    for (int w = ADJ_THREADS / 2; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w)
+            for (int th = 0; th < 3; ++th) red[th][threadIdx.x] += red[th][threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        for (int th = 0; th < 3; ++th) atomicAdd(&gth[th], red[th][0]);
+}
+
 template <int PASS>
 __global__ void __launch_bounds__(ADJ_THREADS) k_adj_theta(const Args a) {
     const DiskView& d = a.d;
@@ -546,16 +560,7 @@ __global__ void __launch_bounds__(ADJ_THREADS) k_adj_theta(const Args a) {
 #pragma unroll 1
         for (int th = 0; th < 3; ++th) acc[th] += contract<PASS>(a, Seed{-1, -1, -1, th}, i, j);
     }
-    __shared__ double red[3][ADJ_THREADS];
-    for (int th = 0; th < 3; ++th) red[th][threadIdx.x] = acc[th];
-    __syncthreads();
-    for (int w = ADJ_THREADS / 2; w > 0; w >>= 1) {
-        if ((int)threadIdx.x < w)
-            for (int th = 0; th < 3; ++th) red[th][threadIdx.x] += red[th][threadIdx.x + w];
-        __syncthreads();
-    }
-    if (threadIdx.x == 0)
-        for (int th = 0; th < 3; ++th) atomicAdd(&a.gth[th], red[th][0]);
+    block_add3(acc, a.gth);
 }
 
 // ------------------------------------------------- structured adjoints
@@ -588,12 +593,15 @@ __device__ __forceinline__ void sweep_D(const Args& a, int i, int j, const FluxT
 
 // per cell (i, j) of the pass input (pre-shift row for DIR 1): the direct
 // adjoint of Q into lam_in and lambda_D of the slots into lslot (3 planes)
+// theta: with the hand-written reverse, also the theta derivative of the update
+// itself (DIR 1: (rot + r Omega) D_Sigma in the v_phi slot).
 template <int DIR>
-__global__ void __launch_bounds__(ADJ_THREADS) k_adj_upd(const Args a, double* lslot) {
+__global__ void __launch_bounds__(ADJ_THREADS) k_adj_upd(const Args a, double* lslot, bool theta) {
     const DiskView& d = a.d;
     const long long n = (long long)d.xres * d.yres;
     const size_t P = plane(d);
     const Seed s0{-1, -1, -1, -1};
+    double acc[3] = {0.0, 0.0, 0.0};
     for (long long m = blockIdx.x * (long long)blockDim.x + threadIdx.x; m < n; m += (long long)gridDim.x * blockDim.x) {
         const int i = NPAD + (int)(m % d.xres), j = d.ypad + (int)(m / d.xres);
         const size_t mo = (DIR == 1) ? pidx(d, i, sy_post_row(d, a.inc, i, j)) : (size_t)m;
@@ -629,7 +637,10 @@ __global__ void __launch_bounds__(ADJ_THREADS) k_adj_upd(const Args a, double* l
         lslot[m] = g[3];
         lslot[P + m] = g[4];
         lslot[2 * P + m] = g[5];
+        if (DIR == 1 && theta)
+            for (int th = 0; th < 3; ++th) acc[th] += g[5] * Dr * a.dtab[((size_t)th * NTAB + T_ROT) * d.xarr + i];
     }
+    if (theta) block_add3(acc, a.gth);
 }
 
 // lambda of the flux of face f of a pencil (between pencil cells f-1 and f) from
@@ -729,9 +740,11 @@ __device__ __forceinline__ void rev_dims(const DiskView& d, int& n, int& npen, i
 // of DIR 1 carry the 4th half-state component); out[k][f]: adjoint of state
 // variable f (Sigma with p = cs^2 Sigma folded in, v_r, v_phi) of stencil cell
 // c - 2 + k.
+// g3 (optional): accumulates the theta derivative contracted with the same
+// adjoints: p = cs^2(theta) Sigma of the cells, the bound-0 ghost state, rot.
 template <int DIR>
 __device__ __forceinline__ void edge_rev(const Args& a, int c, int q, const double* bl, const double* br,
-                                         double out[5][3]) {
+                                         double out[5][3], double* g3) {
     const DiskView& d = a.d;
     const Seed s0{-1, -1, -1, -1};
     double r[5], p[5], u[5], v[5];
@@ -797,6 +810,23 @@ __device__ __forceinline__ void edge_rev(const Args& a, int c, int q, const doub
     ap[2] += bA * d.gam / r[2] + bp0c;
     ar[2] += br0c - bA * d.gam * p[2] / (r[2] * r[2]);
     au[2] += bu0c;
+    if (g3) {
+        for (int th = 0; th < 3; ++th) {
+            const double* dt = a.dtab + (size_t)th * NTAB * d.xarr;
+            double g = 0.0;
+            for (int k = 0; k < 5; ++k) {
+                const int ik = (DIR == 0) ? c - 2 + k : q;
+                if (ik >= NPAD && ik < NPAD + d.xres) {
+                    g += ap[k] * r[k] * dt[T_CS2 * d.xarr + ik];
+                } else {  // radial ghost: init_C of the disk
+                    g += ap[k] * dt[T_P0 * d.xarr + ik] + au[k] * dt[T_U0 * d.xarr + ik] +
+                         av[k] * d.radx[ik] * dt[T_V0 * d.xarr + ik];
+                }
+                if (DIR == 1) g -= au[k] * dt[T_ROT * d.xarr + q];
+            }
+            g3[th] += g;
+        }
+    }
 #pragma unroll
     for (int k = 0; k < 5; ++k) {
         const int ik = (DIR == 0) ? c - 2 + k : q;
@@ -855,25 +885,27 @@ __global__ void __launch_bounds__(ADJ_THREADS) k_rev_face(const Args a, const do
 }
 
 template <int DIR>
-__global__ void __launch_bounds__(ADJ_THREADS) k_rev_cell(const Args a, double* buf) {
+__global__ void __launch_bounds__(ADJ_THREADS) k_rev_cell(const Args a, double* buf, bool theta) {
     const DiskView& d = a.d;
     int n, npen, p0;
     rev_dims<DIR>(d, n, npen, p0);
     const int nc = (DIR == 0) ? n + 2 : n;  // cells per pencil with half-state adjoints
     const int c0 = (DIR == 0) ? p0 - 1 : p0;
     const long long total = (long long)nc * npen;
+    double acc[3] = {0.0, 0.0, 0.0};
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
          t += (long long)gridDim.x * blockDim.x) {
         const int pen = (int)(t / nc), c = c0 + (int)(t % nc);
         const int q = ((DIR == 0) ? d.ypad : NPAD) + pen;
         double* o = buf + ((size_t)pen * (n + 2) + (c - (p0 - 1))) * REV_SLOT;
         double out[5][3];
-        edge_rev<DIR>(a, c, q, o, o + 4, out);
+        edge_rev<DIR>(a, c, q, o, o + 4, out, theta ? acc : nullptr);
 #pragma unroll
         for (int k = 0; k < 5; ++k)
 #pragma unroll
             for (int f = 0; f < 3; ++f) o[REV_HALF + 3 * k + f] = out[k][f];
     }
+    if (theta) block_add3(acc, a.gth);
 }
 
 template <int DIR>
@@ -1246,15 +1278,15 @@ static void launch_pass(const Args& a, bool theta, double* scratch, double* rev,
     const unsigned g = grid_for(n);
     if (PASS == P_SX || PASS == P_SY) {
         constexpr int DIR = (PASS == P_SX) ? 0 : 1;
-        k_adj_upd<DIR><<<g, ADJ_THREADS, 0, s>>>(a, scratch);
+        k_adj_upd<DIR><<<g, ADJ_THREADS, 0, s>>>(a, scratch, theta && rev);
         if (rev) {
             const long long pen = (DIR == 0) ? a.d.yres : a.d.xres, len = (DIR == 0) ? a.d.xres + 2 : a.d.yres;
             k_rev_face<DIR><<<grid_for(pen * len), ADJ_THREADS, 0, s>>>(a, scratch, rev);
-            k_rev_cell<DIR><<<grid_for(pen * len), ADJ_THREADS, 0, s>>>(a, rev);
+            k_rev_cell<DIR><<<grid_for(pen * len), ADJ_THREADS, 0, s>>>(a, rev, theta);
             k_rev_gather<DIR><<<g, ADJ_THREADS, 0, s>>>(a, rev);
-        } else {
-            k_adj_flux<DIR><<<g, ADJ_THREADS, 0, s>>>(a, scratch);
+            return;  // theta done by the reverse kernels
         }
+        k_adj_flux<DIR><<<g, ADJ_THREADS, 0, s>>>(a, scratch);
     } else if (PASS == P_K2 && a.d.visc) {
         k_adj_k2a<<<g, ADJ_THREADS, 0, s>>>(a, scratch);
         k_adj_k2b<<<g, ADJ_THREADS, 0, s>>>(a, scratch);
