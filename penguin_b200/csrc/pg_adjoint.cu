@@ -941,6 +941,134 @@ __global__ void __launch_bounds__(ADJ_THREADS) k_rev_gather(const Args a, const 
     }
 }
 
+// Residual advection in reverse mode (same buffer).  Per cell (k_radv_upd): the
+// direct adjoint of the update Q -> (Q.r + D_r, (Q.u Q.r + D_w) / r', (Q.v Q.r
+// + D_u) / r') into lam_in and the adjoints of its three flux differences into
+// lslot.  Per face (k_radv_face): the upwind cell's parabola averaged over the
+// swept fraction, times the residual speed; the reverse of the averages and of
+// the reconstruction gives the adjoints of the upwind cell's 5-cell stencil
+// (15 values per face) and, through res = rot - shift dy / dt, the theta
+// derivative.  Per cell (k_radv_gather): the stencil adjoints of the faces
+// whose upwind stencil holds it.
+__global__ void __launch_bounds__(ADJ_THREADS) k_radv_upd(const Args a, double* lslot) {
+    const DiskView& d = a.d;
+    const long long n = (long long)d.xres * d.yres;
+    const size_t P = plane(d);
+    const Seed s0{-1, -1, -1, -1};
+    for (long long m = blockIdx.x * (long long)blockDim.x + threadIdx.x; m < n; m += (long long)gridDim.x * blockDim.x) {
+        const int i = NPAD + (int)(m % d.xres), j = d.ypad + (int)(m / d.xres);
+        const S3<double> Q = ld<double>(a, s0, i, j);
+        const S3<double> O = eval_adv<double>(a, s0, i, j);
+        const double lr = a.lam[m], lu = a.lam[P + m], lv = a.lam[2 * P + m];
+        const double iR = 1.0 / O.r;  // 1 / (Q.r + D_r)
+        a.lam_in[m] = lr + (lu * (Q.u - O.u) + lv * (Q.v - O.v)) * iR;
+        a.lam_in[P + m] = lu * Q.r * iR;
+        a.lam_in[2 * P + m] = lv * Q.r * iR;
+        const double f = a.dt * d.iyv[j] * d.irad[i];  // D = (F_j - F_j+1) f
+        lslot[m] = (lr - (lu * O.u + lv * O.v) * iR) * f;  // adjoint of F_r at the lower face, minus at the upper
+        lslot[P + m] = lu * iR * f;                         // ... of F_w (v_r)
+        lslot[2 * P + m] = lv * iR * f;                     // ... of F_u (v_phi)
+    }
+}
+
+__global__ void __launch_bounds__(ADJ_THREADS) k_radv_face(const Args a, const double* lslot, double* buf,
+                                                           bool theta) {
+    const DiskView& d = a.d;
+    const long long n = (long long)d.xres * d.yres;
+    const size_t P = plane(d);
+    const Seed s0{-1, -1, -1, -1};
+    double acc[3] = {0.0, 0.0, 0.0};
+    for (long long m = blockIdx.x * (long long)blockDim.x + threadIdx.x; m < n; m += (long long)gridDim.x * blockDim.x) {
+        const int i = NPAD + (int)(m % d.xres), f = d.ypad + (int)(m / d.xres);  // face f: between rows f - 1, f
+        const double speed = a.res[i];
+        // the face is the lower face of row f (+) and the upper face of row f - 1 (-)
+        const size_t mb = pidx(d, i, wrap_row(d, f - 1));
+        const double bFr = lslot[m] - lslot[mb];
+        const double bFw = lslot[P + m] - lslot[P + mb];
+        const double bFu = lslot[2 * P + m] - lslot[2 * P + mb];
+        const int c = (speed > 0.0) ? f - 1 : f;  // the upwind row
+        double r[5], u[5], w[5];
+        for (int k = 0; k < 5; ++k) {
+            const S3<double> C = ld<double>(a, s0, i, c - 2 + k);
+            r[k] = C.r;
+            u[k] = C.v;
+            w[k] = C.u;
+        }
+        const double* wt = d.wy + 6 * c;
+        rev::ReconTape tR, tU, tW;
+        const Par R = rev::recon_tape(wt, r[0], r[1], r[2], r[3], r[4], 0.0, tR);
+        const Par U = rev::recon_tape(wt, u[0], u[1], u[2], u[3], u[4], 0.0, tU);
+        const Par W = rev::recon_tape(wt, w[0], w[1], w[2], w[3], w[4], 0.0, tW);
+        const double xl = d.ya[c], xr = d.ya[c + 1];
+        const double sdt = a.dt * d.irad[i];
+        const double idx = d.idx_y[c];
+        const double x0 = (speed > 0.0) ? xr - speed * sdt : xl - speed * sdt;
+        const double ax = (x0 - xl) * idx;
+        const double x = lim01(ax);
+        double aR, aU, aW;
+        if (speed > 0.0) {
+            const Frac q = frac_right(x);
+            aR = aveR(q, R);
+            aU = aveR(q, U);
+            aW = aveR(q, W);
+        } else {
+            const Frac q = frac_left(x);
+            aR = aveL(q, R);
+            aU = aveL(q, U);
+            aW = aveL(q, W);
+        }
+        // fr = aR speed, fu = (aU aR) speed, fw = (aW aR) speed
+        const double b_aR = speed * (bFr + bFu * aU + bFw * aW);
+        const double b_aU = speed * bFu * aR, b_aW = speed * bFw * aR;
+        Par bR{0.0, 0.0, 0.0}, bU{0.0, 0.0, 0.0}, bW{0.0, 0.0, 0.0};
+        double bx;
+        if (speed > 0.0) {
+            bx = rev::aveR_rev(x, R, b_aR, bR) + rev::aveR_rev(x, U, b_aU, bU) + rev::aveR_rev(x, W, b_aW, bW);
+        } else {
+            bx = rev::aveL_rev(x, R, b_aR, bR) + rev::aveL_rev(x, U, b_aU, bU) + rev::aveL_rev(x, W, b_aW, bW);
+        }
+        double ar[5] = {0.0, 0.0, 0.0, 0.0, 0.0}, au[5] = {0.0, 0.0, 0.0, 0.0, 0.0}, aw[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+        double bflat = 0.0;
+        rev::recon_rev(wt, tR, 0.0, bR, ar, bflat);
+        rev::recon_rev(wt, tU, 0.0, bU, au, bflat);
+        rev::recon_rev(wt, tW, 0.0, bW, aw, bflat);
+        double* o = buf + (size_t)m * REV_STEN;
+        for (int k = 0; k < 5; ++k) {
+            o[3 * k] = ar[k];
+            o[3 * k + 1] = aw[k];  // v_r
+            o[3 * k + 2] = au[k];  // v_phi
+        }
+        if (theta) {
+            // d/d speed: the flux factor and, through x0, the swept fraction
+            double bs = bFr * aR + bFu * aU * aR + bFw * aW * aR;
+            if (rev::lim_pass(ax)) bs -= bx * sdt * idx;
+            for (int th = 0; th < 3; ++th) acc[th] += bs * a.dtab[((size_t)th * NTAB + T_ROT) * d.xarr + i];
+        }
+    }
+    if (theta) block_add3(acc, a.gth);
+}
+
+__global__ void __launch_bounds__(ADJ_THREADS) k_radv_gather(const Args a, const double* buf) {
+    const DiskView& d = a.d;
+    const long long n = (long long)d.xres * d.yres;
+    const size_t P = plane(d);
+    for (long long m = blockIdx.x * (long long)blockDim.x + threadIdx.x; m < n; m += (long long)gridDim.x * blockDim.x) {
+        const int i = NPAD + (int)(m % d.xres), j = d.ypad + (int)(m / d.xres);
+        const int up = (a.res[i] > 0.0) ? 1 : 0;  // face f has upwind row f - up
+        double acc[3] = {0.0, 0.0, 0.0};
+        for (int k = 0; k < 5; ++k) {
+            const int f = wrap_row(d, j + 2 - k + up);  // its upwind stencil holds row j at position k
+            const double* o = buf + pidx(d, i, f) * REV_STEN + 3 * k;
+            acc[0] += o[0];
+            acc[1] += o[1];
+            acc[2] += o[2];
+        }
+        a.lam_in[m] += acc[0];
+        a.lam_in[P + m] += acc[1];
+        a.lam_in[2 * P + m] += acc[2];
+    }
+}
+
 // kick2.  The corrector at each output is transposed per cell (k_adj_k2a: the
 // direct adjoint of C and lambda of the viscous force it reads); the force is a
 // function of the predicted 3x3 stencil, and each predicted cell of its own
@@ -1287,6 +1415,11 @@ static void launch_pass(const Args& a, bool theta, double* scratch, double* rev,
             return;  // theta done by the reverse kernels
         }
         k_adj_flux<DIR><<<g, ADJ_THREADS, 0, s>>>(a, scratch);
+    } else if (PASS == P_ADV && rev) {
+        k_radv_upd<<<g, ADJ_THREADS, 0, s>>>(a, scratch);
+        k_radv_face<<<g, ADJ_THREADS, 0, s>>>(a, scratch, rev, theta);
+        k_radv_gather<<<g, ADJ_THREADS, 0, s>>>(a, rev);
+        return;  // theta done by k_radv_face
     } else if (PASS == P_K2 && a.d.visc) {
         k_adj_k2a<<<g, ADJ_THREADS, 0, s>>>(a, scratch);
         k_adj_k2b<<<g, ADJ_THREADS, 0, s>>>(a, scratch);
