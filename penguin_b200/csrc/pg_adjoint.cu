@@ -1069,6 +1069,81 @@ __global__ void __launch_bounds__(ADJ_THREADS) k_radv_gather(const Args a, const
     }
 }
 
+// kick1 in reverse mode (same buffer).  Per output cell (k_rk1_cell): the
+// pointwise adjoint of the half-kick (mdt = 0) into lam_in, and the adjoint of
+// its viscous force (from the kick and from kick2's use of the force, lamv)
+// through the reverse of the viscous stencil: 9 cells x 3 state variables per
+// output cell.  Per input cell (k_rk1_gather): the stencil adjoints of the 9
+// outputs whose stencil holds it (periodic rows wrap; the constant bound-0
+// ghost columns drop out).  theta stays with k_adj_theta.
+constexpr int RK1_STEN = 27;
+
+__global__ void __launch_bounds__(ADJ_THREADS) k_rk1_cell(const Args a, double* buf) {
+    const DiskView& d = a.d;
+    const long long n = (long long)d.xres * d.yres;
+    const size_t P = plane(d);
+    const Seed s0{-1, -1, -1, -1};
+    const double dt = 0.5 * a.dt;
+    for (long long m = blockIdx.x * (long long)blockDim.x + threadIdx.x; m < n; m += (long long)gridDim.x * blockDim.x) {
+        const int i = NPAD + (int)(m % d.xres), j = d.ypad + (int)(m / d.xres);
+        const S3<double> C = ld<double>(a, s0, i, j);
+        double vx = 0.0, vy = 0.0, nu[3], u[9], v[9], nr[9];
+        if (d.visc) {
+            for (int k = 0; k < 3; ++k) nu[k] = d.nux[i + k - 1];
+            for (int k = 0; k < 9; ++k) {
+                int dx, dy;
+                nb(k, dx, dy);
+                const S3<double> X = ld<double>(a, s0, i + dx, j + dy);
+                nr[k] = X.r * nu[k % 3];
+                u[k] = X.u;
+                v[k] = X.v;
+            }
+            viscous<double>(d.visx + 5 * i, d.visy + 4 * j, u, v, nr, vx, vy);
+        }
+        const double ix = d.irad[i];
+        const double ir = d.visc ? 1.0 / C.r : 0.0;
+        const double lr = a.lam[m], lu = a.lam[P + m], lv = a.lam[2 * P + m];
+        // o.r = C.r, o.u = C.u + (C.v^2 ix + vx ir + gx) dt, o.v = C.v + (vy ir + gy) dt
+        a.lam_in[m] = lr - (lu * vx + lv * vy) * dt * ir * ir;
+        a.lam_in[P + m] = lu;
+        a.lam_in[2 * P + m] = lv + lu * dt * 2.0 * C.v * ix;
+        if (d.visc) {
+            const double bvx = lu * dt * ir + a.lamv[m], bvy = lv * dt * ir + a.lamv[P + m];
+            double bu[9] = {}, bv[9] = {}, bn[9] = {};
+            rev::viscous_rev(d.visx + 5 * i, d.visy + 4 * j, u, v, nr, bvx, bvy, bu, bv, bn);
+            double* o = buf + (size_t)m * RK1_STEN;
+            for (int k = 0; k < 9; ++k) {
+                o[3 * k] = bn[k] * nu[k % 3];
+                o[3 * k + 1] = bu[k];
+                o[3 * k + 2] = bv[k];
+            }
+        }
+    }
+}
+
+__global__ void __launch_bounds__(ADJ_THREADS) k_rk1_gather(const Args a, const double* buf) {
+    const DiskView& d = a.d;
+    const long long n = (long long)d.xres * d.yres;
+    const size_t P = plane(d);
+    for (long long m = blockIdx.x * (long long)blockDim.x + threadIdx.x; m < n; m += (long long)gridDim.x * blockDim.x) {
+        const int i = NPAD + (int)(m % d.xres), j = d.ypad + (int)(m / d.xres);
+        double acc[3] = {0.0, 0.0, 0.0};
+        for (int k = 0; k < 9; ++k) {
+            int dx, dy;
+            nb(k, dx, dy);
+            const int oi = i - dx;  // the output whose stencil slot k is this cell
+            if (oi < NPAD || oi >= NPAD + d.xres) continue;
+            const double* o = buf + pidx(d, oi, wrap_row(d, j - dy)) * RK1_STEN + 3 * k;
+            acc[0] += o[0];
+            acc[1] += o[1];
+            acc[2] += o[2];
+        }
+        a.lam_in[m] += acc[0];
+        a.lam_in[P + m] += acc[1];
+        a.lam_in[2 * P + m] += acc[2];
+    }
+}
+
 // kick2.  The corrector at each output is transposed per cell (k_adj_k2a: the
 // direct adjoint of C and lambda of the viscous force it reads); the force is a
 // function of the predicted 3x3 stencil, and each predicted cell of its own
@@ -1415,6 +1490,9 @@ static void launch_pass(const Args& a, bool theta, double* scratch, double* rev,
             return;  // theta done by the reverse kernels
         }
         k_adj_flux<DIR><<<g, ADJ_THREADS, 0, s>>>(a, scratch);
+    } else if (PASS == P_K1 && rev) {
+        k_rk1_cell<<<g, ADJ_THREADS, 0, s>>>(a, rev);
+        if (a.d.visc) k_rk1_gather<<<g, ADJ_THREADS, 0, s>>>(a, rev);
     } else if (PASS == P_ADV && rev) {
         k_radv_upd<<<g, ADJ_THREADS, 0, s>>>(a, scratch);
         k_radv_face<<<g, ADJ_THREADS, 0, s>>>(a, scratch, rev, theta);
@@ -1622,7 +1700,8 @@ pg_status pg_adj_create(const pg_params* P, int device, void* stream, int checkp
     {
         const size_t nx = (size_t)P->xres, ny = (size_t)P->yres;
         const size_t cells = std::max(ny * (nx + 2), nx * (ny + 2));
-        if ((s = adj_alloc(a, &a->rev, cells * REV_SLOT * sizeof(double))) != PG_OK) return bail(s);
+        const size_t words = std::max(cells * REV_SLOT, nx * ny * (size_t)RK1_STEN);
+        if ((s = adj_alloc(a, &a->rev, words * sizeof(double))) != PG_OK) return bail(s);
     }
     if ((s = adj_make_disk(a)) != PG_OK) return bail(s);
     *out = a;

@@ -520,5 +520,71 @@ __device__ __forceinline__ void state_right_rev(double gam, double xl, double xr
     }
 }
 
+// ------------------------------------------------------------ viscosity
+// Adjoint of viscous() (viscosity.cu:84-194, 2D polar): the force is bilinear
+// in nr = Sigma nu and the velocity derivatives.  Accumulates into bu[9],
+// bv[9], bnr[9] (stencil order of viscous()).
+__device__ __forceinline__ void viscous_rev(const double* __restrict__ X, const double* __restrict__ Y, const double* u,
+                                            const double* v, const double* nr, double bfx, double bfy, double* bu,
+                                            double* bv, double* bnr) {
+    const double i_r20 = X[0], i_r21 = X[1], i_r10 = X[2], i_hr20 = X[3], i_r1 = X[4];
+    const double i_t20 = Y[0], i_t21 = Y[1], i_t10 = Y[2], i_ht20 = Y[3];
+    const double dudx = (u[2] - u[0]) * i_r20;
+    const double d2udx2 = ((u[2] - u[1]) * i_r21 - (u[1] - u[0]) * i_r10) * i_hr20;
+    const double dndx = (nr[2] - nr[0]) * i_r20;
+    const double dvdx = (v[2] - v[0]) * i_r20;
+    const double d2vdx2 = ((v[2] - v[1]) * i_r21 - (v[1] - v[0]) * i_r10) * i_hr20;
+    const double dvdy = (v[7] - v[4]) * i_t20 * i_r1;
+    const double d2vdy2 = ((v[7] - v[1]) * i_t21 - (v[1] - v[4]) * i_t10) * i_ht20 * i_r1 * i_r1;
+    const double d2vdxy = (v[8] - v[6] - v[5] + v[3]) * i_r20 * i_t20 * i_r1;
+    const double dudy = (u[7] - u[4]) * i_t20 * i_r1;
+    const double d2udy2 = ((u[7] - u[1]) * i_t21 - (u[1] - u[4]) * i_t10) * i_ht20 * i_r1 * i_r1;
+    const double d2udxy = (u[8] - u[6] - u[5] + u[3]) * i_r20 * i_t20 * i_r1;
+    const double dndy = (nr[7] - nr[4]) * i_t20 * i_r1;
+    const double n1 = nr[1], u1 = u[1], v1 = v[1];
+    const double a = bfx, b = bfy;
+    // adjoints of the derivatives and of the middle values
+    const double b_dndx = a * 2.0 * dudx + b * ((dudy + dvdx) - v1 * i_r1);
+    const double b_dudx = a * (2.0 * dndx + 2.0 * n1 * i_r1);
+    const double b_d2udx2 = a * 2.0 * n1;
+    const double b_dndy = a * ((dudy + dvdx) - v1 * i_r1) + b * (2.0 * dvdy + 2.0 * u1 * i_r1);
+    const double b_dudy = a * dndy + b * (dndx + 4.0 * n1 * i_r1);
+    const double b_dvdx = a * dndy + b * (dndx + n1 * i_r1);
+    const double b_d2udy2 = a * n1, b_d2vdxy = a * n1;
+    const double b_dvdy = -3.0 * a * n1 * i_r1 + 2.0 * b * dndy;
+    const double b_d2vdy2 = b * 2.0 * n1;
+    const double b_d2udxy = b * n1, b_d2vdx2 = b * n1;
+    bnr[1] += a * (2.0 * d2udx2 + 2.0 * dudx * i_r1 + (d2udy2 + d2vdxy) - dvdy * i_r1 -
+                   2.0 * (dvdy + u1 * i_r1) * i_r1) +
+              b * (2.0 * d2vdy2 + 2.0 * dudy * i_r1 + (d2udxy + d2vdx2) - dvdx * i_r1 + v1 * i_r1 * i_r1 +
+                   2.0 * (dudy + dvdx - v1 * i_r1) * i_r1);
+    bu[1] += -a * 2.0 * n1 * i_r1 * i_r1 + b * 2.0 * dndy * i_r1;
+    bv[1] += -a * dndy * i_r1 + b * (-dndx * i_r1 - n1 * i_r1 * i_r1);
+    // the difference stencils
+    const double K = i_ht20 * i_r1 * i_r1, L = i_r20 * i_t20 * i_r1, M = i_t20 * i_r1;
+    bu[2] += b_dudx * i_r20 + b_d2udx2 * i_r21 * i_hr20;
+    bu[0] += -b_dudx * i_r20 + b_d2udx2 * i_r10 * i_hr20;
+    bu[1] += -b_d2udx2 * (i_r21 + i_r10) * i_hr20 - b_d2udy2 * (i_t21 + i_t10) * K;
+    bu[7] += b_dudy * M + b_d2udy2 * i_t21 * K;
+    bu[4] += -b_dudy * M + b_d2udy2 * i_t10 * K;
+    bu[8] += b_d2udxy * L;
+    bu[6] -= b_d2udxy * L;
+    bu[5] -= b_d2udxy * L;
+    bu[3] += b_d2udxy * L;
+    bv[2] += b_dvdx * i_r20 + b_d2vdx2 * i_r21 * i_hr20;
+    bv[0] += -b_dvdx * i_r20 + b_d2vdx2 * i_r10 * i_hr20;
+    bv[1] += -b_d2vdx2 * (i_r21 + i_r10) * i_hr20 - b_d2vdy2 * (i_t21 + i_t10) * K;
+    bv[7] += b_dvdy * M + b_d2vdy2 * i_t21 * K;
+    bv[4] += -b_dvdy * M + b_d2vdy2 * i_t10 * K;
+    bv[8] += b_d2vdxy * L;
+    bv[6] -= b_d2vdxy * L;
+    bv[5] -= b_d2vdxy * L;
+    bv[3] += b_d2vdxy * L;
+    bnr[2] += b_dndx * i_r20;
+    bnr[0] -= b_dndx * i_r20;
+    bnr[7] += b_dndy * M;
+    bnr[4] -= b_dndy * M;
+}
+
 }  // namespace rev
 }  // namespace pg
