@@ -1144,6 +1144,162 @@ __global__ void __launch_bounds__(ADJ_THREADS) k_rk1_gather(const Args a, const 
     }
 }
 
+// Reverse of kick() (sweeps.cu:597-711 as restated above): the adjoints of the
+// cell, of the viscous force (vx, vy) and of the gravity (gx, gy) from the
+// adjoint (lr, lu, lv) of the kicked cell.
+struct KickAdj {
+    double r, u, v, vx, vy, gx, gy;
+};
+__device__ __forceinline__ KickAdj kick_rev(bool visc, const S3<double>& C, double gy, double vx, double vy, double ix,
+                                            double mdt, double dt, double lr, double lu, double lv) {
+    KickAdj b{0.0, lu, lv, 0.0, 0.0, lu * dt, lv * dt};
+    const double ir = visc ? 1.0 / C.r : 0.0;
+    double b_ir = 0.0;
+    const double b_fx = lu * dt, b_fy = lv * dt;
+    if (mdt != 0.0) {
+        const double fy0 = visc ? vy * ir : 0.0;
+        const double tv = C.v + fy0 * mdt + gy * mdt;
+        const double b_tv = b_fx * 2.0 * tv * ix;
+        b.v += b_tv;
+        b.gy += b_tv * mdt;
+        if (visc) {
+            const double b_fy0 = b_tv * mdt;
+            b.vy += b_fy0 * ir;
+            b_ir += b_fy0 * vy;
+        }
+    } else {
+        b.v += b_fx * 2.0 * C.v * ix;
+    }
+    if (visc) {
+        b.vx += b_fx * ir;
+        b_ir += b_fx * vx;
+        b.vy += b_fy * ir;
+        b_ir += b_fy * vy;
+    }
+    b.r = lr - b_ir * ir * ir;
+    return b;
+}
+
+// theta derivative of the gravity of body `which` at (i, j), contracted with (bgx, bgy)
+__device__ __forceinline__ void gravity_theta(const Args& a, int i, int j, int which, double bgx, double bgy,
+                                              double* acc) {
+    for (int th = 0; th < 3; th += 2) {  // q (planet mass) and h (smoothing); alpha does not enter
+        Dual gx, gy;
+        gravity<Dual>(a, Seed{-1, -1, -1, th}, i, j, which, gx, gy);
+        acc[th] += bgx * gx.d + bgy * gy.d;
+    }
+}
+
+// kick2 in reverse mode (same buffer).  Per output cell (k_rk2_cell): the
+// corrector's adjoint into lam_in; with viscosity, the reverse of the viscous
+// force over the 3x3 stencil of predicted states: their adjoints, 27 values per
+// output.  Per input cell (k_rk2_gather): the predicted-state adjoint gathered
+// from the 9 outputs, then the reverse of the predictor: lam_in of the cell and
+// lamv_in of kick1's force.  theta: gravity (q, h) of both half-kicks, nu in the
+// force, the bound-0 ghosts' init_C.
+__global__ void __launch_bounds__(ADJ_THREADS) k_rk2_cell(const Args a, double* buf, bool theta) {
+    const DiskView& d = a.d;
+    const long long n = (long long)d.xres * d.yres;
+    const size_t P = plane(d);
+    const Seed s0{-1, -1, -1, -1};
+    const double h = 0.5 * a.dt;
+    double acc[3] = {0.0, 0.0, 0.0};
+    for (long long m = blockIdx.x * (long long)blockDim.x + threadIdx.x; m < n; m += (long long)gridDim.x * blockDim.x) {
+        const int i = NPAD + (int)(m % d.xres), j = d.ypad + (int)(m / d.xres);
+        double vx = 0.0, vy = 0.0, nu[3], u[9], v[9], nr[9], rX[9];
+        if (d.visc) {
+            for (int k = 0; k < 3; ++k) nu[k] = d.nux[i + k - 1];
+            for (int k = 0; k < 9; ++k) {
+                int dx, dy;
+                nb(k, dx, dy);
+                const int ii = i + dx, jj = j + dy;
+                S3<double> X = ld<double>(a, s0, ii, jj);
+                if (ii >= NPAD && ii < NPAD + d.xres) {
+                    double ox, oy, gx, gy;
+                    ld_vis<double>(a, s0, ii, jj, ox, oy);
+                    gravity<double>(a, s0, ii, jj, 1, gx, gy);
+                    X = kick<double>(d, X, gx, gy, ox, oy, d.irad[ii], h, h);
+                }
+                rX[k] = X.r;
+                nr[k] = X.r * nu[k % 3];
+                u[k] = X.u;
+                v[k] = X.v;
+            }
+            viscous<double>(d.visx + 5 * i, d.visy + 4 * j, u, v, nr, vx, vy);
+        }
+        double gx, gy;
+        gravity<double>(a, s0, i, j, 1, gx, gy);
+        const S3<double> C = ld<double>(a, s0, i, j);
+        const KickAdj b = kick_rev(d.visc, C, gy, vx, vy, d.irad[i], h, h, a.lam[m], a.lam[P + m], a.lam[2 * P + m]);
+        a.lam_in[m] = b.r;
+        a.lam_in[P + m] = b.u;
+        a.lam_in[2 * P + m] = b.v;
+        if (theta) gravity_theta(a, i, j, 1, b.gx, b.gy, acc);
+        if (d.visc) {
+            double bu[9] = {}, bv[9] = {}, bn[9] = {};
+            rev::viscous_rev(d.visx + 5 * i, d.visy + 4 * j, u, v, nr, b.vx, b.vy, bu, bv, bn);
+            double* o = buf + (size_t)m * RK1_STEN;
+            for (int k = 0; k < 9; ++k) {
+                o[3 * k] = bn[k] * nu[k % 3];
+                o[3 * k + 1] = bu[k];
+                o[3 * k + 2] = bv[k];
+            }
+            if (theta) {
+                for (int th = 0; th < 3; ++th) {
+                    const double* dt = a.dtab + (size_t)th * NTAB * d.xarr;
+                    double g = 0.0;
+                    for (int k = 0; k < 9; ++k) {
+                        int dx, dy;
+                        nb(k, dx, dy);
+                        const int ii = i + dx;
+                        g += bn[k] * rX[k] * dt[T_NU * d.xarr + ii];
+                        if (ii < NPAD || ii >= NPAD + d.xres)  // radial ghost: init_C
+                            g += bu[k] * dt[T_U0 * d.xarr + ii] + bv[k] * dt[T_V0 * d.xarr + ii];
+                    }
+                    acc[th] += g;
+                }
+            }
+        }
+    }
+    if (theta) block_add3(acc, a.gth);
+}
+
+__global__ void __launch_bounds__(ADJ_THREADS) k_rk2_gather(const Args a, const double* buf, bool theta) {
+    const DiskView& d = a.d;
+    const long long n = (long long)d.xres * d.yres;
+    const size_t P = plane(d);
+    const Seed s0{-1, -1, -1, -1};
+    const double h = 0.5 * a.dt;
+    double acc[3] = {0.0, 0.0, 0.0};
+    for (long long m = blockIdx.x * (long long)blockDim.x + threadIdx.x; m < n; m += (long long)gridDim.x * blockDim.x) {
+        const int i = NPAD + (int)(m % d.xres), j = d.ypad + (int)(m / d.xres);
+        double bX[3] = {0.0, 0.0, 0.0};
+        for (int k = 0; k < 9; ++k) {
+            int dx, dy;
+            nb(k, dx, dy);
+            const int oi = i - dx;
+            if (oi < NPAD || oi >= NPAD + d.xres) continue;
+            const double* o = buf + pidx(d, oi, wrap_row(d, j - dy)) * RK1_STEN + 3 * k;
+            bX[0] += o[0];
+            bX[1] += o[1];
+            bX[2] += o[2];
+        }
+        // the predictor X = kick(C, g, kick1's force, dt/2, dt/2)
+        const S3<double> C = ld<double>(a, s0, i, j);
+        double ox, oy, gx, gy;
+        ld_vis<double>(a, s0, i, j, ox, oy);
+        gravity<double>(a, s0, i, j, 1, gx, gy);
+        const KickAdj b = kick_rev(true, C, gy, ox, oy, d.irad[i], h, h, bX[0], bX[1], bX[2]);
+        a.lam_in[m] += b.r;
+        a.lam_in[P + m] += b.u;
+        a.lam_in[2 * P + m] += b.v;
+        a.lamv_in[m] = b.vx;
+        a.lamv_in[P + m] = b.vy;
+        if (theta) gravity_theta(a, i, j, 1, b.gx, b.gy, acc);
+    }
+    if (theta) block_add3(acc, a.gth);
+}
+
 // kick2.  The corrector at each output is transposed per cell (k_adj_k2a: the
 // direct adjoint of C and lambda of the viscous force it reads); the force is a
 // function of the predicted 3x3 stencil, and each predicted cell of its own
@@ -1493,6 +1649,10 @@ static void launch_pass(const Args& a, bool theta, double* scratch, double* rev,
     } else if (PASS == P_K1 && rev) {
         k_rk1_cell<<<g, ADJ_THREADS, 0, s>>>(a, rev);
         if (a.d.visc) k_rk1_gather<<<g, ADJ_THREADS, 0, s>>>(a, rev);
+    } else if (PASS == P_K2 && rev) {
+        k_rk2_cell<<<g, ADJ_THREADS, 0, s>>>(a, rev, theta);
+        if (a.d.visc) k_rk2_gather<<<g, ADJ_THREADS, 0, s>>>(a, rev, theta);
+        return;  // theta done by the reverse kernels
     } else if (PASS == P_ADV && rev) {
         k_radv_upd<<<g, ADJ_THREADS, 0, s>>>(a, scratch);
         k_radv_face<<<g, ADJ_THREADS, 0, s>>>(a, scratch, rev, theta);
