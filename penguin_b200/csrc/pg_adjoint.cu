@@ -591,58 +591,6 @@ __device__ __forceinline__ void sweep_D(const Args& a, int i, int j, const FluxT
     }
 }
 
-// per cell (i, j) of the pass input (pre-shift row for DIR 1): the direct
-// adjoint of Q into lam_in and lambda_D of the slots into lslot (3 planes)
-// theta: with the hand-written reverse, also the theta derivative of the update
-// itself (DIR 1: (rot + r Omega) D_Sigma in the v_phi slot).
-template <int DIR>
-__global__ void __launch_bounds__(ADJ_THREADS) k_adj_upd(const Args a, double* lslot, bool theta) {
-    const DiskView& d = a.d;
-    const long long n = (long long)d.xres * d.yres;
-    const size_t P = plane(d);
-    const Seed s0{-1, -1, -1, -1};
-    double acc[3] = {0.0, 0.0, 0.0};
-    for (long long m = blockIdx.x * (long long)blockDim.x + threadIdx.x; m < n; m += (long long)gridDim.x * blockDim.x) {
-        const int i = NPAD + (int)(m % d.xres), j = d.ypad + (int)(m / d.xres);
-        const size_t mo = (DIR == 1) ? pidx(d, i, sy_post_row(d, a.inc, i, j)) : (size_t)m;
-        const double lr = a.lam[mo], lu = a.lam[P + mo], lv = a.lam[2 * P + mo];
-        FluxT<double> F0, F1;
-        if (DIR == 0) {
-            F0 = face_flux<double, 0>(a, s0, i, j);
-            F1 = face_flux<double, 0>(a, s0, i + 1, j);
-        } else {
-            F0 = face_flux<double, 1>(a, s0, j, i);
-            F1 = face_flux<double, 1>(a, s0, j + 1, i);
-        }
-        double Dr, D1, D2;
-        sweep_D<DIR>(a, i, j, F0, F1, Dr, D1, D2);
-        const S3<double> Q = ld<double>(a, s0, i, j);
-        double g[6];
-#pragma unroll
-        for (int k = 0; k < 6; ++k) {
-            S3<Dual> q{Q.r, Q.p, Q.u, Q.v};
-            Dual r = Dr, u1 = D1, u2 = D2;
-            if (k == 0) q.r.d = 1.0;
-            else if (k == 1) q.u.d = 1.0;
-            else if (k == 2) q.v.d = 1.0;
-            else if (k == 3) r.d = 1.0;
-            else if (k == 4) u1.d = 1.0;
-            else u2.d = 1.0;
-            const S3<Dual> o = update_iso<Dual>(q, r, u1, u2);
-            g[k] = lr * o.r.d + lu * o.u.d + lv * o.v.d;
-        }
-        a.lam_in[m] = g[0];
-        a.lam_in[P + m] = g[1];
-        a.lam_in[2 * P + m] = g[2];
-        lslot[m] = g[3];
-        lslot[P + m] = g[4];
-        lslot[2 * P + m] = g[5];
-        if (DIR == 1 && theta)
-            for (int th = 0; th < 3; ++th) acc[th] += g[5] * Dr * a.dtab[((size_t)th * NTAB + T_ROT) * d.xarr + i];
-    }
-    if (theta) block_add3(acc, a.gth);
-}
-
 // lambda of the flux of face f of a pencil (between pencil cells f-1 and f) from
 // lambda_D of its two cells; position f along the pencil, q the pencil
 template <int DIR>
@@ -725,15 +673,151 @@ __global__ void __launch_bounds__(ADJ_THREADS) k_adj_flux(const Args a, const do
 // periodic, covers each of the yres faces of a column once, its adjoint
 // collected from both neighbouring cells like face_lambda, so every interior
 // cell owns both of its half-states and ghost-row stencil entries wrap.
-// Buffer per pencil: (n + 2) cells x (8 half-state adjoints + 15 stencil
-// adjoints).
-constexpr int REV_HALF = 8, REV_STEN = 15, REV_SLOT = REV_HALF + REV_STEN;
+// Before them, the cells' half-states (k_rev_states) and the face fluxes
+// (k_rev_flux) are formed once and kept, for the update's adjoint (k_adj_upd)
+// and the HLLC reverse.  Buffer per pencil: (n + 2) cells x (8 half-state
+// adjoints, 15 stencil adjoints, the two half-states (r, p, u and v for DIR 0,
+// w for DIR 1) and the flux of the cell's lower face (r, u, v or w, pres)).
+constexpr int REV_HALF = 8, REV_STEN = 15, REV_ST = REV_HALF + REV_STEN, REV_FX = REV_ST + 8, REV_SLOT = REV_FX + 4;
 
 template <int DIR>
 __device__ __forceinline__ void rev_dims(const DiskView& d, int& n, int& npen, int& p0) {
     n = (DIR == 0) ? d.xres : d.yres;
     npen = (DIR == 0) ? d.yres : d.xres;
     p0 = (DIR == 0) ? NPAD : d.ypad;
+}
+
+// the half-states of the cells that have them (see k_rev_face)
+template <int DIR>
+__global__ void __launch_bounds__(ADJ_THREADS) k_rev_states(const Args a, double* buf) {
+    const DiskView& d = a.d;
+    int n, npen, p0;
+    rev_dims<DIR>(d, n, npen, p0);
+    const int nc = (DIR == 0) ? n + 2 : n;
+    const int c0 = (DIR == 0) ? p0 - 1 : p0;
+    const long long total = (long long)nc * npen;
+    const Seed s0{-1, -1, -1, -1};
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int pen = (int)(t / nc), c = c0 + (int)(t % nc);
+        const int q = ((DIR == 0) ? d.ypad : NPAD) + pen;
+        HalfT<double> L, R;
+        edge_states<double, DIR>(a, s0, c, q, L, R);
+        double* o = buf + ((size_t)pen * (n + 2) + (c - (p0 - 1))) * REV_SLOT + REV_ST;
+        o[0] = L.r;
+        o[1] = L.p;
+        o[2] = L.u;
+        o[3] = (DIR == 0) ? L.v : L.w;
+        o[4] = R.r;
+        o[5] = R.p;
+        o[6] = R.u;
+        o[7] = (DIR == 0) ? R.v : R.w;
+    }
+}
+
+template <int DIR>
+__device__ __forceinline__ Half rev_half(const double* o) {  // a stored half-state
+    return Half{o[0], o[1], o[2], DIR == 0 ? o[3] : 0.0, DIR == 0 ? 0.0 : o[3]};
+}
+
+// the pencil cell whose right half-state feeds face f from below (DIR 1: wrapped)
+template <int DIR>
+__device__ __forceinline__ int rev_below(const DiskView& d, int f) {
+    return (DIR == 0) ? f - 1 : wrap_row(d, f - 1);
+}
+
+// HLLC at every face of the pencils from the stored half-states
+template <int DIR>
+__global__ void __launch_bounds__(ADJ_THREADS) k_rev_flux(const Args a, double* buf) {
+    const DiskView& d = a.d;
+    int n, npen, p0;
+    rev_dims<DIR>(d, n, npen, p0);
+    const int nf = (DIR == 0) ? n + 1 : n;
+    const long long total = (long long)nf * npen;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int pen = (int)(t / nf), f = p0 + (int)(t % nf);
+        double* pb = buf + (size_t)pen * (n + 2) * REV_SLOT;
+        const Half L = rev_half<DIR>(pb + (size_t)(rev_below<DIR>(d, f) - (p0 - 1)) * REV_SLOT + REV_ST + 4);
+        double* o = pb + (size_t)(f - (p0 - 1)) * REV_SLOT;
+        const Half R = rev_half<DIR>(o + REV_ST);
+        const Flux F = hllc<double>(0, d.ie, d.gam, L, R);
+        o[REV_FX] = F.r;
+        o[REV_FX + 1] = F.u;
+        o[REV_FX + 2] = (DIR == 0) ? F.v : F.w;
+        o[REV_FX + 3] = F.pres;
+    }
+}
+
+// the flux of face f of pencil q kept by k_rev_flux (DIR 1: face p0 + n is face p0)
+template <int DIR>
+__device__ __forceinline__ FluxT<double> rev_flux(const DiskView& d, const double* buf, int f, int q) {
+    int n, npen, p0;
+    rev_dims<DIR>(d, n, npen, p0);
+    if (DIR == 1 && f >= p0 + n) f -= n;
+    const int pen = q - ((DIR == 0) ? d.ypad : NPAD);
+    const double* o = buf + ((size_t)pen * (n + 2) + (f - (p0 - 1))) * REV_SLOT + REV_FX;
+    FluxT<double> F{o[0], 0.0, o[1], 0.0, 0.0, o[3], 0.0};
+    if (DIR == 0) F.v = o[2];
+    else F.w = o[2];
+    return F;
+}
+
+// per cell (i, j) of the pass input (pre-shift row for DIR 1): the direct
+// adjoint of Q into lam_in and lambda_D of the slots into lslot (3 planes)
+// theta: with the hand-written reverse, also the theta derivative of the update
+// itself (DIR 1: (rot + r Omega) D_Sigma in the v_phi slot).  rbuf: the face
+// fluxes kept by k_rev_flux, or null to evaluate them here.
+template <int DIR>
+__global__ void __launch_bounds__(ADJ_THREADS) k_adj_upd(const Args a, double* lslot, bool theta, const double* rbuf) {
+    const DiskView& d = a.d;
+    const long long n = (long long)d.xres * d.yres;
+    const size_t P = plane(d);
+    const Seed s0{-1, -1, -1, -1};
+    double acc[3] = {0.0, 0.0, 0.0};
+    for (long long m = blockIdx.x * (long long)blockDim.x + threadIdx.x; m < n; m += (long long)gridDim.x * blockDim.x) {
+        const int i = NPAD + (int)(m % d.xres), j = d.ypad + (int)(m / d.xres);
+        const size_t mo = (DIR == 1) ? pidx(d, i, sy_post_row(d, a.inc, i, j)) : (size_t)m;
+        const double lr = a.lam[mo], lu = a.lam[P + mo], lv = a.lam[2 * P + mo];
+        FluxT<double> F0, F1;
+        if (rbuf) {
+            const int c = (DIR == 0) ? i : j, q = (DIR == 0) ? j : i;
+            F0 = rev_flux<DIR>(d, rbuf, c, q);
+            F1 = rev_flux<DIR>(d, rbuf, c + 1, q);
+        } else if (DIR == 0) {
+            F0 = face_flux<double, 0>(a, s0, i, j);
+            F1 = face_flux<double, 0>(a, s0, i + 1, j);
+        } else {
+            F0 = face_flux<double, 1>(a, s0, j, i);
+            F1 = face_flux<double, 1>(a, s0, j + 1, i);
+        }
+        double Dr, D1, D2;
+        sweep_D<DIR>(a, i, j, F0, F1, Dr, D1, D2);
+        const S3<double> Q = ld<double>(a, s0, i, j);
+        double g[6];
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+            S3<Dual> q{Q.r, Q.p, Q.u, Q.v};
+            Dual r = Dr, u1 = D1, u2 = D2;
+            if (k == 0) q.r.d = 1.0;
+            else if (k == 1) q.u.d = 1.0;
+            else if (k == 2) q.v.d = 1.0;
+            else if (k == 3) r.d = 1.0;
+            else if (k == 4) u1.d = 1.0;
+            else u2.d = 1.0;
+            const S3<Dual> o = update_iso<Dual>(q, r, u1, u2);
+            g[k] = lr * o.r.d + lu * o.u.d + lv * o.v.d;
+        }
+        a.lam_in[m] = g[0];
+        a.lam_in[P + m] = g[1];
+        a.lam_in[2 * P + m] = g[2];
+        lslot[m] = g[3];
+        lslot[P + m] = g[4];
+        lslot[2 * P + m] = g[5];
+        if (DIR == 1 && theta)
+            for (int th = 0; th < 3; ++th) acc[th] += g[5] * Dr * a.dtab[((size_t)th * NTAB + T_ROT) * d.xarr + i];
+    }
+    if (theta) block_add3(acc, a.gth);
 }
 
 // Adjoint of both edge states of pencil cell c (the v slot of DIR 0, the w slot
@@ -848,19 +932,17 @@ __global__ void __launch_bounds__(ADJ_THREADS) k_rev_face(const Args a, const do
     rev_dims<DIR>(d, n, npen, p0);
     const int nf = (DIR == 0) ? n + 1 : n;  // faces per pencil
     const long long total = (long long)nf * npen;
-    const Seed s0{-1, -1, -1, -1};
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
          t += (long long)gridDim.x * blockDim.x) {
         const int pen = (int)(t / nf), f = p0 + (int)(t % nf);
         const int q = ((DIR == 0) ? d.ypad : NPAD) + pen;
         const FluxT<double> LF = face_lambda<DIR>(a, lslot, f, q);
-        HalfT<double> l0, r0, l1, r1;
-        edge_states<double, DIR>(a, s0, f - 1, q, l0, r0);
-        edge_states<double, DIR>(a, s0, f, q, l1, r1);
+        double* pb = buf + (size_t)pen * (n + 2) * REV_SLOT;
+        const Half r0 = rev_half<DIR>(pb + (size_t)(rev_below<DIR>(d, f) - (p0 - 1)) * REV_SLOT + REV_ST + 4);
+        const Half l1 = rev_half<DIR>(pb + (size_t)(f - (p0 - 1)) * REV_SLOT + REV_ST);
         const double bF[5] = {LF.r, LF.u, LF.v, LF.w, LF.pres};
         Half bL{0.0, 0.0, 0.0, 0.0, 0.0}, bR{0.0, 0.0, 0.0, 0.0, 0.0};
         rev::hllc_rev(d.gam, r0, l1, bF, bL, bR);
-        double* pb = buf + (size_t)pen * (n + 2) * REV_SLOT;
         // the right half-state of cell f - 1 (DIR 1: wrapped to its interior row)
         const int cm = (DIR == 0) ? f - 1 : wrap_row(d, f - 1);
         double* o = pb + (size_t)(cm - (p0 - 1)) * REV_SLOT;
@@ -1069,81 +1151,6 @@ __global__ void __launch_bounds__(ADJ_THREADS) k_radv_gather(const Args a, const
     }
 }
 
-// kick1 in reverse mode (same buffer).  Per output cell (k_rk1_cell): the
-// pointwise adjoint of the half-kick (mdt = 0) into lam_in, and the adjoint of
-// its viscous force (from the kick and from kick2's use of the force, lamv)
-// through the reverse of the viscous stencil: 9 cells x 3 state variables per
-// output cell.  Per input cell (k_rk1_gather): the stencil adjoints of the 9
-// outputs whose stencil holds it (periodic rows wrap; the constant bound-0
-// ghost columns drop out).  theta stays with k_adj_theta.
-constexpr int RK1_STEN = 27;
-
-__global__ void __launch_bounds__(ADJ_THREADS) k_rk1_cell(const Args a, double* buf) {
-    const DiskView& d = a.d;
-    const long long n = (long long)d.xres * d.yres;
-    const size_t P = plane(d);
-    const Seed s0{-1, -1, -1, -1};
-    const double dt = 0.5 * a.dt;
-    for (long long m = blockIdx.x * (long long)blockDim.x + threadIdx.x; m < n; m += (long long)gridDim.x * blockDim.x) {
-        const int i = NPAD + (int)(m % d.xres), j = d.ypad + (int)(m / d.xres);
-        const S3<double> C = ld<double>(a, s0, i, j);
-        double vx = 0.0, vy = 0.0, nu[3], u[9], v[9], nr[9];
-        if (d.visc) {
-            for (int k = 0; k < 3; ++k) nu[k] = d.nux[i + k - 1];
-            for (int k = 0; k < 9; ++k) {
-                int dx, dy;
-                nb(k, dx, dy);
-                const S3<double> X = ld<double>(a, s0, i + dx, j + dy);
-                nr[k] = X.r * nu[k % 3];
-                u[k] = X.u;
-                v[k] = X.v;
-            }
-            viscous<double>(d.visx + 5 * i, d.visy + 4 * j, u, v, nr, vx, vy);
-        }
-        const double ix = d.irad[i];
-        const double ir = d.visc ? 1.0 / C.r : 0.0;
-        const double lr = a.lam[m], lu = a.lam[P + m], lv = a.lam[2 * P + m];
-        // o.r = C.r, o.u = C.u + (C.v^2 ix + vx ir + gx) dt, o.v = C.v + (vy ir + gy) dt
-        a.lam_in[m] = lr - (lu * vx + lv * vy) * dt * ir * ir;
-        a.lam_in[P + m] = lu;
-        a.lam_in[2 * P + m] = lv + lu * dt * 2.0 * C.v * ix;
-        if (d.visc) {
-            const double bvx = lu * dt * ir + a.lamv[m], bvy = lv * dt * ir + a.lamv[P + m];
-            double bu[9] = {}, bv[9] = {}, bn[9] = {};
-            rev::viscous_rev(d.visx + 5 * i, d.visy + 4 * j, u, v, nr, bvx, bvy, bu, bv, bn);
-            double* o = buf + (size_t)m * RK1_STEN;
-            for (int k = 0; k < 9; ++k) {
-                o[3 * k] = bn[k] * nu[k % 3];
-                o[3 * k + 1] = bu[k];
-                o[3 * k + 2] = bv[k];
-            }
-        }
-    }
-}
-
-__global__ void __launch_bounds__(ADJ_THREADS) k_rk1_gather(const Args a, const double* buf) {
-    const DiskView& d = a.d;
-    const long long n = (long long)d.xres * d.yres;
-    const size_t P = plane(d);
-    for (long long m = blockIdx.x * (long long)blockDim.x + threadIdx.x; m < n; m += (long long)gridDim.x * blockDim.x) {
-        const int i = NPAD + (int)(m % d.xres), j = d.ypad + (int)(m / d.xres);
-        double acc[3] = {0.0, 0.0, 0.0};
-        for (int k = 0; k < 9; ++k) {
-            int dx, dy;
-            nb(k, dx, dy);
-            const int oi = i - dx;  // the output whose stencil slot k is this cell
-            if (oi < NPAD || oi >= NPAD + d.xres) continue;
-            const double* o = buf + pidx(d, oi, wrap_row(d, j - dy)) * RK1_STEN + 3 * k;
-            acc[0] += o[0];
-            acc[1] += o[1];
-            acc[2] += o[2];
-        }
-        a.lam_in[m] += acc[0];
-        a.lam_in[P + m] += acc[1];
-        a.lam_in[2 * P + m] += acc[2];
-    }
-}
-
 // Reverse of kick() (sweeps.cu:597-711 as restated above): the adjoints of the
 // cell, of the viscous force (vx, vy) and of the gravity (gx, gy) from the
 // adjoint (lr, lu, lv) of the kicked cell.
@@ -1180,6 +1187,27 @@ __device__ __forceinline__ KickAdj kick_rev(bool visc, const S3<double>& C, doub
     return b;
 }
 
+// theta derivative of a viscous force through nu (tab T_NU) and the bound-0
+// ghosts' init_C in its 3x3 stencil around column i, contracted with the
+// stencil adjoints bu, bv, bn (of u, v and nr = Sigma nu); rX: the stencil's Sigma
+__device__ __forceinline__ void stencil_theta(const Args& a, int i, const double* bu, const double* bv,
+                                              const double* bn, const double* rX, double* acc) {
+    const DiskView& d = a.d;
+    for (int th = 0; th < 3; ++th) {
+        const double* dt = a.dtab + (size_t)th * NTAB * d.xarr;
+        double g = 0.0;
+        for (int k = 0; k < 9; ++k) {
+            int dx, dy;
+            nb(k, dx, dy);
+            const int ii = i + dx;
+            g += bn[k] * rX[k] * dt[T_NU * d.xarr + ii];
+            if (ii < NPAD || ii >= NPAD + d.xres)  // radial ghost: init_C
+                g += bu[k] * dt[T_U0 * d.xarr + ii] + bv[k] * dt[T_V0 * d.xarr + ii];
+        }
+        acc[th] += g;
+    }
+}
+
 // theta derivative of the gravity of body `which` at (i, j), contracted with (bgx, bgy)
 __device__ __forceinline__ void gravity_theta(const Args& a, int i, int j, int which, double bgx, double bgy,
                                               double* acc) {
@@ -1187,6 +1215,86 @@ __device__ __forceinline__ void gravity_theta(const Args& a, int i, int j, int w
         Dual gx, gy;
         gravity<Dual>(a, Seed{-1, -1, -1, th}, i, j, which, gx, gy);
         acc[th] += bgx * gx.d + bgy * gy.d;
+    }
+}
+
+// kick1 in reverse mode (same buffer).  Per output cell (k_rk1_cell): the
+// pointwise adjoint of the half-kick (mdt = 0) into lam_in, and the adjoint of
+// its viscous force (from the kick and from kick2's use of the force, lamv)
+// through the reverse of the viscous stencil: 9 cells x 3 state variables per
+// output cell.  Per input cell (k_rk1_gather): the stencil adjoints of the 9
+// outputs whose stencil holds it (periodic rows wrap; the constant bound-0
+// ghost columns drop out).  theta: gravity (q, h), nu, the ghosts' init_C.
+constexpr int RK1_STEN = 27;
+
+__global__ void __launch_bounds__(ADJ_THREADS) k_rk1_cell(const Args a, double* buf, bool theta) {
+    const DiskView& d = a.d;
+    const long long n = (long long)d.xres * d.yres;
+    const size_t P = plane(d);
+    const Seed s0{-1, -1, -1, -1};
+    const double dt = 0.5 * a.dt;
+    double acc[3] = {0.0, 0.0, 0.0};
+    for (long long m = blockIdx.x * (long long)blockDim.x + threadIdx.x; m < n; m += (long long)gridDim.x * blockDim.x) {
+        const int i = NPAD + (int)(m % d.xres), j = d.ypad + (int)(m / d.xres);
+        const S3<double> C = ld<double>(a, s0, i, j);
+        double vx = 0.0, vy = 0.0, nu[3], u[9], v[9], nr[9], rX[9];
+        if (d.visc) {
+            for (int k = 0; k < 3; ++k) nu[k] = d.nux[i + k - 1];
+            for (int k = 0; k < 9; ++k) {
+                int dx, dy;
+                nb(k, dx, dy);
+                const S3<double> X = ld<double>(a, s0, i + dx, j + dy);
+                rX[k] = X.r;
+                nr[k] = X.r * nu[k % 3];
+                u[k] = X.u;
+                v[k] = X.v;
+            }
+            viscous<double>(d.visx + 5 * i, d.visy + 4 * j, u, v, nr, vx, vy);
+        }
+        const double ix = d.irad[i];
+        const double ir = d.visc ? 1.0 / C.r : 0.0;
+        const double lr = a.lam[m], lu = a.lam[P + m], lv = a.lam[2 * P + m];
+        if (theta) gravity_theta(a, i, j, 0, lu * dt, lv * dt, acc);
+        // o.r = C.r, o.u = C.u + (C.v^2 ix + vx ir + gx) dt, o.v = C.v + (vy ir + gy) dt
+        a.lam_in[m] = lr - (lu * vx + lv * vy) * dt * ir * ir;
+        a.lam_in[P + m] = lu;
+        a.lam_in[2 * P + m] = lv + lu * dt * 2.0 * C.v * ix;
+        if (d.visc) {
+            const double bvx = lu * dt * ir + a.lamv[m], bvy = lv * dt * ir + a.lamv[P + m];
+            double bu[9] = {}, bv[9] = {}, bn[9] = {};
+            rev::viscous_rev(d.visx + 5 * i, d.visy + 4 * j, u, v, nr, bvx, bvy, bu, bv, bn);
+            double* o = buf + (size_t)m * RK1_STEN;
+            for (int k = 0; k < 9; ++k) {
+                o[3 * k] = bn[k] * nu[k % 3];
+                o[3 * k + 1] = bu[k];
+                o[3 * k + 2] = bv[k];
+            }
+            if (theta) stencil_theta(a, i, bu, bv, bn, rX, acc);
+        }
+    }
+    if (theta) block_add3(acc, a.gth);
+}
+
+__global__ void __launch_bounds__(ADJ_THREADS) k_rk1_gather(const Args a, const double* buf) {
+    const DiskView& d = a.d;
+    const long long n = (long long)d.xres * d.yres;
+    const size_t P = plane(d);
+    for (long long m = blockIdx.x * (long long)blockDim.x + threadIdx.x; m < n; m += (long long)gridDim.x * blockDim.x) {
+        const int i = NPAD + (int)(m % d.xres), j = d.ypad + (int)(m / d.xres);
+        double acc[3] = {0.0, 0.0, 0.0};
+        for (int k = 0; k < 9; ++k) {
+            int dx, dy;
+            nb(k, dx, dy);
+            const int oi = i - dx;  // the output whose stencil slot k is this cell
+            if (oi < NPAD || oi >= NPAD + d.xres) continue;
+            const double* o = buf + pidx(d, oi, wrap_row(d, j - dy)) * RK1_STEN + 3 * k;
+            acc[0] += o[0];
+            acc[1] += o[1];
+            acc[2] += o[2];
+        }
+        a.lam_in[m] += acc[0];
+        a.lam_in[P + m] += acc[1];
+        a.lam_in[2 * P + m] += acc[2];
     }
 }
 
@@ -1244,21 +1352,7 @@ __global__ void __launch_bounds__(ADJ_THREADS) k_rk2_cell(const Args a, double* 
                 o[3 * k + 1] = bu[k];
                 o[3 * k + 2] = bv[k];
             }
-            if (theta) {
-                for (int th = 0; th < 3; ++th) {
-                    const double* dt = a.dtab + (size_t)th * NTAB * d.xarr;
-                    double g = 0.0;
-                    for (int k = 0; k < 9; ++k) {
-                        int dx, dy;
-                        nb(k, dx, dy);
-                        const int ii = i + dx;
-                        g += bn[k] * rX[k] * dt[T_NU * d.xarr + ii];
-                        if (ii < NPAD || ii >= NPAD + d.xres)  // radial ghost: init_C
-                            g += bu[k] * dt[T_U0 * d.xarr + ii] + bv[k] * dt[T_V0 * d.xarr + ii];
-                    }
-                    acc[th] += g;
-                }
-            }
+            if (theta) stencil_theta(a, i, bu, bv, bn, rX, acc);
         }
     }
     if (theta) block_add3(acc, a.gth);
@@ -1637,18 +1731,22 @@ static void launch_pass(const Args& a, bool theta, double* scratch, double* rev,
     const unsigned g = grid_for(n);
     if (PASS == P_SX || PASS == P_SY) {
         constexpr int DIR = (PASS == P_SX) ? 0 : 1;
-        k_adj_upd<DIR><<<g, ADJ_THREADS, 0, s>>>(a, scratch, theta && rev);
         if (rev) {
             const long long pen = (DIR == 0) ? a.d.yres : a.d.xres, len = (DIR == 0) ? a.d.xres + 2 : a.d.yres;
+            k_rev_states<DIR><<<grid_for(pen * len), ADJ_THREADS, 0, s>>>(a, rev);
+            k_rev_flux<DIR><<<grid_for(pen * len), ADJ_THREADS, 0, s>>>(a, rev);
+            k_adj_upd<DIR><<<g, ADJ_THREADS, 0, s>>>(a, scratch, theta, rev);
             k_rev_face<DIR><<<grid_for(pen * len), ADJ_THREADS, 0, s>>>(a, scratch, rev);
             k_rev_cell<DIR><<<grid_for(pen * len), ADJ_THREADS, 0, s>>>(a, rev, theta);
             k_rev_gather<DIR><<<g, ADJ_THREADS, 0, s>>>(a, rev);
             return;  // theta done by the reverse kernels
         }
+        k_adj_upd<DIR><<<g, ADJ_THREADS, 0, s>>>(a, scratch, false, nullptr);
         k_adj_flux<DIR><<<g, ADJ_THREADS, 0, s>>>(a, scratch);
     } else if (PASS == P_K1 && rev) {
-        k_rk1_cell<<<g, ADJ_THREADS, 0, s>>>(a, rev);
+        k_rk1_cell<<<g, ADJ_THREADS, 0, s>>>(a, rev, theta);
         if (a.d.visc) k_rk1_gather<<<g, ADJ_THREADS, 0, s>>>(a, rev);
+        return;  // theta done by k_rk1_cell
     } else if (PASS == P_K2 && rev) {
         k_rk2_cell<<<g, ADJ_THREADS, 0, s>>>(a, rev, theta);
         if (a.d.visc) k_rk2_gather<<<g, ADJ_THREADS, 0, s>>>(a, rev, theta);
