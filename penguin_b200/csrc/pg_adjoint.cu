@@ -62,6 +62,7 @@ struct Args {
     const double* dtab;        // [3][NTAB][xarr]
     double* gth;               // 3 accumulators
     const double* dir;         // direction mode (Seed.i == DIRECTION): 5 interior planes r, u, v, vis x, vis y
+    const double* trig;        // per row: sin, cos of (azimuth - planet y) for pl[0], then pl[1] (k_adj_trig)
 };
 
 constexpr int DIRECTION = -2;  // Seed.i: every input cell moves along Args.dir (forward mode)
@@ -351,8 +352,7 @@ __device__ __forceinline__ void gravity(const Args& a, const Seed& s, int i, int
         T plm = p.m, rs = p.rs;
         if (s.th == 0) set_d(plm, a.dmdq[which]);
         if (s.th == 2) set_d(rs, a.drsdh);
-        double sinfac, cosfac;
-        sincos(d.ycj[j] - (p.y + 0.0 * p.vy), &sinfac, &cosfac);
+        const double sinfac = a.trig[4 * j + 2 * which], cosfac = a.trig[4 * j + 2 * which + 1];
         const double iplx2 = 1.0 / p.x / p.x;
         const double rad = d.radx[i], plx = p.x;
         const T Rp = sqrt(rad * rad + plx * plx - 2.0 * plx * rad * cosfac + rs * rs);
@@ -361,6 +361,14 @@ __device__ __forceinline__ void gravity(const Args& a, const Seed& s, int i, int
         gx += -plm * (rad - plx * cosfac) * rs_fac - plm * cosfac * iplx2;
         gy += -plm * plx * sinfac * rs_fac + plm * sinfac * iplx2;
     }
+}
+
+// the per-row angles of the step's two planets that gravity() reads
+__global__ void k_adj_trig(const DiskView d, pg_body p0, pg_body p1, double* trig) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= d.yarr) return;
+    sincos(d.ycj[j] - (p0.y + 0.0 * p0.vy), &trig[4 * j], &trig[4 * j + 1]);
+    sincos(d.ycj[j] - (p1.y + 0.0 * p1.vy), &trig[4 * j + 2], &trig[4 * j + 3]);
 }
 
 // apply_source_terms for one cell (sweeps.cu:597-711), geomx 1, 2D
@@ -1809,6 +1817,7 @@ struct pg_adj {
     Scalars* ssc = nullptr;  // scratch copy of the device scalars
     double* scratch = nullptr;  // 3 interior planes: lambda of the update slots / of kick1's force
     double* rev = nullptr;      // hand-written sweep reverse: REV_SLOT doubles per pencil cell
+    double* trig = nullptr;     // the planets' per-row angles of the step being transposed
     bool hand = true;           // sweeps in reverse mode (false: the dual-number kernels)
     size_t bytes = 0;
 
@@ -1960,6 +1969,7 @@ pg_status pg_adj_create(const pg_params* P, int device, void* stream, int checkp
         const size_t cells = std::max(ny * (nx + 2), nx * (ny + 2));
         const size_t words = std::max(cells * REV_SLOT, nx * ny * (size_t)RK1_STEN);
         if ((s = adj_alloc(a, &a->rev, words * sizeof(double))) != PG_OK) return bail(s);
+        if ((s = adj_alloc(a, &a->trig, 4 * (ny + 2 * NPAD) * sizeof(double))) != PG_OK) return bail(s);
     }
     if ((s = adj_make_disk(a)) != PG_OK) return bail(s);
     *out = a;
@@ -1988,6 +1998,7 @@ pg_status pg_adj_destroy(pg_adj* a) {
     cudaFree(a->ssc);
     cudaFree(a->scratch);
     cudaFree(a->rev);
+    cudaFree(a->trig);
     if (a->own_stream && a->stream) cudaStreamDestroy(a->stream);
     delete a;
     return PG_OK;
@@ -2074,6 +2085,8 @@ static Args base_args(pg_adj* a, int n, int slot, const pg_body* pl) {
     g.dt = a->dts[n];
     g.dtab = a->dtab;
     g.gth = a->gth;
+    g.trig = a->trig;
+    k_adj_trig<<<(g.d.yarr + 127) / 128, 128, 0, a->stream>>>(g.d, g.pl[0], g.pl[1], a->trig);
     return g;
 }
 
