@@ -254,6 +254,14 @@ int pg_ens_kernels_per_step(const pg_ens* e);
 /* As pg_disk_profile, for the whole ensemble (slots 0 clocks + planet tables,
    1 kick1, 2 sweep_x, 3 sweep_y, 4 advect, 5 kick2). */
 pg_status pg_ens_profile(pg_ens* e, int nsteps, double end_time, float* ms, int nslot);
+/* Launch-configuration autotuner of the five FP32 passes: for each pass the
+   compiled occupancy variant (0/1) and CTAs-per-SM cap (0 = none) with the
+   shortest time on the current state, `reps` launches per candidate.  The
+   state is not changed and results are bit for bit the same under any choice.
+   out10 (optional): variants of kick1, sweep x, sweep y, advect, kick2, then
+   their caps. */
+pg_status pg_ens_autotune(pg_ens* e, int reps, int* out10);
+pg_status pg_ens_set_tuning(pg_ens* e, const int* in10);
 
 /* ---------------------------------------------------------------- adjoint
  * Gradient of a loss on the surface density after N steps of the FP64 step

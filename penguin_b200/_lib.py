@@ -30,7 +30,7 @@ EXPORTS = [
     "pg_ens_check_params", "pg_ens_create", "pg_ens_destroy", "pg_ens_size", "pg_ens_dims", "pg_ens_set_state",
     "pg_ens_get_state", "pg_ens_run", "pg_ens_sync", "pg_ens_clock", "pg_ens_planet", "pg_ens_check",
     "pg_ens_totals", "pg_ens_torque", "pg_ens_kernels_per_step", "pg_ens_profile", "pg_ens_set_dust",
-    "pg_ens_get_dust",
+    "pg_ens_get_dust", "pg_ens_autotune", "pg_ens_set_tuning",
     "pg_adj_check_params", "pg_adj_create", "pg_adj_destroy", "pg_adj_set_params", "pg_adj_forward",
     "pg_adj_backward", "pg_adj_model_error", "pg_adj_dot_test", "pg_adj_pass_check", "pg_adj_replay_diff", "pg_adj_pass_fields", "pg_adj_schedule", "pg_adj_steps", "pg_adj_device_bytes", "pg_adj_set_sweep_reverse",
 ]
@@ -128,6 +128,8 @@ def lib() -> ctypes.CDLL:
         "pg_adj_set_sweep_reverse": (i, [vp, i]),
         "pg_ens_kernels_per_step": (i, [vp]),
         "pg_ens_profile": (i, [vp, i, d, ctypes.POINTER(ctypes.c_float), i]),
+        "pg_ens_autotune": (i, [vp, i, ip]),
+        "pg_ens_set_tuning": (i, [vp, ip]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

@@ -87,6 +87,7 @@ struct pg_ens {
     int maxn = 0;
     int cur = 0;
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    Tune32 tune = DEFAULT_TUNE32;  // launch configuration of the passes (pg_ens_autotune)
 
     ~pg_ens() {
         for (auto& g : graph)
@@ -117,7 +118,7 @@ pg_status enqueue_step(pg_ens* e, int in) {
     launch_time32(e->dV, e->n, e->stream);
     launch_trig32(e->dV, e->n, e->maxn, e->stream);
     for (int p = 0; p < kPasses; ++p) {
-        launch_pass32(p, e->dV, e->dFirst, e->n, e->ntiles, in ^ (p & 1), e->stream);
+        launch_pass32(p, e->dV, e->dFirst, e->n, e->ntiles, in ^ (p & 1), e->stream, &e->tune);
         launch_dust_pass32(p, e->dV, e->dDoff, e->n, e->dcount, in ^ (p & 1), e->stream);
     }
     ENS_CUDA(cudaGetLastError());
@@ -556,7 +557,7 @@ pg_status pg_ens_profile(pg_ens* e, int nsteps, double end_time, float* ms, int 
         launch_trig32(e->dV, e->n, e->maxn, e->stream);
         for (int p = 0; p < kPasses; ++p) {
             ENS_CUDA(cudaEventRecord(ev[1 + p], e->stream));
-            launch_pass32(p, e->dV, e->dFirst, e->n, e->ntiles, c0 ^ (p & 1), e->stream);
+            launch_pass32(p, e->dV, e->dFirst, e->n, e->ntiles, c0 ^ (p & 1), e->stream, &e->tune);
             launch_dust_pass32(p, e->dV, e->dDoff, e->n, e->dcount, c0 ^ (p & 1), e->stream);
         }
         ENS_CUDA(cudaEventRecord(ev[6], e->stream));
@@ -570,6 +571,88 @@ pg_status pg_ens_profile(pg_ens* e, int nsteps, double end_time, float* ms, int 
         }
     }
     for (auto& x : ev) cudaEventDestroy(x);
+    return PG_OK;
+}
+
+// For each pass and each compiled occupancy variant, every CTAs-per-SM cap up to
+// what the variant allows: the mean time of `reps` launches on the current
+// state (read from the current buffer, written to the other, which the next
+// step overwrites), and the fastest is kept.  The disks' device scalars (the
+// signal-rate maximum the timed kick2 launches raise, floor counters) are saved
+// before and restored after.  Results do not depend on the choice: tiles are
+// independent and the CFL rate is a maximum.
+pg_status pg_ens_autotune(pg_ens* e, int reps, int* out10) {
+    if (!e || reps < 1) return ens_fail(PG_ERR_ARG, "bad argument");
+    ENS_CUDA(cudaSetDevice(e->device));
+    Scalars* saved = nullptr;
+    ENS_CUDA(cudaMalloc(&saved, sizeof(Scalars) * (size_t)e->n));
+    for (int k = 0; k < e->n; ++k)
+        ENS_CUDA(cudaMemcpyAsync(saved + k, e->disks[k].v.d64.sc, sizeof(Scalars), cudaMemcpyDeviceToDevice,
+                                 e->stream));
+    cudaEvent_t a, b;
+    ENS_CUDA(cudaEventCreate(&a));
+    ENS_CUDA(cudaEventCreate(&b));
+    for (int p = 0; p < kPasses; ++p) {
+        float best = -1.0f;
+        int bv = e->tune.v[p], bc = e->tune.cps[p];
+        for (int v = 0; v < 2; ++v) {
+            const int occ = pass_occupancy32(p, v);
+            for (int cap = 1; cap <= occ; ++cap) {
+                Tune32 t = e->tune;
+                t.v[p] = v;
+                t.cps[p] = (cap == occ) ? 0 : cap;
+                launch_pass32(p, e->dV, e->dFirst, e->n, e->ntiles, e->cur, e->stream, &t);  // warm-up
+                ENS_CUDA(cudaEventRecord(a, e->stream));
+                for (int r = 0; r < reps; ++r)
+                    launch_pass32(p, e->dV, e->dFirst, e->n, e->ntiles, e->cur, e->stream, &t);
+                ENS_CUDA(cudaEventRecord(b, e->stream));
+                ENS_CUDA(cudaEventSynchronize(b));
+                ENS_CUDA(cudaGetLastError());
+                float ms = 0.0f;
+                ENS_CUDA(cudaEventElapsedTime(&ms, a, b));
+                if (best < 0.0f || ms < best) {
+                    best = ms;
+                    bv = v;
+                    bc = t.cps[p];
+                }
+            }
+        }
+        e->tune.v[p] = bv;
+        e->tune.cps[p] = bc;
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    for (int k = 0; k < e->n; ++k)
+        ENS_CUDA(cudaMemcpyAsync(e->disks[k].v.d64.sc, saved + k, sizeof(Scalars), cudaMemcpyDeviceToDevice,
+                                 e->stream));
+    ENS_CUDA(cudaStreamSynchronize(e->stream));
+    cudaFree(saved);
+    for (auto& g : e->graph)
+        if (g) {
+            cudaGraphExecDestroy(g);
+            g = nullptr;
+        }
+    if (out10)
+        for (int p = 0; p < kPasses; ++p) {
+            out10[p] = e->tune.v[p];
+            out10[5 + p] = e->tune.cps[p];
+        }
+    return PG_OK;
+}
+
+pg_status pg_ens_set_tuning(pg_ens* e, const int* in10) {
+    if (!e || !in10) return ens_fail(PG_ERR_ARG, "bad argument");
+    for (int p = 0; p < kPasses; ++p) {
+        if (in10[p] != 0 && in10[p] != 1) return ens_fail(PG_ERR_ARG, "variant must be 0 or 1");
+        if (in10[5 + p] < 0) return ens_fail(PG_ERR_ARG, "CTA cap must be >= 0");
+        e->tune.v[p] = in10[p];
+        e->tune.cps[p] = in10[5 + p];
+    }
+    for (auto& g : e->graph)
+        if (g) {
+            cudaGraphExecDestroy(g);
+            g = nullptr;
+        }
     return PG_OK;
 }
 

@@ -540,8 +540,10 @@ __device__ __forceinline__ void dust_drag32(const View32& w, int i, float Sg, fl
 }
 
 // ============================================================ radial sweep
-// 4 CTAs per SM (56 registers, no spills): 9 % faster than the 3 that 70 registers allow
-__global__ void __launch_bounds__(SWT, 4) k32_sweep_x(const View32* __restrict__ V, const int* __restrict__ first,
+// Each pass is compiled for two occupancies (MB: the CTAs per SM its register
+// budget must allow); the ensemble's autotuner picks one per pass.
+template <int MB>
+__global__ void __launch_bounds__(SWT, MB) k32_sweep_x(const View32* __restrict__ V, const int* __restrict__ first,
                                                    int nd, int ntiles, int in) {
     extern __shared__ __align__(128) float fsm_raw[];
     float* sm = smem_base128f(fsm_raw);
@@ -709,7 +711,8 @@ __global__ void __launch_bounds__(SWT, 4) k32_sweep_x(const View32* __restrict__
 }
 
 // ========================================= azimuthal sweep + orbital shift
-__global__ void __launch_bounds__(SWT) k32_sweep_y(const View32* __restrict__ V, const int* __restrict__ first,
+template <int MB>
+__global__ void __launch_bounds__(SWT, MB) k32_sweep_y(const View32* __restrict__ V, const int* __restrict__ first,
                                                    int nd, int ntiles, int in) {
     extern __shared__ __align__(128) float fsm_raw[];
     float* sm = smem_base128f(fsm_raw);
@@ -891,7 +894,8 @@ __global__ void __launch_bounds__(SWT) k32_sweep_y(const View32* __restrict__ V,
 }
 
 // ===================================================== residual advection
-__global__ void __launch_bounds__(SWT) k32_advect(const View32* __restrict__ V, const int* __restrict__ first,
+template <int MB>
+__global__ void __launch_bounds__(SWT, MB) k32_advect(const View32* __restrict__ V, const int* __restrict__ first,
                                                   int nd, int ntiles, int in) {
     extern __shared__ __align__(128) float fsm_raw[];
     float* sm = smem_base128f(fsm_raw);
@@ -1004,7 +1008,8 @@ __global__ void __launch_bounds__(SWT) k32_advect(const View32* __restrict__ V, 
 }
 
 // ====================================================== kick 1 (+ stress)
-__global__ void __launch_bounds__(STT) k32_kick1(const View32* __restrict__ V, const int* __restrict__ first, int nd,
+template <int MB>
+__global__ void __launch_bounds__(STT, MB) k32_kick1(const View32* __restrict__ V, const int* __restrict__ first, int nd,
                                                  int ntiles, int in) {
     extern __shared__ __align__(128) float fsm_raw[];
     float* sm = smem_base128f(fsm_raw);
@@ -1083,8 +1088,8 @@ __global__ void __launch_bounds__(STT) k32_kick1(const View32* __restrict__ V, c
 }
 
 // ============================================ kick 2 + damping + CFL speed
-// 5 CTAs per SM: 4 % faster than 4 despite ~50 bytes of spills (kick1 is faster at 4)
-__global__ void __launch_bounds__(STT, 5) k32_kick2(const View32* __restrict__ V, const int* __restrict__ first, int nd,
+template <int MB>
+__global__ void __launch_bounds__(STT, MB) k32_kick2(const View32* __restrict__ V, const int* __restrict__ first, int nd,
                                                  int ntiles, int in) {
     extern __shared__ __align__(128) float fsm_raw[];
     float* sm = smem_base128f(fsm_raw);
@@ -1489,7 +1494,7 @@ __global__ void k32_init_tables(const View32 w, float* tx, float* ty, double* cs
 // ============================================================== launchers
 static inline unsigned cdiv(long long a, long long b) { return (unsigned)((a + b - 1) / b); }
 
-static unsigned persistent_grid(const void* kernel, int threads, size_t smem, long long ntiles) {
+static unsigned persistent_grid(const void* kernel, int threads, size_t smem, long long ntiles, int cap = 0) {
     static int nsm = 0;
     if (nsm == 0) {
         int dev = 0;
@@ -1513,9 +1518,43 @@ static unsigned persistent_grid(const void* kernel, int threads, size_t smem, lo
                 break;
             }
     }
+    if (cap > 0 && cap < per_sm) per_sm = cap;
     long long g = (long long)per_sm * nsm;
     if (g > ntiles) g = ntiles;
     return (unsigned)(g < 1 ? 1 : g);
+}
+
+// The two compiled occupancies of each pass (kick1, sweep x, sweep y, advect,
+// kick2): variant 0 is the one the register count allows by itself, variant 1
+// one CTA per SM more (fewer registers, possibly spills).
+constexpr int MB32[5][2] = {{4, 5}, {3, 4}, {4, 5}, {5, 6}, {4, 5}};
+
+template <int P, int V>
+static const void* pass_kernel() {
+    constexpr int MB = MB32[P][V];
+    if constexpr (P == 0) return (const void*)k32_kick1<MB>;
+    else if constexpr (P == 1) return (const void*)k32_sweep_x<MB>;
+    else if constexpr (P == 2) return (const void*)k32_sweep_y<MB>;
+    else if constexpr (P == 3) return (const void*)k32_advect<MB>;
+    else return (const void*)k32_kick2<MB>;
+}
+static const void* pass_kernel(int pass, int v) {
+    static const void* const k[5][2] = {{pass_kernel<0, 0>(), pass_kernel<0, 1>()},
+                                        {pass_kernel<1, 0>(), pass_kernel<1, 1>()},
+                                        {pass_kernel<2, 0>(), pass_kernel<2, 1>()},
+                                        {pass_kernel<3, 0>(), pass_kernel<3, 1>()},
+                                        {pass_kernel<4, 0>(), pass_kernel<4, 1>()}};
+    return k[pass][v ? 1 : 0];
+}
+static const int PASS_THREADS[5] = {STT, SWT, SWT, SWT, STT};
+static const size_t PASS_SMEM[5] = {K1_SMEM, SX_SMEM, SY_SMEM, AD_SMEM, K2_SMEM};
+
+int pass_occupancy32(int pass, int variant) {
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pass_kernel(pass, variant), PASS_THREADS[pass],
+                                                      PASS_SMEM[pass]) != cudaSuccess)
+        return 1;
+    return per_sm < 1 ? 1 : per_sm;
 }
 
 cudaError_t set_attributes32() {
@@ -1526,11 +1565,8 @@ cudaError_t set_attributes32() {
         r = cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
         if (r != cudaSuccess) e = r;
     };
-    set((const void*)k32_sweep_x, SX_SMEM);
-    set((const void*)k32_sweep_y, SY_SMEM);
-    set((const void*)k32_advect, AD_SMEM);
-    set((const void*)k32_kick1, K1_SMEM);
-    set((const void*)k32_kick2, K2_SMEM);
+    for (int p = 0; p < 5; ++p)
+        for (int v = 0; v < 2; ++v) set(pass_kernel(p, v), PASS_SMEM[p]);
     return e;
 }
 
@@ -1538,28 +1574,31 @@ void launch_time32(const View32* V, int nd, cudaStream_t s) { k32_time<<<cdiv(nd
 void launch_trig32(const View32* V, int nd, int maxn, cudaStream_t s) {
     k32_trig<<<dim3(cdiv(maxn, 128), nd), 128, 0, s>>>(V);
 }
-void launch_pass32(int pass, const View32* V, const int* first, int nd, const int* ntiles, int in, cudaStream_t s) {
+template <int P, int V>
+static void launch_variant(const View32* V_, const int* first, int nd, int nt, int in, int cap, cudaStream_t s) {
+    constexpr int MB = MB32[P][V];
+    const unsigned g = persistent_grid(pass_kernel<P, V>(), PASS_THREADS[P], PASS_SMEM[P], nt, cap);
+    if constexpr (P == 0) k32_kick1<MB><<<g, STT, K1_SMEM, s>>>(V_, first, nd, nt, in);
+    else if constexpr (P == 1) k32_sweep_x<MB><<<g, SWT, SX_SMEM, s>>>(V_, first, nd, nt, in);
+    else if constexpr (P == 2) k32_sweep_y<MB><<<g, SWT, SY_SMEM, s>>>(V_, first, nd, nt, in);
+    else if constexpr (P == 3) k32_advect<MB><<<g, SWT, AD_SMEM, s>>>(V_, first, nd, nt, in);
+    else k32_kick2<MB><<<g, STT, K2_SMEM, s>>>(V_, first, nd, nt, in);
+}
+template <int P>
+static void launch_p(const View32* V, const int* first, int nd, int nt, int in, const Tune32* t, cudaStream_t s) {
+    const int v = t ? t->v[P] : DEFAULT_TUNE32.v[P];
+    const int cap = t ? t->cps[P] : 0;
+    if (v) launch_variant<P, 1>(V, first, nd, nt, in, cap, s);
+    else launch_variant<P, 0>(V, first, nd, nt, in, cap, s);
+}
+void launch_pass32(int pass, const View32* V, const int* first, int nd, const int* ntiles, int in, cudaStream_t s,
+                   const Tune32* t) {
     switch (pass) {
-        case 0: {
-            const unsigned g = persistent_grid((const void*)k32_kick1, STT, K1_SMEM, ntiles[2]);
-            k32_kick1<<<g, STT, K1_SMEM, s>>>(V, first, nd, ntiles[2], in);
-        } break;
-        case 1: {
-            const unsigned g = persistent_grid((const void*)k32_sweep_x, SWT, SX_SMEM, ntiles[0]);
-            k32_sweep_x<<<g, SWT, SX_SMEM, s>>>(V, first, nd, ntiles[0], in);
-        } break;
-        case 2: {
-            const unsigned g = persistent_grid((const void*)k32_sweep_y, SWT, SY_SMEM, ntiles[1]);
-            k32_sweep_y<<<g, SWT, SY_SMEM, s>>>(V, first, nd, ntiles[1], in);
-        } break;
-        case 3: {
-            const unsigned g = persistent_grid((const void*)k32_advect, SWT, AD_SMEM, ntiles[1]);
-            k32_advect<<<g, SWT, AD_SMEM, s>>>(V, first, nd, ntiles[1], in);
-        } break;
-        default: {
-            const unsigned g = persistent_grid((const void*)k32_kick2, STT, K2_SMEM, ntiles[2]);
-            k32_kick2<<<g, STT, K2_SMEM, s>>>(V, first, nd, ntiles[2], in);
-        } break;
+        case 0: launch_p<0>(V, first, nd, ntiles[2], in, t, s); break;
+        case 1: launch_p<1>(V, first, nd, ntiles[0], in, t, s); break;
+        case 2: launch_p<2>(V, first, nd, ntiles[1], in, t, s); break;
+        case 3: launch_p<3>(V, first, nd, ntiles[1], in, t, s); break;
+        default: launch_p<4>(V, first, nd, ntiles[2], in, t, s); break;
     }
 }
 void launch_cfl32(const View32* Vk, int b, cudaStream_t s) { k32_cfl<<<592, 256, 0, s>>>(Vk, b); }

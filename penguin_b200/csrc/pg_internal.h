@@ -103,7 +103,16 @@ struct View32;
 cudaError_t set_attributes32();
 void launch_time32(const View32* V, int nd, cudaStream_t s);
 void launch_trig32(const View32* V, int nd, int maxn, cudaStream_t s);
-void launch_pass32(int pass, const View32* V, const int* first, int nd, const int* ntiles, int in, cudaStream_t s);
+// Launch configuration of the five FP32 passes (kick1, sweep x, sweep y, advect,
+// kick2): the compiled occupancy variant (0 or 1) and a CTAs-per-SM cap (0 = none).
+struct Tune32 {
+    int v[5];
+    int cps[5];
+};
+constexpr Tune32 DEFAULT_TUNE32{{0, 1, 0, 0, 1}, {0, 0, 0, 0, 0}};
+void launch_pass32(int pass, const View32* V, const int* first, int nd, const int* ntiles, int in, cudaStream_t s,
+                   const Tune32* t = nullptr);
+int pass_occupancy32(int pass, int variant);
 void launch_cfl32(const View32* Vk, int b, cudaStream_t s);
 void launch_dust_pass32(int pass, const View32* V, const int* doff, int nd, const long long* counts, int in,
                         cudaStream_t s);

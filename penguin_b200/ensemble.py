@@ -100,6 +100,20 @@ class Ensemble:
         check(lib().pg_ens_torque(self._h, k, ctypes.byref(out)))
         return out.value
 
+    TUNING = ("v_kick1", "v_sweep_x", "v_sweep_y", "v_advect", "v_kick2",
+              "cps_kick1", "cps_sweep_x", "cps_sweep_y", "cps_advect", "cps_kick2")
+
+    def autotune(self, reps: int = 5) -> dict:
+        """Times the compiled occupancy variants and CTAs-per-SM caps of each pass
+        on the current state and keeps the fastest (results are unchanged)."""
+        out = (ctypes.c_int * 10)()
+        check(lib().pg_ens_autotune(self._h, reps, out))
+        return {k: int(out[n]) for n, k in enumerate(self.TUNING)}
+
+    def set_tuning(self, choice: dict) -> None:
+        arr = (ctypes.c_int * 10)(*[int(choice[k]) for k in self.TUNING])
+        check(lib().pg_ens_set_tuning(self._h, arr))
+
     def profile(self, nsteps: int, end_time: float = 1.0e30) -> dict:
         ms = (ctypes.c_float * 6)()
         check(lib().pg_ens_profile(self._h, nsteps, end_time, ms, 6))

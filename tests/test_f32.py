@@ -109,6 +109,34 @@ def test_ensemble_members_equal_solo_runs_bitwise():
     assert len(set(dts)) == len(dts)
 
 
+def test_ensemble_autotune_keeps_results_bitwise():
+    """The autotuner changes only launch configurations: after tuning (on the
+    current state, which it leaves alone) the run equals an untuned one bit for
+    bit, and every configuration it can pick is valid."""
+    ps = [_member(m) for m in MEMBERS]
+    sts = [I.disk_state(p, seed=21 + k) for k, p in enumerate(ps)]
+    runs = []
+    for tune in (False, True, "max"):
+        e = Ensemble(ps)
+        for k, st in enumerate(sts):
+            e.set_state(k, C.T0_DISK, st)
+        e.run(2)
+        if tune is True:
+            choice = e.autotune(reps=2)
+            assert set(choice) == set(Ensemble.TUNING)
+        elif tune == "max":  # the other occupancy variant of every pass, one CTA per SM
+            e.set_tuning({k: 1 for k in Ensemble.TUNING})
+        e.run(20)
+        e.sync()
+        e.check()
+        runs.append([e.get_state(k) for k in range(len(ps))])
+        e.close()
+    for other in runs[1:]:
+        for a, b in zip(runs[0], other):
+            for key in ("r", "u", "v"):
+                assert np.array_equal(a[key], b[key]), key
+
+
 def test_f32_first_dt_matches_fp64():
     p = P.planet_disk(128, 384)
     st = I.disk_state(p, seed=5)
