@@ -9,8 +9,8 @@ Three phases:
   collect  (here):  copy the .npz files of the golden cases into tests/golden/.
 
     python tests/golden/make_golden.py build
-    python tests/golden/make_golden.py run --out gpurun_out/golden [--timing]
-    python tests/golden/make_golden.py collect --src gpurun_out/golden
+    python tests/golden/make_golden.py run --out <outdir> [--timing]
+    python tests/golden/make_golden.py collect --src <outdir>
 """
 from __future__ import annotations
 
@@ -158,8 +158,8 @@ def collect(src: str) -> None:
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("phase", choices=["build", "run", "collect"])
-    ap.add_argument("--out", default="gpurun_out/golden")
-    ap.add_argument("--src", default="gpurun_out/golden")
+    ap.add_argument("--out", default="golden_out")
+    ap.add_argument("--src", default="golden_out")
     ap.add_argument("--timing", action="store_true")
     ap.add_argument("--only", default=None)
     ap.add_argument("--jobs", type=int, default=6)
