@@ -57,7 +57,31 @@ def cases() -> list[dict]:
     for k, kw in variants.items():
         out.append(dict(name=f"disk32_{k}_n10", params=_disk32(**kw), init="disk", t0=T0_DISK, max_step=10,
                         end_time=1.0e30, tol=2e-12 if k == "kill_planet" else 1e-14, cuda_tol=1e-13))
-    return out + adiabatic_cases() + two_body_cases()
+    return out + adiabatic_cases() + two_body_cases() + preset_cases()
+
+
+def preset_default(nr: int = 64, nphi: int = 192):
+    """The reference's include/para_files/default.h at a reduced resolution: log
+    radii on [0.3, 10], Sigma ~ r^-1.5, flat h/r 0.05, alpha 1e-3, the two-body
+    frame with q 1e-3 on an e = 0.05 orbit (smoothing 0.5 H, mass ramp over one
+    orbit), cooling with beta 0.01 (cool_flag 1; the EOS is isothermal),
+    zero-gradient inner and analytic outer boundaries, orbital advection, no
+    wave damping, CFL 0.3."""
+    return P.Params(
+        ndim=2, xres=nr, yres=nphi, geomx=1, geomy=3, gridx=1, gridy=0, xmin=0.3, xmax=10.0,
+        EOS_flag=0, internal_e_flag=1, gam=1.0, CFL=0.3, bound_lft=1, bound_rgh=0, init_flag=2,
+        frame_omega=1.0, p_alpha=1.5, p_beta=1.0, ss_alpha=1.0e-3, sc_h=0.05, planet_radius=1.0,
+        visc_flag=1, OrbAdv_flag=1, kill_flag=0, kill_width=1.0, kill_width_out=1.0, n_planet=1,
+        planet_mass=1.0e-3, planet_ecc=0.05, rs_fac=0.5, ramp_time=2.0 * math.pi,
+        cool_flag=1, beta_cool=0.01, twobd_flag=1)
+
+
+def preset_cases() -> list[dict]:
+    """The reference's default configuration (include/para_files/default.h; CI_Tau.h
+    differs only in resolution), 64x192, from the seeded disk after 5 orbits."""
+    p = preset_default()
+    return [dict(name="default64_n10", params=p, init="disk", t0=T0_DISK, max_step=10, end_time=1.0e30,
+                 tol=1e-10, cuda_tol=1e-12)]
 
 
 def two_body_cases() -> list[dict]:

@@ -23,7 +23,7 @@ def rel_l1(a, b):
     return np.abs(a - b).sum() / np.abs(b).sum()
 
 
-@pytest.mark.parametrize("name", ["disk64_n10", "dust64_st01_n10", "adi64_cool1_n10", "tb64_n10"])
+@pytest.mark.parametrize("name", ["disk64_n10", "dust64_st01_n10", "adi64_cool1_n10", "tb64_n10", "default64_n10"])
 def test_relinked_main_reproduces_reference(name, tmp_path):
     exe = os.path.join(ROOT, "oracle", "_ref", name, "dropin", "penguin")
     fx = os.path.join(GOLDEN, name + ".npz")
