@@ -81,7 +81,7 @@ def preset_cases() -> list[dict]:
     differs only in resolution), 64x192, from the seeded disk after 5 orbits."""
     p = preset_default()
     return [dict(name="default64_n10", params=p, init="disk", t0=T0_DISK, max_step=10, end_time=1.0e30,
-                 tol=1e-10, cuda_tol=1e-12)]
+                 tol=1e-13, cuda_tol=1e-12)]
 
 
 def two_body_cases() -> list[dict]:
