@@ -1217,13 +1217,27 @@ __device__ __forceinline__ void stencil_theta(const Args& a, int i, const double
 }
 
 // theta derivative of the gravity of body `which` at (i, j), contracted with (bgx, bgy)
+// (gravity() above: the planet part is linear in m; rs enters through
+// Rp^2 = ... + rs^2, so d(1/Rp^3)/d rs = -3 rs / Rp^5)
 __device__ __forceinline__ void gravity_theta(const Args& a, int i, int j, int which, double bgx, double bgy,
                                               double* acc) {
-    for (int th = 0; th < 3; th += 2) {  // q (planet mass) and h (smoothing); alpha does not enter
-        Dual gx, gy;
-        gravity<Dual>(a, Seed{-1, -1, -1, th}, i, j, which, gx, gy);
-        acc[th] += bgx * gx.d + bgy * gy.d;
-    }
+    const DiskView& d = a.d;
+    if (d.nplanet <= 0) return;
+    const pg_body& p = a.pl[which];
+    const double sinfac = a.trig[4 * j + 2 * which], cosfac = a.trig[4 * j + 2 * which + 1];
+    const double iplx2 = 1.0 / p.x / p.x;
+    const double rad = d.radx[i], plx = p.x;
+    const double Rp = sqrt(rad * rad + plx * plx - 2.0 * plx * rad * cosfac + p.rs * p.rs);
+    const double ir = 1.0 / Rp;
+    const double rs_fac = ir * ir * ir;
+    const double ax = rad - plx * cosfac, ay = plx * sinfac;
+    // d/dm
+    const double gxm = -ax * rs_fac - cosfac * iplx2, gym = -ay * rs_fac + sinfac * iplx2;
+    // d/d rs
+    const double drf = -3.0 * p.rs * rs_fac * ir * ir;
+    const double gxr = -p.m * ax * drf, gyr = -p.m * ay * drf;
+    acc[0] += a.dmdq[which] * (bgx * gxm + bgy * gym);  // q
+    acc[2] += a.drsdh * (bgx * gxr + bgy * gyr);       // h
 }
 
 // kick1 in reverse mode (same buffer).  Per output cell (k_rk1_cell): the
@@ -1313,7 +1327,31 @@ __global__ void __launch_bounds__(ADJ_THREADS) k_rk1_gather(const Args a, const 
 // from the 9 outputs, then the reverse of the predictor: lam_in of the cell and
 // lamv_in of kick1's force.  theta: gravity (q, h) of both half-kicks, nu in the
 // force, the bound-0 ghosts' init_C.
-__global__ void __launch_bounds__(ADJ_THREADS) k_rk2_cell(const Args a, double* buf, bool theta) {
+// kick2's predicted state of every cell its force stencils reach (interior and
+// one ring of ghosts; bound-0 radial ghosts keep init_C): (xres+2) x (yres+2)
+// cells, 3 values each
+__global__ void __launch_bounds__(ADJ_THREADS) k_rk2_pred(const Args a, double* pred) {
+    const DiskView& d = a.d;
+    const int W = d.xres + 2;
+    const long long n = (long long)W * (d.yres + 2);
+    const Seed s0{-1, -1, -1, -1};
+    const double h = 0.5 * a.dt;
+    for (long long m = blockIdx.x * (long long)blockDim.x + threadIdx.x; m < n; m += (long long)gridDim.x * blockDim.x) {
+        const int ii = NPAD - 1 + (int)(m % W), jj = d.ypad - 1 + (int)(m / W);
+        S3<double> X = ld<double>(a, s0, ii, jj);
+        if (ii >= NPAD && ii < NPAD + d.xres) {
+            double ox, oy, gx, gy;
+            ld_vis<double>(a, s0, ii, jj, ox, oy);
+            gravity<double>(a, s0, ii, jj, 1, gx, gy);
+            X = kick<double>(d, X, gx, gy, ox, oy, d.irad[ii], h, h);
+        }
+        pred[3 * m] = X.r;
+        pred[3 * m + 1] = X.u;
+        pred[3 * m + 2] = X.v;
+    }
+}
+
+__global__ void __launch_bounds__(ADJ_THREADS) k_rk2_cell(const Args a, double* buf, const double* pred, bool theta) {
     const DiskView& d = a.d;
     const long long n = (long long)d.xres * d.yres;
     const size_t P = plane(d);
@@ -1328,18 +1366,11 @@ __global__ void __launch_bounds__(ADJ_THREADS) k_rk2_cell(const Args a, double* 
             for (int k = 0; k < 9; ++k) {
                 int dx, dy;
                 nb(k, dx, dy);
-                const int ii = i + dx, jj = j + dy;
-                S3<double> X = ld<double>(a, s0, ii, jj);
-                if (ii >= NPAD && ii < NPAD + d.xres) {
-                    double ox, oy, gx, gy;
-                    ld_vis<double>(a, s0, ii, jj, ox, oy);
-                    gravity<double>(a, s0, ii, jj, 1, gx, gy);
-                    X = kick<double>(d, X, gx, gy, ox, oy, d.irad[ii], h, h);
-                }
-                rX[k] = X.r;
-                nr[k] = X.r * nu[k % 3];
-                u[k] = X.u;
-                v[k] = X.v;
+                const double* X = pred + 3 * ((size_t)(i + dx - (NPAD - 1)) + (size_t)(d.xres + 2) * (j + dy - (d.ypad - 1)));
+                rX[k] = X[0];
+                nr[k] = X[0] * nu[k % 3];
+                u[k] = X[1];
+                v[k] = X[2];
             }
             viscous<double>(d.visx + 5 * i, d.visy + 4 * j, u, v, nr, vx, vy);
         }
@@ -1756,7 +1787,10 @@ static void launch_pass(const Args& a, bool theta, double* scratch, double* rev,
         if (a.d.visc) k_rk1_gather<<<g, ADJ_THREADS, 0, s>>>(a, rev);
         return;  // theta done by k_rk1_cell
     } else if (PASS == P_K2 && rev) {
-        k_rk2_cell<<<g, ADJ_THREADS, 0, s>>>(a, rev, theta);
+        double* pred = rev + (size_t)a.d.xres * a.d.yres * RK1_STEN;  // after the 27 stencil adjoints per cell
+        if (a.d.visc)
+            k_rk2_pred<<<grid_for((long long)(a.d.xres + 2) * (a.d.yres + 2)), ADJ_THREADS, 0, s>>>(a, pred);
+        k_rk2_cell<<<g, ADJ_THREADS, 0, s>>>(a, rev, pred, theta);
         if (a.d.visc) k_rk2_gather<<<g, ADJ_THREADS, 0, s>>>(a, rev, theta);
         return;  // theta done by the reverse kernels
     } else if (PASS == P_ADV && rev) {
@@ -1967,7 +2001,7 @@ pg_status pg_adj_create(const pg_params* P, int device, void* stream, int checkp
     {
         const size_t nx = (size_t)P->xres, ny = (size_t)P->yres;
         const size_t cells = std::max(ny * (nx + 2), nx * (ny + 2));
-        const size_t words = std::max(cells * REV_SLOT, nx * ny * (size_t)RK1_STEN);
+        const size_t words = std::max(cells * REV_SLOT, nx * ny * (size_t)RK1_STEN + (nx + 2) * (ny + 2) * 3);
         if ((s = adj_alloc(a, &a->rev, words * sizeof(double))) != PG_OK) return bail(s);
         if ((s = adj_alloc(a, &a->trig, 4 * (ny + 2 * NPAD) * sizeof(double))) != PG_OK) return bail(s);
     }
