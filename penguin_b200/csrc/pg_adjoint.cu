@@ -695,6 +695,44 @@ __device__ __forceinline__ void rev_dims(const DiskView& d, int& n, int& npen, i
     p0 = (DIR == 0) ? NPAD : d.ypad;
 }
 
+// The buffer is planar: REV_SLOT fields of npen (n + 2) pencil cells each.  A
+// pencil cell's index runs along the pencil for DIR 0 and across the pencils
+// for DIR 1, and so do the kernels' threads: consecutive threads then touch
+// consecutive buffer entries and consecutive cells of the AoS state.
+template <int DIR>
+struct RevBuf {
+    double* p;
+    size_t ns;  // cells per field
+    int n, npen, p0;
+    __device__ __forceinline__ RevBuf(const DiskView& d, const double* buf) : p(const_cast<double*>(buf)) {
+        rev_dims<DIR>(d, n, npen, p0);
+        ns = (size_t)npen * (n + 2);
+    }
+    __device__ __forceinline__ size_t cell(int pen, int c) const {
+        const int slot = c - (p0 - 1);
+        return (DIR == 0) ? (size_t)pen * (n + 2) + slot : (size_t)slot * npen + pen;
+    }
+    __device__ __forceinline__ double& operator()(int f, int pen, int c) const { return p[(size_t)f * ns + cell(pen, c)]; }
+    // a stored half-state (fields f0 .. f0 + 3: r, p, u and v (DIR 0) or w (DIR 1))
+    __device__ __forceinline__ Half half(int f0, int pen, int c) const {
+        const double* o = p + (size_t)f0 * ns + cell(pen, c);
+        const double t = o[3 * ns];
+        return Half{o[0], o[ns], o[2 * ns], DIR == 0 ? t : 0.0, DIR == 0 ? 0.0 : t};
+    }
+};
+// thread t of a sweep-reverse kernel covering `per` cells (or faces) per pencil from c0
+template <int DIR>
+__device__ __forceinline__ void rev_thread(long long t, int per, int npen, int c0, int& pen, int& c) {
+    if (DIR == 0) {
+        pen = (int)(t / per);
+        c = c0 + (int)(t % per);
+    } else {
+        pen = (int)(t % npen);
+        c = c0 + (int)(t / npen);
+    }
+}
+
+
 // the half-states of the cells that have them (see k_rev_face)
 template <int DIR>
 __global__ void __launch_bounds__(ADJ_THREADS) k_rev_states(const Args a, double* buf) {
@@ -705,27 +743,23 @@ __global__ void __launch_bounds__(ADJ_THREADS) k_rev_states(const Args a, double
     const int c0 = (DIR == 0) ? p0 - 1 : p0;
     const long long total = (long long)nc * npen;
     const Seed s0{-1, -1, -1, -1};
+    const RevBuf<DIR> B(d, buf);
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
          t += (long long)gridDim.x * blockDim.x) {
-        const int pen = (int)(t / nc), c = c0 + (int)(t % nc);
+        int pen, c;
+        rev_thread<DIR>(t, nc, npen, c0, pen, c);
         const int q = ((DIR == 0) ? d.ypad : NPAD) + pen;
         HalfT<double> L, R;
         edge_states<double, DIR>(a, s0, c, q, L, R);
-        double* o = buf + ((size_t)pen * (n + 2) + (c - (p0 - 1))) * REV_SLOT + REV_ST;
-        o[0] = L.r;
-        o[1] = L.p;
-        o[2] = L.u;
-        o[3] = (DIR == 0) ? L.v : L.w;
-        o[4] = R.r;
-        o[5] = R.p;
-        o[6] = R.u;
-        o[7] = (DIR == 0) ? R.v : R.w;
+        B(REV_ST, pen, c) = L.r;
+        B(REV_ST + 1, pen, c) = L.p;
+        B(REV_ST + 2, pen, c) = L.u;
+        B(REV_ST + 3, pen, c) = (DIR == 0) ? L.v : L.w;
+        B(REV_ST + 4, pen, c) = R.r;
+        B(REV_ST + 5, pen, c) = R.p;
+        B(REV_ST + 6, pen, c) = R.u;
+        B(REV_ST + 7, pen, c) = (DIR == 0) ? R.v : R.w;
     }
-}
-
-template <int DIR>
-__device__ __forceinline__ Half rev_half(const double* o) {  // a stored half-state
-    return Half{o[0], o[1], o[2], DIR == 0 ? o[3] : 0.0, DIR == 0 ? 0.0 : o[3]};
 }
 
 // the pencil cell whose right half-state feeds face f from below (DIR 1: wrapped)
@@ -742,18 +776,18 @@ __global__ void __launch_bounds__(ADJ_THREADS) k_rev_flux(const Args a, double* 
     rev_dims<DIR>(d, n, npen, p0);
     const int nf = (DIR == 0) ? n + 1 : n;
     const long long total = (long long)nf * npen;
+    const RevBuf<DIR> B(d, buf);
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
          t += (long long)gridDim.x * blockDim.x) {
-        const int pen = (int)(t / nf), f = p0 + (int)(t % nf);
-        double* pb = buf + (size_t)pen * (n + 2) * REV_SLOT;
-        const Half L = rev_half<DIR>(pb + (size_t)(rev_below<DIR>(d, f) - (p0 - 1)) * REV_SLOT + REV_ST + 4);
-        double* o = pb + (size_t)(f - (p0 - 1)) * REV_SLOT;
-        const Half R = rev_half<DIR>(o + REV_ST);
+        int pen, f;
+        rev_thread<DIR>(t, nf, npen, p0, pen, f);
+        const Half L = B.half(REV_ST + 4, pen, rev_below<DIR>(d, f));
+        const Half R = B.half(REV_ST, pen, f);
         const Flux F = hllc<double>(0, d.ie, d.gam, L, R);
-        o[REV_FX] = F.r;
-        o[REV_FX + 1] = F.u;
-        o[REV_FX + 2] = (DIR == 0) ? F.v : F.w;
-        o[REV_FX + 3] = F.pres;
+        B(REV_FX, pen, f) = F.r;
+        B(REV_FX + 1, pen, f) = F.u;
+        B(REV_FX + 2, pen, f) = (DIR == 0) ? F.v : F.w;
+        B(REV_FX + 3, pen, f) = F.pres;
     }
 }
 
@@ -764,10 +798,10 @@ __device__ __forceinline__ FluxT<double> rev_flux(const DiskView& d, const doubl
     rev_dims<DIR>(d, n, npen, p0);
     if (DIR == 1 && f >= p0 + n) f -= n;
     const int pen = q - ((DIR == 0) ? d.ypad : NPAD);
-    const double* o = buf + ((size_t)pen * (n + 2) + (f - (p0 - 1))) * REV_SLOT + REV_FX;
-    FluxT<double> F{o[0], 0.0, o[1], 0.0, 0.0, o[3], 0.0};
-    if (DIR == 0) F.v = o[2];
-    else F.w = o[2];
+    const RevBuf<DIR> B(d, buf);
+    FluxT<double> F{B(REV_FX, pen, f), 0.0, B(REV_FX + 1, pen, f), 0.0, 0.0, B(REV_FX + 3, pen, f), 0.0};
+    if (DIR == 0) F.v = B(REV_FX + 2, pen, f);
+    else F.w = B(REV_FX + 2, pen, f);
     return F;
 }
 
@@ -940,37 +974,31 @@ __global__ void __launch_bounds__(ADJ_THREADS) k_rev_face(const Args a, const do
     rev_dims<DIR>(d, n, npen, p0);
     const int nf = (DIR == 0) ? n + 1 : n;  // faces per pencil
     const long long total = (long long)nf * npen;
+    const RevBuf<DIR> B(d, buf);
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
          t += (long long)gridDim.x * blockDim.x) {
-        const int pen = (int)(t / nf), f = p0 + (int)(t % nf);
+        int pen, f;
+        rev_thread<DIR>(t, nf, npen, p0, pen, f);
         const int q = ((DIR == 0) ? d.ypad : NPAD) + pen;
         const FluxT<double> LF = face_lambda<DIR>(a, lslot, f, q);
-        double* pb = buf + (size_t)pen * (n + 2) * REV_SLOT;
-        const Half r0 = rev_half<DIR>(pb + (size_t)(rev_below<DIR>(d, f) - (p0 - 1)) * REV_SLOT + REV_ST + 4);
-        const Half l1 = rev_half<DIR>(pb + (size_t)(f - (p0 - 1)) * REV_SLOT + REV_ST);
+        const int cm = rev_below<DIR>(d, f);  // the cell whose right half-state is the face's left state
+        const Half r0 = B.half(REV_ST + 4, pen, cm);
+        const Half l1 = B.half(REV_ST, pen, f);
         const double bF[5] = {LF.r, LF.u, LF.v, LF.w, LF.pres};
         Half bL{0.0, 0.0, 0.0, 0.0, 0.0}, bR{0.0, 0.0, 0.0, 0.0, 0.0};
         rev::hllc_rev(d.gam, r0, l1, bF, bL, bR);
-        // the right half-state of cell f - 1 (DIR 1: wrapped to its interior row)
-        const int cm = (DIR == 0) ? f - 1 : wrap_row(d, f - 1);
-        double* o = pb + (size_t)(cm - (p0 - 1)) * REV_SLOT;
-        o[4] = bL.r;
-        o[5] = bL.p;
-        o[6] = bL.u;
-        o[7] = (DIR == 0) ? bL.v : bL.w;
-        o = pb + (size_t)(f - (p0 - 1)) * REV_SLOT;  // the left half-state of cell f
-        o[0] = bR.r;
-        o[1] = bR.p;
-        o[2] = bR.u;
-        o[3] = (DIR == 0) ? bR.v : bR.w;
-        if (DIR == 0 && f == p0) {  // ghost cell p0 - 1 has no left face in the pencil
-            o = pb;
-            o[0] = o[1] = o[2] = o[3] = 0.0;
-        }
-        if (DIR == 0 && f == p0 + n) {  // nor ghost cell p0 + n a right face
-            o = pb + (size_t)(n + 1) * REV_SLOT;
-            o[4] = o[5] = o[6] = o[7] = 0.0;
-        }
+        B(4, pen, cm) = bL.r;
+        B(5, pen, cm) = bL.p;
+        B(6, pen, cm) = bL.u;
+        B(7, pen, cm) = (DIR == 0) ? bL.v : bL.w;
+        B(0, pen, f) = bR.r;  // the left half-state of cell f
+        B(1, pen, f) = bR.p;
+        B(2, pen, f) = bR.u;
+        B(3, pen, f) = (DIR == 0) ? bR.v : bR.w;
+        if (DIR == 0 && f == p0)  // ghost cell p0 - 1 has no left face in the pencil
+            for (int k = 0; k < 4; ++k) B(k, pen, p0 - 1) = 0.0;
+        if (DIR == 0 && f == p0 + n)  // nor ghost cell p0 + n a right face
+            for (int k = 4; k < 8; ++k) B(k, pen, p0 + n) = 0.0;
     }
 }
 
@@ -983,17 +1011,23 @@ __global__ void __launch_bounds__(ADJ_THREADS) k_rev_cell(const Args a, double* 
     const int c0 = (DIR == 0) ? p0 - 1 : p0;
     const long long total = (long long)nc * npen;
     double acc[3] = {0.0, 0.0, 0.0};
+    const RevBuf<DIR> B(d, buf);
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
          t += (long long)gridDim.x * blockDim.x) {
-        const int pen = (int)(t / nc), c = c0 + (int)(t % nc);
+        int pen, c;
+        rev_thread<DIR>(t, nc, npen, c0, pen, c);
         const int q = ((DIR == 0) ? d.ypad : NPAD) + pen;
-        double* o = buf + ((size_t)pen * (n + 2) + (c - (p0 - 1))) * REV_SLOT;
+        double bl[4], br[4];
+        for (int k = 0; k < 4; ++k) {
+            bl[k] = B(k, pen, c);
+            br[k] = B(4 + k, pen, c);
+        }
         double out[5][3];
-        edge_rev<DIR>(a, c, q, o, o + 4, out, theta ? acc : nullptr);
+        edge_rev<DIR>(a, c, q, bl, br, out, theta ? acc : nullptr);
 #pragma unroll
         for (int k = 0; k < 5; ++k)
 #pragma unroll
-            for (int f = 0; f < 3; ++f) o[REV_HALF + 3 * k + f] = out[k][f];
+            for (int f = 0; f < 3; ++f) B(REV_HALF + 3 * k + f, pen, c) = out[k][f];
     }
     if (theta) block_add3(acc, a.gth);
 }
@@ -1005,13 +1039,13 @@ __global__ void __launch_bounds__(ADJ_THREADS) k_rev_gather(const Args a, const 
     rev_dims<DIR>(d, n, npen, p0);
     const long long total = (long long)d.xres * d.yres;
     const size_t P = plane(d);
+    const RevBuf<DIR> B(d, buf);
     const int lo = (DIR == 0) ? p0 - 1 : p0, hi = (DIR == 0) ? p0 + n : p0 + n - 1;  // cells holding adjoints
     for (long long m = blockIdx.x * (long long)blockDim.x + threadIdx.x; m < total;
          m += (long long)gridDim.x * blockDim.x) {
         const int i = NPAD + (int)(m % d.xres), j = d.ypad + (int)(m / d.xres);
         const int pos = (DIR == 0) ? i : j;
         const int pen = (DIR == 0) ? j - d.ypad : i - NPAD;
-        const double* pb = buf + (size_t)pen * (n + 2) * REV_SLOT;
         double acc[3] = {0.0, 0.0, 0.0};
         for (int img = -1; img <= 1; ++img) {  // the cell itself and, periodic, its ghost-row images
             if (DIR == 0 && img != 0) continue;
@@ -1019,10 +1053,9 @@ __global__ void __launch_bounds__(ADJ_THREADS) k_rev_gather(const Args a, const 
             for (int k = 0; k < 5; ++k) {
                 const int src = s + 2 - k;
                 if (src < lo || src > hi) continue;
-                const double* o = pb + (size_t)(src - (p0 - 1)) * REV_SLOT + REV_HALF + 3 * k;
-                acc[0] += o[0];
-                acc[1] += o[1];
-                acc[2] += o[2];
+                acc[0] += B(REV_HALF + 3 * k, pen, src);
+                acc[1] += B(REV_HALF + 3 * k + 1, pen, src);
+                acc[2] += B(REV_HALF + 3 * k + 2, pen, src);
             }
         }
         a.lam_in[m] += acc[0];
@@ -1122,11 +1155,10 @@ __global__ void __launch_bounds__(ADJ_THREADS) k_radv_face(const Args a, const d
         rev::recon_rev(wt, tR, 0.0, bR, ar, bflat);
         rev::recon_rev(wt, tU, 0.0, bU, au, bflat);
         rev::recon_rev(wt, tW, 0.0, bW, aw, bflat);
-        double* o = buf + (size_t)m * REV_STEN;
-        for (int k = 0; k < 5; ++k) {
-            o[3 * k] = ar[k];
-            o[3 * k + 1] = aw[k];  // v_r
-            o[3 * k + 2] = au[k];  // v_phi
+        for (int k = 0; k < 5; ++k) {  // planar: field 3 k + f of face m at buf[(3 k + f) n + m]
+            buf[(size_t)(3 * k) * n + m] = ar[k];
+            buf[(size_t)(3 * k + 1) * n + m] = aw[k];  // v_r
+            buf[(size_t)(3 * k + 2) * n + m] = au[k];  // v_phi
         }
         if (theta) {
             // d/d speed: the flux factor and, through x0, the swept fraction
@@ -1148,10 +1180,10 @@ __global__ void __launch_bounds__(ADJ_THREADS) k_radv_gather(const Args a, const
         double acc[3] = {0.0, 0.0, 0.0};
         for (int k = 0; k < 5; ++k) {
             const int f = wrap_row(d, j + 2 - k + up);  // its upwind stencil holds row j at position k
-            const double* o = buf + pidx(d, i, f) * REV_STEN + 3 * k;
-            acc[0] += o[0];
-            acc[1] += o[1];
-            acc[2] += o[2];
+            const size_t mf = pidx(d, i, f);
+            acc[0] += buf[(size_t)(3 * k) * n + mf];
+            acc[1] += buf[(size_t)(3 * k + 1) * n + mf];
+            acc[2] += buf[(size_t)(3 * k + 2) * n + mf];
         }
         a.lam_in[m] += acc[0];
         a.lam_in[P + m] += acc[1];
@@ -1285,11 +1317,10 @@ __global__ void __launch_bounds__(ADJ_THREADS) k_rk1_cell(const Args a, double* 
             const double bvx = lu * dt * ir + a.lamv[m], bvy = lv * dt * ir + a.lamv[P + m];
             double bu[9] = {}, bv[9] = {}, bn[9] = {};
             rev::viscous_rev(d.visx + 5 * i, d.visy + 4 * j, u, v, nr, bvx, bvy, bu, bv, bn);
-            double* o = buf + (size_t)m * RK1_STEN;
-            for (int k = 0; k < 9; ++k) {
-                o[3 * k] = bn[k] * nu[k % 3];
-                o[3 * k + 1] = bu[k];
-                o[3 * k + 2] = bv[k];
+            for (int k = 0; k < 9; ++k) {  // planar: field 3 k + f of output m at buf[(3 k + f) n + m]
+                buf[(size_t)(3 * k) * n + m] = bn[k] * nu[k % 3];
+                buf[(size_t)(3 * k + 1) * n + m] = bu[k];
+                buf[(size_t)(3 * k + 2) * n + m] = bv[k];
             }
             if (theta) stencil_theta(a, i, bu, bv, bn, rX, acc);
         }
@@ -1309,10 +1340,10 @@ __global__ void __launch_bounds__(ADJ_THREADS) k_rk1_gather(const Args a, const 
             nb(k, dx, dy);
             const int oi = i - dx;  // the output whose stencil slot k is this cell
             if (oi < NPAD || oi >= NPAD + d.xres) continue;
-            const double* o = buf + pidx(d, oi, wrap_row(d, j - dy)) * RK1_STEN + 3 * k;
-            acc[0] += o[0];
-            acc[1] += o[1];
-            acc[2] += o[2];
+            const size_t mo = pidx(d, oi, wrap_row(d, j - dy));
+            acc[0] += buf[(size_t)(3 * k) * n + mo];
+            acc[1] += buf[(size_t)(3 * k + 1) * n + mo];
+            acc[2] += buf[(size_t)(3 * k + 2) * n + mo];
         }
         a.lam_in[m] += acc[0];
         a.lam_in[P + m] += acc[1];
@@ -1345,9 +1376,9 @@ __global__ void __launch_bounds__(ADJ_THREADS) k_rk2_pred(const Args a, double* 
             gravity<double>(a, s0, ii, jj, 1, gx, gy);
             X = kick<double>(d, X, gx, gy, ox, oy, d.irad[ii], h, h);
         }
-        pred[3 * m] = X.r;
-        pred[3 * m + 1] = X.u;
-        pred[3 * m + 2] = X.v;
+        pred[m] = X.r;  // planar: 3 fields of n cells
+        pred[n + m] = X.u;
+        pred[2 * n + m] = X.v;
     }
 }
 
@@ -1366,11 +1397,12 @@ __global__ void __launch_bounds__(ADJ_THREADS) k_rk2_cell(const Args a, double* 
             for (int k = 0; k < 9; ++k) {
                 int dx, dy;
                 nb(k, dx, dy);
-                const double* X = pred + 3 * ((size_t)(i + dx - (NPAD - 1)) + (size_t)(d.xres + 2) * (j + dy - (d.ypad - 1)));
-                rX[k] = X[0];
-                nr[k] = X[0] * nu[k % 3];
-                u[k] = X[1];
-                v[k] = X[2];
+                const size_t np = (size_t)(d.xres + 2) * (d.yres + 2);
+                const size_t mp = (size_t)(i + dx - (NPAD - 1)) + (size_t)(d.xres + 2) * (j + dy - (d.ypad - 1));
+                rX[k] = pred[mp];
+                nr[k] = pred[mp] * nu[k % 3];
+                u[k] = pred[np + mp];
+                v[k] = pred[2 * np + mp];
             }
             viscous<double>(d.visx + 5 * i, d.visy + 4 * j, u, v, nr, vx, vy);
         }
@@ -1385,11 +1417,10 @@ __global__ void __launch_bounds__(ADJ_THREADS) k_rk2_cell(const Args a, double* 
         if (d.visc) {
             double bu[9] = {}, bv[9] = {}, bn[9] = {};
             rev::viscous_rev(d.visx + 5 * i, d.visy + 4 * j, u, v, nr, b.vx, b.vy, bu, bv, bn);
-            double* o = buf + (size_t)m * RK1_STEN;
             for (int k = 0; k < 9; ++k) {
-                o[3 * k] = bn[k] * nu[k % 3];
-                o[3 * k + 1] = bu[k];
-                o[3 * k + 2] = bv[k];
+                buf[(size_t)(3 * k) * n + m] = bn[k] * nu[k % 3];
+                buf[(size_t)(3 * k + 1) * n + m] = bu[k];
+                buf[(size_t)(3 * k + 2) * n + m] = bv[k];
             }
             if (theta) stencil_theta(a, i, bu, bv, bn, rX, acc);
         }
@@ -1412,10 +1443,10 @@ __global__ void __launch_bounds__(ADJ_THREADS) k_rk2_gather(const Args a, const 
             nb(k, dx, dy);
             const int oi = i - dx;
             if (oi < NPAD || oi >= NPAD + d.xres) continue;
-            const double* o = buf + pidx(d, oi, wrap_row(d, j - dy)) * RK1_STEN + 3 * k;
-            bX[0] += o[0];
-            bX[1] += o[1];
-            bX[2] += o[2];
+            const size_t mo = pidx(d, oi, wrap_row(d, j - dy));
+            bX[0] += buf[(size_t)(3 * k) * n + mo];
+            bX[1] += buf[(size_t)(3 * k + 1) * n + mo];
+            bX[2] += buf[(size_t)(3 * k + 2) * n + mo];
         }
         // the predictor X = kick(C, g, kick1's force, dt/2, dt/2)
         const S3<double> C = ld<double>(a, s0, i, j);
