@@ -837,18 +837,39 @@ __global__ void __launch_bounds__(ADJ_THREADS) k_adj_upd(const Args a, double* l
         sweep_D<DIR>(a, i, j, F0, F1, Dr, D1, D2);
         const S3<double> Q = ld<double>(a, s0, i, j);
         double g[6];
+        if (rbuf) {
+            // update_iso in reverse: r' = r + D_r, u' = (u r + D_1) / r', v' = (v r + D_2) / r',
+            // or the floor r' = max(1e-10 r, smallr) with u, v kept
+            const S3<double> O = update_iso<double>(Q, Dr, D1, D2);
+            const double r_min = fmax(Q.r * 1.0e-10, SMALLR);
+            if (Q.r + Dr < r_min) {
+                g[0] = (SMALLR > Q.r * 1.0e-10) ? 0.0 : lr * 1.0e-10;
+                g[1] = lu;
+                g[2] = lv;
+                g[3] = g[4] = g[5] = 0.0;
+            } else {
+                const double iR = 1.0 / O.r;
+                g[0] = lr + (lu * (Q.u - O.u) + lv * (Q.v - O.v)) * iR;
+                g[1] = lu * Q.r * iR;
+                g[2] = lv * Q.r * iR;
+                g[3] = lr - (lu * O.u + lv * O.v) * iR;
+                g[4] = lu * iR;
+                g[5] = lv * iR;
+            }
+        } else {
 #pragma unroll
-        for (int k = 0; k < 6; ++k) {
-            S3<Dual> q{Q.r, Q.p, Q.u, Q.v};
-            Dual r = Dr, u1 = D1, u2 = D2;
-            if (k == 0) q.r.d = 1.0;
-            else if (k == 1) q.u.d = 1.0;
-            else if (k == 2) q.v.d = 1.0;
-            else if (k == 3) r.d = 1.0;
-            else if (k == 4) u1.d = 1.0;
-            else u2.d = 1.0;
-            const S3<Dual> o = update_iso<Dual>(q, r, u1, u2);
-            g[k] = lr * o.r.d + lu * o.u.d + lv * o.v.d;
+            for (int k = 0; k < 6; ++k) {
+                S3<Dual> q{Q.r, Q.p, Q.u, Q.v};
+                Dual r = Dr, u1 = D1, u2 = D2;
+                if (k == 0) q.r.d = 1.0;
+                else if (k == 1) q.u.d = 1.0;
+                else if (k == 2) q.v.d = 1.0;
+                else if (k == 3) r.d = 1.0;
+                else if (k == 4) u1.d = 1.0;
+                else u2.d = 1.0;
+                const S3<Dual> o = update_iso<Dual>(q, r, u1, u2);
+                g[k] = lr * o.r.d + lu * o.u.d + lv * o.v.d;
+            }
         }
         a.lam_in[m] = g[0];
         a.lam_in[P + m] = g[1];
