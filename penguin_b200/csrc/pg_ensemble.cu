@@ -79,6 +79,7 @@ struct pg_ens {
     std::vector<EDisk> disks;
     View32* dV = nullptr;
     int* dFirst = nullptr;
+    int4* dTiles = nullptr;             // per tile of each kind: {disk, origin along the fast index, along the slow}
     CUtensorMap* dMaps = nullptr;
     double* dPart = nullptr;
     int ntiles[3] = {0, 0, 0};
@@ -104,6 +105,7 @@ struct pg_ens {
         }
         cudaFree(dV);
         cudaFree(dFirst);
+        cudaFree(dTiles);
         cudaFree(dMaps);
         cudaFree(dPart);
         cudaFree(dDoff);
@@ -118,7 +120,7 @@ pg_status enqueue_step(pg_ens* e, int in) {
     launch_time32(e->dV, e->n, e->stream);
     launch_trig32(e->dV, e->n, e->maxn, e->stream);
     for (int p = 0; p < kPasses; ++p) {
-        launch_pass32(p, e->dV, e->dFirst, e->n, e->ntiles, in ^ (p & 1), e->stream, &e->tune);
+        launch_pass32(p, e->dV, e->dTiles, e->n, e->ntiles, in ^ (p & 1), e->stream, &e->tune);
         launch_dust_pass32(p, e->dV, e->dDoff, e->n, e->dcount, in ^ (p & 1), e->stream);
     }
     ENS_CUDA(cudaGetLastError());
@@ -282,7 +284,20 @@ pg_status pg_ens_create(const pg_params* P, int n, int device, void* stream, pg_
         hv[k] = v;
     }
     for (int p = 0; p < 3; ++p) e->ntiles[p] = first[p * (n + 1) + n];
-    if ((ce = cudaMalloc(&e->dDoff, sizeof(int) * doff.size())) != cudaSuccess ||
+    // tile table: a tile's disk and origin (32 cells along the fast index x 8
+    // along the slow), so the passes need no search over the disks' offsets
+    std::vector<int4> tiles;
+    tiles.reserve((size_t)e->ntiles[0] + e->ntiles[1] + e->ntiles[2]);
+    for (int p = 0; p < 3; ++p)
+        for (int k = 0; k < n; ++k) {
+            const int ntx = hv[k].ntx[p];
+            for (int loc = 0; loc < first[p * (n + 1) + k + 1] - first[p * (n + 1) + k]; ++loc)
+                tiles.push_back(make_int4(k, NPAD + 32 * (loc % ntx), NPAD + 8 * (loc / ntx), 0));
+        }
+    if ((ce = cudaMalloc(&e->dTiles, sizeof(int4) * tiles.size())) != cudaSuccess ||
+        (ce = cudaMemcpyAsync(e->dTiles, tiles.data(), sizeof(int4) * tiles.size(), cudaMemcpyHostToDevice,
+                              e->stream)) != cudaSuccess ||
+        (ce = cudaMalloc(&e->dDoff, sizeof(int) * doff.size())) != cudaSuccess ||
         (ce = cudaMemcpyAsync(e->dDoff, doff.data(), sizeof(int) * doff.size(), cudaMemcpyHostToDevice, e->stream)) !=
             cudaSuccess ||
         (ce = cudaMemcpyAsync(e->dMaps, maps.data(), sizeof(CUtensorMap) * maps.size(), cudaMemcpyHostToDevice,
@@ -557,7 +572,7 @@ pg_status pg_ens_profile(pg_ens* e, int nsteps, double end_time, float* ms, int 
         launch_trig32(e->dV, e->n, e->maxn, e->stream);
         for (int p = 0; p < kPasses; ++p) {
             ENS_CUDA(cudaEventRecord(ev[1 + p], e->stream));
-            launch_pass32(p, e->dV, e->dFirst, e->n, e->ntiles, c0 ^ (p & 1), e->stream, &e->tune);
+            launch_pass32(p, e->dV, e->dTiles, e->n, e->ntiles, c0 ^ (p & 1), e->stream, &e->tune);
             launch_dust_pass32(p, e->dV, e->dDoff, e->n, e->dcount, c0 ^ (p & 1), e->stream);
         }
         ENS_CUDA(cudaEventRecord(ev[6], e->stream));
@@ -601,10 +616,10 @@ pg_status pg_ens_autotune(pg_ens* e, int reps, int* out10) {
                 Tune32 t = e->tune;
                 t.v[p] = v;
                 t.cps[p] = (cap == occ) ? 0 : cap;
-                launch_pass32(p, e->dV, e->dFirst, e->n, e->ntiles, e->cur, e->stream, &t);  // warm-up
+                launch_pass32(p, e->dV, e->dTiles, e->n, e->ntiles, e->cur, e->stream, &t);  // warm-up
                 ENS_CUDA(cudaEventRecord(a, e->stream));
                 for (int r = 0; r < reps; ++r)
-                    launch_pass32(p, e->dV, e->dFirst, e->n, e->ntiles, e->cur, e->stream, &t);
+                    launch_pass32(p, e->dV, e->dTiles, e->n, e->ntiles, e->cur, e->stream, &t);
                 ENS_CUDA(cudaEventRecord(b, e->stream));
                 ENS_CUDA(cudaEventSynchronize(b));
                 ENS_CUDA(cudaGetLastError());

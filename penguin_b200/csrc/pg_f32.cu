@@ -543,7 +543,7 @@ __device__ __forceinline__ void dust_drag32(const View32& w, int i, float Sg, fl
 // Each pass is compiled for two occupancies (MB: the CTAs per SM its register
 // budget must allow); the ensemble's autotuner picks one per pass.
 template <int MB>
-__global__ void __launch_bounds__(SWT, MB) k32_sweep_x(const View32* __restrict__ V, const int* __restrict__ first,
+__global__ void __launch_bounds__(SWT, MB) k32_sweep_x(const View32* __restrict__ V, const int4* __restrict__ tiles,
                                                    int nd, int ntiles, int in) {
     extern __shared__ __align__(128) float fsm_raw[];
     float* sm = smem_base128f(fsm_raw);
@@ -552,12 +552,11 @@ __global__ void __launch_bounds__(SWT, MB) k32_sweep_x(const View32* __restrict_
     float* fl = st + NSX * P1N;   // [4][P2N]
     uint64_t* bar = reinterpret_cast<uint64_t*>(fl + 4 * P2N);
     const int tid = threadIdx.x;
-    auto locate = [&](int tile, int& k, int& s0, int& q0) {
-        k = find_disk(first, nd, tile);
-        const int loc = tile - first[k];
-        const int ntx = V[k].ntx[0];
-        s0 = NPAD + T_LEN * (loc % ntx);
-        q0 = NPAD + T_W * (loc / ntx);
+    auto locate = [&](int tile, int& k, int& s0, int& q0) {  // the tile's disk and origin (pg_ens tile table)
+        const int4 t = tiles[tile];
+        k = t.x;
+        s0 = t.y;
+        q0 = t.z;
     };
     auto issue = [&](int tile, int kt) {
         int k, s0, q0;
@@ -712,7 +711,7 @@ __global__ void __launch_bounds__(SWT, MB) k32_sweep_x(const View32* __restrict_
 
 // ========================================= azimuthal sweep + orbital shift
 template <int MB>
-__global__ void __launch_bounds__(SWT, MB) k32_sweep_y(const View32* __restrict__ V, const int* __restrict__ first,
+__global__ void __launch_bounds__(SWT, MB) k32_sweep_y(const View32* __restrict__ V, const int4* __restrict__ tiles,
                                                    int nd, int ntiles, int in) {
     extern __shared__ __align__(128) float fsm_raw[];
     float* sm = smem_base128f(fsm_raw);
@@ -722,13 +721,11 @@ __global__ void __launch_bounds__(SWT, MB) k32_sweep_y(const View32* __restrict_
     uint64_t* bar = reinterpret_cast<uint64_t*>(fl + 4 * P2N);
     __shared__ int s_inc[T_W];
     const int tid = threadIdx.x;
-    const int* fst = first + (nd + 1);
-    auto locate = [&](int tile, int& k, int& s0, int& q0) {
-        k = find_disk(fst, nd, tile);
-        const int loc = tile - fst[k];
-        const int ntx = V[k].ntx[1];
-        s0 = NPAD + T_LEN * (loc % ntx);  // first output row
-        q0 = NPAD + T_W * (loc / ntx);    // first column
+    auto locate = [&](int tile, int& k, int& s0, int& q0) {  // the tile's disk and origin (pg_ens tile table)
+        const int4 t = tiles[tile];
+        k = t.x;
+        s0 = t.y;
+        q0 = t.z;
     };
     auto issue = [&](int tile, int kt) {
         int k, s0, q0;
@@ -895,7 +892,7 @@ __global__ void __launch_bounds__(SWT, MB) k32_sweep_y(const View32* __restrict_
 
 // ===================================================== residual advection
 template <int MB>
-__global__ void __launch_bounds__(SWT, MB) k32_advect(const View32* __restrict__ V, const int* __restrict__ first,
+__global__ void __launch_bounds__(SWT, MB) k32_advect(const View32* __restrict__ V, const int4* __restrict__ tiles,
                                                   int nd, int ntiles, int in) {
     extern __shared__ __align__(128) float fsm_raw[];
     float* sm = smem_base128f(fsm_raw);
@@ -903,13 +900,11 @@ __global__ void __launch_bounds__(SWT, MB) k32_advect(const View32* __restrict__
     float* fl = sm + 2 * YS;  // [3][NFA]: mass flux, then the upwind carriers of v and u
     uint64_t* bar = reinterpret_cast<uint64_t*>(fl + 3 * NFA);
     const int tid = threadIdx.x;
-    const int* fst = first + (nd + 1);
-    auto locate = [&](int tile, int& k, int& s0, int& q0) {
-        k = find_disk(fst, nd, tile);
-        const int loc = tile - fst[k];
-        const int ntx = V[k].ntx[1];
-        s0 = NPAD + T_LEN * (loc % ntx);
-        q0 = NPAD + T_W * (loc / ntx);
+    auto locate = [&](int tile, int& k, int& s0, int& q0) {  // the tile's disk and origin (pg_ens tile table)
+        const int4 t = tiles[tile];
+        k = t.x;
+        s0 = t.y;
+        q0 = t.z;
     };
     auto issue = [&](int tile, int kt) {
         int k, s0, q0;
@@ -1009,20 +1004,18 @@ __global__ void __launch_bounds__(SWT, MB) k32_advect(const View32* __restrict__
 
 // ====================================================== kick 1 (+ stress)
 template <int MB>
-__global__ void __launch_bounds__(STT, MB) k32_kick1(const View32* __restrict__ V, const int* __restrict__ first, int nd,
+__global__ void __launch_bounds__(STT, MB) k32_kick1(const View32* __restrict__ V, const int4* __restrict__ tiles, int nd,
                                                  int ntiles, int in) {
     extern __shared__ __align__(128) float fsm_raw[];
     float* sm = smem_base128f(fsm_raw);
     auto stage = [&](int n) { return sm + (n & 1) * SS; };
     uint64_t* bar = reinterpret_cast<uint64_t*>(sm + 2 * SS);
     const int tid = threadIdx.x;
-    const int* fst = first + 2 * (nd + 1);
-    auto locate = [&](int tile, int& k, int& i0, int& j0) {
-        k = find_disk(fst, nd, tile);
-        const int loc = tile - fst[k];
-        const int ntx = V[k].ntx[2];
-        i0 = NPAD + T_LEN * (loc % ntx);
-        j0 = NPAD + T_W * (loc / ntx);
+    auto locate = [&](int tile, int& k, int& i0, int& j0) {  // the tile's disk and origin (pg_ens tile table)
+        const int4 t = tiles[tile];
+        k = t.x;
+        i0 = t.y;
+        j0 = t.z;
     };
     auto issue = [&](int tile, int kt) {
         int k, i0, j0;
@@ -1089,7 +1082,7 @@ __global__ void __launch_bounds__(STT, MB) k32_kick1(const View32* __restrict__ 
 
 // ============================================ kick 2 + damping + CFL speed
 template <int MB>
-__global__ void __launch_bounds__(STT, MB) k32_kick2(const View32* __restrict__ V, const int* __restrict__ first, int nd,
+__global__ void __launch_bounds__(STT, MB) k32_kick2(const View32* __restrict__ V, const int4* __restrict__ tiles, int nd,
                                                  int ntiles, int in) {
     extern __shared__ __align__(128) float fsm_raw[];
     float* sm = smem_base128f(fsm_raw);
@@ -1098,13 +1091,11 @@ __global__ void __launch_bounds__(STT, MB) k32_kick2(const View32* __restrict__ 
     float* tp = sm + 2 * SS + 2 * VS;  // predicted state with 1 halo, same layout as a stage
     uint64_t* bar = reinterpret_cast<uint64_t*>(tp + SS);
     const int tid = threadIdx.x;
-    const int* fst = first + 2 * (nd + 1);
-    auto locate = [&](int tile, int& k, int& i0, int& j0) {
-        k = find_disk(fst, nd, tile);
-        const int loc = tile - fst[k];
-        const int ntx = V[k].ntx[2];
-        i0 = NPAD + T_LEN * (loc % ntx);
-        j0 = NPAD + T_W * (loc / ntx);
+    auto locate = [&](int tile, int& k, int& i0, int& j0) {  // the tile's disk and origin (pg_ens tile table)
+        const int4 t = tiles[tile];
+        k = t.x;
+        i0 = t.y;
+        j0 = t.z;
     };
     auto issue = [&](int tile, int kt) {
         int k, i0, j0;
@@ -1575,7 +1566,7 @@ void launch_trig32(const View32* V, int nd, int maxn, cudaStream_t s) {
     k32_trig<<<dim3(cdiv(maxn, 128), nd), 128, 0, s>>>(V);
 }
 template <int P, int V>
-static void launch_variant(const View32* V_, const int* first, int nd, int nt, int in, int cap, cudaStream_t s) {
+static void launch_variant(const View32* V_, const int4* first, int nd, int nt, int in, int cap, cudaStream_t s) {
     constexpr int MB = MB32[P][V];
     const unsigned g = persistent_grid(pass_kernel<P, V>(), PASS_THREADS[P], PASS_SMEM[P], nt, cap);
     if constexpr (P == 0) k32_kick1<MB><<<g, STT, K1_SMEM, s>>>(V_, first, nd, nt, in);
@@ -1585,20 +1576,24 @@ static void launch_variant(const View32* V_, const int* first, int nd, int nt, i
     else k32_kick2<MB><<<g, STT, K2_SMEM, s>>>(V_, first, nd, nt, in);
 }
 template <int P>
-static void launch_p(const View32* V, const int* first, int nd, int nt, int in, const Tune32* t, cudaStream_t s) {
+static void launch_p(const View32* V, const int4* first, int nd, int nt, int in, const Tune32* t, cudaStream_t s) {
     const int v = t ? t->v[P] : DEFAULT_TUNE32.v[P];
     const int cap = t ? t->cps[P] : 0;
     if (v) launch_variant<P, 1>(V, first, nd, nt, in, cap, s);
     else launch_variant<P, 0>(V, first, nd, nt, in, cap, s);
 }
-void launch_pass32(int pass, const View32* V, const int* first, int nd, const int* ntiles, int in, cudaStream_t s,
+// tiles: the ensemble's tile table, radial-sweep tiles, then azimuthal, then stencil
+void launch_pass32(int pass, const View32* V, const int4* tiles, int nd, const int* ntiles, int in, cudaStream_t s,
                    const Tune32* t) {
+    const int4* tx = tiles;
+    const int4* ty = tiles + ntiles[0];
+    const int4* ts = tiles + ntiles[0] + ntiles[1];
     switch (pass) {
-        case 0: launch_p<0>(V, first, nd, ntiles[2], in, t, s); break;
-        case 1: launch_p<1>(V, first, nd, ntiles[0], in, t, s); break;
-        case 2: launch_p<2>(V, first, nd, ntiles[1], in, t, s); break;
-        case 3: launch_p<3>(V, first, nd, ntiles[1], in, t, s); break;
-        default: launch_p<4>(V, first, nd, ntiles[2], in, t, s); break;
+        case 0: launch_p<0>(V, ts, nd, ntiles[2], in, t, s); break;
+        case 1: launch_p<1>(V, tx, nd, ntiles[0], in, t, s); break;
+        case 2: launch_p<2>(V, ty, nd, ntiles[1], in, t, s); break;
+        case 3: launch_p<3>(V, ty, nd, ntiles[1], in, t, s); break;
+        default: launch_p<4>(V, ts, nd, ntiles[2], in, t, s); break;
     }
 }
 void launch_cfl32(const View32* Vk, int b, cudaStream_t s) { k32_cfl<<<592, 256, 0, s>>>(Vk, b); }

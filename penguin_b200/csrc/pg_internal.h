@@ -110,7 +110,7 @@ struct Tune32 {
     int cps[5];
 };
 constexpr Tune32 DEFAULT_TUNE32{{0, 1, 0, 0, 1}, {0, 0, 0, 0, 0}};
-void launch_pass32(int pass, const View32* V, const int* first, int nd, const int* ntiles, int in, cudaStream_t s,
+void launch_pass32(int pass, const View32* V, const int4* tiles, int nd, const int* ntiles, int in, cudaStream_t s,
                    const Tune32* t = nullptr);
 int pass_occupancy32(int pass, int variant);
 void launch_cfl32(const View32* Vk, int b, cudaStream_t s);
