@@ -298,16 +298,21 @@ def measure_dust(local, stream, steps, pk):
 
 
 SEED_DUST = 1234
-ADJOINT_STEPS = 256
+ADJOINT_STEPS = 256  # the finite-difference checks
+ADJOINT_TIMING_STEPS = 1024  # the timed run: 16 checkpoint segments
 
 
-def measure_adjoint(steps, local, stream):
+def measure_adjoint(steps, local, stream, timing_steps=None):
     """Gradient of the azimuthally averaged Sigma(r) misfit after `steps` steps of the
     256x768 adjoint disk (q 5e-4, alpha 1e-3, h/r 0.05) with respect to the initial
     Sigma field and (q, alpha, h/r), against a target made by the same code at
-    q 1e-3, alpha 3e-4 from the same seed; checkpoints every 64 steps.  Forward
-    and adjoint timed with CUDA events; central finite differences (FP64) of the
-    loss along a smooth Sigma0 direction and along each parameter check it."""
+    q 1e-3, alpha 3e-4 from the same seed; checkpoints every 64 steps.  Central
+    finite differences (FP64) of the loss along a smooth Sigma0 direction and
+    along each parameter check it.  Forward and adjoint are timed with CUDA
+    events on a run of `timing_steps` steps (default `steps`): the backward
+    overlaps the recompute of each segment with the transposition of the next,
+    so only the first segment's recompute is exposed, and a longer run (config
+    5 is about 10,900 steps, 170 segments) shows the steady cost."""
     import numpy as np
     import torch
 
@@ -339,12 +344,21 @@ def measure_adjoint(steps, local, stream):
     def bwd():
         res["g"] = m.backward(g)
 
-    bwd()  # warm-up
-    # medians of 3: the forward replaying the recorded dt schedule (what the
-    # backward recomputes per segment) and the backward
-    ms_f = sorted(timed(stream, lambda: m.forward(s0, replay=True)) for _ in range(3))[1]
-    ms_b = sorted(timed(stream, bwd) for _ in range(3))[1]
+    bwd()
     gs0, gth = res["g"]
+    # timing: medians of 3 after a warm-up, the forward replaying the recorded dt
+    # schedule (what the backward recomputes per segment) and the backward
+    tsteps = timing_steps or steps
+    mt = m if tsteps == steps else DiskAdjoint(p, nsteps=tsteps, checkpoint_every=64, device=local,
+                                               stream=stream.cuda_stream)
+    if mt is not m:
+        ms_rec = timed(stream, lambda: mt.forward(s0))
+        mt.backward(torch.zeros_like(g))
+    gt = torch.zeros_like(g) + g
+    ms_f = sorted(timed(stream, lambda: mt.forward(s0, replay=True)) for _ in range(3))[1]
+    ms_b = sorted(timed(stream, lambda: mt.backward(gt)) for _ in range(3))[1]
+    if mt is not m:
+        mt.close()
     x = I.cell_centres(p)
     y = (np.arange(p.yres) + 0.5) * 2 * np.pi / p.yres
     d = torch.tensor(np.cos(2 * y[:, None] + 1.0) * np.sin(3 * x[None, :]) + 0.3, device=s0.device) * s0
@@ -382,9 +396,11 @@ def measure_adjoint(steps, local, stream):
     m.set_theta(*theta)
     out_line = {
         "workload": "256x768 gradient disk, FP64 forward + adjoint, checkpoint every 64 steps",
-        "steps": steps, "forward_ms_per_step": ms_f / steps, "adjoint_ms_per_step": ms_b / steps,
-        "adjoint_over_forward": ms_b / ms_f, "forward_record_ms_per_step": ms_rec / steps,
-        "timing": "medians of 3 after a warm-up backward; forward = replay of the recorded dt schedule",
+        "steps": steps, "timing_steps": tsteps, "forward_ms_per_step": ms_f / tsteps,
+        "adjoint_ms_per_step": ms_b / tsteps, "adjoint_over_forward": ms_b / ms_f,
+        "forward_record_ms_per_step": ms_rec / tsteps,
+        "timing": "medians of 3 after a warm-up backward over timing_steps steps (checkpoint segments of 64); "
+                  "forward = replay of the recorded dt schedule",
         "device_bytes": m.device_bytes,
         "fd_sigma0": {"state": "the workload's noisy disk", "adjoint": ad, "central": fd,
                       "rel_err": {k: abs(ad - v) / abs(v) for k, v in fd.items()}},
@@ -551,7 +567,8 @@ def main():
     if "dust" in forms:
         line["dust"] = measure_dust(local, stream, min(DUST_STEPS, max(K, 3)), pk)
     if "adjoint" in forms:
-        line["adjoint"] = measure_adjoint(min(ADJOINT_STEPS, max(K, 8)), local, stream)
+        line["adjoint"] = measure_adjoint(min(ADJOINT_STEPS, max(K, 8)), local, stream,
+                                          min(ADJOINT_TIMING_STEPS, max(K, 8)))
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(p, state, 0.0)
     if rank == 0:

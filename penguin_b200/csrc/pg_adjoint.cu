@@ -1879,6 +1879,11 @@ struct pg_adj {
     pg_disk* disk = nullptr;
     Engine* E = nullptr;
     int every = 64;
+    // the backward recomputes segment s - 1 on fstream into one bank of step
+    // records while segment s is transposed on `stream` from the other
+    cudaStream_t fstream = nullptr;
+    cudaEvent_t ev_rec[2] = {nullptr, nullptr}, ev_rev[2] = {nullptr, nullptr};
+    pg_body* pl_host = nullptr;  // pinned: the recorded planets of both banks
     // dt schedule of the recorded forward run
     double t0 = 0.0;
     std::vector<double> ts, dts;
@@ -2035,11 +2040,21 @@ pg_status pg_adj_create(const pg_params* P, int device, void* stream, int checkp
         pg_adj_destroy(a);
         return st;
     };
-    if ((s = adj_alloc(a, &a->stages, 5 * K * nc * sizeof(Cell))) != PG_OK) return bail(s);
-    if ((s = adj_alloc(a, &a->rvis, 2 * K * nc * sizeof(double))) != PG_OK) return bail(s);
-    if ((s = adj_alloc(a, &a->rpl, 2 * K * sizeof(pg_body))) != PG_OK) return bail(s);
-    if ((s = adj_alloc(a, &a->rres, K * xarr * sizeof(double))) != PG_OK) return bail(s);
-    if ((s = adj_alloc(a, &a->rinc, K * xarr * sizeof(int))) != PG_OK) return bail(s);
+    // step records: two banks of K steps each
+    if ((s = adj_alloc(a, &a->stages, 2 * 5 * K * nc * sizeof(Cell))) != PG_OK) return bail(s);
+    if ((s = adj_alloc(a, &a->rvis, 2 * 2 * K * nc * sizeof(double))) != PG_OK) return bail(s);
+    if ((s = adj_alloc(a, &a->rpl, 2 * 2 * K * sizeof(pg_body))) != PG_OK) return bail(s);
+    if ((s = adj_alloc(a, &a->rres, 2 * K * xarr * sizeof(double))) != PG_OK) return bail(s);
+    if ((s = adj_alloc(a, &a->rinc, 2 * K * xarr * sizeof(int))) != PG_OK) return bail(s);
+    {
+        cudaError_t ce = cudaStreamCreateWithFlags(&a->fstream, cudaStreamNonBlocking);
+        for (int b = 0; b < 2 && ce == cudaSuccess; ++b) {
+            ce = cudaEventCreateWithFlags(&a->ev_rec[b], cudaEventDisableTiming);
+            if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&a->ev_rev[b], cudaEventDisableTiming);
+        }
+        if (ce == cudaSuccess) ce = cudaMallocHost(&a->pl_host, 2 * 2 * K * sizeof(pg_body));
+        if (ce != cudaSuccess) return bail(adj_fail(PG_ERR_CUDA, std::string("adjoint streams: ") + cudaGetErrorString(ce)));
+    }
     if ((s = adj_alloc(a, &a->lam[0], 3 * ni * sizeof(double))) != PG_OK) return bail(s);
     if ((s = adj_alloc(a, &a->lam[1], 3 * ni * sizeof(double))) != PG_OK) return bail(s);
     if ((s = adj_alloc(a, &a->lamv, 2 * ni * sizeof(double))) != PG_OK) return bail(s);
@@ -2085,6 +2100,15 @@ pg_status pg_adj_destroy(pg_adj* a) {
     cudaFree(a->scratch);
     cudaFree(a->rev);
     cudaFree(a->trig);
+    for (int b = 0; b < 2; ++b) {
+        if (a->ev_rec[b]) cudaEventDestroy(a->ev_rec[b]);
+        if (a->ev_rev[b]) cudaEventDestroy(a->ev_rev[b]);
+    }
+    if (a->pl_host) cudaFreeHost(a->pl_host);
+    if (a->fstream) {
+        cudaStreamSynchronize(a->fstream);
+        cudaStreamDestroy(a->fstream);
+    }
     if (a->own_stream && a->stream) cudaStreamDestroy(a->stream);
     delete a;
     return PG_OK;
@@ -2155,7 +2179,7 @@ pg_status pg_adj_forward(pg_adj* a, const double* sigma0, double t0, int nsteps,
     return pg_disk_check(a->disk);
 }
 
-static Args base_args(pg_adj* a, int n, int slot, const pg_body* pl) {
+static Args base_args(pg_adj* a, int n, int slot, const pg_body* pl, int bank = 0) {
     Args g{};
     g.d = engine_view(a->E);
     g.pl[0] = pl[0];
@@ -2165,9 +2189,10 @@ static Args base_args(pg_adj* a, int n, int slot, const pg_body* pl) {
     g.dmdq[1] = ramp_function(a->ts[n] + a->dts[n], tau, 1.0);
     g.drsdh = a->P.rs_fac * a->P.planet_radius;  // rs = rs_fac h a (2D)
     const size_t xarr = (size_t)a->P.xres + 2 * NPAD;
-    g.res = a->rres + (size_t)slot * xarr;
-    g.inc = a->rinc + (size_t)slot * xarr;
-    g.vis = a->rvis + (size_t)slot * 2 * a->ncell();
+    const size_t sl = (size_t)bank * a->every + slot;
+    g.res = a->rres + sl * xarr;
+    g.inc = a->rinc + sl * xarr;
+    g.vis = a->rvis + sl * 2 * a->ncell();
     g.dt = a->dts[n];
     g.dtab = a->dtab;
     g.gth = a->gth;
@@ -2176,14 +2201,15 @@ static Args base_args(pg_adj* a, int n, int slot, const pg_body* pl) {
     return g;
 }
 
-static StepRecord record_slot(pg_adj* a, int slot) {
+static StepRecord record_slot(pg_adj* a, int slot, int bank = 0) {
     StepRecord r{};
     const size_t nc = a->ncell(), xarr = (size_t)a->P.xres + 2 * NPAD;
-    for (int k = 0; k < 5; ++k) r.stage[k] = a->stages + ((size_t)slot * 5 + k) * nc;
-    r.vis = a->rvis + (size_t)slot * 2 * nc;
-    r.planets = a->rpl + 2 * (size_t)slot;
-    r.res = a->rres + (size_t)slot * xarr;
-    r.inc = a->rinc + (size_t)slot * xarr;
+    const size_t sl = (size_t)bank * a->every + slot;  // bank b holds steps b K .. b K + K - 1 of the buffers
+    for (int k = 0; k < 5; ++k) r.stage[k] = a->stages + (sl * 5 + k) * nc;
+    r.vis = a->rvis + sl * 2 * nc;
+    r.planets = a->rpl + 2 * sl;
+    r.res = a->rres + sl * xarr;
+    r.inc = a->rinc + sl * xarr;
     return r;
 }
 
@@ -2204,21 +2230,44 @@ pg_status pg_adj_backward(pg_adj* a, const double* grad_out, double* grad_sigma0
     ADJ_CUDA(cudaMemcpyAsync(a->lam[0], grad_out, ni * sizeof(double), cudaMemcpyDeviceToDevice, st));
     ADJ_CUDA(cudaMemsetAsync(a->gth, 0, 3 * sizeof(double), st));
     ADJ_CUDA(cudaMemsetAsync(a->lamv, 0, 2 * ni * sizeof(double), st));
-    std::vector<pg_body> pl(2 * (size_t)a->every);
-    pg_status s;
-    for (int seg = a->nckpt - 1; seg >= 0; --seg) {
+    pg_status s = PG_OK;
+    const size_t K = (size_t)a->every;
+    // Segment seg's records are recomputed on fstream into bank (nckpt - 1 - seg) % 2
+    // from its checkpoint, with the recorded planets copied to pinned host memory;
+    // the recompute of segment seg - 1 runs while segment seg is transposed on st.
+    cudaStream_t st_engine = engine_set_stream(a->E, a->fstream);
+    auto recompute = [&](int seg, int bank) -> pg_status {
         const int n0 = seg * a->every, n1 = std::min(n0 + a->every, N);
-        if ((s = engine_restore(a->E, a->ckpt + (size_t)seg * a->ncell(), a->ckpt_sc + seg)) != PG_OK) return s;
-        for (int n = n0; n < n1; ++n) {
-            const StepRecord r = record_slot(a, n - n0);
-            if ((s = engine_step(a->E, a->ts[n], a->dts[n], &r)) != PG_OK) return s;
+        pg_status r = engine_restore(a->E, a->ckpt + (size_t)seg * a->ncell(), a->ckpt_sc + seg);
+        for (int n = n0; n < n1 && r == PG_OK; ++n) {
+            const StepRecord rec = record_slot(a, n - n0, bank);
+            r = engine_step(a->E, a->ts[n], a->dts[n], &rec);
         }
-        ADJ_CUDA(cudaMemcpyAsync(pl.data(), a->rpl, 2 * (size_t)(n1 - n0) * sizeof(pg_body), cudaMemcpyDeviceToHost, st));
-        ADJ_CUDA(cudaStreamSynchronize(st));
+        if (r != PG_OK) return r;
+        const StepRecord rec0 = record_slot(a, 0, bank);
+        ADJ_CUDA(cudaMemcpyAsync(a->pl_host + 2 * K * bank, rec0.planets, 2 * (size_t)(n1 - n0) * sizeof(pg_body),
+                                 cudaMemcpyDeviceToHost, a->fstream));
+        ADJ_CUDA(cudaEventRecord(a->ev_rec[bank], a->fstream));
+        return PG_OK;
+    };
+    ADJ_CUDA(cudaEventRecord(a->ev_rev[1], st));  // nothing reads bank 1 yet
+    s = recompute(a->nckpt - 1, 0);
+    for (int seg = a->nckpt - 1; seg >= 0 && s == PG_OK; --seg) {
+        const int bank = (a->nckpt - 1 - seg) % 2;
+        const int n0 = seg * a->every, n1 = std::min(n0 + a->every, N);
+        if (cudaEventSynchronize(a->ev_rec[bank]) != cudaSuccess) {
+            s = adj_fail(PG_ERR_CUDA, "adjoint recompute failed");
+            break;
+        }
+        if (seg > 0) {  // the other bank is free once the previous segment's transposition is done
+            ADJ_CUDA(cudaStreamWaitEvent(a->fstream, a->ev_rev[1 - bank], 0));
+            if ((s = recompute(seg - 1, 1 - bank)) != PG_OK) break;
+        }
+        const pg_body* pl = a->pl_host + 2 * K * bank;
         for (int n = n1 - 1; n >= n0; --n) {
             const int slot = n - n0;
-            const StepRecord r = record_slot(a, slot);
-            Args g = base_args(a, n, slot, &pl[2 * (size_t)slot]);
+            const StepRecord r = record_slot(a, slot, bank);
+            Args g = base_args(a, n, slot, &pl[2 * (size_t)slot], bank);
             auto run = [&](int pass, const Cell* in) {
                 g.in = in;
                 g.lam = a->lam[c];
@@ -2239,7 +2288,11 @@ pg_status pg_adj_backward(pg_adj* a, const double* grad_out, double* grad_sigma0
             run(P_K1, r.stage[0]);
             ADJ_CUDA(cudaGetLastError());
         }
+        ADJ_CUDA(cudaEventRecord(a->ev_rev[bank], st));
     }
+    cudaStreamSynchronize(a->fstream);
+    engine_set_stream(a->E, st_engine);
+    if (s != PG_OK) return s;
     k_init_theta<<<grid_for((long long)ni), ADJ_THREADS, 0, st>>>(d, a->lam[c] + 2 * ni, a->dtab, a->gth);
     ADJ_CUDA(cudaGetLastError());
     if (grad_sigma0)

@@ -882,6 +882,12 @@ pg_status engine_save(Engine* E, Cell* cells, Scalars* sc) {
     return PG_OK;
 }
 
+cudaStream_t engine_set_stream(Engine* E, cudaStream_t s) {
+    cudaStream_t old = E->stream;
+    E->stream = s;
+    return old;
+}
+
 pg_status engine_restore(Engine* E, const Cell* cells, const Scalars* sc) {
     const size_t n = (size_t)E->view.xarr * E->view.yarr;
     E->cur = 0;

@@ -73,6 +73,8 @@ pg_status engine_set_state_device(Engine* E, double t, const double* r, const do
 pg_status engine_step(Engine* E, double t, double dt, const StepRecord* rec);
 pg_status engine_save(Engine* E, Cell* cells, Scalars* sc);
 pg_status engine_restore(Engine* E, const Cell* cells, const Scalars* sc);
+// the stream the engine launches on; returns the previous one
+cudaStream_t engine_set_stream(Engine* E, cudaStream_t s);
 pg_status engine_extract_device(Engine* E, double* r, double* p, double* u, double* v);
 pg_status engine_run_pass(Engine* E, int pass, const Cell* in, Cell* out, const double* vis_in, double* vis_out);
 pg_status table_engine_create(const pg_params* P, int device, cudaStream_t s, Engine** out);
