@@ -427,30 +427,24 @@ def main():
                          "(fp32, ensemble, dust, adjoint)")
     args = ap.parse_args()
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
-        run_reference(args, rank, world)
+        run_reference(args, int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")))
         return
 
     import numpy as np
     import torch
 
-    torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
+    from penguin_b200.replicas import Replicas
 
-        import torch.distributed as dist
-
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    job = Replicas("nccl")
+    world, local = job.world, job.local
 
     from penguin_b200 import initial as I
     from penguin_b200.disk import Disk
 
     p = workload()
-    state = I.disk_state(p, seed=1234 + rank)
+    state = I.disk_state(p, seed=job.seed(1234))
     stream = torch.cuda.Stream()
     disk = Disk(p, device=local, stream=stream.cuda_stream)
     disk.set_state(0.0, state)
@@ -461,9 +455,7 @@ def main():
     tuning = disk.autotune(reps=5) if not args.no_tune else None
 
     def barrier():
-        if dist:
-            dist.barrier()
-        torch.cuda.synchronize()
+        job.barrier(torch.cuda.synchronize)
 
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with Clocks(local) as clk:
@@ -476,12 +468,9 @@ def main():
     ms = e0.elapsed_time(e1)
     disk.check()
     clocks = clk.summary()
-    if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = job.max_over_ranks(ms)
     cells = p.cells
-    value = cells * K * world / (ms / 1000.0)
+    value = job.job_rate(cells * K, ms)
 
     # per-stage device times (events between the launches, same stream)
     prof = disk.profile(max(5, min(50, K // 10)))
@@ -527,11 +516,8 @@ def main():
     g1.synchronize()
     h3 = time.perf_counter()
     e2e_ms = g0.elapsed_time(g1)
-    if dist:
-        t = torch.tensor([e2e_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e = {"value": cells * Ke * world / (e2e_ms / 1000.0), "unit": UNIT,
+    e2e_ms = job.max_over_ranks(e2e_ms)
+    e2e = {"value": job.job_rate(cells * Ke, e2e_ms), "unit": UNIT,
            "h2d_bytes_per_step": 4 * 8 * cells // Ke,
            "d2h_bytes_per_step": 8 + 4 * 8 * cells // Ke,
            "steps": Ke,
@@ -569,13 +555,12 @@ def main():
     if "adjoint" in forms:
         line["adjoint"] = measure_adjoint(min(ADJOINT_STEPS, max(K, 8)), local, stream,
                                           min(ADJOINT_TIMING_STEPS, max(K, 8)))
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if job.printer and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(p, state, 0.0)
-    if rank == 0:
+    if job.printer:
         print(json.dumps(line), flush=True)
     disk.close()
-    if dist:
-        dist.destroy_process_group()
+    job.close()
 
 
 if __name__ == "__main__":

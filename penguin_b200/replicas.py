@@ -1,0 +1,87 @@
+"""Replicas across the GPUs of one node.
+
+A Godunov step of one disk has no exchange with any other disk: the
+reference runs one disk per process and never splits it (main.cu:165-360
+allocates the whole grid on one device).  So several GPUs run independent
+replicas, one process per GPU, each stepping its own seeded disk, and the
+data path carries no collective.  The process group is used for timing only:
+a barrier on both sides of the timed region and the maximum of the ranks'
+device times, from which the whole-job rate is the units every rank
+processed divided by that maximum.
+
+The launcher (torchrun) sets WORLD_SIZE, RANK and LOCAL_RANK and the
+MASTER_ADDR / MASTER_PORT rendezvous.  The backend is NCCL on the GPUs and
+gloo on the host cores; every rank takes the same collective calls in the same
+order.
+"""
+from __future__ import annotations
+
+import datetime
+import os
+from typing import Callable, Mapping
+
+
+class Replicas:
+    """The ranks of one job.  With WORLD_SIZE 1 (or unset) no process group is
+    created and every call is local."""
+
+    def __init__(self, backend: str | None = None, timeout_s: float = 120.0,
+                 env: Mapping[str, str] | None = None):
+        env = os.environ if env is None else env
+        self.world = int(env.get("WORLD_SIZE", "1"))
+        self.rank = int(env.get("RANK", "0"))
+        self.local = int(env.get("LOCAL_RANK", "0"))
+        if self.world < 1 or not 0 <= self.rank < self.world or self.local < 0:
+            raise ValueError(f"bad rank layout: world {self.world}, rank {self.rank}, local {self.local}")
+        import torch
+
+        if backend is None:
+            backend = "nccl" if torch.cuda.is_available() else "gloo"
+        self.backend = backend
+        self.device = torch.device("cuda", self.local) if backend == "nccl" else torch.device("cpu")
+        self.dist = None
+        if self.world > 1:
+            import torch.distributed as dist
+
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=timeout_s))
+            if dist.get_world_size() != self.world or dist.get_rank() != self.rank:
+                raise RuntimeError("process group disagrees with WORLD_SIZE / RANK")
+            self.dist = dist
+
+    @property
+    def printer(self) -> bool:
+        """Rank 0 alone reports for the job."""
+        return self.rank == 0
+
+    def seed(self, base: int) -> int:
+        """Each replica steps its own disk: the seed of its initial noise."""
+        return base + self.rank
+
+    def barrier(self, sync: Callable[[], None] | None = None) -> None:
+        """All ranks meet, then ``sync`` (the local device synchronise) runs."""
+        if self.dist is not None:
+            self.dist.barrier()
+        if sync is not None:
+            sync()
+
+    def max_over_ranks(self, x: float) -> float:
+        """The largest of the ranks' values (each rank passes its own)."""
+        if self.dist is None:
+            return float(x)
+        import torch
+
+        t = torch.tensor([float(x)], dtype=torch.float64, device=self.device)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def job_rate(self, units_per_rank: float, ms: float) -> float:
+        """Whole-job throughput: every rank processed ``units_per_rank`` in at
+        most ``ms`` (the max over ranks)."""
+        if ms <= 0.0:
+            raise ValueError("non-positive time")
+        return units_per_rank * self.world / (ms / 1000.0)
+
+    def close(self) -> None:
+        if self.dist is not None:
+            self.dist.destroy_process_group()
+            self.dist = None
