@@ -9,6 +9,10 @@ a barrier on both sides of the timed region and the maximum of the ranks'
 device times, from which the whole-job rate is the units every rank
 processed divided by that maximum.
 
+An ensemble of disks shards the same way, by whole disks: ``partition``
+splits the disks across the ranks by their cell counts, each rank steps its
+share as one ensemble, and ``gather`` brings the results to rank 0 at the end.
+
 The launcher (torchrun) sets WORLD_SIZE, RANK and LOCAL_RANK and the
 MASTER_ADDR / MASTER_PORT rendezvous.  The backend is NCCL on the GPUs and
 gloo on the host cores; every rank takes the same collective calls in the same
@@ -81,7 +85,40 @@ class Replicas:
             raise ValueError("non-positive time")
         return units_per_rank * self.world / (ms / 1000.0)
 
+    def share(self, weights) -> list[int]:
+        """The indices of the independent units (ensemble disks) this rank runs."""
+        return partition(weights, self.world)[self.rank]
+
+    def gather(self, obj):
+        """Every rank's ``obj`` in rank order on rank 0 (None on the others): the
+        final host-side gather of a partitioned ensemble's results."""
+        if self.dist is None:
+            return [obj]
+        out = [None] * self.world if self.printer else None
+        self.dist.gather_object(obj, out, dst=0)
+        return out
+
     def close(self) -> None:
         if self.dist is not None:
             self.dist.destroy_process_group()
             self.dist = None
+
+
+def partition(weights, world: int) -> list[list[int]]:
+    """Whole units across ``world`` ranks, balanced by weight (cells x steps):
+    the heaviest unit first, each to the rank with the least weight so far
+    (ties to the lower rank).  Deterministic, so every rank computes the same
+    split without communication.  Each rank's list is in ascending index
+    order."""
+    if world < 1:
+        raise ValueError("world must be positive")
+    w = [float(x) for x in weights]
+    if any(not x >= 0.0 for x in w):
+        raise ValueError("weights must be non-negative")
+    load = [0.0] * world
+    parts: list[list[int]] = [[] for _ in range(world)]
+    for k in sorted(range(len(w)), key=lambda i: (-w[i], i)):
+        r = min(range(world), key=lambda q: (load[q], q))
+        parts[r].append(k)
+        load[r] += w[k]
+    return [sorted(p) for p in parts]

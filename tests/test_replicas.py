@@ -4,8 +4,9 @@ Each rank steps its own seeded disk with no exchange between ranks; the
 process group carries only the timing (barriers and the max over ranks).  On
 the GPUs the same calls run over NCCL.  Here the disks are stepped by the
 CPU restatement, which stands in for the device step: the test covers the
-rank layout, seeds, barrier, max-over-ranks reduction and job rate, and how a
-rank that fails or never joins surfaces on the others.
+rank layout, seeds, barrier, max-over-ranks reduction and job rate, an
+ensemble split across the ranks by whole disks and gathered on rank 0, and
+how a rank that fails or never joins surfaces on the others.
 """
 from __future__ import annotations
 
@@ -207,3 +208,70 @@ def test_reference_arm_under_torchrun():
     j = json.loads(lines[0])
     assert j["impl"] == "reference" and j["n_gpus"] == 2 and j["value"] > 0
     assert j["e2e"]["h2d_bytes_per_step"] == 0 and j["cpu_baseline"]["kind"] == "port"
+
+
+def test_partition_balances_whole_units():
+    from penguin_b200 import params as P
+    from penguin_b200.replicas import partition
+
+    cells = [p.cells for p in P.disk_ensemble()]
+    for world in (1, 2, 3, 8):
+        parts = partition(cells, world)
+        assert sorted(k for q in parts for k in q) == list(range(len(cells)))
+        loads = [sum(cells[k] for k in q) for q in parts]
+        # greedy heaviest-first: no rank exceeds the mean by more than one disk
+        assert max(loads) <= sum(cells) / world + max(cells)
+        assert parts == partition(cells, world)
+    assert partition([5.0, 1.0], 4) == [[0], [1], [], []]
+    assert partition([], 2) == [[], []]
+    with pytest.raises(ValueError):
+        partition([1.0], 0)
+    with pytest.raises(ValueError):
+        partition([-1.0], 2)
+
+
+def _ensemble_disks():
+    from penguin_b200 import params as P
+
+    return [P.reference_disk(nr, 3 * nr, q=q).replace(kill_flag=0)
+            for nr, q in ((32, 1e-3), (64, 3e-4), (32, 0.0), (48, 1e-4), (32, 5e-4))]
+
+
+def _ensemble_rank(rank: int, world: int, port: int, out: str) -> None:
+    """One rank of a partitioned ensemble: its share of the disks, then the gather."""
+    _env(rank, world, port)
+    from oracle.oracle import Oracle
+    from penguin_b200 import initial as I
+    from penguin_b200.replicas import Replicas
+
+    job = Replicas("gloo", timeout_s=60)
+    ps = _ensemble_disks()
+    mine = job.share([p.cells for p in ps])
+    res = {}
+    for k in mine:
+        o = Oracle(ps[k], I.disk_state(ps[k], seed=100 + k), 0.0)
+        o.run(2)
+        res[k] = float(np.sum(o.interior()["r"]))
+    allres = job.gather({"rank": job.rank, "disks": mine, "r_sum": res})
+    job.close()
+    if job.printer:
+        with open(out, "w") as f:
+            json.dump(allres, f)
+
+
+def test_partitioned_ensemble_gloo(tmp_path):
+    procs, outs = _run_ranks(_ensemble_rank, 2, tmp_path)
+    assert [q.exitcode for q in procs] == [0, 0]
+    allres = json.load(open(outs[0]))
+    assert [r["rank"] for r in allres] == [0, 1]
+    got = {int(k): v for r in allres for k, v in r["r_sum"].items()}
+    ps = _ensemble_disks()
+    assert sorted(got) == list(range(len(ps)))
+    assert all(r["disks"] for r in allres)
+    from oracle.oracle import Oracle
+    from penguin_b200 import initial as I
+
+    for k, p in enumerate(ps):
+        o = Oracle(p, I.disk_state(p, seed=100 + k), 0.0)
+        o.run(2)
+        assert got[k] == float(np.sum(o.interior()["r"]))
