@@ -436,7 +436,6 @@ def main():
 
     from penguin_b200.replicas import Replicas
 
-    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
     job = Replicas("nccl")
     world, local = job.world, job.local
 

@@ -43,6 +43,8 @@ class Replicas:
             backend = "nccl" if torch.cuda.is_available() else "gloo"
         self.backend = backend
         self.device = torch.device("cuda", self.local) if backend == "nccl" else torch.device("cpu")
+        if backend == "nccl":
+            torch.cuda.set_device(self.local)  # this process's GPU, before the group binds one
         self.dist = None
         if self.world > 1:
             import torch.distributed as dist
