@@ -52,7 +52,7 @@ def _replica_rank(rank: int, world: int, port: int, out: str) -> None:
     p = _small_disk()
     o = Oracle(p, I.disk_state(p, seed=job.seed(1234)), 0.0)
     if rank == 1:
-        time.sleep(0.5)           # the other rank must wait for this one at the barrier
+        time.sleep(1.5)           # the other rank must wait for this one at the barrier
     t0 = time.perf_counter()
     job.barrier()
     waited = time.perf_counter() - t0
@@ -93,7 +93,7 @@ def test_two_replicas_gloo(tmp_path):
     assert all(r["world"] == 2 for r in res)
     assert [r["printer"] for r in res] == [True, False]
     # the barrier held rank 0 until the late rank arrived
-    assert res[0]["waited"] > 0.3
+    assert res[0]["waited"] > 0.75
     # every rank sees the slowest rank's time, and counts both ranks' zone-updates
     assert all(r["worst"] == 20.0 for r in res)
     for r in res:
