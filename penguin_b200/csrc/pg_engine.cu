@@ -329,6 +329,8 @@ struct Engine {
     Cell* ave = nullptr;                     // time average (pg_disk_set_average)
     double* snap = nullptr;                  // pinned staging of snapshots
     size_t snap_n = 0;
+    double* xfer = nullptr;                  // device staging of host exchanges (xfer_buffer)
+    size_t xfer_n = 0;
 
     ~Engine() {
         for (auto& g : graph)
@@ -347,6 +349,7 @@ struct Engine {
         cudaFree(dbuf[1]);
         cudaFree(ave);
         if (snap) cudaFreeHost(snap);
+        cudaFree(xfer);
         cudaFree(grid);
         cudaFree(tab);
         cudaFree(part);
@@ -354,6 +357,26 @@ struct Engine {
         if (own_stream && stream) cudaStreamDestroy(stream);
     }
 };
+
+// Device staging for the host <-> device exchanges of the state, the dust and
+// the time average (interior planes, up to 4 x xres*yres doubles).  Allocated on
+// first use and kept, so an exchange neither allocates nor frees device memory
+// (a per-call stream-ordered allocation goes back to the driver at every
+// synchronisation under the default pool threshold and is mapped again at the
+// next call).  Every user runs on E.stream; a larger request waits for the
+// stream before replacing the buffer.
+static pg_status xfer_buffer(Engine& E, size_t count, double** out) {
+    if (E.xfer_n < count) {
+        PG_CUDA(cudaStreamSynchronize(E.stream));
+        cudaFree(E.xfer);
+        E.xfer = nullptr;
+        E.xfer_n = 0;
+        PG_CUDA(cudaMalloc(&E.xfer, count * sizeof(double)));
+        E.xfer_n = count;
+    }
+    *out = E.xfer;
+    return PG_OK;
+}
 
 // Builds the grid (owned mode) or adopts the caller's device grid, then all tables.
 static pg_status engine_setup(Engine& E, const double* dev_xa, const double* dev_xv, const double* dev_ya,
@@ -808,13 +831,15 @@ pg_status pg_disk_set_state(pg_disk* dk, double t, const double* r, const double
     PG_CUDA(cudaSetDevice(E.device));
     const size_t n = (size_t)d.xres * d.yres;
     double* stage = nullptr;
-    PG_CUDA(cudaMallocAsync(&stage, 4 * n * sizeof(double), E.stream));
+    {
+        const pg_status sx = xfer_buffer(E, 4 * n, &stage);
+        if (sx != PG_OK) return sx;
+    }
     PG_CUDA(cudaMemcpyAsync(stage, r, n * sizeof(double), cudaMemcpyHostToDevice, E.stream));
     PG_CUDA(cudaMemcpyAsync(stage + n, p, n * sizeof(double), cudaMemcpyHostToDevice, E.stream));
     PG_CUDA(cudaMemcpyAsync(stage + 2 * n, u, n * sizeof(double), cudaMemcpyHostToDevice, E.stream));
     if (v) PG_CUDA(cudaMemcpyAsync(stage + 3 * n, v, n * sizeof(double), cudaMemcpyHostToDevice, E.stream));
     const pg_status s = set_state_device(E, t, stage, stage + n, stage + 2 * n, v ? stage + 3 * n : nullptr);
-    cudaFreeAsync(stage, E.stream);
     return s;
 }
 
@@ -948,7 +973,10 @@ pg_status pg_disk_get_state(pg_disk* dk, double* r, double* p, double* u, double
     PG_CUDA(cudaSetDevice(E.device));
     const size_t n = (size_t)d.xres * d.yres;
     double* stage = nullptr;
-    PG_CUDA(cudaMallocAsync(&stage, 4 * n * sizeof(double), E.stream));
+    {
+        const pg_status sx = xfer_buffer(E, 4 * n, &stage);
+        if (sx != PG_OK) return sx;
+    }
     pg_status s0 = resolve_cur(E);
     if (s0 != PG_OK) return s0;
     k_extract<<<1184, 256, 0, E.stream>>>(d, E.buf[E.cur], stage, stage + n, stage + 2 * n, stage + 3 * n);
@@ -957,7 +985,6 @@ pg_status pg_disk_get_state(pg_disk* dk, double* r, double* p, double* u, double
     PG_CUDA(cudaMemcpyAsync(p, stage + n, n * sizeof(double), cudaMemcpyDeviceToHost, E.stream));
     PG_CUDA(cudaMemcpyAsync(u, stage + 2 * n, n * sizeof(double), cudaMemcpyDeviceToHost, E.stream));
     if (v) PG_CUDA(cudaMemcpyAsync(v, stage + 3 * n, n * sizeof(double), cudaMemcpyDeviceToHost, E.stream));
-    PG_CUDA(cudaFreeAsync(stage, E.stream));
     if (t_out) PG_CUDA(cudaMemcpyAsync(t_out, &E.sc->t, sizeof(double), cudaMemcpyDeviceToHost, E.stream));
     PG_CUDA(cudaStreamSynchronize(E.stream));
     return PG_OK;
@@ -973,13 +1000,15 @@ pg_status pg_disk_set_dust(pg_disk* dk, const double* r, const double* u, const 
     if (s0 != PG_OK) return s0;
     const size_t n = (size_t)d.xres * d.yres;
     double* stage = nullptr;
-    PG_CUDA(cudaMallocAsync(&stage, 3 * n * sizeof(double), E.stream));
+    {
+        const pg_status sx = xfer_buffer(E, 3 * n, &stage);
+        if (sx != PG_OK) return sx;
+    }
     PG_CUDA(cudaMemcpyAsync(stage, r, n * sizeof(double), cudaMemcpyHostToDevice, E.stream));
     PG_CUDA(cudaMemcpyAsync(stage + n, u, n * sizeof(double), cudaMemcpyHostToDevice, E.stream));
     PG_CUDA(cudaMemcpyAsync(stage + 2 * n, v, n * sizeof(double), cudaMemcpyHostToDevice, E.stream));
     launch_dust_fill(d, E.dbuf[E.cur], stage, stage + n, stage + 2 * n, E.stream);
     PG_CUDA(cudaGetLastError());
-    PG_CUDA(cudaFreeAsync(stage, E.stream));
     // the CFL rate of the first step includes the dust speeds
     launch_cfl(d, E.buf[E.cur], E.stream, E.dbuf[E.cur]);
     PG_CUDA(cudaGetLastError());
@@ -997,13 +1026,15 @@ pg_status pg_disk_get_dust(pg_disk* dk, double* r, double* u, double* v) {
     if (s0 != PG_OK) return s0;
     const size_t n = (size_t)d.xres * d.yres;
     double* stage = nullptr;
-    PG_CUDA(cudaMallocAsync(&stage, 3 * n * sizeof(double), E.stream));
+    {
+        const pg_status sx = xfer_buffer(E, 3 * n, &stage);
+        if (sx != PG_OK) return sx;
+    }
     launch_dust_extract(d, E.dbuf[E.cur], stage, stage + n, stage + 2 * n, E.stream);
     PG_CUDA(cudaGetLastError());
     PG_CUDA(cudaMemcpyAsync(r, stage, n * sizeof(double), cudaMemcpyDeviceToHost, E.stream));
     PG_CUDA(cudaMemcpyAsync(u, stage + n, n * sizeof(double), cudaMemcpyDeviceToHost, E.stream));
     PG_CUDA(cudaMemcpyAsync(v, stage + 2 * n, n * sizeof(double), cudaMemcpyDeviceToHost, E.stream));
-    PG_CUDA(cudaFreeAsync(stage, E.stream));
     PG_CUDA(cudaStreamSynchronize(E.stream));
     return PG_OK;
 }
@@ -1312,14 +1343,16 @@ pg_status pg_disk_get_average(pg_disk* dk, double* r, double* p, double* u, doub
     PG_CUDA(cudaSetDevice(E.device));
     const size_t n = (size_t)d.xres * d.yres;
     double* stage = nullptr;
-    PG_CUDA(cudaMallocAsync(&stage, 4 * n * sizeof(double), E.stream));
+    {
+        const pg_status sx = xfer_buffer(E, 4 * n, &stage);
+        if (sx != PG_OK) return sx;
+    }
     k_extract<<<1184, 256, 0, E.stream>>>(d, E.ave, stage, stage + n, stage + 2 * n, stage + 3 * n);
     PG_CUDA(cudaGetLastError());
     PG_CUDA(cudaMemcpyAsync(r, stage, n * sizeof(double), cudaMemcpyDeviceToHost, E.stream));
     PG_CUDA(cudaMemcpyAsync(p, stage + n, n * sizeof(double), cudaMemcpyDeviceToHost, E.stream));
     PG_CUDA(cudaMemcpyAsync(u, stage + 2 * n, n * sizeof(double), cudaMemcpyDeviceToHost, E.stream));
     if (v) PG_CUDA(cudaMemcpyAsync(v, stage + 3 * n, n * sizeof(double), cudaMemcpyDeviceToHost, E.stream));
-    PG_CUDA(cudaFreeAsync(stage, E.stream));
     PG_CUDA(cudaStreamSynchronize(E.stream));
     return PG_OK;
 }
