@@ -89,6 +89,8 @@ struct pg_ens {
     int cur = 0;
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     Tune32 tune = DEFAULT_TUNE32;  // launch configuration of the passes (pg_ens_autotune)
+    double* xfer = nullptr;        // device staging of host exchanges, kept between calls
+    size_t xfer_n = 0;
 
     ~pg_ens() {
         for (auto& g : graph)
@@ -109,11 +111,18 @@ struct pg_ens {
         cudaFree(dMaps);
         cudaFree(dPart);
         cudaFree(dDoff);
+        cudaFree(xfer);
         if (own_stream && stream) cudaStreamDestroy(stream);
     }
 };
 
 namespace {
+
+// Device staging for a member's state or dust on its way to or from the host
+// (up to 4 interior planes of the largest member), allocated on first use and
+// kept: exchanges allocate nothing.  All users run on e->stream; a larger
+// request waits for the stream before replacing the buffer.
+pg_status xfer_buffer(pg_ens* e, size_t count, double** out);
 
 // Kernels of one step reading buffer `in`: clocks, planet tables, five passes.
 pg_status enqueue_step(pg_ens* e, int in) {
@@ -154,6 +163,19 @@ pg_status arm_clocks(pg_ens* e, double end_time) {
 pg_status check_index(const pg_ens* e, int k) {
     if (!e) return ens_fail(PG_ERR_ARG, "null ensemble");
     if (k < 0 || k >= e->n) return ens_fail(PG_ERR_ARG, "disk index out of range");
+    return PG_OK;
+}
+
+pg_status xfer_buffer(pg_ens* e, size_t count, double** out) {
+    if (e->xfer_n < count) {
+        ENS_CUDA(cudaStreamSynchronize(e->stream));
+        cudaFree(e->xfer);
+        e->xfer = nullptr;
+        e->xfer_n = 0;
+        ENS_CUDA(cudaMalloc(&e->xfer, count * sizeof(double)));
+        e->xfer_n = count;
+    }
+    *out = e->xfer;
     return PG_OK;
 }
 
@@ -338,13 +360,15 @@ pg_status pg_ens_set_state(pg_ens* e, int k, double t, const double* r, const do
     EDisk& D = e->disks[k];
     const size_t n = (size_t)D.v.xres * D.v.yres;
     double* st = nullptr;
-    ENS_CUDA(cudaMallocAsync(&st, 3 * n * sizeof(double), e->stream));
+    {
+        const pg_status sx = xfer_buffer(e, 3 * n, &st);
+        if (sx != PG_OK) return sx;
+    }
     ENS_CUDA(cudaMemcpyAsync(st, r, n * sizeof(double), cudaMemcpyHostToDevice, e->stream));
     ENS_CUDA(cudaMemcpyAsync(st + n, u, n * sizeof(double), cudaMemcpyHostToDevice, e->stream));
     if (v) ENS_CUDA(cudaMemcpyAsync(st + 2 * n, v, n * sizeof(double), cudaMemcpyHostToDevice, e->stream));
     launch_fill32(e->dV + k, e->cur, st, st + n, v ? st + 2 * n : nullptr, e->stream);
     ENS_CUDA(cudaGetLastError());
-    ENS_CUDA(cudaFreeAsync(st, e->stream));
     if (D.v.dust)  // a restart's dust is init_CD (the reference's load_grid reads the gas only)
         ENS_CUDA(cudaMemsetAsync(D.v.dbuf[e->cur], 0, sizeof(float) * NPL * (size_t)D.v.pitch * D.v.yarr,
                                  e->stream));
@@ -376,14 +400,16 @@ pg_status pg_ens_get_state(pg_ens* e, int k, double* r, double* p, double* u, do
     EDisk& D = e->disks[k];
     const size_t n = (size_t)D.v.xres * D.v.yres;
     double* st = nullptr;
-    ENS_CUDA(cudaMallocAsync(&st, 4 * n * sizeof(double), e->stream));
+    {
+        const pg_status sx = xfer_buffer(e, 4 * n, &st);
+        if (sx != PG_OK) return sx;
+    }
     launch_extract32(e->dV + k, e->cur, st, st + n, st + 2 * n, st + 3 * n, e->stream);
     ENS_CUDA(cudaGetLastError());
     ENS_CUDA(cudaMemcpyAsync(r, st, n * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
     ENS_CUDA(cudaMemcpyAsync(p, st + n, n * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
     ENS_CUDA(cudaMemcpyAsync(u, st + 2 * n, n * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
     ENS_CUDA(cudaMemcpyAsync(v, st + 3 * n, n * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
-    ENS_CUDA(cudaFreeAsync(st, e->stream));
     if (t_out) ENS_CUDA(cudaMemcpyAsync(t_out, &D.v.d64.sc->t, sizeof(double), cudaMemcpyDeviceToHost, e->stream));
     ENS_CUDA(cudaStreamSynchronize(e->stream));
     return PG_OK;
@@ -524,12 +550,14 @@ pg_status pg_ens_set_dust(pg_ens* e, int k, const double* r, const double* u, co
     ENS_CUDA(cudaSetDevice(e->device));
     const size_t n = (size_t)D.v.xres * D.v.yres;
     double* st = nullptr;
-    ENS_CUDA(cudaMallocAsync(&st, 3 * n * sizeof(double), e->stream));
+    {
+        const pg_status sx = xfer_buffer(e, 3 * n, &st);
+        if (sx != PG_OK) return sx;
+    }
     ENS_CUDA(cudaMemcpyAsync(st, r, n * sizeof(double), cudaMemcpyHostToDevice, e->stream));
     ENS_CUDA(cudaMemcpyAsync(st + n, u, n * sizeof(double), cudaMemcpyHostToDevice, e->stream));
     ENS_CUDA(cudaMemcpyAsync(st + 2 * n, v, n * sizeof(double), cudaMemcpyHostToDevice, e->stream));
     launch_dfill32(e->dV + k, e->cur, st, st + n, st + 2 * n, e->stream);
-    ENS_CUDA(cudaFreeAsync(st, e->stream));
     ENS_CUDA(cudaMemsetAsync(&D.v.d64.sc->vmax_bits, 0, sizeof(unsigned long long), e->stream));
     launch_cfl32(e->dV + k, e->cur, e->stream);
     ENS_CUDA(cudaGetLastError());
@@ -546,13 +574,15 @@ pg_status pg_ens_get_dust(pg_ens* e, int k, double* r, double* u, double* v) {
     ENS_CUDA(cudaSetDevice(e->device));
     const size_t n = (size_t)D.v.xres * D.v.yres;
     double* st = nullptr;
-    ENS_CUDA(cudaMallocAsync(&st, 3 * n * sizeof(double), e->stream));
+    {
+        const pg_status sx = xfer_buffer(e, 3 * n, &st);
+        if (sx != PG_OK) return sx;
+    }
     launch_dextract32(e->dV + k, e->cur, st, st + n, st + 2 * n, e->stream);
     ENS_CUDA(cudaGetLastError());
     ENS_CUDA(cudaMemcpyAsync(r, st, n * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
     ENS_CUDA(cudaMemcpyAsync(u, st + n, n * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
     ENS_CUDA(cudaMemcpyAsync(v, st + 2 * n, n * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
-    ENS_CUDA(cudaFreeAsync(st, e->stream));
     ENS_CUDA(cudaStreamSynchronize(e->stream));
     return PG_OK;
 }
