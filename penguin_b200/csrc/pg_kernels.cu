@@ -54,7 +54,8 @@ constexpr int ST_TILE = (ST_TILE_N + 15) / 16 * 16;     // rounded so every TMA 
 constexpr int ST_VIS_N = ST_HX * ST_HY * 2;
 constexpr int ST_VIS = (ST_VIS_N + 15) / 16 * 16;
 constexpr size_t K1_SMEM = (size_t)2 * ST_TILE * 8 + 16 + 128;
-constexpr size_t K5_SMEM = (size_t)(3 * ST_TILE + 2 * ST_VIS) * 8 + 16 + 128;
+constexpr int ST_GRAV = (ST_HX * ST_HY * 3 + 15) / 16 * 16;  // kick2: gravity of the predictor, per tile cell
+constexpr size_t K5_SMEM = (size_t)(3 * ST_TILE + 2 * ST_VIS + ST_GRAV) * 8 + 16 + 128;
 
 // --------------------------------------------------------- source terms
 struct Grav {
@@ -641,7 +642,8 @@ __global__ void __launch_bounds__(ST_THREADS)
     auto stage = [&](int n) { return smem + (n & 1) * ST_TILE; };                   // C with 1 halo
     auto vstage = [&](int n) { return smem + 2 * ST_TILE + (n & 1) * ST_VIS; };  // stress of the first evaluation
     double* tp = smem + 2 * ST_TILE + 2 * ST_VIS;                      // predicted state with 1 halo
-    uint64_t* bar = reinterpret_cast<uint64_t*>(tp + ST_TILE);
+    double* gc = tp + ST_TILE;  // gravity at the predictor's cells: the corrector's is the same (time `next`)
+    uint64_t* bar = reinterpret_cast<uint64_t*>(gc + ST_GRAV);
     Scalars* sc = d.sc;
     if (sc->done) return;
     const int tid = threadIdx.x;
@@ -684,13 +686,20 @@ __global__ void __launch_bounds__(ST_THREADS)
                     const double* c = tile + it * 5;
                     const Cell C{c[0], c[1], c[2], c[3], c[4]};
                     const Grav g = body_gravity(d, i, j, 1, pl, st);
+                    gc[3 * it] = g.gx;
+                    gc[3 * it + 1] = g.gy;
+                    gc[3 * it + 2] = g.gz;
                     const Cell Q = kick<true>(d, C, d.irad[i], g, tvis[2 * it], tvis[2 * it + 1], hdt, hdt);
                     double* o = tp + it * 5;
                     o[0] = Q.r; o[1] = Q.p; o[2] = Q.u; o[3] = Q.v; o[4] = Q.w;
                 }
                 __syncthreads();
                 // radial ghosts of the predicted state (boundx2, src/boundary/boundary.cu:722-820):
-                // the stencil only reaches the innermost ghost column on either side
+                // the stencil only reaches the innermost ghost column on either side, which
+                // only tiles at the radial edges hold (a CTA-uniform test, so the barrier
+                // below is skipped by all threads or none)
+                const bool redge = i0 - 1 <= NPAD - 1 || i0 - 2 + ST_HX >= NPAD + d.xres;
+                if (redge) {
                 for (int it = tid; it < ST_HX * ST_HY; it += ST_THREADS) {
                     const int hx = it % ST_HX, hy = it / ST_HX;
                     const int i = i0 - 1 + hx;
@@ -709,6 +718,7 @@ __global__ void __launch_bounds__(ST_THREADS)
                     if (bnd == 2) o[2] = -o[2];
                 }
                 __syncthreads();
+                }
             }
 
             const int hx = 1 + tid % ST_TX, hy = 1 + tid / ST_TX;
@@ -724,7 +734,8 @@ __global__ void __launch_bounds__(ST_THREADS)
                     gather9(tp, hx, hy, nu, u, v, nr);
                     viscous(d.visx + 5 * i, d.visy + 4 * j, u, v, nr, vx, vy);
                 }
-                const Grav g = body_gravity(d, i, j, 1, pl, st);
+                const int ic = 3 * (hy * ST_HX + hx);
+                const Grav g = VISC ? Grav{gc[ic], gc[ic + 1], gc[ic + 2]} : body_gravity(d, i, j, 1, pl, st);
                 double Tu = C.u, Tv = C.v;
                 Cell Q = kick<VISC>(d, C, d.irad[i], g, vx, vy, hdt, hdt, &Tu, &Tv);
                 // cooling over dt/2; the predictor cools over mdt = dt/2 as well, so Q.p is also
