@@ -475,30 +475,35 @@ __global__ void __launch_bounds__(Sw<NW>::THREADS, Sw<NW>::MINB)
             r[k] = c[0]; p[k] = c[1]; u[k] = c[3]; v[k] = c[4]; w[k] = c[2];
         }
         const double* wt = d.wy + 6 * s;
+        // CTA-uniform: with the isothermal EOS the pressure is reset from the density
+        // after the update, so its flux is never used; in 2D the z-velocity is
+        // identically zero, so its flux is zero
+        const bool need_p = d.eos != 0, need_w = d.ndim != 2;
         const Par R = recon(wt, r[0], r[1], r[2], r[3], r[4], 0.0);
-        const Par P = recon(wt, p[0], p[1], p[2], p[3], p[4], 0.0);
         const Par U = recon(wt, u[0], u[1], u[2], u[3], u[4], 0.0);
-        const Par V = recon(wt, v[0], v[1], v[2], v[3], v[4], 0.0);
         const Par W = recon(wt, w[0], w[1], w[2], w[3], w[4], 0.0);
+        Par P = R, V = R;
+        if (need_p) P = recon(wt, p[0], p[1], p[2], p[3], p[4], 0.0);
+        if (need_w) V = recon(wt, v[0], v[1], v[2], v[3], v[4], 0.0);
         const double xl = d.ya[s], xr = d.ya[s + 1];
-        double fr, fp, fu, fv, fw;
+        double fr, fp = 0.0, fu, fv = 0.0, fw;
         int face;
         if (speed > 0.0) {  // this cell is upwind of its upper face
             const double x0 = xr - speed * sdt;
             const Frac q_ = frac_right(lim01((x0 - xl) * idx));
             fr = aveR(q_, R);
-            fp = aveR(q_, P);
+            if (need_p) fp = aveR(q_, P);
             fu = aveR(q_, U) * fr;
-            fv = aveR(q_, V) * fr;
+            if (need_w) fv = aveR(q_, V) * fr;
             fw = aveR(q_, W) * fr;
             face = t + 1;
         } else {  // ... of its lower face
             const double x0 = xl - speed * sdt;
             const Frac q_ = frac_left(lim01((x0 - xl) * idx));
             fr = aveL(q_, R);
-            fp = aveL(q_, P);
+            if (need_p) fp = aveL(q_, P);
             fu = aveL(q_, U) * fr;
-            fv = aveL(q_, V) * fr;
+            if (need_w) fv = aveL(q_, V) * fr;
             fw = aveL(q_, W) * fr;
             face = t;
         }
