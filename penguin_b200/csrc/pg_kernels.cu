@@ -310,8 +310,11 @@ __global__ void __launch_bounds__(Sw<NW>::THREADS, Sw<NW>::MINB)
         const Par R = recon(wt, r[0], r[1], r[2], r[3], r[4], flat);
         const Par P = recon(wt, p[0], p[1], p[2], p[3], p[4], flat);
         const Par U = recon(wt, u[0], u[1], u[2], u[3], u[4], flat);
-        const Par V = recon(wt, v[0], v[1], v[2], v[3], v[4], flat);
-        const Par W = recon(wt, w[0], w[1], w[2], w[3], w[4], flat);
+        // in 2D the z-velocity (v here for DIR 1, w for DIR 0) is identically zero, and the
+        // reconstruction of a zero stencil is exactly {+0, a0, +0}: skip it (CTA-uniform)
+        const bool flat2d = d.ndim == 2;
+        const Par V = (DIR == 1 && flat2d) ? Par{0.0, v[2], 0.0} : recon(wt, v[0], v[1], v[2], v[3], v[4], flat);
+        const Par W = (DIR == 0 && flat2d) ? Par{0.0, w[2], 0.0} : recon(wt, w[0], w[1], w[2], w[3], w[4], flat);
         const double xl = fa[sc_], xr = fa[sc_ + 1];
         const double sdt = (DIR == 0) ? dt : dt * irad_q;
         const Half a = state_at_left_edge(gam, xl, idx, sdt, cs0, r[2], p[2], u[2], R, P, U, V, W);
