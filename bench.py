@@ -110,9 +110,10 @@ class Clocks:
                 "samples": len(rows)}
 
 
-def cpu_baseline(p, state, t0, budget_s=15.0):
+def cpu_baseline(p, state, t0, budget_s=15.0, keep=False):
     """The oracle (CPU restatement of the reference step, OpenMP over all host
-    cores) on the same workload, for a bounded number of steps."""
+    cores) on the same workload, for a bounded number of steps.  keep=True also
+    returns the oracle, advanced by 1 + the timed steps, for a parity check."""
     from oracle.oracle import Oracle
 
     o = Oracle(p, state, t0)
@@ -124,29 +125,65 @@ def cpu_baseline(p, state, t0, budget_s=15.0):
     o.run(n)
     el = time.perf_counter() - t
     cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
-    return {"value": p.cells * n / el, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": f"{n} steps of the full {p.xres}x{p.yres} workload after 1 warm-up step ({el:.1f} s)"}
+    cb = {"value": p.cells * n / el, "unit": UNIT, "cores": cores, "kind": "port",
+          "sample": f"{n} steps of the full {p.xres}x{p.yres} workload after 1 warm-up step ({el:.1f} s)"}
+    if keep:
+        return cb, o, 1 + n
+    o.close()
+    return cb
+
+
+def config_of(p, world):
+    """The workload description both arms print."""
+    return {"workload": f"planet-disk {p.xres}x{p.yres} FP64 (plain form), seeded 1e-4 Sigma noise, t0=0",
+            "cells_per_gpu": p.cells, "state_bytes": 2 * 40 * (p.xres + 6) * (p.yres + 6),
+            "l2": "inputs larger than L2 (two 127 MB AoS state buffers)",
+            "parallelism": f"replicas x{world}" if world > 1 else "single device"}
+
+
+REFERENCE_BUDGET_S = 150.0
 
 
 def run_reference(args, rank, world):
-    """Reference arm: the reference has no CPU implementation of the step, so
-    the CPU restatement (oracle/) stands in, on all host cores."""
+    """Reference arm: the reference has no CPU implementation of the step (its
+    only path is its CUDA build), so the CPU restatement (oracle/) stands in,
+    on all host cores: W untimed warm-up steps, then K timed steps of the same
+    workload (fewer only when K steps would exceed REFERENCE_BUDGET_S, and then
+    the line says how many ran)."""
     if rank != 0:
         return
+    from oracle.oracle import Oracle
     from penguin_b200 import initial as I
 
     p = workload()
     st = I.disk_state(p, seed=1234)
-    cb = cpu_baseline(p, st, 0.0, budget_s=max(5.0, min(60.0, 2.0 * args.steps / 100.0)))
+    o = Oracle(p, st, 0.0)
+    t = time.perf_counter()
+    o.run(1)
+    one = time.perf_counter() - t
+    W = max(1, min(args.warmup, int(0.2 * REFERENCE_BUDGET_S / max(one, 1e-3))))
+    if W > 1:
+        o.run(W - 1)
+    K = max(1, min(args.steps, int(REFERENCE_BUDGET_S / max(one, 1e-3))))
+    t = time.perf_counter()
+    o.run(K)
+    el = time.perf_counter() - t
+    o.close()
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    value = p.cells * K / el
+    cb = {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+          "sample": f"{K} timed steps of the full {p.xres}x{p.yres} workload after {W} warm-up steps ({el:.1f} s)"}
     line = {
-        "metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": 1000.0 * p.cells / cb["value"], "higher_is_better": True,
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": K,
+        "warmup": W, "ms_per_step": 1000.0 * el / K, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"planet-disk {p.xres}x{p.yres} FP64, seeded 1e-4 Sigma noise", "parallelism": "cpu"},
+        "config": config_of(p, args.gpus),
         "impl": "reference",
         "cpu_baseline": cb,
-        "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    if K != args.steps or W != args.warmup:
+        line["steps_requested"], line["warmup_requested"] = args.steps, args.warmup
     print(json.dumps(line), flush=True)
 
 
@@ -189,18 +226,23 @@ def measure_fp32(p, state, K, W, local, stream, pk):
     return out
 
 
-def measure_ensemble(local, stream, steps):
+def measure_ensemble(job, local, stream, steps):
     """48 seeded disks of uneven size: one FP32-mixed ensemble (one persistent
     launch per pass, graph-captured step) against the same disks run one after
-    another by the plain FP64 form, `steps` steps each with their own dt."""
+    another by the plain FP64 form, `steps` steps each with their own dt.  With
+    several ranks each rank runs its share of whole disks (Replicas.share) as
+    one ensemble, both arms are timed as the max over ranks, and rank 0 gathers
+    every disk's final mass."""
     from penguin_b200 import initial as I
     from penguin_b200 import params as P
     from penguin_b200.disk import Disk
     from penguin_b200.ensemble import Ensemble
 
-    ps = P.disk_ensemble()
-    sts = [I.disk_state(p, seed=100 + k) for k, p in enumerate(ps)]
-    cells = sum(p.cells for p in ps)
+    ps_all = P.disk_ensemble()
+    mine = job.share([p.cells for p in ps_all])
+    ps = [ps_all[k] for k in mine]
+    sts = [I.disk_state(ps_all[k], seed=100 + k) for k in mine]
+    cells_all = sum(p.cells for p in ps_all)
     e = Ensemble(ps, device=local, stream=stream.cuda_stream)
     for k, st in enumerate(sts):
         e.set_state(k, 0.0, st)
@@ -209,8 +251,10 @@ def measure_ensemble(local, stream, steps):
     tuning = e.autotune()
     e.run(1)
     e.sync()
-    ms_e = timed(stream, lambda: e.run(steps))
+    job.barrier(e.sync)
+    ms_e = job.max_over_ranks(timed(stream, lambda: e.run(steps)))
     e.check()
+    masses = {k: e.totals(n)[0] for n, k in enumerate(mine)}
     launches = e.kernels_per_step * steps
     e.close()
     # each disk timed on its own (device time of its graph launches), summed;
@@ -227,13 +271,19 @@ def measure_ensemble(local, stream, steps):
         ms_s += timed(stream, lambda: d.run(steps))
         d.check()
         d.close()
-    v_e = cells * steps / (ms_e / 1000.0)
-    v_s = cells * steps / (ms_s / 1000.0)
-    return {"disks": len(ps), "cells": cells, "steps": steps, "value": v_e, "ms_per_step": ms_e / steps,
-            "gpu_launches": launches, "sequential_fp64": {"value": v_s, "ms_per_step": ms_s / steps},
-            "over_sequential_fp64": v_e / v_s, "tuning": tuning,
-            "note": "both arms autotuned (ensemble: pass variants and CTA caps; each FP64 disk: pencils per tile, CTA caps)",
-            "config": "Nr in 32*[4,16], Nphi=3Nr, q log-U[1e-5,3e-3], alpha log-U[1e-4,1e-2], h/r U[0.03,0.08], seed 2024"}
+    ms_s = job.max_over_ranks(ms_s)
+    gathered = job.gather(masses)
+    v_e = cells_all * steps / (ms_e / 1000.0)
+    v_s = cells_all * steps / (ms_s / 1000.0)
+    out = {"disks": len(ps_all), "cells": cells_all, "steps": steps, "value": v_e, "ms_per_step": ms_e / steps,
+           "gpu_launches": launches, "sequential_fp64": {"value": v_s, "ms_per_step": ms_s / steps},
+           "over_sequential_fp64": v_e / v_s, "tuning": tuning,
+           "note": "both arms autotuned (ensemble: pass variants and CTA caps; each FP64 disk: pencils per tile, CTA caps)",
+           "config": "Nr in 32*[4,16], Nphi=3Nr, q log-U[1e-5,3e-3], alpha log-U[1e-4,1e-2], h/r U[0.03,0.08], seed 2024"}
+    if job.world > 1:
+        out["partition"] = {"ranks": job.world, "disks_per_rank": [len(g) for g in gathered] if gathered else None,
+                            "scaling": "strong (the same 48 disks split by whole disks)"}
+    return out
 
 
 DUST_STEPS = 2000
@@ -245,7 +295,10 @@ ALGO_BYTES_DUST = {"time": 0, "kick1": 96 + 64, "sweep_x": 80 + 64, "sweep_y": 8
 
 def measure_dust(local, stream, steps, pk):
     """Gas + one dust fluid, 768x2048, alpha 1e-4, q 3e-4, dust-to-gas 0.01,
-    Stokes 0.01 and 0.1, plain FP64 form: `steps` steps each from t = 0."""
+    Stokes 0.01 and 0.1: the plain FP64 form for 3 warm-up + `steps` timed steps
+    from t = 0, then the FP32-mixed form for the same number of steps from the
+    same state (warm-up first, then reset; no end time, so no clip and no
+    copy-through steps), and the dust profiles of the two compared at that step."""
     import numpy as np
 
     from penguin_b200 import initial as I
@@ -256,44 +309,47 @@ def measure_dust(local, stream, steps, pk):
     out = {}
     for st in (0.01, 0.1):
         p = P.dust_disk(stokes=st)
+        init = I.disk_state(p, seed=SEED_DUST)
         d = Disk(p, device=local, stream=stream.cuda_stream)
-        d.set_state(0.0, I.disk_state(p, seed=SEED_DUST))
+        d.set_state(0.0, init)
         m0 = float(d.get_dust()["r"].sum())
         d.run(3)
         d.sync()
         ms = timed(stream, lambda: d.run(steps))
         d.check()
-        prof = d.profile(20)
+        t64, _, n64 = d.clock()
         dust = d.get_dust()
-        t_end = d.clock()[0]
-        # the FP32-mixed form of the same disk to the same time: its speed and the
-        # error of the azimuthally averaged dust profile against the FP64 form
+        gas = d.get_state()
+        prof = d.profile(20)  # advances the disk; everything compared is read before
+        # the FP32-mixed form of the same disk, the same number of steps
         e = Ensemble([p], device=local, stream=stream.cuda_stream)
-        e.set_state(0, 0.0, I.disk_state(p, seed=SEED_DUST))
+        e.set_state(0, 0.0, init)
         e.run(3)
         e.sync()
-        e.set_state(0, 0.0, I.disk_state(p, seed=SEED_DUST))
-        ms32 = timed(stream, lambda: e.run(10 ** 7, t_end))
+        e.set_state(0, 0.0, init)
+        ms32 = timed(stream, lambda: e.run(n64))
         e.check()
-        n32 = e.clock(0)[2]
+        t32, _, n32 = e.clock(0)
         d32 = e.get_dust(0)
         prof64, prof32 = dust["r"].mean(axis=0), d32["r"].mean(axis=0)
-        g64, g32 = d.get_state()["r"].mean(axis=0), e.get_state(0)["r"].mean(axis=0)
+        g64, g32 = gas["r"].mean(axis=0), e.get_state(0)["r"].mean(axis=0)
         fp32 = {"value": p.cells * n32 / (ms32 / 1000.0), "ms_per_step": ms32 / n32, "steps": n32,
                 "dust_profile_l1_vs_fp64": float(np.abs(prof32 - prof64).sum() / np.abs(prof64).sum()),
                 "dust_sigma_l1_vs_fp64": float(np.abs(d32["r"] - dust["r"]).sum() / np.abs(dust["r"]).sum()),
                 "gas_profile_l1_vs_fp64": float(np.abs(g32 - g64).sum() / np.abs(g64).sum()),
-                "t": t_end, "gpu_launches": e.kernels_per_step * n32}
+                "t": t32, "t_fp64": t64, "gpu_launches": e.kernels_per_step * n32}
         e.close()
         out[f"stokes_{st}"] = {
             "value": p.cells * steps / (ms / 1000.0), "ms_per_step": ms / steps, "steps": steps,
+            "steps_from_t0": n64,
             "stage_ms": prof, "roofline": roofline_of(prof, p.cells, ALGO_BYTES_DUST, pk),
             "gpu_launches": d.kernels_per_step * steps,
             "dust_sigma_sum_over_initial": float(dust["r"].sum()) / m0,
             "fp32_mixed": fp32,
         }
+        out[f"stokes_{st}"]["fp32_mixed"]["over_fp64"] = fp32["value"] / out[f"stokes_{st}"]["value"]
         d.close()
-    return {"workload": "768x2048 gas+dust planet-disk, FP64 form and FP32-mixed form to the same time",
+    return {"workload": "768x2048 gas+dust planet-disk, FP64 form and FP32-mixed form, the same steps from t=0",
             "dtype": "f64 / f32 (FP64 dt, shift)", **out}
 
 
@@ -394,6 +450,28 @@ def measure_adjoint(steps, local, stream, timing_steps=None):
             v.append(loss(m.forward(s0, replay=True)))
         fdt.append((v[0] - v[1]) / (2 * step))
     m.set_theta(*theta)
+    # the loss as a function of each parameter at 9 points 1e-6 apart (relative):
+    # the forward map is two-valued there (a branch decision at a rounding-level
+    # tie flips with the parameter's last bits, shifting the loss by a fixed
+    # amount), so a central difference whose two points fall on different levels
+    # is no derivative; the two-level least-squares slope is, and the plain
+    # central difference at 1e-6 is reported beside it
+    scan = []
+    for k in range(3):
+        ss = [j * 1.0e-6 for j in range(-4, 5)]
+        Ls = []
+        for s_ in ss:
+            th = list(theta)
+            th[k] = theta[k] * (1.0 + s_)
+            m.set_theta(*th)
+            Ls.append(loss(m.forward(s0, replay=True)))
+        m.set_theta(*theta)
+        fit = two_level_slope(np.array(ss) * theta[k], np.array(Ls))
+        central = (Ls[5] - Ls[3]) / (2.0e-6 * theta[k])
+        scan.append({"two_level_slope": fit["slope"], "levels": fit["levels"], "jump": fit["jump"],
+                     "central_1e-6": central,
+                     "rel_err_two_level": abs(fit["slope"] - gth[k]) / abs(gth[k]),
+                     "rel_err_central_1e-6": abs(central - gth[k]) / abs(gth[k])})
     out_line = {
         "workload": "256x768 gradient disk, FP64 forward + adjoint, checkpoint every 64 steps",
         "steps": steps, "timing_steps": tsteps, "forward_ms_per_step": ms_f / tsteps,
@@ -408,9 +486,39 @@ def measure_adjoint(steps, local, stream, timing_steps=None):
                              "rel_err": {k: abs(ad_s - v) / abs(v) for k, v in fd_s.items()}},
         "fd_theta": {"names": ["q", "alpha", "h"], "adjoint": [float(v) for v in gth], "central_rel_step_1e-4": fdt,
                      "rel_err": [abs(a - b) / abs(b) for a, b in zip(gth, fdt)]},
+        "fd_theta_scan": {"names": ["q", "alpha", "h"], "points": "9 at relative spacing 1e-6", "per_parameter": scan},
     }
     m.close()
     return out_line
+
+
+def two_level_slope(x, y):
+    """Least-squares slope of y(x) allowing the samples to sit on two levels a
+    fixed jump apart.  A robust line (Theil-Sen: the median of the pairwise
+    slopes, which pairs on one level give exactly) leaves residuals in two
+    clusters; they are split at their largest gap when it exceeds 20x the spread
+    on either side, and y = a + J z + b x is solved with z the level of each
+    sample."""
+    import numpy as np
+
+    n = len(x)
+    pair = [(y[j] - y[i]) / (x[j] - x[i]) for i in range(n) for j in range(i + 1, n) if x[j] != x[i]]
+    b0 = float(np.median(pair))
+    r = y - b0 * x
+    order = np.argsort(r)
+    gaps = np.diff(r[order])
+    z = np.zeros_like(x)
+    if len(gaps):
+        g = int(np.argmax(gaps))
+        lo, hi = r[order[:g + 1]], r[order[g + 1:]]
+        spread = max(np.ptp(lo) if len(lo) > 1 else 0.0, np.ptp(hi) if len(hi) > 1 else 0.0)
+        if gaps[g] > 20.0 * spread and len(lo) >= 2 and len(hi) >= 2:
+            z[order[g + 1:]] = 1.0
+    if z.any():
+        a, J, b = np.linalg.lstsq(np.vstack([np.ones_like(x), z, x]).T, y, rcond=None)[0]
+    else:
+        (a, b), J = np.linalg.lstsq(np.vstack([np.ones_like(x), x]).T, y, rcond=None)[0], 0.0
+    return {"slope": float(b), "jump": float(J), "levels": [int((z == 0).sum()), int((z == 1).sum())]}
 
 
 def main():
@@ -529,11 +637,8 @@ def main():
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
         "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"planet-disk {p.xres}x{p.yres} FP64 (plain form), seeded 1e-4 Sigma noise, t0=0",
-                   "cells_per_gpu": cells, "state_bytes": 2 * 40 * (p.xres + 6) * (p.yres + 6),
-                   "l2": "inputs larger than L2 (two 127 MB AoS state buffers)",
-                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
-                   "tuning": tuning},
+        "config": config_of(p, world),
+        "tuning": tuning,
         "gpu_launches": disk.kernels_per_step * K,
         "stage_ms": prof,
         "roofline": {"bound": "hbm", "kernel": stage, "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
@@ -548,18 +653,79 @@ def main():
         f32["over_fp64"] = f32["value"] / (value / world)
         line["fp32_mixed"] = f32
     if "ensemble" in forms:
-        line["ensemble"] = measure_ensemble(local, stream, ENSEMBLE_STEPS)
+        line["ensemble"] = measure_ensemble(job, local, stream, ENSEMBLE_STEPS)
     if "dust" in forms:
         line["dust"] = measure_dust(local, stream, min(DUST_STEPS, max(K, 3)), pk)
     if "adjoint" in forms:
-        line["adjoint"] = measure_adjoint(min(ADJOINT_STEPS, max(K, 8)), local, stream,
-                                          min(ADJOINT_TIMING_STEPS, max(K, 8)))
+        # fixed sizes, independent of --steps: the finite-difference checks over
+        # ADJOINT_STEPS steps and the timing over ADJOINT_TIMING_STEPS (16
+        # checkpoint segments); together well under a second of GPU time
+        line["adjoint"] = measure_adjoint(ADJOINT_STEPS, local, stream, ADJOINT_TIMING_STEPS)
     if job.printer and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(p, state, 0.0)
+        cb, orc, n_orc = cpu_baseline(p, state, 0.0, keep=True)
+        line["cpu_baseline"] = cb
+        line["parity"] = parity_vs_oracle(p, state, orc, n_orc, local, stream)
+        orc.close()
+    line["summary"] = summary_of(line)
     if job.printer:
         print(json.dumps(line), flush=True)
     disk.close()
     job.close()
+
+
+def parity_vs_oracle(p, state, orc, n, local, stream):
+    """The oracle's state after the CPU-baseline leg (n steps of main.cu's loop
+    from the workload's initial state) against the CUDA path stepped the same n
+    steps from the same state: relative L1 of Sigma, p and the momentum vector."""
+    import numpy as np
+
+    from penguin_b200.disk import Disk
+
+    d = Disk(p, device=local, stream=stream.cuda_stream)
+    d.set_state(0.0, state)
+    d.run(n)
+    d.sync()
+    d.check()
+    t, _, steps = d.clock()
+    g, o = d.get_state(), orc.interior()
+    d.close()
+
+    def rl1(a, b):
+        return float(np.abs(a - b).sum() / np.abs(b).sum())
+
+    mom = float((np.abs(g["r"] * g["u"] - o["r"] * o["u"]) + np.abs(g["r"] * g["v"] - o["r"] * o["v"])).sum()
+                / (np.abs(o["r"] * o["u"]) + np.abs(o["r"] * o["v"])).sum())
+    return {"steps": int(steps), "rel_l1_r": rl1(g["r"], o["r"]), "rel_l1_p": rl1(g["p"], o["p"]),
+            "rel_l1_mom": mom, "t_rel_diff": abs(t - orc.t) / orc.t,
+            "against": "the oracle (CPU restatement of the reference step), same initial state and step count"}
+
+
+def summary_of(line):
+    """The ratios the north star states, in one place at the end of the line."""
+    out = {"fp64_gzone_s": line["value"] / 1e9, "fp64_ms_per_step": line["ms_per_step"],
+           "sweep_hbm_frac": line["roofline"]["frac"]}
+    if "e2e" in line:
+        out["e2e_gzone_s"] = line["e2e"]["value"] / 1e9
+    if "fp32_mixed" in line:
+        out["fp32_over_fp64"] = line["fp32_mixed"]["over_fp64"]
+    if "ensemble" in line:
+        out["ensemble_over_sequential_fp64"] = line["ensemble"]["over_sequential_fp64"]
+    if "dust" in line:
+        out["dust_fp32_over_fp64"] = {k: v["fp32_mixed"]["over_fp64"] for k, v in line["dust"].items()
+                                      if isinstance(v, dict) and "fp32_mixed" in v}
+    if "adjoint" in line:
+        a = line["adjoint"]
+        out["adjoint_over_forward"] = a["adjoint_over_forward"]
+        out["adjoint_fd_rel_err"] = {"sigma0_smooth_1e-6": a["fd_sigma0_smooth"]["rel_err"]["1e-06"],
+                                     "sigma0_noisy_1e-6": a["fd_sigma0"]["rel_err"]["1e-06"],
+                                     "theta_1e-4": a["fd_theta"]["rel_err"],
+                                     "theta_two_level_1e-6": [v["rel_err_two_level"]
+                                                              for v in a["fd_theta_scan"]["per_parameter"]]}
+    if "parity" in line:
+        q = line["parity"]
+        out["parity_rel_l1_max"] = max(q["rel_l1_r"], q["rel_l1_p"], q["rel_l1_mom"])
+        out["parity_steps"] = q["steps"]
+    return out
 
 
 if __name__ == "__main__":

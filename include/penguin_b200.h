@@ -10,9 +10,10 @@
  *        pg_grid_global_dt  <- double global_dt(Grid* hst, Grid* dev, double dt)   include/timestep.h:4
  *        pg_grid_solve      <- void solve(Grid* dev, double time, double dt)        include/solver.h:4
  *        pg_grid_init_orbadv<- void init_OrbAdv(Grid* dev)                          include/orbit.h:4
- *     A five-line C++ shim keeps those original names.  The
- *     reference fixes its parameters at compile time in include/parameters.h;
- *     here they are passed once through pg_configure().
+ *     A C++ shim (penguin_b200/shim/penguin_shim.cu) keeps those original
+ *     names so that main.cu relinks unchanged.  The reference fixes its
+ *     parameters at compile time in include/parameters.h; here they are
+ *     passed once through pg_configure().
  *
  *  2. The handle API (pg_disk_*) owns its buffers: used by the Python binding,
  *     the benchmark and the multi-step device-resident loop (CUDA graph).
@@ -124,16 +125,20 @@ pg_status pg_grid_release(void);
 /*
  * No counterpart in the reference.  The CFL step size of global_dt for callers
  * that cannot allocate device memory (their own pool or fixed budget owns the
- * GPU): it reads the caller's state C (xarr*yarr cells), faces xa/ya and
- * orb_rot (NULL = no orbital advection) and keeps its scratch in a fixed
- * 64 KiB file-scope device array instead of cudaMalloc'd memory.  Grids above
- * 8192*4096 interior cells are rejected (PG_ERR_CONFIG).  The first call on a
- * device resolves the array's device address once, with that device current.
- * Calls that overlap on the GPU share the array and race.
+ * GPU): it reads the caller's state C (xarr*yarr cells), the dust state CD
+ * (same layout; required when P->dust_flag is set, ignored otherwise: the dust
+ * speeds bound dt as in timestep.cu:64-75), faces xa and ya (ya unused and may
+ * be NULL when ndim == 1) and orb_rot (NULL = no orbital advection), and keeps
+ * its scratch in a fixed 64 KiB file-scope device array instead of
+ * cudaMalloc'd memory.  Grids above 8192*4096 interior cells are rejected
+ * (PG_ERR_CONFIG), as is a 1D grid with yres != 1.  The first call on a device
+ * resolves the array's device address once, with that device current; a
+ * process that resets that device must not call it there again.  Calls that
+ * overlap on the GPU share the array and race.
  * Blocking; dt = min(CFL dt, 1.1*dt_prev) like pg_grid_global_dt.
  */
-pg_status pg_global_dt_noalloc(const pg_params* P, const pg_cell* C, const double* xa, const double* ya,
-                               const double* orb_rot, double dt_prev, double* dt_out, void* stream);
+pg_status pg_global_dt_noalloc(const pg_params* P, const pg_cell* C, const pg_dust* CD, const double* xa,
+                               const double* ya, const double* orb_rot, double dt_prev, double* dt_out, void* stream);
 
 /* ------------------------------------------------------- handle API */
 typedef struct pg_disk pg_disk;
@@ -151,15 +156,28 @@ pg_status pg_disk_set_state(pg_disk* d, double t, const double* r, const double*
                             const double* v);
 /* The newest state back to host arrays; t_out may be NULL. */
 pg_status pg_disk_get_state(pg_disk* d, double* r, double* p, double* u, double* v, double* t_out);
-/* Autotuner: times every launch configuration of each pass of the step
-   (pencils per tile 8 or 4 for the sweeps and the residual advection, CTAs per
-   SM) on the disk's current state over `reps` launches and keeps the fastest;
-   the state is unchanged and results stay bit for bit the same.  choice (may
-   be NULL, 8 ints): pencils per tile of sweep_x, sweep_y, advect, then CTAs per
+/* Autotuner: times every launch configuration of each pass of the step on the
+   disk's current state over `reps` launches and keeps the fastest; the state is
+   unchanged and results stay bit for bit the same.  The sweeps and the
+   residual advection choose a tile variant (pg_sweep_variant: pencils per
+   tile, outputs per pencil, cells per thread, TMA stages in flight), every pass
+   its CTAs per SM.  It replaces the reference's fixed tiling
+   (include/parameters.h:81-97, x_xdiv / x_ydiv / y_xdiv / y_ydiv).  choice (may
+   be NULL, 8 ints): the variants of sweep_x, sweep_y, advect, then the CTAs per
    SM of kick1, sweep_x, sweep_y, advect, kick2 (0: all that fit).
    pg_disk_set_tuning applies a choice found earlier. */
 pg_status pg_disk_autotune(pg_disk* d, int reps, int* choice);
 pg_status pg_disk_set_tuning(pg_disk* d, const int* choice);
+/* Tile variant v of the FP64 sweeps and advection (0 .. 7), 6 ints: pencils
+   per tile, outputs per pencil, cells per thread, TMA stages, threads per CTA,
+   CTAs per SM its registers are compiled for.  PG_ERR_ARG past the last. */
+pg_status pg_sweep_variant(int v, int* out6);
+/* test support: the per-index 4th-order slope weights the kernels apply in
+   direction dir (0 radial, 1 azimuthal) of the grid P builds, 6 per index
+   (sL on the three differences left of the cell, then sR), host array of
+   6 * (xres + 6) or 6 * (yres + 6) doubles.  The reference evaluates the same
+   slopes per call (src/solver/recon/recon.cu:216-378).  Uses the GPU. */
+pg_status pg_recon_weights(const pg_params* P, int dir, double* w);
 /* Snapshots in the reference's checkpoint format (write_check_point /
    load_grid, src/output/output.cu:125-248; file names binary_<label>_<frame>,
    main.cu:403): t, interior faces, r, p, u, v (2D), then the dust fields.

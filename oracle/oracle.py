@@ -127,11 +127,14 @@ class Oracle:
         lib().orc_init_planet(self.h, t0)
         lib().orc_init_orbadv(self.h)
 
-    def __del__(self):
+    def close(self) -> None:
         h = getattr(self, "h", None)
         if h:
             lib().orc_destroy(h)
             self.h = None
+
+    def __del__(self):
+        self.close()
 
     def grid(self):
         xa = np.zeros(self.xarr + 1); xv = np.zeros(self.xarr)

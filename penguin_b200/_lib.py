@@ -22,7 +22,8 @@ EXPORTS = [
     "pg_configure", "pg_grid_init_orbadv", "pg_grid_global_dt", "pg_grid_solve", "pg_grid_release",
     "pg_global_dt_noalloc",
     "pg_disk_create", "pg_disk_destroy", "pg_disk_dims", "pg_disk_set_state", "pg_disk_get_state",
-    "pg_disk_set_dust", "pg_disk_get_dust", "pg_disk_autotune", "pg_disk_set_tuning",
+    "pg_disk_set_dust", "pg_disk_get_dust", "pg_disk_autotune", "pg_disk_set_tuning", "pg_sweep_variant",
+    "pg_recon_weights",
     "pg_disk_write_snapshot", "pg_disk_read_snapshot", "pg_disk_set_average", "pg_disk_reset_average",
     "pg_disk_get_average",
     "pg_disk_state_ptr", "pg_disk_global_dt", "pg_disk_solve", "pg_disk_run", "pg_disk_sync", "pg_disk_clock",
@@ -69,7 +70,7 @@ def lib() -> ctypes.CDLL:
         "pg_grid_global_dt": (i, [vp, vp, d, dp]),
         "pg_grid_solve": (i, [vp, d, d]),
         "pg_grid_release": (i, []),
-        "pg_global_dt_noalloc": (i, [PP, vp, vp, vp, vp, d, dp, vp]),
+        "pg_global_dt_noalloc": (i, [PP, vp, vp, vp, vp, vp, d, dp, vp]),
         "pg_disk_create": (i, [PP, i, vp, ctypes.POINTER(vp)]),
         "pg_disk_destroy": (i, [vp]),
         "pg_disk_dims": (i, [vp, ip, ip, ip]),
@@ -78,6 +79,8 @@ def lib() -> ctypes.CDLL:
         "pg_disk_set_dust": (i, [vp, dp, dp, dp]),
         "pg_disk_autotune": (i, [vp, i, ip]),
         "pg_disk_set_tuning": (i, [vp, ip]),
+        "pg_sweep_variant": (i, [i, ip]),
+        "pg_recon_weights": (i, [PP, i, dp]),
         "pg_disk_write_snapshot": (i, [vp, ctypes.c_char_p, i]),
         "pg_disk_read_snapshot": (i, [vp, ctypes.c_char_p, dp]),
         "pg_disk_set_average": (i, [vp, d]),

@@ -1903,6 +1903,9 @@ struct pg_adj {
     double* lamv_in = nullptr;
     double* work = nullptr;  // 4 interior planes
     double* dtab = nullptr;
+    // the azimuthal slope weights with the ghost rows taking their images'
+    // (the transposition of the sweep treats the periodic seam as one face)
+    double* wy_seam = nullptr;
     double* gth = nullptr;
     unsigned long long* err = nullptr;
     Scalars* ssc = nullptr;  // scratch copy of the device scalars
@@ -1993,6 +1996,19 @@ static pg_status adj_make_disk(pg_adj* a) {
     pg_status s = pg_disk_create(&a->P, a->device, a->stream, &a->disk);
     if (s != PG_OK) return s;
     a->E = disk_engine(a->disk);
+    // The production sweep evaluates the seam's ghost rows with their own
+    // weights, as the reference does: on a fine azimuth their rounding differs
+    // from the rows they image by ~1e-9 of a slope, so its seam has two faces a
+    // rounding apart.  The adjoint transposes the sweep with one face at the
+    // seam, so its passes read weights whose ghost rows are their images'.
+    const DiskView& d = engine_view(a->E);
+    std::vector<double> wy(6 * (size_t)d.yarr);
+    if (!a->wy_seam && (s = adj_alloc(a, &a->wy_seam, wy.size() * sizeof(double))) != PG_OK) return s;
+    ADJ_CUDA(cudaMemcpyAsync(wy.data(), d.wy, wy.size() * sizeof(double), cudaMemcpyDeviceToHost, a->stream));
+    ADJ_CUDA(cudaStreamSynchronize(a->stream));
+    periodic_seam_weights(wy.data(), d.ypad, d.yres);
+    ADJ_CUDA(cudaMemcpyAsync(a->wy_seam, wy.data(), wy.size() * sizeof(double), cudaMemcpyHostToDevice, a->stream));
+    ADJ_CUDA(cudaStreamSynchronize(a->stream));
     return adj_tables(a);
 }
 
@@ -2094,6 +2110,7 @@ pg_status pg_adj_destroy(pg_adj* a) {
     cudaFree(a->lamv_in);
     cudaFree(a->work);
     cudaFree(a->dtab);
+    cudaFree(a->wy_seam);
     cudaFree(a->gth);
     cudaFree(a->err);
     cudaFree(a->ssc);
@@ -2182,6 +2199,7 @@ pg_status pg_adj_forward(pg_adj* a, const double* sigma0, double t0, int nsteps,
 static Args base_args(pg_adj* a, int n, int slot, const pg_body* pl, int bank = 0) {
     Args g{};
     g.d = engine_view(a->E);
+    g.d.wy = a->wy_seam;
     g.pl[0] = pl[0];
     g.pl[1] = pl[1];
     const double tau = a->P.ramp_time;

@@ -238,13 +238,13 @@ __device__ __forceinline__ void block_max_to(unsigned long long* dst, double v) 
     }
 }
 
-// Two-stage TMA pipeline of a persistent CTA: tile k computes from stage k&1
-// while tile k+1 streams into the other stage.  Barrier k&1 completes phase
-// (k>>1)&1 when tile k has landed.
+// TMA pipeline of a persistent CTA with NS stages (NS - 1 tiles in flight while
+// one is computed): tile k computes from stage k % NS, barrier k % NS completes
+// phase (k / NS) & 1 when tile k has landed.
+template <int NS = 2>
 __device__ __forceinline__ void pipe_init(uint64_t* bar) {
     if (threadIdx.x == 0) {
-        mbar_init(&bar[0], 1);
-        mbar_init(&bar[1], 1);
+        for (int n = 0; n < NS; ++n) mbar_init(&bar[n], 1);
         fence_barrier_init();
     }
     __syncthreads();
@@ -260,14 +260,19 @@ __device__ __forceinline__ void issue_begin(uint64_t* bar, uint32_t bytes) {
 }
 // every thread of the CTA gets the same answer, so a timed-out wait makes the
 // whole CTA leave together
+template <int NS = 2>
 __device__ __forceinline__ bool pipe_wait(uint64_t* bar, int k, Scalars* sc) {
-    const bool ok = mbar_wait(&bar[k & 1], (uint32_t)((k >> 1) & 1), sc);
+    const bool ok = mbar_wait(&bar[k % NS], (uint32_t)((k / NS) & 1), sc);
     return __syncthreads_and(ok ? 1 : 0) != 0;
 }
 // after a timed-out wait: before the CTA leaves, wait (again bounded) for the
-// copy of tile k+1 if one was issued, so no copy lands in released shared memory
-__device__ __forceinline__ void pipe_drain(uint64_t* bar, int k, bool issued_next, Scalars* sc) {
-    if (threadIdx.x == 0 && issued_next) mbar_wait(&bar[(k + 1) & 1], (uint32_t)(((k + 1) >> 1) & 1), sc);
+// copies of tiles k+1 .. k+NS-1 that were issued (issued_ahead of them), so no
+// copy lands in released shared memory
+template <int NS = 2>
+__device__ __forceinline__ void pipe_drain(uint64_t* bar, int k, int issued_ahead, Scalars* sc) {
+    if (threadIdx.x == 0)
+        for (int m = 1; m <= issued_ahead && m < NS; ++m)
+            mbar_wait(&bar[(k + m) % NS], (uint32_t)(((k + m) / NS) & 1), sc);
 }
 
 }  // namespace pg

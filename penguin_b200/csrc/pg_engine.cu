@@ -78,90 +78,158 @@ static void make_grid(double* a, double* v, double amin, double amax, int res, i
 // the cell average and the cubic at the cell's left / right face as the PPM
 // slopes sL / sR (src/solver/recon/recon.cu:216-378, cells i-2..i+1 for sL and
 // i-1..i+2 for sR).  Those slopes are linear in the data with coefficients that
-// depend only on the grid; they are computed here once, in extended precision
-// and in coordinates centred on the cell (where the moments are well
-// conditioned), as weights on the differences of neighbouring averages.
+// depend only on the grid, so the kernels apply them as 3 weights per slope on
+// the differences of neighbouring averages.
+//
+// The reference evaluates the fit per call from grid moments (B, D below) whose
+// differences cancel: on the 1024-cell unit interval a third difference loses
+// ~11 of 53 bits, on the azimuthal grid ~20.  The rounded moments are the same
+// on every call, so they are a fixed, per-index deviation of the reference's
+// effective weights from the exact fit.  k_recon_terms evaluates exactly those
+// rounded moments with the reference's expressions (on the device, where the
+// compiler contracts them into FMAs as it does the reference's); the host then
+// expands the fit's algebra on them in extended precision.  The weights thus
+// carry the reference's fixed deviation; what remains is the rounding of its
+// per-call arithmetic on the data, which no weight can reproduce.
 typedef long double ld;
 
-static ld moment(int geom, ld xc, ld a, ld b, int m) {
-    // integral of w(x) (x - xc)^m over [a, b] with w = 1 (geom 0/3) or x (geom 1), in xi = x - xc
-    const ld A = a - xc, B = b - xc;
-    auto pw = [](ld x, int k) {
-        ld r = 1;
-        for (int i = 0; i < k; ++i) r *= x;
-        return r;
-    };
-    ld s = (pw(B, m + 1) - pw(A, m + 1)) / (m + 1);
-    if (geom == 1) s = (pw(B, m + 2) - pw(A, m + 2)) / (m + 2) + xc * s;
-    return s;
+// grid-only terms of one side of one cell: D02 D12 D22 D03 D04 E1 E2 T N g1 g2 g3
+constexpr int kReconTerms = 12;
+
+__global__ void k_recon_terms(const double* __restrict__ x, int ncell, int geom, double* __restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < 2 || i + 3 > ncell) return;
+    // recon.cu:222-301
+    const double x0 = x[i - 2], x1 = x[i - 1], x2 = x[i], x3 = x[i + 1], x4 = x[i + 2], x5 = x[i + 3];
+    double B02, B12, B22, B32, B42;
+    double B03, B13, B23, B33, B43;
+    double B04, B14, B24, B34, B44;
+    if (geom == 2) {
+        B02 = (x1*x1*x1*x1-x0*x0*x0*x0)/(x1*x1*x1-x0*x0*x0)/(4.0/3.0);
+        B12 = (x2*x2*x2*x2-x1*x1*x1*x1)/(x2*x2*x2-x1*x1*x1)/(4.0/3.0);
+        B22 = (x3*x3*x3*x3-x2*x2*x2*x2)/(x3*x3*x3-x2*x2*x2)/(4.0/3.0);
+        B32 = (x4*x4*x4*x4-x3*x3*x3*x3)/(x4*x4*x4-x3*x3*x3)/(4.0/3.0);
+        B42 = (x5*x5*x5*x5-x4*x4*x4*x4)/(x5*x5*x5-x4*x4*x4)/(4.0/3.0);
+        B03 = (x1*x1*x1*x1*x1-x0*x0*x0*x0*x0)/(x1*x1*x1-x0*x0*x0)/(5.0/3.0);
+        B13 = (x2*x2*x2*x2*x2-x1*x1*x1*x1*x1)/(x2*x2*x2-x1*x1*x1)/(5.0/3.0);
+        B23 = (x3*x3*x3*x3*x3-x2*x2*x2*x2*x2)/(x3*x3*x3-x2*x2*x2)/(5.0/3.0);
+        B33 = (x4*x4*x4*x4*x4-x3*x3*x3*x3*x3)/(x4*x4*x4-x3*x3*x3)/(5.0/3.0);
+        B43 = (x5*x5*x5*x5*x5-x4*x4*x4*x4*x4)/(x5*x5*x5-x4*x4*x4)/(5.0/3.0);
+        B04 = (x1*x1*x1*x1*x1*x1-x0*x0*x0*x0*x0*x0)/(x1*x1*x1-x0*x0*x0)/2.0;
+        B14 = (x2*x2*x2*x2*x2*x2-x1*x1*x1*x1*x1*x1)/(x2*x2*x2-x1*x1*x1)/2.0;
+        B24 = (x3*x3*x3*x3*x3*x3-x2*x2*x2*x2*x2*x2)/(x3*x3*x3-x2*x2*x2)/2.0;
+        B34 = (x4*x4*x4*x4*x4*x4-x3*x3*x3*x3*x3*x3)/(x4*x4*x4-x3*x3*x3)/2.0;
+        B44 = (x5*x5*x5*x5*x5*x5-x4*x4*x4*x4*x4*x4)/(x5*x5*x5-x4*x4*x4)/2.0;
+    } else if (geom == 1) {
+        B02 = (x1*x1*x1-x0*x0*x0)/(x1*x1-x0*x0)/1.5;
+        B12 = (x2*x2*x2-x1*x1*x1)/(x2*x2-x1*x1)/1.5;
+        B22 = (x3*x3*x3-x2*x2*x2)/(x3*x3-x2*x2)/1.5;
+        B32 = (x4*x4*x4-x3*x3*x3)/(x4*x4-x3*x3)/1.5;
+        B42 = (x5*x5*x5-x4*x4*x4)/(x5*x5-x4*x4)/1.5;
+        B03 = (x1*x1*x1*x1-x0*x0*x0*x0)/(x1*x1-x0*x0)/2.0;
+        B13 = (x2*x2*x2*x2-x1*x1*x1*x1)/(x2*x2-x1*x1)/2.0;
+        B23 = (x3*x3*x3*x3-x2*x2*x2*x2)/(x3*x3-x2*x2)/2.0;
+        B33 = (x4*x4*x4*x4-x3*x3*x3*x3)/(x4*x4-x3*x3)/2.0;
+        B43 = (x5*x5*x5*x5-x4*x4*x4*x4)/(x5*x5-x4*x4)/2.0;
+        B04 = (x1*x1*x1*x1*x1-x0*x0*x0*x0*x0)/(x1*x1-x0*x0)/2.5;
+        B14 = (x2*x2*x2*x2*x2-x1*x1*x1*x1*x1)/(x2*x2-x1*x1)/2.5;
+        B24 = (x3*x3*x3*x3*x3-x2*x2*x2*x2*x2)/(x3*x3-x2*x2)/2.5;
+        B34 = (x4*x4*x4*x4*x4-x3*x3*x3*x3*x3)/(x4*x4-x3*x3)/2.5;
+        B44 = (x5*x5*x5*x5*x5-x4*x4*x4*x4*x4)/(x5*x5-x4*x4)/2.5;
+    } else {
+        B02 = (x1*x1-x0*x0)/(x1-x0)/2.0;
+        B12 = (x2*x2-x1*x1)/(x2-x1)/2.0;
+        B22 = (x3*x3-x2*x2)/(x3-x2)/2.0;
+        B32 = (x4*x4-x3*x3)/(x4-x3)/2.0;
+        B42 = (x5*x5-x4*x4)/(x5-x4)/2.0;
+        B03 = (x1*x1*x1-x0*x0*x0)/(x1-x0)/3.0;
+        B13 = (x2*x2*x2-x1*x1*x1)/(x2-x1)/3.0;
+        B23 = (x3*x3*x3-x2*x2*x2)/(x3-x2)/3.0;
+        B33 = (x4*x4*x4-x3*x3*x3)/(x4-x3)/3.0;
+        B43 = (x5*x5*x5-x4*x4*x4)/(x5-x4)/3.0;
+        B04 = (x1*x1*x1*x1-x0*x0*x0*x0)/(x1-x0)/4.0;
+        B14 = (x2*x2*x2*x2-x1*x1*x1*x1)/(x2-x1)/4.0;
+        B24 = (x3*x3*x3*x3-x2*x2*x2*x2)/(x3-x2)/4.0;
+        B34 = (x4*x4*x4*x4-x3*x3*x3*x3)/(x4-x3)/4.0;
+        B44 = (x5*x5*x5*x5-x4*x4*x4*x4)/(x5-x4)/4.0;
+    }
+    double* o = out + 2 * kReconTerms * (size_t)i;
+    // left face (recon.cu:315-337): moments of cells i-2..i+1
+    {
+        const double D02 = B12-B02, D12 = B22-B12, D22 = B32-B22;
+        const double D03 = B13-B03, D13 = B23-B13, D23 = B33-B23;
+        const double D04 = B14-B04, D14 = B24-B14, D24 = B34-B24;
+        o[0] = D02; o[1] = D12; o[2] = D22; o[3] = D03; o[4] = D04;
+        o[5] = (D23*D02-D03*D22);
+        o[6] = (D13*D02 - D03*D12);
+        o[7] = (D02*D24 - D22*D04)/(D23*D02-D03*D22) - (D14*D02 - D04*D12)/(D13*D02 - D03*D12);
+        o[8] = (D14*D02 - D04*D12);
+        o[9] = (B22-x2); o[10] = (B23-x2*x2); o[11] = (B24-x2*x2*x2);
+    }
+    // right face (recon.cu:341-359): moments of cells i-1..i+2
+    {
+        const double D02 = B22-B12, D12 = B32-B22, D22 = B42-B32;
+        const double D03 = B23-B13, D13 = B33-B23, D23 = B43-B33;
+        const double D04 = B24-B14, D14 = B34-B24, D24 = B44-B34;
+        o += kReconTerms;
+        o[0] = D02; o[1] = D12; o[2] = D22; o[3] = D03; o[4] = D04;
+        o[5] = (D23*D02-D03*D22);
+        o[6] = (D13*D02 - D03*D12);
+        o[7] = (D02*D24 - D22*D04)/(D23*D02-D03*D22) - (D14*D02 - D04*D12)/(D13*D02 - D03*D12);
+        o[8] = (D14*D02 - D04*D12);
+        o[9] = (x3-B22); o[10] = (x3*x3-B23); o[11] = (x3*x3*x3-B24);
+    }
 }
 
-// weights on (a1-a0, a2-a1, a3-a2) of the jump between the average of cell `mid`
-// (of the 4 cells with faces f[0..4]) and the fitted cubic at face f[mid + side]
-static void cubic_jump_weights(int geom, const ld* f, int mid, int side, ld xc, ld* w3) {
-    ld A[4][4];  // A[k][m]: average of xi^m over cell k
-    for (int k = 0; k < 4; ++k) {
-        const ld m0 = moment(geom, xc, f[k], f[k + 1], 0);
-        for (int m = 0; m < 4; ++m) A[k][m] = moment(geom, xc, f[k], f[k + 1], m) / m0;
-    }
-    const ld xf = f[mid + side] - xc;
-    ld wa[4];
-    for (int e = 0; e < 4; ++e) {
-        // solve A c = unit vector e (Gaussian elimination with partial pivoting)
-        ld M[4][5];
-        for (int r = 0; r < 4; ++r) {
-            for (int c = 0; c < 4; ++c) M[r][c] = A[r][c];
-            M[r][4] = (r == e) ? 1 : 0;
-        }
-        for (int c = 0; c < 4; ++c) {
-            int piv = c;
-            for (int r = c + 1; r < 4; ++r)
-                if (fabsl(M[r][c]) > fabsl(M[piv][c])) piv = r;
-            if (piv != c)
-                for (int k = 0; k < 5; ++k) std::swap(M[c][k], M[piv][k]);
-            for (int r = c + 1; r < 4; ++r) {
-                const ld fct = M[r][c] / M[c][c];
-                for (int k = c; k < 5; ++k) M[r][k] -= fct * M[c][k];
-            }
-        }
-        ld cf[4];
-        for (int r = 3; r >= 0; --r) {
-            ld s = M[r][4];
-            for (int k = r + 1; k < 4; ++k) s -= M[r][k] * cf[k];
-            cf[r] = s / M[r][r];
-        }
-        // jump: side 0 -> average - cubic(left face); side 1 -> cubic(right face) - average
-        ld val = 0, avg = 0;
-        for (int m = 0; m < 4; ++m) {
-            ld xm = 1;
-            for (int i = 0; i < m; ++i) xm *= xf;
-            val += cf[m] * xm;
-            avg += cf[m] * A[mid][m];
-        }
-        wa[e] = (side == 0) ? avg - val : val - avg;
-    }
-    // weights on values -> weights on consecutive differences
-    for (int m = 0; m < 3; ++m) {
-        ld s = 0;
-        for (int k = m + 1; k < 4; ++k) s += wa[k];
-        w3[m] = s;
+// The slope of one side as the reference forms it from the differences
+// (d10, d21, d32) of its 4 cells (recon.cu:315-337 / 341-359):
+//   c3 = ((D02 d32 - D22 d10)/E1 - (D02 d21 - D12 d10)/E2) / T
+//   c2 = (D02 d21 - D12 d10)/E2 - c3 N/E2
+//   c1 = d10/D02 - c2 D03/D02 - c3 D04/D02
+//   s  = c1 g1 + c2 g2 + c3 g3
+// expanded into weights on (d10, d21, d32), in extended precision.
+static void side_weights(const double* q, double* w3) {
+    const ld D02 = q[0], D12 = q[1], D22 = q[2], D03 = q[3], D04 = q[4];
+    const ld E1 = q[5], E2 = q[6], T = q[7], N = q[8], g1 = q[9], g2 = q[10], g3 = q[11];
+    for (int k = 0; k < 3; ++k) {
+        const ld d10 = (k == 0), d21 = (k == 1), d32 = (k == 2);
+        const ld n2 = D02 * d21 - D12 * d10;
+        const ld c3 = ((D02 * d32 - D22 * d10) / E1 - n2 / E2) / T;
+        const ld c2 = n2 / E2 - c3 * N / E2;
+        const ld c1 = d10 / D02 - c2 * D03 / D02 - c3 * D04 / D02;
+        w3[k] = (double)(c1 * g1 + c2 * g2 + c3 * g3);
     }
 }
 
-static void recon_weights(int geom, const double* x, int ncell, double* w) {
-    for (int i = 0; i < ncell; ++i) {
-        double* wi = w + 6 * i;
-        for (int k = 0; k < 6; ++k) wi[k] = 0.0;
-        if (i < 2 || i + 3 > ncell) continue;
-        ld f[6];
-        for (int k = 0; k < 6; ++k) f[k] = (ld)x[i - 2 + k];
-        const ld xc = 0.5L * (f[2] + f[3]);
-        ld w3[3];
-        cubic_jump_weights(geom, f, 2, 0, xc, w3);  // cells i-2..i+1, left face of cell i
-        for (int k = 0; k < 3; ++k) wi[k] = (double)w3[k];
-        cubic_jump_weights(geom, f + 1, 1, 1, xc, w3);  // cells i-1..i+2, right face of cell i
-        for (int k = 0; k < 3; ++k) wi[3 + k] = (double)w3[k];
+// the ghost rows of the periodic azimuth take the weights of the rows they image
+// (the adjoint's transposition of the sweep treats the seam as one face)
+void periodic_seam_weights(double* wy, int ypad, int yres) {
+    for (int k = 1; k <= ypad; ++k)
+        for (int m = 0; m < 6; ++m) {
+            wy[6 * (ypad - k) + m] = wy[6 * (ypad + yres - k) + m];
+            wy[6 * (ypad + yres - 1 + k) + m] = wy[6 * (ypad - 1 + k) + m];
+        }
+}
+
+// weights of every index of one direction from the device faces x[ncell+1]
+static pg_status recon_weights(int geom, const double* dev_x, int ncell, double* w, cudaStream_t s) {
+    for (int k = 0; k < 6 * ncell; ++k) w[k] = 0.0;
+    if (ncell < 6) return PG_OK;  // no cell has the 6 faces of a 4-cell fit (1D tube: y)
+    double* terms = nullptr;
+    const size_t n = 2 * kReconTerms * (size_t)ncell;
+    PG_CUDA(cudaMalloc(&terms, sizeof(double) * n));
+    k_recon_terms<<<(ncell + 127) / 128, 128, 0, s>>>(dev_x, ncell, geom, terms);
+    cudaError_t e = cudaGetLastError();
+    std::vector<double> q(n);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(q.data(), terms, sizeof(double) * n, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    cudaFree(terms);
+    PG_CUDA(e);
+    for (int i = 2; i + 3 <= ncell; ++i) {
+        side_weights(&q[2 * kReconTerms * (size_t)i], w + 6 * i);
+        side_weights(&q[2 * kReconTerms * (size_t)i + kReconTerms], w + 6 * i + 3);
     }
+    return PG_OK;
 }
 
 // ------------------------------------------------------------- init_CD
@@ -237,11 +305,17 @@ static pg_status make_map(CUtensorMap* m, const void* base, uint64_t inner, uint
 static pg_status make_cell_maps(CellMaps& M, const Cell* buf, int xarr, int yarr) {
     if (M.base == buf) return PG_OK;
     pg_status s;
-    if ((s = make_map(&M.sweep_x, buf, 5ull * xarr, yarr, 5 * 38, 8)) != PG_OK) return s;
-    if ((s = make_map(&M.sweep_y, buf, 5ull * xarr, yarr, 5 * 10, 38)) != PG_OK) return s;
     if ((s = make_map(&M.stencil, buf, 5ull * xarr, yarr, 5 * 34, 10)) != PG_OK) return s;
-    if ((s = make_map(&M.sweep_x4, buf, 5ull * xarr, yarr, 5 * 38, 4)) != PG_OK) return s;
-    if ((s = make_map(&M.sweep_y4, buf, 5ull * xarr, yarr, 5 * 6, 38)) != PG_OK) return s;
+    for (int v = 0; v < NSWEEP_VARIANTS; ++v) {
+        const SweepVariant& g = SWEEP_VARIANTS[v];
+        const uint32_t tl = (uint32_t)(g.len + 2 * NPAD);
+        if (sweep_variant_x_ok(v)) {
+            if ((s = make_map(&M.sx[v], buf, 5ull * xarr, yarr, 5 * tl, (uint32_t)g.w)) != PG_OK) return s;
+        } else {
+            memset(&M.sx[v], 0, sizeof(CUtensorMap));
+        }
+        if ((s = make_map(&M.sy[v], buf, 5ull * xarr, yarr, 5 * (uint32_t)(g.w + 2), tl)) != PG_OK) return s;
+    }
     M.base = buf;
     return PG_OK;
 }
@@ -414,8 +488,15 @@ static pg_status engine_setup(Engine& E, const double* dev_xa, const double* dev
                         (P.twobd_flag ? 4 * (size_t)yarr : 0);
     PG_CUDA(cudaMalloc(&E.tab, sizeof(double) * ntab));
     std::vector<double> wx(6 * xarr), wy(6 * yarr);
-    recon_weights(P.geomx, xa.data(), xarr, wx.data());
-    recon_weights(P.geomy, ya.data(), yarr, wy.data());
+    {
+        pg_status ws = recon_weights(P.geomx, dev_xa, xarr, wx.data(), E.stream);
+        if (ws == PG_OK) ws = recon_weights(P.geomy, dev_ya, yarr, wy.data(), E.stream);
+        if (ws != PG_OK) return ws;
+        // The ghost rows of the periodic azimuth keep the weights of their own
+        // coordinates, as the reference evaluates them: their rounding differs
+        // from the rows they image (on a 3072-cell azimuth by ~1e-9 of a slope),
+        // so the seam has two slightly different faces, in the reference as here.
+    }
     PG_CUDA(cudaMemcpyAsync(E.tab, wx.data(), sizeof(double) * wx.size(), cudaMemcpyHostToDevice, E.stream));
     PG_CUDA(cudaMemcpyAsync(E.tab + 6 * xarr, wy.data(), sizeof(double) * wy.size(), cudaMemcpyHostToDevice, E.stream));
     PG_CUDA(cudaStreamSynchronize(E.stream));  // host vectors go out of scope
@@ -1199,12 +1280,14 @@ pg_status pg_disk_torque(pg_disk* dk, double* torque) {
 
 int pg_kernels_per_step(const pg_disk* dk) { return dk ? kernels_per_step(dk->E->view) : 0; }
 
-// Autotuner: for every pass, times each launch configuration (pencils per tile
-// W in {8, 4} for the sweeps and the advection; CTAs per SM from 1 to what
-// fits) on the disk's current state with CUDA events over `reps` launches and
-// keeps the fastest.  The state, clock and planet are restored afterwards; the
-// per-cell arithmetic does not depend on the configuration, so results stay
-// bit for bit the same.  choice (may be NULL): w[3] then cps[5].
+// Autotuner: for every pass, times each launch configuration (for the sweeps
+// and the advection each tile variant of SWEEP_VARIANTS: pencils per tile,
+// outputs per pencil, cells per thread, TMA stages; for every pass the CTAs per
+// SM from 1 to what fits) on the disk's current state with CUDA events over
+// `reps` launches and keeps the fastest.  The state, clock and planet are
+// restored afterwards; the per-cell arithmetic does not depend on the
+// configuration, so results stay bit for bit the same.  choice (may be NULL):
+// the variants of sweep_x, sweep_y, advect, then the CTA caps of the 5 passes.
 pg_status pg_disk_autotune(pg_disk* dk, int reps, int* choice) {
     if (!dk || reps < 1) return fail(PG_ERR_ARG, "bad argument");
     Engine& E = *dk->E;
@@ -1245,12 +1328,13 @@ pg_status pg_disk_autotune(pg_disk* dk, int reps, int* choice) {
     for (int p = 0; p < 5; ++p) {
         if ((p == 2 && d.ndim < 2) || (p == 3 && !(d.ndim > 1 && d.orbadv))) continue;
         float best_ms = 1.0e30f;
-        for (int w : {8, 4}) {
-            if (w == 4 && (p == 0 || p == 4)) continue;
-            const int occ = pass_occupancy(d, p, w);
+        const int nv = (p >= 1 && p <= 3) ? NSWEEP_VARIANTS : 1;
+        for (int v = 0; v < nv; ++v) {
+            if (p == 1 && !sweep_variant_x_ok(v)) continue;
+            const int occ = pass_occupancy(d, p, v);
             for (int cps = 1; cps <= occ; ++cps) {
                 Tune t = best;
-                if (p >= 1 && p <= 3) t.w[p - 1] = w;
+                if (p >= 1 && p <= 3) t.v[p - 1] = v;
                 t.cps[p] = cps;
                 launch(p, t);  // warm-up
                 PG_CUDA(cudaEventRecord(e0, E.stream));
@@ -1262,7 +1346,7 @@ pg_status pg_disk_autotune(pg_disk* dk, int reps, int* choice) {
                 PG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
                 if (ms < best_ms) {
                     best_ms = ms;
-                    if (p >= 1 && p <= 3) best.w[p - 1] = w;
+                    if (p >= 1 && p <= 3) best.v[p - 1] = v;
                     best.cps[p] = cps;
                 }
             }
@@ -1283,7 +1367,7 @@ pg_status pg_disk_autotune(pg_disk* dk, int reps, int* choice) {
     PG_CUDA(cudaFreeAsync(ssc, E.stream));
     PG_CUDA(cudaStreamSynchronize(E.stream));
     if (choice) {
-        for (int k = 0; k < 3; ++k) choice[k] = best.w[k];
+        for (int k = 0; k < 3; ++k) choice[k] = best.v[k];
         for (int k = 0; k < 5; ++k) choice[3 + k] = best.cps[k];
     }
     return PG_OK;
@@ -1421,12 +1505,45 @@ pg_status pg_disk_read_snapshot(pg_disk* dk, const char* path, double* t_out) {
     return s;
 }
 
+pg_status pg_recon_weights(const pg_params* P, int dir, double* w) {
+    if (!P || !w || (dir != 0 && dir != 1)) return fail(PG_ERR_ARG, "bad argument");
+    pg_status s = pg_check_params(P);
+    if (s != PG_OK) return s;
+    const int ypad = P->ndim > 1 ? NPAD : 0;
+    const int n = dir == 0 ? P->xres + 2 * NPAD : P->yres + 2 * ypad;
+    std::vector<double> a(n + 1), v(n);
+    if (dir == 0) make_grid(a.data(), v.data(), P->xmin, P->xmax, P->xres, NPAD, P->geomx, P->gridx);
+    else make_grid(a.data(), v.data(), P->ymin, P->ymax, P->yres, ypad, P->geomy, P->gridy);
+    double* dev = nullptr;
+    PG_CUDA(cudaMalloc(&dev, sizeof(double) * (n + 1)));
+    cudaError_t e = cudaMemcpy(dev, a.data(), sizeof(double) * (n + 1), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        cudaFree(dev);
+        PG_CUDA(e);
+    }
+    s = recon_weights(dir == 0 ? P->geomx : P->geomy, dev, n, w, 0);
+    cudaFree(dev);
+    return s;
+}
+
+pg_status pg_sweep_variant(int v, int* out6) {
+    if (v < 0 || v >= NSWEEP_VARIANTS || !out6) return fail(PG_ERR_ARG, "no such tile variant");
+    const SweepVariant& g = SWEEP_VARIANTS[v];
+    out6[0] = g.w;
+    out6[1] = g.len;
+    out6[2] = g.cpt;
+    out6[3] = g.stages;
+    sweep_variant_launch(v, &out6[4], &out6[5]);
+    return PG_OK;
+}
+
 pg_status pg_disk_set_tuning(pg_disk* dk, const int* choice) {
     if (!dk || !choice) return fail(PG_ERR_ARG, "bad argument");
     Tune t;
     for (int k = 0; k < 3; ++k) {
-        if (choice[k] != 8 && choice[k] != 4) return fail(PG_ERR_ARG, "pencils per tile must be 8 or 4");
-        t.w[k] = choice[k];
+        if (choice[k] < 0 || choice[k] >= NSWEEP_VARIANTS || (k == 0 && !sweep_variant_x_ok(choice[k])))
+            return fail(PG_ERR_ARG, "no such tile variant for this pass");
+        t.v[k] = choice[k];
     }
     for (int k = 0; k < 5; ++k) {
         if (choice[3 + k] < 0) return fail(PG_ERR_ARG, "CTAs per SM must be >= 0");

@@ -8,18 +8,29 @@
 
 namespace pg {
 
+// Tile variants of the FP64 sweeps and residual advection, the autotuner's knobs
+// (pg_disk_autotune): pencils per tile W, outputs per pencil L, cells per thread
+// in each phase, TMA stages in flight.  pg_kernels.cu instantiates each (SV<v>).
+struct SweepVariant {
+    int w, len, cpt, stages;
+};
+constexpr int NSWEEP_VARIANTS = 8;
+constexpr SweepVariant SWEEP_VARIANTS[NSWEEP_VARIANTS] = {
+    {8, 32, 1, 2}, {4, 32, 1, 2}, {16, 16, 1, 2}, {8, 16, 1, 2},
+    {8, 32, 2, 2}, {8, 32, 1, 3}, {4, 32, 1, 3}, {4, 64, 1, 2}};
+// the radial box holds 5 (L + 6) doubles in one row, at most 256 TMA elements
+inline bool sweep_variant_x_ok(int v) { return 5 * (SWEEP_VARIANTS[v].len + 2 * NPAD) <= 256; }
+
 // Tensor maps of one AoS cell buffer, one per tile shape.
 struct CellMaps {
     const void* base = nullptr;
-    CUtensorMap sweep_x;   // box {5*38, 8}: x-pencils
-    CUtensorMap sweep_y;   // box {5*10, 38}: y-pencils (one extra column each side for 16-B alignment)
-    CUtensorMap stencil;   // box {5*34, 10}: 32x8 cells + 1 halo
-    CUtensorMap sweep_x4;  // box {5*38, 4}: 4 x-pencils per tile
-    CUtensorMap sweep_y4;  // box {5*6, 38}: 4 y-pencils per tile
+    CUtensorMap stencil;                   // box {5*34, 10}: 32x8 cells + 1 halo
+    CUtensorMap sx[NSWEEP_VARIANTS];       // box {5*(L+6), W}: x-pencils (variants whose box fits)
+    CUtensorMap sy[NSWEEP_VARIANTS];       // box {5*(W+2), L+6}: y-pencils, one extra column each side
 };
 // Launch configuration of the FP64 passes (pg_disk_autotune).
 struct Tune {
-    int w[3] = {8, 8, 8};          // pencils per tile: sweep_x, sweep_y, advect (8 or 4)
+    int v[3] = {0, 0, 0};          // tile variant of sweep_x, sweep_y, advect (SWEEP_VARIANTS)
     int cps[5] = {0, 0, 0, 0, 0};  // CTAs per SM: kick1, sweep_x, sweep_y, advect, kick2 (0: all that fit)
 };
 struct VisMaps {
@@ -56,7 +67,10 @@ void launch_sweep_y(const DiskView& d, const CellMaps& in, Cell* out, cudaStream
 void launch_advect(const DiskView& d, const CellMaps& in, Cell* out, cudaStream_t s, const Tune* t = nullptr);
 void launch_kick2(const DiskView& d, const CellMaps& in, const VisMaps& vis, Cell* out, cudaStream_t s,
                   const pg_dust* din = nullptr, pg_dust* dout = nullptr, const Tune* t = nullptr);
-int pass_occupancy(const DiskView& d, int pass, int w);
+int pass_occupancy(const DiskView& d, int pass, int v);
+void sweep_variant_launch(int v, int* threads, int* minb);
+// the ghost rows of the periodic azimuth take the weights of the rows they image
+void periodic_seam_weights(double* wy, int ypad, int yres);
 void launch_init_planet(const DiskView& d, const pg_params& P, double t, cudaStream_t s);
 void launch_torque(const DiskView& d, const Cell* buf, double* part, int nblocks, cudaStream_t s);
 // compensated sum of n doubles in index order

@@ -26,25 +26,42 @@
 namespace pg {
 
 // ---------------------------------------------------------------- tiles
-// Sweep and advection tiles: SW_LEN outputs along the sweep times W pencils per
-// CTA; W (8 or 4) is chosen per pass by the autotuner (pg_disk_autotune).
-constexpr int SW_LEN = 32;                  // outputs along the sweep per CTA
-constexpr int SW_TL = SW_LEN + 2 * NPAD;    // 38 tile cells along the sweep
-constexpr int SW_P1 = SW_LEN + 2;           // cells reconstructed per pencil
-constexpr int SW_P2 = SW_LEN + 1;           // faces per pencil
-template <int W>
-struct Sw {
-    static constexpr int THREADS = (SW_P1 * W + 31) / 32 * 32;  // 288 for W 8, 160 for W 4
-    static constexpr int MINB = (W == 8) ? 2 : 4;                 // CTAs per SM the registers allow
-    static constexpr int YCOLS = W + 2;                           // y tiles start one column early (16-B TMA x)
-    static constexpr int XTILE = W * SW_TL * 5;                   // doubles
-    static constexpr int YTILE = SW_TL * YCOLS * 5;
-    static constexpr int TILE_MAX = (YTILE + 15) / 16 * 16;
-    static constexpr int NST = SW_P1 * W;                         // reconstructed cells
-    static constexpr int NFX = SW_P2 * W;                         // faces
-    static constexpr size_t SMEM = (size_t)(2 * TILE_MAX + 10 * NST + 7 * NFX) * 8 + 16 + 128;
-    static constexpr size_t AD_SMEM = (size_t)(2 * TILE_MAX + 5 * SW_TL * W) * 8 + 16 + 128;
+// Sweep and advection tiles: L outputs along the sweep times W pencils per CTA,
+// each thread taking CPT cells (or faces, or outputs) of a phase, with NS TMA
+// stages in flight (SwCfg).  The autotuner (pg_disk_autotune) picks one of the
+// variants listed in SWEEP_VARIANTS per pass; the per-cell arithmetic does not
+// depend on the choice.
+template <int W_, int L_, int CPT_, int NS_, int MINB_ = 0>
+struct SwCfg {
+    static constexpr int W = W_, L = L_, CPT = CPT_, NS = NS_;
+    static constexpr int TL = L + 2 * NPAD;                       // tile cells along the sweep
+    static constexpr int P1 = L + 2;                               // cells reconstructed per pencil
+    static constexpr int P2 = L + 1;                               // faces per pencil
+    static constexpr int NST = P1 * W;                             // reconstructed cells
+    static constexpr int NFX = P2 * W;                             // faces
+    static constexpr int NOUT = L * W;                             // outputs
+    static constexpr int THREADS = ((NST + CPT - 1) / CPT + 31) / 32 * 32;
+    // CTAs per SM the registers allow at ~96 registers a thread, unless given
+    static constexpr int MINB = MINB_ > 0 ? MINB_ : (65536 / (THREADS * 96) > 0 ? 65536 / (THREADS * 96) : 1);
+    static constexpr int YCOLS = W + 2;                            // y tiles start one column early (16-B TMA x)
+    static constexpr int XTILE = W * TL * 5;                       // doubles
+    static constexpr int YTILE = TL * YCOLS * 5;
+    static constexpr int TILE_MAX = ((XTILE > YTILE ? XTILE : YTILE) + 15) / 16 * 16;
+    static constexpr bool X_OK = 5 * TL <= 256;                    // a TMA box is at most 256 elements wide
+    static constexpr size_t SMEM = (size_t)(NS * TILE_MAX + 10 * NST + 7 * NFX) * 8 + 8 * NS + 128;
+    static constexpr size_t AD_SMEM = (size_t)(NS * TILE_MAX + 5 * TL * W) * 8 + 8 * NS + 128;
 };
+// The variants, in the order of SweepVariant ids (pg_internal.h SWEEP_VARIANTS).
+template <int V> struct SV;
+template <> struct SV<0> { using G = SwCfg<8, 32, 1, 2>; };   // default
+template <> struct SV<1> { using G = SwCfg<4, 32, 1, 2>; };
+template <> struct SV<2> { using G = SwCfg<16, 16, 1, 2>; };
+template <> struct SV<3> { using G = SwCfg<8, 16, 1, 2>; };
+template <> struct SV<4> { using G = SwCfg<8, 32, 2, 2>; };
+template <> struct SV<5> { using G = SwCfg<8, 32, 1, 3>; };
+template <> struct SV<6> { using G = SwCfg<4, 32, 1, 3>; };
+template <> struct SV<7> { using G = SwCfg<4, 64, 1, 2>; };   // azimuthal passes only (x box too wide)
+static_assert(NSWEEP_VARIANTS == 8, "SV<> and SWEEP_VARIANTS list the same variants");
 
 constexpr int ST_TX = 32, ST_TY = 8;        // stencil kernels: 32 x 8 outputs
 constexpr int ST_HX = ST_TX + 2, ST_HY = ST_TY + 2;
@@ -203,17 +220,18 @@ __device__ __forceinline__ double signal_rate(const DiskView& d, const Cell& c, 
 
 // ================================================================ sweeps
 // DIR 0: radial pencils (rows of the array), DIR 1: azimuthal pencils (columns).
-template <int DIR, int NW>
-__global__ void __launch_bounds__(Sw<NW>::THREADS, Sw<NW>::MINB)
+// G: the tile configuration (SwCfg).
+template <int DIR, class G>
+__global__ void __launch_bounds__(G::THREADS, G::MINB)
     k_sweep(const __grid_constant__ CUtensorMap tm, const DiskView d, Cell* __restrict__ out, int ntx, int ntiles) {
-    using G = Sw<NW>;
-    constexpr int SW_W = NW, SW_TILE_MAX = G::TILE_MAX, SW_NST = G::NST, SW_NFX = G::NFX, SWY_COLS = G::YCOLS;
-    constexpr int SWX_TILE = G::XTILE, SWY_TILE = G::YTILE;
+    constexpr int SW_W = G::W, SW_LEN = G::L, SW_TL = G::TL, SW_P1 = G::P1, SW_P2 = G::P2;
+    constexpr int SW_TILE_MAX = G::TILE_MAX, SW_NST = G::NST, SW_NFX = G::NFX, SWY_COLS = G::YCOLS;
+    constexpr int SWX_TILE = G::XTILE, SWY_TILE = G::YTILE, NS = G::NS, NT = G::THREADS;
     extern __shared__ __align__(128) double smem_raw[];
     double* smem = smem_base128(smem_raw);
-    auto stage = [&](int n) { return smem + (n & 1) * SW_TILE_MAX; };
-    double* st = smem + 2 * SW_TILE_MAX;  // [10][SW_NST] interface states
-    double* fl = st + 10 * SW_NST;        // [7][SW_NFX] fluxes
+    auto stage = [&](int n) { return smem + (n % NS) * SW_TILE_MAX; };
+    double* st = smem + NS * SW_TILE_MAX;  // [10][SW_NST] interface states
+    double* fl = st + 10 * SW_NST;         // [7][SW_NFX] fluxes
     uint64_t* bar = reinterpret_cast<uint64_t*>(fl + 7 * SW_NFX);
     __shared__ int s_inc[SW_W];
     Scalars* sc = d.sc;
@@ -231,16 +249,21 @@ __global__ void __launch_bounds__(Sw<NW>::THREADS, Sw<NW>::MINB)
     auto issue = [&](int tile, int k) {
         int s0, q0;
         origin(tile, s0, q0);
-        issue_begin(&bar[k & 1], bytes);
-        if (DIR == 0) issue_box(stage(k), &tm, 5 * (s0 - NPAD), q0, &bar[k & 1]);
-        else issue_box(stage(k), &tm, 5 * (q0 - 1), s0 - NPAD, &bar[k & 1]);
+        issue_begin(&bar[k % NS], bytes);
+        if (DIR == 0) issue_box(stage(k), &tm, 5 * (s0 - NPAD), q0, &bar[k % NS]);
+        else issue_box(stage(k), &tm, 5 * (q0 - 1), s0 - NPAD, &bar[k % NS]);
     };
-    pipe_init(bar);
+    pipe_init<NS>(bar);
     if ((int)blockIdx.x >= ntiles) return;
-    if (tid == 0) issue(blockIdx.x, 0);
+    if (tid == 0)
+        for (int m = 0; m < NS - 1; ++m)
+            if ((int)blockIdx.x + m * (int)gridDim.x < ntiles) issue(blockIdx.x + m * gridDim.x, m);
     int kt = 0;
     for (int tile_id = blockIdx.x; tile_id < ntiles; tile_id += gridDim.x, ++kt) {
-    if (tid == 0 && tile_id + (int)gridDim.x < ntiles) issue(tile_id + gridDim.x, kt + 1);
+    // tiles issued beyond this one (the one NS - 1 ahead is issued now)
+    int ahead = 0;
+    while (ahead < NS - 1 && tile_id + (ahead + 1) * (int)gridDim.x < ntiles) ++ahead;
+    if (tid == 0 && ahead == NS - 1) issue(tile_id + (NS - 1) * gridDim.x, kt + NS - 1);
     int s0, q0;
     origin(tile_id, s0, q0);
     double* tile = stage(kt);
@@ -263,14 +286,13 @@ __global__ void __launch_bounds__(Sw<NW>::THREADS, Sw<NW>::MINB)
         }
         s_inc[tid] = shift;
     }
-    if (!pipe_wait(bar, kt, sc)) {
-        pipe_drain(bar, kt, tile_id + (int)gridDim.x < ntiles, sc);
+    if (!pipe_wait<NS>(bar, kt, sc)) {
+        pipe_drain<NS>(bar, kt, ahead, sc);
         return;
     }
 
     // ---- P1: reconstruction + both edge states of every cell
-    if (tid < SW_NST) {
-        const int it = tid;
+    for (int it = tid; it < SW_NST; it += NT) {
         const int q = (DIR == 0) ? it / SW_P1 : it % SW_W;
         const int t = 2 + ((DIR == 0) ? it % SW_P1 : it / SW_W);
         const int s = s0 - NPAD + t;
@@ -333,8 +355,7 @@ __global__ void __launch_bounds__(Sw<NW>::THREADS, Sw<NW>::MINB)
     __syncthreads();
 
     // ---- P2: HLLC flux at every face (left state from cell t-1, right from cell t)
-    if (tid < SW_NFX) {
-        const int it = tid;
+    for (int it = tid; it < SW_NFX; it += NT) {
         const int q = (DIR == 0) ? it / SW_P2 : it % SW_W;
         const int t = 3 + ((DIR == 0) ? it % SW_P2 : it / SW_W);
         const int iL = (DIR == 0) ? q * SW_P1 + (t - 3) : (t - 3) * SW_W + q;
@@ -362,8 +383,7 @@ __global__ void __launch_bounds__(Sw<NW>::THREADS, Sw<NW>::MINB)
     __syncthreads();
 
     // ---- P3: flux differences, geometric sources, conservative update
-    if (tid < SW_LEN * SW_W) {
-        const int it = tid;
+    for (int it = tid; it < SW_LEN * SW_W; it += NT) {
         const int q = (DIR == 0) ? it / SW_LEN : it % SW_W;
         const int t = 3 + ((DIR == 0) ? it % SW_LEN : it / SW_W);
         const int s = s0 - NPAD + t;
@@ -418,20 +438,20 @@ __global__ void __launch_bounds__(Sw<NW>::THREADS, Sw<NW>::MINB)
             }
         }
     }
-    __syncthreads();  // stage k&1, the state / flux arrays and s_inc are free again
+    __syncthreads();  // stage k % NS, the state / flux arrays and s_inc are free again
     }
 }
 
 // ===================================================== residual advection
-template <int NW>
-__global__ void __launch_bounds__(Sw<NW>::THREADS, Sw<NW>::MINB)
+template <class G>
+__global__ void __launch_bounds__(G::THREADS, G::MINB)
     k_advect(const __grid_constant__ CUtensorMap tm, const DiskView d, Cell* __restrict__ out, int ntx, int ntiles) {
-    using G = Sw<NW>;
-    constexpr int SW_W = NW, SW_TILE_MAX = G::TILE_MAX, SW_NST = G::NST, SWY_COLS = G::YCOLS, SWY_TILE = G::YTILE;
+    constexpr int SW_W = G::W, SW_LEN = G::L, SW_TL = G::TL, SW_TILE_MAX = G::TILE_MAX, SW_NST = G::NST;
+    constexpr int SWY_COLS = G::YCOLS, SWY_TILE = G::YTILE, NS = G::NS, NT = G::THREADS;
     extern __shared__ __align__(128) double smem_raw[];
     double* smem = smem_base128(smem_raw);
-    auto stage = [&](int n) { return smem + (n & 1) * SW_TILE_MAX; };
-    double* fl = smem + 2 * SW_TILE_MAX;  // [5][SW_TL * SW_W] face fluxes, indexed by face t
+    auto stage = [&](int n) { return smem + (n % NS) * SW_TILE_MAX; };
+    double* fl = smem + NS * SW_TILE_MAX;  // [5][SW_TL * SW_W] face fluxes, indexed by face t
     uint64_t* bar = reinterpret_cast<uint64_t*>(fl + 5 * SW_TL * SW_W);
     Scalars* sc = d.sc;
     if (sc->done) return;
@@ -445,27 +465,31 @@ __global__ void __launch_bounds__(Sw<NW>::THREADS, Sw<NW>::MINB)
     auto issue = [&](int tile, int k) {
         int s0, q0;
         origin(tile, s0, q0);
-        issue_begin(&bar[k & 1], SWY_TILE * 8);
-        issue_box(stage(k), &tm, 5 * (q0 - 1), s0 - NPAD, &bar[k & 1]);
+        issue_begin(&bar[k % NS], SWY_TILE * 8);
+        issue_box(stage(k), &tm, 5 * (q0 - 1), s0 - NPAD, &bar[k % NS]);
     };
-    pipe_init(bar);
+    pipe_init<NS>(bar);
     if ((int)blockIdx.x >= ntiles) return;
-    if (tid == 0) issue(blockIdx.x, 0);
+    if (tid == 0)
+        for (int m = 0; m < NS - 1; ++m)
+            if ((int)blockIdx.x + m * (int)gridDim.x < ntiles) issue(blockIdx.x + m * gridDim.x, m);
     int kt = 0;
     for (int tile_id = blockIdx.x; tile_id < ntiles; tile_id += gridDim.x, ++kt) {
-    if (tid == 0 && tile_id + (int)gridDim.x < ntiles) issue(tile_id + gridDim.x, kt + 1);
+    int ahead = 0;
+    while (ahead < NS - 1 && tile_id + (ahead + 1) * (int)gridDim.x < ntiles) ++ahead;
+    if (tid == 0 && ahead == NS - 1) issue(tile_id + (NS - 1) * gridDim.x, kt + NS - 1);
     int s0, q0;
     origin(tile_id, s0, q0);
     double* tile = stage(kt);
-    if (!pipe_wait(bar, kt, sc)) {
-        pipe_drain(bar, kt, tile_id + (int)gridDim.x < ntiles, sc);
+    if (!pipe_wait<NS>(bar, kt, sc)) {
+        pipe_drain<NS>(bar, kt, ahead, sc);
         return;
     }
 
     // ---- P1: upwind PPM average over the swept fraction (advection.cu:20-67)
-    if (tid < SW_NST) {
-        const int q = tid % SW_W;
-        const int t = 2 + tid / SW_W;
+    for (int it = tid; it < SW_NST; it += NT) {
+        const int q = it % SW_W;
+        const int t = 2 + it / SW_W;
         const int s = min(s0 - NPAD + t, d.yarr - 1);
         const int i = min(q0 + q, d.xarr - 1);
         const double speed = d.res[i];
@@ -520,9 +544,9 @@ __global__ void __launch_bounds__(Sw<NW>::THREADS, Sw<NW>::MINB)
     __syncthreads();
 
     // ---- P2: flux difference and update_Cell_advect (advection.cu:88-105, 153-170)
-    if (tid < SW_LEN * SW_W) {
-        const int q = tid % SW_W;
-        const int t = 3 + tid / SW_W;
+    for (int it = tid; it < SW_LEN * SW_W; it += NT) {
+        const int q = it % SW_W;
+        const int t = 3 + it / SW_W;
         const int s = s0 - NPAD + t;
         const int i = q0 + q;
         if (s < NPAD + d.yres && i < NPAD + d.xres) {
@@ -1069,12 +1093,20 @@ cudaError_t set_kernel_attributes() {
         r = cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
         if (r != cudaSuccess) e = r;
     };
-    set((const void*)k_sweep<0, 8>, Sw<8>::SMEM);
-    set((const void*)k_sweep<1, 8>, Sw<8>::SMEM);
-    set((const void*)k_advect<8>, Sw<8>::AD_SMEM);
-    set((const void*)k_sweep<0, 4>, Sw<4>::SMEM);
-    set((const void*)k_sweep<1, 4>, Sw<4>::SMEM);
-    set((const void*)k_advect<4>, Sw<4>::AD_SMEM);
+    auto set_v = [&](auto tag) {
+        using G = typename decltype(tag)::G;
+        if constexpr (G::X_OK) set((const void*)k_sweep<0, G>, G::SMEM);
+        set((const void*)k_sweep<1, G>, G::SMEM);
+        set((const void*)k_advect<G>, G::AD_SMEM);
+    };
+    set_v(SV<0>{});
+    set_v(SV<1>{});
+    set_v(SV<2>{});
+    set_v(SV<3>{});
+    set_v(SV<4>{});
+    set_v(SV<5>{});
+    set_v(SV<6>{});
+    set_v(SV<7>{});
     set((const void*)k_kick1<true>, K1_SMEM);
     set((const void*)k_kick1<false>, K1_SMEM);
     set((const void*)k_kick2<true>, K5_SMEM);
@@ -1159,16 +1191,16 @@ static unsigned persistent_grid(const void* kernel, int threads, size_t smem, lo
 
 static int kernel_occupancy(const void* kernel, int threads, size_t smem) {
     // occupancy of each kernel, queried once (launches repeat every step)
-    static const void* keys[32] = {nullptr};
-    static int vals[32] = {0};
+    static const void* keys[64] = {nullptr};
+    static int vals[64] = {0};
     int per_sm = 0;
-    for (int n = 0; n < 32 && keys[n]; ++n)
+    for (int n = 0; n < 64 && keys[n]; ++n)
         if (keys[n] == kernel) per_sm = vals[n];
     if (per_sm == 0) {
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem) != cudaSuccess ||
             per_sm < 1)
             per_sm = 1;
-        for (int n = 0; n < 32; ++n)
+        for (int n = 0; n < 64; ++n)
             if (!keys[n]) {
                 keys[n] = kernel;
                 vals[n] = per_sm;
@@ -1191,34 +1223,59 @@ void launch_kick1(const DiskView& d, const CellMaps& in, Cell* out, double* vis,
     }
 }
 
-template <int DIR, int W>
-static void sweep_w(const DiskView& d, const CUtensorMap& m, Cell* out, cudaStream_t s, int cps) {
-    const int ntx = (int)cdiv(DIR == 0 ? d.xres : d.yres, SW_LEN);
-    const int nt = ntx * (int)cdiv(DIR == 0 ? d.yres : d.xres, W);
-    const unsigned g = persistent_grid((const void*)k_sweep<DIR, W>, Sw<W>::THREADS, Sw<W>::SMEM, nt, cps);
-    k_sweep<DIR, W><<<g, Sw<W>::THREADS, Sw<W>::SMEM, s>>>(m, d, out, ntx, nt);
+template <int DIR, class G>
+static void sweep_g(const DiskView& d, const CUtensorMap& m, Cell* out, cudaStream_t s, int cps) {
+    if constexpr (DIR == 0 && !G::X_OK) {
+        return;  // never chosen: the autotuner skips radial variants whose box does not fit
+    } else {
+        const int ntx = (int)cdiv(DIR == 0 ? d.xres : d.yres, G::L);
+        const int nt = ntx * (int)cdiv(DIR == 0 ? d.yres : d.xres, G::W);
+        const unsigned g = persistent_grid((const void*)k_sweep<DIR, G>, G::THREADS, G::SMEM, nt, cps);
+        k_sweep<DIR, G><<<g, G::THREADS, G::SMEM, s>>>(m, d, out, ntx, nt);
+    }
+}
+
+template <class G>
+static void advect_g(const DiskView& d, const CUtensorMap& m, Cell* out, cudaStream_t s, int cps) {
+    const int ntx = (int)cdiv(d.yres, G::L), nt = ntx * (int)cdiv(d.xres, G::W);
+    const unsigned g = persistent_grid((const void*)k_advect<G>, G::THREADS, G::AD_SMEM, nt, cps);
+    k_advect<G><<<g, G::THREADS, G::AD_SMEM, s>>>(m, d, out, ntx, nt);
+}
+
+// calls f(SV<v>{}) for the variant id v
+template <class F>
+static void with_variant(int v, F&& f) {
+    switch (v) {
+        case 1: f(SV<1>{}); break;
+        case 2: f(SV<2>{}); break;
+        case 3: f(SV<3>{}); break;
+        case 4: f(SV<4>{}); break;
+        case 5: f(SV<5>{}); break;
+        case 6: f(SV<6>{}); break;
+        case 7: f(SV<7>{}); break;
+        default: f(SV<0>{}); break;
+    }
+}
+
+static int variant_of(const Tune* t, int k, int dir) {
+    const int v = t ? t->v[k] : 0;
+    if (v < 0 || v >= NSWEEP_VARIANTS || (dir == 0 && !sweep_variant_x_ok(v))) return 0;
+    return v;
 }
 
 void launch_sweep_x(const DiskView& d, const CellMaps& in, Cell* out, cudaStream_t s, const Tune* t) {
-    if (t && t->w[0] == 4) sweep_w<0, 4>(d, in.sweep_x4, out, s, t->cps[1]);
-    else sweep_w<0, 8>(d, in.sweep_x, out, s, t ? t->cps[1] : 0);
+    const int v = variant_of(t, 0, 0);
+    with_variant(v, [&](auto tag) { sweep_g<0, typename decltype(tag)::G>(d, in.sx[v], out, s, t ? t->cps[1] : 0); });
 }
 
 void launch_sweep_y(const DiskView& d, const CellMaps& in, Cell* out, cudaStream_t s, const Tune* t) {
-    if (t && t->w[1] == 4) sweep_w<1, 4>(d, in.sweep_y4, out, s, t->cps[2]);
-    else sweep_w<1, 8>(d, in.sweep_y, out, s, t ? t->cps[2] : 0);
-}
-
-template <int W>
-static void advect_w(const DiskView& d, const CUtensorMap& m, Cell* out, cudaStream_t s, int cps) {
-    const int ntx = (int)cdiv(d.yres, SW_LEN), nt = ntx * (int)cdiv(d.xres, W);
-    const unsigned g = persistent_grid((const void*)k_advect<W>, Sw<W>::THREADS, Sw<W>::AD_SMEM, nt, cps);
-    k_advect<W><<<g, Sw<W>::THREADS, Sw<W>::AD_SMEM, s>>>(m, d, out, ntx, nt);
+    const int v = variant_of(t, 1, 1);
+    with_variant(v, [&](auto tag) { sweep_g<1, typename decltype(tag)::G>(d, in.sy[v], out, s, t ? t->cps[2] : 0); });
 }
 
 void launch_advect(const DiskView& d, const CellMaps& in, Cell* out, cudaStream_t s, const Tune* t) {
-    if (t && t->w[2] == 4) advect_w<4>(d, in.sweep_y4, out, s, t->cps[3]);
-    else advect_w<8>(d, in.sweep_y, out, s, t ? t->cps[3] : 0);
+    const int v = variant_of(t, 2, 1);
+    with_variant(v, [&](auto tag) { advect_g<typename decltype(tag)::G>(d, in.sy[v], out, s, t ? t->cps[3] : 0); });
 }
 
 void launch_kick2(const DiskView& d, const CellMaps& in, const VisMaps& vis, Cell* out, cudaStream_t s,
@@ -1234,19 +1291,41 @@ void launch_kick2(const DiskView& d, const CellMaps& in, const VisMaps& vis, Cel
     }
 }
 
-// CTAs per SM that fit for a pass (0 kick1, 1 sweep_x, 2 sweep_y, 3 advect, 4 kick2) with W pencils
-int pass_occupancy(const DiskView& d, int pass, int w) {
-    const bool v = d.visc && d.ndim == 2;
+// CTAs per SM that fit for a pass (0 kick1, 1 sweep_x, 2 sweep_y, 3 advect, 4 kick2) with tile variant v
+int pass_occupancy(const DiskView& d, int pass, int v) {
+    const bool vis = d.visc && d.ndim == 2;
+    int occ = 1;
     switch (pass) {
-        case 0: return kernel_occupancy(v ? (const void*)k_kick1<true> : (const void*)k_kick1<false>, ST_THREADS, K1_SMEM);
-        case 1: return w == 4 ? kernel_occupancy((const void*)k_sweep<0, 4>, Sw<4>::THREADS, Sw<4>::SMEM)
-                              : kernel_occupancy((const void*)k_sweep<0, 8>, Sw<8>::THREADS, Sw<8>::SMEM);
-        case 2: return w == 4 ? kernel_occupancy((const void*)k_sweep<1, 4>, Sw<4>::THREADS, Sw<4>::SMEM)
-                              : kernel_occupancy((const void*)k_sweep<1, 8>, Sw<8>::THREADS, Sw<8>::SMEM);
-        case 3: return w == 4 ? kernel_occupancy((const void*)k_advect<4>, Sw<4>::THREADS, Sw<4>::AD_SMEM)
-                              : kernel_occupancy((const void*)k_advect<8>, Sw<8>::THREADS, Sw<8>::AD_SMEM);
-        default: return kernel_occupancy(v ? (const void*)k_kick2<true> : (const void*)k_kick2<false>, ST_THREADS, K5_SMEM);
+        case 0: return kernel_occupancy(vis ? (const void*)k_kick1<true> : (const void*)k_kick1<false>, ST_THREADS, K1_SMEM);
+        case 4: return kernel_occupancy(vis ? (const void*)k_kick2<true> : (const void*)k_kick2<false>, ST_THREADS, K5_SMEM);
+        case 1:
+            with_variant(v, [&](auto tag) {
+                using G = typename decltype(tag)::G;
+                if constexpr (G::X_OK) occ = kernel_occupancy((const void*)k_sweep<0, G>, G::THREADS, G::SMEM);
+            });
+            return occ;
+        case 2:
+            with_variant(v, [&](auto tag) {
+                using G = typename decltype(tag)::G;
+                occ = kernel_occupancy((const void*)k_sweep<1, G>, G::THREADS, G::SMEM);
+            });
+            return occ;
+        default:
+            with_variant(v, [&](auto tag) {
+                using G = typename decltype(tag)::G;
+                occ = kernel_occupancy((const void*)k_advect<G>, G::THREADS, G::AD_SMEM);
+            });
+            return occ;
     }
+}
+
+// threads per CTA and the CTAs per SM its registers were compiled for, of a tile variant
+void sweep_variant_launch(int v, int* threads, int* minb) {
+    with_variant(v, [&](auto tag) {
+        using G = typename decltype(tag)::G;
+        *threads = G::THREADS;
+        *minb = G::MINB;
+    });
 }
 
 int kernels_per_step(const DiskView& d) {

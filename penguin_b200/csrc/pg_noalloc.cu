@@ -6,8 +6,9 @@
 // or that runs with a fixed, pre-reserved device budget), and code that must not
 // trigger an allocation mid-run at all.  pg_grid_global_dt needs per-grid private
 // scratch (an accumulator, reciprocal tables) that it cudaMallocs on first use;
-// this entry point instead reads the state, the faces and orb_rot the caller
-// already owns and keeps its scratch in the file-scope device array below.
+// this entry point instead reads the state (and the dust state, when the
+// parameters carry dust_flag), the faces and orb_rot the caller already owns and
+// keeps its scratch in the file-scope device array below.
 //
 // The scratch array is PG_NOALLOC_MAX_PARTIALS + 1 doubles (64 KiB + 8 B) per
 // GPU; every GPU that loads the library holds it until the process exits.  Each
@@ -15,7 +16,10 @@
 // size, so it needs no clearing beforehand; grids above
 // PG_NOALLOC_MAX_PARTIALS * 4096 cells are rejected.  All calls share the array:
 // calls whose kernels overlap on the GPU (different streams, or several host
-// threads) race on it.
+// threads) race on it.  The array's device address is looked up once per device
+// (first call with that device current) and kept; a cudaDeviceReset of that
+// device unloads the module, so a process that resets a device must not call
+// this entry point on it again.
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -36,9 +40,11 @@ std::mutex g_mu;
 void* g_scratch[64] = {nullptr};  // device address of pg_noalloc_scratch per device
 
 // one partial per block: max over its cells of the signal rate (timestep.cu:46-77),
-// evaluated from the faces the caller owns
-__global__ void k_cfl_partial(pg_params P, const pg_cell* __restrict__ C, const double* __restrict__ xa,
-                              const double* __restrict__ ya, const double* __restrict__ rot, double* scratch) {
+// evaluated from the faces the caller owns; with dust the dust speeds bound it
+// too (timestep.cu:64-66, 73-75)
+__global__ void k_cfl_partial(pg_params P, const pg_cell* __restrict__ C, const pg_dust* __restrict__ CD,
+                              const double* __restrict__ xa, const double* __restrict__ ya,
+                              const double* __restrict__ rot, double* scratch) {
     const int xarr = P.xres + 2 * pg::NPAD;
     const int ypad = P.ndim > 1 ? pg::NPAD : 0;
     const long long n = (long long)P.xres * P.yres;
@@ -49,14 +55,18 @@ __global__ void k_cfl_partial(pg_params P, const pg_cell* __restrict__ C, const 
         if (m >= n) break;
         const int i = pg::NPAD + (int)(m % P.xres);
         const int j = ypad + (int)(m / P.xres);
-        const pg_cell c = C[(size_t)i + (size_t)xarr * j];
+        const size_t ind = (size_t)i + (size_t)xarr * j;
+        const pg_cell c = C[ind];
         const double rad_cyl = (P.geomy == 3) ? 0.5 * (xa[i + 1] + xa[i]) : 1.0;
         const double cs = sqrt(P.gam * c.p / c.r);
         double spd = fabs(c.u) + cs;
+        if (CD) spd = fmax(fabs(CD[ind].u), spd);
         double wid = fabs(xa[i + 1] - xa[i]);
         tmp = fmax(spd / wid, tmp);
         if (P.ndim > 1) {
-            spd = fabs(c.v - rad_cyl * P.frame_omega - (rot ? rot[i] : 0.0)) + cs;
+            const double rot_i = rot ? rot[i] : 0.0;
+            spd = fabs(c.v - rad_cyl * P.frame_omega - rot_i) + cs;
+            if (CD) spd = fmax(fabs(CD[ind].v - rad_cyl * P.frame_omega - rot_i), spd);
             wid = fabs(ya[j + 1] - ya[j]) * rad_cyl;
             tmp = fmax(spd / wid, tmp);
         }
@@ -94,10 +104,16 @@ pg_status fail(pg_status s, const char* msg) {
 
 }  // namespace
 
-extern "C" pg_status pg_global_dt_noalloc(const pg_params* P, const pg_cell* C, const double* xa, const double* ya,
-                                          const double* orb_rot, double dt_prev, double* dt_out, void* stream) {
-    if (!P || !C || !xa || !ya || !dt_out) return fail(PG_ERR_ARG, "pg_global_dt_noalloc: null argument");
+extern "C" pg_status pg_global_dt_noalloc(const pg_params* P, const pg_cell* C, const pg_dust* CD, const double* xa,
+                                          const double* ya, const double* orb_rot, double dt_prev, double* dt_out,
+                                          void* stream) {
+    if (!P || !C || !xa || !dt_out) return fail(PG_ERR_ARG, "pg_global_dt_noalloc: null argument");
     if (P->ndim != 1 && P->ndim != 2) return fail(PG_ERR_CONFIG, "pg_global_dt_noalloc: ndim must be 1 or 2");
+    if (P->ndim == 1 && P->yres != 1)
+        return fail(PG_ERR_CONFIG, "pg_global_dt_noalloc: a 1D grid has yres 1");
+    if (P->ndim == 2 && !ya) return fail(PG_ERR_ARG, "pg_global_dt_noalloc: a 2D grid needs its faces ya");
+    if (P->dust_flag && !CD) return fail(PG_ERR_ARG, "pg_global_dt_noalloc: dust_flag needs the dust state CD");
+    if (!P->dust_flag) CD = nullptr;
     const long long n = (long long)P->xres * P->yres;
     const long long nparts = (n + PG_NOALLOC_CELLS_PER_BLOCK - 1) / PG_NOALLOC_CELLS_PER_BLOCK;
     if (n <= 0) return fail(PG_ERR_CONFIG, "pg_global_dt_noalloc: empty grid");
@@ -128,7 +144,7 @@ extern "C" pg_status pg_global_dt_noalloc(const pg_params* P, const pg_cell* C, 
         scratch = g_scratch[dev];
     }
     cudaStream_t s = (cudaStream_t)stream;
-    k_cfl_partial<<<(unsigned)nparts, PG_NOALLOC_THREADS, 0, s>>>(*P, C, xa, ya, orb_rot,
+    k_cfl_partial<<<(unsigned)nparts, PG_NOALLOC_THREADS, 0, s>>>(*P, C, CD, xa, ya, orb_rot,
                                                                    static_cast<double*>(scratch));
     k_cfl_final<<<1, PG_NOALLOC_THREADS, 0, s>>>(P->cfl, (int)nparts, static_cast<double*>(scratch));
     cudaError_t le = cudaGetLastError();

@@ -151,15 +151,17 @@ class Disk:
         check(lib().pg_disk_get_average(self._h, _dp(out["r"]), _dp(out["p"]), _dp(out["u"]), _dp(out["v"])))
         return out
 
-    TUNING = ("w_sweep_x", "w_sweep_y", "w_advect", "cps_kick1", "cps_sweep_x", "cps_sweep_y", "cps_advect",
+    TUNING = ("v_sweep_x", "v_sweep_y", "v_advect", "cps_kick1", "cps_sweep_x", "cps_sweep_y", "cps_advect",
               "cps_kick2")
 
     def autotune(self, reps: int = 10) -> dict:
         """Times every launch configuration of each pass on the current state and
-        keeps the fastest (results stay bit for bit the same)."""
+        keeps the fastest (results stay bit for bit the same).  Returns the raw
+        choice (TUNING keys) and, under "passes", every pass's knobs."""
         out = (ctypes.c_int * 8)()
         check(lib().pg_disk_autotune(self._h, reps, out))
-        return {k: int(out[n]) for n, k in enumerate(self.TUNING)}
+        choice = {k: int(out[n]) for n, k in enumerate(self.TUNING)}
+        return dict(choice, passes=describe_tuning(choice))
 
     def set_tuning(self, choice: dict) -> None:
         arr = (ctypes.c_int * 8)(*[int(choice[k]) for k in self.TUNING])
@@ -187,6 +189,27 @@ class Disk:
             self.close()
         except Exception:
             pass
+
+
+def sweep_variant(v: int) -> dict:
+    """Knobs of tile variant v of the sweeps and the residual advection."""
+    out = (ctypes.c_int * 6)()
+    check(lib().pg_sweep_variant(v, out))
+    return {"pencils_per_tile": out[0], "pencil_length": out[1], "cells_per_thread": out[2],
+            "tma_stages": out[3], "threads": out[4], "ctas_per_sm_compiled": out[5]}
+
+
+def describe_tuning(choice: dict) -> dict:
+    """Every pass's launch knobs from an autotuner choice (Disk.TUNING keys)."""
+    out = {}
+    for p in ("kick1", "sweep_x", "sweep_y", "advect", "kick2"):
+        k = {"ctas_per_sm": choice["cps_" + p] or "all that fit"}
+        if p in ("sweep_x", "sweep_y", "advect"):
+            k.update(sweep_variant(choice["v_" + p]))
+        else:  # the stencil passes: 32 x 8 cells per tile, one cell per thread, two TMA stages
+            k.update({"tile": "32x8", "cells_per_thread": 1, "tma_stages": 2})
+        out[p] = k
+    return out
 
 
 def make_grid(params: Params):

@@ -38,5 +38,7 @@ def build(objdir: str, header: str, out: str, reference_include: str) -> str:
 
 
 if __name__ == "__main__":
-    ref_inc = os.path.join(os.environ.get("PENGUIN_REFERENCE", "/root/reference"), "include")
-    print(build(sys.argv[1], sys.argv[2], sys.argv[3], ref_inc))
+    sys.path.insert(0, ROOT)
+    from oracle.ref_build import REFERENCE_ROOT  # where the recipe reads the reference's sources
+
+    print(build(sys.argv[1], sys.argv[2], sys.argv[3], os.path.join(REFERENCE_ROOT, "include")))

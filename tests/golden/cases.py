@@ -33,19 +33,25 @@ def cases() -> list[dict]:
     # tol: relative-L1 bound (density, pressure and momentum) between the oracle and
     # the reference's own output, set from the measured differences with margin.
     # Cases with the planet amplify rounding-level differences near it step by step.
-    # cuda_tol: the same bound for the CUDA path against the reference's output.  It
-    # is tighter than tol on the disks (same CUDA math library as the reference) and
-    # looser on the Sod tube, where the precomputed slope weights round differently
-    # from the reference's per-call moment algebra and the limiter / monotonicity
-    # branches at the discontinuities amplify that (measured 3.8e-10 after 10 steps).
+    # cuda_tol: the same bound for the CUDA path against the reference's output,
+    # 1e-12 or below wherever the reference itself allows it.  floors.json (beside
+    # this file, made by make_golden.py's floor phase) holds how far the reference
+    # moves from itself when every input density moves by one ulp; the three bounds
+    # above 1e-12 sit at that floor: the Sod tube after 10 steps (CUDA 1.65e-12,
+    # floor 2.55e-12) and to t = 0.2 (8.7e-13, floor 1.2e-12), where the limiter
+    # and monotonicity branches at the discontinuities amplify rounding, and the
+    # total-energy adiabatic disk (5.9e-11, floor 4.1e-11; see adiabatic_cases).
+    # The CUDA kernels apply the 4th-order slopes as per-index weights built from
+    # the reference's own rounded grid moments (penguin_b200/csrc/pg_engine.cu), so
+    # what remains is the rounding of the reference's per-call arithmetic.
     sod = P.sod_tube(1024)
     out = [
         dict(name="sod_n1", params=sod, init="sod", t0=0.0, max_step=1, end_time=0.2, tol=1e-14, cuda_tol=1e-14),
-        dict(name="sod_n10", params=sod, init="sod", t0=0.0, max_step=10, end_time=0.2, tol=1e-11, cuda_tol=1e-9),
+        dict(name="sod_n10", params=sod, init="sod", t0=0.0, max_step=10, end_time=0.2, tol=1e-11, cuda_tol=3e-12),
         dict(name="sod_t02", params=sod, init="sod", t0=0.0, max_step=1000000000, end_time=0.2, tol=5e-12,
-             cuda_tol=5e-10),
+             cuda_tol=1e-12),
     ]
-    for n, tol, ctol in ((1, 1e-12, 1e-13), (10, 1e-10, 2e-12), (50, 1e-9, 1e-10)):
+    for n, tol, ctol in ((1, 1e-12, 1e-14), (10, 1e-10, 2e-13), (50, 1e-9, 1e-12)):
         out.append(dict(name=f"disk64_n{n}", params=_disk64(), init="disk", t0=T0_DISK, max_step=n, end_time=1.0e30,
                         tol=tol, cuda_tol=ctol))
     variants = {
@@ -56,7 +62,7 @@ def cases() -> list[dict]:
     }
     for k, kw in variants.items():
         out.append(dict(name=f"disk32_{k}_n10", params=_disk32(**kw), init="disk", t0=T0_DISK, max_step=10,
-                        end_time=1.0e30, tol=2e-12 if k == "kill_planet" else 1e-14, cuda_tol=1e-13))
+                        end_time=1.0e30, tol=2e-12 if k == "kill_planet" else 1e-14, cuda_tol=3e-14))
     return out + adiabatic_cases() + two_body_cases() + preset_cases()
 
 
@@ -81,7 +87,7 @@ def preset_cases() -> list[dict]:
     differs only in resolution), 64x192, from the seeded disk after 5 orbits."""
     p = preset_default()
     return [dict(name="default64_n10", params=p, init="disk", t0=T0_DISK, max_step=10, end_time=1.0e30,
-                 tol=1e-13, cuda_tol=1e-12)]
+                 tol=1e-13, cuda_tol=1e-13)]
 
 
 def two_body_cases() -> list[dict]:
@@ -99,11 +105,11 @@ def two_body_cases() -> list[dict]:
     base = _disk64().replace(twobd_flag=1)
     return [
         dict(name="tb64_n1", params=base, init="disk", t0=T0_DISK, max_step=1, end_time=1.0e30,
-             tol=5e-12, cuda_tol=1e-13),
+             tol=5e-12, cuda_tol=1e-14),
         dict(name="tb64_n10", params=base, init="disk", t0=T0_DISK, max_step=10, end_time=1.0e30,
-             tol=1e-9, cuda_tol=1e-12),
+             tol=1e-9, cuda_tol=3e-13),
         dict(name="tb64_ecc_n10", params=base.replace(planet_ecc=0.05), init="disk", t0=T0_DISK, max_step=10,
-             end_time=1.0e30, tol=1e-9, cuda_tol=1e-12),
+             end_time=1.0e30, tol=1e-9, cuda_tol=3e-13),
     ]
 
 
@@ -133,12 +139,12 @@ def adiabatic_cases() -> list[dict]:
     c2 = dict(internal_e_flag=1, cool_flag=2, beta_cool=0.05)
     et = dict(internal_e_flag=0)
     specs = [  # name, params, init, steps, tol, cuda_tol
-        ("adi64_n10", e1, "disk", 10, 1e-10, 1e-12),
-        ("adi64_etot_n1", et, "disk", 1, 1e-10, 1e-11),
-        ("adi64_etot_n10", et, "disk", 10, 1e-7, 1e-8),
-        ("adi64_cool1_nokill_n1", dict(c1, kill_flag=0), "disk_hot", 1, 1e-14, 1e-13),
-        ("adi64_cool1_n10", c1, "disk_hot", 10, 2e-9, 1e-12),
-        ("adi64_cool2_n10", c2, "disk_hot", 10, 2e-10, 1e-12),
+        ("adi64_n10", e1, "disk", 10, 1e-10, 2e-13),
+        ("adi64_etot_n1", et, "disk", 1, 1e-10, 3e-13),
+        ("adi64_etot_n10", et, "disk", 10, 1e-7, 1.2e-10),
+        ("adi64_cool1_nokill_n1", dict(c1, kill_flag=0), "disk_hot", 1, 1e-14, 1e-14),
+        ("adi64_cool1_n10", c1, "disk_hot", 10, 2e-9, 3e-13),
+        ("adi64_cool2_n10", c2, "disk_hot", 10, 2e-10, 3e-13),
     ]
     return [dict(name=n, params=base.replace(**kw), init=init, t0=T0_DISK, max_step=m, end_time=1.0e30,
                  tol=tol, cuda_tol=ctol) for n, kw, init, m, tol, ctol in specs]
@@ -157,13 +163,41 @@ def dust_cases() -> list[dict]:
     for st, tag in ((0.01, "st001"), (0.1, "st01")):
         p = P.reference_disk(64, 192, q=3.0e-4, alpha=1.0e-4).replace(dust_flag=1, Stokes=st, D_G_ratio=0.01)
         out.append(dict(name=f"dust64_{tag}_n10", params=p, init="disk", t0=T0_DISK, max_step=10, end_time=1.0e30,
-                        tol=1e-10, cuda_tol=1e-10, dust=True))
+                        tol=1e-10, cuda_tol=5e-13, dust=True))
     p = P.reference_disk(64, 192, q=3.0e-4, alpha=1.0e-4).replace(dust_flag=1, Stokes=0.1, D_G_ratio=0.01)
     out.append(dict(name="dust64_st01_n1", params=p, init="disk", t0=T0_DISK, max_step=1, end_time=1.0e30,
-                    tol=1e-12, cuda_tol=1e-12, dust=True))
+                    tol=1e-12, cuda_tol=1e-14, dust=True))
     out.append(dict(name="dust64_st01_noplanet_n10", params=p.replace(planet_mass=0.0), init="disk", t0=T0_DISK,
-                    max_step=10, end_time=1.0e30, tol=1e-10, cuda_tol=1e-10, dust=True))
+                    max_step=10, end_time=1.0e30, tol=1e-10, cuda_tol=5e-13, dust=True))
     return out
+
+
+def ave_cases() -> list[dict]:
+    """ave_flag: the 64x192 disk case of ``cases`` built with the time average on
+    (interval 10, longer than the 10 steps' 0.44, so no dump clips a step): at
+    max_step the reference writes the state and the trapezoid average of the
+    states over the steps divided by the interval (main.cu:343-351, 411-422;
+    src/output/output.cu:250-330) as binary_<label>_ave_00001."""
+    return [dict(name="disk64_ave_n10", params=_disk64(), init="disk", t0=T0_DISK, max_step=10, end_time=1.0e30,
+                 tol=1e-10, cuda_tol=2e-12, ave_interval=10.0)]
+
+
+def size_cases() -> list[dict]:
+    """The workloads at their own sizes, built from the reference for a direct
+    comparison on the GPU (the outputs, 100 MB and more, are made at test time
+    and not stored): the 1024x3072 planet-disk from t = 0 (the workload's start,
+    planet mass ramping from zero) and from 5 orbits (planet at half mass), and
+    the 256x768 gradient disk (no wave damping).  The 1024x3072 disk takes the
+    single damping width the reference has (2.4 H on both sides)."""
+    d1024 = P.reference_disk(1024, 3072)
+    return [
+        dict(name="size_disk1024_n5", params=d1024, init="disk", seed=1234, t0=0.0, max_step=5, end_time=1.0e30,
+             cuda_tol=1e-12, tools=("slopes",)),
+        dict(name="size_disk1024_orb5_n5", params=d1024, init="disk", seed=1234, t0=T0_DISK, max_step=5,
+             end_time=1.0e30, cuda_tol=1e-12),
+        dict(name="size_adj256_n20", params=P.adjoint_disk(), init="disk", seed=1234, t0=0.0, max_step=20,
+             end_time=1.0e30, cuda_tol=1e-12),
+    ]
 
 
 def timing_cases() -> list[dict]:
@@ -181,7 +215,7 @@ def initial_state(case: dict) -> dict:
     p = case["params"]
     if case["init"] == "sod":
         return I.sod_state(p)
-    st = I.disk_state(p, seed=SEED)
+    st = I.disk_state(p, seed=case.get("seed", SEED))
     if case["init"] == "disk_hot":
         st["p"] = 1.2 * st["p"]
     return st

@@ -1,15 +1,23 @@
 """Generate the golden fixtures by running the unmodified reference.
 
-Three phases:
+Four phases:
   build    (here, where the reference sources are):  compile one reference binary
            per case into oracle/_ref/<case>/ with oracle/ref_build.py;
   run      (on a B200):  for each case write the restart file, run
            ``penguin init.bin 0`` in the case folder and save the reference's
            output snapshot plus the initial state as <out>/<case>.npz;
-  collect  (here):  copy the .npz files of the golden cases into tests/golden/.
+  floor    (on a B200):  the reference's own sensitivity to rounding: each case
+           is run again from its restart file with every interior density moved
+           by one ulp (up or down, seeded), and the relative L1 distance of that
+           output from the unperturbed one (density, pressure, momentum; dust
+           density and momentum) goes to <out>/floors.json.  The unperturbed
+           run is repeated too and must equal the committed fixture bit for bit;
+  collect  (here):  copy the .npz files of the golden cases (and floors.json)
+           into tests/golden/.
 
     python tests/golden/make_golden.py build
     python tests/golden/make_golden.py run --out <outdir> [--timing]
+    python tests/golden/make_golden.py floor --out <outdir> [--only <regex>]
     python tests/golden/make_golden.py collect --src <outdir>
 """
 from __future__ import annotations
@@ -39,18 +47,18 @@ from penguin_b200.params import make_grid_np  # noqa: E402
 
 
 def _all(timing: bool):
-    return C.cases() + C.dust_cases() + (C.timing_cases() if timing else [])
+    return C.cases() + C.dust_cases() + C.ave_cases() + (C.timing_cases() if timing else [])
 
 
 def build(timing: bool, jobs: int) -> None:
     for c in _all(timing):
-        hdr = ref_build.parameters_h(dataclasses.asdict(c["params"]), c["max_step"], c["end_time"])
+        hdr = ref_build.case_header(c)
         t = time.time()
-        exe = ref_build.build_case(c["name"], hdr, jobs=jobs)
+        exe = ref_build.build_case(c["name"], hdr, jobs=jobs, tools=tuple(c.get("tools", ())))
         print(f"{c['name']}: {exe} ({time.time() - t:.0f} s)", flush=True)
 
 
-def _run_dust(c: dict, d: str, out: str, st: dict) -> int:
+def _run_dust(c: dict, d: str, out: str, st: dict, tag: str = "") -> int:
     """Dust cases: the reference's dust reconstruction reads a flattening coefficient
     from shared memory it never writes (src/solver/recon/PPM.cu:68-77 reached from
     src/solver/dust/dust.cu:105-147), so its snapshots depend on what earlier kernels
@@ -62,9 +70,9 @@ def _run_dust(c: dict, d: str, out: str, st: dict) -> int:
     r = subprocess.run(["./stages", "init.bin", str(c["max_step"]), "stages.bin", "scrub"], cwd=d,
                        capture_output=True, text=True, timeout=900)
     wall = time.time() - t
-    with open(os.path.join(out, c["name"] + ".log"), "w") as f:
+    with open(os.path.join(out, c["name"] + tag + ".log"), "w") as f:
         f.write(r.stdout + "\n--- stderr ---\n" + r.stderr)
-    print(f"{c['name']}: rc={r.returncode} wall={wall:.2f}s (stage driver, scrub)", flush=True)
+    print(f"{c['name']}{tag}: rc={r.returncode} wall={wall:.2f}s (stage driver, scrub)", flush=True)
     if r.returncode != 0 or "CUDA error" in r.stdout:
         return 1
     xarr, yarr = p.xres + 6, p.yres + 6
@@ -80,7 +88,7 @@ def _run_dust(c: dict, d: str, out: str, st: dict) -> int:
     res = {k: np.ascontiguousarray(cells[..., m]) for m, k in ((0, "r"), (1, "p"), (2, "u"), (3, "v"))}
     res.update({"dust_" + k: np.ascontiguousarray(dust[..., m]) for m, k in enumerate(("r", "u", "v", "w"))})
     np.savez_compressed(
-        os.path.join(out, c["name"] + ".npz"),
+        os.path.join(out, c["name"] + tag + ".npz"),
         t0=c["t0"], t=t_stage + dt_stage, max_step=c["max_step"], end_time=c["end_time"],
         params=json.dumps(dataclasses.asdict(p)), source="ref_stages scrub",
         **{"init_" + k: np.asarray(st[k], dtype=np.float64) for k in keys},
@@ -89,7 +97,14 @@ def _run_dust(c: dict, d: str, out: str, st: dict) -> int:
     return 0
 
 
-def run(out: str, timing: bool, only: str | None) -> int:
+def perturb_ulp(st: dict, seed: int = 99) -> dict:
+    """Every interior density one ulp up or down (the sign drawn per cell)."""
+    r = np.asarray(st["r"], dtype=np.float64)
+    up = np.random.default_rng(seed).integers(0, 2, size=r.shape).astype(bool)
+    return dict(st, r=np.where(up, np.nextafter(r, np.inf), np.nextafter(r, -np.inf)))
+
+
+def run(out: str, timing: bool, only: str | None, perturb: bool = False, tag: str = "") -> int:
     os.makedirs(out, exist_ok=True)
     bad = 0
     for c in _all(timing):
@@ -105,24 +120,27 @@ def run(out: str, timing: bool, only: str | None) -> int:
         for f in glob.glob(os.path.join(d, "binary_*")):
             os.remove(f)
         st = C.initial_state(c)
+        st_run = perturb_ulp(st) if perturb else st
         xa, _ = make_grid_np(p.xmin, p.xmax, p.xres, 3, p.geomx, p.gridx)
         ya, _ = make_grid_np(p.ymin, p.ymax, p.yres, 3 if p.ndim > 1 else 0, p.geomy, p.gridy)
         init = os.path.join(d, "init.bin")
         snapshot.write_snapshot(init, c["t0"], xa[3:3 + p.xres + 1], ya[3:3 + p.yres + 1] if p.ndim > 1 else None,
-                                st, p.ndim)
+                                st_run, p.ndim)
         if c.get("dust"):
-            bad += _run_dust(c, d, out, st)
+            bad += _run_dust(c, d, out, st, tag)
             continue
         t = time.time()
         r = subprocess.run(["./penguin", "init.bin", "0"], cwd=d, capture_output=True, text=True, timeout=900)
         wall = time.time() - t
-        outs = sorted(glob.glob(os.path.join(d, "binary_*_00001")))
+        outs = sorted(f for f in glob.glob(os.path.join(d, "binary_*_00001")) if "_ave_" not in os.path.basename(f))
+        aves = sorted(glob.glob(os.path.join(d, "binary_*_ave_00001")))
         sps = re.findall(r"([0-9.eE+-]+) seconds per step", r.stdout)
-        print(f"{c['name']}: rc={r.returncode} wall={wall:.2f}s s/step={sps[-1] if sps else '?'} out={outs}",
+        print(f"{c['name']}{tag}: rc={r.returncode} wall={wall:.2f}s s/step={sps[-1] if sps else '?'} out={outs}",
               flush=True)
-        with open(os.path.join(out, c["name"] + ".log"), "w") as f:
+        with open(os.path.join(out, c["name"] + tag + ".log"), "w") as f:
             f.write(r.stdout + "\n--- stderr ---\n" + r.stderr)
         if r.returncode != 0 or not outs:
+            print(f"{c['name']}: files {sorted(os.listdir(d))}\n{r.stdout[-1500:]}", flush=True)
             bad += 1
             continue
         if c["name"].startswith("ref_"):
@@ -135,29 +153,90 @@ def run(out: str, timing: bool, only: str | None) -> int:
         res = snapshot.read_snapshot(outs[0], p.xres, p.yres, p.ndim, dust=dust)
         keys = ["r", "p", "u"] + (["v"] if p.ndim > 1 else [])
         dkeys = ["dust_r", "dust_u", "dust_v", "dust_w"] if dust else []
+        extra = {}
+        if c.get("ave_interval"):  # the time average the reference wrote beside the state
+            if not aves:
+                bad += 1
+                continue
+            ave = snapshot.read_snapshot(aves[0], p.xres, p.yres, p.ndim)
+            extra = {"ave_" + k: ave[k] for k in keys}
+            extra["ave_interval"] = c["ave_interval"]
         np.savez_compressed(
-            os.path.join(out, c["name"] + ".npz"),
+            os.path.join(out, c["name"] + tag + ".npz"),
             t0=c["t0"], t=res["t"], max_step=c["max_step"], end_time=c["end_time"],
             params=json.dumps(dataclasses.asdict(p)),
             **{"init_" + k: np.asarray(st[k], dtype=np.float64) for k in keys},
             **{"out_" + k: res[k] for k in keys + dkeys},
+            **extra,
         )
     return bad
 
 
-def collect(src: str) -> None:
+def _rel_l1(a, b):
+    den = float(np.abs(b).sum())
+    return float(np.abs(a - b).sum()) / den if den > 0 else float(np.abs(a - b).sum())
+
+
+def _distances(a: dict, b: dict, ndim: int, dust: bool) -> dict:
+    """Relative L1 of density, pressure and the momentum vector of a against b
+    (and of the dust density and momentum)."""
+    def mom(z, pre=""):
+        r = z[f"out_{pre}r"]
+        return r * z[f"out_{pre}u"], (r * z[f"out_{pre}v"] if ndim > 1 else 0 * r)
+
+    out = {"r": _rel_l1(a["out_r"], b["out_r"]), "p": _rel_l1(a["out_p"], b["out_p"])}
+    (ax, ay), (bx, by) = mom(a), mom(b)
+    out["momentum"] = float((np.abs(ax - bx) + np.abs(ay - by)).sum() / (np.abs(bx) + np.abs(by)).sum())
+    if dust:
+        out["dust_r"] = _rel_l1(a["out_dust_r"], b["out_dust_r"])
+        (ax, ay), (bx, by) = mom(a, "dust_"), mom(b, "dust_")
+        out["dust_momentum"] = float((np.abs(ax - bx) + np.abs(ay - by)).sum() / (np.abs(bx) + np.abs(by)).sum())
+    return out
+
+
+def floor(out: str, only: str | None) -> int:
+    """The reference against itself: unperturbed (must equal the committed
+    fixture) and with one-ulp density perturbations (the sensitivity floor)."""
+    bad = run(out, False, only, perturb=False, tag=".rerun")
+    bad += run(out, False, only, perturb=True, tag=".ulp")
+    res = {}
     for c in C.cases() + C.dust_cases():
+        if only and not re.search(only, c["name"]):
+            continue
+        fx = os.path.join(HERE, c["name"] + ".npz")
+        fr, fu = (os.path.join(out, c["name"] + t + ".npz") for t in (".rerun", ".ulp"))
+        if not all(os.path.exists(f) for f in (fx, fr, fu)):
+            print(f"{c['name']}: missing output", flush=True)
+            bad += 1
+            continue
+        zx, zr, zu = np.load(fx), np.load(fr), np.load(fu)
+        p, dust = c["params"], bool(c.get("dust"))
+        rerun = _distances(zr, zx, p.ndim, dust)
+        res[c["name"]] = {"steps": c["max_step"], "floor": _distances(zu, zr, p.ndim, dust),
+                          "rerun_vs_fixture": rerun, "deterministic": all(v == 0.0 for v in rerun.values())}
+        print(c["name"], json.dumps(res[c["name"]]), flush=True)
+    with open(os.path.join(out, "floors.json"), "w") as f:
+        json.dump(res, f, indent=1, sort_keys=True)
+    return bad
+
+
+def collect(src: str) -> None:
+    for c in C.cases() + C.dust_cases() + C.ave_cases():
         f = os.path.join(src, c["name"] + ".npz")
         if os.path.exists(f):
             shutil.copy(f, os.path.join(HERE, c["name"] + ".npz"))
             print("collected", c["name"])
         else:
             print("missing", f)
+    f = os.path.join(src, "floors.json")
+    if os.path.exists(f):
+        shutil.copy(f, os.path.join(HERE, "floors.json"))
+        print("collected floors.json")
 
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("phase", choices=["build", "run", "collect"])
+    ap.add_argument("phase", choices=["build", "run", "floor", "collect"])
     ap.add_argument("--out", default="golden_out")
     ap.add_argument("--src", default="golden_out")
     ap.add_argument("--timing", action="store_true")
@@ -168,6 +247,8 @@ def main():
         build(a.timing, a.jobs)
     elif a.phase == "run":
         sys.exit(1 if run(a.out, a.timing, a.only) else 0)
+    elif a.phase == "floor":
+        sys.exit(1 if floor(a.out, a.only) else 0)
     else:
         collect(a.src)
 

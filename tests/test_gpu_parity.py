@@ -11,7 +11,7 @@ from oracle.oracle import Oracle
 from penguin_b200 import initial as I
 from penguin_b200 import params as P
 from penguin_b200._lib import PG_ERR_NAN, PGError
-from penguin_b200.disk import Disk
+from penguin_b200.disk import Disk, sweep_variant
 
 pytestmark = pytest.mark.gpu
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
@@ -213,8 +213,9 @@ def test_torque_matches_oracle():
 
 def test_autotuned_launches_give_identical_results():
     """The autotuner changes tiles and grid sizes, not the arithmetic of a cell:
-    the tuned step equals the default one bit for bit, and every configuration
-    it may choose (4 pencils per tile everywhere, one CTA per SM) does too."""
+    the tuned step equals the default one bit for bit, and so does every tile
+    variant it may choose (pencils per tile, pencil length, cells per thread,
+    TMA stages), each with one CTA per SM."""
     case = [c for c in C.cases() if c["name"] == "disk64_n10"][0]
     p, st = case["params"], C.initial_state(case)
     ref = Disk(p)
@@ -225,20 +226,24 @@ def test_autotuned_launches_give_identical_results():
     tuned = Disk(p)
     tuned.set_state(case["t0"], st)
     choice = tuned.autotune(reps=3)
-    assert set(choice) == set(Disk.TUNING)
-    assert all(choice[k] in (4, 8) for k in Disk.TUNING[:3])
+    assert set(choice) == set(Disk.TUNING) | {"passes"}
+    assert set(choice["passes"]) == {"kick1", "sweep_x", "sweep_y", "advect", "kick2"}
     tuned.run(10)
     tuned.sync()
     b = tuned.get_state()
-    forced = Disk(p)
-    forced.set_state(case["t0"], st)
-    forced.set_tuning(dict(zip(Disk.TUNING, (4, 4, 4, 1, 1, 1, 1, 1))))
-    forced.run(10)
-    forced.sync()
-    c = forced.get_state()
     for k in _keys(p):
         assert np.array_equal(a[k], b[k]), k
-        assert np.array_equal(a[k], c[k]), k
+    for v in range(8):
+        vx = v if sweep_variant(v)["pencil_length"] + 6 <= 51 else 0  # radial boxes of at most 256 doubles
+        forced = Disk(p)
+        forced.set_state(case["t0"], st)
+        forced.set_tuning(dict(zip(Disk.TUNING, (vx, v, v, 1, 1, 1, 1, 1))))
+        forced.run(10)
+        forced.sync()
+        c = forced.get_state()
+        forced.close()
+        for k in _keys(p):
+            assert np.array_equal(a[k], c[k]), (v, k)
 
 
 def test_state_exchange_round_trip_allocates_nothing():
