@@ -431,7 +431,7 @@ def measure_adjoint(steps, local, stream, timing_steps=None):
                        * (1.0 + 0.01 * np.sin(y[:, None] + 3.0 * np.log(x[None, :]))), device=s0.device)
     outs = m.forward(s0s, replay=True)
     gsm = (2.0 * (outs.mean(0) - target) / p.yres)[None, :].expand(p.yres, p.xres).contiguous()
-    gs_s, _ = m.backward(gsm)
+    gs_s, gth_s = m.backward(gsm)
     ds = d / s0 * s0s
     ad_s = float((gs_s * ds).sum())
     fd_s = {}
@@ -456,22 +456,34 @@ def measure_adjoint(steps, local, stream, timing_steps=None):
     # amount), so a central difference whose two points fall on different levels
     # is no derivative; the two-level least-squares slope is, and the plain
     # central difference at 1e-6 is reported beside it
-    scan = []
-    for k in range(3):
-        ss = [j * 1.0e-6 for j in range(-4, 5)]
-        Ls = []
-        for s_ in ss:
-            th = list(theta)
-            th[k] = theta[k] * (1.0 + s_)
-            m.set_theta(*th)
-            Ls.append(loss(m.forward(s0, replay=True)))
-        m.set_theta(*theta)
-        fit = two_level_slope(np.array(ss) * theta[k], np.array(Ls))
-        central = (Ls[5] - Ls[3]) / (2.0e-6 * theta[k])
-        scan.append({"two_level_slope": fit["slope"], "levels": fit["levels"], "jump": fit["jump"],
-                     "central_1e-6": central,
-                     "rel_err_two_level": abs(fit["slope"] - gth[k]) / abs(gth[k]),
-                     "rel_err_central_1e-6": abs(central - gth[k]) / abs(gth[k])})
+    def theta_scan(state, model, target_loss):
+        res = []
+        for k in range(3):
+            ss = [j * 1.0e-6 for j in range(-4, 5)]
+            Ls = []
+            for s_ in ss:
+                th = list(theta)
+                th[k] = theta[k] * (1.0 + s_)
+                model.set_theta(*th)
+                Ls.append(target_loss(model.forward(state, replay=True)))
+            model.set_theta(*theta)
+            res.append((np.array(ss) * theta[k], np.array(Ls)))
+        return res
+
+    def scan_summary(res, grad):
+        out = []
+        for k, (xs, Ls) in enumerate(res):
+            fit = two_level_slope(xs, Ls)
+            central = (Ls[5] - Ls[3]) / (xs[5] - xs[3])
+            out.append({"two_level_slope": fit["slope"], "levels": fit["levels"], "jump": fit["jump"],
+                        "central_1e-6": central,
+                        "rel_err_two_level": abs(fit["slope"] - grad[k]) / abs(grad[k]),
+                        "rel_err_central_1e-6": abs(central - grad[k]) / abs(grad[k])})
+        return out
+
+    scan = scan_summary(theta_scan(s0, m, loss), gth)
+    # the same on the smooth state, against its adjoint of the same loss (gth_s)
+    scan_s = scan_summary(theta_scan(s0s, m, loss), gth_s)
     out_line = {
         "workload": "256x768 gradient disk, FP64 forward + adjoint, checkpoint every 64 steps",
         "steps": steps, "timing_steps": tsteps, "forward_ms_per_step": ms_f / tsteps,
@@ -486,7 +498,11 @@ def measure_adjoint(steps, local, stream, timing_steps=None):
                              "rel_err": {k: abs(ad_s - v) / abs(v) for k, v in fd_s.items()}},
         "fd_theta": {"names": ["q", "alpha", "h"], "adjoint": [float(v) for v in gth], "central_rel_step_1e-4": fdt,
                      "rel_err": [abs(a - b) / abs(b) for a, b in zip(gth, fdt)]},
-        "fd_theta_scan": {"names": ["q", "alpha", "h"], "points": "9 at relative spacing 1e-6", "per_parameter": scan},
+        "fd_theta_scan": {"names": ["q", "alpha", "h"], "points": "9 at relative spacing 1e-6",
+                          "state": "the workload's noisy disk", "per_parameter": scan},
+        "fd_theta_scan_smooth": {"names": ["q", "alpha", "h"], "points": "9 at relative spacing 1e-6",
+                                 "state": "no noise, 1 % spiral", "adjoint": [float(v) for v in gth_s],
+                                 "per_parameter": scan_s},
     }
     m.close()
     return out_line
@@ -530,6 +546,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-forms", action="store_true", help="skip the FP32-mixed, ensemble and dust measurements")
     ap.add_argument("--no-tune", action="store_true", help="default launch configuration instead of the autotuner's")
+    ap.add_argument("--tuning", default=None,
+                    help="a fixed launch configuration instead of the autotuner's: comma list of "
+                         "key=value over Disk.TUNING (v_sweep_x, ..., cps_kick2)")
     ap.add_argument("--forms", default="fp32,ensemble,dust,adjoint",
                     help="comma list of the extra measurements after the FP64 headline "
                          "(fp32, ensemble, dust, adjoint)")
@@ -559,7 +578,14 @@ def main():
     disk.run(W)
     disk.sync()
     disk.check()
-    tuning = disk.autotune(reps=5) if not args.no_tune else None
+    if args.tuning:
+        from penguin_b200.disk import describe_tuning
+
+        choice = {k: int(v) for k, v in (kv.split("=") for kv in args.tuning.split(","))}
+        disk.set_tuning(choice)
+        tuning = dict(choice, passes=describe_tuning(choice), source="--tuning")
+    else:
+        tuning = disk.autotune(reps=5) if not args.no_tune else None
 
     def barrier():
         job.barrier(torch.cuda.synchronize)
@@ -591,6 +617,27 @@ def main():
             f = line.split()
             if len(f) >= 2 and f[0] == stage and not line.startswith("#"):
                 traffic = float(f[1])
+
+    # the same kernel against its FP64-issue roofline: FP64 arithmetic
+    # instructions per cell (ncu, profiles/fp64_per_cell.txt) x cells / its time,
+    # against 64 FP64 lanes per SM x SMs x the max SM clock
+    roofline_fp64 = None
+    ffile = os.path.join(ROOT, "profiles", "fp64_per_cell.txt")
+    if os.path.exists(ffile):
+        per_cell = {}
+        for fl in open(ffile):
+            f = fl.split()
+            if len(f) >= 2 and not fl.startswith("#"):
+                per_cell[f[0]] = float(f[1])
+        if stage in per_cell:
+            nsm = torch.cuda.get_device_properties(local).multi_processor_count
+            mhz = clocks.get("sm_max_mhz") or 1965.0
+            peak64 = 64.0 * nsm * mhz * 1e6
+            ach = per_cell[stage] * cells / (prof[stage] / 1000.0)
+            roofline_fp64 = {"bound": "fp64", "kernel": stage, "achieved": ach, "peak": peak64,
+                             "unit": "FP64 thread-instructions/s", "frac": ach / peak64,
+                             "instructions_per_cell": per_cell[stage],
+                             "peak_source": f"nominal: 64 FP64 lanes per SM x {nsm} SMs x {mhz:.0f} MHz"}
 
     # end to end through the public API with host buffers: pinned H2D of the
     # initial state, main.cu's host loop (global_dt read back every step, solve),
@@ -644,6 +691,7 @@ def main():
         "roofline": {"bound": "hbm", "kernel": stage, "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
                      "frac": achieved / pk["hbm_gbs"], "traffic": traffic, "peak_source": pk["source"],
                      "algorithmic_bytes_per_cell": ALGO_BYTES[stage]},
+        "roofline_fp64": roofline_fp64,
         "clocks": clocks,
         "e2e": e2e,
     }
@@ -704,6 +752,8 @@ def summary_of(line):
     """The ratios the north star states, in one place at the end of the line."""
     out = {"fp64_gzone_s": line["value"] / 1e9, "fp64_ms_per_step": line["ms_per_step"],
            "sweep_hbm_frac": line["roofline"]["frac"]}
+    if line.get("roofline_fp64"):
+        out["sweep_fp64_issue_frac"] = line["roofline_fp64"]["frac"]
     if "e2e" in line:
         out["e2e_gzone_s"] = line["e2e"]["value"] / 1e9
     if "fp32_mixed" in line:
@@ -720,7 +770,9 @@ def summary_of(line):
                                      "sigma0_noisy_1e-6": a["fd_sigma0"]["rel_err"]["1e-06"],
                                      "theta_1e-4": a["fd_theta"]["rel_err"],
                                      "theta_two_level_1e-6": [v["rel_err_two_level"]
-                                                              for v in a["fd_theta_scan"]["per_parameter"]]}
+                                                              for v in a["fd_theta_scan"]["per_parameter"]],
+                                     "theta_smooth_two_level_1e-6": [
+                                         v["rel_err_two_level"] for v in a["fd_theta_scan_smooth"]["per_parameter"]]}
     if "parity" in line:
         q = line["parity"]
         out["parity_rel_l1_max"] = max(q["rel_l1_r"], q["rel_l1_p"], q["rel_l1_mom"])

@@ -674,7 +674,10 @@ __global__ void __launch_bounds__(ADJ_THREADS) k_adj_flux(const Args a, const do
 // per face, the HLLC reverse gives the adjoints of the two half-states it
 // reads (k_rev_face); per cell, the reverse of its edge-state function
 // (reconstruction, flattening, characteristic tracing) gives the adjoints of
-// the 5 cells of its stencil (k_rev_cell); per interior cell, a gather adds
+// the 5 cells of its stencil (k_rev_cell_a: the characteristic tracing into the
+// reconstructions' adjoints, k_rev_cell_b: the reconstructions, flattening and
+// cs0 into the stencil; two kernels so that each holds fewer live values); per
+// interior cell, a gather adds
 // them to lam_in (k_rev_gather).  No atomics.  DIR 0 covers the xres + 1 faces
 // of a radial pencil and the cells NPAD - 1 .. NPAD + xres whose half-states
 // they read (stencil entries on the constant bound-0 ghosts drop out); DIR 1,
@@ -686,7 +689,11 @@ __global__ void __launch_bounds__(ADJ_THREADS) k_adj_flux(const Args a, const do
 // and the HLLC reverse.  Buffer per pencil: (n + 2) cells x (8 half-state
 // adjoints, 15 stencil adjoints, the two half-states (r, p, u and v for DIR 0,
 // w for DIR 1) and the flux of the cell's lower face (r, u, v or w, pres)).
-constexpr int REV_HALF = 8, REV_STEN = 15, REV_ST = REV_HALF + REV_STEN, REV_FX = REV_ST + 8, REV_SLOT = REV_FX + 4;
+constexpr int REV_HALF = 8, REV_STEN = 15, REV_ST = REV_HALF + REV_STEN, REV_FX = REV_ST + 8, REV_MID = REV_FX + 4;
+// REV_MID: the 16 adjoints between the two halves of a cell's edge-state
+// transposition (k_rev_cell_a -> k_rev_cell_b): of the four reconstructions'
+// {sL, a, sR}, then of cs0 and of the cell averages r, p, u the states read
+constexpr int REV_SLOT = REV_MID + 16;
 
 template <int DIR>
 __device__ __forceinline__ void rev_dims(const DiskView& d, int& n, int& npen, int& p0) {
@@ -889,73 +896,119 @@ __global__ void __launch_bounds__(ADJ_THREADS) k_adj_upd(const Args a, double* l
 // c - 2 + k.
 // g3 (optional): accumulates the theta derivative contracted with the same
 // adjoints: p = cs^2(theta) Sigma of the cells, the bound-0 ghost state, rot.
+// The stencil, cs0, flattening and the four reconstructions of pencil cell c
+// (the forward's expressions; the tapes record the branches taken).
 template <int DIR>
-__device__ __forceinline__ void edge_rev(const Args& a, int c, int q, const double* bl, const double* br,
-                                         double out[5][3], double* g3) {
-    const DiskView& d = a.d;
-    const Seed s0{-1, -1, -1, -1};
+struct EdgeFwd {
     double r[5], p[5], u[5], v[5];
-    double rad = 1.0, irad_q = 1.0, rot = 0.0;
-    if (DIR == 1) {
-        rad = d.radx[q];
-        irad_q = d.irad[q];
-        rot = d.rot[q];
-    }
-#pragma unroll
-    for (int k = 0; k < 5; ++k) {
-        const S3<double> C = (DIR == 0) ? ld<double>(a, s0, c - 2 + k, q) : ld<double>(a, s0, q, c - 2 + k);
-        r[k] = C.r;
-        p[k] = C.p;
-        if (DIR == 0) {
-            u[k] = C.u;
-            v[k] = C.v * d.radx[c - 2 + k];
-        } else {
-            u[k] = C.v - rot;
-            u[k] -= rad * d.frame_omega;
-            v[k] = C.u;
-        }
-    }
-    const double cs0 = sqrt(d.gam * p[2] / r[2]);
+    double rad, irad_q, cs0, flat, idx, xl, xr, sdt;
+    const double* wt;
     rev::FlatTape ft;
-    const double flat = rev::flatten_tape(1.0 / cs0, p[2], p[0], p[1], p[3], p[4], u[1], u[2], u[3], ft);
-    const double* wt = ((DIR == 0) ? d.wx : d.wy) + 6 * c;
-    const double* fa = (DIR == 0) ? d.xa : d.ya;
-    const double idx = ((DIR == 0) ? d.idx_x : d.idx_y)[c];
     rev::ReconTape tR, tP, tU, tV;
-    const Par R = rev::recon_tape(wt, r[0], r[1], r[2], r[3], r[4], flat, tR);
-    const Par P = rev::recon_tape(wt, p[0], p[1], p[2], p[3], p[4], flat, tP);
-    const Par U = rev::recon_tape(wt, u[0], u[1], u[2], u[3], u[4], flat, tU);
-    const Par V = rev::recon_tape(wt, v[0], v[1], v[2], v[3], v[4], flat, tV);
+    Par R, P, U, V;
+    __device__ __forceinline__ EdgeFwd(const Args& a, int c, int q) {
+        const DiskView& d = a.d;
+        const Seed s0{-1, -1, -1, -1};
+        rad = 1.0;
+        irad_q = 1.0;
+        double rot = 0.0;
+        if (DIR == 1) {
+            rad = d.radx[q];
+            irad_q = d.irad[q];
+            rot = d.rot[q];
+        }
+#pragma unroll
+        for (int k = 0; k < 5; ++k) {
+            const S3<double> C = (DIR == 0) ? ld<double>(a, s0, c - 2 + k, q) : ld<double>(a, s0, q, c - 2 + k);
+            r[k] = C.r;
+            p[k] = C.p;
+            if (DIR == 0) {
+                u[k] = C.u;
+                v[k] = C.v * d.radx[c - 2 + k];
+            } else {
+                u[k] = C.v - rot;
+                u[k] -= rad * d.frame_omega;
+                v[k] = C.u;
+            }
+        }
+        cs0 = sqrt(d.gam * p[2] / r[2]);
+        flat = rev::flatten_tape(1.0 / cs0, p[2], p[0], p[1], p[3], p[4], u[1], u[2], u[3], ft);
+        wt = ((DIR == 0) ? d.wx : d.wy) + 6 * c;
+        const double* fa = (DIR == 0) ? d.xa : d.ya;
+        idx = ((DIR == 0) ? d.idx_x : d.idx_y)[c];
+        R = rev::recon_tape(wt, r[0], r[1], r[2], r[3], r[4], flat, tR);
+        P = rev::recon_tape(wt, p[0], p[1], p[2], p[3], p[4], flat, tP);
+        U = rev::recon_tape(wt, u[0], u[1], u[2], u[3], u[4], flat, tU);
+        V = rev::recon_tape(wt, v[0], v[1], v[2], v[3], v[4], flat, tV);
+        xl = fa[c];
+        xr = fa[c + 1];
+        sdt = (DIR == 0) ? a.dt : a.dt * irad_q;
+    }
+};
+
+// First half of the transposition of both edge states of pencil cell c: the
+// characteristic tracing, from the half-state adjoints bl, br to the adjoints
+// of the four reconstructions and of the cell averages the states read
+// directly (mid[16], see REV_MID).
+template <int DIR>
+__device__ __forceinline__ void edge_rev_states(const Args& a, int c, int q, const double* bl, const double* br,
+                                                double* mid) {
+    const DiskView& d = a.d;
+    const EdgeFwd<DIR> F(a, c, q);
     const Par Z{0.0, 0.0, 0.0};
-    const double xl = fa[c], xr = fa[c + 1];
-    const double sdt = (DIR == 0) ? a.dt : a.dt * irad_q;
     const Half bsl{bl[0], bl[1], bl[2], DIR == 0 ? bl[3] : 0.0, DIR == 0 ? 0.0 : bl[3]};
     const Half bsr{br[0], br[1], br[2], DIR == 0 ? br[3] : 0.0, DIR == 0 ? 0.0 : br[3]};
     double bcs0 = 0.0, br0c = 0.0, bp0c = 0.0, bu0c = 0.0;
     Par bR{0.0, 0.0, 0.0}, bP{0.0, 0.0, 0.0}, bU{0.0, 0.0, 0.0}, bV{0.0, 0.0, 0.0}, bZ{0.0, 0.0, 0.0};
     if (DIR == 0) {
-        rev::state_left_rev(d.gam, xl, idx, sdt, cs0, r[2], p[2], u[2], R, P, U, V, Z, bsl, bcs0, br0c, bp0c, bu0c,
-                            bR, bP, bU, bV, bZ);
-        rev::state_right_rev(d.gam, xl, xr, idx, sdt, cs0, r[2], p[2], u[2], R, P, U, V, Z, bsr, bcs0, br0c, bp0c,
-                             bu0c, bR, bP, bU, bV, bZ);
+        rev::state_left_rev(d.gam, F.xl, F.idx, F.sdt, F.cs0, F.r[2], F.p[2], F.u[2], F.R, F.P, F.U, F.V, Z, bsl,
+                            bcs0, br0c, bp0c, bu0c, bR, bP, bU, bV, bZ);
+        rev::state_right_rev(d.gam, F.xl, F.xr, F.idx, F.sdt, F.cs0, F.r[2], F.p[2], F.u[2], F.R, F.P, F.U, F.V, Z,
+                             bsr, bcs0, br0c, bp0c, bu0c, bR, bP, bU, bV, bZ);
     } else {
-        rev::state_left_rev(d.gam, xl, idx, sdt, cs0, r[2], p[2], u[2], R, P, U, Z, V, bsl, bcs0, br0c, bp0c, bu0c,
-                            bR, bP, bU, bZ, bV);
-        rev::state_right_rev(d.gam, xl, xr, idx, sdt, cs0, r[2], p[2], u[2], R, P, U, Z, V, bsr, bcs0, br0c, bp0c,
-                             bu0c, bR, bP, bU, bZ, bV);
+        rev::state_left_rev(d.gam, F.xl, F.idx, F.sdt, F.cs0, F.r[2], F.p[2], F.u[2], F.R, F.P, F.U, Z, F.V, bsl,
+                            bcs0, br0c, bp0c, bu0c, bR, bP, bU, bZ, bV);
+        rev::state_right_rev(d.gam, F.xl, F.xr, F.idx, F.sdt, F.cs0, F.r[2], F.p[2], F.u[2], F.R, F.P, F.U, Z, F.V,
+                             bsr, bcs0, br0c, bp0c, bu0c, bR, bP, bU, bZ, bV);
     }
+    const Par* bs[4] = {&bR, &bP, &bU, &bV};
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        mid[3 * k] = bs[k]->sL;
+        mid[3 * k + 1] = bs[k]->a;
+        mid[3 * k + 2] = bs[k]->sR;
+    }
+    mid[12] = bcs0;
+    mid[13] = br0c;
+    mid[14] = bp0c;
+    mid[15] = bu0c;
+}
+
+// Second half: the reconstructions, the flattening and cs0 transposed into the
+// cell's 5-cell stencil; out[k][f]: adjoint of state variable f (Sigma with
+// p = cs^2 Sigma folded in, v_r, v_phi) of stencil cell c - 2 + k.
+// g3 (optional): accumulates the theta derivative contracted with the same
+// adjoints: p = cs^2(theta) Sigma of the cells, the bound-0 ghost state, rot.
+template <int DIR>
+__device__ __forceinline__ void edge_rev_recon(const Args& a, int c, int q, const double* mid, double out[5][3],
+                                               double* g3) {
+    const DiskView& d = a.d;
+    const EdgeFwd<DIR> F(a, c, q);
+    const Par bR{mid[0], mid[1], mid[2]}, bP{mid[3], mid[4], mid[5]};
+    const Par bU{mid[6], mid[7], mid[8]}, bV{mid[9], mid[10], mid[11]};
+    const double bcs0 = mid[12], br0c = mid[13], bp0c = mid[14], bu0c = mid[15];
     double ar[5] = {0.0, 0.0, 0.0, 0.0, 0.0}, ap[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
     double au[5] = {0.0, 0.0, 0.0, 0.0, 0.0}, av[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
     double bflat = 0.0;
-    rev::recon_rev(wt, tR, flat, bR, ar, bflat);
-    rev::recon_rev(wt, tP, flat, bP, ap, bflat);
-    rev::recon_rev(wt, tU, flat, bU, au, bflat);
-    rev::recon_rev(wt, tV, flat, bV, av, bflat);
-    rev::flatten_rev(ft, bflat, ap);
+    rev::recon_rev(F.wt, F.tR, F.flat, bR, ar, bflat);
+    rev::recon_rev(F.wt, F.tP, F.flat, bP, ap, bflat);
+    rev::recon_rev(F.wt, F.tU, F.flat, bU, au, bflat);
+    rev::recon_rev(F.wt, F.tV, F.flat, bV, av, bflat);
+    rev::flatten_rev(F.ft, bflat, ap);
     // cs0 = sqrt(gam p / r) of the middle cell, which also enters the states directly
-    const double bA = rev::dsqrt(cs0, bcs0);
-    ap[2] += bA * d.gam / r[2] + bp0c;
-    ar[2] += br0c - bA * d.gam * p[2] / (r[2] * r[2]);
+    const double bA = rev::dsqrt(F.cs0, bcs0);
+    ap[2] += bA * d.gam / F.r[2] + bp0c;
+    ar[2] += br0c - bA * d.gam * F.p[2] / (F.r[2] * F.r[2]);
     au[2] += bu0c;
     if (g3) {
         for (int th = 0; th < 3; ++th) {
@@ -964,7 +1017,7 @@ __device__ __forceinline__ void edge_rev(const Args& a, int c, int q, const doub
             for (int k = 0; k < 5; ++k) {
                 const int ik = (DIR == 0) ? c - 2 + k : q;
                 if (ik >= NPAD && ik < NPAD + d.xres) {
-                    g += ap[k] * r[k] * dt[T_CS2 * d.xarr + ik];
+                    g += ap[k] * F.r[k] * dt[T_CS2 * d.xarr + ik];
                 } else {  // radial ghost: init_C of the disk
                     g += ap[k] * dt[T_P0 * d.xarr + ik] + au[k] * dt[T_U0 * d.xarr + ik] +
                          av[k] * d.radx[ik] * dt[T_V0 * d.xarr + ik];
@@ -1024,11 +1077,36 @@ __global__ void __launch_bounds__(ADJ_THREADS) k_rev_face(const Args a, const do
 }
 
 template <int DIR>
-__global__ void __launch_bounds__(ADJ_THREADS) k_rev_cell(const Args a, double* buf, bool theta) {
+__global__ void __launch_bounds__(ADJ_THREADS, 3) k_rev_cell_a(const Args a, double* buf) {
     const DiskView& d = a.d;
     int n, npen, p0;
     rev_dims<DIR>(d, n, npen, p0);
     const int nc = (DIR == 0) ? n + 2 : n;  // cells per pencil with half-state adjoints
+    const int c0 = (DIR == 0) ? p0 - 1 : p0;
+    const long long total = (long long)nc * npen;
+    const RevBuf<DIR> B(d, buf);
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        int pen, c;
+        rev_thread<DIR>(t, nc, npen, c0, pen, c);
+        const int q = ((DIR == 0) ? d.ypad : NPAD) + pen;
+        double bl[4], br[4], mid[16];
+        for (int k = 0; k < 4; ++k) {
+            bl[k] = B(k, pen, c);
+            br[k] = B(4 + k, pen, c);
+        }
+        edge_rev_states<DIR>(a, c, q, bl, br, mid);
+#pragma unroll
+        for (int k = 0; k < 16; ++k) B(REV_MID + k, pen, c) = mid[k];
+    }
+}
+
+template <int DIR>
+__global__ void __launch_bounds__(ADJ_THREADS, 3) k_rev_cell_b(const Args a, double* buf, bool theta) {
+    const DiskView& d = a.d;
+    int n, npen, p0;
+    rev_dims<DIR>(d, n, npen, p0);
+    const int nc = (DIR == 0) ? n + 2 : n;
     const int c0 = (DIR == 0) ? p0 - 1 : p0;
     const long long total = (long long)nc * npen;
     double acc[3] = {0.0, 0.0, 0.0};
@@ -1038,13 +1116,11 @@ __global__ void __launch_bounds__(ADJ_THREADS) k_rev_cell(const Args a, double* 
         int pen, c;
         rev_thread<DIR>(t, nc, npen, c0, pen, c);
         const int q = ((DIR == 0) ? d.ypad : NPAD) + pen;
-        double bl[4], br[4];
-        for (int k = 0; k < 4; ++k) {
-            bl[k] = B(k, pen, c);
-            br[k] = B(4 + k, pen, c);
-        }
+        double mid[16];
+#pragma unroll
+        for (int k = 0; k < 16; ++k) mid[k] = B(REV_MID + k, pen, c);
         double out[5][3];
-        edge_rev<DIR>(a, c, q, bl, br, out, theta ? acc : nullptr);
+        edge_rev_recon<DIR>(a, c, q, mid, out, theta ? acc : nullptr);
 #pragma unroll
         for (int k = 0; k < 5; ++k)
 #pragma unroll
@@ -1828,7 +1904,8 @@ static void launch_pass(const Args& a, bool theta, double* scratch, double* rev,
             k_rev_flux<DIR><<<grid_for(pen * len), ADJ_THREADS, 0, s>>>(a, rev);
             k_adj_upd<DIR><<<g, ADJ_THREADS, 0, s>>>(a, scratch, theta, rev);
             k_rev_face<DIR><<<grid_for(pen * len), ADJ_THREADS, 0, s>>>(a, scratch, rev);
-            k_rev_cell<DIR><<<grid_for(pen * len), ADJ_THREADS, 0, s>>>(a, rev, theta);
+            k_rev_cell_a<DIR><<<grid_for(pen * len), ADJ_THREADS, 0, s>>>(a, rev);
+            k_rev_cell_b<DIR><<<grid_for(pen * len), ADJ_THREADS, 0, s>>>(a, rev, theta);
             k_rev_gather<DIR><<<g, ADJ_THREADS, 0, s>>>(a, rev);
             return;  // theta done by the reverse kernels
         }
