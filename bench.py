@@ -546,6 +546,10 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-forms", action="store_true", help="skip the FP32-mixed, ensemble and dust measurements")
     ap.add_argument("--no-tune", action="store_true", help="default launch configuration instead of the autotuner's")
+    ap.add_argument("--adjoint-steps", type=int, default=ADJOINT_STEPS,
+                    help="steps of the adjoint's finite-difference checks (the line reports it)")
+    ap.add_argument("--adjoint-timing-steps", type=int, default=ADJOINT_TIMING_STEPS,
+                    help="steps of the adjoint's timed run (the line reports it)")
     ap.add_argument("--tuning", default=None,
                     help="a fixed launch configuration instead of the autotuner's: comma list of "
                          "key=value over Disk.TUNING (v_sweep_x, ..., cps_kick2)")
@@ -575,16 +579,16 @@ def main():
     disk = Disk(p, device=local, stream=stream.cuda_stream)
     disk.set_state(0.0, state)
     W, K = max(3, args.warmup), args.steps
-    disk.run(W)
-    disk.sync()
-    disk.check()
-    if args.tuning:
+    if args.tuning:  # a fixed configuration applies from the first step on
         from penguin_b200.disk import describe_tuning
 
         choice = {k: int(v) for k, v in (kv.split("=") for kv in args.tuning.split(","))}
         disk.set_tuning(choice)
         tuning = dict(choice, passes=describe_tuning(choice), source="--tuning")
-    else:
+    disk.run(W)
+    disk.sync()
+    disk.check()
+    if not args.tuning:
         tuning = disk.autotune(reps=5) if not args.no_tune else None
 
     def barrier():
@@ -708,7 +712,7 @@ def main():
         # fixed sizes, independent of --steps: the finite-difference checks over
         # ADJOINT_STEPS steps and the timing over ADJOINT_TIMING_STEPS (16
         # checkpoint segments); together well under a second of GPU time
-        line["adjoint"] = measure_adjoint(ADJOINT_STEPS, local, stream, ADJOINT_TIMING_STEPS)
+        line["adjoint"] = measure_adjoint(args.adjoint_steps, local, stream, args.adjoint_timing_steps)
     if job.printer and world == 1 and not args.no_cpu_baseline:
         cb, orc, n_orc = cpu_baseline(p, state, 0.0, keep=True)
         line["cpu_baseline"] = cb

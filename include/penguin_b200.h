@@ -168,7 +168,7 @@ pg_status pg_disk_get_state(pg_disk* d, double* r, double* p, double* u, double*
    pg_disk_set_tuning applies a choice found earlier. */
 pg_status pg_disk_autotune(pg_disk* d, int reps, int* choice);
 pg_status pg_disk_set_tuning(pg_disk* d, const int* choice);
-/* Tile variant v of the FP64 sweeps and advection (0 .. 7), 6 ints: pencils
+/* Tile variant v of the FP64 sweeps and advection (0 .. 9), 6 ints: pencils
    per tile, outputs per pencil, cells per thread, TMA stages, threads per CTA,
    CTAs per SM its registers are compiled for.  PG_ERR_ARG past the last. */
 pg_status pg_sweep_variant(int v, int* out6);

@@ -1983,6 +1983,9 @@ struct pg_adj {
     // the azimuthal slope weights with the ghost rows taking their images'
     // (the transposition of the sweep treats the periodic seam as one face)
     double* wy_seam = nullptr;
+    // one backward step's reverse launches as a CUDA graph, updated in place
+    // for every step (only kernel parameters change from step to step)
+    cudaGraphExec_t step_exec = nullptr;
     double* gth = nullptr;
     unsigned long long* err = nullptr;
     Scalars* ssc = nullptr;  // scratch copy of the device scalars
@@ -2188,6 +2191,7 @@ pg_status pg_adj_destroy(pg_adj* a) {
     cudaFree(a->work);
     cudaFree(a->dtab);
     cudaFree(a->wy_seam);
+    if (a->step_exec) cudaGraphExecDestroy(a->step_exec);
     cudaFree(a->gth);
     cudaFree(a->err);
     cudaFree(a->ssc);
@@ -2362,25 +2366,62 @@ pg_status pg_adj_backward(pg_adj* a, const double* grad_out, double* grad_sigma0
         for (int n = n1 - 1; n >= n0; --n) {
             const int slot = n - n0;
             const StepRecord r = record_slot(a, slot, bank);
-            Args g = base_args(a, n, slot, &pl[2 * (size_t)slot], bank);
-            auto run = [&](int pass, const Cell* in) {
-                g.in = in;
-                g.lam = a->lam[c];
-                g.lam_in = a->lam[1 - c];
-                switch (pass) {
-                    case P_K2: g.lamv_in = a->lamv; launch_pass<P_K2>(g, true, a->scratch, a->rev_sweeps(), st); break;
-                    case P_ADV: launch_pass<P_ADV>(g, true, a->scratch, a->rev_sweeps(), st); break;
-                    case P_SY: launch_pass<P_SY>(g, true, a->scratch, a->rev_sweeps(), st); break;
-                    case P_SX: launch_pass<P_SX>(g, true, a->scratch, a->rev_sweeps(), st); break;
-                    default: g.lamv = a->lamv; launch_pass<P_K1>(g, true, a->scratch, a->rev_sweeps(), st); break;
-                }
-                c = 1 - c;
+            // the step's ~27 reverse launches, each pass reading lam[c] and writing lam[1 - c]
+            auto launch_step = [&](int& cc) {
+                Args g = base_args(a, n, slot, &pl[2 * (size_t)slot], bank);
+                auto run = [&](int pass, const Cell* in) {
+                    g.in = in;
+                    g.lam = a->lam[cc];
+                    g.lam_in = a->lam[1 - cc];
+                    switch (pass) {
+                        case P_K2: g.lamv_in = a->lamv; launch_pass<P_K2>(g, true, a->scratch, a->rev_sweeps(), st); break;
+                        case P_ADV: launch_pass<P_ADV>(g, true, a->scratch, a->rev_sweeps(), st); break;
+                        case P_SY: launch_pass<P_SY>(g, true, a->scratch, a->rev_sweeps(), st); break;
+                        case P_SX: launch_pass<P_SX>(g, true, a->scratch, a->rev_sweeps(), st); break;
+                        default: g.lamv = a->lamv; launch_pass<P_K1>(g, true, a->scratch, a->rev_sweeps(), st); break;
+                    }
+                    cc = 1 - cc;
+                };
+                run(P_K2, r.stage[4]);
+                if (d.orbadv) run(P_ADV, r.stage[3]);
+                run(P_SY, r.stage[2]);
+                run(P_SX, r.stage[1]);
+                run(P_K1, r.stage[0]);
             };
-            run(P_K2, r.stage[4]);
-            if (d.orbadv) run(P_ADV, r.stage[3]);
-            run(P_SY, r.stage[2]);
-            run(P_SX, r.stage[1]);
-            run(P_K1, r.stage[0]);
+            // Captured as a graph and launched in one call, the step's kernels follow
+            // one another with shorter gaps than stream launches leave; the graph
+            // of the first step is instantiated and every later step updates its
+            // kernel parameters in place.  Any failure falls back to stream launches.
+            bool done = false;
+            {
+                int cc = c;
+                cudaGraph_t gph = nullptr;
+                if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+                    launch_step(cc);
+                    const cudaError_t ce = cudaStreamEndCapture(st, &gph);
+                    if (ce == cudaSuccess && gph) {
+                        if (a->step_exec) {
+                            cudaGraphExecUpdateResultInfo info;
+                            if (cudaGraphExecUpdate(a->step_exec, gph, &info) != cudaSuccess) {
+                                cudaGetLastError();
+                                cudaGraphExecDestroy(a->step_exec);
+                                a->step_exec = nullptr;
+                            }
+                        }
+                        if (!a->step_exec && cudaGraphInstantiate(&a->step_exec, gph, 0) != cudaSuccess) {
+                            cudaGetLastError();
+                            a->step_exec = nullptr;
+                        }
+                        if (a->step_exec && cudaGraphLaunch(a->step_exec, st) == cudaSuccess) {
+                            done = true;
+                            c = cc;
+                        }
+                    }
+                    if (gph) cudaGraphDestroy(gph);
+                    cudaGetLastError();
+                }
+            }
+            if (!done) launch_step(c);
             ADJ_CUDA(cudaGetLastError());
         }
         ADJ_CUDA(cudaEventRecord(a->ev_rev[bank], st));

@@ -10,14 +10,16 @@ namespace pg {
 
 // Tile variants of the FP64 sweeps and residual advection, the autotuner's knobs
 // (pg_disk_autotune): pencils per tile W, outputs per pencil L, cells per thread
-// in each phase, TMA stages in flight.  pg_kernels.cu instantiates each (SV<v>).
+// in each phase, TMA stages in flight, and CTAs per SM the registers are
+// compiled for (0: as many as ~96 registers a thread allow; more caps the
+// registers and may spill).  pg_kernels.cu instantiates each (SV<v>).
 struct SweepVariant {
-    int w, len, cpt, stages;
+    int w, len, cpt, stages, minb;
 };
-constexpr int NSWEEP_VARIANTS = 8;
+constexpr int NSWEEP_VARIANTS = 10;
 constexpr SweepVariant SWEEP_VARIANTS[NSWEEP_VARIANTS] = {
-    {8, 32, 1, 2}, {4, 32, 1, 2}, {16, 16, 1, 2}, {8, 16, 1, 2},
-    {8, 32, 2, 2}, {8, 32, 1, 3}, {4, 32, 1, 3}, {4, 64, 1, 2}};
+    {8, 32, 1, 2, 0}, {4, 32, 1, 2, 0}, {16, 16, 1, 2, 0}, {8, 16, 1, 2, 0}, {8, 32, 2, 2, 0},
+    {8, 32, 1, 3, 0}, {4, 32, 1, 3, 0}, {4, 64, 1, 2, 0}, {4, 32, 1, 2, 5}, {8, 32, 1, 2, 3}};
 // the radial box holds 5 (L + 6) doubles in one row, at most 256 TMA elements
 inline bool sweep_variant_x_ok(int v) { return 5 * (SWEEP_VARIANTS[v].len + 2 * NPAD) <= 256; }
 

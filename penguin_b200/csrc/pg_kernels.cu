@@ -61,7 +61,9 @@ template <> struct SV<4> { using G = SwCfg<8, 32, 2, 2>; };
 template <> struct SV<5> { using G = SwCfg<8, 32, 1, 3>; };
 template <> struct SV<6> { using G = SwCfg<4, 32, 1, 3>; };
 template <> struct SV<7> { using G = SwCfg<4, 64, 1, 2>; };   // azimuthal passes only (x box too wide)
-static_assert(NSWEEP_VARIANTS == 8, "SV<> and SWEEP_VARIANTS list the same variants");
+template <> struct SV<8> { using G = SwCfg<4, 32, 1, 2, 5>; };  // registers capped for 5 CTAs per SM
+template <> struct SV<9> { using G = SwCfg<8, 32, 1, 2, 3>; };  // registers capped for 3 CTAs per SM
+static_assert(NSWEEP_VARIANTS == 10, "SV<> and SWEEP_VARIANTS list the same variants");
 
 constexpr int ST_TX = 32, ST_TY = 8;        // stencil kernels: 32 x 8 outputs
 constexpr int ST_HX = ST_TX + 2, ST_HY = ST_TY + 2;
@@ -1107,6 +1109,8 @@ cudaError_t set_kernel_attributes() {
     set_v(SV<5>{});
     set_v(SV<6>{});
     set_v(SV<7>{});
+    set_v(SV<8>{});
+    set_v(SV<9>{});
     set((const void*)k_kick1<true>, K1_SMEM);
     set((const void*)k_kick1<false>, K1_SMEM);
     set((const void*)k_kick2<true>, K5_SMEM);
@@ -1253,6 +1257,8 @@ static void with_variant(int v, F&& f) {
         case 5: f(SV<5>{}); break;
         case 6: f(SV<6>{}); break;
         case 7: f(SV<7>{}); break;
+        case 8: f(SV<8>{}); break;
+        case 9: f(SV<9>{}); break;
         default: f(SV<0>{}); break;
     }
 }

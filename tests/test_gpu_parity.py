@@ -233,7 +233,7 @@ def test_autotuned_launches_give_identical_results():
     b = tuned.get_state()
     for k in _keys(p):
         assert np.array_equal(a[k], b[k]), k
-    for v in range(8):
+    for v in range(10):
         vx = v if sweep_variant(v)["pencil_length"] + 6 <= 51 else 0  # radial boxes of at most 256 doubles
         forced = Disk(p)
         forced.set_state(case["t0"], st)
