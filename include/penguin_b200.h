@@ -75,6 +75,14 @@ typedef struct {
        n_planet 1 (the planet).  Through pg_grid_* the caller's planets array
        holds the star (planets[0]) and the planet (planets[1]). */
     int twobd_flag;
+    /* ndim 3 (spherical r, phi, theta or cartesian x, y, z): polar cells, the
+       polar geometry (0 cartesian, 5 polar angle) and grid (0 linear, 1 log,
+       2/3/4 the reference's non-uniform spacings, src/geom/geom.cu:35-89), and
+       the polar boundaries (bound_bom at zmin, bound_top at zmax: 0 analytic
+       state, 1 zero gradient, 2 reflecting, 3 periodic;
+       src/boundary/boundary.cu:270-320).  Ignored when ndim < 3. */
+    int zres, geomz, gridz;
+    int bound_bom, bound_top;
 } pg_params;
 
 /*
@@ -335,6 +343,48 @@ long long pg_adj_device_bytes(const pg_adj* a);
    kernels (hand = 1, the default) or by the dual-number kernels (hand = 0,
    kept as their check).  Both give the same gradient to rounding. */
 pg_status pg_adj_set_sweep_reverse(pg_adj* a, int hand);
+
+/* ------------------------------------------------------ 3D (ndim 3) */
+/*
+ * One 3D grid on one B200: the reference's DS() with the polar sweep
+ * (src/solver/solve.cu:212-292 with ndim 3; sweepz_inplace, src/solver/sweeps.cu:
+ * 458-554) on the spherical (r, phi, theta) grid of its 3D preset
+ * (include/para_files/Adiabatic_CPD.h: geomx 2, geomy 4, geomz 5) or on a
+ * cartesian box (0, 0, 0); ideal or isothermal gas, a periodic azimuth, radial
+ * boundaries 0-2 and polar boundaries 0-3 (bound_bom, bound_top), optional
+ * planet and wave damping; no viscosity, orbital advection, dust, cooling or
+ * two-body frame (PG_ERR_CONFIG).  Fields are interior arrays of
+ * xres*yres*zres values, x fastest, then y, then z (the checkpoint order of
+ * src/output/output.cu:95-123).
+ */
+typedef struct pg_disk3 pg_disk3;
+pg_status pg_disk3_create(const pg_params* P, int device, void* stream, pg_disk3** out);
+pg_status pg_disk3_destroy(pg_disk3* d);
+/* Restart injection (load_grid, src/output/output.cu:182-248): ghosts take
+   init_C, time is set to t, the planet is initialised at t. */
+pg_status pg_disk3_set_state(pg_disk3* d, double t, const double* r, const double* p, const double* u,
+                             const double* v, const double* w);
+pg_status pg_disk3_get_state(pg_disk3* d, double* r, double* p, double* u, double* v, double* w, double* t_out);
+/* global_dt (src/timestep/timestep.cu:113-140, ndim 3): min(CFL dt, 1.1 dt_prev); blocking. */
+pg_status pg_disk3_global_dt(pg_disk3* d, double dt_prev, double* dt_out);
+/* solve (src/solver/solve.cu:279-292) with host t and dt; stream-ordered. */
+pg_status pg_disk3_solve(pg_disk3* d, double t, double dt);
+/* nsteps of main.cu's loop (main.cu:320-360) with t, dt and the planet on the
+   device, each step replayed as a CUDA graph; stream-ordered. */
+pg_status pg_disk3_run(pg_disk3* d, int nsteps, double end_time);
+pg_status pg_disk3_clock(pg_disk3* d, double* t, double* dt, long long* steps);
+/* Synchronises and reports (then clears) the device error word. */
+pg_status pg_disk3_check(pg_disk3* d);
+/* nsteps device-clocked steps with CUDA events between the passes: average ms
+   of the clock, kick1, sweep_x, sweep_y, sweep_z and kick2 (ms6). */
+pg_status pg_disk3_pass_times(pg_disk3* d, int nsteps, double* ms6);
+/* test support: one step with host t and dt, the whole cell array (ghosts
+   included) after each pass into out[5][zarr][yarr][xarr]: kick1, sweep_x,
+   sweep_y, sweep_z, kick2 with the damping.  Blocking. */
+pg_status pg_disk3_stages(pg_disk3* d, double t, double dt, pg_cell* out);
+/* Host copy of one axis of the grid the library builds (src/init/init.cu:472-500
+   with src/geom/geom.cu): axis 0 x, 1 y, 2 z; faces a[arr+1], volumes v[arr]. */
+pg_status pg_make_axis(const pg_params* P, int axis, double* a, double* v);
 
 #ifdef __cplusplus
 }

@@ -1748,3 +1748,6 @@ int orc_run(orc_state* S, double t0, double dt_prev, int max_step, double end_ti
     if (dt_out) *dt_out = dt;
     return nstep;
 }
+
+/* the 3D part shares this file's pencil routines */
+#include "oracle3d.c"

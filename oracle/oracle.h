@@ -34,7 +34,7 @@ typedef struct { double m, a, e, x, y, z, vx, vy, vz, rs; } orc_body;
 typedef struct { double r, u, v, w; } orc_dust;                /* include/structs.h:19 */  /* include/structs.h:105 */
 
 typedef struct {
-    int ndim;                 /* 1 or 2 */
+    int ndim;                 /* 1, 2 or 3 (3: oracle3d.c) */
     int xres, yres;           /* interior cells */
     int geomx, geomy;         /* x: 0 cartesian, 1 cylindrical radius; y: 0 cartesian, 3 azimuth */
     int gridx, gridy;         /* 0 linear, 1 logarithmic */
@@ -58,6 +58,8 @@ typedef struct {
     int cool_flag;            /* 0 off, 1 t_c = beta r^1.5, 2 t_c = beta / r sqrt(p/r) / h (src/solver/cool/cool.cu) */
     double beta_cool;
     int twobd_flag;           /* 1: star and planet orbit their barycentre (src/planet/planet.cu:135-175) */
+    int zres, geomz, gridz;   /* ndim 3: polar cells, geometry (0 cartesian, 5 polar angle), grid (0-4) */
+    int bound_bom, bound_top; /* ndim 3: polar boundaries at zmin / zmax (0 analytic, 1 zero gradient, 2 reflecting, 3 periodic) */
 } orc_params;
 
 typedef struct orc_state orc_state;
@@ -99,6 +101,31 @@ void orc_viscous_forces(orc_state* S, int which, double* vis_out /* 2*xarr*yarr 
 void orc_sweepx(orc_state* S, double dt);
 void orc_sweepy(orc_state* S, double dt);
 int orc_solve_stages(orc_state* S, double t, double dt, orc_cell* out, orc_dust* dout /* or NULL */);
+
+/* ---- ndim 3 (oracle3d.c): the reference's step with the polar sweep ---- */
+typedef struct orc3_state orc3_state;
+orc3_state* orc3_create(const orc_params* P);
+void orc3_destroy(orc3_state* S);
+int orc3_dims(const orc3_state* S, int* xarr, int* yarr, int* zarr);  /* returns the ghost width */
+void orc3_get_axis(const orc3_state* S, int axis, double* a, double* v);  /* faces arr+1, volumes arr */
+void orc3_fill_init(orc3_state* S);
+/* interior fields, x fastest, then y, then z (src/output/output.cu:182-248) */
+void orc3_set_interior(orc3_state* S, const double* r, const double* p, const double* u, const double* v,
+                       const double* w);
+void orc3_get_interior(const orc3_state* S, double* r, double* p, double* u, double* v, double* w);
+void orc3_init_planet(orc3_state* S, double t);
+void orc3_get_planet(const orc3_state* S, orc_body* out);
+void orc3_boundx(orc3_state* S);
+void orc3_boundy(orc3_state* S);
+void orc3_boundz(orc3_state* S);
+void orc3_sweepx(orc3_state* S, double dt);
+void orc3_sweepy(orc3_state* S, double dt);
+void orc3_sweepz(orc3_state* S, double dt);
+double orc3_global_dt(orc3_state* S, double dt_prev);
+void orc3_solve(orc3_state* S, double t, double dt);
+int orc3_run(orc3_state* S, double t0, double dt_prev, int max_step, double end_time, double* t_out, double* dt_out);
+/* one step, the cell array after each stage (see oracle3d.c); returns the stage count */
+int orc3_solve_stages(orc3_state* S, double t, double dt, orc_cell* out);
 
 #ifdef __cplusplus
 }

@@ -36,6 +36,8 @@ class OrcParams(ctypes.Structure):
         ("dust_flag", ctypes.c_int), ("stokes", ctypes.c_double), ("d_g_ratio", ctypes.c_double),
         ("cool_flag", ctypes.c_int), ("beta_cool", ctypes.c_double),
         ("twobd_flag", ctypes.c_int),
+        ("zres", ctypes.c_int), ("geomz", ctypes.c_int), ("gridz", ctypes.c_int),
+        ("bound_bom", ctypes.c_int), ("bound_top", ctypes.c_int),
     ]
 
     @classmethod
@@ -48,6 +50,7 @@ class OrcParams(ctypes.Structure):
             p.visc_flag, p.OrbAdv_flag, p.kill_flag, p.kill_width, p.kill_width_out,
             p.n_planet, p.planet_mass, p.planet_ecc, p.rs_fac, p.ramp_time, p.zmin, p.zmax,
             p.dust_flag, p.Stokes, p.D_G_ratio, p.cool_flag, p.beta_cool, p.twobd_flag,
+            p.zres, p.geomz, p.gridz, p.bound_bom, p.bound_top,
         )
 
 
@@ -57,8 +60,8 @@ class OrcBody(ctypes.Structure):
 
 def build(force: bool = False) -> str:
     """Compile liboracle.so with the Makefile beside this file."""
-    src = os.path.join(HERE, "oracle.c")
-    if force or not os.path.exists(LIB_PATH) or os.path.getmtime(LIB_PATH) < os.path.getmtime(src):
+    srcs = [os.path.join(HERE, f) for f in ("oracle.c", "oracle3d.c", "oracle.h")]
+    if force or not os.path.exists(LIB_PATH) or any(os.path.getmtime(LIB_PATH) < os.path.getmtime(f) for f in srcs):
         subprocess.run(["make", "-s", "-C", HERE, "liboracle.so"], check=True)
     return LIB_PATH
 
@@ -101,6 +104,28 @@ def lib():
         L.orc_sweepy.argtypes = [vp, ctypes.c_double]
         L.orc_solve_stages.restype = ctypes.c_int
         L.orc_solve_stages.argtypes = [vp, ctypes.c_double, ctypes.c_double, dp, dp]
+        L.orc3_create.restype = vp
+        L.orc3_create.argtypes = [ctypes.POINTER(OrcParams)]
+        L.orc3_destroy.argtypes = [vp]
+        L.orc3_dims.restype = ctypes.c_int
+        L.orc3_dims.argtypes = [vp, ip, ip, ip]
+        L.orc3_get_axis.argtypes = [vp, ctypes.c_int, dp, dp]
+        L.orc3_fill_init.argtypes = [vp]
+        L.orc3_set_interior.argtypes = [vp, dp, dp, dp, dp, dp]
+        L.orc3_get_interior.argtypes = [vp, dp, dp, dp, dp, dp]
+        L.orc3_init_planet.argtypes = [vp, ctypes.c_double]
+        L.orc3_get_planet.argtypes = [vp, ctypes.POINTER(OrcBody)]
+        for name in ("orc3_boundx", "orc3_boundy", "orc3_boundz"):
+            getattr(L, name).argtypes = [vp]
+        for name in ("orc3_sweepx", "orc3_sweepy", "orc3_sweepz"):
+            getattr(L, name).argtypes = [vp, ctypes.c_double]
+        L.orc3_global_dt.restype = ctypes.c_double
+        L.orc3_global_dt.argtypes = [vp, ctypes.c_double]
+        L.orc3_solve.argtypes = [vp, ctypes.c_double, ctypes.c_double]
+        L.orc3_solve_stages.restype = ctypes.c_int
+        L.orc3_solve_stages.argtypes = [vp, ctypes.c_double, ctypes.c_double, dp]
+        L.orc3_run.restype = ctypes.c_int
+        L.orc3_run.argtypes = [vp, ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_double, dp, dp]
         _lib = L
     return _lib
 
@@ -198,5 +223,77 @@ class Oracle:
         t_out, dt_out = ctypes.c_double(), ctypes.c_double()
         n = lib().orc_run(self.h, self.t, self.dt if self.dt else -1.0, max_step, end_time,
                          ctypes.byref(t_out), ctypes.byref(dt_out))
+        self.t, self.dt = t_out.value, dt_out.value
+        return n
+
+
+FIELDS3 = ("r", "p", "u", "v", "w")
+
+
+class Oracle3:
+    """One 3D grid (ndim 3) on the CPU, stepping like the reference's main loop.
+    Fields are arrays of shape (zres, yres, xres)."""
+
+    def __init__(self, params, state: dict | None = None, t0: float = 0.0):
+        self.p = params
+        self._P = OrcParams.from_params(params)
+        self.h = lib().orc3_create(ctypes.byref(self._P))
+        xa, ya, za = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        lib().orc3_dims(self.h, ctypes.byref(xa), ctypes.byref(ya), ctypes.byref(za))
+        self.xarr, self.yarr, self.zarr = xa.value, ya.value, za.value
+        lib().orc3_fill_init(self.h)
+        if state is not None:
+            self.set_interior(state)
+        self.t = t0
+        self.dt = None
+        lib().orc3_init_planet(self.h, t0)
+
+    def close(self) -> None:
+        h = getattr(self, "h", None)
+        if h:
+            lib().orc3_destroy(h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def axis(self, axis: int):
+        n = (self.xarr, self.yarr, self.zarr)[axis]
+        a, v = np.zeros(n + 1), np.zeros(n)
+        lib().orc3_get_axis(self.h, axis, _dp(a), _dp(v))
+        return a, v
+
+    def set_interior(self, s: dict) -> None:
+        f = {k: np.ascontiguousarray(s[k], dtype=np.float64) for k in FIELDS3}
+        lib().orc3_set_interior(self.h, *(_dp(f[k]) for k in FIELDS3))
+
+    def interior(self) -> dict:
+        shape = (self.p.zres, self.p.yres, self.p.xres)
+        out = {k: np.zeros(shape) for k in FIELDS3}
+        lib().orc3_get_interior(self.h, *(_dp(out[k]) for k in FIELDS3))
+        return out
+
+    def planet(self) -> dict:
+        b = OrcBody()
+        lib().orc3_get_planet(self.h, ctypes.byref(b))
+        return {k: getattr(b, k) for k, _ in OrcBody._fields_}
+
+    def global_dt(self, dt_prev: float) -> float:
+        return lib().orc3_global_dt(self.h, dt_prev)
+
+    def solve(self, t: float, dt: float) -> None:
+        lib().orc3_solve(self.h, t, dt)
+
+    def solve_stages(self, t: float, dt: float):
+        """One step, returning the cell arrays (zarr, yarr, xarr, 5) after each stage."""
+        buf = np.zeros((6, self.zarr, self.yarr, self.xarr, 5))
+        k = lib().orc3_solve_stages(self.h, t, dt, _dp(buf))
+        return buf[:k]
+
+    def run(self, max_step: int, end_time: float = 1.0e30) -> int:
+        """main.cu:320-360 (see Oracle.run)."""
+        t_out, dt_out = ctypes.c_double(), ctypes.c_double()
+        n = lib().orc3_run(self.h, self.t, self.dt if self.dt else -1.0, max_step, end_time,
+                          ctypes.byref(t_out), ctypes.byref(dt_out))
         self.t, self.dt = t_out.value, dt_out.value
         return n

@@ -9,7 +9,10 @@
 // dust_flag builds (main.cu's dust allocations are repeated).  Used to pin the
 // oracle stage by stage and to locate discrepancies.
 //
-//   stages <restart file> <steps> <dump file> [scrub]
+//   stages <restart file> <steps> <dump file> [scrub] [last]
+//
+// With "last", only the final stage of the last step is written (the state a
+// run of that many steps ends with), for grids whose every stage is too large.
 //
 // With "scrub", a kernel of this driver writes zeros over the dynamic shared
 // memory of every SM right before each dust stage: the reference's dust
@@ -34,6 +37,10 @@ void apply_source_terms(Grid*, double, double, double);
 void apply_source_terms_inplace(Grid*, double, double, double);
 void sweepx_inplace(Grid*, double);
 void sweepy_inplace(Grid*, double);
+#if ndim > 2
+void boundz(Grid*);
+void sweepz_inplace(Grid*, double);
+#endif
 void set_OrbAdv(Grid*, double);
 void shift_OrbAdv(Grid*);
 void advecty(Grid*, double);
@@ -52,6 +59,8 @@ static Dust* g_dhost = nullptr;
 
 static FILE* g_dump = nullptr;
 static bool g_scrub = false;
+static bool g_last_only = false;  // write only the final stage of the last step
+static bool g_final_step = false;
 
 // Zeros the dynamic shared memory of many blocks per SM (diagnostic only).
 __global__ void scrub_smem(int nd) {
@@ -81,6 +90,15 @@ static void scrub() {
 
 static void dump(Grid* dev, const char* name, double t, double dt) {
     check(name);
+#ifdef kill_flag
+    const bool final_stage = std::string(name) == "kill";
+#else
+    const bool final_stage = std::string(name) == "kick2";
+#endif
+    if (g_last_only && !(g_final_step && final_stage)) {
+        printf("stage %2d %-10s t=%.12f dt=%.6e (not written)\n", g_stage++, name, t, dt);
+        return;
+    }
     size_t n = (size_t)dev[0].xarr * dev[0].yarr * dev[0].zarr;
     cudaMemcpy(g_host, dev[0].C, n * sizeof(Cell), cudaMemcpyDeviceToHost);
     char tag[32] = {0};
@@ -101,11 +119,14 @@ static void dump(Grid* dev, const char* name, double t, double dt) {
 
 int main(int argc, char** argv) {
     if (argc < 4) {
-        printf("usage: %s <restart> <steps> <dump>\n", argv[0]);
+        printf("usage: %s <restart> <steps> <dump> [scrub] [last]\n", argv[0]);
         return 2;
     }
     int steps = atoi(argv[2]);
-    g_scrub = (argc > 4 && std::string(argv[4]) == "scrub");
+    for (int a = 4; a < argc; ++a) {
+        if (std::string(argv[a]) == "scrub") g_scrub = true;
+        if (std::string(argv[a]) == "last") g_last_only = true;
+    }
     g_dump = fopen(argv[3], "wb");
     Grid* hst;
     Grid* dev;
@@ -184,6 +205,7 @@ int main(int argc, char** argv) {
 
     double dt = end_time - t;
     for (int s = 0; s < steps; ++s) {
+        g_final_step = (s == steps - 1);
         dt = global_dt(hst, dev, dt);
         double hdt = 0.5 * dt;
 #ifdef visc_flag
@@ -203,6 +225,11 @@ int main(int argc, char** argv) {
         boundy(dev, t + dt);
         sweepy_inplace(dev, dt);
         dump(dev, "sweepy", t, dt);
+#endif
+#if ndim > 2
+        boundz(dev);
+        sweepz_inplace(dev, dt);
+        dump(dev, "sweepz", t, dt);
 #endif
 #ifdef dust_flag
         boundx_dust(dev);

@@ -34,6 +34,8 @@ EXPORTS = [
     "pg_ens_get_dust", "pg_ens_autotune", "pg_ens_set_tuning",
     "pg_adj_check_params", "pg_adj_create", "pg_adj_destroy", "pg_adj_set_params", "pg_adj_forward",
     "pg_adj_backward", "pg_adj_model_error", "pg_adj_dot_test", "pg_adj_pass_check", "pg_adj_replay_diff", "pg_adj_pass_fields", "pg_adj_schedule", "pg_adj_steps", "pg_adj_device_bytes", "pg_adj_set_sweep_reverse",
+    "pg_disk3_create", "pg_disk3_destroy", "pg_disk3_set_state", "pg_disk3_get_state", "pg_disk3_global_dt",
+    "pg_disk3_solve", "pg_disk3_run", "pg_disk3_clock", "pg_disk3_check", "pg_disk3_pass_times", "pg_disk3_stages", "pg_make_axis",
 ]
 
 
@@ -133,6 +135,18 @@ def lib() -> ctypes.CDLL:
         "pg_ens_profile": (i, [vp, i, d, ctypes.POINTER(ctypes.c_float), i]),
         "pg_ens_autotune": (i, [vp, i, ip]),
         "pg_ens_set_tuning": (i, [vp, ip]),
+        "pg_disk3_create": (i, [PP, i, vp, ctypes.POINTER(vp)]),
+        "pg_disk3_destroy": (i, [vp]),
+        "pg_disk3_set_state": (i, [vp, d, dp, dp, dp, dp, dp]),
+        "pg_disk3_get_state": (i, [vp, dp, dp, dp, dp, dp, dp]),
+        "pg_disk3_global_dt": (i, [vp, d, dp]),
+        "pg_disk3_solve": (i, [vp, d, d]),
+        "pg_disk3_run": (i, [vp, i, d]),
+        "pg_disk3_clock": (i, [vp, dp, dp, ctypes.POINTER(ctypes.c_longlong)]),
+        "pg_disk3_check": (i, [vp]),
+        "pg_disk3_pass_times": (i, [vp, i, dp]),
+        "pg_disk3_stages": (i, [vp, d, d, dp]),
+        "pg_make_axis": (i, [PP, i, dp, dp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

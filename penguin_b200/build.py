@@ -19,7 +19,7 @@ INCLUDE = os.path.join(ROOT, "include")
 LIB = os.path.join(PKG, "libpenguin_b200.so")
 OBJ = os.path.join(PKG, "_build")
 
-SOURCES = ["pg_kernels.cu", "pg_engine.cu", "pg_noalloc.cu", "pg_f32.cu", "pg_ensemble.cu", "pg_dust.cu", "pg_adjoint.cu"]
+SOURCES = ["pg_kernels.cu", "pg_engine.cu", "pg_noalloc.cu", "pg_f32.cu", "pg_ensemble.cu", "pg_dust.cu", "pg_adjoint.cu", "pg_3d.cu"]
 HEADERS = ["pg_common.cuh", "pg_hydro.cuh", "pg_internal.h", "pg_planet.cuh", "pg_f32.cuh", "pg_dust.cuh", "pg_dual.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I" + INCLUDE]

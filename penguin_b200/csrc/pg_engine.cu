@@ -47,15 +47,61 @@ double compensated_sum(const double* a, int n) {
     } while (0)
 
 // ------------------------------------------------------------------ grid
-// src/init/init.cu:472-500 with linspace / logspace of src/geom/geom.cu:22-33
-static void make_grid(double* a, double* v, double amin, double amax, int res, int pad, int geom, int grid) {
-    const int len = res + 1;
+// Power-law stretch of the non-uniform spacings (src/geom/geom.cu:43,65,84).
+static double stretch(double dx_max, double dx_min, double L, int N) {
+    return std::log(1.0 - (dx_max - dx_min) / (L - (double)N * dx_min)) / std::log(1.0 - 1.0 / (double)N);
+}
+
+// Faces a[pad .. pad+res] of one axis (src/geom/geom.cu:22-89): 0 linear,
+// 1 logarithmic, 2 fine in the middle, 3 fine towards amax (the midplane),
+// 4 fine over the radial extent around the middle.  2-4 read the radial grid's
+// xres / xmin / xmax and sc_h of P, as the reference reads its constants.
+static void spacing(double* a, double start, double end, int len, int grid, const pg_params* P) {
     if (grid == 1) {
-        const double tmp = std::log(amax / amin);
-        for (int i = 0; i < len; i++) a[pad + i] = amin * std::exp(tmp * (double)i / (double)(len - 1));
+        const double tmp = std::log(end / start);
+        for (int i = 0; i < len; i++) a[i] = start * std::exp(tmp * (double)i / (double)(len - 1));
+    } else if (grid == 2) {
+        const int N = (len - 1) / 2;
+        const double L = (end - start) / 2.0;
+        const double dx_min = (L / (double)N) / 32.0;
+        const double dx_max = (PI - L) / N;
+        const double k = stretch(dx_max, dx_min, L, N);
+        for (int i = 0; i < N; i++)
+            a[i] = (end + start) / 2.0 - (N - i) * dx_min - (L - N * dx_min) * std::pow((double)(N - i) / (double)N, k);
+        for (int i = 0; i < N + 1; i++)
+            a[N + i] = (end + start) / 2.0 + i * dx_min + (L - N * dx_min) * std::pow((double)i / (double)N, k);
+    } else if (grid == 3) {
+        const int N = len - 1;
+        const double L = end - start;
+        const double dx_min = ((P->xmax - P->xmin) / (double)P->xres) / 32.0;
+        const double dx_max = P->sc_h / 16.0;
+        const double k = stretch(dx_max, dx_min, L, N);
+        for (int i = 0; i < N + 1; i++)
+            a[i] = end - (N - i) * dx_min - (L - N * dx_min) * std::pow((double)(N - i) / (double)N, k);
+    } else if (grid == 4) {
+        const int N = P->xres / 2;
+        const int N2 = (len - 1 - 2 * N) / 2;
+        const double L = (P->xmax - P->xmin) / 2.0;
+        const double L2 = (end - start - 2.0 * L) / 2.0;
+        const double dx_min = (L / (double)N) / 32.0;
+        const double dx_max = L2 / (double)N2;
+        const double k = stretch(dx_max, dx_min, L, N);
+        for (int i = 0; i < N2; i++) a[i] = start + (double)i * dx_max;
+        for (int i = 0; i < N; i++)
+            a[i + N2] = (end + start) / 2.0 - (N - i) * dx_min - (L - N * dx_min) * std::pow((double)(N - i) / (double)N, k);
+        for (int i = 0; i < N; i++)
+            a[i + N2 + N] = (end + start) / 2.0 + i * dx_min + (L - N * dx_min) * std::pow((double)i / (double)N, k);
+        for (int i = 0; i < N2 + 1; i++) a[i + N2 + 2 * N] = start + 2.0 * L + L2 + (double)i * dx_max;
     } else {
-        for (int i = 0; i < len; i++) a[pad + i] = amin + (amax - amin) * (double)i / (double)(len - 1);
+        for (int i = 0; i < len; i++) a[i] = start + (end - start) * (double)i / (double)(len - 1);
     }
+}
+
+// make_grid of src/init/init.cu:472-500: faces with ghosts and cell volumes
+// dr * get_dv_dr (src/geom/geom.cu:3-20; geom 5 the polar angle)
+void make_grid(double* a, double* v, double amin, double amax, int res, int pad, int geom, int grid,
+               const pg_params* P) {
+    spacing(&a[pad], amin, amax, res + 1, grid, P);
     for (int i = 0; i < pad; i++) {
         if (grid == 1) {
             a[i] = amin * std::exp(std::log(amax / amin) * (double)(i - pad) / (double)(res));
@@ -66,8 +112,11 @@ static void make_grid(double* a, double* v, double amin, double amax, int res, i
         }
     }
     for (int i = 0; i < res + 2 * pad; i++) {
-        const double dr = a[i + 1] - a[i];
-        const double dvdr = (geom == 2) ? a[i] * a[i] + a[i] * dr + dr * dr / 3.0 : (geom == 1 ? a[i] + dr / 2.0 : 1.0);
+        const double ra = a[i], dr = a[i + 1] - a[i];
+        double dvdr = 1.0;
+        if (geom == 5) dvdr = (dr < 1.0e-4) ? std::sin(ra + 0.5 * dr) : (std::cos(ra) - std::cos(ra + dr)) / dr;
+        else if (geom == 2) dvdr = ra * ra + ra * dr + dr * dr / 3.0;
+        else if (geom == 1) dvdr = ra + dr / 2.0;
         v[i] = dr * dvdr;
     }
 }
@@ -212,7 +261,7 @@ void periodic_seam_weights(double* wy, int ypad, int yres) {
 }
 
 // weights of every index of one direction from the device faces x[ncell+1]
-static pg_status recon_weights(int geom, const double* dev_x, int ncell, double* w, cudaStream_t s) {
+pg_status recon_weights(int geom, const double* dev_x, int ncell, double* w, cudaStream_t s) {
     for (int k = 0; k < 6 * ncell; ++k) w[k] = 0.0;
     if (ncell < 6) return PG_OK;  // no cell has the 6 faces of a 4-cell fit (1D tube: y)
     double* terms = nullptr;
@@ -296,6 +345,25 @@ static pg_status make_map(CUtensorMap* m, const void* base, uint64_t inner, uint
     cuuint32_t box[2] = {box_inner, box_rows};
     cuuint32_t es[2] = {1, 1};
     CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<void*>(base), dims, strides, box, es,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(PG_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+    return PG_OK;
+}
+
+// A 3D FP64 tensor map: dims {d0, d1, d2} elements (d0 innermost, contiguous),
+// box {b0, b1, b2}.
+pg_status make_map3_f64(CUtensorMap* m, const void* base, uint64_t d0, uint64_t d1, uint64_t d2, uint32_t b0,
+                        uint32_t b1, uint32_t b2) {
+    EncodeTiledFn fn = encode_fn();
+    if (!fn) return fail(PG_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
+    if (reinterpret_cast<uintptr_t>(base) % 16 != 0 || (d0 * 8) % 16 != 0)
+        return fail(PG_ERR_CONFIG, "state rows must be 16-byte aligned (even xres)");
+    cuuint64_t dims[3] = {d0, d1, d2};
+    cuuint64_t strides[2] = {d0 * 8, d0 * d1 * 8};
+    cuuint32_t box[3] = {b0, b1, b2};
+    cuuint32_t es[3] = {1, 1, 1};
+    CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, const_cast<void*>(base), dims, strides, box, es,
                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) return fail(PG_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
@@ -460,8 +528,8 @@ static pg_status engine_setup(Engine& E, const double* dev_xa, const double* dev
     const int ypad = P.ndim > 1 ? NPAD : 0;
     const int yarr = P.yres + 2 * ypad;
     std::vector<double> xa(xarr + 1), xv(xarr), ya(yarr + 1), yv(yarr);
-    make_grid(xa.data(), xv.data(), P.xmin, P.xmax, P.xres, NPAD, P.geomx, P.gridx);
-    make_grid(ya.data(), yv.data(), P.ymin, P.ymax, P.yres, ypad, P.geomy, P.gridy);
+    make_grid(xa.data(), xv.data(), P.xmin, P.xmax, P.xres, NPAD, P.geomx, P.gridx, &P);
+    make_grid(ya.data(), yv.data(), P.ymin, P.ymax, P.yres, ypad, P.geomy, P.gridy, &P);
     if (!dev_xa) {
         PG_CUDA(cudaMalloc(&E.grid, sizeof(double) * (2 * xarr + 2 * yarr + 2)));
         double* g = E.grid;
@@ -837,8 +905,8 @@ pg_status pg_make_grid(const pg_params* P, double* xa, double* xv, double* ya, d
     if (s != PG_OK) return s;
     if (!xa || !xv || !ya || !yv) return fail(PG_ERR_ARG, "null output");
     const int ypad = P->ndim > 1 ? NPAD : 0;
-    make_grid(xa, xv, P->xmin, P->xmax, P->xres, NPAD, P->geomx, P->gridx);
-    make_grid(ya, yv, P->ymin, P->ymax, P->yres, ypad, P->geomy, P->gridy);
+    make_grid(xa, xv, P->xmin, P->xmax, P->xres, NPAD, P->geomx, P->gridx, P);
+    make_grid(ya, yv, P->ymin, P->ymax, P->yres, ypad, P->geomy, P->gridy, P);
     return PG_OK;
 }
 
@@ -1512,8 +1580,8 @@ pg_status pg_recon_weights(const pg_params* P, int dir, double* w) {
     const int ypad = P->ndim > 1 ? NPAD : 0;
     const int n = dir == 0 ? P->xres + 2 * NPAD : P->yres + 2 * ypad;
     std::vector<double> a(n + 1), v(n);
-    if (dir == 0) make_grid(a.data(), v.data(), P->xmin, P->xmax, P->xres, NPAD, P->geomx, P->gridx);
-    else make_grid(a.data(), v.data(), P->ymin, P->ymax, P->yres, ypad, P->geomy, P->gridy);
+    if (dir == 0) make_grid(a.data(), v.data(), P->xmin, P->xmax, P->xres, NPAD, P->geomx, P->gridx, P);
+    else make_grid(a.data(), v.data(), P->ymin, P->ymax, P->yres, ypad, P->geomy, P->gridy, P);
     double* dev = nullptr;
     PG_CUDA(cudaMalloc(&dev, sizeof(double) * (n + 1)));
     cudaError_t e = cudaMemcpy(dev, a.data(), sizeof(double) * (n + 1), cudaMemcpyHostToDevice);

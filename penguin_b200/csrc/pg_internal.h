@@ -55,6 +55,13 @@ struct StepRecord {
     int* inc;           // orbital-advection shift per radius (xarr)
 };
 
+// grid, slope weights and tensor maps (pg_engine.cu)
+void make_grid(double* a, double* v, double amin, double amax, int res, int pad, int geom, int grid,
+               const pg_params* P);
+pg_status recon_weights(int geom, const double* dev_x, int ncell, double* w, cudaStream_t s);
+pg_status make_map3_f64(CUtensorMap* m, const void* base, uint64_t d0, uint64_t d1, uint64_t d2, uint32_t b0,
+                        uint32_t b1, uint32_t b2);
+
 // launch helpers (pg_kernels.cu)
 void launch_init_tables(const DiskView& d, const pg_params& P, double* tab_base, cudaStream_t s);
 void launch_init_xghosts(const DiskView& d, Cell* buf, cudaStream_t s);

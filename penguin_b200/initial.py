@@ -84,3 +84,56 @@ def sod_state(p: Params, x0: float = 0.5, left=(1.0, 0.0, 1.0), right=(0.125, 0.
 
 def orbit_time(orbits: float) -> float:
     return orbits * 2.0 * math.pi
+
+
+# --------------------------------------------------------------------- 3D
+def _centres(a):
+    return 0.5 * (a[4:-3] + a[3:-4])
+
+
+def spherical_state(p: Params, seed: int = 1234, noise: float = 1.0e-4, vnoise: float = 0.0) -> dict:
+    """The spherical disk of init_flag 3 (src/init/init.cu:7-71, 90-91, 157-158,
+    269-274): Sigma ~ (r sin(theta))^-p_alpha in vertical hydrostatic balance,
+    p = cs^2 rho, pressure-corrected Keplerian v_phi; density times
+    1 + noise U(-1,1) and, with ``vnoise``, radial and polar velocities of
+    vnoise c_s U(-1,1).  Arrays (zres, yres, xres)."""
+    from .params import axes_np
+
+    (xa, _), _, (za, _) = axes_np(p)
+    x = _centres(xa)[None, None, :]
+    z = _centres(za)[:, None, None]
+    coeff = p.sc_h * p.sc_h * (1.0 / p.planet_radius)
+
+    def cs2(xx, zz):
+        return coeff * np.power(xx * np.sin(zz) / p.planet_radius, -p.p_beta)
+
+    def rho(xx, zz):
+        r = xx * np.sin(zz)
+        return np.power(r / p.planet_radius, -p.p_alpha) * np.exp((1.0 / xx - 1.0 / r) / cs2(xx, zz))
+
+    def pres(xx, zz):
+        return cs2(xx, zz) * rho(xx, zz)
+
+    dr = 1.1514178e-7
+    v0 = np.sqrt(1.0 / x + (x / rho(x, z)) * (pres(x + dr, z) - pres(x - dr, z)) / (2.0 * dr))
+    shape = (p.zres, p.yres, p.xres)
+    u = splitmix64_uniform(seed, 3 * p.cells).reshape((3,) + shape)
+    r = rho(x, z) * (1.0 + noise * u[0])
+    c2 = np.broadcast_to(cs2(x, z), shape)
+    cs = np.sqrt(c2)
+    return {"r": r, "p": c2 * r, "u": vnoise * cs * u[1], "v": np.broadcast_to(v0, shape).copy(),
+            "w": vnoise * cs * u[2]}
+
+
+def box_state(p: Params, seed: int = 4321) -> dict:
+    """A cartesian box state with structure at every scale: density 1 + 0.2 U,
+    pressure 1 + 0.2 U plus a Gaussian overpressure of 2 at (0.3, 0.6, 0.2),
+    velocities 0.1 U per component.  Arrays (zres, yres, xres)."""
+    from .params import axes_np
+
+    (xa, _), (ya, _), (za, _) = axes_np(p)
+    x, y, z = _centres(xa)[None, None, :], _centres(ya)[None, :, None], _centres(za)[:, None, None]
+    shape = (p.zres, p.yres, p.xres)
+    u = splitmix64_uniform(seed, 5 * p.cells).reshape((5,) + shape)
+    blob = 2.0 * np.exp(-((x - 0.3) ** 2 + (y - 0.6) ** 2 + (z - 0.2) ** 2) / 0.02)
+    return {"r": 1.0 + 0.2 * u[0], "p": 1.0 + 0.2 * u[1] + blob, "u": 0.1 * u[2], "v": 0.1 * u[3], "w": 0.1 * u[4]}

@@ -1,8 +1,9 @@
 """Snapshot files in the reference's checkpoint format.
 
 Layout (src/output/output.cu:125-180, parsed by read/read_penguin.py:136-202):
-``[t][xa: xres+1][ya: yres+1 if ndim>1][rho][p][u][v if ndim>1]``, all float64,
-each field xres*yres values with x fastest.  File names follow
+``[t][xa: xres+1][ya: yres+1 if ndim>1][za: zres+1 if ndim>2][rho][p][u]
+[v if ndim>1][w if ndim>2]``, all float64, each field xres*yres(*zres) values
+with x fastest, then y, then z.  File names follow
 ``binary_<label>_<5-digit frame>`` (output.cu:14-92, util.cu:25-36).
 The same file restarts a run (load_grid reads t and the fields, skipping faces).
 """
@@ -11,32 +12,39 @@ from __future__ import annotations
 import numpy as np
 
 
-def write_snapshot(path: str, t: float, xa: np.ndarray, ya: np.ndarray | None, fields: dict, ndim: int) -> None:
+def write_snapshot(path: str, t: float, xa: np.ndarray, ya: np.ndarray | None, fields: dict, ndim: int,
+                   za: np.ndarray | None = None) -> None:
     parts = [np.array([t], dtype=np.float64), np.asarray(xa, dtype=np.float64)]
     if ndim > 1:
         parts.append(np.asarray(ya, dtype=np.float64))
-    names = ["r", "p", "u"] + (["v"] if ndim > 1 else [])
+    if ndim > 2:
+        parts.append(np.asarray(za, dtype=np.float64))
+    names = ["r", "p", "u"] + (["v"] if ndim > 1 else []) + (["w"] if ndim > 2 else [])
     for k in names:
         parts.append(np.ascontiguousarray(fields[k], dtype=np.float64).ravel())
     np.concatenate(parts).tofile(path)
 
 
-def read_snapshot(path: str, xres: int, yres: int, ndim: int, dust: bool = False) -> dict:
+def read_snapshot(path: str, xres: int, yres: int, ndim: int, dust: bool = False, zres: int = 1) -> dict:
+    """Fields come back as (yres, xres) arrays, (zres, yres, xres) when ndim is 3."""
     dat = np.fromfile(path, dtype=np.float64)
     o = 0
     t = float(dat[o]); o += 1
     xa = dat[o:o + xres + 1]; o += xres + 1
-    ya = None
+    ya = za = None
     if ndim > 1:
         ya = dat[o:o + yres + 1]; o += yres + 1
-    n = xres * yres
-    out = {"t": t, "xa": xa, "ya": ya}
-    for k in ["r", "p", "u"] + (["v"] if ndim > 1 else []):
-        out[k] = dat[o:o + n].reshape(yres, xres)
+    if ndim > 2:
+        za = dat[o:o + zres + 1]; o += zres + 1
+    shape = (zres, yres, xres) if ndim > 2 else (yres, xres)
+    n = xres * yres * (zres if ndim > 2 else 1)
+    out = {"t": t, "xa": xa, "ya": ya, "za": za}
+    for k in ["r", "p", "u"] + (["v"] if ndim > 1 else []) + (["w"] if ndim > 2 else []):
+        out[k] = dat[o:o + n].reshape(shape)
         o += n
     if dust:  # dust_flag builds append the dust r, u (and v, w in 2D), src/output/output.cu:159-176
         for k in ["dust_r", "dust_u"] + (["dust_v", "dust_w"] if ndim > 1 else []):
-            out[k] = dat[o:o + n].reshape(yres, xres)
+            out[k] = dat[o:o + n].reshape(shape)
             o += n
     if o != dat.size:
         raise ValueError(f"{path}: {dat.size} values, expected {o}")
@@ -64,8 +72,10 @@ def label(p) -> str:
 
     if p.ndim == 1:
         s = _i(p.xres)
-    else:
+    elif p.ndim == 2:
         s = f"{_i(p.xres)}x{_i(p.yres)}"
+    else:
+        s = f"{_i(p.xres)}x{_i(p.yres)}x{_i(p.zres)}"
     s += "_h" + _i(1000.0 * p.sc_h)
     if p.n_planet > 0:
         if p.planet_mass >= JUPITER_MASS:

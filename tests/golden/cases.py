@@ -209,10 +209,58 @@ def timing_cases() -> list[dict]:
     ]
 
 
+def cases3d() -> list[dict]:
+    """3D configurations (ndim 3): the reference's spherical preset
+    (include/para_files/Adiabatic_CPD.h) at 32x64x16, adiabatic with wave damping,
+    analytic radial ghosts and reflecting polar boundaries, and an isothermal
+    variant with zero-gradient / reflecting radial ends and a zero-gradient upper
+    polar boundary, both restarted after one orbit (planet at full mass) with
+    seeded noise in density and in the radial and polar velocities; and a
+    cartesian box (32x32x16) with structure at every scale.  The fixtures hold
+    only the output fields (the initial states are regenerated from the seeds).
+
+    The preset's grids put 6e-4 wide cells at r = 1 and phi = pi, and there the
+    reference's arithmetic amplifies rounding by x / dx and more (its 4th-order
+    moments (x1^4 - x0^4) / (x1^3 - x0^3), src/solver/recon/recon.cu:242-301,
+    and x_l + u dt in the characteristic states, src/solver/riemann/states.cu:
+    27-60): the same unmodified sources compiled with -fmad=false run 3.4e-10
+    from the default build after 10 steps (floors.json "fma_floor", made by
+    make_golden.py's fmafloor phase).  The oracle, which evaluates the
+    reference's expressions without FMA contraction, sits at that same 3.4e-10
+    (tol) and the CUDA path at 3.6e-12 (cuda_tol 5e-12, 1.5 % of that floor;
+    one step: 1.7e-13 after the radial sweep, confined to the fine cells).  On
+    the cartesian box (uniform grid) the two builds agree to 5e-16 and the CUDA
+    path to 5e-16 (6e-15 in momentum).  The reference is deterministic and its one-ulp density
+    floor is 5e-15 (floors.json "floor")."""
+    sph = P.spherical_disk(32, 64, 16)
+    iso = sph.replace(EOS_flag=0, gam=1.0, kill_flag=0, bound_lft=1, bound_rgh=2, bound_top=1)
+    return [
+        dict(name="sph32_n10", params=sph, init="sph", seed=SEED, t0=2.0 * math.pi, max_step=10,
+             end_time=1.0e30, tol=1e-9, cuda_tol=5e-12, z_zdiv=16),
+        dict(name="sph32_iso_n10", params=iso, init="sph", seed=SEED, t0=2.0 * math.pi, max_step=10,
+             end_time=1.0e30, tol=1e-9, cuda_tol=5e-12, z_zdiv=16),
+        dict(name="box32_n10", params=P.cartesian_box(32, 32, 16), init="box", seed=SEED, t0=0.0, max_step=10,
+             end_time=1.0e30, tol=3e-14, cuda_tol=1e-14, z_zdiv=16),
+    ]
+
+
+def size_cases3d() -> list[dict]:
+    """The reference's 3D preset at its own size (384x768x216, 63.7 M cells),
+    restarted after one orbit from the seeded spherical disk, 3 steps: the
+    reference (default build and -fmad=false build) runs at test time on the
+    GPU and the CUDA path is compared with it there."""
+    return [dict(name="size_sph384_n3", params=P.spherical_disk(), init="sph", seed=1234, t0=2.0 * math.pi,
+                 max_step=3, end_time=1.0e30, z_zdiv=24)]
+
+
 def initial_state(case: dict) -> dict:
     from penguin_b200 import initial as I
 
     p = case["params"]
+    if case["init"] == "sph":
+        return I.spherical_state(p, seed=case.get("seed", SEED), vnoise=1.0e-3)
+    if case["init"] == "box":
+        return I.box_state(p, seed=case.get("seed", SEED))
     if case["init"] == "sod":
         return I.sod_state(p)
     st = I.disk_state(p, seed=case.get("seed", SEED))
