@@ -538,6 +538,66 @@ def two_level_slope(x, y):
     return {"slope": float(b), "jump": float(J), "levels": [int((z == 0).sum()), int((z == 1).sum())]}
 
 
+def measure_sph3d(local, stream, steps, pk, size=None):
+    """The reference's 3D preset (include/para_files/Adiabatic_CPD.h: spherical r,
+    phi, theta, 384x768x216 = 63.7 M cells, adiabatic, planet q 3e-5, wave
+    damping) from the seeded disk after one orbit: zone-updates/s of the
+    device-resident loop over ``steps`` steps, each pass's device time, and the
+    slowest sweep against its HBM and FP64-issue rooflines."""
+    import numpy as np
+    import torch
+
+    from penguin_b200 import initial as I
+    from penguin_b200 import params as P
+    from penguin_b200.disk3 import Disk3
+
+    p = P.spherical_disk(*size) if size else P.spherical_disk()
+    st = I.spherical_state(p, seed=1234, vnoise=1.0e-3)
+    d = Disk3(p, device=local, stream=stream.cuda_stream)
+    d.set_state(2.0 * np.pi, st)
+    d.run(3)
+    d.check()
+    passes = d.pass_times(max(2, min(10, steps)))
+    K = max(2, min(20, steps))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    d.run(K)
+    e1.record(stream)
+    e1.synchronize()
+    d.check()
+    ms = e0.elapsed_time(e1) / K
+    d.close()
+    cells = p.cells
+    sweep = max(("sweep_x", "sweep_y", "sweep_z"), key=lambda k: passes[k])
+    achieved = 80.0 * cells / (passes[sweep] / 1000.0) / 1e9
+    out = {"workload": f"3D spherical preset {p.xres}x{p.yres}x{p.zres} (Adiabatic_CPD.h), FP64, "
+                       "seeded disk after one orbit", "cells": cells, "steps": K,
+           "value": cells / (ms / 1000.0), "unit": UNIT, "ms_per_step": ms, "pass_ms": passes,
+           "roofline": {"bound": "hbm", "kernel": sweep, "achieved": achieved, "peak": pk["hbm_gbs"],
+                        "unit": "GB/s", "frac": achieved / pk["hbm_gbs"], "algorithmic_bytes_per_cell": 80,
+                        "peak_source": pk["source"], "traffic": None}}
+    tfile = os.path.join(ROOT, "profiles", "traffic.txt")
+    if os.path.exists(tfile):  # per-cell DRAM bytes of a smaller capture, scaled to this grid
+        for fl in open(tfile):
+            f = fl.split()
+            if len(f) >= 2 and not fl.startswith("#") and f[0] == f"sph3d_{sweep}_per_cell":
+                out["roofline"]["traffic"] = float(f[1]) * cells
+                out["roofline"]["traffic_note"] = "per-cell bytes of the 192x384x96 capture x cells"
+    ffile = os.path.join(ROOT, "profiles", "fp64_per_cell.txt")
+    if os.path.exists(ffile):
+        for fl in open(ffile):
+            f = fl.split()
+            if len(f) >= 2 and not fl.startswith("#") and f[0] == "sph3d_" + sweep:
+                nsm = torch.cuda.get_device_properties(local).multi_processor_count
+                peak64 = 64.0 * nsm * 1965.0e6
+                ach = float(f[1]) * cells / (passes[sweep] / 1000.0)
+                out["roofline_fp64"] = {"kernel": sweep, "achieved": ach, "peak": peak64,
+                                        "unit": "FP64 thread-instructions/s", "frac": ach / peak64,
+                                        "instructions_per_cell": float(f[1])}
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -554,9 +614,11 @@ def main():
     ap.add_argument("--tuning", default=None,
                     help="a fixed launch configuration instead of the autotuner's: comma list of "
                          "key=value over Disk.TUNING (v_sweep_x, ..., cps_kick2)")
-    ap.add_argument("--forms", default="fp32,ensemble,dust,adjoint",
+    ap.add_argument("--forms", default="fp32,ensemble,dust,adjoint,sph3d",
                     help="comma list of the extra measurements after the FP64 headline "
-                         "(fp32, ensemble, dust, adjoint)")
+                         "(fp32, ensemble, dust, adjoint, sph3d)")
+    ap.add_argument("--sph3d-size", default=None,
+                    help="NR,NPHI,NTHETA of the 3D leg instead of the preset's 384,768,216 (profiling)")
     args = ap.parse_args()
 
     if args.impl == "reference":
@@ -717,6 +779,9 @@ def main():
         # ADJOINT_STEPS steps and the timing over ADJOINT_TIMING_STEPS (16
         # checkpoint segments); together well under a second of GPU time
         line["adjoint"] = measure_adjoint(args.adjoint_steps, local, stream, args.adjoint_timing_steps)
+    if "sph3d" in forms:
+        size = tuple(int(x) for x in args.sph3d_size.split(",")) if args.sph3d_size else None
+        line["sph3d"] = measure_sph3d(local, stream, K, pk, size)
     if job.printer and world == 1 and not args.no_cpu_baseline:
         cb, orc, n_orc = cpu_baseline(p, state, 0.0, keep=True)
         line["cpu_baseline"] = cb
@@ -781,6 +846,8 @@ def summary_of(line):
                                                               for v in a["fd_theta_scan"]["per_parameter"]],
                                      "theta_smooth_two_level_1e-6": [
                                          v["rel_err_two_level"] for v in a["fd_theta_scan_smooth"]["per_parameter"]]}
+    if "sph3d" in line:
+        out["sph3d_gzone_s"] = line["sph3d"]["value"] / 1e9
     if "parity" in line:
         q = line["parity"]
         out["parity_rel_l1_max"] = max(q["rel_l1_r"], q["rel_l1_p"], q["rel_l1_mom"])

@@ -26,6 +26,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <vector>
 
 #include "pg_common.cuh"
@@ -542,6 +543,24 @@ __global__ void k3_extract(const View3 v, const Cell* in, double* r, double* p, 
     }
 }
 
+// The bound-0 radial and polar ghosts of a caller's buffer: init_C as the device
+// evaluates it (boundary.cu:30-33, 56-59, 293-294, 315-316); never rewritten.
+__global__ void k3_analytic_ghosts(const View3 v, Cell* buf) {
+    const DiskView& d = v.d;
+    const long long n = (long long)d.xarr * d.yarr * v.zarr;
+    for (long long m = (long long)blockIdx.x * blockDim.x + threadIdx.x; m < n; m += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(m % d.xarr);
+        const long long rest = m / d.xarr;
+        const int j = (int)(rest % d.yarr);
+        const int k = (int)(rest / d.yarr);
+        const bool gx = (i < NPAD && d.bound_lft == 0) || (i >= NPAD + d.xres && d.bound_rgh == 0);
+        const bool gz = (k < NPAD && v.bound_bom == 0) || (k >= NPAD + v.zres && v.bound_top == 0);
+        if (!gx && !gz) continue;
+        const double* I = v.initc + 5 * ((size_t)i + (size_t)d.xarr * k);
+        put3(buf, v, i, j, k, Cell{I[0], I[1], I[2], I[3], I[4]});
+    }
+}
+
 // ================================================================ tables
 // Evaluated on the device with its own sin / cos / tan / pow / exp / sqrt, as
 // the reference evaluates them in its kernels.
@@ -646,7 +665,10 @@ struct Engine3 {
     bool own_stream = false;
     View3 v{};
     Cell* buf[2] = {nullptr, nullptr};
+    bool own_buffers = true;  // false: the caller's Grid buffers (pg_grid_*)
     CUtensorMap maps[2][3];  // per buffer: radial, azimuthal, polar boxes
+    const void* map_base[2] = {nullptr, nullptr};
+    std::vector<const void*> ghosted;  // caller buffers whose bound-0 ghosts hold the device init_C
     double* tables = nullptr;
     double* stage = nullptr;
     size_t stage_n = 0;
@@ -721,6 +743,7 @@ static pg_status make_maps(Engine3& E, int b) {
     if ((s = make_map3_f64(&E.maps[b][0], E.buf[b], d0, d1, d2, 5 * S3_TL, S3_W, 1)) != PG_OK) return s;
     if ((s = make_map3_f64(&E.maps[b][1], E.buf[b], d0, d1, d2, 5 * S3_COLS, S3_TL, 1)) != PG_OK) return s;
     if ((s = make_map3_f64(&E.maps[b][2], E.buf[b], d0, d1, d2, 5 * S3_COLS, 1, S3_TL)) != PG_OK) return s;
+    E.map_base[b] = E.buf[b];
     return PG_OK;
 }
 
@@ -763,7 +786,7 @@ static void release3(Engine3* E) {
     if (!E) return;
     for (int b = 0; b < 2; ++b) {
         if (E->graph[b]) cudaGraphExecDestroy(E->graph[b]);
-        if (E->buf[b]) cudaFree(E->buf[b]);
+        if (E->buf[b] && E->own_buffers) cudaFree(E->buf[b]);
     }
     if (E->tables) cudaFree(E->tables);
     if (E->stage) cudaFree(E->stage);
@@ -772,7 +795,7 @@ static void release3(Engine3* E) {
     delete E;
 }
 
-static pg_status create3(const pg_params* P, int device, cudaStream_t stream, Engine3** out) {
+static pg_status create3(const pg_params* P, int device, cudaStream_t stream, Engine3** out, bool own = true) {
     pg_status s = check3(P);
     if (s != PG_OK) return s;
     PG3_CUDA(cudaSetDevice(device));
@@ -813,7 +836,8 @@ static pg_status create3(const pg_params* P, int device, cudaStream_t stream, En
         cudaMalloc(&E->sc, sizeof(Scalars)) != cudaSuccess)
         return bad(fail3(PG_ERR_CUDA, "table allocation failed"));
     const size_t ncell = (size_t)xarr * yarr * zarr;
-    for (int b = 0; b < 2; ++b)
+    E->own_buffers = own;
+    for (int b = 0; own && b < 2; ++b)
         if (cudaMalloc(&E->buf[b], ncell * sizeof(Cell)) != cudaSuccess)
             return bad(fail3(PG_ERR_CUDA, "state allocation failed (%zu cells)", ncell));
     cudaMemsetAsync(E->sc, 0, sizeof(Scalars), E->stream);
@@ -929,7 +953,7 @@ static pg_status create3(const pg_params* P, int device, cudaStream_t stream, En
                                                                       gfz, radx, idx_x, killx, ycj, idx_y, cs2, initc);
     if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(E->stream) != cudaSuccess)
         return bad(fail3(PG_ERR_CUDA, "table kernel failed"));
-    for (int b = 0; b < 2; ++b)
+    for (int b = 0; own && b < 2; ++b)
         if ((s = make_maps(*E, b)) != PG_OK) return bad(s);
     cudaFuncSetAttribute(k3_sweep<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S3_SMEM);
     cudaFuncSetAttribute(k3_sweep<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S3_SMEM);
@@ -947,6 +971,94 @@ static pg_status create3(const pg_params* P, int device, cudaStream_t stream, En
     E->grid_kick = occupancy_grid((const void*)k3_kick<2>, K3_THREADS, 0, (ncin + K3_THREADS - 1) / K3_THREADS);
     *out = E;
     return PG_OK;
+}
+
+// ------------------------------------------------------- drop-in (Grid)
+// pg_grid_* with ndim 3: the engine's tables for the caller's grid, keyed by
+// its device xa; the state lives in the caller's C and T.
+static std::map<const double*, Engine3*> g_grids3;
+
+pg_status check_params3(const pg_params* P) { return check3(P); }
+
+static pg_status grid3_engine(const pg_params& P, pg_grid* dev, Engine3** out) {
+    if (!dev) return fail3(PG_ERR_ARG, "null grid");
+    if (dev->xres != P.xres || dev->yres != P.yres || dev->zres != P.zres)
+        return fail3(PG_ERR_CONFIG, "grid dimensions differ from the configured parameters");
+    if (dev->xbgn != 0) return fail3(PG_ERR_CONFIG, "radial domain decomposition is not supported");
+    auto it = g_grids3.find(dev->xa);
+    if (it != g_grids3.end()) {
+        *out = it->second;
+        return PG_OK;
+    }
+    int device = 0;
+    PG3_CUDA(cudaGetDevice(&device));
+    Engine3* E = nullptr;
+    pg_status s = create3(&P, device, (cudaStream_t)dev->stream, &E, false);
+    if (s != PG_OK) return s;
+    g_grids3[dev->xa] = E;
+    *out = E;
+    return PG_OK;
+}
+
+pg_status grid3_init_orbadv(const pg_params& P, pg_grid* dev) {
+    Engine3* E = nullptr;
+    pg_status s = grid3_engine(P, dev, &E);
+    if (s != PG_OK) return s;
+    // init_OrbAdv (src/orbit/orbit.cu:51-72) without OrbAdv_flag: orb_rot 0, orb_shf 0
+    const size_t nxz = (size_t)dev->xarr * dev->zarr;
+    if (dev->orb_rot) PG3_CUDA(cudaMemsetAsync(dev->orb_rot, 0, sizeof(double) * nxz, E->stream));
+    if (dev->orb_shf) PG3_CUDA(cudaMemsetAsync(dev->orb_shf, 0, sizeof(int) * nxz, E->stream));
+    PG3_CUDA(cudaStreamSynchronize(E->stream));
+    return PG_OK;
+}
+
+pg_status grid3_global_dt(const pg_params& P, pg_grid* dev, double dt_prev, double* dt_out) {
+    Engine3* E = nullptr;
+    pg_status s = grid3_engine(P, dev, &E);
+    if (s != PG_OK) return s;
+    PG3_CUDA(cudaMemsetAsync(&E->sc->vmax_bits, 0, sizeof(unsigned long long), E->stream));
+    k3_cfl<<<E->grid_kick, K3_THREADS, 0, E->stream>>>(E->v, reinterpret_cast<const Cell*>(dev->C));
+    PG3_CUDA(cudaGetLastError());
+    unsigned long long bits = 0;
+    PG3_CUDA(cudaMemcpyAsync(&bits, &E->sc->vmax_bits, sizeof(bits), cudaMemcpyDeviceToHost, E->stream));
+    PG3_CUDA(cudaStreamSynchronize(E->stream));
+    double vmax;
+    std::memcpy(&vmax, &bits, sizeof vmax);
+    const double dt = E->P.cfl / vmax;  // get_dt_lv2 (timestep.cu:108)
+    double tmp = dt_prev * 1.1;         // timestep.cu:133-139
+    if (dt < tmp) tmp = dt;
+    *dt_out = tmp;
+    return PG_OK;
+}
+
+pg_status grid3_solve(const pg_params& P, pg_grid* dev, double time, double dt) {
+    Engine3* E = nullptr;
+    pg_status s = grid3_engine(P, dev, &E);
+    if (s != PG_OK) return s;
+    E->buf[0] = reinterpret_cast<Cell*>(dev->C);
+    E->buf[1] = reinterpret_cast<Cell*>(dev->T);
+    for (int b = 0; b < 2; ++b) {
+        if (E->map_base[b] != E->buf[b] && (s = make_maps(*E, b)) != PG_OK) return s;
+        if (std::find(E->ghosted.begin(), E->ghosted.end(), E->buf[b]) == E->ghosted.end()) {
+            k3_analytic_ghosts<<<1184, 256, 0, E->stream>>>(E->v, E->buf[b]);
+            E->ghosted.push_back(E->buf[b]);
+        }
+    }
+    if (E->v.d.nplanet > 0 && dev->planets) k_grid_planet_in<<<1, 1, 0, E->stream>>>(E->sc, dev->planets, 0);
+    launch_set_time(E->v.d, time, dt, E->stream);
+    enqueue_passes(*E, 0);
+    if (E->v.d.nplanet > 0 && dev->planets) k_grid_planet_out<<<1, 1, 0, E->stream>>>(E->sc, dev->planets, 0);
+    PG3_CUDA(cudaGetLastError());
+    // the newest state is in T: swap like the reference (src/solver/sweeps.cu:353-355, 550-552)
+    pg_cell* t = dev->C;
+    dev->C = dev->T;
+    dev->T = t;
+    return PG_OK;
+}
+
+void grid3_release() {
+    for (auto& kv : g_grids3) release3(kv.second);
+    g_grids3.clear();
 }
 
 // Device-clocked steps from here on run towards end_time (main.cu:322-339).

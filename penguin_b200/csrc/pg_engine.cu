@@ -898,7 +898,10 @@ extern "C" {
 const char* pg_version(void) { return "penguin_b200 0.1 (sm_100a, FP64 Godunov step)"; }
 const char* pg_last_error(void) { return g_err.c_str(); }
 
-pg_status pg_check_params(const pg_params* P) { return check_params(P); }
+pg_status pg_check_params(const pg_params* P) {
+    if (P && P->ndim == 3) return check_params3(P);
+    return check_params(P);
+}
 
 pg_status pg_make_grid(const pg_params* P, double* xa, double* xv, double* ya, double* yv) {
     pg_status s = check_params(P);
@@ -1704,7 +1707,7 @@ static bool g_configured = false;
 static std::map<const double*, Engine*> g_grids;  // keyed by the caller's device xa
 
 pg_status pg_configure(const pg_params* P) {
-    pg_status s = check_params(P);
+    pg_status s = (P && P->ndim == 3) ? check_params3(P) : check_params(P);
     if (s != PG_OK) return s;
     std::lock_guard<std::mutex> lk(g_mu);
     g_params = *P;
@@ -1743,6 +1746,10 @@ static pg_status grid_engine(pg_grid* dev, Engine** out) {
 }
 
 pg_status pg_grid_init_orbadv(pg_grid* dev) {
+    if (g_configured && g_params.ndim == 3) {
+        std::lock_guard<std::mutex> lk(g_mu);
+        return grid3_init_orbadv(g_params, dev);
+    }
     Engine* E = nullptr;
     pg_status s = grid_engine(dev, &E);
     if (s != PG_OK) return s;
@@ -1755,6 +1762,10 @@ pg_status pg_grid_init_orbadv(pg_grid* dev) {
 pg_status pg_grid_global_dt(pg_grid* hst, pg_grid* dev, double dt_prev, double* dt_out) {
     (void)hst;
     if (!dt_out) return fail(PG_ERR_ARG, "null dt_out");
+    if (g_configured && g_params.ndim == 3) {
+        std::lock_guard<std::mutex> lk(g_mu);
+        return grid3_global_dt(g_params, dev, dt_prev, dt_out);
+    }
     Engine* E = nullptr;
     pg_status s = grid_engine(dev, &E);
     if (s != PG_OK) return s;
@@ -1765,6 +1776,10 @@ pg_status pg_grid_global_dt(pg_grid* hst, pg_grid* dev, double dt_prev, double* 
 }
 
 pg_status pg_grid_solve(pg_grid* dev, double time, double dt) {
+    if (g_configured && g_params.ndim == 3) {
+        std::lock_guard<std::mutex> lk(g_mu);
+        return grid3_solve(g_params, dev, time, dt);
+    }
     Engine* E = nullptr;
     pg_status s = grid_engine(dev, &E);
     if (s != PG_OK) return s;
@@ -1812,6 +1827,7 @@ pg_status pg_grid_release(void) {
     std::lock_guard<std::mutex> lk(g_mu);
     for (auto& kv : g_grids) delete kv.second;
     g_grids.clear();
+    grid3_release();
     return PG_OK;
 }
 

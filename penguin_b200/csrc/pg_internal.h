@@ -62,6 +62,16 @@ pg_status recon_weights(int geom, const double* dev_x, int ncell, double* w, cud
 pg_status make_map3_f64(CUtensorMap* m, const void* base, uint64_t d0, uint64_t d1, uint64_t d2, uint32_t b0,
                         uint32_t b1, uint32_t b2);
 
+// the caller's planets array in and out of the device scalars (pg_engine.cu)
+__global__ void k_grid_planet_in(Scalars* sc, const pg_body* planets, int twobd);
+__global__ void k_grid_planet_out(const Scalars* sc, pg_body* planets, int twobd);
+// the drop-in entry points with ndim 3 (pg_3d.cu)
+pg_status check_params3(const pg_params* P);
+pg_status grid3_init_orbadv(const pg_params& P, pg_grid* dev);
+pg_status grid3_global_dt(const pg_params& P, pg_grid* dev, double dt_prev, double* dt_out);
+pg_status grid3_solve(const pg_params& P, pg_grid* dev, double time, double dt);
+void grid3_release();
+
 // launch helpers (pg_kernels.cu)
 void launch_init_tables(const DiskView& d, const pg_params& P, double* tab_base, cudaStream_t s);
 void launch_init_xghosts(const DiskView& d, Cell* buf, cudaStream_t s);

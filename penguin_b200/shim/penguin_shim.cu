@@ -21,6 +21,7 @@
 static const int pgs_ndim = ndim;
 static const int pgs_geomx = geomx;
 static const int pgs_geomy = geomy;
+static const int pgs_geomz = geomz;
 static const int pgs_eos = EOS_flag;
 static const int pgs_ie = internal_e_flag;
 static const int pgs_init = init_flag;
@@ -119,6 +120,11 @@ static void pg_shim_configure() {
     P.cool_flag = pgs_cool;
     P.beta_cool = beta_cool;
     P.twobd_flag = pgs_twobd;
+    P.zres = zres;
+    P.geomz = pgs_geomz;
+    P.gridz = gridz;
+    P.bound_bom = bound_bom;
+    P.bound_top = bound_top;
     if (pg_configure(&P) != PG_OK) {
         fprintf(stderr, "penguin_b200: %s\n", pg_last_error());
         exit(1);
