@@ -378,6 +378,11 @@ pg_status pg_disk3_check(pg_disk3* d);
 /* nsteps device-clocked steps with CUDA events between the passes: average ms
    of the clock, kick1, sweep_x, sweep_y, sweep_z and kick2 (ms6). */
 pg_status pg_disk3_pass_times(pg_disk3* d, int nsteps, double* ms6);
+/* Checkpoint files in the reference's format (write_check_point / load_grid,
+   src/output/output.cu:125-248, ndim 3): t, the x, y, z faces, then the r, p,
+   u, v, w planes.  read_snapshot restarts from the file at its t. */
+pg_status pg_disk3_write_snapshot(pg_disk3* d, const char* path);
+pg_status pg_disk3_read_snapshot(pg_disk3* d, const char* path, double* t_out);
 /* test support: one step with host t and dt, the whole cell array (ghosts
    included) after each pass into out[5][zarr][yarr][xarr]: kick1, sweep_x,
    sweep_y, sweep_z, kick2 with the damping.  Blocking. */

@@ -35,7 +35,7 @@ EXPORTS = [
     "pg_adj_check_params", "pg_adj_create", "pg_adj_destroy", "pg_adj_set_params", "pg_adj_forward",
     "pg_adj_backward", "pg_adj_model_error", "pg_adj_dot_test", "pg_adj_pass_check", "pg_adj_replay_diff", "pg_adj_pass_fields", "pg_adj_schedule", "pg_adj_steps", "pg_adj_device_bytes", "pg_adj_set_sweep_reverse",
     "pg_disk3_create", "pg_disk3_destroy", "pg_disk3_set_state", "pg_disk3_get_state", "pg_disk3_global_dt",
-    "pg_disk3_solve", "pg_disk3_run", "pg_disk3_clock", "pg_disk3_check", "pg_disk3_pass_times", "pg_disk3_stages", "pg_make_axis",
+    "pg_disk3_solve", "pg_disk3_run", "pg_disk3_clock", "pg_disk3_check", "pg_disk3_pass_times", "pg_disk3_stages", "pg_disk3_write_snapshot", "pg_disk3_read_snapshot", "pg_make_axis",
 ]
 
 
@@ -146,6 +146,8 @@ def lib() -> ctypes.CDLL:
         "pg_disk3_check": (i, [vp]),
         "pg_disk3_pass_times": (i, [vp, i, dp]),
         "pg_disk3_stages": (i, [vp, d, d, dp]),
+        "pg_disk3_write_snapshot": (i, [vp, ctypes.c_char_p]),
+        "pg_disk3_read_snapshot": (i, [vp, ctypes.c_char_p, dp]),
         "pg_make_axis": (i, [PP, i, dp, dp]),
     }
     for name, (res, args) in sig.items():

@@ -669,6 +669,7 @@ struct Engine3 {
     CUtensorMap maps[2][3];  // per buffer: radial, azimuthal, polar boxes
     const void* map_base[2] = {nullptr, nullptr};
     std::vector<const void*> ghosted;  // caller buffers whose bound-0 ghosts hold the device init_C
+    std::vector<double> hxa, hya, hza; // host faces of each axis (ghosts included), for snapshots
     double* tables = nullptr;
     double* stage = nullptr;
     size_t stage_n = 0;
@@ -823,6 +824,9 @@ static pg_status create3(const pg_params* P, int device, cudaStream_t stream, En
     for (double a : xa) if (!std::isfinite(a)) return bad(fail3(PG_ERR_CONFIG, "the radial spacing needs more cells"));
     for (double a : ya) if (!std::isfinite(a)) return bad(fail3(PG_ERR_CONFIG, "the azimuthal spacing needs more cells"));
     for (double a : za) if (!std::isfinite(a)) return bad(fail3(PG_ERR_CONFIG, "the polar spacing needs more cells"));
+    E->hxa = xa;
+    E->hya = ya;
+    E->hza = za;
     // table block: faces and volumes, weights, per-index and (x, z) tables, trig
     const size_t nxz = (size_t)xarr * zarr;
     const size_t ntab = (xarr + 1) + xarr + (yarr + 1) + yarr + (zarr + 1) + zarr   // grid
@@ -1312,6 +1316,46 @@ pg_status pg_disk3_pass_times(pg_disk3* dk, int nsteps, double* ms6) {
     for (auto& e : ev) cudaEventDestroy(e);
     for (int k = 0; k < 6; ++k) ms6[k] = acc[k] / nsteps;
     return PG_OK;
+}
+
+// write_check_point (src/output/output.cu:125-180, ndim 3): t, the interior
+// faces of x, y and z, then the r, p, u, v, w planes (x fastest, then y, then z)
+pg_status pg_disk3_write_snapshot(pg_disk3* dk, const char* path) {
+    if (!dk || !path) return fail3(PG_ERR_ARG, "null argument");
+    Engine3& E = *dk->E;
+    const size_t n = (size_t)E.P.xres * E.P.yres * E.P.zres;
+    std::vector<double> h(5 * n);
+    double t = 0.0;
+    pg_status s = pg_disk3_get_state(dk, h.data(), h.data() + n, h.data() + 2 * n, h.data() + 3 * n, h.data() + 4 * n, &t);
+    if (s != PG_OK) return s;
+    FILE* f = std::fopen(path, "wb");
+    if (!f) return fail3(PG_ERR_ARG, "cannot open %s", path);
+    bool ok = std::fwrite(&t, sizeof(double), 1, f) == 1;
+    ok = ok && std::fwrite(&E.hxa[NPAD], sizeof(double), E.P.xres + 1, f) == (size_t)E.P.xres + 1;
+    ok = ok && std::fwrite(&E.hya[NPAD], sizeof(double), E.P.yres + 1, f) == (size_t)E.P.yres + 1;
+    ok = ok && std::fwrite(&E.hza[NPAD], sizeof(double), E.P.zres + 1, f) == (size_t)E.P.zres + 1;
+    ok = ok && std::fwrite(h.data(), sizeof(double), 5 * n, f) == 5 * n;
+    ok = (std::fclose(f) == 0) && ok;
+    return ok ? PG_OK : fail3(PG_ERR_ARG, "short write to %s", path);
+}
+
+// load_grid (src/output/output.cu:182-248, ndim 3): t and the five planes of a
+// checkpoint file (the faces are skipped), then a restart at t like set_state
+pg_status pg_disk3_read_snapshot(pg_disk3* dk, const char* path, double* t_out) {
+    if (!dk || !path) return fail3(PG_ERR_ARG, "null argument");
+    Engine3& E = *dk->E;
+    const size_t n = (size_t)E.P.xres * E.P.yres * E.P.zres;
+    std::vector<double> h(5 * n);
+    double t = 0.0;
+    FILE* f = std::fopen(path, "rb");
+    if (!f) return fail3(PG_ERR_ARG, "cannot open %s", path);
+    bool ok = std::fread(&t, sizeof(double), 1, f) == 1;
+    ok = ok && std::fseek(f, (long)sizeof(double) * (1 + E.P.xres + 1 + E.P.yres + 1 + E.P.zres + 1), SEEK_SET) == 0;
+    ok = ok && std::fread(h.data(), sizeof(double), 5 * n, f) == 5 * n;
+    std::fclose(f);
+    if (!ok) return fail3(PG_ERR_ARG, "%s is not a checkpoint of this grid", path);
+    if (t_out) *t_out = t;
+    return pg_disk3_set_state(dk, t, h.data(), h.data() + n, h.data() + 2 * n, h.data() + 3 * n, h.data() + 4 * n);
 }
 
 // test support: one step with host t and dt (as pg_disk3_solve), copying the

@@ -102,6 +102,18 @@ class Disk3:
         check(lib().pg_disk3_pass_times(self._h, nsteps, ms))
         return {k: float(ms[n]) for n, k in enumerate(self.STAGES)}
 
+    def write_snapshot(self, path: str) -> None:
+        """The newest state in the reference's checkpoint format (ndim 3)."""
+        check(lib().pg_disk3_write_snapshot(self._h, str(path).encode()))
+
+    def read_snapshot(self, path: str) -> float:
+        """Restart from a checkpoint file (t and the five fields, like load_grid)."""
+        t = ctypes.c_double()
+        check(lib().pg_disk3_read_snapshot(self._h, str(path).encode(), ctypes.byref(t)))
+        self.t = t.value
+        self.dt = None
+        return t.value
+
     def stages(self, t: float, dt: float) -> np.ndarray:
         """One step with host t and dt; the cell array (zarr, yarr, xarr, 5) after
         each pass: kick1, sweep_x, sweep_y, sweep_z, kick2 (test support)."""

@@ -158,3 +158,35 @@ def test_cuda_matches_reference_at_preset_size(case, tmp_path):
           f"reference {sps} s/step")
     assert g["t"] == pytest.approx(float(ref["t"]), rel=1e-13)
     assert all(e[k] < 0.05 * floor[k] for k in e), (e, floor)
+
+
+def test_snapshot_round_trip_and_reference_reader_3d(tmp_path):
+    """The library's 3D checkpoint has the reference's layout (penguin_b200.snapshot
+    reads it with the faces of the grid) and restarts the same run bit for bit."""
+    case = C.cases3d()[0]
+    p = case["params"]
+    d = Disk3(p)
+    d.set_state(case["t0"], C.initial_state(case))
+    d.run(3)
+    d.check()
+    path = tmp_path / "binary_3d_00001"
+    d.write_snapshot(str(path))
+    assert os.path.getsize(path) == 8 * (1 + p.xres + 1 + p.yres + 1 + p.zres + 1 + 5 * p.cells)
+    f = S.read_snapshot(str(path), p.xres, p.yres, 3, zres=p.zres)
+    g = d.get_state()
+    (xa, _), (ya, _), (za, _) = P.axes_np(p)
+    assert f["t"] == g["t"]
+    assert np.array_equal(f["xa"], xa[3:3 + p.xres + 1]) and np.array_equal(f["za"], za[3:3 + p.zres + 1])
+    for k in "rpuvw":
+        assert np.array_equal(f[k], g[k]), k
+    e = Disk3(p)
+    assert e.read_snapshot(str(path)) == g["t"]
+    h = Disk3(p)  # the same restart from the arrays
+    h.set_state(g["t"], {k: g[k] for k in "rpuvw"})
+    e.run(2)
+    h.run(2)
+    a, b = h.get_state(), e.get_state()
+    for k in "rpuvw":
+        assert np.array_equal(a[k], b[k]), k
+    for x in (d, e, h):
+        x.close()
