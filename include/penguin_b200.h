@@ -383,6 +383,9 @@ pg_status pg_disk3_pass_times(pg_disk3* d, int nsteps, double* ms6);
    u, v, w planes.  read_snapshot restarts from the file at its t. */
 pg_status pg_disk3_write_snapshot(pg_disk3* d, const char* path);
 pg_status pg_disk3_read_snapshot(pg_disk3* d, const char* path, double* t_out);
+/* test support: out2[2k] = the kernels' division-free x[k] / 1.5, out2[2k+1] =
+   the IEEE quotient, for n host values.  Uses the GPU. */
+pg_status pg_test_div_1p5(const double* x, long long n, double* out2);
 /* test support: one step with host t and dt, the whole cell array (ghosts
    included) after each pass into out[5][zarr][yarr][xarr]: kick1, sweep_x,
    sweep_y, sweep_z, kick2 with the damping.  Blocking. */

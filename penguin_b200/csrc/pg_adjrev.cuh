@@ -278,8 +278,9 @@ __device__ __forceinline__ double flatten_tape(double inv_cs, double p0, double 
     t.dp2f = pp2 - pm1;
     t.dp1b = p0 - pm1;
     t.dp2b = pp1 - pm2;
-    const double Mf = (u0 - up1) * inv_cs;
-    const double Mb = (um1 - u0) * inv_cs;
+    (void)inv_cs;  // the branch of flatten (pg_hydro.cuh): signs of the velocity differences
+    const double Mf = u0 - up1;
+    const double Mb = um1 - u0;
     double f = 0.0;
     t.active = ((Mf > 0.0 || Mb > 0.0) && t.dp2f != 0.0 && t.dp2b != 0.0) ? 1 : 0;
     if (t.active) {
@@ -339,7 +340,7 @@ __device__ __forceinline__ void flatten_rev(const FlatTape& t, double bf, double
 // Adjoints of aveL / aveR at fraction x (frac_left / frac_right): accumulate the
 // Par adjoint and return d(ave)/dx.
 __device__ __forceinline__ double aveL_rev(double x, const Par& p, double b, Par& bp) {
-    const double h = x / 2.0, g = 1.0 - x / 1.5;
+    const double h = x / 2.0, g = 1.0 - div_1p5(x);
     const double a6 = 3.0 * (p.sL - p.sR);
     const double S = p.sR + p.sL;
     // aL + h (S + g a6), aL = a - sL
@@ -350,7 +351,7 @@ __device__ __forceinline__ double aveL_rev(double x, const Par& p, double b, Par
 }
 __device__ __forceinline__ double aveR_rev(double x, const Par& p, double b, Par& bp) {
     const double y = 1.0 - x;
-    const double h = y / 2.0, g = 1.0 - y / 1.5;
+    const double h = y / 2.0, g = 1.0 - div_1p5(y);
     const double a6 = 3.0 * (p.sL - p.sR);
     const double S = p.sR + p.sL;
     // aR - h (S - g a6), aR = a + sR

@@ -155,8 +155,9 @@ __device__ __forceinline__ float flatten32(float inv_cs, float p0, float pm2, fl
                                            float um1, float up1) {
     const float dp1f = pp1, dp2f = pp2 - pm1;
     const float dp1b = -pm1, dp2b = pp1 - pm2;
-    const float Mf = -up1 * inv_cs;
-    const float Mb = um1 * inv_cs;
+    (void)inv_cs;  // the signs of the Mach numbers are those of the velocity differences (flatten, pg_hydro.cuh)
+    const float Mf = -up1;
+    const float Mb = um1;
     float f = 0.0f;
     if ((Mf > 0.0f || Mb > 0.0f) && dp2f != 0.0f && dp2b != 0.0f) {
         f = 10.0f * fmaxf(0.0f, fabsf(dp1f / dp2f - 0.5f) - 0.25f);

@@ -52,12 +52,27 @@ struct FracT {
     T x, h, g;
 };
 using Frac = FracT<double>;
+// x / 1.5 correctly rounded without a division: with y = RN(1/1.5) = RN(2/3),
+// q = RN(x y) lies within an ulp of x / 1.5 and the remainder x - 1.5 q is
+// exact in one FMA, so RN(q + (x - 1.5 q) y) is the correctly rounded quotient
+// (Markstein, IBM J. Res. Dev. 34 (1990) 111-119); 2x/3 is never a midpoint of
+// two doubles.  Bit for bit the IEEE quotient the reference computes
+// (src/solver/recon/PPM.cu:100,111), three FP64 instructions.
 template <class T>
-__device__ __forceinline__ FracT<T> frac_left(T x) { return {x, x / 2.0, 1.0 - x / 1.5}; }
+__device__ __forceinline__ T div_1p5(T x) { return x / 1.5; }
+template <>
+__device__ __forceinline__ double div_1p5<double>(double x) {
+    constexpr double y = 2.0 / 3.0;
+    const double q = x * y;
+    const double r = fma(-q, 1.5, x);
+    return copysign(fma(r, y, q), x);  // the quotient of a positive divisor keeps x's sign (-0 / 1.5 = -0)
+}
+template <class T>
+__device__ __forceinline__ FracT<T> frac_left(T x) { return {x, x / 2.0, 1.0 - div_1p5(x)}; }
 template <class T>
 __device__ __forceinline__ FracT<T> frac_right(T x) {
     const T y = 1.0 - x;
-    return {y, y / 2.0, 1.0 - y / 1.5};
+    return {y, y / 2.0, 1.0 - div_1p5(y)};
 }
 template <class T>
 __device__ __forceinline__ T aveL(const FracT<T>& f, const ParT<T>& p) {
@@ -79,14 +94,18 @@ __device__ __forceinline__ T lim01(T a) { return fmin(fmax(a, T(0.0)), T(1.0)); 
 template <class T>
 __device__ __forceinline__ T exp_lim(T x) { return fmax(1.0 + x, T(1.0e-6)); }  // solve.cu:29
 
-// Shock flattening coefficient of the middle cell (src/solver/recon/PPM.cu:7-62);
-// inv_cs = 1/sqrt(gam p0 / r0) is shared with the interface states.
+// Shock flattening coefficient of the middle cell (src/solver/recon/PPM.cu:7-62).
+// The reference forms the Mach numbers (u0 - up1) / cs and (um1 - u0) / cs only
+// to test their signs; with cs > 0 those are the signs of the differences, so
+// the differences are tested (the quotient would differ only by underflowing a
+// difference below cs 2^-1074 to zero).  inv_cs (1 / cs) is not needed.
 template <class T>
 __device__ __forceinline__ T flatten(T inv_cs, T p0, T pm2, T pm1, T pp1, T pp2, T um1, T u0, T up1) {
+    (void)inv_cs;
     const T dp1f = pp1 - p0, dp2f = pp2 - pm1;
     const T dp1b = p0 - pm1, dp2b = pp1 - pm2;
-    const T Mf = (u0 - up1) * inv_cs;
-    const T Mb = (um1 - u0) * inv_cs;
+    const T Mf = u0 - up1;
+    const T Mb = um1 - u0;
     T f = 0.0;
     if ((Mf > 0.0 || Mb > 0.0) && dp2f != 0.0 && dp2b != 0.0) {
         T ddp = 10.0 * fmax(T(0.0), fabs(dp1f / dp2f - 0.5) - 0.25);

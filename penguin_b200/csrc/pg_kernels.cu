@@ -1343,3 +1343,33 @@ int kernels_per_step(const DiskView& d) {
 }
 
 }  // namespace pg
+
+namespace pg {
+// test support: div_1p5 (pg_hydro.cuh) against the IEEE quotient x / 1.5
+__global__ void k_test_div_1p5(const double* x, long long n, double* out) {
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+        const double a = x[k];
+        out[2 * k] = div_1p5(a);
+        out[2 * k + 1] = __ddiv_rn(a, 1.5);
+    }
+}
+}  // namespace pg
+
+extern "C" pg_status pg_test_div_1p5(const double* x, long long n, double* out2) {
+    if (!x || !out2 || n <= 0) return PG_ERR_ARG;
+    double *dx = nullptr, *dout = nullptr;
+    if (cudaMalloc(&dx, n * sizeof(double)) != cudaSuccess) return PG_ERR_CUDA;
+    if (cudaMalloc(&dout, 2 * n * sizeof(double)) != cudaSuccess) {
+        cudaFree(dx);
+        return PG_ERR_CUDA;
+    }
+    cudaError_t e = cudaMemcpy(dx, x, n * sizeof(double), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        pg::k_test_div_1p5<<<592, 256>>>(dx, n, dout);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(out2, dout, 2 * n * sizeof(double), cudaMemcpyDeviceToHost);
+    cudaFree(dx);
+    cudaFree(dout);
+    return e == cudaSuccess ? PG_OK : PG_ERR_CUDA;
+}

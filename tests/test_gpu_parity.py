@@ -267,3 +267,27 @@ def test_state_exchange_round_trip_allocates_nothing():
     for k in ("r", "p", "u", "v"):
         assert np.array_equal(out[k], st[k]), k
     d.close()
+
+
+def test_division_by_1p5_is_the_ieee_quotient():
+    """The kernels' division-free x / 1.5 (the PPM average's 1 - x/1.5) equals
+    the correctly rounded quotient bit for bit: the swept fractions in [0, 1],
+    their complements, random doubles of every magnitude and the edges."""
+    import ctypes
+
+    from penguin_b200._lib import check, lib
+
+    rng = np.random.default_rng(5)
+    q = rng.random(4_000_000)
+    raw = rng.integers(0, 2 ** 63 - 1, size=2_000_000, dtype=np.int64).view(np.float64)
+    raw = raw[np.isfinite(raw)]
+    edge = np.array([0.0, -0.0, 1.0, 0.5, 1.5, 3.0, 2.0 ** -1074, 2.0 ** -1022, 1.0 - 2.0 ** -53, np.nextafter(1.0, 0),
+                     1e-300, 1e300, 1.7976931348623157e308])
+    x = np.ascontiguousarray(np.concatenate([q, 1.0 - q, raw, -raw[:1000], edge]))
+    out = np.zeros(2 * x.size)
+    dp = ctypes.POINTER(ctypes.c_double)
+    check(lib().pg_test_div_1p5(x.ctypes.data_as(dp), x.size, out.ctypes.data_as(dp)))
+    a, b = out[0::2], out[1::2]
+    bad = ~((a == b) | (np.isnan(a) & np.isnan(b)))
+    assert not bad.any(), (x[bad][:5], a[bad][:5], b[bad][:5])
+    assert np.array_equal(np.signbit(a), np.signbit(b))
