@@ -59,27 +59,84 @@ def peaks():
 
 
 class Clocks:
-    """nvidia-smi samples during the timed region (the profiling recipe's clocks line)."""
+    """SM clocks and clock-event reasons while the timed steps run.
 
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    The profiling recipe's nvidia-smi clocks line samples every 200 ms and
+    needs about as long to start, which is longer than a 20-step region of the
+    headline workload (about 20 ms), so the samples are read through NVML
+    instead: `wait(event)` polls the device's clocks from the host until the
+    region's closing CUDA event has completed, i.e. only while the queued
+    steps are running.  Without NVML (no pynvml) it falls back to nvidia-smi
+    over the region."""
+
+    NAMES = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+    SMI = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+           "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+           "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
     def __init__(self, gpu: int):
         self.gpu = gpu
+        self.rows = []  # (sm MHz, max sm MHz, set of active reason names)
+        self.nv = None
+        self.h = None
         self.proc = None
         self.path = None
 
+    def _handle(self):
+        import pynvml as nv
+        import torch
+
+        nv.nvmlInit()
+        self.nv = nv
+        pr = torch.cuda.get_device_properties(self.gpu)
+        bus = getattr(pr, "pci_bus_id", None)
+        if bus is not None:
+            bid = f"{getattr(pr, 'pci_domain_id', 0):08X}:{bus:02X}:{getattr(pr, 'pci_device_id', 0):02X}.0"
+            try:
+                return nv.nvmlDeviceGetHandleByPciBusId(bid)
+            except Exception:
+                pass
+        return nv.nvmlDeviceGetHandleByIndex(self.gpu)
+
     def __enter__(self):
+        try:
+            self.h = self._handle()
+            nv = self.nv
+            self.bits = {"hw_slowdown": nv.nvmlClocksEventReasonHwSlowdown,
+                         "hw_thermal_slowdown": nv.nvmlClocksEventReasonHwThermalSlowdown,
+                         "sw_thermal_slowdown": nv.nvmlClocksEventReasonSwThermalSlowdown,
+                         "sw_power_cap": nv.nvmlClocksEventReasonSwPowerCap}
+            self.max_mhz = float(nv.nvmlDeviceGetMaxClockInfo(self.h, nv.NVML_CLOCK_SM))
+            return self
+        except Exception:
+            self.h = None
         fd, self.path = tempfile.mkstemp(suffix=".csv")
         os.close(fd)
         try:
             self.proc = subprocess.Popen(
-                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.SMI}", "--format=csv,noheader,nounits",
                  "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
         return self
+
+    def sample(self):
+        if self.h is None:
+            return
+        nv = self.nv
+        try:
+            mhz = float(nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM))
+            r = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+        except Exception:
+            return
+        self.rows.append((mhz, self.max_mhz, {n for n, b in self.bits.items() if r & b}))
+
+    def wait(self, event):
+        """Sample until `event` (recorded after the timed steps) has completed."""
+        while not event.query():
+            self.sample()
+            time.sleep(0.0005)
+        event.synchronize()
 
     def __exit__(self, *a):
         if self.proc:
@@ -88,27 +145,36 @@ class Clocks:
                 self.proc.wait(timeout=5)
             except Exception:
                 self.proc.kill()
+        if self.nv is not None:
+            try:
+                self.nv.nvmlShutdown()
+            except Exception:
+                pass
 
-    def summary(self):
-        rows = []
+    def _smi_rows(self):
         try:
             for line in open(self.path):
                 f = [x.strip() for x in line.split(",")]
                 if len(f) >= 9 and f[1].replace(".", "").isdigit():
-                    rows.append(f)
+                    act = {n for k, n in enumerate(self.NAMES) if f[5 + k].lower().startswith("active")}
+                    self.rows.append((float(f[1]), float(f[2]), act))
         except Exception:
             pass
         finally:
-            if self.path and os.path.exists(self.path):
+            if os.path.exists(self.path):
                 os.remove(self.path)
+
+    def summary(self):
+        if self.path:
+            self._smi_rows()
+        rows = self.rows
         if not rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
-        sm = [float(r[1]) for r in rows]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = [n for k, n in enumerate(names) if any(r[5 + k].lower().startswith("active") for r in rows)]
+        sm = [r[0] for r in rows]
+        reasons = [n for n in self.NAMES if any(n in r[2] for r in rows)]
         loaded = [s for s in sm if s > 0.5 * max(sm)] or sm
-        return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": float(rows[0][2]), "reasons": reasons,
-                "samples": len(rows)}
+        return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": rows[0][1], "reasons": reasons,
+                "samples": len(rows), "source": "nvml" if self.h is not None else "nvidia-smi"}
 
 
 def cpu_baseline(p, state, t0, budget_s=15.0, keep=False):
@@ -663,7 +729,7 @@ def main():
         e0.record(stream)
         disk.run(K)
         e1.record(stream)
-        e1.synchronize()
+        clk.wait(e1)
         barrier()
     ms = e0.elapsed_time(e1)
     disk.check()
