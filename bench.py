@@ -888,7 +888,8 @@ def parity_vs_oracle(p, state, orc, n, local, stream):
 
 
 def summary_of(line):
-    """The ratios the north star states, in one place at the end of the line."""
+    """The headline rate and the ratios of every form against the FP64 form, in one
+    place at the end of the line."""
     out = {"fp64_gzone_s": line["value"] / 1e9, "fp64_ms_per_step": line["ms_per_step"],
            "sweep_hbm_frac": line["roofline"]["frac"]}
     if line.get("roofline_fp64"):

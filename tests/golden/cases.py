@@ -151,7 +151,7 @@ def adiabatic_cases() -> list[dict]:
 
 
 def dust_cases() -> list[dict]:
-    """Gas + one dust fluid (config 3's physics at 64x192): alpha 1e-4, q 3e-4,
+    """Gas + one dust fluid (the gas+dust disk's physics at 64x192): alpha 1e-4, q 3e-4,
     Stokes 0.01 and 0.1, dust-to-gas 0.01.  The dust starts from init_CD (the
     reference's restart loads gas only).  tol: oracle vs the reference's output for
     the gas and dust fields; the reference's dust reconstruction reads a stale

@@ -6,7 +6,7 @@ its output snapshot is compared with the CUDA path stepped the same steps from
 the same state: relative L1 of density, pressure and the momentum vector after
 the case's step count.  The outputs (100 MB and more) are made at test time.
 
-The bar is the north star's 1e-12.  Printed beside it for the record: the
+The bar is 1e-12 relative L1.  Printed beside it for the record: the
 reference's own sensitivity floor, measured here by running it again from the
 same restart file with every density moved by one ulp (as make_golden.py's
 floor phase does for the golden cases), and the oracle's distance from the same
