@@ -1231,32 +1231,40 @@ pg_status pg_disk_run(pg_disk* dk, int nsteps, double end_time) {
     if (nsteps <= 0) return PG_OK;
     Engine& E = *dk->E;
     PG_CUDA(cudaSetDevice(E.device));
-    // main.cu:144 + 322: the first cap on dt is end_time - t after a (re)start
     pg_status s0 = resolve_cur(E);
     if (s0 != PG_OK) return s0;
-    Scalars h{};
-    PG_CUDA(cudaMemcpyAsync(&h, E.sc, sizeof(Scalars), cudaMemcpyDeviceToHost, E.stream));
-    PG_CUDA(cudaStreamSynchronize(E.stream));
-    if (E.fresh) h.dt_prev = end_time - h.t;
-    // a run that stopped on a clip at its end_time continues like main.cu after
-    // a dump (main.cu:333-338, 425): the step before the clip caps the next one
-    else if (h.dt_hold > 0.0) h.dt_prev = h.dt_hold;
-    h.dt_hold = 0.0;
-    h.end_time = end_time;
-    h.done = 0;
-    h.pad_ = 0;
-    PG_CUDA(cudaMemcpyAsync(E.sc, &h, sizeof(Scalars), cudaMemcpyHostToDevice, E.stream));
+    // with a finite end_time the device may finish early: check its done flag
+    // every 256 launched steps so the host does not keep launching no-op steps
+    const bool may_finish = end_time < 1.0e29;
+    if (may_finish) {
+        // main.cu:144 + 322: the first cap on dt is end_time - t after a (re)start
+        Scalars h{};
+        PG_CUDA(cudaMemcpyAsync(&h, E.sc, sizeof(Scalars), cudaMemcpyDeviceToHost, E.stream));
+        PG_CUDA(cudaStreamSynchronize(E.stream));
+        if (E.fresh) h.dt_prev = end_time - h.t;
+        // a run that stopped on a clip at its end_time continues like main.cu after
+        // a dump (main.cu:333-338, 425): the step before the clip caps the next one
+        else if (h.dt_hold > 0.0) h.dt_prev = h.dt_hold;
+        h.dt_hold = 0.0;
+        h.end_time = end_time;
+        h.done = 0;
+        h.pad_ = 0;
+        PG_CUDA(cudaMemcpyAsync(E.sc, &h, sizeof(Scalars), cudaMemcpyHostToDevice, E.stream));
+        E.steps_base = h.steps;  // the step count the device reached decides the newest buffer
+        E.pending = true;
+    } else {
+        // every launched step runs, so the newest buffer is known on the host: the
+        // same opening of the run as above, on the device, with no host round trip
+        launch_run_begin(E.sc, end_time, E.fresh, E.stream);
+        PG_CUDA(cudaGetLastError());
+        E.pending = false;
+    }
     E.fresh = false;
     E.cur_base = E.cur;
-    E.steps_base = h.steps;
-    E.pending = true;
     for (int k = 0; k < 2; ++k) {
         pg_status s = make_cell_maps(E.maps[k], E.buf[k], E.view.xarr, E.view.yarr);
         if (s != PG_OK) return s;
     }
-    // with a finite end_time the device may finish early: check its done flag
-    // every 256 launched steps so the host does not keep launching no-op steps
-    const bool may_finish = end_time < 1.0e29;
     for (int step = 0; step < nsteps; ++step) {
         if (may_finish && step > 0 && step % 256 == 0) {
             int done = 0;

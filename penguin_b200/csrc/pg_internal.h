@@ -79,6 +79,7 @@ void launch_bound(const DiskView& d, Cell* buf, cudaStream_t s);
 void launch_cfl(const DiskView& d, const Cell* buf, cudaStream_t s, const pg_dust* dbuf = nullptr);
 void launch_set_time(const DiskView& d, double t, double dt, cudaStream_t s);
 void launch_time_step(const DiskView& d, cudaStream_t s);
+void launch_run_begin(Scalars* sc, double end_time, bool fresh, cudaStream_t s);
 void launch_kick1(const DiskView& d, const CellMaps& in, Cell* out, double* vis, cudaStream_t s,
                   const pg_dust* din = nullptr, pg_dust* dout = nullptr, const Tune* t = nullptr);
 void launch_sweep_x(const DiskView& d, const CellMaps& in, Cell* out, cudaStream_t s, const Tune* t = nullptr);

@@ -836,6 +836,18 @@ __global__ void k_cfl(const DiskView d, const Cell* __restrict__ in, const pg_du
 
 __global__ void k_reset_vmax(Scalars* sc) { sc->vmax_bits = 0ull; }
 
+// Opens a device-resident run without a host round trip.  main.cu:144 + 322:
+// the first step after a (re)start is capped by end_time - t; after a clip at
+// end_time the step the clip replaced caps the next one (main.cu:333-338, 425).
+__global__ void k_run_begin(Scalars* sc, double end_time, int fresh) {
+    if (fresh) sc->dt_prev = end_time - sc->t;
+    else if (sc->dt_hold > 0.0) sc->dt_prev = sc->dt_hold;
+    sc->dt_hold = 0.0;
+    sc->end_time = end_time;
+    sc->done = 0;
+    sc->pad_ = 0;
+}
+
 // Host-supplied t, dt (pg_*_solve): planet for this step, reset of the signal-speed max.
 __global__ void k_set_time(const DiskView d, double t, double dt) {
     Scalars* sc = d.sc;
@@ -1167,6 +1179,10 @@ void launch_set_time(const DiskView& d, double t, double dt, cudaStream_t s) {
     k_set_time<<<1, 1, 0, s>>>(d, t, dt);
     k_planet_trig<<<cdiv(d.yarr, 256), 256, 0, s>>>(d);
 }
+void launch_run_begin(Scalars* sc, double end_time, bool fresh, cudaStream_t s) {
+    k_run_begin<<<1, 1, 0, s>>>(sc, end_time, fresh ? 1 : 0);
+}
+
 void launch_time_step(const DiskView& d, cudaStream_t s) {
     k_time_step<<<1, 1, 0, s>>>(d);
     k_planet_trig<<<cdiv(d.yarr, 256), 256, 0, s>>>(d);
