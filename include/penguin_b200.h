@@ -210,6 +210,12 @@ pg_status pg_disk_state_ptr(pg_disk* d, pg_cell** cells);
 /* global_dt (blocking) and one step with host-supplied t, dt, as in main.cu. */
 pg_status pg_disk_global_dt(pg_disk* d, double dt_prev, double* dt_out);
 pg_status pg_disk_solve(pg_disk* d, double t, double dt);
+/* main.cu's loop (main.cu:320-360) driven from the host, as pg_disk_global_dt and
+   pg_disk_solve called once per step: dt read back every step and clipped at
+   end_time, at most max_step steps.  *t, *dt: the time and the previous step on
+   entry (*dt 0: the first step is capped by end_time - t), the new ones on
+   return; *n: the steps taken. */
+pg_status pg_disk_step_host(pg_disk* d, int max_step, double end_time, double* t, double* dt, int* n);
 /* main.cu's loop on the device: nsteps of (dt = min(CFL dt, 1.1 dt_prev), clipped
    at end_time; solve; t += dt) with dt and t resident in device memory and the
    step captured in a CUDA graph.  Stream-ordered; pg_disk_sync waits.  A run

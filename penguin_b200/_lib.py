@@ -26,7 +26,7 @@ EXPORTS = [
     "pg_recon_weights",
     "pg_disk_write_snapshot", "pg_disk_read_snapshot", "pg_disk_set_average", "pg_disk_reset_average",
     "pg_disk_get_average",
-    "pg_disk_state_ptr", "pg_disk_global_dt", "pg_disk_solve", "pg_disk_run", "pg_disk_sync", "pg_disk_clock",
+    "pg_disk_state_ptr", "pg_disk_global_dt", "pg_disk_solve", "pg_disk_step_host", "pg_disk_run", "pg_disk_sync", "pg_disk_clock",
     "pg_disk_planet", "pg_disk_check", "pg_disk_torque", "pg_kernels_per_step", "pg_disk_profile",
     "pg_ens_check_params", "pg_ens_create", "pg_ens_destroy", "pg_ens_size", "pg_ens_dims", "pg_ens_set_state",
     "pg_ens_get_state", "pg_ens_run", "pg_ens_sync", "pg_ens_clock", "pg_ens_planet", "pg_ens_check",
@@ -93,6 +93,7 @@ def lib() -> ctypes.CDLL:
         "pg_disk_state_ptr": (i, [vp, ctypes.POINTER(vp)]),
         "pg_disk_global_dt": (i, [vp, d, dp]),
         "pg_disk_solve": (i, [vp, d, d]),
+        "pg_disk_step_host": (i, [vp, i, d, dp, dp, ip]),
         "pg_disk_run": (i, [vp, i, d]),
         "pg_disk_sync": (i, [vp]),
         "pg_disk_clock": (i, [vp, dp, dp, ctypes.POINTER(ctypes.c_longlong)]),

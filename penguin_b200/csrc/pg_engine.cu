@@ -473,6 +473,7 @@ struct Engine {
     size_t snap_n = 0;
     double* xfer = nullptr;                  // device staging of host exchanges (xfer_buffer)
     size_t xfer_n = 0;
+    unsigned long long* hbits = nullptr;     // pinned read-back of the signal-rate maximum (global_dt)
 
     ~Engine() {
         for (auto& g : graph)
@@ -491,6 +492,7 @@ struct Engine {
         cudaFree(dbuf[1]);
         cudaFree(ave);
         if (snap) cudaFreeHost(snap);
+        if (hbits) cudaFreeHost(hbits);
         cudaFree(xfer);
         cudaFree(grid);
         cudaFree(tab);
@@ -1202,9 +1204,12 @@ pg_status pg_disk_state_ptr(pg_disk* dk, pg_cell** cells) {
 pg_status pg_disk_global_dt(pg_disk* dk, double dt_prev, double* dt_out) {
     if (!dk || !dt_out) return fail(PG_ERR_ARG, "null argument");
     Engine& E = *dk->E;
-    unsigned long long bits = 0;
-    PG_CUDA(cudaMemcpyAsync(&bits, &E.sc->vmax_bits, sizeof(bits), cudaMemcpyDeviceToHost, E.stream));
+    // into pinned memory: a pageable destination would add a staged copy to every step
+    if (!E.hbits) PG_CUDA(cudaMallocHost(&E.hbits, sizeof(unsigned long long)));
+    PG_CUDA(cudaMemcpyAsync(E.hbits, &E.sc->vmax_bits, sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                            E.stream));
     PG_CUDA(cudaStreamSynchronize(E.stream));
+    const unsigned long long bits = *E.hbits;
     double vmax;
     std::memcpy(&vmax, &bits, sizeof vmax);
     const double dt = E.P.cfl / vmax;  // get_dt_lv2 (timestep.cu:108)
@@ -1223,6 +1228,31 @@ pg_status pg_disk_solve(pg_disk* dk, double t, double dt) {
     launch_set_time(E.view, t, dt, E.stream);
     pg_status s = enqueue_stages(E);
     E.fresh = false;
+    return s;
+}
+
+pg_status pg_disk_step_host(pg_disk* dk, int max_step, double end_time, double* t, double* dt, int* n) {
+    if (!dk || !t || !dt || !n) return fail(PG_ERR_ARG, "null argument");
+    // main.cu:320-360: dt from global_dt (read back every step), clipped at end_time,
+    // then solve and t += dt; a first call without a previous step caps dt by end_time - t
+    double tt = *t, step = (*dt != 0.0) ? *dt : end_time - *t;
+    int k = 0;
+    pg_status s = PG_OK;
+    while (k < max_step) {
+        if ((s = pg_disk_global_dt(dk, step, &step)) != PG_OK) break;
+        bool last = false;
+        if (tt + step > end_time) {
+            step = end_time - tt;
+            last = true;
+        }
+        if ((s = pg_disk_solve(dk, tt, step)) != PG_OK) break;
+        tt += step;
+        ++k;
+        if (last) break;
+    }
+    *t = tt;
+    *dt = step;
+    *n = k;
     return s;
 }
 

@@ -82,22 +82,14 @@ class Disk:
         check(lib().pg_disk_solve(self._h, t, dt))
 
     def step_host(self, max_step: int, end_time: float = 1.0e30) -> int:
-        """main.cu:320-360 driven from the host: dt from global_dt, clipped at end_time."""
-        dt = self.dt if self.dt else end_time - self.t
-        n = 0
-        while n < max_step:
-            dt = self.global_dt(dt)
-            last = False
-            if self.t + dt > end_time:
-                dt = end_time - self.t
-                last = True
-            self.solve(self.t, dt)
-            self.t += dt
-            n += 1
-            if last:
-                break
-        self.dt = dt
-        return n
+        """main.cu:320-360 driven from the host: dt from global_dt (read back every
+        step), clipped at end_time, then solve; the loop runs in the library
+        (pg_disk_step_host)."""
+        t, dt, n = ctypes.c_double(self.t), ctypes.c_double(self.dt or 0.0), ctypes.c_int(0)
+        s = lib().pg_disk_step_host(self._h, max_step, end_time, ctypes.byref(t), ctypes.byref(dt), ctypes.byref(n))
+        self.t, self.dt = t.value, dt.value
+        check(s)
+        return n.value
 
     def run(self, nsteps: int, end_time: float = 1.0e30) -> None:
         """nsteps of the device-resident loop (stream-ordered; call sync())."""
