@@ -74,7 +74,11 @@ constexpr int ST_VIS_N = ST_HX * ST_HY * 2;
 constexpr int ST_VIS = (ST_VIS_N + 15) / 16 * 16;
 constexpr size_t K1_SMEM = (size_t)2 * ST_TILE * 8 + 16 + 128;
 constexpr int ST_GRAV = (ST_HX * ST_HY * 3 + 15) / 16 * 16;  // kick2: gravity of the predictor, per tile cell
-constexpr size_t K5_SMEM = (size_t)(3 * ST_TILE + 2 * ST_VIS + ST_GRAV) * 8 + 16 + 128;
+// kick2: the tile's per-radius (34) and per-row (10) tables, staged once per tile
+enum KRad { KR_RAD, KR_IRAD, KR_GSTAR, KR_NU, KR_IDX, KR_ROT, KR_VX, KR_KILL = KR_VX + 5, KR_N = KR_KILL + 4 };
+enum KRow { KY_SIN, KY_COS, KY_IDY, KY_VY, KY_N = KY_VY + 4 };
+constexpr int ST_TAB = (KR_N * ST_HX + KY_N * ST_HY + 15) / 16 * 16;
+constexpr size_t K5_SMEM = (size_t)(3 * ST_TILE + 2 * ST_VIS + ST_GRAV + ST_TAB) * 8 + 16 + 128;
 
 // --------------------------------------------------------- source terms
 struct Grav {
@@ -84,11 +88,11 @@ struct Grav {
 // 182-327 with twobd_flag 0, pol = 0).  The star term is a per-radius table; the
 // planet's angle enters through the per-row sin/cos table of this step
 // (k_planet_trig) and 1/x_p^2 through the table's tail.
-__device__ __forceinline__ Grav gravity(const DiskView& d, int i, double rad, double sinfac, double cosfac,
-                                        double iplx2, const pg_body& p) {
+__device__ __forceinline__ Grav gravity_at(const DiskView& d, double gstar, double rad, double sinfac,
+                                           double cosfac, double iplx2, const pg_body& p) {
     Grav g{0.0, 0.0, 0.0};
     if (d.geomx == 1) {
-        g.gx = d.gstar[i];
+        g.gx = gstar;
         g.gz = -0.0;
         if (d.nplanet > 0) {
             const double plm = p.m, plx = p.x;
@@ -100,6 +104,10 @@ __device__ __forceinline__ Grav gravity(const DiskView& d, int i, double rad, do
         }
     }
     return g;
+}
+__device__ __forceinline__ Grav gravity(const DiskView& d, int i, double rad, double sinfac, double cosfac,
+                                        double iplx2, const pg_body& p) {
+    return gravity_at(d, d.geomx == 1 ? d.gstar[i] : 0.0, rad, sinfac, cosfac, iplx2, p);
 }
 
 // One body of the two-body frame as an inertial point mass
@@ -216,6 +224,23 @@ __device__ __forceinline__ double signal_rate(const DiskView& d, const Cell& c, 
         spd = fabs(c.v - rad_cyl * d.frame_omega - d.rot[i]) + cs;
         if (dc) spd = fmax(fabs(dc->v - rad_cyl * d.frame_omega - d.rot[i]), spd);
         tmp = fmax(spd * (d.idx_y[j] * ((d.geomy == 3) ? d.irad[i] : 1.0)), tmp);
+    }
+    return tmp;
+}
+
+// signal_rate with the cell's table entries passed in (kick2's staged tables):
+// the same expressions
+__device__ __forceinline__ double signal_rate_at(const DiskView& d, const Cell& c, double radx, double idxx,
+                                                 double rot, double idyj, double irad, const DCell* dc = nullptr) {
+    const double rad_cyl = (d.geomy == 3) ? radx : 1.0;
+    const double cs = sqrt(d.gam * c.p / c.r);
+    double spd = fabs(c.u) + cs;
+    if (dc) spd = fmax(fabs(dc->u), spd);
+    double tmp = fmax(spd * idxx, 0.0);
+    if (d.ndim > 1) {
+        spd = fabs(c.v - rad_cyl * d.frame_omega - rot) + cs;
+        if (dc) spd = fmax(fabs(dc->v - rad_cyl * d.frame_omega - rot), spd);
+        tmp = fmax(spd * (idyj * ((d.geomy == 3) ? irad : 1.0)), tmp);
     }
     return tmp;
 }
@@ -668,7 +693,7 @@ __global__ void __launch_bounds__(ST_THREADS, 4)
 }
 
 // ============================================ kick 2 + damping + CFL speed
-// 3 CTAs per SM (80 registers, no spills; 60 KB of shared memory each): the
+// 3 CTAs per SM (80 registers, no spills; 65 KB of shared memory each): the
 // pass waits on table and tile loads, and 24 warps per SM hide them better than
 // the 16 its natural 102 registers allow (0.222 -> 0.181 ms on the 1024x3072 disk)
 template <bool VISC>
@@ -682,16 +707,57 @@ __global__ void __launch_bounds__(ST_THREADS, 3)
     auto vstage = [&](int n) { return smem + 2 * ST_TILE + (n & 1) * ST_VIS; };  // stress of the first evaluation
     double* tp = smem + 2 * ST_TILE + 2 * ST_VIS;                      // predicted state with 1 halo
     double* gc = tp + ST_TILE;  // gravity at the predictor's cells: the corrector's is the same (time `next`)
-    uint64_t* bar = reinterpret_cast<uint64_t*>(gc + ST_GRAV);
+    double* tb = gc + ST_GRAV;  // the tile's tables: [KR_N][ST_HX] per radius, then [KY_N][ST_HY] per row
+    double* ty = tb + KR_N * ST_HX;
+    uint64_t* bar = reinterpret_cast<uint64_t*>(tb + ST_TAB);
     Scalars* sc = d.sc;
     if (sc->done) return;
     const int tid = threadIdx.x;
     const double dt = sc->dt, hdt = 0.5 * dt;
     const pg_body pl = sc->planet_next;
     const pg_body st = sc->star_next;
+    // the disk's gravity comes from the staged tables; the two-body frame reads its own
+    const bool disk_grav = !d.twobd;
+    const double iplx2 = disk_grav ? d.trig[4 * d.yarr + 1] : 0.0;
     auto origin = [&](int tile, int& i0, int& j0) {
         i0 = NPAD + ST_TX * (tile % ntx);
         j0 = d.ypad + ST_TY * (tile / ntx);
+    };
+    // Per-radius and per-row table entries of the tile and its halo, read once per
+    // tile (coalesced) instead of once per cell: the pass is bound by the latency of
+    // those loads.  Indices past the grid are clamped; those cells are not used.
+    auto stage_tables = [&](int i0, int j0) {
+        for (int it = tid; it < KR_N * ST_HX; it += ST_THREADS) {
+            const int f = it / ST_HX, hx = it % ST_HX;
+            const int i = min(max(i0 - 1 + hx, 0), d.xarr - 1);
+            double v = 0.0;
+            if (f == KR_RAD) v = d.radx[i];
+            else if (f == KR_IRAD) v = d.irad[i];
+            else if (f == KR_GSTAR) v = d.geomx == 1 ? d.gstar[i] : 0.0;
+            else if (f == KR_NU) v = VISC ? d.nux[i] : 0.0;
+            else if (f == KR_IDX) v = d.idx_x[i];
+            else if (f == KR_ROT) v = d.ndim > 1 ? d.rot[i] : 0.0;
+            else if (f < KR_KILL) v = VISC ? d.visx[5 * i + (f - KR_VX)] : 0.0;
+            else v = d.kill ? d.killx[4 * i + (f - KR_KILL)] : 0.0;
+            tb[it] = v;
+        }
+        for (int it = tid; it < KY_N * ST_HY; it += ST_THREADS) {
+            const int f = it / ST_HY, hy = it % ST_HY;
+            const int j = min(max(j0 - 1 + hy, 0), d.yarr - 1);  // 1D: one row, no ghost rows
+            double v = 0.0;
+            if (f == KY_SIN) v = disk_grav ? d.trig[4 * j + 2] : 0.0;
+            else if (f == KY_COS) v = disk_grav ? d.trig[4 * j + 3] : 0.0;
+            else if (f == KY_IDY) v = d.ndim > 1 ? d.idx_y[j] : 0.0;
+            else v = VISC ? d.visy[4 * j + (f - KY_VY)] : 0.0;
+            ty[it] = v;
+        }
+    };
+    // gravity at tile cell (hx, hy), bodies at t + dt
+    auto grav = [&](int hx, int hy, int i, int j) {
+        if (disk_grav)
+            return gravity_at(d, tb[KR_GSTAR * ST_HX + hx], tb[KR_RAD * ST_HX + hx], ty[KY_SIN * ST_HY + hy],
+                              ty[KY_COS * ST_HY + hy], iplx2, pl);
+        return body_gravity(d, i, j, 1, pl, st);
     };
     auto issue = [&](int tile, int k) {
         int i0, j0;
@@ -711,6 +777,8 @@ __global__ void __launch_bounds__(ST_THREADS, 3)
             origin(tile_id, i0, j0);
             const double* tile = stage(kt);
             const double* tvis = vstage(kt);
+            stage_tables(i0, j0);  // while the tile's copy is in flight
+            __syncthreads();
             if (!pipe_wait(bar, kt, sc)) {
         pipe_drain(bar, kt, tile_id + (int)gridDim.x < ntiles, sc);
         return;
@@ -724,11 +792,12 @@ __global__ void __launch_bounds__(ST_THREADS, 3)
                     if (i < NPAD || i >= NPAD + d.xres || j < 0 || j >= d.yarr) continue;
                     const double* c = tile + it * 5;
                     const Cell C{c[0], c[1], c[2], c[3], c[4]};
-                    const Grav g = body_gravity(d, i, j, 1, pl, st);
+                    const Grav g = grav(hx, hy, i, j);
                     gc[3 * it] = g.gx;
                     gc[3 * it + 1] = g.gy;
                     gc[3 * it + 2] = g.gz;
-                    const Cell Q = kick<true>(d, C, d.irad[i], g, tvis[2 * it], tvis[2 * it + 1], hdt, hdt);
+                    const Cell Q = kick<true>(d, C, tb[KR_IRAD * ST_HX + hx], g, tvis[2 * it], tvis[2 * it + 1], hdt,
+                                              hdt);
                     double* o = tp + it * 5;
                     o[0] = Q.r; o[1] = Q.p; o[2] = Q.u; o[3] = Q.v; o[4] = Q.w;
                 }
@@ -766,30 +835,34 @@ __global__ void __launch_bounds__(ST_THREADS, 3)
                 const double* c = tile + (hy * ST_HX + hx) * 5;
                 const Cell C{c[0], c[1], c[2], c[3], c[4]};
                 double vx = 0.0, vy = 0.0;
+                const double irad = tb[KR_IRAD * ST_HX + hx];
                 if (VISC) {
-                    double nu[3], u[9], v[9], nr[9];
+                    double nu[3], u[9], v[9], nr[9], X[5], Y[4];
 #pragma unroll
-                    for (int n = 0; n < 3; ++n) nu[n] = d.nux[i + n - 1];
+                    for (int n = 0; n < 3; ++n) nu[n] = tb[KR_NU * ST_HX + hx + n - 1];
+#pragma unroll
+                    for (int n = 0; n < 5; ++n) X[n] = tb[(KR_VX + n) * ST_HX + hx];
+#pragma unroll
+                    for (int n = 0; n < 4; ++n) Y[n] = ty[(KY_VY + n) * ST_HY + hy];
                     gather9(tp, hx, hy, nu, u, v, nr);
-                    viscous(d.visx + 5 * i, d.visy + 4 * j, u, v, nr, vx, vy);
+                    viscous(X, Y, u, v, nr, vx, vy);
                 }
                 const int ic = 3 * (hy * ST_HX + hx);
-                const Grav g = VISC ? Grav{gc[ic], gc[ic + 1], gc[ic + 2]} : body_gravity(d, i, j, 1, pl, st);
+                const Grav g = VISC ? Grav{gc[ic], gc[ic + 1], gc[ic + 2]} : grav(hx, hy, i, j);
                 double Tu = C.u, Tv = C.v;
-                Cell Q = kick<VISC>(d, C, d.irad[i], g, vx, vy, hdt, hdt, &Tu, &Tv);
+                Cell Q = kick<VISC>(d, C, irad, g, vx, vy, hdt, hdt, &Tu, &Tv);
                 // cooling over dt/2; the predictor cools over mdt = dt/2 as well, so Q.p is also
                 // the predicted pressure the dust's second stopping time reads (sweeps.cu:668-699)
                 if (d.cool) Q.p = p_cool(d, i, C.p, C.r, hdt);
                 const double Tp = Q.p;
                 if (d.kill) {
                     // killwave (src/killwave/killwave.cu:48-100): relax towards init_C
-                    const double* kt = d.killx + 4 * i;
                     const double* I = d.initx + 5 * i;
 #pragma unroll
                     for (int side = 0; side < 2; ++side) {
-                        const double tau = kt[2 * side + 1];
+                        const double tau = tb[(KR_KILL + 2 * side + 1) * ST_HX + hx];
                         if (tau > 0.0) {
-                            double f = kt[2 * side];
+                            double f = tb[(KR_KILL + 2 * side) * ST_HX + hx];
                             f *= dt / tau;
                             Q.r += f * (I[0] - Q.r);
                             Q.p += f * (I[1] - Q.p);
@@ -802,11 +875,13 @@ __global__ void __launch_bounds__(ST_THREADS, 3)
                 if (!(Q.r > 0.0)) atomicOr(&sc->err, 1 << PG_ERR_NAN);
                 if (din) {  // dust corrector half-kick towards the predicted gas velocity (sweeps.cu:663-707)
                     const DCell D = dust_kick(d, C, Tu, Tv, Tp, load_dust(din, d.xarr, i, j), g.gx, g.gy, g.gz,
-                                              d.irad[i], hdt, hdt);
+                                              irad, hdt, hdt);
                     emit_dust(d, dout, i, j, D);
-                    vmax = fmax(vmax, signal_rate(d, Q, i, j, &D));
+                    vmax = fmax(vmax, signal_rate_at(d, Q, tb[KR_RAD * ST_HX + hx], tb[KR_IDX * ST_HX + hx],
+                                                     tb[KR_ROT * ST_HX + hx], ty[KY_IDY * ST_HY + hy], irad, &D));
                 } else {
-                    vmax = fmax(vmax, signal_rate(d, Q, i, j));
+                    vmax = fmax(vmax, signal_rate_at(d, Q, tb[KR_RAD * ST_HX + hx], tb[KR_IDX * ST_HX + hx],
+                                                     tb[KR_ROT * ST_HX + hx], ty[KY_IDY * ST_HY + hy], irad));
                 }
                 emit(d, out, i, j, Q);
                 if (d.ave) accumulate_average(d, i, j, Q, hdt);  // ... and after it
