@@ -389,6 +389,12 @@ pg_status pg_disk3_pass_times(pg_disk3* d, int nsteps, double* ms6);
    u, v, w planes.  read_snapshot restarts from the file at its t. */
 pg_status pg_disk3_write_snapshot(pg_disk3* d, const char* path);
 pg_status pg_disk3_read_snapshot(pg_disk3* d, const char* path, double* t_out);
+/* test support: the passes' bounded wait on a tile copy that is never issued
+   (one CTA).  err_bits: the device error word afterwards (PG_ERR_TIMEOUT's bit
+   set when the wait gave up); left: 1 when the CTA left through the timed-out
+   path; ms: the kernel's duration (the wait's limit is 50 ms, then up to 50 ms
+   more for copies in flight). */
+pg_status pg_test_bounded_wait(int* err_bits, int* left, float* ms);
 /* test support: out2[2k] = the kernels' division-free x[k] / 1.5, out2[2k+1] =
    the IEEE quotient, for n host values.  Uses the GPU. */
 pg_status pg_test_div_1p5(const double* x, long long n, double* out2);

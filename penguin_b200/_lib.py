@@ -36,7 +36,7 @@ EXPORTS = [
     "pg_adj_backward", "pg_adj_model_error", "pg_adj_dot_test", "pg_adj_pass_check", "pg_adj_replay_diff", "pg_adj_pass_fields", "pg_adj_schedule", "pg_adj_steps", "pg_adj_device_bytes", "pg_adj_set_sweep_reverse",
     "pg_disk3_create", "pg_disk3_destroy", "pg_disk3_set_state", "pg_disk3_get_state", "pg_disk3_global_dt",
     "pg_disk3_solve", "pg_disk3_run", "pg_disk3_clock", "pg_disk3_check", "pg_disk3_pass_times", "pg_disk3_stages", "pg_disk3_write_snapshot", "pg_disk3_read_snapshot", "pg_make_axis",
-    "pg_test_div_1p5",
+    "pg_test_div_1p5", "pg_test_bounded_wait",
 ]
 
 
@@ -150,6 +150,7 @@ def lib() -> ctypes.CDLL:
         "pg_disk3_stages": (i, [vp, d, d, dp]),
         "pg_disk3_write_snapshot": (i, [vp, ctypes.c_char_p]),
         "pg_test_div_1p5": (i, [dp, ctypes.c_longlong, dp]),
+        "pg_test_bounded_wait": (i, [ip, ip, ctypes.POINTER(ctypes.c_float)]),
         "pg_disk3_read_snapshot": (i, [vp, ctypes.c_char_p, dp]),
         "pg_make_axis": (i, [PP, i, dp, dp]),
     }

@@ -127,16 +127,20 @@ __device__ __forceinline__ uint64_t globaltimer_ns() {
 // Bounded wait on a TMA completion: a tile lands in microseconds, so after 50 ms
 // the wait records PG_ERR_TIMEOUT, waits up to another 50 ms for the copy that
 // may still be in flight (the CTA must not leave with it pending) and returns
-// false so the caller can exit.
+// false so the caller can exit.  A count of polls bounds both loops as well,
+// should the timer not advance.
+constexpr uint32_t MBAR_MAX_POLLS = 1u << 24;
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, Scalars* sc) {
     if (mbar_try_wait(bar, parity)) return true;
     uint64_t t0 = globaltimer_ns();
+    uint32_t polls = 0;
     while (!mbar_try_wait(bar, parity))
-        if (globaltimer_ns() - t0 > 50000000ull) {
+        if (globaltimer_ns() - t0 > 50000000ull || ++polls > MBAR_MAX_POLLS) {
             atomicOr(&sc->err, 1 << PG_ERR_TIMEOUT);
             t0 = globaltimer_ns();
+            polls = 0;
             while (!mbar_try_wait(bar, parity))
-                if (globaltimer_ns() - t0 > 50000000ull) break;
+                if (globaltimer_ns() - t0 > 50000000ull || ++polls > MBAR_MAX_POLLS) break;
             return false;
         }
     return true;

@@ -1441,6 +1441,23 @@ int kernels_per_step(const DiskView& d) {
 }  // namespace pg
 
 namespace pg {
+// test support: the passes' bounded wait (pipe_wait) on a tile whose copy is
+// never issued: the stage's barrier expects `bytes` that nothing delivers, so
+// every thread gives up after the wait's limit, PG_ERR_TIMEOUT is recorded and
+// the CTA leaves together; nothing is in flight when it does.
+__global__ void k_test_bounded_wait(Scalars* sc, uint32_t bytes, int* left) {
+    __shared__ __align__(8) uint64_t bar[2];
+    pipe_init<2>(bar);
+    if (threadIdx.x == 0) issue_begin(&bar[0], bytes);
+    __syncthreads();
+    if (!pipe_wait<2>(bar, 0, sc)) {
+        pipe_drain<2>(bar, 0, 0, sc);
+        if (threadIdx.x == 0) *left = 1;
+        return;
+    }
+    if (threadIdx.x == 0) *left = 2;  // the copy "landed": not expected
+}
+
 // test support: div_1p5 (pg_hydro.cuh) against the IEEE quotient x / 1.5
 __global__ void k_test_div_1p5(const double* x, long long n, double* out) {
     for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
@@ -1450,6 +1467,36 @@ __global__ void k_test_div_1p5(const double* x, long long n, double* out) {
     }
 }
 }  // namespace pg
+
+extern "C" pg_status pg_test_bounded_wait(int* err_bits, int* left, float* ms) {
+    if (!err_bits || !left || !ms) return PG_ERR_ARG;
+    pg::Scalars* sc = nullptr;
+    int* dleft = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaError_t e = cudaMalloc(&sc, sizeof(pg::Scalars));
+    if (e == cudaSuccess) e = cudaMalloc(&dleft, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(sc, 0, sizeof(pg::Scalars));
+    if (e == cudaSuccess) e = cudaMemset(dleft, 0, sizeof(int));
+    if (e == cudaSuccess) e = cudaEventCreate(&e0);
+    if (e == cudaSuccess) e = cudaEventCreate(&e1);
+    if (e == cudaSuccess) {
+        cudaEventRecord(e0);
+        pg::k_test_bounded_wait<<<1, 64>>>(sc, 4096, dleft);
+        e = cudaGetLastError();
+        cudaEventRecord(e1);
+    }
+    if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+    if (e == cudaSuccess) e = cudaEventElapsedTime(ms, e0, e1);
+    pg::Scalars h{};
+    if (e == cudaSuccess) e = cudaMemcpy(&h, sc, sizeof(h), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(left, dleft, sizeof(int), cudaMemcpyDeviceToHost);
+    *err_bits = h.err;
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    cudaFree(sc);
+    cudaFree(dleft);
+    return e == cudaSuccess ? PG_OK : PG_ERR_CUDA;
+}
 
 extern "C" pg_status pg_test_div_1p5(const double* x, long long n, double* out2) {
     if (!x || !out2 || n <= 0) return PG_ERR_ARG;

@@ -176,6 +176,39 @@ def test_error_word_reports_nan():
     assert e.value.status == PG_ERR_NAN
 
 
+def test_bounded_wait_gives_up_and_leaves_the_context_usable():
+    """A pass's wait on a tile copy that never lands (its barrier expects bytes
+    that no copy delivers) gives up after its limit instead of hanging: the
+    device error word reports PG_ERR_TIMEOUT, the CTA leaves through the
+    timed-out path, and the same context then steps a disk as before."""
+    import ctypes
+
+    from penguin_b200._lib import PG_ERR_TIMEOUT, check, lib
+
+    p = P.reference_disk(32, 96)
+    st = I.disk_state(p, seed=4)
+
+    def five_steps():
+        d = Disk(p)
+        d.set_state(C.T0_DISK, st)
+        d.run(5)
+        d.sync()
+        d.check()
+        g = d.get_state()
+        d.close()
+        return g
+
+    before = five_steps()
+    err, left, ms = ctypes.c_int(0), ctypes.c_int(0), ctypes.c_float(0.0)
+    check(lib().pg_test_bounded_wait(ctypes.byref(err), ctypes.byref(left), ctypes.byref(ms)))
+    assert err.value & (1 << PG_ERR_TIMEOUT), err.value
+    assert left.value == 1
+    assert 45.0 <= ms.value < 2000.0, ms.value  # 50 ms, then up to 50 ms more
+    after = five_steps()
+    for k in _keys(p):
+        assert np.array_equal(before[k], after[k]), k
+
+
 def test_drop_in_grid_entry_points_match_handle_api():
     """main.cu's loop on the pg_grid_* entry points (caller-owned buffers, C/T
     pointer swaps) gives the same state as the handle API."""
