@@ -91,6 +91,9 @@ typedef struct {
  * orb_rot/orb_res/orb_shf/orb_inc, C, T, vis_tensor, planets.  C and T may be
  * swapped by pg_grid_solve exactly as the reference swaps them
  * (src/solver/sweeps.cu:353-355): afterwards C holds the newest state.
+ * In 1D and 2D the cells' z-velocity w must be 0, as the reference's own 1D/2D
+ * states always hold it (init_C writes 0 and no 1D/2D force changes it): the
+ * passes skip its reconstruction and flux there.
  */
 typedef struct {
     void* stream; /* cudaStream_t */
