@@ -460,7 +460,8 @@ struct Engine {
     bool pending = false;
     int cur_base = 0;
     long long steps_base = 0;
-    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};   // pg_disk_run: one step from buffer k
+    cudaGraphExec_t sgraph[2] = {nullptr, nullptr};  // pg_disk_solve: the step after k_set_time, from buffer k
     std::vector<const void*> ghosted;  // buffers whose constant radial ghosts are initialised
     std::vector<const void*> dghosted; // dust buffers likewise (drop-in mode)
     pg_body* grid_planet = nullptr;    // drop-in mode: the caller's planets array
@@ -477,6 +478,8 @@ struct Engine {
 
     ~Engine() {
         for (auto& g : graph)
+            if (g) cudaGraphExecDestroy(g);
+        for (auto& g : sgraph)
             if (g) cudaGraphExecDestroy(g);
         if (own_buffers) {
             cudaFree(buf[0]);
@@ -678,6 +681,16 @@ static pg_status resolve_cur(Engine& E) {
 // Kernels of one step after the time kernel; in = E.cur.  With rec, the input
 // of every pass, kick1's stress and the orbital-advection arrays are copied
 // out for the adjoint.
+// the captured steps hold the view, the tensor maps and the launch configuration
+static void drop_graphs(Engine& E) {
+    for (auto* gs : {E.graph, E.sgraph})
+        for (int k = 0; k < 2; ++k)
+            if (gs[k]) {
+                cudaGraphExecDestroy(gs[k]);
+                gs[k] = nullptr;
+            }
+}
+
 static pg_status enqueue_stages(Engine& E, const StepRecord* rec = nullptr) {
     const DiskView& d = E.view;
     pg_status s;
@@ -1225,10 +1238,32 @@ pg_status pg_disk_solve(pg_disk* dk, double t, double dt) {
     PG_CUDA(cudaSetDevice(E.device));
     pg_status s0 = resolve_cur(E);
     if (s0 != PG_OK) return s0;
-    launch_set_time(E.view, t, dt, E.stream);
-    pg_status s = enqueue_stages(E);
+    // this step's t and dt go in as launch arguments of k_set_time; the rest of the
+    // step (planet angles, five passes) is one captured graph per starting buffer,
+    // one launch instead of six behind the host's dt read-back
+    launch_set_time_only(E.view, t, dt, E.stream);
+    PG_CUDA(cudaGetLastError());
+    const int c0 = E.cur;
+    if (!E.sgraph[c0]) {
+        cudaGraph_t g;
+        PG_CUDA(cudaStreamBeginCapture(E.stream, cudaStreamCaptureModeThreadLocal));
+        launch_planet_trig(E.view, E.stream);
+        pg_status s = enqueue_stages(E);
+        cudaError_t ce = cudaStreamEndCapture(E.stream, &g);
+        E.cur = c0;
+        if (s != PG_OK) {
+            if (ce == cudaSuccess) cudaGraphDestroy(g);
+            return s;
+        }
+        PG_CUDA(ce);
+        cudaError_t ie = cudaGraphInstantiate(&E.sgraph[c0], g, 0);
+        cudaGraphDestroy(g);
+        PG_CUDA(ie);
+    }
+    PG_CUDA(cudaGraphLaunch(E.sgraph[c0], E.stream));
+    E.cur = (passes_per_step(E.view) % 2) ? 1 - c0 : c0;
     E.fresh = false;
-    return s;
+    return PG_OK;
 }
 
 pg_status pg_disk_step_host(pg_disk* dk, int max_step, double end_time, double* t, double* dt, int* n) {
@@ -1465,11 +1500,7 @@ pg_status pg_disk_autotune(pg_disk* dk, int reps, int* choice) {
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     E.tune = best;
-    for (auto& g : E.graph)
-        if (g) {
-            cudaGraphExecDestroy(g);
-            g = nullptr;
-        }
+    drop_graphs(E);
     PG_CUDA(cudaMemcpyAsync(E.buf[c], saved, n * sizeof(Cell), cudaMemcpyDeviceToDevice, E.stream));
     PG_CUDA(cudaMemcpyAsync(E.sc, ssc, sizeof(Scalars), cudaMemcpyDeviceToDevice, E.stream));
     PG_CUDA(cudaFreeAsync(saved, E.stream));
@@ -1486,13 +1517,6 @@ static int snapshot_fields(const DiskView& d) {
     return (d.ndim > 1 ? 4 : 3) + (d.dust ? (d.ndim > 1 ? 4 : 2) : 0);
 }
 
-static void drop_graphs(Engine& E) {
-    for (auto& g : E.graph)
-        if (g) {
-            cudaGraphExecDestroy(g);
-            g = nullptr;
-        }
-}
 
 // ave_flag: the gas state averaged over a save interval T by the trapezoid rule
 // of main.cu:343-351 (A += C (dt/2)/T before and after each step), accumulated
@@ -1660,11 +1684,7 @@ pg_status pg_disk_set_tuning(pg_disk* dk, const int* choice) {
     }
     Engine& E = *dk->E;
     E.tune = t;
-    for (auto& g : E.graph)
-        if (g) {
-            cudaGraphExecDestroy(g);
-            g = nullptr;
-        }
+    drop_graphs(E);
     return PG_OK;
 }
 

@@ -77,7 +77,9 @@ void launch_init_tables(const DiskView& d, const pg_params& P, double* tab_base,
 void launch_init_xghosts(const DiskView& d, Cell* buf, cudaStream_t s);
 void launch_bound(const DiskView& d, Cell* buf, cudaStream_t s);
 void launch_cfl(const DiskView& d, const Cell* buf, cudaStream_t s, const pg_dust* dbuf = nullptr);
-void launch_set_time(const DiskView& d, double t, double dt, cudaStream_t s);
+void launch_set_time(const DiskView& d, double t, double dt, cudaStream_t s);  // the two below
+void launch_set_time_only(const DiskView& d, double t, double dt, cudaStream_t s);
+void launch_planet_trig(const DiskView& d, cudaStream_t s);
 void launch_time_step(const DiskView& d, cudaStream_t s);
 void launch_run_begin(Scalars* sc, double end_time, bool fresh, cudaStream_t s);
 void launch_kick1(const DiskView& d, const CellMaps& in, Cell* out, double* vis, cudaStream_t s,

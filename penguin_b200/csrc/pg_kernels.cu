@@ -1251,7 +1251,13 @@ void launch_cfl(const DiskView& d, const Cell* buf, cudaStream_t s, const pg_dus
 }
 
 void launch_set_time(const DiskView& d, double t, double dt, cudaStream_t s) {
+    launch_set_time_only(d, t, dt, s);
+    launch_planet_trig(d, s);
+}
+void launch_set_time_only(const DiskView& d, double t, double dt, cudaStream_t s) {
     k_set_time<<<1, 1, 0, s>>>(d, t, dt);
+}
+void launch_planet_trig(const DiskView& d, cudaStream_t s) {
     k_planet_trig<<<cdiv(d.yarr, 256), 256, 0, s>>>(d);
 }
 void launch_run_begin(Scalars* sc, double end_time, bool fresh, cudaStream_t s) {
