@@ -210,7 +210,10 @@ pg_status pg_disk_set_dust(pg_disk* d, const double* r, const double* u, const d
 pg_status pg_disk_get_dust(pg_disk* d, double* r, double* u, double* v);
 /* Device pointer of the newest AoS state (xarr*yarr pg_cell) and of the scratch. */
 pg_status pg_disk_state_ptr(pg_disk* d, pg_cell** cells);
-/* global_dt (blocking) and one step with host-supplied t, dt, as in main.cu. */
+/* global_dt (blocking) and one step with host-supplied t, dt, as in main.cu.
+   pg_disk_solve launches the step as one kernel taking t and dt and one CUDA
+   graph of the rest, captured on the disk's stream at the first call from
+   each of the two state buffers: call it outside a stream capture. */
 pg_status pg_disk_global_dt(pg_disk* d, double dt_prev, double* dt_out);
 pg_status pg_disk_solve(pg_disk* d, double t, double dt);
 /* main.cu's loop (main.cu:320-360) driven from the host, as pg_disk_global_dt and
